@@ -1,0 +1,31 @@
+"""Extract the reference's frozen b155550 trajectories into ``tests/golden/b155550.json``.
+
+Run once in a container where the reference tree is mounted:
+
+    python tests/golden/make_golden.py /root/reference
+
+It copies numbers only (S^z profiles, bond dimensions, statuses, errors against the exact answer,
+the discarded weight, norms and the no-symmetry final state) from
+``test/fixtures/b155550/{xx_u1_bug_order1,xx_u1_bug_order2,xx_none_bug_order2}.json``; the
+reference's regression test that reads them is ``test/BUG/TimeEvolution/test_fixtures_b155550.jl``.
+"""
+
+import json
+import pathlib
+import sys
+
+
+def main(ref_root: str) -> None:
+    src = pathlib.Path(ref_root) / "test" / "fixtures" / "b155550"
+    out = {"source": "test/fixtures/b155550", "versions": json.load(open(src / "versions.json"))}
+    for name in ("xx_u1_bug_order1", "xx_u1_bug_order2", "xx_none_bug_order2"):
+        d = json.load(open(src / f"{name}.json"))
+        d.pop("wall_s", None)
+        out[name] = d
+    dst = pathlib.Path(__file__).with_name("b155550.json")
+    dst.write_text(json.dumps(out, indent=1))
+    print("wrote", dst)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

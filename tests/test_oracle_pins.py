@@ -1,0 +1,144 @@
+"""Pins of the CPU oracle against the reference's own known answers and frozen runs.
+
+* Test A lists: ``test/BUG/Randomised/test_expansion.jl:15-88``.
+* The two-spin entangling step: ``test_expansion.jl:90-109``.
+* ``expv`` against sector-diagonal closed forms: ``test/BUG/Core/LocalSolvers/test_krylov.jl:21-168``.
+* The b155550 frozen trajectories, with the reference's own tolerances and settings
+  (``test/BUG/TimeEvolution/test_fixtures_b155550.jl:23-97``): S^z within 1e-5 of the frozen
+  profile and within ``2 err_exact + 1e-6`` of free fermions, status as frozen; the frozen runs used
+  ``work_ceiling_rule = :maxdim`` and the Arnoldi recurrence.
+"""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg
+
+from oracle import blocks as B
+from oracle import krylov as K
+from oracle import models as M
+from oracle import step as S
+from oracle.budget import tail_rank
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "b155550.json")))
+
+
+def mk(sig, degs=None):
+    degs = degs or [1] * len(sig)
+    return [(s, d, None, None) for s, d in zip(sig, degs)]
+
+
+def test_tail_rank_lists():
+    lst = mk([10.0, 9.0, 3.0, 0.1])
+    assert tail_rank(lst, 1.0, 1.0, 4)[0] == 3
+    assert tail_rank(lst, 1.0, 4.0, 4)[0] == 2
+    assert tail_rank(lst, 1.0, 9.6, 4)[0] == 1
+    assert tail_rank(lst, 1.0, 0.05, 4)[0] == 4
+    lst = mk([1.0, 1e-2, 1e-4, 1e-6])
+    k, tail = tail_rank(lst, 1.0, 2e-4, 4)
+    assert k == 2 and tail <= 2e-4
+    assert tail_rank(lst, 1.0, 5e-5, 4)[0] == 3
+    assert tail_rank(lst, 1.0, 2e-2, 4)[0] == 1
+    lst = mk([1.0, 0.5, 0.2, 0.05, 0.01, 1e-3])
+    ks = [tail_rank(lst, 1.0, a, 6)[0] for a in (1e-6, 1e-3, 1e-2, 0.1, 0.5, 2.0)]
+    assert ks == sorted(ks, reverse=True) and ks[0] == 6 and ks[-1] == 0
+    assert tail_rank(mk([1.0, 0.1]), 1.0, 0.5, 2)[0] == 1
+    assert tail_rank(mk([1.0, 0.1], [1, 100]), 1.0, 0.5, 2)[0] == 2
+    lst = mk([1.0, 1e-3])
+    assert tail_rank(lst, 1.0, 0.1, 2)[0] == 1
+    k, tail = tail_rank(lst, 1.0, 0.1, 2, base=0.25)
+    assert k == 2 and tail > 0.1
+    assert tail_rank(mk([1.0, 1e-2]), 1.0, 2e-2, 2)[0] == 1
+    assert tail_rank(mk([1.0, 1e-2]), 10.0, 2e-2, 2)[0] == 2
+    k, tail = tail_rank(mk([1.0] * 4), 1.0, 1e-12, 2)
+    assert k == 2 and tail > 1e-12
+    assert tail_rank(mk([]), 1.0, 1e-3, 4)[0] == 0
+    assert tail_rank(mk([1.0]), 1.0, 1e-3, 0)[0] == 0
+
+
+def test_two_spin_entangling_step():
+    mpo = M.xxz_mpo(2, J=1.0, delta=0.0)
+    psi = M.product_state(["up", "down"])
+    t = 0.3
+    info = S.cbe_bug_step(psi, mpo, -1j * t, tol_basis=1e-10, tol_trunc=1e-14, tol_expv=1e-13,
+                          maxdim=4)
+    v = M.mps_to_dense(psi)
+    v /= np.linalg.norm(v)
+    assert abs(abs(v[1]) - math.cos(t / 2)) < 1e-10
+    assert abs(abs(v[2]) - math.sin(t / 2)) < 1e-10
+    assert info["record"]["policy"] == "dd_qr_streamed"
+
+
+def _multi_sector():
+    rng = np.random.default_rng(7)
+    legs = [B.Leg(-1, {0: 2}), B.Leg(-1, {-1: 1, 1: 1}), B.Leg(+1, {-1: 3, 1: 2})]
+    blocks = {}
+    for qs in (-1, 1):
+        shape = (2, 1, legs[2].sectors[qs])
+        blocks[(0, qs, qs)] = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    return B.BT(legs, blocks)
+
+
+def _diag(x, scale):
+    return B.BT(x.legs, {k: scale(k[2]) * v for k, v in x.blocks.items()})
+
+
+@pytest.mark.parametrize("tau", [-0.4 + 0j, -0.7j, 0.25 + 0.3j])
+def test_expv_closed_form(tau):
+    x = _multi_sector()
+    scale = lambda q: 0.5 * q + 1.0
+    want = B.BT(x.legs, {k: np.exp(tau * scale(k[2])) * v for k, v in x.blocks.items()})
+    for herm in (True, False):
+        y, rep = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=herm)
+        assert B.norm(B.sub(y, want)) < 1e-11
+
+
+def test_arnoldi_terminates_at_true_krylov_dimension():
+    x = _multi_sector()
+    scale = lambda q: (0.5 * q + 1.0) + 0.3j * q
+    tau = -0.35 + 0j
+    want = B.BT(x.legs, {k: np.exp(tau * scale(k[2])) * v for k, v in x.blocks.items()})
+    y, rep = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=False, maxiter=60)
+    assert B.norm(B.sub(y, want)) < 1e-12
+    assert rep[0] == 2
+    y, rep = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=True, maxiter=60)
+    assert rep[0] == 60
+
+
+FROZEN = dict(work_ceiling_rule="maxdim", expansion=S.DDQRExpansion(krylov_mode="arnoldi"))
+
+
+@pytest.mark.parametrize("name,order", [("xx_u1_bug_order1", 1), ("xx_u1_bug_order2", 2)])
+def test_b155550_u1(name, order):
+    fz = GOLDEN[name]
+    L, dt = fz["L"], fz["dt"]
+    mpo = M.xxz_mpo(L, J=1.0, delta=0.0)
+    psi = M.neel_state(L)
+    rng = np.random.default_rng(1234)
+    for step, row in enumerate(fz["trajectory"][:3], start=1):
+        info = S.cbe_bug_step(psi, mpo, -1j * dt, order=order, rng=rng, **FROZEN)
+        sz = M.sz_profile(psi)
+        exact = M.free_fermion_sz(L, step * dt, occupied=range(0, L, 2))
+        assert np.max(np.abs(sz - np.array(row["sz"]))) <= 1e-5
+        assert np.max(np.abs(sz - exact)) <= 2 * row["err_exact"] + 1e-6
+        assert info["status"] == row["status"]
+
+
+def test_b155550_none():
+    fz = GOLDEN["xx_none_bug_order2"]
+    L, dt = fz["L"], fz["dt"]
+    mpo = M.xxz_mpo(L, J=1.0, delta=0.0, symmetry="none")
+    psi = M.neel_state(L, symmetry="none")
+    v0 = M.mps_to_dense(psi)
+    rng = np.random.default_rng(1234)
+    for row in fz["trajectory"][:3]:
+        info = S.cbe_bug_step(psi, mpo, -1j * dt, order=2, rng=rng, **FROZEN)
+        assert info["status"] == row["status"]
+        assert abs(B.norm(psi[psi.center]) - row["norm"]) <= 1e-8
+    H = M.dense_xxz(L, 1.0, 0.0)
+    ex = scipy.linalg.expm(-1j * 3 * dt * H) @ v0
+    err = np.linalg.norm(M.mps_to_dense(psi) - ex) / np.linalg.norm(ex)
+    assert err <= 2 * fz["err_dense"] + 1e-6
