@@ -1,0 +1,121 @@
+"""ctypes binding of ``libbug_b200.so`` (the C-ABI declared in ``include/bug_b200.h``).
+
+The library is built in-tree (``bondupdategalerkin_b200/build.py``) and loaded from this package
+directory. There is no fallback: if the library or a CUDA device is missing, ``context()`` raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbug_b200.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "bug_last_error": (ctypes.c_char_p, []),
+    "bug_version": (ctypes.c_char_p, []),
+    "bug_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp)]),
+    "bug_ctx_destroy": (ctypes.c_int, [_vp]),
+    "bug_ctx_synchronize": (ctypes.c_int, [_vp]),
+    "bug_ctx_launches": (ctypes.c_int64, [_vp]),
+    "bug_ctx_bytes_in_use": (ctypes.c_int64, [_vp]),
+    "bug_tensor_create": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p,
+                                         ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
+    "bug_tensor_upload": (ctypes.c_int, [_vp, _vp, _c_double_p, ctypes.c_int64]),
+    "bug_tensor_download": (ctypes.c_int, [_vp, _vp, _c_double_p, ctypes.c_int64]),
+    "bug_tensor_free": (ctypes.c_int, [_vp, _vp]),
+    "bug_tensor_shape": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_int64), _c_int_p]),
+    "bug_tensor_meta": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    "bug_contract": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, _vp, _c_int_p, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(_vp)]),
+    "bug_svd": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.c_double, ctypes.c_int,
+                               ctypes.POINTER(_vp), ctypes.POINTER(_vp), _c_double_p, _c_int_p,
+                               ctypes.c_int, _c_int_p, _c_int_p]),
+    "bug_scale_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_double_p, ctypes.POINTER(_vp)]),
+    "bug_norm2": (ctypes.c_int, [_vp, _vp, _c_double_p]),
+    "bug_inner": (ctypes.c_int, [_vp, _vp, _vp, _c_double_p]),
+    "bug_inner_many": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _vp, _c_double_p]),
+    "bug_lincomb": (ctypes.c_int, [_vp, ctypes.c_int, _c_double_p, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "bug_permute": (ctypes.c_int, [_vp, _vp, _c_int_p, ctypes.POINTER(_vp)]),
+    "bug_conj": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    "bug_flip_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "bug_oplus": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
+    "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
+}
+
+STATUS = {0: "BUG_OK", 1: "BUG_EINVAL", 2: "BUG_ENONFINITE", 3: "BUG_ENOMEM", 4: "BUG_ETIMEOUT",
+          5: "BUG_EDEVICE", 6: "BUG_ENOTCONV"}
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the engine library and declare every exported signature. Raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`"
+            )
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(code: int) -> None:
+    if code != 0:
+        raise EngineError(code, load().bug_last_error().decode(errors="replace"))
+
+
+class Context:
+    """One engine context (device + stream + memory pool)."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = _vp()
+        check(lib.bug_ctx_create(device, ctypes.byref(h)))
+        self.h = h
+        self.lib = lib
+        self.device = device
+
+    def synchronize(self):
+        check(self.lib.bug_ctx_synchronize(self.h))
+
+    def launches(self) -> int:
+        return int(self.lib.bug_ctx_launches(self.h))
+
+    def bytes_in_use(self) -> int:
+        return int(self.lib.bug_ctx_bytes_in_use(self.h))
+
+
+_ctx = {}
+
+
+def context(device: int = 0) -> Context:
+    """The process-wide context of ``device`` (created on first use)."""
+    c = _ctx.get(device)
+    if c is None:
+        c = Context(device)
+        _ctx[device] = c
+    return c

@@ -1,0 +1,1287 @@
+// Host side of the B200 block-sparse engine: tensor metadata, the contraction and SVD planners,
+// descriptor staging, and the C-ABI of include/bug_b200.h.
+//
+// A tensor keeps its block table on the host (sorted keys, shapes, offsets) and its payload in
+// one HBM allocation from the device's stream-ordered memory pool. Every operation plans on the
+// host from the block tables, ships one descriptor array per kernel through a pinned staging
+// ring, and launches a handful of kernels on the context stream; only operations whose result
+// the host must read (norms, inner products, singular values, downloads) synchronise.
+#include "../../include/bug_b200.h"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using bugk::CopyDesc;
+using bugk::DotDesc;
+using bugk::GemmOut;
+using bugk::GemmPair;
+using bugk::GemmTile;
+using bugk::LinOut;
+using bugk::LinSrc;
+using bugk::ScaleDesc;
+using bugk::SvdDesc;
+
+namespace {
+
+thread_local std::string g_err;
+
+struct BugError : std::runtime_error {
+  int code;
+  BugError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define BUG_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      throw BugError(e_ == cudaErrorMemoryAllocation ? BUG_ENOMEM : BUG_EDEVICE,         \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+inline void require(bool ok, const std::string& msg) {
+  if (!ok) throw BugError(BUG_EINVAL, msg);
+}
+
+using Key = std::array<int, BUG_MAX_RANK>;
+
+struct Leg {
+  int dir = 1;
+  std::vector<int> q;  // ascending charges
+  std::vector<int> d;  // dimensions
+  int dim_of(int c) const {
+    auto it = std::lower_bound(q.begin(), q.end(), c);
+    return (it != q.end() && *it == c) ? d[it - q.begin()] : 0;
+  }
+  int index_of(int c) const {
+    auto it = std::lower_bound(q.begin(), q.end(), c);
+    return (it != q.end() && *it == c) ? int(it - q.begin()) : -1;
+  }
+  int64_t total() const {
+    int64_t s = 0;
+    for (int x : d) s += x;
+    return s;
+  }
+};
+
+struct Block {
+  Key key{};
+  std::array<int, BUG_MAX_RANK> shape{};
+  int64_t off = 0;
+  int64_t size = 0;
+};
+
+}  // namespace
+
+struct bug_ctx;
+
+namespace {
+
+// The context whose scratch the current C-ABI call queued for release (freed, stream-ordered,
+// when the call returns).
+thread_local bug_ctx* g_active_ctx = nullptr;
+
+struct Buffer {
+  double2* ptr = nullptr;
+  int64_t n = 0;
+  bug_ctx* ctx = nullptr;
+  ~Buffer();
+};
+
+}  // namespace
+
+struct bug_tensor {
+  int rank = 0;
+  std::vector<Leg> legs;
+  std::vector<Block> blocks;  // ascending keys, payload laid out in this order
+  std::map<Key, int> index;
+  int64_t nelem = 0;
+  std::shared_ptr<Buffer> buf;
+
+  int find(const Key& k) const {
+    auto it = index.find(k);
+    return it == index.end() ? -1 : it->second;
+  }
+  const double2* data(int b) const { return buf->ptr + blocks[b].off; }
+  double2* mdata(int b) { return buf->ptr + blocks[b].off; }
+};
+
+struct bug_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  int64_t bytes = 0;
+  // pinned staging ring for descriptor uploads
+  static constexpr int kSlots = 32;
+  void* stage_ptr[kSlots] = {};
+  size_t stage_cap[kSlots] = {};
+  cudaEvent_t stage_ev[kSlots] = {};
+  bool stage_used[kSlots] = {};
+  int stage_next = 0;
+  std::vector<void*> deferred;  // device scratch to free after the next launch
+  double* pinned_out = nullptr;  // small pinned buffer for results read back by the host
+  size_t pinned_out_cap = 0;
+
+  void* stage(size_t bytes) {
+    int s = stage_next;
+    stage_next = (stage_next + 1) % kSlots;
+    if (stage_used[s]) BUG_CUDA(cudaEventSynchronize(stage_ev[s]));
+    if (stage_cap[s] < bytes) {
+      if (stage_ptr[s]) BUG_CUDA(cudaFreeHost(stage_ptr[s]));
+      size_t cap = std::max<size_t>(bytes, 1 << 16);
+      BUG_CUDA(cudaHostAlloc(&stage_ptr[s], cap, cudaHostAllocDefault));
+      stage_cap[s] = cap;
+    }
+    cur_slot = s;
+    return stage_ptr[s];
+  }
+  int cur_slot = 0;
+  void stage_done() {
+    BUG_CUDA(cudaEventRecord(stage_ev[cur_slot], stream));
+    stage_used[cur_slot] = true;
+  }
+  template <class T>
+  T* push(const std::vector<T>& v) {
+    size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+    void* h = stage(bytes);
+    if (!v.empty()) std::memcpy(h, v.data(), v.size() * sizeof(T));
+    void* dptr = nullptr;
+    BUG_CUDA(cudaMallocAsync(&dptr, bytes, stream));
+    BUG_CUDA(cudaMemcpyAsync(dptr, h, bytes, cudaMemcpyHostToDevice, stream));
+    stage_done();
+    deferred.push_back(dptr);
+    g_active_ctx = this;
+    return static_cast<T*>(dptr);
+  }
+  void* scratch(size_t bytes) {
+    void* dptr = nullptr;
+    BUG_CUDA(cudaMallocAsync(&dptr, std::max<size_t>(bytes, 16), stream));
+    deferred.push_back(dptr);
+    g_active_ctx = this;
+    return dptr;
+  }
+  void launched() {
+    ++launches;
+    BUG_CUDA(cudaGetLastError());
+  }
+  void flush() {
+    for (void* p : deferred) BUG_CUDA(cudaFreeAsync(p, stream));
+    deferred.clear();
+  }
+  double* readback(size_t n) {
+    if (pinned_out_cap < n) {
+      if (pinned_out) BUG_CUDA(cudaFreeHost(pinned_out));
+      pinned_out_cap = std::max<size_t>(n, 4096);
+      BUG_CUDA(cudaHostAlloc((void**)&pinned_out, pinned_out_cap * sizeof(double),
+                             cudaHostAllocDefault));
+    }
+    return pinned_out;
+  }
+};
+
+namespace {
+
+Buffer::~Buffer() {
+  if (ptr && ctx) {
+    cudaFreeAsync(ptr, ctx->stream);
+    ctx->bytes -= n * int64_t(sizeof(double2));
+  }
+}
+
+std::shared_ptr<Buffer> alloc_buffer(bug_ctx* c, int64_t n, bool zero) {
+  auto b = std::make_shared<Buffer>();
+  b->n = n;
+  b->ctx = c;
+  if (n > 0) {
+    BUG_CUDA(cudaMallocAsync((void**)&b->ptr, size_t(n) * sizeof(double2), c->stream));
+    if (zero) BUG_CUDA(cudaMemsetAsync(b->ptr, 0, size_t(n) * sizeof(double2), c->stream));
+    c->bytes += n * int64_t(sizeof(double2));
+  }
+  return b;
+}
+
+int64_t block_size(const bug_tensor& t, const Key& k, std::array<int, BUG_MAX_RANK>& shape) {
+  int64_t s = 1;
+  for (int l = 0; l < t.rank; ++l) {
+    int dd = t.legs[l].dim_of(k[l]);
+    require(dd > 0, "block key uses a charge its leg does not carry");
+    shape[l] = dd;
+    s *= dd;
+  }
+  for (int l = t.rank; l < BUG_MAX_RANK; ++l) shape[l] = 1;
+  return s;
+}
+
+// Finalise a tensor whose legs are set and whose keys are given (any order, no duplicates).
+std::unique_ptr<bug_tensor> make_tensor(bug_ctx* c, int rank, std::vector<Leg> legs,
+                                        std::vector<Key> keys, bool zero) {
+  auto t = std::make_unique<bug_tensor>();
+  t->rank = rank;
+  t->legs = std::move(legs);
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  int64_t off = 0;
+  for (auto& k : keys) {
+    int flux = 0;
+    for (int l = 0; l < rank; ++l) flux += t->legs[l].dir * k[l];
+    require(flux == 0, "block key violates charge conservation");
+    Block b;
+    b.key = k;
+    b.size = block_size(*t, k, b.shape);
+    b.off = off;
+    off += b.size;
+    t->index[k] = int(t->blocks.size());
+    t->blocks.push_back(b);
+  }
+  t->nelem = off;
+  t->buf = alloc_buffer(c, off, zero);
+  return t;
+}
+
+Leg flipped(const Leg& l) {
+  Leg o = l;
+  o.dir = -l.dir;
+  return o;
+}
+
+Leg merged(const Leg& a, const Leg& b) {
+  require(a.dir == b.dir, "leg arrows differ");
+  Leg o;
+  o.dir = a.dir;
+  std::map<int, int> m;
+  for (size_t i = 0; i < a.q.size(); ++i) m[a.q[i]] = a.d[i];
+  for (size_t i = 0; i < b.q.size(); ++i) {
+    auto it = m.find(b.q[i]);
+    if (it != m.end()) require(it->second == b.d[i], "sector dimensions differ");
+    m[b.q[i]] = b.d[i];
+  }
+  for (auto& kv : m) {
+    o.q.push_back(kv.first);
+    o.d.push_back(kv.second);
+  }
+  return o;
+}
+
+std::array<int64_t, BUG_MAX_RANK> c_strides(const std::array<int, BUG_MAX_RANK>& shape, int rank) {
+  std::array<int64_t, BUG_MAX_RANK> s{};
+  int64_t acc = 1;
+  for (int l = rank - 1; l >= 0; --l) {
+    s[l] = acc;
+    acc *= shape[l];
+  }
+  return s;
+}
+
+void run_copies(bug_ctx* c, std::vector<CopyDesc>& descs) {
+  std::vector<CopyDesc> nz;
+  nz.reserve(descs.size());
+  int64_t total = 0;
+  for (auto& d : descs) {
+    if (d.n <= 0) continue;
+    d.prefix = total;
+    total += d.n;
+    nz.push_back(d);
+  }
+  if (nz.empty()) return;
+  CopyDesc* dd = c->push(nz);
+  bugk::launch_copy(dd, int(nz.size()), total, c->stream);
+  c->launched();
+}
+
+CopyDesc plain_copy(const double2* src, double2* dst, int64_t n, bool conj, double2 alpha,
+                    bool acc) {
+  CopyDesc d{};
+  d.src = src;
+  d.dst = dst;
+  d.n = n;
+  d.ndim = 1;
+  d.dims[0] = int(n);
+  d.sstr[0] = 1;
+  d.dstr[0] = 1;
+  d.conj = conj;
+  d.alpha = alpha;
+  d.accumulate = acc;
+  return d;
+}
+
+// Permuted copy: the result has legs perm[0..r) of t.
+std::unique_ptr<bug_tensor> permute_impl(bug_ctx* c, const bug_tensor& t, const int* perm) {
+  std::vector<Leg> legs(t.rank);
+  std::vector<bool> seen(t.rank, false);
+  for (int i = 0; i < t.rank; ++i) {
+    require(perm[i] >= 0 && perm[i] < t.rank && !seen[perm[i]], "bad permutation");
+    seen[perm[i]] = true;
+    legs[i] = t.legs[perm[i]];
+  }
+  std::vector<Key> keys;
+  for (auto& b : t.blocks) {
+    Key k{};
+    for (int i = 0; i < t.rank; ++i) k[i] = b.key[perm[i]];
+    keys.push_back(k);
+  }
+  auto out = make_tensor(c, t.rank, legs, keys, false);
+  std::vector<CopyDesc> descs;
+  for (auto& b : t.blocks) {
+    Key k{};
+    for (int i = 0; i < t.rank; ++i) k[i] = b.key[perm[i]];
+    const Block& ob = out->blocks[out->find(k)];
+    auto ss = c_strides(b.shape, t.rank);
+    auto ds = c_strides(ob.shape, t.rank);
+    CopyDesc d{};
+    d.src = t.data(&b - &t.blocks[0]);
+    d.dst = out->mdata(out->find(k));
+    d.n = b.size;
+    d.ndim = t.rank;
+    for (int i = 0; i < t.rank; ++i) {
+      d.dims[i] = ob.shape[i];
+      d.sstr[i] = ss[perm[i]];
+      d.dstr[i] = ds[i];
+    }
+    d.alpha = make_double2(1.0, 0.0);
+    descs.push_back(d);
+  }
+  run_copies(c, descs);
+  return out;
+}
+
+// ── contraction ──────────────────────────────────────────────────────────────────────────────
+
+std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int n, const int* ia,
+                                          const bug_tensor& B0, const int* ib, bool conja,
+                                          bool conjb) {
+  require(n >= 0 && n <= A0.rank && n <= B0.rank, "bad contraction arity");
+  std::vector<bool> ca(A0.rank, false), cb(B0.rank, false);
+  for (int k = 0; k < n; ++k) {
+    require(ia[k] >= 0 && ia[k] < A0.rank && !ca[ia[k]], "bad contracted leg of A");
+    require(ib[k] >= 0 && ib[k] < B0.rank && !cb[ib[k]], "bad contracted leg of B");
+    ca[ia[k]] = true;
+    cb[ib[k]] = true;
+    const Leg& la = A0.legs[ia[k]];
+    const Leg& lb = B0.legs[ib[k]];
+    int da = conja ? -la.dir : la.dir, db = conjb ? -lb.dir : lb.dir;
+    require(da == -db, "contract: paired legs must have opposite arrows");
+    for (size_t i = 0; i < la.q.size(); ++i) {
+      int dbb = lb.dim_of(la.q[i]);
+      require(dbb == 0 || dbb == la.d[i], "contract: sector dimensions differ");
+    }
+  }
+  std::vector<int> fa, fb;
+  for (int i = 0; i < A0.rank; ++i)
+    if (!ca[i]) fa.push_back(i);
+  for (int i = 0; i < B0.rank; ++i)
+    if (!cb[i]) fb.push_back(i);
+  const int ro = int(fa.size() + fb.size());
+  require(ro <= BUG_MAX_RANK, "result rank exceeds the engine limit");
+  std::vector<Leg> legs;
+  for (int i : fa) legs.push_back(conja ? flipped(A0.legs[i]) : A0.legs[i]);
+  for (int i : fb) legs.push_back(conjb ? flipped(B0.legs[i]) : B0.legs[i]);
+
+  // operand layouts: contracted legs trailing (N) or leading (T), else permute
+  bool a_tail = true, a_head = true, b_tail = true, b_head = true;
+  for (int k = 0; k < n; ++k) {
+    if (ia[k] != A0.rank - n + k) a_tail = false;
+    if (ia[k] != k) a_head = false;
+    if (ib[k] != B0.rank - n + k) b_tail = false;
+    if (ib[k] != k) b_head = false;
+  }
+  std::unique_ptr<bug_tensor> Ap, Bp;
+  const bug_tensor* A = &A0;
+  const bug_tensor* B = &B0;
+  int opa = 0, opb = 0;  // bit0: transposed storage
+  std::vector<int> iaa(ia, ia + n), ibb(ib, ib + n);
+  if (n == 0) {
+    opa = 0;
+    opb = 0;
+  } else {
+    if (a_tail) opa = 0;
+    else if (a_head) opa = 1;
+    else {
+      std::vector<int> perm(fa);
+      for (int k = 0; k < n; ++k) perm.push_back(ia[k]);
+      Ap = permute_impl(c, A0, perm.data());
+      A = Ap.get();
+      for (int k = 0; k < n; ++k) iaa[k] = int(fa.size()) + k;
+      opa = 0;
+    }
+    if (b_head) opb = 0;
+    else if (b_tail) opb = 1;
+    else {
+      std::vector<int> perm(ib, ib + n);
+      for (int i : fb) perm.push_back(i);
+      Bp = permute_impl(c, B0, perm.data());
+      B = Bp.get();
+      for (int k = 0; k < n; ++k) ibb[k] = k;
+      opb = 0;
+    }
+  }
+  // free-leg positions in the (possibly permuted) operands
+  std::vector<int> fa2, fb2;
+  {
+    std::vector<bool> c2(A->rank, false);
+    for (int k = 0; k < n; ++k) c2[iaa[k]] = true;
+    for (int i = 0; i < A->rank; ++i)
+      if (!c2[i]) fa2.push_back(i);
+    std::vector<bool> d2(B->rank, false);
+    for (int k = 0; k < n; ++k) d2[ibb[k]] = true;
+    for (int i = 0; i < B->rank; ++i)
+      if (!d2[i]) fb2.push_back(i);
+  }
+  // match blocks
+  std::map<std::vector<int>, std::vector<int>> groups;
+  for (int bi = 0; bi < int(B->blocks.size()); ++bi) {
+    std::vector<int> ck(n);
+    for (int k = 0; k < n; ++k) ck[k] = B->blocks[bi].key[ibb[k]];
+    groups[ck].push_back(bi);
+  }
+  std::map<Key, std::vector<std::pair<int, int>>> outmap;
+  for (int ai = 0; ai < int(A->blocks.size()); ++ai) {
+    std::vector<int> ck(n);
+    for (int k = 0; k < n; ++k) ck[k] = A->blocks[ai].key[iaa[k]];
+    auto it = groups.find(ck);
+    if (it == groups.end()) continue;
+    for (int bi : it->second) {
+      Key ok{};
+      int p = 0;
+      for (int i : fa2) ok[p++] = A->blocks[ai].key[i];
+      for (int i : fb2) ok[p++] = B->blocks[bi].key[i];
+      outmap[ok].push_back({ai, bi});
+    }
+  }
+  std::vector<Key> keys;
+  for (auto& kv : outmap) keys.push_back(kv.first);
+  auto out = make_tensor(c, ro, legs, keys, false);
+  if (keys.empty()) return out;
+  std::vector<GemmOut> outs;
+  std::vector<GemmPair> pairs;
+  std::vector<GemmTile> tiles;
+  for (auto& kv : outmap) {
+    int oj = out->find(kv.first);
+    const Block& ob = out->blocks[oj];
+    GemmOut go{};
+    go.C = out->mdata(oj);
+    int64_t m = 1, nn = 1;
+    for (size_t i = 0; i < fa2.size(); ++i) m *= ob.shape[i];
+    for (size_t i = 0; i < fb2.size(); ++i) nn *= ob.shape[fa2.size() + i];
+    go.m = int(m);
+    go.n = int(nn);
+    go.pair_begin = int(pairs.size());
+    for (auto& pr : kv.second) {
+      const Block& ab = A->blocks[pr.first];
+      const Block& bb = B->blocks[pr.second];
+      int64_t K = 1;
+      for (int k = 0; k < n; ++k) K *= ab.shape[iaa[k]];
+      GemmPair gp{};
+      gp.A = A->data(pr.first);
+      gp.B = B->data(pr.second);
+      gp.k = int(K);
+      gp.lda = (opa & 1) ? int(m) : int(K);
+      gp.ldb = (opb & 1) ? int(K) : int(nn);
+      gp.opa = opa | (conja ? 2 : 0);
+      gp.opb = opb | (conjb ? 2 : 0);
+      pairs.push_back(gp);
+    }
+    go.pair_end = int(pairs.size());
+    int o = int(outs.size());
+    outs.push_back(go);
+    for (int tm = 0; tm * 32 < m; ++tm)
+      for (int tn = 0; tn * 32 < nn; ++tn) tiles.push_back(GemmTile{o, tm, tn});
+  }
+  GemmOut* d_outs = c->push(outs);
+  GemmPair* d_pairs = c->push(pairs);
+  GemmTile* d_tiles = c->push(tiles);
+  bugk::launch_gemm(d_outs, d_pairs, d_tiles, int(tiles.size()), c->stream);
+  c->launched();
+  return out;  // Ap/Bp are released stream-ordered
+}
+
+// ── SVD ──────────────────────────────────────────────────────────────────────────────────────
+
+struct SectorPlan {
+  int charge;
+  std::vector<std::vector<int>> rows, cols;  // left / right charge tuples
+  std::vector<int64_t> rdim, cdim, roff, coff;
+  int64_t m = 0, n = 0;
+};
+
+int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
+             std::unique_ptr<bug_tensor>& U, std::unique_ptr<bug_tensor>& Vd,
+             std::vector<double>& sv_sorted, std::vector<int>& sv_q, int& nkept) {
+  require(nleft >= 0 && nleft <= t.rank, "bad split");
+  std::vector<bool> isl(t.rank, false);
+  std::vector<int> L(left, left + nleft), R;
+  for (int i : L) {
+    require(i >= 0 && i < t.rank && !isl[i], "bad left leg");
+    isl[i] = true;
+  }
+  for (int i = 0; i < t.rank; ++i)
+    if (!isl[i]) R.push_back(i);
+  std::map<int, SectorPlan> plans;
+  for (auto& b : t.blocks) {
+    int cq = 0;
+    for (int i : L) cq -= t.legs[i].dir * b.key[i];
+    std::vector<int> rk, ck;
+    for (int i : L) rk.push_back(b.key[i]);
+    for (int i : R) ck.push_back(b.key[i]);
+    auto& p = plans[cq];
+    p.charge = cq;
+    p.rows.push_back(rk);
+    p.cols.push_back(ck);
+  }
+  std::vector<SectorPlan*> order;
+  for (auto& kv : plans) {
+    auto& p = kv.second;
+    std::sort(p.rows.begin(), p.rows.end());
+    p.rows.erase(std::unique(p.rows.begin(), p.rows.end()), p.rows.end());
+    std::sort(p.cols.begin(), p.cols.end());
+    p.cols.erase(std::unique(p.cols.begin(), p.cols.end()), p.cols.end());
+    for (auto& rk : p.rows) {
+      int64_t s = 1;
+      for (size_t j = 0; j < L.size(); ++j) s *= t.legs[L[j]].dim_of(rk[j]);
+      p.roff.push_back(p.m);
+      p.rdim.push_back(s);
+      p.m += s;
+    }
+    for (auto& ck : p.cols) {
+      int64_t s = 1;
+      for (size_t j = 0; j < R.size(); ++j) s *= t.legs[R[j]].dim_of(ck[j]);
+      p.coff.push_back(p.n);
+      p.cdim.push_back(s);
+      p.n += s;
+    }
+    order.push_back(&p);
+  }
+  const int np = int(order.size());
+  // workspace per sector: work (mm*r), vwork (r*r), U (m*r), V (n*r), S (r)
+  std::vector<int64_t> woff(np), vwoff(np), uoff(np), voff(np), soff(np);
+  int64_t wtot = 0, stot = 0;
+  for (int s = 0; s < np; ++s) {
+    auto& p = *order[s];
+    int64_t mm = std::max(p.m, p.n), r = std::min(p.m, p.n);
+    require(r <= 1024, "SVD sector wider than the engine's 1024-column limit");
+    woff[s] = wtot;
+    wtot += mm * r;
+    vwoff[s] = wtot;
+    wtot += r * r;
+    uoff[s] = wtot;
+    wtot += p.m * r;
+    voff[s] = wtot;
+    wtot += p.n * r;
+    soff[s] = stot;
+    stot += r;
+  }
+  double2* W = static_cast<double2*>(c->scratch(size_t(wtot) * sizeof(double2)));
+  double* S = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
+  int* sweeps = static_cast<int*>(c->scratch(size_t(std::max(np, 1)) * sizeof(int)));
+  // pack sector matrices (column-major M, or M^H when m < n)
+  std::vector<CopyDesc> descs;
+  for (int bi = 0; bi < int(t.blocks.size()); ++bi) {
+    const Block& b = t.blocks[bi];
+    int cq = 0;
+    for (int i : L) cq -= t.legs[i].dir * b.key[i];
+    auto& p = plans[cq];
+    int s = int(std::find(order.begin(), order.end(), &p) - order.begin());
+    std::vector<int> rk, ck;
+    for (int i : L) rk.push_back(b.key[i]);
+    for (int i : R) ck.push_back(b.key[i]);
+    int ri = int(std::lower_bound(p.rows.begin(), p.rows.end(), rk) - p.rows.begin());
+    int ci = int(std::lower_bound(p.cols.begin(), p.cols.end(), ck) - p.cols.begin());
+    const bool trans = p.m < p.n;
+    auto ss = c_strides(b.shape, t.rank);
+    CopyDesc d{};
+    d.src = t.data(bi);
+    d.dst = W + woff[s];
+    d.n = b.size;
+    d.ndim = t.rank;
+    d.conj = trans ? 1 : 0;
+    d.alpha = make_double2(1.0, 0.0);
+    // element multi-index in (L..., R...) order; row = C-order over L dims, col over R dims
+    int p_i = 0;
+    int64_t rs = 1, cs = 1;
+    std::array<int64_t, BUG_MAX_RANK> rstr{}, cstr{};
+    for (int j = int(L.size()) - 1; j >= 0; --j) {
+      rstr[j] = rs;
+      rs *= b.shape[L[j]];
+    }
+    for (int j = int(R.size()) - 1; j >= 0; --j) {
+      cstr[j] = cs;
+      cs *= b.shape[R[j]];
+    }
+    const int64_t ldw = trans ? p.n : p.m;  // leading dimension of the column-major work
+    for (size_t j = 0; j < L.size(); ++j, ++p_i) {
+      d.dims[p_i] = b.shape[L[j]];
+      d.sstr[p_i] = ss[L[j]];
+      d.dstr[p_i] = trans ? rstr[j] * ldw : rstr[j];
+    }
+    for (size_t j = 0; j < R.size(); ++j, ++p_i) {
+      d.dims[p_i] = b.shape[R[j]];
+      d.sstr[p_i] = ss[R[j]];
+      d.dstr[p_i] = trans ? cstr[j] : cstr[j] * ldw;
+    }
+    const int64_t base = trans ? (p.coff[ci] + p.roff[ri] * ldw) : (p.roff[ri] + p.coff[ci] * ldw);
+    d.dst = W + woff[s] + base;
+    descs.push_back(d);
+  }
+  run_copies(c, descs);
+  // launch Jacobi
+  std::vector<SvdDesc> sd(np);
+  int max_smem = 0;
+  for (int s = 0; s < np; ++s) {
+    auto& p = *order[s];
+    int64_t mm = std::max(p.m, p.n), r = std::min(p.m, p.n);
+    SvdDesc& d = sd[s];
+    d.work = W + woff[s];
+    d.vwork = W + vwoff[s];
+    d.U = W + uoff[s];
+    d.V = W + voff[s];
+    d.S = S + soff[s];
+    d.sweeps = sweeps + s;
+    d.m = int(p.m);
+    d.n = int(p.n);
+    d.trans = p.m < p.n ? 1 : 0;
+    int64_t bytes = (mm * r + r * r) * int64_t(sizeof(double2));
+    d.use_smem = bytes <= 200 * 1024 ? 1 : 0;
+    if (d.use_smem) max_smem = std::max<int>(max_smem, int(bytes));
+  }
+  if (np > 0) {
+    SvdDesc* dsd = c->push(sd);
+    bugk::launch_svd(dsd, np, max_smem, c->stream);
+    c->launched();
+  }
+  // read back singular values and sweep counts
+  const size_t nread = size_t(stot) + size_t(np);
+  double* host = c->readback(std::max<size_t>(nread, 1));
+  if (stot > 0) BUG_CUDA(cudaMemcpyAsync(host, S, size_t(stot) * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c->stream));
+  std::vector<int> hsweeps(np);
+  if (np > 0) BUG_CUDA(cudaMemcpyAsync(host + stot, sweeps, size_t(np) * sizeof(int),
+                                      cudaMemcpyDeviceToHost, c->stream));
+  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  if (np > 0) std::memcpy(hsweeps.data(), host + stot, size_t(np) * sizeof(int));
+  for (int s = 0; s < np; ++s)
+    if (hsweeps[s] < 0) {
+      throw BugError(BUG_ENOTCONV, "Jacobi SVD did not converge within its sweep bound");
+    }
+  // selection (Telum): sigma > cutoff*smax, stable descending sort, Nkeep
+  struct Entry {
+    double sv;
+    int s, j;
+  };
+  std::vector<Entry> entries;
+  double smax = 0.0;
+  for (int s = 0; s < np; ++s) {
+    int64_t r = std::min(order[s]->m, order[s]->n);
+    for (int j = 0; j < r; ++j) {
+      double v = host[soff[s] + j];
+      require(std::isfinite(v), "non-finite singular value");
+      smax = std::max(smax, v);
+      entries.push_back({v, s, j});
+    }
+  }
+  std::stable_sort(entries.begin(), entries.end(),
+                   [](const Entry& a, const Entry& b) { return a.sv > b.sv; });
+  const double thresh = cutoff * smax;
+  int nsel = 0;
+  for (auto& e : entries)
+    if (e.sv > thresh) ++nsel;
+  if (nkeep >= 0) nsel = std::min(nsel, nkeep);
+  std::vector<int> kc(np, 0);
+  for (int i = 0; i < nsel; ++i) kc[entries[i].s]++;
+  sv_sorted.clear();
+  sv_q.clear();
+  for (auto& e : entries) {
+    sv_sorted.push_back(e.sv);
+    sv_q.push_back(order[e.s]->charge);
+  }
+  nkept = nsel;
+  // build U and Vd
+  Leg bondU, bondV;
+  bondU.dir = +1;
+  bondV.dir = -1;
+  for (int s = 0; s < np; ++s)
+    if (kc[s] > 0) {
+      bondU.q.push_back(order[s]->charge);
+      bondU.d.push_back(kc[s]);
+    }
+  bondV.q = bondU.q;
+  bondV.d = bondU.d;
+  std::vector<Leg> ulegs, vlegs;
+  for (int i : L) ulegs.push_back(t.legs[i]);
+  ulegs.push_back(bondU);
+  vlegs.push_back(bondV);
+  for (int i : R) vlegs.push_back(t.legs[i]);
+  std::vector<Key> ukeys, vkeys;
+  for (int s = 0; s < np; ++s) {
+    if (kc[s] == 0) continue;
+    auto& p = *order[s];
+    for (auto& rk : p.rows) {
+      Key k{};
+      for (size_t j = 0; j < rk.size(); ++j) k[j] = rk[j];
+      k[rk.size()] = p.charge;
+      ukeys.push_back(k);
+    }
+    for (auto& ck : p.cols) {
+      Key k{};
+      k[0] = p.charge;
+      for (size_t j = 0; j < ck.size(); ++j) k[j + 1] = ck[j];
+      vkeys.push_back(k);
+    }
+  }
+  U = make_tensor(c, int(L.size()) + 1, ulegs, ukeys, false);
+  Vd = make_tensor(c, int(R.size()) + 1, vlegs, vkeys, false);
+  std::vector<CopyDesc> out;
+  for (int s = 0; s < np; ++s) {
+    if (kc[s] == 0) continue;
+    auto& p = *order[s];
+    for (size_t ri = 0; ri < p.rows.size(); ++ri) {
+      Key k{};
+      for (size_t j = 0; j < p.rows[ri].size(); ++j) k[j] = p.rows[ri][j];
+      k[p.rows[ri].size()] = p.charge;
+      int ub = U->find(k);
+      CopyDesc d{};
+      d.src = W + uoff[s] + p.roff[ri];
+      d.dst = U->mdata(ub);
+      d.n = p.rdim[ri] * kc[s];
+      d.ndim = 2;
+      d.dims[0] = int(p.rdim[ri]);
+      d.dims[1] = kc[s];
+      d.sstr[0] = 1;
+      d.sstr[1] = p.m;
+      d.dstr[0] = kc[s];
+      d.dstr[1] = 1;
+      d.alpha = make_double2(1.0, 0.0);
+      out.push_back(d);
+    }
+    for (size_t ci = 0; ci < p.cols.size(); ++ci) {
+      Key k{};
+      k[0] = p.charge;
+      for (size_t j = 0; j < p.cols[ci].size(); ++j) k[j + 1] = p.cols[ci][j];
+      int vb = Vd->find(k);
+      CopyDesc d{};
+      d.src = W + voff[s] + p.coff[ci];
+      d.dst = Vd->mdata(vb);
+      d.n = p.cdim[ci] * kc[s];
+      d.ndim = 2;
+      d.dims[0] = kc[s];
+      d.dims[1] = int(p.cdim[ci]);
+      d.sstr[0] = p.n;
+      d.sstr[1] = 1;
+      d.dstr[0] = p.cdim[ci];
+      d.dstr[1] = 1;
+      d.conj = 1;
+      d.alpha = make_double2(1.0, 0.0);
+      out.push_back(d);
+    }
+  }
+  run_copies(c, out);
+  return BUG_OK;
+}
+
+// ── reductions and linear combinations ───────────────────────────────────────────────────────
+
+constexpr int64_t kDotChunk = 16384;
+
+void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
+          double* out_re_im) {
+  std::vector<DotDesc> descs;
+  std::vector<int> seg(pairs.size() + 1, 0);
+  for (size_t o = 0; o < pairs.size(); ++o) {
+    seg[o] = int(descs.size());
+    const bug_tensor& a = *pairs[o].first;
+    const bug_tensor& b = *pairs[o].second;
+    for (int ai = 0; ai < int(a.blocks.size()); ++ai) {
+      int bi = b.find(a.blocks[ai].key);
+      if (bi < 0) continue;
+      require(a.blocks[ai].size == b.blocks[bi].size, "inner: block shapes differ");
+      for (int64_t s = 0; s < a.blocks[ai].size; s += kDotChunk) {
+        DotDesc d{};
+        d.a = a.data(ai) + s;
+        d.b = b.data(bi) + s;
+        d.n = std::min(kDotChunk, a.blocks[ai].size - s);
+        d.out = int(o);
+        descs.push_back(d);
+      }
+    }
+  }
+  seg[pairs.size()] = int(descs.size());
+  const int nout = int(pairs.size());
+  double2* partial = static_cast<double2*>(c->scratch(std::max<size_t>(descs.size(), 1) * sizeof(double2)));
+  double2* res = static_cast<double2*>(c->scratch(std::max(nout, 1) * sizeof(double2)));
+  if (!descs.empty()) {
+    DotDesc* dd = c->push(descs);
+    bugk::launch_dot(dd, int(descs.size()), partial, c->stream);
+    c->launched();
+  }
+  int* dseg = c->push(seg);
+  bugk::launch_dot_reduce(partial, dseg, nout, res, c->stream);
+  c->launched();
+  double* host = c->readback(size_t(2 * std::max(nout, 1)));
+  BUG_CUDA(cudaMemcpyAsync(host, res, size_t(nout) * sizeof(double2), cudaMemcpyDeviceToHost,
+                           c->stream));
+  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  std::memcpy(out_re_im, host, size_t(nout) * sizeof(double2));
+}
+
+std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
+                                         const bug_tensor* const* ts) {
+  require(n >= 1, "lincomb needs at least one tensor");
+  const int rank = ts[0]->rank;
+  std::vector<Leg> legs = ts[0]->legs;
+  for (int i = 1; i < n; ++i) {
+    require(ts[i]->rank == rank, "lincomb: ranks differ");
+    for (int l = 0; l < rank; ++l) legs[l] = merged(legs[l], ts[i]->legs[l]);
+  }
+  std::vector<Key> keys;
+  for (int i = 0; i < n; ++i)
+    for (auto& b : ts[i]->blocks) keys.push_back(b.key);
+  auto out = make_tensor(c, rank, legs, keys, false);
+  std::vector<LinOut> outs;
+  std::vector<LinSrc> srcs;
+  int64_t total = 0;
+  for (int j = 0; j < int(out->blocks.size()); ++j) {
+    LinOut o{};
+    o.dst = out->mdata(j);
+    o.n = out->blocks[j].size;
+    o.prefix = total;
+    total += o.n;
+    o.src_begin = int(srcs.size());
+    for (int i = 0; i < n; ++i) {
+      int b = ts[i]->find(out->blocks[j].key);
+      if (b < 0) continue;
+      srcs.push_back(LinSrc{ts[i]->data(b), make_double2(coef[2 * i], coef[2 * i + 1])});
+    }
+    o.src_end = int(srcs.size());
+    outs.push_back(o);
+  }
+  if (!outs.empty()) {
+    LinOut* dout = c->push(outs);
+    LinSrc* dsrc = c->push(srcs);
+    bugk::launch_lincomb(dout, int(outs.size()), dsrc, total, c->stream);
+    c->launched();
+  }
+  return out;
+}
+
+}  // namespace
+
+namespace {
+int guard(const std::function<void()>& f) {
+  struct Flush {
+    ~Flush() {
+      if (bug_ctx* c = g_active_ctx) {
+        for (void* p : c->deferred) cudaFreeAsync(p, c->stream);
+        c->deferred.clear();
+      }
+      g_active_ctx = nullptr;
+    }
+  } fl;
+  try {
+    f();
+    return BUG_OK;
+  } catch (const BugError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return BUG_ENOMEM;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return BUG_EINVAL;
+  }
+}
+}  // namespace
+
+// ── C-ABI ────────────────────────────────────────────────────────────────────────────────────
+
+extern "C" {
+
+const char* bug_last_error(void) { return g_err.c_str(); }
+const char* bug_version(void) { return "bug_b200 0.1 (sm_100a, complex FP64)"; }
+
+int bug_ctx_create(int device, bug_ctx** out) {
+  return guard([&] {
+    require(out != nullptr, "null output");
+    int count = 0;
+    BUG_CUDA(cudaGetDeviceCount(&count));
+    require(device >= 0 && device < count, "no such CUDA device");
+    BUG_CUDA(cudaSetDevice(device));
+    auto c = std::make_unique<bug_ctx>();
+    c->device = device;
+    BUG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < bug_ctx::kSlots; ++i)
+      BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
+    cudaMemPool_t pool;
+    BUG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    BUG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    *out = c.release();
+  });
+}
+
+int bug_ctx_destroy(bug_ctx* c) {
+  return guard([&] {
+    if (!c) return;
+    cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < bug_ctx::kSlots; ++i) {
+      if (c->stage_ptr[i]) cudaFreeHost(c->stage_ptr[i]);
+      cudaEventDestroy(c->stage_ev[i]);
+    }
+    if (c->pinned_out) cudaFreeHost(c->pinned_out);
+    cudaStreamDestroy(c->stream);
+    delete c;
+  });
+}
+
+int bug_ctx_synchronize(bug_ctx* c) {
+  return guard([&] { BUG_CUDA(cudaStreamSynchronize(c->stream)); });
+}
+
+int64_t bug_ctx_launches(const bug_ctx* c) { return c ? c->launches : 0; }
+int64_t bug_ctx_bytes_in_use(const bug_ctx* c) { return c ? c->bytes : 0; }
+
+int bug_tensor_create(bug_ctx* c, int rank, const int* dirs, const int* nsec, const int* charges,
+                      const int* dims, int nblocks, const int* keys, bug_tensor** out) {
+  return guard([&] {
+    require(c && out, "null argument");
+    require(rank >= 0 && rank <= BUG_MAX_RANK, "rank out of range");
+    std::vector<Leg> legs(rank);
+    int p = 0;
+    for (int l = 0; l < rank; ++l) {
+      require(dirs[l] == 1 || dirs[l] == -1, "leg arrow must be +1 or -1");
+      legs[l].dir = dirs[l];
+      for (int s = 0; s < nsec[l]; ++s, ++p) {
+        require(dims[p] > 0, "sector dimension must be positive");
+        require(legs[l].q.empty() || charges[p] > legs[l].q.back(), "sector charges must ascend");
+        legs[l].q.push_back(charges[p]);
+        legs[l].d.push_back(dims[p]);
+      }
+    }
+    std::vector<Key> ks(nblocks);
+    for (int b = 0; b < nblocks; ++b) {
+      Key k{};
+      for (int l = 0; l < rank; ++l) k[l] = keys[b * rank + l];
+      ks[b] = k;
+    }
+    auto t = make_tensor(c, rank, legs, ks, true);
+    require(int(t->blocks.size()) == nblocks, "duplicate block keys");
+    *out = t.release();
+  });
+}
+
+int bug_tensor_upload(bug_ctx* c, bug_tensor* t, const double* host, int64_t nelem) {
+  return guard([&] {
+    require(c && t, "null argument");
+    require(nelem == t->nelem, "upload: element count mismatch");
+    if (nelem > 0)
+      BUG_CUDA(cudaMemcpyAsync(t->buf->ptr, host, size_t(nelem) * sizeof(double2),
+                               cudaMemcpyHostToDevice, c->stream));
+    BUG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int bug_tensor_download(bug_ctx* c, const bug_tensor* t, double* host, int64_t nelem) {
+  return guard([&] {
+    require(c && t, "null argument");
+    require(nelem == t->nelem, "download: element count mismatch");
+    if (nelem > 0)
+      BUG_CUDA(cudaMemcpyAsync(host, t->buf->ptr, size_t(nelem) * sizeof(double2),
+                               cudaMemcpyDeviceToHost, c->stream));
+    BUG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int bug_tensor_free(bug_ctx* c, bug_tensor* t) {
+  return guard([&] { delete t; });
+}
+
+int bug_tensor_shape(const bug_tensor* t, int* rank, int* nblocks, int64_t* nelem,
+                     int* total_sectors) {
+  return guard([&] {
+    require(t != nullptr, "null tensor");
+    *rank = t->rank;
+    *nblocks = int(t->blocks.size());
+    *nelem = t->nelem;
+    int s = 0;
+    for (auto& l : t->legs) s += int(l.q.size());
+    *total_sectors = s;
+  });
+}
+
+int bug_tensor_meta(const bug_tensor* t, int* dirs, int* nsec, int* charges, int* dims, int* keys) {
+  return guard([&] {
+    int p = 0;
+    for (int l = 0; l < t->rank; ++l) {
+      dirs[l] = t->legs[l].dir;
+      nsec[l] = int(t->legs[l].q.size());
+      for (size_t s = 0; s < t->legs[l].q.size(); ++s, ++p) {
+        charges[p] = t->legs[l].q[s];
+        dims[p] = t->legs[l].d[s];
+      }
+    }
+    for (size_t b = 0; b < t->blocks.size(); ++b)
+      for (int l = 0; l < t->rank; ++l) keys[b * t->rank + l] = t->blocks[b].key[l];
+  });
+}
+
+int bug_contract(bug_ctx* c, const bug_tensor* a, int n, const int* ia, const bug_tensor* b,
+                 const int* ib, int conja, int conjb, bug_tensor** out) {
+  return guard([&] {
+    require(c && a && b && out, "null argument");
+    *out = contract_impl(c, *a, n, ia, *b, ib, conja != 0, conjb != 0).release();
+  });
+}
+
+int bug_svd(bug_ctx* c, const bug_tensor* t, int nleft, const int* left, double cutoff, int nkeep,
+            bug_tensor** U, bug_tensor** Vd, double* sv_all, int* sv_charge, int cap, int* nsv_all,
+            int* nkept) {
+  return guard([&] {
+    require(c && t && U && Vd, "null argument");
+    std::unique_ptr<bug_tensor> u, v;
+    std::vector<double> sv;
+    std::vector<int> q;
+    int nk = 0;
+    svd_impl(c, *t, nleft, left, cutoff, nkeep, u, v, sv, q, nk);
+    int ncopy = std::min<int>(cap, int(sv.size()));
+    for (int i = 0; i < ncopy; ++i) {
+      sv_all[i] = sv[i];
+      sv_charge[i] = q[i];
+    }
+    *nsv_all = int(sv.size());
+    *nkept = nk;
+    *U = u.release();
+    *Vd = v.release();
+  });
+}
+
+int bug_scale_leg(bug_ctx* c, const bug_tensor* t, int leg, const double* w, bug_tensor** out) {
+  return guard([&] {
+    require(c && t && out && leg >= 0 && leg < t->rank, "bad argument");
+    const Leg& L = t->legs[leg];
+    std::vector<double> wv(w, w + L.total());
+    std::vector<int64_t> woff(L.q.size());
+    int64_t acc = 0;
+    for (size_t s = 0; s < L.q.size(); ++s) {
+      woff[s] = acc;
+      acc += L.d[s];
+    }
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, t->legs, keys, false);
+    double* dw = c->push(wv);
+    std::vector<ScaleDesc> descs;
+    int64_t total = 0;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      const Block& b = t->blocks[bi];
+      auto st = c_strides(b.shape, t->rank);
+      ScaleDesc d{};
+      d.src = t->data(bi);
+      d.dst = o->mdata(bi);
+      d.n = b.size;
+      d.prefix = total;
+      total += b.size;
+      d.leg_stride = st[leg];
+      d.leg_dim = b.shape[leg];
+      d.w = dw + woff[L.index_of(b.key[leg])];
+      descs.push_back(d);
+    }
+    if (!descs.empty()) {
+      ScaleDesc* dd = c->push(descs);
+      bugk::launch_scale(dd, int(descs.size()), total, c->stream);
+      c->launched();
+    }
+    *out = o.release();
+  });
+}
+
+int bug_norm2(bug_ctx* c, const bug_tensor* t, double* out) {
+  return guard([&] {
+    double r[2];
+    dots(c, {{t, t}}, r);
+    *out = r[0];
+  });
+}
+
+int bug_inner(bug_ctx* c, const bug_tensor* a, const bug_tensor* b, double* out) {
+  return guard([&] { dots(c, {{a, b}}, out); });
+}
+
+int bug_inner_many(bug_ctx* c, int n, const bug_tensor* const* v, const bug_tensor* w,
+                   double* out) {
+  return guard([&] {
+    std::vector<std::pair<const bug_tensor*, const bug_tensor*>> ps;
+    for (int i = 0; i < n; ++i) ps.push_back({v[i], w});
+    if (n > 0) dots(c, ps, out);
+  });
+}
+
+int bug_lincomb(bug_ctx* c, int n, const double* coef, const bug_tensor* const* t,
+                bug_tensor** out) {
+  return guard([&] { *out = lincomb_impl(c, n, coef, t).release(); });
+}
+
+int bug_permute(bug_ctx* c, const bug_tensor* t, const int* perm, bug_tensor** out) {
+  return guard([&] { *out = permute_impl(c, *t, perm).release(); });
+}
+
+int bug_conj(bug_ctx* c, const bug_tensor* t, bug_tensor** out) {
+  return guard([&] {
+    std::vector<Leg> legs;
+    for (auto& l : t->legs) legs.push_back(flipped(l));
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    if (t->nelem > 0)
+      d.push_back(plain_copy(t->buf->ptr, o->buf->ptr, t->nelem, true, make_double2(1.0, 0.0), false));
+    run_copies(c, d);
+    *out = o.release();
+  });
+}
+
+int bug_flip_leg(bug_ctx* c, const bug_tensor* t, int leg, bug_tensor** out) {
+  return guard([&] {
+    require(leg >= 0 && leg < t->rank, "bad leg");
+    std::vector<Leg> legs = t->legs;
+    Leg L;
+    L.dir = -t->legs[leg].dir;
+    for (int s = int(t->legs[leg].q.size()) - 1; s >= 0; --s) {
+      L.q.push_back(-t->legs[leg].q[s]);
+      L.d.push_back(t->legs[leg].d[s]);
+    }
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) {
+      Key k = b.key;
+      k[leg] = -k[leg];
+      keys.push_back(k);
+    }
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      Key k = t->blocks[bi].key;
+      k[leg] = -k[leg];
+      int ob = o->find(k);
+      d.push_back(plain_copy(t->data(bi), o->mdata(ob), t->blocks[bi].size, false,
+                             make_double2(1.0, 0.0), false));
+    }
+    run_copies(c, d);
+    *out = o.release();
+  });
+}
+
+int bug_oplus(bug_ctx* c, int n, const bug_tensor* const* ts, int leg, bug_tensor** out) {
+  return guard([&] {
+    require(n >= 1, "oplus needs at least one tensor");
+    const int rank = ts[0]->rank;
+    require(leg >= 0 && leg < rank, "bad leg");
+    std::map<int, int> dims;
+    std::vector<Leg> legs = ts[0]->legs;
+    for (int i = 0; i < n; ++i) {
+      require(ts[i]->rank == rank, "oplus: ranks differ");
+      require(ts[i]->legs[leg].dir == ts[0]->legs[leg].dir, "oplus: arrows differ");
+      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) dims[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
+      if (i > 0)
+        for (int l = 0; l < rank; ++l)
+          if (l != leg) legs[l] = merged(legs[l], ts[i]->legs[l]);
+    }
+    Leg L;
+    L.dir = ts[0]->legs[leg].dir;
+    for (auto& kv : dims) {
+      L.q.push_back(kv.first);
+      L.d.push_back(kv.second);
+    }
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (int i = 0; i < n; ++i)
+      for (auto& b : ts[i]->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, rank, legs, keys, true);
+    std::map<int, int> offs;
+    std::vector<CopyDesc> d;
+    for (int i = 0; i < n; ++i) {
+      for (int bi = 0; bi < int(ts[i]->blocks.size()); ++bi) {
+        const Block& b = ts[i]->blocks[bi];
+        int ob = o->find(b.key);
+        const Block& obb = o->blocks[ob];
+        auto ss = c_strides(b.shape, rank);
+        auto ds = c_strides(obb.shape, rank);
+        CopyDesc cd{};
+        cd.src = ts[i]->data(bi);
+        cd.dst = o->mdata(ob) + int64_t(offs[b.key[leg]]) * ds[leg];
+        cd.n = b.size;
+        cd.ndim = rank;
+        for (int l = 0; l < rank; ++l) {
+          cd.dims[l] = b.shape[l];
+          cd.sstr[l] = ss[l];
+          cd.dstr[l] = ds[l];
+        }
+        cd.alpha = make_double2(1.0, 0.0);
+        d.push_back(cd);
+      }
+      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) offs[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
+    }
+    run_copies(c, d);
+    *out = o.release();
+  });
+}
+
+int bug_trim(bug_ctx* c, const bug_tensor* t, int leg, const int* counts, bug_tensor** out) {
+  return guard([&] {
+    require(leg >= 0 && leg < t->rank, "bad leg");
+    const Leg& L0 = t->legs[leg];
+    Leg L;
+    L.dir = L0.dir;
+    std::map<int, int> keep;
+    for (size_t s = 0; s < L0.q.size(); ++s) {
+      int k = std::min(std::max(counts[s], 0), L0.d[s]);
+      if (k > 0) {
+        L.q.push_back(L0.q[s]);
+        L.d.push_back(k);
+        keep[L0.q[s]] = k;
+      }
+    }
+    if (L.q.empty()) {
+      *out = nullptr;
+      return;
+    }
+    std::vector<Leg> legs = t->legs;
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (auto& b : t->blocks)
+      if (keep.count(b.key[leg])) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      const Block& b = t->blocks[bi];
+      if (!keep.count(b.key[leg])) continue;
+      int ob = o->find(b.key);
+      const Block& obb = o->blocks[ob];
+      auto ss = c_strides(b.shape, t->rank);
+      auto ds = c_strides(obb.shape, t->rank);
+      CopyDesc cd{};
+      cd.src = t->data(bi);
+      cd.dst = o->mdata(ob);
+      cd.n = obb.size;
+      cd.ndim = t->rank;
+      for (int l = 0; l < t->rank; ++l) {
+        cd.dims[l] = obb.shape[l];
+        cd.sstr[l] = ss[l];
+        cd.dstr[l] = ds[l];
+      }
+      cd.alpha = make_double2(1.0, 0.0);
+      d.push_back(cd);
+    }
+    run_copies(c, d);
+    *out = o.release();
+  });
+}
+
+}  // extern "C"

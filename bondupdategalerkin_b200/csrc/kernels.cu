@@ -1,0 +1,409 @@
+// Device kernels of the B200 block-sparse engine. See kernels.cuh for the role of each family.
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <cmath>
+
+namespace bugk {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSmCount = 148;  // B200: 2 dies x 74 SMs
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename D>
+__device__ __forceinline__ int find_desc(const D* d, int nd, int64_t e) {
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (d[mid].prefix <= e) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+inline int grid_for(int64_t total) {
+  int64_t g = (total + kThreads - 1) / kThreads;
+  int64_t cap = int64_t(kSmCount) * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return int(g);
+}
+
+// ── batched strided copy ──────────────────────────────────────────────────────────────────────
+
+__global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restrict__ d, int nd,
+                                                        int64_t total) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const CopyDesc& c = d[find_desc(d, nd, e)];
+    int64_t r = e - c.prefix;
+    int64_t so = 0, dof = 0;
+    for (int k = c.ndim - 1; k >= 0; --k) {
+      int64_t i = r % c.dims[k];
+      r /= c.dims[k];
+      so += i * c.sstr[k];
+      dof += i * c.dstr[k];
+    }
+    double2 v = c.src[so];
+    if (c.conj) v.y = -v.y;
+    double2 w = cmul(c.alpha, v);
+    if (c.accumulate) {
+      double2 o = c.dst[dof];
+      w.x += o.x;
+      w.y += o.y;
+    }
+    c.dst[dof] = w;
+  }
+}
+
+// ── segmented grouped complex GEMM ────────────────────────────────────────────────────────────
+// Tile 32x32 per CTA, K chunks of 16, 256 threads each owning a 2x2 patch. Every output block is
+// covered by its own tiles, and each tile sums over all block pairs of that output block.
+
+constexpr int TM = 32, TN = 32, TK = 16;
+
+__global__ void __launch_bounds__(kThreads)
+gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs,
+            const GemmTile* __restrict__ tiles) {
+  __shared__ double2 As[TM][TK + 1];
+  __shared__ double2 Bs[TK][TN + 1];
+  const GemmTile t = tiles[blockIdx.x];
+  const GemmOut o = outs[t.out];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int row0 = t.tm * TM, col0 = t.tn * TN;
+  double2 acc[2][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) acc[i][j] = make_double2(0.0, 0.0);
+
+  for (int p = o.pair_begin; p < o.pair_end; ++p) {
+    const GemmPair g = pairs[p];
+    const bool ta = g.opa & 1, ca = g.opa & 2, tb = g.opb & 1, cb = g.opb & 2;
+    for (int k0 = 0; k0 < g.k; k0 += TK) {
+      for (int i = threadIdx.x; i < TM * TK; i += kThreads) {
+        int mm, kk;
+        if (ta) { kk = i / TM; mm = i % TM; } else { mm = i / TK; kk = i % TK; }
+        const int gm = row0 + mm, gk = k0 + kk;
+        double2 v = make_double2(0.0, 0.0);
+        if (gm < o.m && gk < g.k)
+          v = ta ? g.A[int64_t(gk) * g.lda + gm] : g.A[int64_t(gm) * g.lda + gk];
+        if (ca) v.y = -v.y;
+        As[mm][kk] = v;
+      }
+      for (int i = threadIdx.x; i < TK * TN; i += kThreads) {
+        int kk, nn;
+        if (tb) { nn = i / TK; kk = i % TK; } else { kk = i / TN; nn = i % TN; }
+        const int gk = k0 + kk, gn = col0 + nn;
+        double2 v = make_double2(0.0, 0.0);
+        if (gk < g.k && gn < o.n)
+          v = tb ? g.B[int64_t(gn) * g.ldb + gk] : g.B[int64_t(gk) * g.ldb + gn];
+        if (cb) v.y = -v.y;
+        Bs[kk][nn] = v;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < TK; ++kk) {
+        const double2 a0 = As[ty * 2][kk], a1 = As[ty * 2 + 1][kk];
+        const double2 b0 = Bs[kk][tx * 2], b1 = Bs[kk][tx * 2 + 1];
+        cfma(acc[0][0], a0, b0);
+        cfma(acc[0][1], a0, b1);
+        cfma(acc[1][0], a1, b0);
+        cfma(acc[1][1], a1, b1);
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int gm = row0 + ty * 2 + i;
+    if (gm >= o.m) continue;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int gn = col0 + tx * 2 + j;
+      if (gn < o.n) o.C[int64_t(gm) * o.n + gn] = acc[i][j];
+    }
+  }
+}
+
+// ── batched one-sided Jacobi SVD ──────────────────────────────────────────────────────────────
+// Problem: work = A (mm x r, column-major, mm >= r). Columns are orthogonalised pairwise in a
+// round-robin order (r-1 rounds of disjoint pairs per sweep, one warp per pair) until no pair has
+// |a_p^H a_q| > tol*|a_p||a_q|. Then sigma_j = |a_j|, sorted descending (ties by index), and the
+// phase of each singular pair is fixed on the left vectors of M.
+
+constexpr int kMaxSweeps = 60;
+constexpr int kMaxR = 1024;
+
+__device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b) {
+  const int n1 = re - 1;
+  if (i == 0) {
+    a = round % n1;
+    b = n1;
+  } else {
+    a = (round + i) % n1;
+    b = (round + n1 - i) % n1;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __restrict__ descs,
+                                                              double tol_scale) {
+  extern __shared__ double2 dyn[];
+  __shared__ double sig[kMaxR];
+  __shared__ int perm[kMaxR];
+  __shared__ int rotated;
+  const SvdDesc d = descs[blockIdx.x];
+  const int mm = d.m > d.n ? d.m : d.n;
+  const int r = d.m < d.n ? d.m : d.n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  if (r <= 0) return;
+  double2* A = d.work;
+  double2* V = d.vwork;
+  if (d.use_smem) {
+    A = dyn;
+    V = dyn + int64_t(mm) * r;
+    for (int64_t i = tid; i < int64_t(mm) * r; i += blockDim.x) A[i] = d.work[i];
+  }
+  for (int64_t i = tid; i < int64_t(r) * r; i += blockDim.x)
+    V[i] = (i % (r + 1) == 0) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
+  __syncthreads();
+  const double tol = tol_scale * sqrt(double(mm));
+  const int re = r + (r & 1);
+  int sweep = 0;
+  bool converged = (r == 1);
+  for (; sweep < kMaxSweeps && !converged; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int round = 0; round < re - 1; ++round) {
+      for (int pi = warp; pi < re / 2; pi += nwarps) {
+        int a, b;
+        rr_pair(pi, round, re, a, b);
+        const int p = a < b ? a : b, q = a < b ? b : a;
+        if (q >= r) continue;
+        double2* ap = A + int64_t(p) * mm;
+        double2* aq = A + int64_t(q) * mm;
+        double al = 0.0, be = 0.0, gr = 0.0, gi = 0.0;
+        for (int i = lane; i < mm; i += 32) {
+          const double2 x = ap[i], y = aq[i];
+          al = fma(x.x, x.x, fma(x.y, x.y, al));
+          be = fma(y.x, y.x, fma(y.y, y.y, be));
+          gr = fma(x.x, y.x, fma(x.y, y.y, gr));
+          gi = fma(x.x, y.y, fma(-x.y, y.x, gi));
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        gr = warp_sum(gr);
+        gi = warp_sum(gi);
+        const double g = sqrt(gr * gr + gi * gi);
+        if (al > 0.0 && be > 0.0 && g > tol * sqrt(al) * sqrt(be)) {
+          if (lane == 0) rotated = 1;
+          const double zeta = (be - al) / (2.0 * g);
+          const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+          const double2 e = make_double2(gr / g, -gi / g);  // e^{-i phi}, gamma = g e^{i phi}
+          for (int i = lane; i < mm; i += 32) {
+            const double2 x = ap[i];
+            const double2 ey = cmul(e, aq[i]);
+            ap[i] = make_double2(c * x.x - s * ey.x, c * x.y - s * ey.y);
+            aq[i] = make_double2(s * x.x + c * ey.x, s * x.y + c * ey.y);
+          }
+          double2* vp = V + int64_t(p) * r;
+          double2* vq = V + int64_t(q) * r;
+          for (int i = lane; i < r; i += 32) {
+            const double2 x = vp[i];
+            const double2 ey = cmul(e, vq[i]);
+            vp[i] = make_double2(c * x.x - s * ey.x, c * x.y - s * ey.y);
+            vq[i] = make_double2(s * x.x + c * ey.x, s * x.y + c * ey.y);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    converged = (rotated == 0);
+    __syncthreads();
+  }
+  if (tid == 0) *d.sweeps = converged ? sweep : -1;
+  // singular values
+  for (int j = warp; j < r; j += nwarps) {
+    const double2* aj = A + int64_t(j) * mm;
+    double s2 = 0.0;
+    for (int i = lane; i < mm; i += 32) s2 = fma(aj[i].x, aj[i].x, fma(aj[i].y, aj[i].y, s2));
+    s2 = warp_sum(s2);
+    if (lane == 0) sig[j] = sqrt(s2);
+  }
+  __syncthreads();
+  for (int j = tid; j < r; j += blockDim.x) {
+    const double sj = sig[j];
+    int pos = 0;
+    for (int k = 0; k < r; ++k) {
+      const double sk = sig[k];
+      pos += (sk > sj) || (sk == sj && k < j);
+    }
+    perm[pos] = j;
+  }
+  __syncthreads();
+  const double phi = 1.6180339887498949;
+  for (int o = warp; o < r; o += nwarps) {
+    const int j = perm[o];
+    const double sj = sig[j];
+    const double inv = sj > 0.0 ? 1.0 / sj : 0.0;
+    const double2* aj = A + int64_t(j) * mm;  // left vector of work (times sigma)
+    const double2* vj = V + int64_t(j) * r;   // right vector of work
+    double2* uo = d.U + int64_t(o) * d.m;
+    double2* vo = d.V + int64_t(o) * d.n;
+    // left vectors of M: work's left vectors (no transpose) or work's right vectors (M^H)
+    double fr = 0.0, fi = 0.0;
+    for (int i = lane; i < d.m; i += 32) {
+      double2 u = d.trans ? vj[i] : make_double2(aj[i].x * inv, aj[i].y * inv);
+      const double c = 1.0 / (double(i) + phi);
+      fr = fma(c, u.x, fr);
+      fi = fma(c, u.y, fi);
+    }
+    fr = warp_sum(fr);
+    fi = warp_sum(fi);
+    const double fa = sqrt(fr * fr + fi * fi);
+    const double2 ph = fa > 0.0 ? make_double2(fr / fa, -fi / fa) : make_double2(1.0, 0.0);
+    for (int i = lane; i < d.m; i += 32) {
+      double2 u = d.trans ? vj[i] : make_double2(aj[i].x * inv, aj[i].y * inv);
+      uo[i] = cmul(u, ph);
+    }
+    for (int i = lane; i < d.n; i += 32) {
+      double2 v = d.trans ? make_double2(aj[i].x * inv, aj[i].y * inv) : vj[i];
+      vo[i] = cmul(v, ph);
+    }
+    if (lane == 0) d.S[o] = sj;
+  }
+}
+
+// ── deterministic reductions, linear combinations, leg scaling ───────────────────────────────
+
+__global__ void __launch_bounds__(kThreads) dot_kernel(const DotDesc* __restrict__ d,
+                                                       double2* __restrict__ partial) {
+  __shared__ double sr[kThreads / 32], si[kThreads / 32];
+  const DotDesc c = d[blockIdx.x];
+  double re = 0.0, im = 0.0;
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
+    const double2 a = c.a[i], b = c.b[i];
+    re = fma(a.x, b.x, fma(a.y, b.y, re));
+    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+  }
+  re = warp_sum(re);
+  im = warp_sum(im);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sr[warp] = re;
+    si[warp] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, ti = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tr += sr[w];
+      ti += si[w];
+    }
+    partial[blockIdx.x] = make_double2(tr, ti);
+  }
+}
+
+__global__ void dot_reduce_kernel(const double2* __restrict__ partial,
+                                  const int* __restrict__ seg, int nout, double2* __restrict__ out) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nout) return;
+  double tr = 0.0, ti = 0.0;
+  for (int k = seg[o]; k < seg[o + 1]; ++k) {
+    tr += partial[k].x;
+    ti += partial[k].y;
+  }
+  out[o] = make_double2(tr, ti);
+}
+
+__global__ void __launch_bounds__(kThreads) lincomb_kernel(const LinOut* __restrict__ outs, int nout,
+                                                           const LinSrc* __restrict__ srcs,
+                                                           int64_t total) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const LinOut& o = outs[find_desc(outs, nout, e)];
+    const int64_t i = e - o.prefix;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int s = o.src_begin; s < o.src_end; ++s) {
+      const double2 v = srcs[s].src[i];
+      cfma(acc, srcs[s].coef, v);
+    }
+    o.dst[i] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) scale_kernel(const ScaleDesc* __restrict__ d, int nd,
+                                                         int64_t total) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const ScaleDesc& c = d[find_desc(d, nd, e)];
+    const int64_t i = e - c.prefix;
+    const int coord = int((i / c.leg_stride) % c.leg_dim);
+    const double w = c.w[coord];
+    const double2 v = c.src[i];
+    c.dst[i] = make_double2(v.x * w, v.y * w);
+  }
+}
+
+}  // namespace
+
+void launch_copy(const CopyDesc* d_desc, int ndesc, int64_t total, cudaStream_t s) {
+  if (ndesc <= 0 || total <= 0) return;
+  copy_kernel<<<grid_for(total), kThreads, 0, s>>>(d_desc, ndesc, total);
+}
+
+void launch_gemm(const GemmOut* outs, const GemmPair* pairs, const GemmTile* tiles, int ntiles,
+                 cudaStream_t s) {
+  if (ntiles <= 0) return;
+  gemm_kernel<<<ntiles, kThreads, 0, s>>>(outs, pairs, tiles);
+}
+
+void launch_svd(const SvdDesc* d_desc, int nprob, int max_smem_bytes, cudaStream_t s) {
+  if (nprob <= 0) return;
+  if (max_smem_bytes > 0)
+    cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         max_smem_bytes);
+  jacobi_svd_kernel<<<nprob, kThreads, max_smem_bytes, s>>>(d_desc, 2.220446049250313e-16);
+}
+
+void launch_dot(const DotDesc* d_desc, int ndesc, double2* partial, cudaStream_t s) {
+  if (ndesc <= 0) return;
+  dot_kernel<<<ndesc, kThreads, 0, s>>>(d_desc, partial);
+}
+
+void launch_dot_reduce(const double2* partial, const int* seg_begin, int nout, double2* out,
+                       cudaStream_t s) {
+  if (nout <= 0) return;
+  dot_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(partial, seg_begin, nout, out);
+}
+
+void launch_lincomb(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,
+                    cudaStream_t s) {
+  if (nout <= 0 || total <= 0) return;
+  lincomb_kernel<<<grid_for(total), kThreads, 0, s>>>(outs, nout, srcs, total);
+}
+
+void launch_scale(const ScaleDesc* d_desc, int ndesc, int64_t total, cudaStream_t s) {
+  if (ndesc <= 0 || total <= 0) return;
+  scale_kernel<<<grid_for(total), kThreads, 0, s>>>(d_desc, ndesc, total);
+}
+
+}  // namespace bugk

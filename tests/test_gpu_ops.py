@@ -1,0 +1,134 @@
+"""Engine operations against the oracle's block-sparse arithmetic, one by one (GPU).
+
+Each case builds random U(1) block tensors on the host, runs the oracle operation
+(``oracle/blocks.py``) and the engine operation through the C-ABI, and compares: contractions
+(every operand layout the planner distinguishes), the Telum-selection SVD with its phase
+convention, reductions, linear combinations, permutations, direct sums and trims.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import blocks as OB
+from tests.gpu_util import rand_bt, same, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+S3 = {-2: 3, 0: 4, 2: 2}
+S2 = {-1: 2, 1: 3}
+SS = {-1: 1, 1: 1}
+
+
+@pytest.fixture(scope="module")
+def D():
+    from bondupdategalerkin_b200 import build, tensor
+
+    build.build()
+    return tensor
+
+
+def mps_like(rng, L=S3, R=None):
+    R = R or {q + s: d for q, d in L.items() for s in (-1, 1)}
+    R = {q: (d % 5) + 2 for q, d in R.items()}
+    return rand_bt(rng, (-1, -1, +1), (L, SS, R))
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_contract(D, case):
+    rng = np.random.default_rng(100 + case)
+    A = mps_like(rng)
+    # env-like (bra:-1, w:+1, ket:+1) contracted on its ket with A's left link
+    E = rand_bt(rng, (-1, +1, +1), ({q: 3 for q in range(-4, 5)}, {-2: 1, 0: 3, 2: 1}, A.legs[0].sectors))
+    patterns = [
+        (E, (2,), A, (0,), False, False),           # tail x head
+        (A, (0, 1), A, (0, 1), True, False),        # head x head, conj
+        (A, (2,), A, (2,), False, True),            # tail x tail, conj
+        (A, (1, 2), A, (1, 2), False, True),        # tail x tail (2 legs)
+        (A, (0, 2), A, (0, 2), True, False),        # split legs -> permute both
+        (E, (0, 2), E, (0, 2), True, False),
+        (A, (1,), E, (1,), False, False) if False else (A, (0,), E, (2,), False, False),  # head x tail
+        (E, (1,), E, (1,), True, False),            # middle legs -> permute
+    ]
+    a, ia, b, ib, ca, cb = patterns[case]
+    want = OB.contract(a, ia, b, ib, conja=ca, conjb=cb)
+    got = to_host(D.contract(to_dev(a), ia, to_dev(b), ib, conja=ca, conjb=cb))
+    assert sorted(got.blocks) == sorted(want.blocks)
+    assert same(got, want) < 1e-13
+
+
+@pytest.mark.parametrize("left,cutoff,nkeep", [((0, 1), 0.0, None), ((0,), 0.0, None),
+                                                ((0, 1), 1e-1, None), ((0, 1), 0.0, 5),
+                                                ((1, 2), 0.0, None), ((0, 2), 1e-3, 7)])
+def test_svd(D, left, cutoff, nkeep):
+    rng = np.random.default_rng(7)
+    A = mps_like(rng)
+    want = OB.svd(A, left, cutoff=cutoff, nkeep=nkeep)
+    got = D.svd(to_dev(A), left, cutoff=cutoff, nkeep=nkeep)
+    assert len(got.kept) == len(want.kept) and len(got.trunc) == len(want.trunc)
+    for (s1, _, q1, _), (s2, _, q2, _) in zip(got.kept + got.trunc, want.kept + want.trunc):
+        assert q1 == q2 and abs(s1 - s2) <= 1e-13 * max(1.0, want.kept[0][0])
+    assert same(to_host(got.U), want.U) < 1e-11
+    assert same(to_host(got.Vd), want.Vd) < 1e-11
+    rec = OB.contract(to_host(got.US()), (len(left),), to_host(got.Vd), (0,))
+    ref = OB.contract(want.US(), (len(left),), want.Vd, (0,))
+    assert same(rec, ref) < 1e-12
+
+
+def test_svd_wide_and_big(D):
+    rng = np.random.default_rng(11)
+    A = rand_bt(rng, (-1, -1, +1), ({0: 40}, {0: 2}, {0: 130}))   # 80 x 130: transposed path
+    want = OB.svd(A, (0, 1))
+    got = D.svd(to_dev(A), (0, 1))
+    assert np.allclose([s for s, *_ in got.kept], [s for s, *_ in want.kept], rtol=1e-12)
+    assert same(to_host(got.U), want.U) < 1e-10
+    B = rand_bt(rng, (-1, -1, +1), ({0: 200}, {0: 2}, {0: 150}))  # global-memory path
+    want = OB.svd(B, (0, 1))
+    got = D.svd(to_dev(B), (0, 1))
+    assert np.allclose([s for s, *_ in got.kept], [s for s, *_ in want.kept], rtol=1e-12)
+    assert same(to_host(got.U), want.U) < 1e-10
+
+
+def test_reductions_and_lincomb(D):
+    rng = np.random.default_rng(3)
+    A = mps_like(rng)
+    B = OB.BT(A.legs, {k: v * (1 + 0.5j) + 0.1 for k, v in A.blocks.items() if rng.random() < 0.7})
+    dA, dB = to_dev(A), to_dev(B)
+    assert abs(D.norm(dA) - OB.norm(A)) < 1e-12 * OB.norm(A)
+    assert abs(D.inner(dA, dB) - OB.inner(A, B)) < 1e-12 * OB.norm(A) * OB.norm(B)
+    many = D.inner_many([dA, dB, dA], dB)
+    assert abs(many[1] - OB.inner(B, B)) < 1e-12 * OB.norm(B) ** 2
+    lc = to_host(D.lincomb([(0.3 - 1j, dA), (2.0, dB), (-1.0, dA)]))
+    want = OB.add(OB.add(OB.scale(A, 0.3 - 1j), B, 1.0, 2.0), A, 1.0, -1.0)
+    assert same(lc, want) < 1e-13
+
+
+def test_permute_conj_flip_oplus_trim_scale(D):
+    rng = np.random.default_rng(5)
+    A = mps_like(rng)
+    dA = to_dev(A)
+    assert same(to_host(D.permute(dA, (2, 0, 1))), OB.permute(A, (2, 0, 1))) < 1e-15
+    assert same(to_host(D.conj(dA)), OB.conj(A)) < 1e-15
+    B = mps_like(np.random.default_rng(6), L=S3)
+    B = OB.BT([A.legs[0], A.legs[1], B.legs[2]], {k: v for k, v in B.blocks.items()
+                                                   if k[0] in A.legs[0].sectors})
+    got = to_host(D.oplus([dA, to_dev(B)], 2))
+    assert same(got, OB.oplus([A, B], 2)) < 1e-15
+    counts = {q: 1 + i % 2 for i, q in enumerate(A.legs[2].sectors)}
+    assert same(to_host(D.trim_per_sector(dA, 2, counts)), OB.trim_per_sector(A, 2, counts)) < 1e-15
+    res = OB.svd(A, (0, 1))
+    w = {q: np.arange(1, d + 1, dtype=float) for q, d in A.legs[2].sectors.items()}
+    got = to_host(D.scale_leg(dA, 2, w))
+    want = OB.BT(A.legs, {k: v * w[k[2]][None, None, :] for k, v in A.blocks.items()})
+    assert same(got, want) < 1e-15
+    fl = to_host(D.flip_leg(dA, 2))
+    assert fl.legs[2].dir == -A.legs[2].dir
+    assert all(np.array_equal(fl.blocks[(k[0], k[1], -k[2])], v) for k, v in A.blocks.items())
+
+
+def test_gaussian_matches_oracle_draws(D):
+    la, lb = D.Leg(-1, {-1: 2, 1: 3}), D.Leg(-1, {-1: 1, 1: 1})
+    cols = {-2: 1, 0: 3, 2: 2}
+    got = to_host(D.gaussian_fused(np.random.default_rng(9), la, lb, cols, new_first=False))
+    want = OB.gaussian_fused(np.random.default_rng(9), OB.Leg(-1, la.sectors), OB.Leg(-1, lb.sectors),
+                             cols, new_first=False)
+    assert same(got, want) == 0.0
