@@ -1,0 +1,345 @@
+"""DD-QR controlled bond expansion on device tensors (``mode = :rank_tail``).
+
+The sketch, projections, SVD candidates and Test B estimates all run in the engine; only the
+Gaussian probe is drawn on the host (from the step's seeded generator, in a fixed order) and
+uploaded. Follows:
+
+* ``perp_component`` / ``perp_component_right`` (``src/BUG/Core/TensorNetworks/sectors.jl:215-240``);
+* ``_rank_cut`` (``src/BUG/Core/RankAdaptation/truncation.jl:194-195``), ``_reortho_left/right``
+  (``:374-394``), ``_cap_to_local_room`` (``:332-351``), ``_frame_sector_dims`` (``:297-322``);
+* ``_alloc_columns`` (``src/BUG/Randomised/cbe.jl:188-195``), ``_dd_probe`` (``dd_cbe.jl:132-161``),
+  ``sector_graded_sketch(...; comp_ratio = nothing)`` (``sketch.jl:14-54``), ``_sample_residual``
+  (``sketch.jl:141-180``), ``sampled_leak`` (``cbe.jl:355-391``), ``_fold_sketch_closures``
+  (``cbe.jl:62-144``);
+* ``dd_cbe_expand`` with its default ``tail_dd`` branch (``dd_cbe_expand.jl:19-301,383-419``).
+
+A right frame's bond leg is incoming; an SVD over ``(site, link_r)`` returns that leg outgoing, so
+the orthonormal rows are re-expressed on an incoming leg (:func:`rows_from_u`) before they join a
+right frame -- the U(1) label of a leg depends on its arrow (``sectors.jl:193-206``).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import tensor as B
+from .budget import indicator
+from .env import stream_left, stream_right
+
+EPS = 2.220446049250313e-16
+CBE_EPS = 100 * EPS
+REORTH_KEEP = 1 / math.sqrt(2)
+
+
+def perp_left(U: B.DT, K: B.DT) -> B.DT:
+    """``K - U (U^dag K)`` over the ``(link, site)`` legs."""
+    ov = B.contract(U, (0, 1), K, (0, 1), conja=True)
+    proj = B.contract(U, (2,), ov, (0,))
+    return B.sub(K, proj)
+
+
+def perp_right(V: B.DT, K: B.DT) -> B.DT:
+    """``K - (K V^dag) V`` over the ``(site, link)`` legs."""
+    ov = B.contract(K, (1, 2), V, (1, 2), conjb=True)
+    proj = B.contract(ov, (1,), V, (0,))
+    return B.sub(K, proj)
+
+
+flip_leg = B.flip_leg
+
+
+def rows_from_u(U: B.DT) -> B.DT:
+    """``U`` = (site, link, new:+1) of an SVD over a right frame's legs -> rows ``(new:-1, site,
+    link)`` spanning the same space (``permutedims(U, (3, 1, 2))``)."""
+    return flip_leg(B.permute(U, (2, 0, 1)), 0)
+
+
+def rank_cut(stol: float, sketch_norm: float, outside_norm: float) -> float:
+    return stol if stol > 0 else CBE_EPS * max(sketch_norm, outside_norm) / outside_norm
+
+
+def reortho(frame, block, side):
+    """``orth(perp(block))`` or ``None`` (``truncation.jl:374-394``)."""
+    if block is None:
+        return None
+    perp = perp_left if side == "left" else perp_right
+    outside = perp(frame, block)
+    if B.norm(outside) <= CBE_EPS * max(B.norm(block), 1.0):
+        return None
+    if side == "left":
+        return B.svd(outside, (0, 1), cutoff=1e-14).U
+    return rows_from_u(B.svd(outside, (1, 2), cutoff=1e-14).U)
+
+
+def fused_dims(frame, side):
+    """``(dfull, dT)``: per charge of the frame's local space, its dimension and the frame's
+    width there (``truncation.jl:297-322``)."""
+    if side == "left":
+        fs = B.fused_sectors(frame.legs[0], frame.legs[1], +1)
+        la, lb, bl = frame.legs[0], frame.legs[1], frame.legs[2]
+    else:
+        fs = B.fused_sectors(frame.legs[1], frame.legs[2], -1)
+        la, lb, bl = frame.legs[1], frame.legs[2], frame.legs[0]
+    dfull = {c: sum(la.sectors[a] * lb.sectors[b] for a, b in pairs) for c, pairs in fs.items()}
+    dT = {c: bl.sectors.get(c, 0) for c in dfull}
+    for c, w in dT.items():
+        if w > dfull[c]:
+            raise RuntimeError(f"frame holds {w} directions in sector {c}, local space {dfull[c]}")
+    return dfull, dT
+
+
+def cap_to_local_room(frame, cand, side):
+    if cand is None:
+        return None
+    fl = 2 if side == "left" else 0
+    dfull, dT = fused_dims(frame, side)
+    counts = {}
+    over = False
+    for c, lw in dfull.items():
+        du = cand.legs[fl].sectors.get(c, 0)
+        if du == 0:
+            continue
+        counts[c] = min(du, lw - dT[c])
+        over |= counts[c] < du
+    if not over:
+        return cand
+    return B.trim_per_sector(cand, fl, counts)
+
+
+def alloc_columns(dims: dict, budget: int) -> dict:
+    tot = sum(dims.values())
+    if tot == 0 or budget <= 0:
+        return {q: 0 for q in dims}
+    return {q: min(d, math.ceil(d / tot * budget)) for q, d in dims.items()}
+
+
+def dd_probe(opp, oside, width, rng):
+    """Sector-graded Gaussian probe in ``opp``'s discarded space (``dd_cbe.jl:132-161``)."""
+    dfull, dT = fused_dims(opp, oside)
+    dC = {c: max(dfull[c] - dT[c], 0) for c in dfull}
+    if sum(dC.values()) == 0:
+        return None
+    cols = alloc_columns(dC, width)
+    if oside == "left":
+        om = B.gaussian_fused(rng, opp.legs[0], opp.legs[1], cols, new_first=False)
+    else:
+        om = B.gaussian_fused(rng, opp.legs[1], opp.legs[2], cols, new_first=True)
+    if om is None:
+        return None
+    projected = (perp_left if oside == "left" else perp_right)(opp, om)
+    return projected if B.norm(projected) > 0 else None
+
+
+def graded_sketch(frame, side, npre, rng):
+    """``sector_graded_sketch(frame, side, npre; comp_ratio = nothing)`` (``sketch.jl:14-54``)."""
+    dfull, _ = fused_dims(frame, side)
+    cols = alloc_columns(dfull, npre)
+    if side == "left":
+        r = B.gaussian_fused(rng, frame.legs[0], frame.legs[1], cols, new_first=False)
+    else:
+        r = B.gaussian_fused(rng, frame.legs[1], frame.legs[2], cols, new_first=True)
+    if r is None:
+        return None
+    return r if B.norm(r) > 0 else None
+
+
+def sample_residual(basis, project, sketch, Om, wleg, side):
+    """Test B with ``nh = 1`` and fixed probe ``Om`` (``sketch.jl:141-180``):
+    ``(est, per_sector, cols)``."""
+    per, cols = {}, {}
+    if Om is None:
+        return 0.0, per, cols
+    for q, d in Om.legs[wleg].sectors.items():
+        if d > 0:
+            cols[q] = d
+    if not cols:
+        return 0.0, per, cols
+    sketched = sketch(Om)
+    if sketched is None:
+        return 0.0, per, cols
+    residual = project(sketched)
+    if B.norm(residual) <= CBE_EPS:
+        return 0.0, per, cols
+    if basis is not None:
+        off = perp_left(basis, residual) if side == "left" else perp_right(basis, residual)
+        residual = project(off)
+    rleg = 2 if side == "left" else 0
+    for q, d in residual.legs[rleg].sectors.items():
+        nq = cols.get(q, 0)
+        if not nq > 0:
+            raise RuntimeError(f"Test B: residual sector {q} has no holdout column")
+        rq = B.trim_per_sector(residual, rleg, {q: d}) if len(residual.legs[rleg].sectors) > 1 else residual
+        per[q] = (B.norm(rq) ** 2 if rq is not None else 0.0) / nq
+    return math.sqrt(sum(per.values())), per, cols
+
+
+@dataclass
+class BondFrame:
+    U0: B.DT
+    S0: B.DT
+    V0: B.DT
+    old_rank: int
+
+
+def frame_theta(fr: BondFrame) -> B.DT:
+    return B.contract(B.contract(fr.U0, (2,), fr.S0, (0,)), (2,), fr.V0, (0,))
+
+
+def folded_closures(fr: BondFrame, mpo, bond, lenv, renv):
+    """``_fold_sketch_closures`` (``cbe.jl:62-132``): ``(skl, skr)`` with the projection applied."""
+    Wl, Wr = mpo[bond], mpo[bond + 1]
+    theta = frame_theta(fr)
+
+    def skl(Om):
+        t = B.contract(Om, (2,), renv, (0,), conja=True)
+        rc = B.contract(t, (1, 2), Wr, (2, 3))                  # (g, ket_r, w_mid, s_ket_r)
+        tc = B.contract(theta, (2, 3), rc, (3, 1))               # (l, s_l, g, w_mid)
+        wm = B.contract(tc, (1, 3), Wl, (1, 3))                  # (l, g, w_l, s_bra_l)
+        t = B.contract(wm, (0, 2), lenv, (2, 1))                 # (g, s_bra_l, bra)
+        return perp_left(fr.U0, B.permute(t, (2, 1, 0)))
+
+    def skr(Om):
+        t = B.contract(Om, (0,), lenv, (0,), conja=True)         # (s_bra_l, g, w, ket_l)
+        cap = B.permute(B.contract(t, (0, 2), Wl, (2, 0)), (1, 0, 2, 3))  # (ket_l, g, s_ket_l, w_mid)
+        tc = B.contract(theta, (0, 1), cap, (0, 2))              # (s_r, r, g, w_mid)
+        wm = B.contract(tc, (0, 3), Wr, (1, 0))                  # (r, g, s_bra_r, w_r)
+        t = B.contract(wm, (0, 3), renv, (2, 1))                 # (g, s_bra_r, bra_r)
+        return perp_right(fr.V0, t)
+
+    return skl, skr
+
+
+def sampled_leak(fr: BondFrame, skl, skr, side, column_count, rng) -> float:
+    """``sampled_leak`` (``cbe.jl:355-391``)."""
+    if side == "left":
+        Om = graded_sketch(fr.V0, "right", column_count, rng)
+        return sample_residual(None, lambda s: perp_left(fr.U0, s), skl, Om, 0, "left")[0]
+    Om = graded_sketch(fr.U0, "left", column_count, rng)
+    return sample_residual(None, lambda s: perp_right(fr.V0, s), skr, Om, 2, "right")[0]
+
+
+@dataclass
+class Expansion:
+    U_ex: B.DT
+    V_ex: B.DT
+    n_new_l: int
+    n_new_r: int
+    err_pre: float = 0.0
+    err_fnl: float = 0.0
+
+
+def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
+                  fixed_width=8, tail_factor=0.10, mode="rank_tail") -> Expansion:
+    """Grow one frame of the bond by the DD-projected sketch, rank by tail bisection
+    (``dd_cbe_expand.jl:19-301``)."""
+    if mode != "rank_tail":
+        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail is restated")
+    if fixed_width < 1:
+        raise ValueError("rank_tail requires positive fixed_width")
+    if not 0 < tail_factor <= 1:
+        raise ValueError("tail_factor must lie in (0,1]")
+    left = side == "left"
+    U0, V0 = fr.U0, fr.V0
+    old_rank = fr.old_rank
+    frame, opp = (U0, V0) if left else (V0, U0)
+    oside = "right" if left else "left"
+    fl, wleg = (2, 0) if left else (0, 2)
+    none = Expansion(U0, V0, 0, 0)
+    full_self = U0.dim(0) * U0.dim(1) if left else V0.dim(1) * V0.dim(2)
+    full_opp = V0.dim(1) * V0.dim(2) if left else U0.dim(0) * U0.dim(1)
+    cap = full_self - old_rank
+    wbind = False
+    if alloc is not None and workcap > 0:
+        wk = max(workcap - old_rank, 0)
+        wbind = wk < cap
+        cap = min(cap, wk)
+    if cap <= 0:
+        return none
+    if left:
+        core = B.contract(U0, (2,), fr.S0, (0,))
+
+        def sketch(Om):
+            return stream_left(core, V0, mpo, bond, lenv, renv, Om)
+
+        def project(b):
+            return perp_left(U0, b)
+    else:
+        core = B.contract(fr.S0, (1,), V0, (0,))
+
+        def sketch(Om):
+            return stream_right(U0, core, mpo, bond, lenv, renv, Om)
+
+        def project(b):
+            return perp_right(V0, b)
+
+    # tail_dd
+    Om = dd_probe(opp, oside, min(fixed_width, full_opp), rng)
+    directions, direction_count = None, 0
+    if Om is not None:
+        if ledger is not None:
+            ledger.n_probes += Om.dim(wleg)
+        Y = project(sketch(Om))
+        nY = B.norm(Y)
+        if not nY <= CBE_EPS:
+            legs = (0, 1) if left else (1, 2)
+            rmax = min(cap, Om.dim(wleg))
+            cache = {}
+
+            def candidate(k):
+                if k <= 0:
+                    return None
+                if k in cache:
+                    return cache[k]
+                fac = B.svd(Y, legs, cutoff=rank_cut(0.0, nY, nY), nkeep=k)
+                if not fac.kept:
+                    res = None
+                elif left:
+                    res = reortho(frame, fac.U, "left")
+                else:
+                    res = reortho(frame, rows_from_u(fac.U), "right")
+                cache[k] = res
+                return res
+
+            limit = tail_factor * alloc.sample
+
+            def metric(k):
+                est = sample_residual(candidate(k), project, lambda _: Y, Om, wleg, side)[0]
+                return indicator(alloc, est)
+
+            if metric(0) <= limit:
+                directions, direction_count = None, 0
+            else:
+                hi = rmax
+                if metric(hi) > limit:
+                    directions, direction_count = candidate(hi), hi
+                else:
+                    lo = 0
+                    while hi - lo > 1:
+                        k = (hi + lo) // 2
+                        if metric(k) <= limit:
+                            hi = k
+                        else:
+                            lo = k
+                    Bk = candidate(hi)
+                    directions, direction_count = Bk, (0 if Bk is None else Bk.dim(fl))
+    if directions is None:
+        return none
+    if direction_count > cap:
+        directions = B.trim_total(directions, fl, cap)
+        if directions is None:
+            return none
+    if ledger is not None and wbind and direction_count >= cap:
+        ledger.workcap_reached = True
+    directions = cap_to_local_room(frame, directions, side)
+    if directions is None:
+        return none
+    nq = directions.dim(fl)
+    if ledger is not None:
+        ledger.n_selected += nq
+    grown = B.oplus([frame, directions], fl)
+    if left:
+        return Expansion(grown, V0, nq, 0)
+    return Expansion(U0, grown, 0, nq)

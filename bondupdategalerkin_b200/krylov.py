@@ -1,0 +1,417 @@
+"""Krylov solvers on device vectors: the root ``expv`` and the local enrichment recurrences.
+
+The vectors (root cores, one-site tensors) stay in HBM; each matvec is engine contractions, each
+classical Gram-Schmidt pass is ONE ``bug_inner_many`` launch (all overlaps against the fixed
+residual) plus ONE ``bug_lincomb``, and a three-term update is one ``bug_lincomb``. Only the
+k x k projected matrices (k <= 64) come to the host, where their eigen/exponential solves run in
+FP64. The recurrences and stopping rules follow:
+
+* ``_shift``, ``_tridiag_eigen``, ``_coeffs_from_eigen`` (``src/BUG/Core/LocalSolvers/krylov.jl:44-117``),
+  ``lanczos_expv`` (``krylov.jl:128-263``), ``arnoldi_expv`` (``krylov.jl:343-442``), ``_combine``
+  (``:305-311``), ``_cgs2!`` (``:321-332``), ``_apply_scale`` (``:296-302``);
+* ``_tail``, ``_tail_sup``, ``_pick_tau``, ``_hess_coeffs`` (``root_methods.jl:87-141``);
+* ``_kry_weight``, ``_residual_integral`` (``src/BUG/Core/RankAdaptation/krylov_enrichment.jl:58-120``);
+* ``_lanczos_chain`` (``krylov_lanczos.jl:18-71``), ``_arnoldi_chain`` (``krylov_arnoldi.jl:13-58``),
+  ``_krylov_basis`` / ``_krylov_stop`` (``krylov_recurrence.jl:27-72``).
+
+The module needs ``inner``, ``inner_many``, ``norm`` and ``lin`` from ``ops``.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import scipy.linalg
+
+EXPV_SAFE_EXPONENT = 60.0
+EXPV_SHIFT_TRIGGER = 30.0
+EXPV_MAX_NORM = 1e150
+TAIL_NODES = 8
+KRY_BREAKDOWN = 1e-13
+KRY_MAXDEPTH = 64
+ROOT_MAXITER = 30
+KRY_SKEW_TOL = 1e-12
+RESIDUAL_MAX_PANELS = 4096
+
+
+class DevOps:
+    """Vector operations on engine tensors: every call is one launch (plus one read-back)."""
+
+    def __init__(self):
+        from . import tensor as T
+
+        self.T = T
+
+    def inner(self, a, b):
+        return self.T.inner(a, b)
+
+    def inner_many(self, vs, w):
+        return self.T.inner_many(vs, w)
+
+    def norm(self, a):
+        return self.T.norm(a)
+
+    def lin(self, terms):
+        """``sum c_i v_i`` in one launch."""
+        return self.T.lincomb(terms)
+
+
+def shift(vals, tau) -> float:
+    if len(vals) == 0:
+        return 0.0
+    ex = [(tau * complex(v)).real for v in vals]
+    top = int(np.argmax(ex))
+    return float(np.real(vals[top])) if ex[top] > EXPV_SHIFT_TRIGGER else 0.0
+
+
+def tridiag_eigen(alpha, beta):
+    alpha = np.asarray(alpha, dtype=np.float64)
+    beta = np.asarray(beta, dtype=np.float64)
+    if not (np.all(np.isfinite(alpha)) and np.all(np.isfinite(beta))):
+        raise ValueError("Lanczos tridiagonal has non-finite entries: the input vector or the operator is not finite")
+    n = len(alpha)
+    T = np.diag(alpha)
+    if n > 1:
+        T += np.diag(beta, 1) + np.diag(beta, -1)
+    return np.linalg.eigh(T)
+
+
+def coeffs_from_eigen(vals, vecs, tau):
+    sigma = shift(vals, tau)
+    w = np.exp(tau * (vals.astype(np.complex128) - sigma)) * vecs[0, :].astype(np.complex128)
+    return vecs.astype(np.complex128) @ w, tau * sigma
+
+
+def hess_coeffs(Hm, tau):
+    if Hm.size == 0:
+        return np.zeros(0, dtype=np.complex128), 0j
+    sigma = shift(np.linalg.eigvals(Hm), tau)
+    P = scipy.linalg.expm(tau * (Hm - sigma * np.eye(Hm.shape[0])))
+    return P[:, 0].copy(), tau * sigma
+
+
+def tail(coeff, betak):
+    return 0.0 if len(coeff) == 0 else betak * abs(coeff[-1])
+
+
+def tail_sup(evalcoeff, step, betak, above=math.inf):
+    t = tail(evalcoeff(step)[0], betak)
+    if step.real != 0:
+        return t
+    for node in range(1, TAIL_NODES):
+        if t >= above:
+            return t
+        t = max(t, tail(evalcoeff(step * (node / TAIL_NODES))[0], betak))
+    return t
+
+
+def pick_tau(evalcoeff, tau_rem, betak, conv_tol):
+    def accepted(trial):
+        tl = tail_sup(evalcoeff, trial, betak, above=conv_tol if conv_tol > 0 else math.inf)
+        return math.isfinite(tl) and (conv_tol <= 0 or tl <= conv_tol)
+
+    if accepted(tau_rem):
+        return tau_rem
+    lo, hi = 0.0, 1.0
+    for _ in range(40):
+        mid = 0.5 * (lo + hi)
+        if accepted(mid * tau_rem):
+            lo = mid
+        else:
+            hi = mid
+    return max(lo, 1e-6) * tau_rem
+
+
+def combine(ops, coeff, basis, beta0):
+    return ops.lin([(coeff[c] * beta0, basis[c]) for c in range(len(coeff))])
+
+
+def apply_scale(ops, cur, logscale):
+    sc = np.exp(logscale)
+    if not (math.isfinite(abs(sc)) and sc != 0):
+        return cur
+    n = ops.norm(cur)
+    if math.isfinite(n) and n > 0 and abs(sc) * n > EXPV_MAX_NORM:
+        return cur
+    if sc == 1:
+        return cur
+    return ops.lin([(sc, cur)])
+
+
+def lanczos_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, reorth=False, conv_tol=0.0,
+                 substeps=1):
+    """``exp(tau*A) vector`` for Hermitian ``A`` (``krylov.jl:128-263``). Returns
+    ``(result, report)`` with ``report = (iterations, substeps, err)``."""
+    tau = complex(tau)
+    beta0 = ops.norm(vector)
+    if beta0 == 0:
+        return vector, (0, 0, 0.0)
+    cur = vector
+    tau_rem = tau
+    logscale = 0j
+    total = nsub = 0
+    err = 0.0
+    while True:
+        nsub += 1
+        cur_norm = ops.norm(cur)
+        if cur_norm == 0:
+            break
+        v = ops.lin([(1.0 / cur_norm, cur)])
+        basis = [v]
+        alpha, betas = [], []
+        residual = apply(v)
+        total += 1
+        a = ops.inner(v, residual).real
+        alpha.append(a)
+        residual = ops.lin([(1.0, residual), (-a, v)])
+        for _ in range(2, maxiter + 1):
+            off = ops.norm(residual)
+            if off < tol:
+                break
+            if conv_tol > 0:
+                vals, vecs = tridiag_eigen(alpha, betas)
+                tt = tail_sup(lambda s: coeffs_from_eigen(vals, vecs, s), tau_rem, off, above=conv_tol)
+                if tt < conv_tol:
+                    break
+            betas.append(off)
+            v = ops.lin([(1.0 / off, residual)])
+            basis.append(v)
+            residual = apply(v)
+            total += 1
+            a = ops.inner(v, residual).real
+            alpha.append(a)
+            residual = ops.lin([(1.0, residual), (-a, v), (-off, basis[-2])])
+            if reorth:
+                for _p in range(2):
+                    cs = ops.inner_many(basis, residual)
+                    residual = ops.lin([(1.0, residual)] + [(-c, p) for c, p in zip(cs, basis)])
+        vals, vecs = tridiag_eigen(alpha, betas)
+        evalcoeff = lambda s: coeffs_from_eigen(vals, vecs, complex(s))
+        betak = ops.norm(residual)
+        if substeps == 1:
+            tau_s = tau_rem
+        elif substeps > 1:
+            tau_s = tau_rem / (substeps - nsub + 1)
+        else:
+            tau_s = pick_tau(evalcoeff, tau_rem, betak, conv_tol)
+        coeff, ls = evalcoeff(tau_s)
+        err += tail_sup(evalcoeff, tau_s, betak) * cur_norm / beta0
+        cur = combine(ops, coeff, basis, cur_norm)
+        logscale += ls
+        tau_rem -= tau_s
+        if substeps == 1 or abs(tau_rem) <= 1e-14 * max(abs(tau), 1.0):
+            break
+        if nsub >= 10_000:
+            raise RuntimeError(f"expv: substep search failed to advance (tau_rem = {tau_rem})")
+    return apply_scale(ops, cur, logscale), (total, nsub, err)
+
+
+def cgs2(ops, H, column, basis, vector):
+    for _p in range(2):
+        cs = ops.inner_many(basis, vector)
+        for row, ov in enumerate(cs):
+            H[row, column] += ov
+        vector = ops.lin([(1.0, vector)] + [(-c, b) for c, b in zip(cs, basis)])
+    return vector
+
+
+def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, substeps=1):
+    """``exp(tau*A) vector`` for any ``A`` by Arnoldi with CGS2 (``krylov.jl:343-442``)."""
+    tau = complex(tau)
+    beta0 = ops.norm(vector)
+    if beta0 == 0:
+        return vector, (0, 0, 0.0)
+    cur = vector
+    tau_rem = tau
+    logscale = 0j
+    total = nsub = 0
+    err = 0.0
+    while True:
+        nsub += 1
+        cur_norm = ops.norm(cur)
+        if cur_norm == 0:
+            break
+        basis = [ops.lin([(1.0 / cur_norm, cur)])]
+        H = np.zeros((maxiter + 1, maxiter), dtype=np.complex128)
+        dim = 0
+        betak = 0.0
+        for k in range(maxiter):
+            residual = cgs2(ops, H, k, basis, apply(basis[k]))
+            total += 1
+            dim = k + 1
+            rn = ops.norm(residual)
+            betak = rn
+            if rn < tol:
+                break
+            if conv_tol > 0:
+                lead = H[:dim, :dim].copy()
+                tt = tail_sup(lambda s: hess_coeffs(lead, s), tau_rem, rn, above=conv_tol)
+                if tt < conv_tol:
+                    break
+            H[k + 1, k] = rn
+            if k + 1 == maxiter:
+                break
+            basis.append(ops.lin([(1.0 / rn, residual)]))
+        Hm = H[:dim, :dim].copy()
+        evalcoeff = lambda s: hess_coeffs(Hm, complex(s))
+        if substeps == 1:
+            tau_s = tau_rem
+        elif substeps > 1:
+            tau_s = tau_rem / (substeps - nsub + 1)
+        else:
+            tau_s = pick_tau(evalcoeff, tau_rem, betak, conv_tol)
+        coeff, ls = evalcoeff(tau_s)
+        err += tail_sup(evalcoeff, tau_s, betak) * cur_norm / beta0
+        cur = combine(ops, coeff, basis[:dim], cur_norm)
+        logscale += ls
+        tau_rem -= tau_s
+        if substeps == 1 or abs(tau_rem) <= 1e-14 * max(abs(tau), 1.0):
+            break
+        if nsub >= 10_000:
+            raise RuntimeError(f"expv: substep search failed to advance (tau_rem = {tau_rem})")
+    return apply_scale(ops, cur, logscale), (total, nsub, err)
+
+
+def expv(ops, apply, tau, vector, hermitian=True, **kw):
+    """``expv`` dispatcher (``root_methods.jl:359-402``), ``root_method = :exp`` only."""
+    if hermitian:
+        return lanczos_expv(ops, apply, tau, vector, **kw)
+    kw.pop("reorth", None)
+    return arnoldi_expv(ops, apply, tau, vector, **kw)
+
+
+# ── local Krylov weights and chains ──────────────────────────────────────────────────────────
+
+
+def residual_integral(defect_norm, generator, tau, state_seed=True):
+    """``|tau| int_0^1 defect_norm(exp(s M) e_1) ds`` by composite Simpson in log space
+    (``krylov_enrichment.jl:89-120``)."""
+    g = np.asarray(generator, dtype=np.complex128)
+    n = g.shape[0]
+    unitary = np.linalg.norm(g + g.conj().T) <= KRY_SKEW_TOL * np.linalg.norm(g)
+    sigma = 0.0 if unitary else float(np.max(np.linalg.eigvals(g).real))
+    shifted = g - sigma * np.eye(n)
+    intervals = 2 * min(max(math.ceil(2 * np.linalg.norm(shifted, 1)), 8), RESIDUAL_MAX_PANELS)
+    spacing = 1.0 / intervals
+    prop = scipy.linalg.expm(spacing * shifted)
+    col = np.zeros(n, dtype=np.complex128)
+    col[0] = 1
+    logs = np.empty(intervals + 1)
+    for node in range(intervals + 1):
+        if node > 0:
+            col = prop @ col
+        w = 1.0 if node in (0, intervals) else (4.0 if node % 2 == 1 else 2.0)
+        mag = defect_norm(col)
+        logs[node] = -math.inf if mag == 0 else math.log(w * spacing / 3 * mag) + node * spacing * sigma
+    peak = float(np.max(logs))
+    if peak == -math.inf:
+        return 0.0
+    lw = math.log(abs(tau)) + peak + math.log(float(np.sum(np.exp(logs - peak))))
+    if unitary or not state_seed:
+        return math.exp(lw)
+    return math.exp(lw - sigma - math.log(max(np.linalg.norm(col), np.finfo(float).tiny)))
+
+
+def kry_weight(Hm, k, tau, state_seed=True):
+    """Weight of ``v_{k+1}`` in ``exp(tau H) v_1`` (``krylov_enrichment.jl:58-73``); ``k`` 1-based."""
+    beta = abs(Hm[k, k - 1])
+    if beta == 0:
+        return 0.0
+    return beta * residual_integral(lambda c: abs(c[k - 1]), tau * Hm[:k, :k], tau, state_seed)
+
+
+def krylov_stop(weight, allowance, step, fixed_depth):
+    if fixed_depth > 0:
+        return step >= fixed_depth, step >= fixed_depth and weight <= allowance
+    return weight <= allowance, weight <= allowance
+
+
+def lanczos_chain(ops, unit_seed, applyH, tau, allowance, score, maxdepth=KRY_MAXDEPTH, amp=1.0,
+                  state_seed=True, fixed_depth=0):
+    vs, weights = [unit_seed], [amp]
+    Hm = np.zeros((maxdepth + 1, maxdepth + 1), dtype=np.complex128)
+    closed = capped = False
+    n_h1 = 0
+    prev_beta = 0.0
+    for step in range(1, maxdepth + 1):
+        image = applyH(vs[step - 1])
+        n_h1 += 1
+        if step > 1:
+            image = ops.lin([(1.0, image), (-prev_beta, vs[step - 2])])
+        alpha = ops.inner(vs[step - 1], image)
+        if not abs(alpha.imag) <= 1e-9 * max(abs(alpha), 1.0):
+            raise ValueError(f"Lanczos needs a Hermitian one-site generator (imag alpha = {alpha})")
+        Hm[step - 1, step - 1] = alpha.real
+        image = ops.lin([(1.0, image), (-alpha.real, vs[step - 1])])
+        if step >= 20 and step % 2 == 0:
+            cs = ops.inner_many(vs, image)
+            image = ops.lin([(1.0, image)] + [(-c, b) for c, b in zip(cs, vs)])
+        beta = ops.norm(image)
+        if beta <= KRY_BREAKDOWN:
+            closed = True
+            break
+        Hm[step, step - 1] = beta
+        Hm[step - 1, step] = beta
+        nv = ops.lin([(1.0 / beta, image)])
+        vs.append(nv)
+        w = amp * kry_weight(Hm, step, tau, state_seed)
+        weights.append(w)
+        if not score(nv, w, step == 1):
+            capped = True
+            break
+        stop, closed = krylov_stop(w, allowance, step, fixed_depth)
+        if stop:
+            break
+        prev_beta = beta
+    if not closed:
+        capped = True
+    return dict(basis=vs, weights=weights, n_h1=n_h1, closed=closed, capped=capped)
+
+
+def arnoldi_chain(ops, unit_seed, applyH, tau, allowance, score, maxdepth=KRY_MAXDEPTH, amp=1.0,
+                  state_seed=True, fixed_depth=0):
+    nh = 0
+    capped = closed = False
+    vs, ws = [unit_seed], [amp]
+    Hm = np.zeros((maxdepth + 1, maxdepth + 1), dtype=np.complex128)
+    for step in range(1, maxdepth + 1):
+        image = applyH(vs[-1])
+        nh += 1
+        for _p in range(2):
+            cs = ops.inner_many(vs, image)
+            for row, ov in enumerate(cs):
+                Hm[row, step - 1] += ov
+            image = ops.lin([(1.0, image)] + [(-c, b) for c, b in zip(cs, vs)])
+        rn = ops.norm(image)
+        if rn <= KRY_BREAKDOWN:
+            closed = True
+            break
+        Hm[step, step - 1] = rn
+        nv = ops.lin([(1.0 / rn, image)])
+        vs.append(nv)
+        w = amp * kry_weight(Hm, step, tau, state_seed)
+        ws.append(w)
+        if not score(nv, w, step == 1):
+            capped = True
+            break
+        stop, closed = krylov_stop(w, allowance, step, fixed_depth)
+        if stop:
+            break
+    if not closed:
+        capped = True
+    return dict(basis=vs, weights=ws, n_h1=nh, closed=closed, capped=capped)
+
+
+def krylov_basis(ops, seed, applyH, tau, allowance, score, maxdepth=KRY_MAXDEPTH, amp=1.0,
+                 state_seed=True, recurrence="arnoldi", fixed_depth=0):
+    if recurrence not in ("lanczos", "arnoldi"):
+        raise ValueError(f"unknown local Krylov recurrence: {recurrence}")
+    sn = ops.norm(seed)
+    if not sn > 0:
+        return dict(basis=[], weights=[], n_h1=0, closed=True, capped=False)
+    teff = 1.0 + 0j if tau == 0 else complex(tau)
+    unit = ops.lin([(1.0 / sn, seed)])
+    chain = lanczos_chain if recurrence == "lanczos" else arnoldi_chain
+    return chain(ops, unit, applyH, teff, allowance, score, maxdepth=maxdepth, amp=amp,
+                 state_seed=state_seed, fixed_depth=fixed_depth)

@@ -53,3 +53,30 @@ def same(a, b, tol=1e-12):
             y = np.zeros_like(x)
         err = max(err, float(np.max(np.abs(x - y))) if x.size else 0.0)
     return err / scale
+
+
+def mps_to_host(psi):
+    """Download a device MPS into an oracle MPS (same centre)."""
+    from oracle.models import MPS as OMPS
+
+    return OMPS([to_host(t) for t in psi.tensors], psi.center)
+
+
+def overlap(a, b):
+    """<a|b> of two oracle MPS by left-to-right transfer contraction."""
+    E = None
+    for i in range(1, len(a) + 1):
+        if E is None:
+            E = OB.contract(a[i], (0, 1), b[i], (0, 1), conja=True)
+        else:
+            t = OB.contract(E, (0,), a[i], (0,), conjb=True)      # (b_r, s, a_r')
+            E = OB.contract(t, (0, 1), b[i], (0, 1))             # (a_r', b_r)
+    tot = 0j
+    for k, v in E.blocks.items():
+        tot += complex(np.sum(v))
+    return tot
+
+
+def fidelity(a, b):
+    ab = overlap(a, b)
+    return abs(ab) ** 2 / (overlap(a, a).real * overlap(b, b).real)

@@ -1,0 +1,100 @@
+"""The device BUG step against the CPU oracle on identical inputs and identical Gaussian draws.
+
+Both sides start from the same state, take their probes from generators seeded alike, and must
+agree after every step on: bond dimensions, ledger verdict and its failed checks, the root
+solve's Krylov iterations, the state (infidelity <= 1e-12) and the S^z profile (relative error
+<= 1e-10). Cases: the b155550 XX fixtures' setting (L = 10 Neel, U(1) order 1 and 2, and the
+no-symmetry L = 8 run), the XX domain-wall chain L = 20 at maxdim 64 and tol_basis 1e-3
+(checked against free fermions as well), an XXZ quench, and the two-spin known answer.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import models as OM
+from oracle import step as OS
+from tests.gpu_util import fidelity, mps_to_host
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    from bondupdategalerkin_b200 import build
+
+    build.build()
+    from bondupdategalerkin_b200 import models as DM
+    from bondupdategalerkin_b200 import step as DS
+
+    return DM, DS
+
+
+def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_every=1, **kw):
+    DM, DS = dev
+    ostate = getattr(OM, start)(L, symmetry=sym)
+    dstate = getattr(DM, start)(L, symmetry=sym)
+    ompo = OM.xxz_mpo(L, J=1.0, delta=delta, symmetry=sym)
+    dmpo = DM.xxz_mpo(L, J=1.0, delta=delta, symmetry=sym)
+    orng, drng = np.random.default_rng(1234), np.random.default_rng(1234)
+    okw = dict(kw)
+    dkw = dict(kw)
+    if "expansion" in kw:
+        e = kw["expansion"]
+        okw["expansion"] = OS.DDQRExpansion(**e)
+        dkw["expansion"] = DS.DDQRExpansion(**e)
+    worst = (0.0, 0.0)
+    for n in range(1, steps + 1):
+        oi = OS.cbe_bug_step(ostate, ompo, tau, order=order, rng=orng, **okw)
+        di = DS.cbe_bug_step(dstate, dmpo, tau, order=order, rng=drng, **dkw)
+        assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
+        assert di["status"] == oi["status"], n
+        assert di["ledger"].unmet == oi["ledger"].unmet, n
+        assert di["ledger"].expv_iters == oi["ledger"].expv_iters, n
+        assert di["expanded"] == oi["expanded"], n
+        if n % check_every == 0 or n == steps:
+            h = mps_to_host(dstate)
+            inf = 1.0 - fidelity(h, ostate)
+            sz_o = OM.sz_profile(ostate)
+            sz_d = OM.sz_profile(h)
+            rel = np.max(np.abs(sz_d - sz_o)) / max(np.max(np.abs(sz_o)), 1e-300)
+            worst = (max(worst[0], inf), max(worst[1], rel))
+            assert inf <= 1e-12, (n, inf)
+            assert rel <= 1e-10, (n, rel)
+    return ostate, dstate, worst
+
+
+FROZEN = dict(work_ceiling_rule="maxdim", expansion=dict(krylov_mode="arnoldi"))
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_fixture_setting_u1(dev, order):
+    run_pair(dev, 10, 5, "neel_state", 0.0, order, **FROZEN)
+
+
+def test_fixture_setting_none(dev):
+    run_pair(dev, 8, 3, "neel_state", 0.0, 2, sym="none", **FROZEN)
+
+
+def test_xx_domain_wall_l20(dev):
+    ostate, dstate, worst = run_pair(dev, 20, 20, "domain_wall_state", 0.0, 2, tol_basis=1e-3,
+                                     maxdim=64, check_every=5,
+                                     expansion=dict(mode="rank_tail", fixed_width=8))
+    h = mps_to_host(dstate)
+    exact = OM.free_fermion_sz(20, 20 * 0.05)
+    assert np.max(np.abs(OM.sz_profile(h) - exact)) < 1e-3
+
+
+def test_xxz_quench(dev):
+    run_pair(dev, 12, 6, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=32, check_every=3)
+
+
+def test_two_spin(dev):
+    DM, DS = dev
+    mpo = DM.xxz_mpo(2, J=1.0, delta=0.0)
+    psi = DM.product_state(["up", "down"])
+    t = 0.3
+    DS.cbe_bug_step(psi, mpo, -1j * t, tol_basis=1e-10, tol_trunc=1e-14, tol_expv=1e-13, maxdim=4)
+    v = OM.mps_to_dense(mps_to_host(psi))
+    v /= np.linalg.norm(v)
+    assert abs(abs(v[1]) - np.cos(t / 2)) < 1e-10
+    assert abs(abs(v[2]) - np.sin(t / 2)) < 1e-10
