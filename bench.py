@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the rank-adaptive BUG step (``cbe_bug_step``) on B200.
+
+Metric: BUG steps/s. Workload (the L = 64 U(1) XXZ quench): J = 1, delta = 0.5, domain-wall
+start, tau = -0.05i, order 2, tol_basis 1e-4, maxdim 256, bond_ceiling_factor 1.2, DD-QR
+:rank_tail with an 8-column sketch, Gaussians from a generator seeded 1234. A "step" is one
+``cbe_bug_step`` of the chain. ``--warmup W`` steps from the product state are untimed, then the
+next ``--steps K`` steps of the same trajectory are timed, each between CUDA events on the engine
+stream with a 256 MiB write (2x L2) flushing the cache before it.
+
+Printed JSON line: ``value`` (steps/s, HBM-resident state), ``e2e`` (the same K steps replayed
+through host buffers: the state and MPO uploaded and the new state downloaded every step),
+``roofline`` (the dominant kernel family from a profiled replay of the same K steps),
+``cpu_baseline`` (the CPU oracle over a bounded sample of the same steps), ``clocks``.
+``--impl reference`` times the CPU oracle (the restatement of the reference's CPU path) on the
+same steps. Under torchrun each rank runs an independent replica (the step does not shard).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(L=64, J=1.0, delta=0.5, tau=-0.05j, order=2, tol_basis=1e-4, maxdim=256,
+                bond_ceiling_factor=1.2, seed=1234)
+WORKLOAD_NAME = "xxz_quench_L64_delta0.5_domainwall_maxdim256_order2_tol1e-4"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def step_kwargs():
+    w = WORKLOAD
+    return dict(order=w["order"], tol_basis=w["tol_basis"], maxdim=w["maxdim"],
+                bond_ceiling_factor=w["bond_ceiling_factor"])
+
+
+def config_dict(args, ws, max_bond=None):
+    w = WORKLOAD
+    cfg = {"workload": WORKLOAD_NAME, "L": w["L"], "delta": w["delta"], "tau": "-0.05i",
+           "order": w["order"], "tol_basis": w["tol_basis"], "maxdim": w["maxdim"],
+           "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+           "l2": "flushed before every step (256 MiB write)",
+           "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+    if max_bond is not None:
+        cfg["max_bond_dim_after"] = max_bond
+    return cfg
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """``nvidia-smi`` clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measure_zgemm_tflops(torch, device):
+    """cuBLAS ZGEMM (torch.matmul, complex128, n = 4096) as the FP64 compute reference, burst."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device=device)
+    b = torch.randn(n, n, dtype=torch.complex128, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(device)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(device)
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return 8.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+
+        return max([i.get("num_threads", 1) for i in threadpool_info()] or [1])
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_steps(warmup, k):
+    """Run the CPU oracle over the same trajectory: ``warmup`` untimed steps, then ``k`` timed.
+    Returns (seconds for the k steps, bond dims after)."""
+    from oracle import models as OM
+    from oracle import step as OS
+
+    w = WORKLOAD
+    psi = OM.domain_wall_state(w["L"])
+    mpo = OM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
+    rng = np.random.default_rng(w["seed"])
+    for _ in range(warmup):
+        OS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+    t0 = time.perf_counter()
+    for _ in range(k):
+        OS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+    return time.perf_counter() - t0, psi.bond_dims()
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    k = args.steps
+    secs, bd = oracle_steps(args.warmup, k)
+    value = k / secs
+    cores = blas_threads()
+    line = {
+        "impl": "reference", "metric": "bug_steps_per_s", "value": value, "unit": "steps/s",
+        "n_gpus": ws, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * secs / k,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
+        "config": config_dict(args, ws, max(bd)),
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"steps {args.warmup + 1}..{args.warmup + k} of the quench, "
+                                   f"max bond dim after {max(bd)}"},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def mps_bytes(psi):
+    return sum(16 * t.nelem for t in psi.tensors)
+
+
+def run_engine(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from bondupdategalerkin_b200 import _engine as E
+    from bondupdategalerkin_b200 import build as Bld
+
+    if Bld.needs_build():
+        Bld.build()
+    E.set_default_device(local)
+    from bondupdategalerkin_b200 import models as DM
+    from bondupdategalerkin_b200 import step as DS
+    from bondupdategalerkin_b200 import tensor as DT
+
+    ctx = E.context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    w = WORKLOAD
+    psi = DM.domain_wall_state(w["L"])
+    mpo = DM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
+    rng = np.random.default_rng(w["seed"])
+    for _ in range(args.warmup):
+        DS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+    start_psi = psi.copy()
+    start_rng = rng.bit_generator.state
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    # ── timed region ──
+    ctx.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.launches()
+    evs = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        DS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        e1.record(stream)
+        evs.append((e0, e1))
+    ctx.synchronize()
+    torch.cuda.synchronize(dev)
+    launches = ctx.launches() - launches0
+    barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(sum(step_ms))
+    if ws > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * args.steps / (total_ms / 1e3)
+    final_dims = psi.bond_dims()
+
+    # ── profiled replay of the same steps (kernel durations on the engine stream) ──
+    psi_r = start_psi.copy()
+    rng_r = np.random.default_rng()
+    rng_r.bit_generator.state = start_rng
+    ctx.reset_stats()
+    ctx.set_profiling(True)
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        DS.cbe_bug_step(psi_r, mpo, w["tau"], rng=rng_r, **step_kwargs())
+    ctx.synchronize()
+    stats = ctx.kernel_stats()
+    ctx.set_profiling(False)
+    assert psi_r.bond_dims() == final_dims, "profiled replay diverged from the timed steps"
+
+    # ── end to end through host buffers: upload state+MPO, step, download the new state ──
+    from bondupdategalerkin_b200.api import step_host
+
+    host_state = [DT.to_blocks(t) for t in start_psi.tensors]
+    host_mpo = [DT.to_blocks(t) for t in mpo.tensors]
+    rng_e = np.random.default_rng()
+    rng_e.bit_generator.state = start_rng
+    center = start_psi.center
+    e2e_ms, h2d, d2h = 0.0, 0, 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        host_state, center, io = step_host(host_state, center, host_mpo, w["tau"], rng=rng_e,
+                                           **step_kwargs())
+        e1.record(stream)
+        ctx.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        h2d += io["h2d_bytes"]
+        d2h += io["d2h_bytes"]
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = ws * args.steps / (e2e_ms / 1e3)
+
+    # ── roofline of the dominant kernel family ──
+    hbm_peak, hbm_src = measured_peaks()
+    fam = max(stats, key=lambda f: stats[f]["ms"])
+    st = stats[fam]
+    per_launch_ms = st["ms"] / max(st["launches"], 1)
+    zgemm = None
+    if fam == "gemm":
+        zgemm = measure_zgemm_tflops(torch, dev)
+        achieved = st["flops"] / max(st["launches"], 1) / (per_launch_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": zgemm, "unit": "TFLOP/s",
+                "frac": achieved / zgemm, "traffic": None,
+                "peak_source": "cuBLAS ZGEMM (torch.matmul complex128 4096^3) measured in this run"}
+    else:
+        achieved = st["bytes"] / max(st["launches"], 1) / (per_launch_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
+    tot_ms = sum(s["ms"] for s in stats.values())
+    roof["kernel"] = E.KERNEL_NAMES[fam]
+    roof["launches"] = st["launches"]
+    roof["avg_launch_us"] = 1e3 * per_launch_ms
+    roof["share_of_device_time"] = st["ms"] / tot_ms if tot_ms > 0 else None
+    roof["families"] = {f: {"launches": s["launches"], "ms": round(s["ms"], 3)} for f, s in stats.items()}
+
+    line = {
+        "metric": "bug_steps_per_s", "value": value, "unit": "steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
+        "config": config_dict(args, ws, max(final_dims)),
+        "gpu_launches": int(launches),
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps},
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        k = min(args.cpu_steps, args.steps)
+        secs, _ = oracle_steps(args.warmup, k)
+        line["cpu_baseline"] = {"value": k / secs, "unit": "steps/s", "cores": blas_threads(),
+                                "kind": "port",
+                                "sample": f"CPU oracle, steps {args.warmup + 1}..{args.warmup + k} "
+                                          "of the same trajectory"}
+    if zgemm is not None:
+        line["fp64_zgemm_tflops_measured"] = zgemm
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

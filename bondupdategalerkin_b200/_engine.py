@@ -26,6 +26,11 @@ SIGNATURES = {
     "bug_ctx_synchronize": (ctypes.c_int, [_vp]),
     "bug_ctx_launches": (ctypes.c_int64, [_vp]),
     "bug_ctx_bytes_in_use": (ctypes.c_int64, [_vp]),
+    "bug_ctx_stream": (_vp, [_vp]),
+    "bug_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "bug_ctx_kernel_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                            _c_double_p, _c_double_p, _c_double_p]),
+    "bug_ctx_reset_stats": (ctypes.c_int, [_vp]),
     "bug_tensor_create": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p,
                                          ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_tensor_upload": (ctypes.c_int, [_vp, _vp, _c_double_p, ctypes.c_int64]),
@@ -49,6 +54,10 @@ SIGNATURES = {
     "bug_oplus": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
 }
+
+FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
+KERNEL_NAMES = {"copy": "copy_kernel", "gemm": "gemm_kernel", "svd": "jacobi_svd_kernel",
+                "dot": "dot_kernel", "lincomb": "lincomb_kernel", "scale": "scale_kernel"}
 
 STATUS = {0: "BUG_OK", 1: "BUG_EINVAL", 2: "BUG_ENONFINITE", 3: "BUG_ENOMEM", 4: "BUG_ETIMEOUT",
           5: "BUG_EDEVICE", 6: "BUG_ENOTCONV"}
@@ -108,12 +117,40 @@ class Context:
     def bytes_in_use(self) -> int:
         return int(self.lib.bug_ctx_bytes_in_use(self.h))
 
+    def stream(self) -> int:
+        """The context's ``cudaStream_t`` as an integer (for ``torch.cuda.ExternalStream``)."""
+        return int(self.lib.bug_ctx_stream(self.h) or 0)
+
+    def set_profiling(self, on: bool) -> None:
+        check(self.lib.bug_ctx_set_profiling(self.h, int(on)))
+
+    def reset_stats(self) -> None:
+        check(self.lib.bug_ctx_reset_stats(self.h))
+
+    def kernel_stats(self) -> dict:
+        """Per kernel family: launches, algorithmic flops and bytes, device ms (profiling only)."""
+        out = {}
+        for fam, name in enumerate(FAMILIES):
+            n = ctypes.c_int64()
+            f, b, ms = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+            check(self.lib.bug_ctx_kernel_stats(self.h, fam, ctypes.byref(n), ctypes.byref(f),
+                                                ctypes.byref(b), ctypes.byref(ms)))
+            out[name] = dict(launches=int(n.value), flops=f.value, bytes=b.value, ms=ms.value)
+        return out
+
 
 _ctx = {}
+_default_device = [0]
 
 
-def context(device: int = 0) -> Context:
+def set_default_device(device: int) -> None:
+    """Device used by ``context()`` when none is given (one process per GPU sets its own)."""
+    _default_device[0] = int(device)
+
+
+def context(device: int | None = None) -> Context:
     """The process-wide context of ``device`` (created on first use)."""
+    device = _default_device[0] if device is None else device
     c = _ctx.get(device)
     if c is None:
         c = Context(device)

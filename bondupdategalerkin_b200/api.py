@@ -1,0 +1,46 @@
+"""Public entry points of the B200 BUG engine.
+
+* ``cbe_bug_step(psi, mpo, tau; ...)`` -- the drop-in for ``cbe_bug_step!``
+  (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on HBM-resident states (``step.py``);
+* ``step_host(...)`` -- the same step for a caller whose state lives in host memory: the site
+  tensors and the MPO are uploaded, the step runs on the device, and the new site tensors come back
+  (the shape of a ``ccall`` from a Julia host that keeps its own containers);
+* ``magnetisation(psi)`` -- ``<S^z_j>`` for every site (``src/QMB/Observables/bond_observables.jl:15``).
+"""
+
+from __future__ import annotations
+
+from .models import MPO, MPS, domain_wall_state, neel_state, product_state, sz_profile, xxz_mpo
+from .step import DDQRExpansion, cbe_bug_step
+from .tensor import from_blocks, to_blocks
+
+__all__ = ["cbe_bug_step", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
+           "domain_wall_state", "neel_state", "product_state", "xxz_mpo"]
+
+
+def magnetisation(psi):
+    return sz_profile(psi)
+
+
+def step_host(host_state, center, host_mpo, tau, **kwargs):
+    """One BUG step on host-resident data.
+
+    ``host_state`` / ``host_mpo``: per site ``(legs, {key: ndarray})`` as ``tensor.to_blocks``
+    returns. Returns ``(new_host_state, new_center, io)`` with ``io`` holding the bytes moved each
+    way and the step info."""
+    h2d = 0
+    sites = []
+    for legs, blocks in host_state:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        sites.append(t)
+    ws = []
+    for legs, blocks in host_mpo:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        ws.append(t)
+    psi = MPS(sites, center)
+    info = cbe_bug_step(psi, MPO(ws), tau, **kwargs)
+    out = [to_blocks(t) for t in psi.tensors]
+    d2h = sum(16 * t.nelem for t in psi.tensors)
+    return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)

@@ -121,6 +121,47 @@ struct bug_ctx {
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
   int64_t bytes = 0;
+  // per kernel family: launches, algorithmic flops and bytes, device time (profiling only)
+  int64_t k_launches[BUG_K_NFAMILIES] = {};
+  double k_flops[BUG_K_NFAMILIES] = {};
+  double k_bytes[BUG_K_NFAMILIES] = {};
+  double k_ms[BUG_K_NFAMILIES] = {};
+  bool profiling = false;
+  struct Pending {
+    int fam;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
+  cudaEvent_t cur_start = nullptr;
+  cudaEvent_t take_event() {
+    if (event_pool.empty()) {
+      cudaEvent_t e;
+      BUG_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = event_pool.back();
+    event_pool.pop_back();
+    return e;
+  }
+  void harvest() {
+    if (pending.empty()) return;
+    BUG_CUDA(cudaEventSynchronize(pending.back().b));
+    for (auto& p : pending) {
+      float ms = 0.f;
+      BUG_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+      k_ms[p.fam] += ms;
+      event_pool.push_back(p.a);
+      event_pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+  void begin() {
+    if (profiling) {
+      cur_start = take_event();
+      BUG_CUDA(cudaEventRecord(cur_start, stream));
+    }
+  }
   // pinned staging ring for descriptor uploads
   static constexpr int kSlots = 32;
   void* stage_ptr[kSlots] = {};
@@ -170,9 +211,19 @@ struct bug_ctx {
     g_active_ctx = this;
     return dptr;
   }
-  void launched() {
+  void launched(int fam, double flops, double bytes_moved) {
     ++launches;
     BUG_CUDA(cudaGetLastError());
+    k_launches[fam] += 1;
+    k_flops[fam] += flops;
+    k_bytes[fam] += bytes_moved;
+    if (profiling && cur_start) {
+      cudaEvent_t e = take_event();
+      BUG_CUDA(cudaEventRecord(e, stream));
+      pending.push_back({fam, cur_start, e});
+      cur_start = nullptr;
+      if (pending.size() > 8192) harvest();
+    }
   }
   void flush() {
     for (void* p : deferred) BUG_CUDA(cudaFreeAsync(p, stream));
@@ -294,8 +345,9 @@ void run_copies(bug_ctx* c, std::vector<CopyDesc>& descs) {
   }
   if (nz.empty()) return;
   CopyDesc* dd = c->push(nz);
+  c->begin();
   bugk::launch_copy(dd, int(nz.size()), total, c->stream);
-  c->launched();
+  c->launched(BUG_K_COPY, 0.0, 32.0 * double(total));
 }
 
 CopyDesc plain_copy(const double2* src, double2* dst, int64_t n, bool conj, double2 alpha,
@@ -499,8 +551,17 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   GemmOut* d_outs = c->push(outs);
   GemmPair* d_pairs = c->push(pairs);
   GemmTile* d_tiles = c->push(tiles);
+  double flops = 0.0, gbytes = 0.0;
+  for (auto& go : outs) {
+    gbytes += 16.0 * double(go.m) * double(go.n);
+    for (int p = go.pair_begin; p < go.pair_end; ++p) {
+      flops += 8.0 * double(go.m) * double(go.n) * double(pairs[p].k);
+      gbytes += 16.0 * (double(go.m) + double(go.n)) * double(pairs[p].k);
+    }
+  }
+  c->begin();
   bugk::launch_gemm(d_outs, d_pairs, d_tiles, int(tiles.size()), c->stream);
-  c->launched();
+  c->launched(BUG_K_GEMM, flops, gbytes);
   return out;  // Ap/Bp are released stream-ordered
 }
 
@@ -654,8 +715,15 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
   }
   if (np > 0) {
     SvdDesc* dsd = c->push(sd);
+    double sbytes = 0.0, sflops = 0.0;
+    for (int s2 = 0; s2 < np; ++s2) {
+      double mm = double(std::max(order[s2]->m, order[s2]->n)), r = double(std::min(order[s2]->m, order[s2]->n));
+      sbytes += 16.0 * (2.0 * mm * r + r * r + (order[s2]->m + order[s2]->n) * r);
+      sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
+    }
+    c->begin();
     bugk::launch_svd(dsd, np, max_smem, c->stream);
-    c->launched();
+    c->launched(BUG_K_SVD, sflops, sbytes);
   }
   // read back singular values and sweep counts
   const size_t nread = size_t(stot) + size_t(np);
@@ -818,12 +886,16 @@ void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_t
   double2* res = static_cast<double2*>(c->scratch(std::max(nout, 1) * sizeof(double2)));
   if (!descs.empty()) {
     DotDesc* dd = c->push(descs);
+    double dbytes = 0.0;
+    for (auto& d : descs) dbytes += 32.0 * double(d.n);
+    c->begin();
     bugk::launch_dot(dd, int(descs.size()), partial, c->stream);
-    c->launched();
+    c->launched(BUG_K_DOT, 0.0, dbytes);
   }
   int* dseg = c->push(seg);
+  c->begin();
   bugk::launch_dot_reduce(partial, dseg, nout, res, c->stream);
-  c->launched();
+  c->launched(BUG_K_DOT, 0.0, 16.0 * double(descs.size()));
   double* host = c->readback(size_t(2 * std::max(nout, 1)));
   BUG_CUDA(cudaMemcpyAsync(host, res, size_t(nout) * sizeof(double2), cudaMemcpyDeviceToHost,
                            c->stream));
@@ -865,8 +937,11 @@ std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
   if (!outs.empty()) {
     LinOut* dout = c->push(outs);
     LinSrc* dsrc = c->push(srcs);
+    double lbytes = 0.0;
+    for (auto& o : outs) lbytes += 16.0 * double(o.n) * double(o.src_end - o.src_begin + 1);
+    c->begin();
     bugk::launch_lincomb(dout, int(outs.size()), dsrc, total, c->stream);
-    c->launched();
+    c->launched(BUG_K_LINCOMB, 0.0, lbytes);
   }
   return out;
 }
@@ -946,6 +1021,39 @@ int bug_ctx_synchronize(bug_ctx* c) {
 }
 
 int64_t bug_ctx_launches(const bug_ctx* c) { return c ? c->launches : 0; }
+
+void* bug_ctx_stream(bug_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int bug_ctx_set_profiling(bug_ctx* c, int on) {
+  return guard([&] {
+    require(c != nullptr, "null context");
+    c->harvest();
+    c->profiling = on != 0;
+  });
+}
+
+int bug_ctx_kernel_stats(bug_ctx* c, int family, int64_t* launches, double* flops, double* bytes,
+                         double* device_ms) {
+  return guard([&] {
+    require(c && family >= 0 && family < BUG_K_NFAMILIES, "bad argument");
+    c->harvest();
+    *launches = c->k_launches[family];
+    *flops = c->k_flops[family];
+    *bytes = c->k_bytes[family];
+    *device_ms = c->k_ms[family];
+  });
+}
+
+int bug_ctx_reset_stats(bug_ctx* c) {
+  return guard([&] {
+    require(c != nullptr, "null context");
+    c->harvest();
+    for (int f = 0; f < BUG_K_NFAMILIES; ++f) {
+      c->k_launches[f] = 0;
+      c->k_flops[f] = c->k_bytes[f] = c->k_ms[f] = 0.0;
+    }
+  });
+}
 int64_t bug_ctx_bytes_in_use(const bug_ctx* c) { return c ? c->bytes : 0; }
 
 int bug_tensor_create(bug_ctx* c, int rank, const int* dirs, const int* nsec, const int* charges,
@@ -1095,8 +1203,9 @@ int bug_scale_leg(bug_ctx* c, const bug_tensor* t, int leg, const double* w, bug
     }
     if (!descs.empty()) {
       ScaleDesc* dd = c->push(descs);
+      c->begin();
       bugk::launch_scale(dd, int(descs.size()), total, c->stream);
-      c->launched();
+      c->launched(BUG_K_SCALE, 0.0, 32.0 * double(total));
     }
     *out = o.release();
   });

@@ -58,6 +58,26 @@ int bug_ctx_synchronize(bug_ctx* ctx);
 int64_t bug_ctx_launches(const bug_ctx* ctx);
 /* Bytes currently held by tensors of this context. */
 int64_t bug_ctx_bytes_in_use(const bug_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that time it with their own events. */
+void* bug_ctx_stream(bug_ctx* ctx);
+
+/* Kernel families for bug_ctx_kernel_stats. No reference counterpart: the reference's
+ * KernelCounters (src/BUG/Core/diagnostics.jl:17-53) count calls and seconds per kernel family on
+ * the CPU; these count device launches, algorithmic flops/bytes and (when profiling) device time. */
+enum {
+  BUG_K_COPY = 0,     /* strided gathers: permutes, packing, direct sums, trims */
+  BUG_K_GEMM = 1,     /* segmented grouped complex GEMM */
+  BUG_K_SVD = 2,      /* batched Jacobi SVD */
+  BUG_K_DOT = 3,      /* inner products and norms */
+  BUG_K_LINCOMB = 4,  /* linear combinations */
+  BUG_K_SCALE = 5,    /* leg scaling (U*S, S*Vd) */
+  BUG_K_NFAMILIES = 6
+};
+/* Profiling on: every launch is bracketed by CUDA events on the context stream. */
+int bug_ctx_set_profiling(bug_ctx* ctx, int on);
+int bug_ctx_kernel_stats(bug_ctx* ctx, int family, int64_t* launches, double* flops, double* bytes,
+                         double* device_ms);
+int bug_ctx_reset_stats(bug_ctx* ctx);
 
 /* ── tensors: create / upload / download / inspect ────────────────────────────────────────── */
 /* A zero tensor with the given legs and block keys (TLArray construction,
@@ -118,11 +138,6 @@ int bug_oplus(bug_ctx* ctx, int n, const bug_tensor* const* t, int leg, bug_tens
 /* Keep the leading counts[s] entries of sector s (ascending sector order) of `leg`
  * (_trim_per_sector, truncation.jl:283-288). *out is NULL when nothing is kept. */
 int bug_trim(bug_ctx* ctx, const bug_tensor* t, int leg, const int* counts, bug_tensor** out);
-
-/* ── fused root solve ─────────────────────────────────────────────────────────────────────── */
-/* The zero-site generator H0 S = sum_w L[w] S R[w] (zero_site_h/apply_zero_site,
- * effective_operators.jl:91-107), applied n times in one call is not needed by the host; the
- * root Krylov loop instead runs on device through bug_contract/bug_inner_many/bug_lincomb. */
 
 #ifdef __cplusplus
 }
