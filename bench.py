@@ -208,8 +208,12 @@ def run_engine(args):
         Bld.build()
     E.set_default_device(local)
     from bondupdategalerkin_b200 import models as DM
-    from bondupdategalerkin_b200 import step as DS
     from bondupdategalerkin_b200 import tensor as DT
+
+    if args.host == "python":
+        from bondupdategalerkin_b200 import step as DS
+    else:
+        from bondupdategalerkin_b200 import native as DS
 
     ctx = E.context(local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
@@ -256,6 +260,16 @@ def run_engine(args):
         total_ms = float(t.item())
     value = ws * args.steps / (total_ms / 1e3)
     final_dims = psi.bond_dims()
+    if args.no_replay:
+        if rank == 0:
+            print(json.dumps({"metric": "bug_steps_per_s", "value": value, "unit": "steps/s",
+                              "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": total_ms / args.steps, "gpu_launches": int(launches),
+                              "note": "--no-replay: timing run only (no e2e, roofline or baseline)"}),
+                  flush=True)
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
 
     # ── profiled replay of the same steps (kernel durations on the engine stream) ──
     psi_r = start_psi.copy()
@@ -287,7 +301,7 @@ def run_engine(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         host_state, center, io = step_host(host_state, center, host_mpo, w["tau"], rng=rng_e,
-                                           **step_kwargs())
+                                           native=args.host == "native", **step_kwargs())
         e1.record(stream)
         ctx.synchronize()
         e2e_ms += e0.elapsed_time(e1)
@@ -328,7 +342,7 @@ def run_engine(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
-        "config": config_dict(args, ws, max(final_dims)),
+        "config": dict(config_dict(args, ws, max(final_dims)), host=args.host),
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
@@ -358,9 +372,19 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--host", default="native", choices=["native", "python"],
+                    help="native: the step runs inside libbug_b200.so; python: the Python host")
+    ap.add_argument("--no-replay", action="store_true",
+                    help="time the steps only (for profiler runs)")
+    ap.add_argument("--L", type=int, default=None,
+                    help="chain length override (smaller cases for profiler captures only)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.L is not None:
+        WORKLOAD["L"] = args.L
+        global WORKLOAD_NAME
+        WORKLOAD_NAME = WORKLOAD_NAME.replace("L64", f"L{args.L}")
     if args.impl == "reference":
         run_reference(args)
     else:

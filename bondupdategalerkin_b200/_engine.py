@@ -53,7 +53,12 @@ SIGNATURES = {
     "bug_flip_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     "bug_oplus": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
+    "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
+    "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
+    "bug_la_eigvals_hess": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
 }
+# declared in native.py (structure arguments)
+NATIVE_ONLY = ("bug_mps_step",)
 
 FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
 KERNEL_NAMES = {"copy": "copy_kernel", "gemm": "gemm_kernel", "svd": "jacobi_svd_kernel",

@@ -1,7 +1,10 @@
 """Public entry points of the B200 BUG engine.
 
 * ``cbe_bug_step(psi, mpo, tau; ...)`` -- the drop-in for ``cbe_bug_step!``
-  (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on HBM-resident states (``step.py``);
+  (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on HBM-resident states, run as one call into the
+  library (``native.py``); ``cbe_bug_step_python_host`` is the same step with the sweep logic in
+  Python over the kernel-granular C-ABI (``step.py``), the shape of a Julia host that keeps its
+  sweeps;
 * ``step_host(...)`` -- the same step for a caller whose state lives in host memory: the site
   tensors and the MPO are uploaded, the step runs on the device, and the new site tensors come back
   (the shape of a ``ccall`` from a Julia host that keeps its own containers);
@@ -11,10 +14,12 @@
 from __future__ import annotations
 
 from .models import MPO, MPS, domain_wall_state, neel_state, product_state, sz_profile, xxz_mpo
-from .step import DDQRExpansion, cbe_bug_step
+from .native import cbe_bug_step
+from .step import DDQRExpansion
+from .step import cbe_bug_step as cbe_bug_step_python_host
 from .tensor import from_blocks, to_blocks
 
-__all__ = ["cbe_bug_step", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
+__all__ = ["cbe_bug_step", "cbe_bug_step_python_host", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
            "domain_wall_state", "neel_state", "product_state", "xxz_mpo"]
 
 
@@ -22,7 +27,7 @@ def magnetisation(psi):
     return sz_profile(psi)
 
 
-def step_host(host_state, center, host_mpo, tau, **kwargs):
+def step_host(host_state, center, host_mpo, tau, native=True, **kwargs):
     """One BUG step on host-resident data.
 
     ``host_state`` / ``host_mpo``: per site ``(legs, {key: ndarray})`` as ``tensor.to_blocks``
@@ -40,7 +45,8 @@ def step_host(host_state, center, host_mpo, tau, **kwargs):
         h2d += 16 * t.nelem
         ws.append(t)
     psi = MPS(sites, center)
-    info = cbe_bug_step(psi, MPO(ws), tau, **kwargs)
+    step = cbe_bug_step if native else cbe_bug_step_python_host
+    info = step(psi, MPO(ws), tau, **kwargs)
     out = [to_blocks(t) for t in psi.tensors]
     d2h = sum(16 * t.nelem for t in psi.tensors)
     return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)

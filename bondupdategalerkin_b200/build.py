@@ -6,7 +6,7 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "kernels.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "kernels.cu", "step.cu")]
 OUTPUT = os.path.join(HERE, "libbug_b200.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared"]
@@ -16,7 +16,7 @@ def needs_build() -> bool:
     if not os.path.exists(OUTPUT):
         return True
     t = os.path.getmtime(OUTPUT)
-    deps = SOURCES + [os.path.join(HERE, "csrc", "kernels.cuh"),
+    deps = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "engine.h", "smallla.h")] + [
                       os.path.join(os.path.dirname(HERE), "include", "bug_b200.h")]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 

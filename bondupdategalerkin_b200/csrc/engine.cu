@@ -1,246 +1,17 @@
-// Host side of the B200 block-sparse engine: tensor metadata, the contraction and SVD planners,
-// descriptor staging, and the C-ABI of include/bug_b200.h.
+// Host side of the B200 block-sparse engine: the contraction and SVD planners, descriptor staging,
+// and the C-ABI of include/bug_b200.h.
 //
 // A tensor keeps its block table on the host (sorted keys, shapes, offsets) and its payload in
 // one HBM allocation from the device's stream-ordered memory pool. Every operation plans on the
 // host from the block tables, ships one descriptor array per kernel through a pinned staging
 // ring, and launches a handful of kernels on the context stream; only operations whose result
 // the host must read (norms, inner products, singular values, downloads) synchronise.
-#include "../../include/bug_b200.h"
-#include "kernels.cuh"
+#include "engine.h"
 
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <array>
-#include <cmath>
-#include <cstring>
-#include <functional>
-#include <map>
-#include <memory>
-#include <stdexcept>
-#include <string>
-#include <vector>
-
-using bugk::CopyDesc;
-using bugk::DotDesc;
-using bugk::GemmOut;
-using bugk::GemmPair;
-using bugk::GemmTile;
-using bugk::LinOut;
-using bugk::LinSrc;
-using bugk::ScaleDesc;
-using bugk::SvdDesc;
-
-namespace {
+namespace bugi {
 
 thread_local std::string g_err;
-
-struct BugError : std::runtime_error {
-  int code;
-  BugError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define BUG_CUDA(call)                                                                   \
-  do {                                                                                   \
-    cudaError_t e_ = (call);                                                             \
-    if (e_ != cudaSuccess)                                                               \
-      throw BugError(e_ == cudaErrorMemoryAllocation ? BUG_ENOMEM : BUG_EDEVICE,         \
-                     std::string(#call) + ": " + cudaGetErrorString(e_));                \
-  } while (0)
-
-inline void require(bool ok, const std::string& msg) {
-  if (!ok) throw BugError(BUG_EINVAL, msg);
-}
-
-using Key = std::array<int, BUG_MAX_RANK>;
-
-struct Leg {
-  int dir = 1;
-  std::vector<int> q;  // ascending charges
-  std::vector<int> d;  // dimensions
-  int dim_of(int c) const {
-    auto it = std::lower_bound(q.begin(), q.end(), c);
-    return (it != q.end() && *it == c) ? d[it - q.begin()] : 0;
-  }
-  int index_of(int c) const {
-    auto it = std::lower_bound(q.begin(), q.end(), c);
-    return (it != q.end() && *it == c) ? int(it - q.begin()) : -1;
-  }
-  int64_t total() const {
-    int64_t s = 0;
-    for (int x : d) s += x;
-    return s;
-  }
-};
-
-struct Block {
-  Key key{};
-  std::array<int, BUG_MAX_RANK> shape{};
-  int64_t off = 0;
-  int64_t size = 0;
-};
-
-}  // namespace
-
-struct bug_ctx;
-
-namespace {
-
-// The context whose scratch the current C-ABI call queued for release (freed, stream-ordered,
-// when the call returns).
 thread_local bug_ctx* g_active_ctx = nullptr;
-
-struct Buffer {
-  double2* ptr = nullptr;
-  int64_t n = 0;
-  bug_ctx* ctx = nullptr;
-  ~Buffer();
-};
-
-}  // namespace
-
-struct bug_tensor {
-  int rank = 0;
-  std::vector<Leg> legs;
-  std::vector<Block> blocks;  // ascending keys, payload laid out in this order
-  std::map<Key, int> index;
-  int64_t nelem = 0;
-  std::shared_ptr<Buffer> buf;
-
-  int find(const Key& k) const {
-    auto it = index.find(k);
-    return it == index.end() ? -1 : it->second;
-  }
-  const double2* data(int b) const { return buf->ptr + blocks[b].off; }
-  double2* mdata(int b) { return buf->ptr + blocks[b].off; }
-};
-
-struct bug_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int64_t launches = 0;
-  int64_t bytes = 0;
-  // per kernel family: launches, algorithmic flops and bytes, device time (profiling only)
-  int64_t k_launches[BUG_K_NFAMILIES] = {};
-  double k_flops[BUG_K_NFAMILIES] = {};
-  double k_bytes[BUG_K_NFAMILIES] = {};
-  double k_ms[BUG_K_NFAMILIES] = {};
-  bool profiling = false;
-  struct Pending {
-    int fam;
-    cudaEvent_t a, b;
-  };
-  std::vector<Pending> pending;
-  std::vector<cudaEvent_t> event_pool;
-  cudaEvent_t cur_start = nullptr;
-  cudaEvent_t take_event() {
-    if (event_pool.empty()) {
-      cudaEvent_t e;
-      BUG_CUDA(cudaEventCreate(&e));
-      return e;
-    }
-    cudaEvent_t e = event_pool.back();
-    event_pool.pop_back();
-    return e;
-  }
-  void harvest() {
-    if (pending.empty()) return;
-    BUG_CUDA(cudaEventSynchronize(pending.back().b));
-    for (auto& p : pending) {
-      float ms = 0.f;
-      BUG_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
-      k_ms[p.fam] += ms;
-      event_pool.push_back(p.a);
-      event_pool.push_back(p.b);
-    }
-    pending.clear();
-  }
-  void begin() {
-    if (profiling) {
-      cur_start = take_event();
-      BUG_CUDA(cudaEventRecord(cur_start, stream));
-    }
-  }
-  // pinned staging ring for descriptor uploads
-  static constexpr int kSlots = 32;
-  void* stage_ptr[kSlots] = {};
-  size_t stage_cap[kSlots] = {};
-  cudaEvent_t stage_ev[kSlots] = {};
-  bool stage_used[kSlots] = {};
-  int stage_next = 0;
-  std::vector<void*> deferred;  // device scratch to free after the next launch
-  double* pinned_out = nullptr;  // small pinned buffer for results read back by the host
-  size_t pinned_out_cap = 0;
-
-  void* stage(size_t bytes) {
-    int s = stage_next;
-    stage_next = (stage_next + 1) % kSlots;
-    if (stage_used[s]) BUG_CUDA(cudaEventSynchronize(stage_ev[s]));
-    if (stage_cap[s] < bytes) {
-      if (stage_ptr[s]) BUG_CUDA(cudaFreeHost(stage_ptr[s]));
-      size_t cap = std::max<size_t>(bytes, 1 << 16);
-      BUG_CUDA(cudaHostAlloc(&stage_ptr[s], cap, cudaHostAllocDefault));
-      stage_cap[s] = cap;
-    }
-    cur_slot = s;
-    return stage_ptr[s];
-  }
-  int cur_slot = 0;
-  void stage_done() {
-    BUG_CUDA(cudaEventRecord(stage_ev[cur_slot], stream));
-    stage_used[cur_slot] = true;
-  }
-  template <class T>
-  T* push(const std::vector<T>& v) {
-    size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
-    void* h = stage(bytes);
-    if (!v.empty()) std::memcpy(h, v.data(), v.size() * sizeof(T));
-    void* dptr = nullptr;
-    BUG_CUDA(cudaMallocAsync(&dptr, bytes, stream));
-    BUG_CUDA(cudaMemcpyAsync(dptr, h, bytes, cudaMemcpyHostToDevice, stream));
-    stage_done();
-    deferred.push_back(dptr);
-    g_active_ctx = this;
-    return static_cast<T*>(dptr);
-  }
-  void* scratch(size_t bytes) {
-    void* dptr = nullptr;
-    BUG_CUDA(cudaMallocAsync(&dptr, std::max<size_t>(bytes, 16), stream));
-    deferred.push_back(dptr);
-    g_active_ctx = this;
-    return dptr;
-  }
-  void launched(int fam, double flops, double bytes_moved) {
-    ++launches;
-    BUG_CUDA(cudaGetLastError());
-    k_launches[fam] += 1;
-    k_flops[fam] += flops;
-    k_bytes[fam] += bytes_moved;
-    if (profiling && cur_start) {
-      cudaEvent_t e = take_event();
-      BUG_CUDA(cudaEventRecord(e, stream));
-      pending.push_back({fam, cur_start, e});
-      cur_start = nullptr;
-      if (pending.size() > 8192) harvest();
-    }
-  }
-  void flush() {
-    for (void* p : deferred) BUG_CUDA(cudaFreeAsync(p, stream));
-    deferred.clear();
-  }
-  double* readback(size_t n) {
-    if (pinned_out_cap < n) {
-      if (pinned_out) BUG_CUDA(cudaFreeHost(pinned_out));
-      pinned_out_cap = std::max<size_t>(n, 4096);
-      BUG_CUDA(cudaHostAlloc((void**)&pinned_out, pinned_out_cap * sizeof(double),
-                             cudaHostAllocDefault));
-    }
-    return pinned_out;
-  }
-};
-
-namespace {
 
 Buffer::~Buffer() {
   if (ptr && ctx) {
@@ -406,7 +177,49 @@ std::unique_ptr<bug_tensor> permute_impl(bug_ctx* c, const bug_tensor& t, const 
   return out;
 }
 
-// ── contraction ──────────────────────────────────────────────────────────────────────────────
+// ── contraction ──
+
+// View one block as a matrix: rows = legs `rl` (C order), cols = legs `cl`; adjacent dims whose
+// strides chain are merged, so the kernel decomposes as few indices as possible.
+void make_group(const Block& b, const std::array<int64_t, BUG_MAX_RANK>& st,
+                const std::vector<int>& legs, int& n, int* d, int64_t* s) {
+  std::vector<int> dd;
+  std::vector<int64_t> ss;
+  for (int l : legs) {
+    if (!dd.empty() && ss.back() == int64_t(b.shape[l]) * st[l]) {
+      dd.back() *= b.shape[l];
+      ss.back() = st[l];
+    } else {
+      dd.push_back(b.shape[l]);
+      ss.push_back(st[l]);
+    }
+  }
+  // drop unit dims
+  std::vector<int> d2;
+  std::vector<int64_t> s2;
+  for (size_t i = 0; i < dd.size(); ++i)
+    if (dd[i] != 1) {
+      d2.push_back(dd[i]);
+      s2.push_back(ss[i]);
+    }
+  require(int(d2.size()) <= bugk::kGroup, "contract: operand index group too deep");
+  n = int(d2.size());
+  for (int i = 0; i < n; ++i) {
+    d[i] = d2[i];
+    s[i] = s2[i];
+  }
+}
+
+void make_operand(bugk::Operand& op, const double2* p, const Block& b, const std::vector<int>& rows,
+                  const std::vector<int>& cols, bool conj) {
+  // shape entries past the tensor's rank are 1, so full-rank C strides equal the tensor's own
+  const auto st = c_strides(b.shape, BUG_MAX_RANK);
+  op.p = p;
+  op.conj = conj ? 1 : 0;
+  make_group(b, st, rows, op.nr, op.rd, op.rs);
+  make_group(b, st, cols, op.nc, op.cd, op.cs);
+  op.row_fast = (op.nr > 0 && op.rs[op.nr - 1] == 1) ? 1 : 0;
+}
 
 std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int n, const int* ia,
                                           const bug_tensor& B0, const int* ib, bool conja,
@@ -438,56 +251,11 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   for (int i : fa) legs.push_back(conja ? flipped(A0.legs[i]) : A0.legs[i]);
   for (int i : fb) legs.push_back(conjb ? flipped(B0.legs[i]) : B0.legs[i]);
 
-  // operand layouts: contracted legs trailing (N) or leading (T), else permute
-  bool a_tail = true, a_head = true, b_tail = true, b_head = true;
-  for (int k = 0; k < n; ++k) {
-    if (ia[k] != A0.rank - n + k) a_tail = false;
-    if (ia[k] != k) a_head = false;
-    if (ib[k] != B0.rank - n + k) b_tail = false;
-    if (ib[k] != k) b_head = false;
-  }
-  std::unique_ptr<bug_tensor> Ap, Bp;
   const bug_tensor* A = &A0;
   const bug_tensor* B = &B0;
-  int opa = 0, opb = 0;  // bit0: transposed storage
   std::vector<int> iaa(ia, ia + n), ibb(ib, ib + n);
-  if (n == 0) {
-    opa = 0;
-    opb = 0;
-  } else {
-    if (a_tail) opa = 0;
-    else if (a_head) opa = 1;
-    else {
-      std::vector<int> perm(fa);
-      for (int k = 0; k < n; ++k) perm.push_back(ia[k]);
-      Ap = permute_impl(c, A0, perm.data());
-      A = Ap.get();
-      for (int k = 0; k < n; ++k) iaa[k] = int(fa.size()) + k;
-      opa = 0;
-    }
-    if (b_head) opb = 0;
-    else if (b_tail) opb = 1;
-    else {
-      std::vector<int> perm(ib, ib + n);
-      for (int i : fb) perm.push_back(i);
-      Bp = permute_impl(c, B0, perm.data());
-      B = Bp.get();
-      for (int k = 0; k < n; ++k) ibb[k] = k;
-      opb = 0;
-    }
-  }
-  // free-leg positions in the (possibly permuted) operands
-  std::vector<int> fa2, fb2;
-  {
-    std::vector<bool> c2(A->rank, false);
-    for (int k = 0; k < n; ++k) c2[iaa[k]] = true;
-    for (int i = 0; i < A->rank; ++i)
-      if (!c2[i]) fa2.push_back(i);
-    std::vector<bool> d2(B->rank, false);
-    for (int k = 0; k < n; ++k) d2[ibb[k]] = true;
-    for (int i = 0; i < B->rank; ++i)
-      if (!d2[i]) fb2.push_back(i);
-  }
+  const std::vector<int>& fa2 = fa;
+  const std::vector<int>& fb2 = fb;
   // match blocks
   std::map<std::vector<int>, std::vector<int>> groups;
   for (int bi = 0; bi < int(B->blocks.size()); ++bi) {
@@ -533,13 +301,9 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
       int64_t K = 1;
       for (int k = 0; k < n; ++k) K *= ab.shape[iaa[k]];
       GemmPair gp{};
-      gp.A = A->data(pr.first);
-      gp.B = B->data(pr.second);
       gp.k = int(K);
-      gp.lda = (opa & 1) ? int(m) : int(K);
-      gp.ldb = (opb & 1) ? int(K) : int(nn);
-      gp.opa = opa | (conja ? 2 : 0);
-      gp.opb = opb | (conjb ? 2 : 0);
+      make_operand(gp.A, A->data(pr.first), ab, fa2, iaa, conja);
+      make_operand(gp.B, B->data(pr.second), bb, ibb, fb2, conjb);
       pairs.push_back(gp);
     }
     go.pair_end = int(pairs.size());
@@ -562,7 +326,7 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   c->begin();
   bugk::launch_gemm(d_outs, d_pairs, d_tiles, int(tiles.size()), c->stream);
   c->launched(BUG_K_GEMM, flops, gbytes);
-  return out;  // Ap/Bp are released stream-ordered
+  return out;
 }
 
 // ── SVD ──────────────────────────────────────────────────────────────────────────────────────
@@ -946,9 +710,9 @@ std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
   return out;
 }
 
-}  // namespace
+}  // namespace bugi
 
-namespace {
+namespace bugi {
 int guard(const std::function<void()>& f) {
   struct Flush {
     ~Flush() {
@@ -973,7 +737,224 @@ int guard(const std::function<void()>& f) {
     return BUG_EINVAL;
   }
 }
-}  // namespace
+}  // namespace bugi
+
+
+namespace bugi {
+
+TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& tt, int leg, const double* w) {
+  const bug_tensor* t = &tt;
+  TensorPtr result;
+
+    require(c && t && leg >= 0 && leg < t->rank, "bad argument");
+    const Leg& L = t->legs[leg];
+    std::vector<double> wv(w, w + L.total());
+    std::vector<int64_t> woff(L.q.size());
+    int64_t acc = 0;
+    for (size_t s = 0; s < L.q.size(); ++s) {
+      woff[s] = acc;
+      acc += L.d[s];
+    }
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, t->legs, keys, false);
+    double* dw = c->push(wv);
+    std::vector<ScaleDesc> descs;
+    int64_t total = 0;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      const Block& b = t->blocks[bi];
+      auto st = c_strides(b.shape, t->rank);
+      ScaleDesc d{};
+      d.src = t->data(bi);
+      d.dst = o->mdata(bi);
+      d.n = b.size;
+      d.prefix = total;
+      total += b.size;
+      d.leg_stride = st[leg];
+      d.leg_dim = b.shape[leg];
+      d.w = dw + woff[L.index_of(b.key[leg])];
+      descs.push_back(d);
+    }
+    if (!descs.empty()) {
+      ScaleDesc* dd = c->push(descs);
+      c->begin();
+      bugk::launch_scale(dd, int(descs.size()), total, c->stream);
+      c->launched(BUG_K_SCALE, 0.0, 32.0 * double(total));
+    }
+    result = std::move(o);
+    return result;
+}
+
+TensorPtr conj_impl(bug_ctx* c, const bug_tensor& tt) {
+  const bug_tensor* t = &tt;
+  TensorPtr result;
+
+    std::vector<Leg> legs;
+    for (auto& l : t->legs) legs.push_back(flipped(l));
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    if (t->nelem > 0)
+      d.push_back(plain_copy(t->buf->ptr, o->buf->ptr, t->nelem, true, make_double2(1.0, 0.0), false));
+    run_copies(c, d);
+    result = std::move(o);
+    return result;
+}
+
+TensorPtr flip_leg_impl(bug_ctx* c, const bug_tensor& tt, int leg) {
+  const bug_tensor* t = &tt;
+  TensorPtr result;
+
+    require(leg >= 0 && leg < t->rank, "bad leg");
+    std::vector<Leg> legs = t->legs;
+    Leg L;
+    L.dir = -t->legs[leg].dir;
+    for (int s = int(t->legs[leg].q.size()) - 1; s >= 0; --s) {
+      L.q.push_back(-t->legs[leg].q[s]);
+      L.d.push_back(t->legs[leg].d[s]);
+    }
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (auto& b : t->blocks) {
+      Key k = b.key;
+      k[leg] = -k[leg];
+      keys.push_back(k);
+    }
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      Key k = t->blocks[bi].key;
+      k[leg] = -k[leg];
+      int ob = o->find(k);
+      d.push_back(plain_copy(t->data(bi), o->mdata(ob), t->blocks[bi].size, false,
+                             make_double2(1.0, 0.0), false));
+    }
+    run_copies(c, d);
+    result = std::move(o);
+    return result;
+}
+
+TensorPtr oplus_impl(bug_ctx* c, int n, const bug_tensor* const* ts, int leg) {
+  TensorPtr result;
+
+    require(n >= 1, "oplus needs at least one tensor");
+    const int rank = ts[0]->rank;
+    require(leg >= 0 && leg < rank, "bad leg");
+    std::map<int, int> dims;
+    std::vector<Leg> legs = ts[0]->legs;
+    for (int i = 0; i < n; ++i) {
+      require(ts[i]->rank == rank, "oplus: ranks differ");
+      require(ts[i]->legs[leg].dir == ts[0]->legs[leg].dir, "oplus: arrows differ");
+      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) dims[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
+      if (i > 0)
+        for (int l = 0; l < rank; ++l)
+          if (l != leg) legs[l] = merged(legs[l], ts[i]->legs[l]);
+    }
+    Leg L;
+    L.dir = ts[0]->legs[leg].dir;
+    for (auto& kv : dims) {
+      L.q.push_back(kv.first);
+      L.d.push_back(kv.second);
+    }
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (int i = 0; i < n; ++i)
+      for (auto& b : ts[i]->blocks) keys.push_back(b.key);
+    auto o = make_tensor(c, rank, legs, keys, true);
+    std::map<int, int> offs;
+    std::vector<CopyDesc> d;
+    for (int i = 0; i < n; ++i) {
+      for (int bi = 0; bi < int(ts[i]->blocks.size()); ++bi) {
+        const Block& b = ts[i]->blocks[bi];
+        int ob = o->find(b.key);
+        const Block& obb = o->blocks[ob];
+        auto ss = c_strides(b.shape, rank);
+        auto ds = c_strides(obb.shape, rank);
+        CopyDesc cd{};
+        cd.src = ts[i]->data(bi);
+        cd.dst = o->mdata(ob) + int64_t(offs[b.key[leg]]) * ds[leg];
+        cd.n = b.size;
+        cd.ndim = rank;
+        for (int l = 0; l < rank; ++l) {
+          cd.dims[l] = b.shape[l];
+          cd.sstr[l] = ss[l];
+          cd.dstr[l] = ds[l];
+        }
+        cd.alpha = make_double2(1.0, 0.0);
+        d.push_back(cd);
+      }
+      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) offs[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
+    }
+    run_copies(c, d);
+    result = std::move(o);
+    return result;
+}
+
+TensorPtr trim_impl(bug_ctx* c, const bug_tensor& tt, int leg, const int* counts) {
+  const bug_tensor* t = &tt;
+  TensorPtr result;
+
+    require(leg >= 0 && leg < t->rank, "bad leg");
+    const Leg& L0 = t->legs[leg];
+    Leg L;
+    L.dir = L0.dir;
+    std::map<int, int> keep;
+    for (size_t s = 0; s < L0.q.size(); ++s) {
+      int k = std::min(std::max(counts[s], 0), L0.d[s]);
+      if (k > 0) {
+        L.q.push_back(L0.q[s]);
+        L.d.push_back(k);
+        keep[L0.q[s]] = k;
+      }
+    }
+    if (L.q.empty()) return nullptr;
+    std::vector<Leg> legs = t->legs;
+    legs[leg] = L;
+    std::vector<Key> keys;
+    for (auto& b : t->blocks)
+      if (keep.count(b.key[leg])) keys.push_back(b.key);
+    auto o = make_tensor(c, t->rank, legs, keys, false);
+    std::vector<CopyDesc> d;
+    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
+      const Block& b = t->blocks[bi];
+      if (!keep.count(b.key[leg])) continue;
+      int ob = o->find(b.key);
+      const Block& obb = o->blocks[ob];
+      auto ss = c_strides(b.shape, t->rank);
+      auto ds = c_strides(obb.shape, t->rank);
+      CopyDesc cd{};
+      cd.src = t->data(bi);
+      cd.dst = o->mdata(ob);
+      cd.n = obb.size;
+      cd.ndim = t->rank;
+      for (int l = 0; l < t->rank; ++l) {
+        cd.dims[l] = obb.shape[l];
+        cd.sstr[l] = ss[l];
+        cd.dstr[l] = ds[l];
+      }
+      cd.alpha = make_double2(1.0, 0.0);
+      d.push_back(cd);
+    }
+    run_copies(c, d);
+    result = std::move(o);
+    return result;
+}
+
+TensorPtr upload_impl(bug_ctx* c, int rank, const std::vector<Leg>& legs, const std::vector<Key>& keys,
+                      const double* data) {
+  auto t = make_tensor(c, rank, legs, keys, false);
+  require(int(t->blocks.size()) == int(keys.size()), "duplicate block keys");
+  if (t->nelem > 0)
+    BUG_CUDA(cudaMemcpyAsync(t->buf->ptr, data, size_t(t->nelem) * sizeof(double2),
+                             cudaMemcpyHostToDevice, c->stream));
+  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  return t;
+}
+
+}  // namespace bugi
+
+using namespace bugi;
 
 // ── C-ABI ────────────────────────────────────────────────────────────────────────────────────
 
@@ -1011,6 +992,8 @@ int bug_ctx_destroy(bug_ctx* c) {
       cudaEventDestroy(c->stage_ev[i]);
     }
     if (c->pinned_out) cudaFreeHost(c->pinned_out);
+    if (c->arena) cudaFreeAsync(c->arena, c->stream);
+    cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
     delete c;
   });
@@ -1170,46 +1153,6 @@ int bug_svd(bug_ctx* c, const bug_tensor* t, int nleft, const int* left, double 
   });
 }
 
-int bug_scale_leg(bug_ctx* c, const bug_tensor* t, int leg, const double* w, bug_tensor** out) {
-  return guard([&] {
-    require(c && t && out && leg >= 0 && leg < t->rank, "bad argument");
-    const Leg& L = t->legs[leg];
-    std::vector<double> wv(w, w + L.total());
-    std::vector<int64_t> woff(L.q.size());
-    int64_t acc = 0;
-    for (size_t s = 0; s < L.q.size(); ++s) {
-      woff[s] = acc;
-      acc += L.d[s];
-    }
-    std::vector<Key> keys;
-    for (auto& b : t->blocks) keys.push_back(b.key);
-    auto o = make_tensor(c, t->rank, t->legs, keys, false);
-    double* dw = c->push(wv);
-    std::vector<ScaleDesc> descs;
-    int64_t total = 0;
-    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
-      const Block& b = t->blocks[bi];
-      auto st = c_strides(b.shape, t->rank);
-      ScaleDesc d{};
-      d.src = t->data(bi);
-      d.dst = o->mdata(bi);
-      d.n = b.size;
-      d.prefix = total;
-      total += b.size;
-      d.leg_stride = st[leg];
-      d.leg_dim = b.shape[leg];
-      d.w = dw + woff[L.index_of(b.key[leg])];
-      descs.push_back(d);
-    }
-    if (!descs.empty()) {
-      ScaleDesc* dd = c->push(descs);
-      c->begin();
-      bugk::launch_scale(dd, int(descs.size()), total, c->stream);
-      c->launched(BUG_K_SCALE, 0.0, 32.0 * double(total));
-    }
-    *out = o.release();
-  });
-}
 
 int bug_norm2(bug_ctx* c, const bug_tensor* t, double* out) {
   return guard([&] {
@@ -1241,156 +1184,32 @@ int bug_permute(bug_ctx* c, const bug_tensor* t, const int* perm, bug_tensor** o
   return guard([&] { *out = permute_impl(c, *t, perm).release(); });
 }
 
-int bug_conj(bug_ctx* c, const bug_tensor* t, bug_tensor** out) {
+
+
+
+
+
+int bug_scale_leg(bug_ctx* c, const bug_tensor* t, int leg, const double* w, bug_tensor** out) {
   return guard([&] {
-    std::vector<Leg> legs;
-    for (auto& l : t->legs) legs.push_back(flipped(l));
-    std::vector<Key> keys;
-    for (auto& b : t->blocks) keys.push_back(b.key);
-    auto o = make_tensor(c, t->rank, legs, keys, false);
-    std::vector<CopyDesc> d;
-    if (t->nelem > 0)
-      d.push_back(plain_copy(t->buf->ptr, o->buf->ptr, t->nelem, true, make_double2(1.0, 0.0), false));
-    run_copies(c, d);
-    *out = o.release();
+    require(c && t && out, "null argument");
+    *out = scale_leg_impl(c, *t, leg, w).release();
   });
+}
+
+int bug_conj(bug_ctx* c, const bug_tensor* t, bug_tensor** out) {
+  return guard([&] { *out = conj_impl(c, *t).release(); });
 }
 
 int bug_flip_leg(bug_ctx* c, const bug_tensor* t, int leg, bug_tensor** out) {
-  return guard([&] {
-    require(leg >= 0 && leg < t->rank, "bad leg");
-    std::vector<Leg> legs = t->legs;
-    Leg L;
-    L.dir = -t->legs[leg].dir;
-    for (int s = int(t->legs[leg].q.size()) - 1; s >= 0; --s) {
-      L.q.push_back(-t->legs[leg].q[s]);
-      L.d.push_back(t->legs[leg].d[s]);
-    }
-    legs[leg] = L;
-    std::vector<Key> keys;
-    for (auto& b : t->blocks) {
-      Key k = b.key;
-      k[leg] = -k[leg];
-      keys.push_back(k);
-    }
-    auto o = make_tensor(c, t->rank, legs, keys, false);
-    std::vector<CopyDesc> d;
-    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
-      Key k = t->blocks[bi].key;
-      k[leg] = -k[leg];
-      int ob = o->find(k);
-      d.push_back(plain_copy(t->data(bi), o->mdata(ob), t->blocks[bi].size, false,
-                             make_double2(1.0, 0.0), false));
-    }
-    run_copies(c, d);
-    *out = o.release();
-  });
+  return guard([&] { *out = flip_leg_impl(c, *t, leg).release(); });
 }
 
 int bug_oplus(bug_ctx* c, int n, const bug_tensor* const* ts, int leg, bug_tensor** out) {
-  return guard([&] {
-    require(n >= 1, "oplus needs at least one tensor");
-    const int rank = ts[0]->rank;
-    require(leg >= 0 && leg < rank, "bad leg");
-    std::map<int, int> dims;
-    std::vector<Leg> legs = ts[0]->legs;
-    for (int i = 0; i < n; ++i) {
-      require(ts[i]->rank == rank, "oplus: ranks differ");
-      require(ts[i]->legs[leg].dir == ts[0]->legs[leg].dir, "oplus: arrows differ");
-      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) dims[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
-      if (i > 0)
-        for (int l = 0; l < rank; ++l)
-          if (l != leg) legs[l] = merged(legs[l], ts[i]->legs[l]);
-    }
-    Leg L;
-    L.dir = ts[0]->legs[leg].dir;
-    for (auto& kv : dims) {
-      L.q.push_back(kv.first);
-      L.d.push_back(kv.second);
-    }
-    legs[leg] = L;
-    std::vector<Key> keys;
-    for (int i = 0; i < n; ++i)
-      for (auto& b : ts[i]->blocks) keys.push_back(b.key);
-    auto o = make_tensor(c, rank, legs, keys, true);
-    std::map<int, int> offs;
-    std::vector<CopyDesc> d;
-    for (int i = 0; i < n; ++i) {
-      for (int bi = 0; bi < int(ts[i]->blocks.size()); ++bi) {
-        const Block& b = ts[i]->blocks[bi];
-        int ob = o->find(b.key);
-        const Block& obb = o->blocks[ob];
-        auto ss = c_strides(b.shape, rank);
-        auto ds = c_strides(obb.shape, rank);
-        CopyDesc cd{};
-        cd.src = ts[i]->data(bi);
-        cd.dst = o->mdata(ob) + int64_t(offs[b.key[leg]]) * ds[leg];
-        cd.n = b.size;
-        cd.ndim = rank;
-        for (int l = 0; l < rank; ++l) {
-          cd.dims[l] = b.shape[l];
-          cd.sstr[l] = ss[l];
-          cd.dstr[l] = ds[l];
-        }
-        cd.alpha = make_double2(1.0, 0.0);
-        d.push_back(cd);
-      }
-      for (size_t s = 0; s < ts[i]->legs[leg].q.size(); ++s) offs[ts[i]->legs[leg].q[s]] += ts[i]->legs[leg].d[s];
-    }
-    run_copies(c, d);
-    *out = o.release();
-  });
+  return guard([&] { *out = oplus_impl(c, n, ts, leg).release(); });
 }
 
 int bug_trim(bug_ctx* c, const bug_tensor* t, int leg, const int* counts, bug_tensor** out) {
-  return guard([&] {
-    require(leg >= 0 && leg < t->rank, "bad leg");
-    const Leg& L0 = t->legs[leg];
-    Leg L;
-    L.dir = L0.dir;
-    std::map<int, int> keep;
-    for (size_t s = 0; s < L0.q.size(); ++s) {
-      int k = std::min(std::max(counts[s], 0), L0.d[s]);
-      if (k > 0) {
-        L.q.push_back(L0.q[s]);
-        L.d.push_back(k);
-        keep[L0.q[s]] = k;
-      }
-    }
-    if (L.q.empty()) {
-      *out = nullptr;
-      return;
-    }
-    std::vector<Leg> legs = t->legs;
-    legs[leg] = L;
-    std::vector<Key> keys;
-    for (auto& b : t->blocks)
-      if (keep.count(b.key[leg])) keys.push_back(b.key);
-    auto o = make_tensor(c, t->rank, legs, keys, false);
-    std::vector<CopyDesc> d;
-    for (int bi = 0; bi < int(t->blocks.size()); ++bi) {
-      const Block& b = t->blocks[bi];
-      if (!keep.count(b.key[leg])) continue;
-      int ob = o->find(b.key);
-      const Block& obb = o->blocks[ob];
-      auto ss = c_strides(b.shape, t->rank);
-      auto ds = c_strides(obb.shape, t->rank);
-      CopyDesc cd{};
-      cd.src = t->data(bi);
-      cd.dst = o->mdata(ob);
-      cd.n = obb.size;
-      cd.ndim = t->rank;
-      for (int l = 0; l < t->rank; ++l) {
-        cd.dims[l] = obb.shape[l];
-        cd.sstr[l] = ss[l];
-        cd.dstr[l] = ds[l];
-      }
-      cd.alpha = make_double2(1.0, 0.0);
-      d.push_back(cd);
-    }
-    run_copies(c, d);
-    *out = o.release();
-  });
+  return guard([&] { *out = trim_impl(c, *t, leg, counts).release(); });
 }
 
 }  // extern "C"

@@ -79,6 +79,18 @@ __global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restri
 
 constexpr int TM = 32, TN = 32, TK = 16;
 
+__device__ __forceinline__ int64_t group_off(int idx, int n, const int* d, const int64_t* s) {
+  if (n == 0) return 0;
+  if (n == 1) return int64_t(idx) * s[0];
+  int64_t off = 0;
+  for (int j = n - 1; j >= 0; --j) {
+    const int q = idx % d[j];
+    idx /= d[j];
+    off += int64_t(q) * s[j];
+  }
+  return off;
+}
+
 __global__ void __launch_bounds__(kThreads)
 gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs,
             const GemmTile* __restrict__ tiles) {
@@ -95,27 +107,28 @@ gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs
     for (int j = 0; j < 2; ++j) acc[i][j] = make_double2(0.0, 0.0);
 
   for (int p = o.pair_begin; p < o.pair_end; ++p) {
-    const GemmPair g = pairs[p];
-    const bool ta = g.opa & 1, ca = g.opa & 2, tb = g.opb & 1, cb = g.opb & 2;
-    for (int k0 = 0; k0 < g.k; k0 += TK) {
+    const Operand& A = pairs[p].A;
+    const Operand& B = pairs[p].B;
+    const int K = pairs[p].k;
+    for (int k0 = 0; k0 < K; k0 += TK) {
       for (int i = threadIdx.x; i < TM * TK; i += kThreads) {
         int mm, kk;
-        if (ta) { kk = i / TM; mm = i % TM; } else { mm = i / TK; kk = i % TK; }
+        if (A.row_fast) { kk = i / TM; mm = i % TM; } else { mm = i / TK; kk = i % TK; }
         const int gm = row0 + mm, gk = k0 + kk;
         double2 v = make_double2(0.0, 0.0);
-        if (gm < o.m && gk < g.k)
-          v = ta ? g.A[int64_t(gk) * g.lda + gm] : g.A[int64_t(gm) * g.lda + gk];
-        if (ca) v.y = -v.y;
+        if (gm < o.m && gk < K)
+          v = A.p[group_off(gm, A.nr, A.rd, A.rs) + group_off(gk, A.nc, A.cd, A.cs)];
+        if (A.conj) v.y = -v.y;
         As[mm][kk] = v;
       }
       for (int i = threadIdx.x; i < TK * TN; i += kThreads) {
         int kk, nn;
-        if (tb) { nn = i / TK; kk = i % TK; } else { kk = i / TN; nn = i % TN; }
+        if (B.row_fast) { nn = i / TK; kk = i % TK; } else { kk = i / TN; nn = i % TN; }
         const int gk = k0 + kk, gn = col0 + nn;
         double2 v = make_double2(0.0, 0.0);
-        if (gk < g.k && gn < o.n)
-          v = tb ? g.B[int64_t(gn) * g.ldb + gk] : g.B[int64_t(gk) * g.ldb + gn];
-        if (cb) v.y = -v.y;
+        if (gk < K && gn < o.n)
+          v = B.p[group_off(gk, B.nr, B.rd, B.rs) + group_off(gn, B.nc, B.cd, B.cs)];
+        if (B.conj) v.y = -v.y;
         Bs[kk][nn] = v;
       }
       __syncthreads();

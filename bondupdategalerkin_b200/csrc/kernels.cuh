@@ -42,13 +42,23 @@ struct GemmOut {
   int pair_begin, pair_end;
 };
 
-// op bits: 1 = transposed storage (A stored k x m, B stored n x k), 2 = conjugate values
+// A GEMM operand viewed as a matrix over two index groups (A: rows = free legs, cols = contracted
+// legs in contraction order; B: rows = contracted legs, cols = free legs). Each group is up to
+// kGroup dims (C order, last fastest) with element strides, so any leg order of a block is read
+// in place -- no transpose pass.
+constexpr int kGroup = 4;
+struct Operand {
+  const double2* p;
+  int nr, nc;               // dims in the row / column group (0 = that extent is 1)
+  int rd[kGroup], cd[kGroup];
+  int64_t rs[kGroup], cs[kGroup];
+  int conj;
+  int row_fast;             // the row group holds the unit stride: let threads vary along rows
+};
+
 struct GemmPair {
-  const double2* A;
-  const double2* B;
+  Operand A, B;
   int k;
-  int lda, ldb;
-  int opa, opb;
   int pad_;
 };
 

@@ -1,0 +1,269 @@
+// Small dense FP64 linear algebra for the Krylov logic of the step (k x k, k <= 65).
+//
+// The reference calls LAPACK (syevr/syev for the Lanczos tridiagonal, geev for Hessenberg
+// eigenvalues; src/BUG/Core/LocalSolvers/krylov.jl:77-98, root_methods.jl:136-141) and Julia's
+// matrix `exp` for these. This file holds the engine's own implementations:
+//   * eigh_jacobi   -- cyclic Jacobi eigen-decomposition of a real symmetric matrix;
+//   * expm          -- scaling and squaring with the degree-13 Pade approximant (Higham, "The
+//                      scaling and squaring method for the matrix exponential revisited", SIAM J.
+//                      Matrix Anal. Appl. 26 (2005)); the Pade coefficients are computed from
+//                      their closed form (2m-j)! m! / ((2m)! j! (m-j)!);
+//   * eigvals_hess  -- eigenvalues of a complex upper-Hessenberg matrix by the single-shift QR
+//                      algorithm with Wilkinson shifts and deflation.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <stdexcept>
+#include <vector>
+
+namespace smallla {
+
+using cd = std::complex<double>;
+
+// Row-major dense matrix.
+template <class V>
+struct Mat {
+  int n = 0, m = 0;
+  std::vector<V> a;
+  Mat() = default;
+  Mat(int rows, int cols) : n(rows), m(cols), a(size_t(rows) * cols, V(0)) {}
+  V& operator()(int i, int j) { return a[size_t(i) * m + j]; }
+  const V& operator()(int i, int j) const { return a[size_t(i) * m + j]; }
+};
+
+using CMat = Mat<cd>;
+using RMat = Mat<double>;
+
+inline CMat matmul(const CMat& x, const CMat& y) {
+  CMat z(x.n, y.m);
+  for (int i = 0; i < x.n; ++i)
+    for (int k = 0; k < x.m; ++k) {
+      const cd v = x(i, k);
+      if (v == cd(0)) continue;
+      for (int j = 0; j < y.m; ++j) z(i, j) += v * y(k, j);
+    }
+  return z;
+}
+
+inline double norm1(const CMat& x) {
+  double best = 0.0;
+  for (int j = 0; j < x.m; ++j) {
+    double s = 0.0;
+    for (int i = 0; i < x.n; ++i) s += std::abs(x(i, j));
+    best = std::max(best, s);
+  }
+  return best;
+}
+
+inline double frob(const CMat& x) {
+  double s = 0.0;
+  for (auto& v : x.a) s += std::norm(v);
+  return std::sqrt(s);
+}
+
+// Symmetric eigen-decomposition: returns eigenvalues (ascending) and eigenvectors as columns of V.
+inline void eigh_jacobi(const RMat& A0, std::vector<double>& vals, RMat& V) {
+  const int n = A0.n;
+  RMat A = A0;
+  V = RMat(n, n);
+  for (int i = 0; i < n; ++i) V(i, i) = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        tot += A(i, j) * A(i, j);
+        if (i != j) off += A(i, j) * A(i, j);
+      }
+    if (off <= 1e-32 * tot || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A(p, q);
+        if (apq == 0.0) continue;
+        const double theta = (A(q, q) - A(p, p)) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = A(k, p), akq = A(k, q);
+          A(k, p) = c * akp - s * akq;
+          A(k, q) = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = A(p, k), aqk = A(q, k);
+          A(p, k) = c * apk - s * aqk;
+          A(q, k) = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V(k, p), vkq = V(k, q);
+          V(k, p) = c * vkp - s * vkq;
+          V(k, q) = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return A(x, x) < A(y, y); });
+  vals.resize(n);
+  RMat W(n, n);
+  for (int j = 0; j < n; ++j) {
+    vals[j] = A(order[j], order[j]);
+    for (int i = 0; i < n; ++i) W(i, j) = V(i, order[j]);
+  }
+  V = W;
+}
+
+// Solve X from P X = Q (complex, partial pivoting); P is overwritten.
+inline CMat solve(CMat P, CMat Q) {
+  const int n = P.n;
+  for (int k = 0; k < n; ++k) {
+    int piv = k;
+    double best = std::abs(P(k, k));
+    for (int i = k + 1; i < n; ++i)
+      if (std::abs(P(i, k)) > best) {
+        best = std::abs(P(i, k));
+        piv = i;
+      }
+    if (best == 0.0) throw std::runtime_error("expm: singular Pade denominator");
+    if (piv != k) {
+      for (int j = 0; j < n; ++j) std::swap(P(k, j), P(piv, j));
+      for (int j = 0; j < Q.m; ++j) std::swap(Q(k, j), Q(piv, j));
+    }
+    for (int i = k + 1; i < n; ++i) {
+      const cd f = P(i, k) / P(k, k);
+      if (f == cd(0)) continue;
+      for (int j = k; j < n; ++j) P(i, j) -= f * P(k, j);
+      for (int j = 0; j < Q.m; ++j) Q(i, j) -= f * Q(k, j);
+    }
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    for (int j = 0; j < Q.m; ++j) {
+      cd s = Q(k, j);
+      for (int i = k + 1; i < n; ++i) s -= P(k, i) * Q(i, j);
+      Q(k, j) = s / P(k, k);
+    }
+  }
+  return Q;
+}
+
+// exp(A) by scaling and squaring with the [13/13] Pade approximant.
+inline CMat expm(const CMat& A0) {
+  const int n = A0.n;
+  CMat I(n, n);
+  for (int i = 0; i < n; ++i) I(i, i) = 1.0;
+  if (n == 0) return I;
+  // Pade coefficients b_j = (2m-j)! m! / ((2m)! j! (m-j)!), m = 13
+  const int m = 13;
+  double b[m + 1];
+  for (int j = 0; j <= m; ++j) {
+    long double v = 1.0L;
+    for (int k = 1; k <= m; ++k) v *= (long double)k;          // m!
+    for (int k = 1; k <= 2 * m - j; ++k) v *= (long double)k;  // (2m-j)!
+    for (int k = 1; k <= 2 * m; ++k) v /= (long double)k;      // (2m)!
+    for (int k = 1; k <= j; ++k) v /= (long double)k;          // j!
+    for (int k = 1; k <= m - j; ++k) v /= (long double)k;      // (m-j)!
+    b[j] = double(v);
+  }
+  const double theta13 = 5.371920351148152;  // Higham (2005), Table 2.3
+  const double nrm = norm1(A0);
+  int s = 0;
+  if (nrm > theta13) s = std::max(0, int(std::ceil(std::log2(nrm / theta13))));
+  CMat A = A0;
+  const double scale = std::ldexp(1.0, -s);
+  for (auto& v : A.a) v *= scale;
+  CMat A2 = matmul(A, A), A4 = matmul(A2, A2), A6 = matmul(A4, A2);
+  CMat Ut(n, n), V(n, n), W1(n, n), Z1(n, n);
+  for (size_t i = 0; i < A.a.size(); ++i) {
+    W1.a[i] = b[13] * A6.a[i] + b[11] * A4.a[i] + b[9] * A2.a[i];
+    Z1.a[i] = b[12] * A6.a[i] + b[10] * A4.a[i] + b[8] * A2.a[i];
+  }
+  CMat W = matmul(A6, W1);
+  for (size_t i = 0; i < A.a.size(); ++i)
+    W.a[i] += b[7] * A6.a[i] + b[5] * A4.a[i] + b[3] * A2.a[i] + b[1] * I.a[i];
+  CMat U = matmul(A, W);
+  V = matmul(A6, Z1);
+  for (size_t i = 0; i < A.a.size(); ++i)
+    V.a[i] += b[6] * A6.a[i] + b[4] * A4.a[i] + b[2] * A2.a[i] + b[0] * I.a[i];
+  CMat P(n, n), Q(n, n);
+  for (size_t i = 0; i < A.a.size(); ++i) {
+    P.a[i] = V.a[i] - U.a[i];
+    Q.a[i] = V.a[i] + U.a[i];
+  }
+  CMat R = solve(P, Q);
+  for (int k = 0; k < s; ++k) R = matmul(R, R);
+  return R;
+}
+
+// Eigenvalues of a complex upper-Hessenberg matrix (entries below the subdiagonal are ignored).
+inline std::vector<cd> eigvals_hess(const CMat& H0) {
+  const int n = H0.n;
+  CMat H = H0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j + 1 < i; ++j) H(i, j) = 0.0;
+  std::vector<cd> ev(n);
+  int hi = n - 1;
+  int iter = 0;
+  const double eps = 2.220446049250313e-16;
+  while (hi >= 0) {
+    if (hi == 0) {
+      ev[0] = H(0, 0);
+      break;
+    }
+    // deflation search
+    int lo = hi;
+    while (lo > 0) {
+      const double sub = std::abs(H(lo, lo - 1));
+      const double diag = std::abs(H(lo, lo)) + std::abs(H(lo - 1, lo - 1));
+      if (sub <= eps * (diag > 0 ? diag : 1.0)) {
+        H(lo, lo - 1) = 0.0;
+        break;
+      }
+      --lo;
+    }
+    if (lo == hi) {
+      ev[hi] = H(hi, hi);
+      --hi;
+      iter = 0;
+      continue;
+    }
+    if (++iter > 60 * n) throw std::runtime_error("Hessenberg QR did not converge");
+    // Wilkinson shift from the trailing 2x2 block
+    const cd a = H(hi - 1, hi - 1), bb = H(hi - 1, hi), c = H(hi, hi - 1), d = H(hi, hi);
+    const cd tr = a + d, det = a * d - bb * c;
+    const cd disc = std::sqrt(tr * tr / 4.0 - det);
+    cd mu1 = tr / 2.0 + disc, mu2 = tr / 2.0 - disc;
+    cd mu = (std::abs(mu1 - d) < std::abs(mu2 - d)) ? mu1 : mu2;
+    if (iter % 11 == 0) mu += cd(std::abs(H(hi, hi - 1)), 0.0);  // exceptional shift
+    // QR step on the active block lo..hi with Givens rotations
+    std::vector<cd> cs(hi - lo), sn(hi - lo);
+    for (int k = lo; k <= hi; ++k) H(k, k) -= mu;
+    for (int k = lo; k < hi; ++k) {
+      const cd x = H(k, k), y = H(k + 1, k);
+      const double r = std::sqrt(std::norm(x) + std::norm(y));
+      cd cc = 1.0, ss = 0.0;
+      if (r > 0) {
+        cc = x / r;
+        ss = y / r;
+      }
+      cs[k - lo] = cc;
+      sn[k - lo] = ss;
+      for (int j = k; j < n; ++j) {  // rows k, k+1: G^H
+        const cd u = H(k, j), v = H(k + 1, j);
+        H(k, j) = std::conj(cc) * u + std::conj(ss) * v;
+        H(k + 1, j) = -ss * u + cc * v;
+      }
+    }
+    for (int k = lo; k < hi; ++k) {  // columns k, k+1: G
+      const cd cc = cs[k - lo], ss = sn[k - lo];
+      for (int i = 0; i <= std::min(k + 2, hi); ++i) {
+        const cd u = H(i, k), v = H(i, k + 1);
+        H(i, k) = u * cc + v * ss;
+        H(i, k + 1) = -u * std::conj(ss) + v * std::conj(cc);
+      }
+    }
+    for (int k = lo; k <= hi; ++k) H(k, k) += mu;
+  }
+  return ev;
+}
+
+}  // namespace smallla

@@ -1,0 +1,164 @@
+"""The native step: ``cbe_bug_step`` as ONE call into ``libbug_b200.so`` (``bug_mps_step``).
+
+The sweep logic, ledger and every tensor operation run inside the library; Python only passes
+handles, the keyword arguments and a callback through which the library draws the Gaussian probes
+from the caller's seeded ``numpy.random.Generator`` (the same draw stream, in the same order, as
+the Python host in ``step.py`` and the CPU oracle).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from types import SimpleNamespace
+
+import numpy as np
+
+from . import _engine as E
+from .tensor import DT
+
+MAX_SITES = 1024
+UNMET_NAMES = {1: "sample", 2: "tail", 3: "krylov", 4: "trunc", 5: "projection", 6: "expv", 7: "closure"}
+
+
+class StepParams(ctypes.Structure):
+    _fields_ = [("tol_basis", ctypes.c_double), ("tol_trunc", ctypes.c_double),
+                ("tol_expv", ctypes.c_double), ("tol_krylov", ctypes.c_double),
+                ("order", ctypes.c_int), ("maxdim", ctypes.c_int), ("hermitian", ctypes.c_int),
+                ("work_ceiling_rule", ctypes.c_int), ("bond_ceiling_factor", ctypes.c_double),
+                ("root", ctypes.c_int), ("reorth", ctypes.c_int), ("truncate", ctypes.c_int),
+                ("root_maxiter", ctypes.c_int), ("fixed_width", ctypes.c_int),
+                ("tail_factor", ctypes.c_double), ("krylov_mode", ctypes.c_int),
+                ("krylov_fixed_depth", ctypes.c_int)]
+
+
+class BondLog(ctypes.Structure):
+    _fields_ = [("bond", ctypes.c_int), ("side", ctypes.c_int), ("sample", ctypes.c_double),
+                ("tail", ctypes.c_double), ("krylov_c", ctypes.c_double), ("krylov_d", ctypes.c_double),
+                ("n_probes", ctypes.c_int64), ("n_selected", ctypes.c_int64),
+                ("n_krylov", ctypes.c_int64), ("n_h1", ctypes.c_int64), ("c_pass", ctypes.c_int),
+                ("d_after_c", ctypes.c_int), ("workcap", ctypes.c_int), ("met", ctypes.c_int),
+                ("unmet_mask", ctypes.c_int), ("width", ctypes.c_int), ("r_old", ctypes.c_int),
+                ("r_final", ctypes.c_int), ("discarded", ctypes.c_double)]
+
+
+class StepInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("unmet_mask", ctypes.c_int),
+                ("unmet_order", ctypes.c_int * 8), ("root_link", ctypes.c_int),
+                ("root_rank", ctypes.c_int), ("root_frame_width", ctypes.c_int),
+                ("discarded", ctypes.c_double), ("n_matvec", ctypes.c_int64),
+                ("max_sample", ctypes.c_double), ("max_tail", ctypes.c_double),
+                ("max_krylov", ctypes.c_double), ("max_krylov_c", ctypes.c_double),
+                ("max_krylov_d", ctypes.c_double), ("ledger_discarded", ctypes.c_double),
+                ("expv_err", ctypes.c_double), ("expv_iters", ctypes.c_int64),
+                ("n_probes", ctypes.c_int64), ("n_selected", ctypes.c_int64),
+                ("n_krylov", ctypes.c_int64), ("n_h1", ctypes.c_int64), ("n_c_pass", ctypes.c_int64),
+                ("n_d_after_c", ctypes.c_int64), ("workcap_reached", ctypes.c_int),
+                ("maxdim_reached", ctypes.c_int), ("proj_err", ctypes.c_double),
+                ("r_old", ctypes.c_int64), ("r_aug", ctypes.c_int64), ("r_final", ctypes.c_int64),
+                ("n_passes", ctypes.c_int64), ("n_closure_sweeps", ctypes.c_int64),
+                ("defect", ctypes.c_double), ("n_root_frontier", ctypes.c_int64),
+                ("n_h1_closure", ctypes.c_int64), ("n_compress", ctypes.c_int64),
+                ("leak1", ctypes.c_double), ("expanded", ctypes.c_int * MAX_SITES),
+                ("n_new", ctypes.c_int * MAX_SITES), ("workcap", ctypes.c_int * MAX_SITES)]
+
+
+DRAW_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double))
+
+_declared = [False]
+
+
+def _lib():
+    lib = E.load()
+    if not _declared[0]:
+        lib.bug_mps_step.restype = ctypes.c_int
+        lib.bug_mps_step.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_void_p), ctypes.c_double, ctypes.c_double,
+            ctypes.POINTER(StepParams), DRAW_FN, ctypes.c_void_p, ctypes.POINTER(StepInfo),
+            ctypes.POINTER(BondLog), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        _declared[0] = True
+    return lib
+
+
+def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
+                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
+                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
+                 root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
+                 closure_checks=False):
+    """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
+    HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields)."""
+    L = len(psi)
+    if len(mpo) != L:
+        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
+    if L < 2:
+        raise ValueError("cbe_bug_step needs at least two sites")
+    if L - 1 > MAX_SITES:
+        raise ValueError(f"at most {MAX_SITES + 1} sites")
+    if work_ceiling_rule not in ("bond", "maxdim"):
+        raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r}")
+    if closure_checks or frontier_tol or krylov_rank_tol:
+        raise NotImplementedError("closure_checks / frontier_tol / krylov_rank_tol > 0")
+    if fold_omega is False and order > 1:
+        raise NotImplementedError("the exact (unfolded) closure leak")
+    mode, width, tail_factor, kmode, fixed_depth = "rank_tail", 8, 0.10, "auto", 0
+    if expansion is not None:
+        mode, width = expansion.mode, expansion.fixed_width
+        tail_factor, kmode = expansion.tail_factor, expansion.krylov_mode
+        fixed_depth = expansion.krylov_fixed_depth
+    if mode != "rank_tail":
+        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail")
+    p = StepParams(
+        tol_basis=tol_basis or 0.0, tol_trunc=-1.0 if tol_trunc is None else tol_trunc,
+        tol_expv=tol_expv or 0.0, tol_krylov=tol_krylov or 0.0, order=order,
+        maxdim=maxdim or 0, hermitian=int(hermitian),
+        work_ceiling_rule=1 if work_ceiling_rule == "maxdim" else 0,
+        bond_ceiling_factor=-1.0 if bond_ceiling_factor is None else float(bond_ceiling_factor),
+        root=root or 0, reorth=int(reorth), truncate=int(truncate), root_maxiter=root_maxiter,
+        fixed_width=width, tail_factor=tail_factor,
+        krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth)
+    if rng is None:
+        rng = np.random.default_rng(0x5EED)
+
+    @DRAW_FN
+    def draw(user, n, out):
+        x = rng.standard_normal(int(n))
+        ctypes.memmove(out, x.ctypes.data, 8 * int(n))
+
+    ctx = psi.tensors[0].ctx
+    tau = complex(tau)
+    arr = (ctypes.c_void_p * L)(*[t.h.value for t in psi.tensors])
+    warr = (ctypes.c_void_p * L)(*[w.h.value for w in mpo.tensors])
+    center = ctypes.c_int(psi.center)
+    info = StepInfo()
+    cap = 8 * L
+    logs = (BondLog * cap)()
+    nlog = ctypes.c_int()
+    E.check(_lib().bug_mps_step(ctx.h, L, arr, ctypes.byref(center), warr, tau.real, tau.imag,
+                                ctypes.byref(p), draw, None, ctypes.byref(info), logs, cap,
+                                ctypes.byref(nlog)))
+    for i in range(L):
+        if arr[i]:
+            psi.tensors[i] = DT(ctx, ctypes.c_void_p(arr[i]))
+    psi.center = center.value
+    unmet = [UNMET_NAMES[c] for c in info.unmet_order if c]
+    ledger = SimpleNamespace(
+        unmet=unmet, tolerance_met=info.status == 0, expv_err=info.expv_err,
+        expv_iters=info.expv_iters, discarded=info.ledger_discarded, max_sample=info.max_sample,
+        max_tail=info.max_tail, max_krylov=info.max_krylov, max_krylov_c=info.max_krylov_c,
+        max_krylov_d=info.max_krylov_d, n_probes=info.n_probes, n_selected=info.n_selected,
+        n_krylov=info.n_krylov, n_h1=info.n_h1, n_c_pass=info.n_c_pass, n_d_after_c=info.n_d_after_c,
+        workcap_reached=bool(info.workcap_reached), maxdim_reached=bool(info.maxdim_reached),
+        proj_err=info.proj_err, r_old=info.r_old, r_aug=info.r_aug, r_final=info.r_final,
+        order=order, n_passes=info.n_passes, n_closure_sweeps=info.n_closure_sweeps,
+        defect=info.defect, n_root_frontier=info.n_root_frontier, n_h1_closure=info.n_h1_closure,
+        n_compress=info.n_compress,
+        bond_log=[{f: getattr(logs[i], f) for f, _ in BondLog._fields_} for i in range(min(nlog.value, cap))],
+    )
+    ledger.status = lambda: "met" if ledger.tolerance_met else "budget_unmet"
+    return dict(
+        expanded=list(info.expanded[:L - 1]), n_new=list(info.n_new[:L - 1]),
+        root_link=info.root_link, root_rank=info.root_rank, err_pre=0.0, err_fnl=0.0,
+        discarded=info.discarded, n_matvec=info.n_matvec, root_frame_width=info.root_frame_width,
+        ledger=ledger, status="met" if info.status == 0 else "budget_unmet",
+        bond_dims=psi.bond_dims(), workcap=list(info.workcap[:L - 1]),
+    )

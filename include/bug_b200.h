@@ -139,6 +139,89 @@ int bug_oplus(bug_ctx* ctx, int n, const bug_tensor* const* t, int leg, bug_tens
  * (_trim_per_sector, truncation.jl:283-288). *out is NULL when nothing is kept. */
 int bug_trim(bug_ctx* ctx, const bug_tensor* t, int leg, const int* counts, bug_tensor** out);
 
+/* ── the whole step ───────────────────────────────────────────────────────────────────────── */
+/* Keyword arguments of `cbe_bug_step!` (bug_step.jl:17-148); a non-positive value selects the
+ * reference default noted beside it (TOL_DEFAULTS, basis_budget.jl:568; DDQRExpansion,
+ * src/BUG/Randomised/cbe.jl:254-290). */
+typedef struct {
+  double tol_basis;           /* <= 0: 1e-5 */
+  double tol_trunc;           /* < 0: 1e-7 */
+  double tol_expv;            /* <= 0: 1e-10 */
+  double tol_krylov;          /* <= 0: tol_basis */
+  int order;                  /* temporal order p >= 1 */
+  int maxdim;                 /* <= 0: 128 */
+  int hermitian;              /* 1: Lanczos root solve, 0: Arnoldi */
+  int work_ceiling_rule;      /* 0: :bond, 1: :maxdim */
+  double bond_ceiling_factor; /* < 0: 1.2 under :bond, 0 under :maxdim */
+  int root;                   /* root link; <= 0: L/2 */
+  int reorth;                 /* re-orthogonalise the root Lanczos basis */
+  int truncate;               /* run the final compression */
+  int root_maxiter;           /* <= 0: 30 */
+  int fixed_width;            /* DD sketch width (:rank_tail); <= 0: 8 */
+  double tail_factor;         /* :rank_tail acceptance share; <= 0: 0.10 */
+  int krylov_mode;            /* 0 :auto, 1 :lanczos, 2 :arnoldi */
+  int krylov_fixed_depth;     /* 0: residual-controlled stop */
+} bug_step_params;
+
+/* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
+ * sqrt(1/2), in the probe order documented in DESIGN.md (the caller's seeded generator stands in
+ * for the reference's `rng`, bug_step.jl:147). */
+typedef void (*bug_normal_fn)(void* user, int64_t n, double* out);
+
+#define BUG_MAX_SITES 1024
+
+/* One bond visit of a sweep (the ledger's bond_log, basis_budget.jl:399-436). side 0 left, 1 right. */
+typedef struct {
+  int bond, side;
+  double sample, tail, krylov_c, krylov_d;
+  int64_t n_probes, n_selected, n_krylov, n_h1;
+  int c_pass, d_after_c, workcap, met, unmet_mask, width, r_old, r_final;
+  double discarded;
+} bug_bond_log;
+
+/* CBEBugSweepInfo + AdaptiveLedger fields (diagnostics.jl:209-255, basis_budget.jl:144-228).
+ * status 0 = :met, 1 = :budget_unmet; unmet bits / unmet_order codes (1-based): 1 sample, 2 tail,
+ * 3 krylov, 4 trunc, 5 projection, 6 expv, 7 closure. */
+typedef struct {
+  int status;
+  int unmet_mask;
+  int unmet_order[8];
+  int root_link, root_rank, root_frame_width;
+  double discarded;
+  int64_t n_matvec;
+  double max_sample, max_tail, max_krylov, max_krylov_c, max_krylov_d, ledger_discarded, expv_err;
+  int64_t expv_iters, n_probes, n_selected, n_krylov, n_h1, n_c_pass, n_d_after_c;
+  int workcap_reached, maxdim_reached;
+  double proj_err;
+  int64_t r_old, r_aug, r_final, n_passes, n_closure_sweeps;
+  double defect;
+  int64_t n_root_frontier, n_h1_closure, n_compress;
+  double leak1;
+  int expanded[BUG_MAX_SITES];
+  int n_new[BUG_MAX_SITES];
+  int workcap[BUG_MAX_SITES];
+} bug_step_info;
+
+/* One rank-adaptive BUG step in place: `cbe_bug_step!(psi, mpo, tau; ...)`
+ * (src/BUG/TimeEvolution/bug_step.jl:17-513), DD-QR :rank_tail expansion, Lanczos/Arnoldi local
+ * Krylov, order-p single-pass closure with folded leak estimates, :exp root. `psi_io[L]` holds the
+ * state's site handles on entry; on return each slot holds a new handle owned by the caller, or
+ * NULL where the caller's handle is unchanged. The MPO handles are only read. */
+int bug_mps_step(bug_ctx* ctx, int L, bug_tensor** psi_io, int* center_io,
+                 const bug_tensor* const* mpo, double tau_re, double tau_im,
+                 const bug_step_params* params, bug_normal_fn draw, void* user,
+                 bug_step_info* info, bug_bond_log* bond_log, int bond_log_cap, int* n_bond_log);
+
+/* ── host small-matrix routines of the step (no device work; usable without a GPU) ────────── */
+/* exp(A) for a complex n x n row-major matrix (Pade-13 scaling and squaring); replaces Julia's
+ * matrix `exp` in _kry_weight/_hess_coeffs (krylov_enrichment.jl:89-120, root_methods.jl:136-141). */
+int bug_la_expm(int n, const double* a, double* out);
+/* Eigen-decomposition of a real symmetric n x n matrix (cyclic Jacobi): ascending eigenvalues and
+ * eigenvectors as columns; replaces syevr in _tridiag_eigen (krylov.jl:77-98). */
+int bug_la_eigh(int n, const double* a, double* vals, double* vecs);
+/* Eigenvalues of a complex upper-Hessenberg n x n matrix; replaces geev in _hess_coeffs. */
+int bug_la_eigvals_hess(int n, const double* a, double* vals_re_im);
+
 #ifdef __cplusplus
 }
 #endif

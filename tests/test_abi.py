@@ -28,7 +28,7 @@ def test_library_exports_every_declared_symbol():
 def test_python_binding_covers_the_header():
     from bondupdategalerkin_b200 import _engine
 
-    assert set(declared()) == set(_engine.SIGNATURES)
+    assert set(declared()) == set(_engine.SIGNATURES) | set(_engine.NATIVE_ONLY)
     lib = _engine.load()
     assert lib.bug_version().decode().startswith("bug_b200")
 
@@ -43,3 +43,41 @@ def test_context_creation_fails_loudly_without_a_device():
 
     with pytest.raises(_engine.EngineError):
         _engine.Context(0)
+
+
+def test_small_matrix_routines_match_scipy():
+    """The host-side k x k routines the native step uses, against scipy (CPU only)."""
+    import numpy as np
+    import scipy.linalg
+
+    from bondupdategalerkin_b200 import _engine
+
+    lib = _engine.load()
+    rng = np.random.default_rng(0)
+    for n, scale in ((1, 1.0), (5, 0.3), (12, 3.0), (30, 20.0)):
+        A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) * scale / np.sqrt(n)
+        a = np.ascontiguousarray(A).view(np.float64)
+        out = np.zeros(2 * n * n)
+        _engine.check(lib.bug_la_expm(n, a.ctypes.data_as(_engine._c_double_p),
+                                      out.ctypes.data_as(_engine._c_double_p)))
+        want = scipy.linalg.expm(A)
+        got = out.view(np.complex128).reshape(n, n)
+        assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+        S = rng.standard_normal((n, n))
+        S = S + S.T
+        vals = np.zeros(n)
+        vecs = np.zeros(n * n)
+        _engine.check(lib.bug_la_eigh(n, np.ascontiguousarray(S).ctypes.data_as(_engine._c_double_p),
+                                      vals.ctypes.data_as(_engine._c_double_p),
+                                      vecs.ctypes.data_as(_engine._c_double_p)))
+        assert np.allclose(vals, np.linalg.eigvalsh(S), atol=1e-12 * max(1, np.max(np.abs(S))))
+        V = vecs.reshape(n, n)
+        assert np.allclose(V @ np.diag(vals) @ V.T, S, atol=1e-11 * max(1, np.max(np.abs(S))))
+        Hs = np.triu(A, -1)
+        h = np.ascontiguousarray(Hs).view(np.float64)
+        ev = np.zeros(2 * n)
+        _engine.check(lib.bug_la_eigvals_hess(n, h.ctypes.data_as(_engine._c_double_p),
+                                              ev.ctypes.data_as(_engine._c_double_p)))
+        got = np.sort_complex(ev.view(np.complex128))
+        want = np.sort_complex(np.linalg.eigvals(Hs))
+        assert np.max(np.abs(got - want)) <= 1e-9 * max(1.0, np.max(np.abs(want)))

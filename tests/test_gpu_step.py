@@ -29,8 +29,12 @@ def dev():
     return DM, DS
 
 
-def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_every=1, **kw):
+def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_every=1,
+             native=False, **kw):
     DM, DS = dev
+    from bondupdategalerkin_b200 import native as DN
+
+    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
     ostate = getattr(OM, start)(L, symmetry=sym)
     dstate = getattr(DM, start)(L, symmetry=sym)
     ompo = OM.xxz_mpo(L, J=1.0, delta=delta, symmetry=sym)
@@ -45,7 +49,7 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
     worst = (0.0, 0.0)
     for n in range(1, steps + 1):
         oi = OS.cbe_bug_step(ostate, ompo, tau, order=order, rng=orng, **okw)
-        di = DS.cbe_bug_step(dstate, dmpo, tau, order=order, rng=drng, **dkw)
+        di = dstep(dstate, dmpo, tau, order=order, rng=drng, **dkw)
         assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
         assert di["status"] == oi["status"], n
         assert di["ledger"].unmet == oi["ledger"].unmet, n
@@ -66,34 +70,53 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
 FROZEN = dict(work_ceiling_rule="maxdim", expansion=dict(krylov_mode="arnoldi"))
 
 
+HOSTS = [pytest.param(False, id="python-host"), pytest.param(True, id="native-step")]
+
+
+@pytest.mark.parametrize("native", HOSTS)
 @pytest.mark.parametrize("order", [1, 2])
-def test_fixture_setting_u1(dev, order):
-    run_pair(dev, 10, 5, "neel_state", 0.0, order, **FROZEN)
+def test_fixture_setting_u1(dev, order, native):
+    run_pair(dev, 10, 5, "neel_state", 0.0, order, native=native, **FROZEN)
 
 
-def test_fixture_setting_none(dev):
-    run_pair(dev, 8, 3, "neel_state", 0.0, 2, sym="none", **FROZEN)
+@pytest.mark.parametrize("native", HOSTS)
+def test_fixture_setting_none(dev, native):
+    run_pair(dev, 8, 3, "neel_state", 0.0, 2, sym="none", native=native, **FROZEN)
 
 
-def test_xx_domain_wall_l20(dev):
+@pytest.mark.parametrize("native", HOSTS)
+def test_xx_domain_wall_l20(dev, native):
     ostate, dstate, worst = run_pair(dev, 20, 20, "domain_wall_state", 0.0, 2, tol_basis=1e-3,
-                                     maxdim=64, check_every=5,
+                                     maxdim=64, check_every=5, native=native,
                                      expansion=dict(mode="rank_tail", fixed_width=8))
     h = mps_to_host(dstate)
     exact = OM.free_fermion_sz(20, 20 * 0.05)
     assert np.max(np.abs(OM.sz_profile(h) - exact)) < 1e-3
 
 
-def test_xxz_quench(dev):
-    run_pair(dev, 12, 6, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=32, check_every=3)
+@pytest.mark.parametrize("native", HOSTS)
+def test_xxz_quench(dev, native):
+    run_pair(dev, 12, 6, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=32, check_every=3,
+             native=native)
 
 
-def test_two_spin(dev):
+@pytest.mark.parametrize("native", HOSTS)
+def test_xxz_quench_l64_native_vs_oracle(dev, native):
+    """The benchmark workload's first steps (L = 64, delta = 0.5, maxdim 256, tol 1e-4)."""
+    run_pair(dev, 64, 6, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=256, check_every=3,
+             native=native)
+
+
+@pytest.mark.parametrize("native", HOSTS)
+def test_two_spin(dev, native):
     DM, DS = dev
+    from bondupdategalerkin_b200 import native as DN
+
+    step = DN.cbe_bug_step if native else DS.cbe_bug_step
     mpo = DM.xxz_mpo(2, J=1.0, delta=0.0)
     psi = DM.product_state(["up", "down"])
     t = 0.3
-    DS.cbe_bug_step(psi, mpo, -1j * t, tol_basis=1e-10, tol_trunc=1e-14, tol_expv=1e-13, maxdim=4)
+    step(psi, mpo, -1j * t, tol_basis=1e-10, tol_trunc=1e-14, tol_expv=1e-13, maxdim=4)
     v = OM.mps_to_dense(mps_to_host(psi))
     v /= np.linalg.norm(v)
     assert abs(abs(v[1]) - np.cos(t / 2)) < 1e-10
