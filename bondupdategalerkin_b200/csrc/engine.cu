@@ -340,7 +340,8 @@ struct SectorPlan {
 
 int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
              std::unique_ptr<bug_tensor>& U, std::unique_ptr<bug_tensor>& Vd,
-             std::vector<double>& sv_sorted, std::vector<int>& sv_q, int& nkept) {
+             std::vector<double>& sv_sorted, std::vector<int>& sv_q, int& nkept, int want,
+             std::unique_ptr<bug_tensor>* USo, std::unique_ptr<bug_tensor>* SVdo) {
   require(nleft >= 0 && nleft <= t.rank, "bad split");
   std::vector<bool> isl(t.rank, false);
   std::vector<int> L(left, left + nleft), R;
@@ -407,8 +408,9 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
   double2* W = static_cast<double2*>(c->scratch(size_t(wtot) * sizeof(double2)));
   double* S = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
   int* sweeps = static_cast<int*>(c->scratch(size_t(std::max(np, 1)) * sizeof(int)));
-  // pack sector matrices (column-major M, or M^H when m < n)
-  std::vector<CopyDesc> descs;
+  // gather descriptors of the sector matrices (column-major M, or M^H when m < n), run inside the
+  // Jacobi kernel itself
+  std::vector<std::vector<CopyDesc>> packs_of(order.size());
   for (int bi = 0; bi < int(t.blocks.size()); ++bi) {
     const Block& b = t.blocks[bi];
     int cq = 0;
@@ -454,9 +456,9 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
     }
     const int64_t base = trans ? (p.coff[ci] + p.roff[ri] * ldw) : (p.roff[ri] + p.coff[ci] * ldw);
     d.dst = W + woff[s] + base;
-    descs.push_back(d);
+    packs_of[s].push_back(d);
   }
-  run_copies(c, descs);
+  std::vector<CopyDesc> packs;
   // launch Jacobi
   std::vector<SvdDesc> sd(np);
   int max_smem = 0;
@@ -476,9 +478,13 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
     int64_t bytes = (mm * r + r * r) * int64_t(sizeof(double2));
     d.use_smem = bytes <= 200 * 1024 ? 1 : 0;
     if (d.use_smem) max_smem = std::max<int>(max_smem, int(bytes));
+    d.pack_begin = int(packs.size());
+    packs.insert(packs.end(), packs_of[s].begin(), packs_of[s].end());
+    d.pack_end = int(packs.size());
   }
   if (np > 0) {
     SvdDesc* dsd = c->push(sd);
+    CopyDesc* dpk = c->push(packs);
     double sbytes = 0.0, sflops = 0.0;
     for (int s2 = 0; s2 < np; ++s2) {
       double mm = double(std::max(order[s2]->m, order[s2]->n)), r = double(std::min(order[s2]->m, order[s2]->n));
@@ -486,7 +492,7 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
     }
     c->begin();
-    bugk::launch_svd(dsd, np, max_smem, c->stream);
+    bugk::launch_svd(dsd, np, dpk, max_smem, c->stream);
     c->launched(BUG_K_SVD, sflops, sbytes);
   }
   // read back singular values and sweep counts
@@ -568,8 +574,10 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       vkeys.push_back(k);
     }
   }
-  U = make_tensor(c, int(L.size()) + 1, ulegs, ukeys, false);
-  Vd = make_tensor(c, int(R.size()) + 1, vlegs, vkeys, false);
+  if (want & 1) U = make_tensor(c, int(L.size()) + 1, ulegs, ukeys, false);
+  if (want & 2) Vd = make_tensor(c, int(R.size()) + 1, vlegs, vkeys, false);
+  if ((want & 4) && USo) *USo = make_tensor(c, int(L.size()) + 1, ulegs, ukeys, false);
+  if ((want & 8) && SVdo) *SVdo = make_tensor(c, int(R.size()) + 1, vlegs, vkeys, false);
   std::vector<CopyDesc> out;
   for (int s = 0; s < np; ++s) {
     if (kc[s] == 0) continue;
@@ -578,10 +586,8 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       Key k{};
       for (size_t j = 0; j < p.rows[ri].size(); ++j) k[j] = p.rows[ri][j];
       k[p.rows[ri].size()] = p.charge;
-      int ub = U->find(k);
       CopyDesc d{};
       d.src = W + uoff[s] + p.roff[ri];
-      d.dst = U->mdata(ub);
       d.n = p.rdim[ri] * kc[s];
       d.ndim = 2;
       d.dims[0] = int(p.rdim[ri]);
@@ -591,16 +597,23 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       d.dstr[0] = kc[s];
       d.dstr[1] = 1;
       d.alpha = make_double2(1.0, 0.0);
-      out.push_back(d);
+      if (want & 1) {
+        d.dst = U->mdata(U->find(k));
+        out.push_back(d);
+      }
+      if ((want & 4) && USo) {
+        d.dst = (*USo)->mdata((*USo)->find(k));
+        d.w = S + soff[s];
+        d.wdim = 1;
+        out.push_back(d);
+      }
     }
     for (size_t ci = 0; ci < p.cols.size(); ++ci) {
       Key k{};
       k[0] = p.charge;
       for (size_t j = 0; j < p.cols[ci].size(); ++j) k[j + 1] = p.cols[ci][j];
-      int vb = Vd->find(k);
       CopyDesc d{};
       d.src = W + voff[s] + p.coff[ci];
-      d.dst = Vd->mdata(vb);
       d.n = p.cdim[ci] * kc[s];
       d.ndim = 2;
       d.dims[0] = kc[s];
@@ -611,7 +624,16 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       d.dstr[1] = 1;
       d.conj = 1;
       d.alpha = make_double2(1.0, 0.0);
-      out.push_back(d);
+      if (want & 2) {
+        d.dst = Vd->mdata(Vd->find(k));
+        out.push_back(d);
+      }
+      if ((want & 8) && SVdo) {
+        d.dst = (*SVdo)->mdata((*SVdo)->find(k));
+        d.w = S + soff[s];
+        d.wdim = 0;
+        out.push_back(d);
+      }
     }
   }
   run_copies(c, out);
@@ -621,6 +643,34 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
 // ── reductions and linear combinations ───────────────────────────────────────────────────────
 
 constexpr int64_t kDotChunk = 16384;
+
+// Run a descriptor list whose descriptors are grouped by output slot (seg[o]..seg[o+1]) through
+// the one-launch reduction; returns nout complex sums (read back, synchronising).
+void run_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<int>& seg, int nout,
+              double* out_re_im, double bytes_per_elem) {
+  if (nout <= 0) return;
+  if (descs.empty()) {
+    for (int i = 0; i < 2 * nout; ++i) out_re_im[i] = 0.0;
+    return;
+  }
+  if (!c->dot_counter) {
+    BUG_CUDA(cudaMalloc((void**)&c->dot_counter, sizeof(unsigned int)));
+    BUG_CUDA(cudaMemsetAsync(c->dot_counter, 0, sizeof(unsigned int), c->stream));
+  }
+  double2* partial = static_cast<double2*>(c->scratch(descs.size() * sizeof(double2)));
+  double2* res = static_cast<double2*>(c->scratch(size_t(nout) * sizeof(double2)));
+  DotDesc* dd = c->push(descs);
+  int* dseg = c->push(seg);
+  double dbytes = 0.0;
+  for (auto& d : descs) dbytes += bytes_per_elem * double(d.n);
+  c->begin();
+  bugk::launch_dot_fused(dd, int(descs.size()), partial, dseg, nout, res, c->dot_counter, c->stream);
+  c->launched(BUG_K_DOT, 0.0, dbytes);
+  double* host = c->readback(size_t(2 * nout));
+  BUG_CUDA(cudaMemcpyAsync(host, res, size_t(nout) * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  std::memcpy(out_re_im, host, size_t(nout) * sizeof(double2));
+}
 
 void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
           double* out_re_im) {
@@ -645,26 +695,39 @@ void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_t
     }
   }
   seg[pairs.size()] = int(descs.size());
-  const int nout = int(pairs.size());
-  double2* partial = static_cast<double2*>(c->scratch(std::max<size_t>(descs.size(), 1) * sizeof(double2)));
-  double2* res = static_cast<double2*>(c->scratch(std::max(nout, 1) * sizeof(double2)));
-  if (!descs.empty()) {
-    DotDesc* dd = c->push(descs);
-    double dbytes = 0.0;
-    for (auto& d : descs) dbytes += 32.0 * double(d.n);
-    c->begin();
-    bugk::launch_dot(dd, int(descs.size()), partial, c->stream);
-    c->launched(BUG_K_DOT, 0.0, dbytes);
+  run_dots(c, descs, seg, int(pairs.size()), out_re_im, 32.0);
+}
+
+// sum of |x|^2 over the blocks of `t` whose charge on `leg` is sector s, for every sector s of
+// that leg (ascending), in one launch and one read-back.
+std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg) {
+  const Leg& L = t.legs[leg];
+  const int nout = int(L.q.size());
+  std::vector<std::vector<DotDesc>> per(nout);
+  for (int bi = 0; bi < int(t.blocks.size()); ++bi) {
+    const int s = L.index_of(t.blocks[bi].key[leg]);
+    for (int64_t o = 0; o < t.blocks[bi].size; o += kDotChunk) {
+      DotDesc d{};
+      d.a = t.data(bi) + o;
+      d.b = t.data(bi) + o;
+      d.n = std::min(kDotChunk, t.blocks[bi].size - o);
+      d.out = s;
+      per[s].push_back(d);
+    }
   }
-  int* dseg = c->push(seg);
-  c->begin();
-  bugk::launch_dot_reduce(partial, dseg, nout, res, c->stream);
-  c->launched(BUG_K_DOT, 0.0, 16.0 * double(descs.size()));
-  double* host = c->readback(size_t(2 * std::max(nout, 1)));
-  BUG_CUDA(cudaMemcpyAsync(host, res, size_t(nout) * sizeof(double2), cudaMemcpyDeviceToHost,
-                           c->stream));
-  BUG_CUDA(cudaStreamSynchronize(c->stream));
-  std::memcpy(out_re_im, host, size_t(nout) * sizeof(double2));
+  std::vector<DotDesc> descs;
+  std::vector<int> seg(nout + 1, 0);
+  for (int s = 0; s < nout; ++s) {
+    seg[s] = int(descs.size());
+    descs.insert(descs.end(), per[s].begin(), per[s].end());
+  }
+  seg[nout] = int(descs.size());
+  std::vector<double> out(nout, 0.0);
+  if (nout == 0) return out;
+  std::vector<double> tmp(2 * size_t(nout));
+  run_dots(c, descs, seg, nout, tmp.data(), 16.0);
+  for (int s = 0; s < nout; ++s) out[s] = tmp[2 * s];
+  return out;
 }
 
 std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
@@ -993,6 +1056,7 @@ int bug_ctx_destroy(bug_ctx* c) {
     }
     if (c->pinned_out) cudaFreeHost(c->pinned_out);
     if (c->arena) cudaFreeAsync(c->arena, c->stream);
+    if (c->dot_counter) cudaFree(c->dot_counter);
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -1140,7 +1204,7 @@ int bug_svd(bug_ctx* c, const bug_tensor* t, int nleft, const int* left, double 
     std::vector<double> sv;
     std::vector<int> q;
     int nk = 0;
-    svd_impl(c, *t, nleft, left, cutoff, nkeep, u, v, sv, q, nk);
+    svd_impl(c, *t, nleft, left, cutoff, nkeep, u, v, sv, q, nk, 3, nullptr, nullptr);
     int ncopy = std::min<int>(cap, int(sv.size()));
     for (int i = 0; i < ncopy; ++i) {
       sv_all[i] = sv[i];

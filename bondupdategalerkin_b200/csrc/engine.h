@@ -198,6 +198,7 @@ struct bug_ctx {
   // in one pinned copy + one H2D transfer (commit, run by begin() right before the launch). The
   // arena is reused by every launch: the next transfer into it is stream-ordered after the kernel
   // that read it.
+  unsigned int* dot_counter = nullptr;  // last-block counter of the fused reduction
   char* arena = nullptr;
   size_t arena_cap = 0;
   std::vector<char> batch;
@@ -279,12 +280,14 @@ Leg merged(const Leg& a, const Leg& b);
 TensorPtr permute_impl(bug_ctx* c, const bug_tensor& t, const int* perm);
 TensorPtr contract_impl(bug_ctx* c, const bug_tensor& A, int n, const int* ia, const bug_tensor& B,
                         const int* ib, bool conja, bool conjb);
+// want: 1 = U, 2 = Vd, 4 = U*S (into *US), 8 = S*Vd (into *SVd); all produced by one unpack launch
 int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
              TensorPtr& U, TensorPtr& Vd, std::vector<double>& sv_sorted, std::vector<int>& sv_q,
-             int& nkept);
+             int& nkept, int want = 3, TensorPtr* US = nullptr, TensorPtr* SVd = nullptr);
 void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
           double* out_re_im);
 TensorPtr lincomb_impl(bug_ctx* c, int n, const double* coef, const bug_tensor* const* ts);
+std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg);
 TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& t, int leg, const double* w);
 TensorPtr conj_impl(bug_ctx* c, const bug_tensor& t);
 TensorPtr flip_leg_impl(bug_ctx* c, const bug_tensor& t, int leg);

@@ -55,14 +55,21 @@ __global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restri
     const CopyDesc& c = d[find_desc(d, nd, e)];
     int64_t r = e - c.prefix;
     int64_t so = 0, dof = 0;
+    int64_t widx = 0;
     for (int k = c.ndim - 1; k >= 0; --k) {
       int64_t i = r % c.dims[k];
       r /= c.dims[k];
       so += i * c.sstr[k];
       dof += i * c.dstr[k];
+      if (k == c.wdim) widx = i;
     }
     double2 v = c.src[so];
     if (c.conj) v.y = -v.y;
+    if (c.w) {
+      const double s = c.w[widx];
+      v.x *= s;
+      v.y *= s;
+    }
     double2 w = cmul(c.alpha, v);
     if (c.accumulate) {
       double2 o = c.dst[dof];
@@ -177,6 +184,7 @@ __device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b
 }
 
 __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __restrict__ descs,
+                                                              const CopyDesc* __restrict__ packs,
                                                               double tol_scale) {
   extern __shared__ double2 dyn[];
   __shared__ double sig[kMaxR];
@@ -187,6 +195,23 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __r
   const int r = d.m < d.n ? d.m : d.n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   if (r <= 0) return;
+  // gather the sector matrix from the tensor's blocks (column-major M, or M^H)
+  for (int pk = d.pack_begin; pk < d.pack_end; ++pk) {
+    const CopyDesc& c = packs[pk];
+    for (int64_t e = tid; e < c.n; e += blockDim.x) {
+      int64_t rr = e, so = 0, dof = 0;
+      for (int k = c.ndim - 1; k >= 0; --k) {
+        const int64_t i = rr % c.dims[k];
+        rr /= c.dims[k];
+        so += i * c.sstr[k];
+        dof += i * c.dstr[k];
+      }
+      double2 v = c.src[so];
+      if (c.conj) v.y = -v.y;
+      c.dst[dof] = v;
+    }
+  }
+  __syncthreads();
   double2* A = d.work;
   double2* V = d.vwork;
   if (d.use_smem) {
@@ -335,6 +360,57 @@ __global__ void __launch_bounds__(kThreads) dot_kernel(const DotDesc* __restrict
   }
 }
 
+// One-launch reduction: every block writes its partial, and the last block to finish (counted on
+// a persistent counter that it resets) sums each output's partials in index order, so the result
+// is deterministic.
+__global__ void __launch_bounds__(kThreads) dot_fused_kernel(const DotDesc* __restrict__ d,
+                                                             double2* __restrict__ partial,
+                                                             const int* __restrict__ seg, int nout,
+                                                             double2* __restrict__ out,
+                                                             unsigned int* counter) {
+  __shared__ double sr[kThreads / 32], si[kThreads / 32];
+  __shared__ bool last;
+  const DotDesc c = d[blockIdx.x];
+  double re = 0.0, im = 0.0;
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
+    const double2 a = c.a[i], b = c.b[i];
+    re = fma(a.x, b.x, fma(a.y, b.y, re));
+    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+  }
+  re = warp_sum(re);
+  im = warp_sum(im);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sr[warp] = re;
+    si[warp] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, ti = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tr += sr[w];
+      ti += si[w];
+    }
+    partial[blockIdx.x] = make_double2(tr, ti);
+    __threadfence();
+    const unsigned int t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+    double tr = 0.0, ti = 0.0;
+    for (int k = seg[o]; k < seg[o + 1]; ++k) {
+      const double2 p = __ldcg(&partial[k]);
+      tr += p.x;
+      ti += p.y;
+    }
+    out[o] = make_double2(tr, ti);
+  }
+  if (threadIdx.x == 0) *counter = 0u;
+}
+
 __global__ void dot_reduce_kernel(const double2* __restrict__ partial,
                                   const int* __restrict__ seg, int nout, double2* __restrict__ out) {
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -389,17 +465,24 @@ void launch_gemm(const GemmOut* outs, const GemmPair* pairs, const GemmTile* til
   gemm_kernel<<<ntiles, kThreads, 0, s>>>(outs, pairs, tiles);
 }
 
-void launch_svd(const SvdDesc* d_desc, int nprob, int max_smem_bytes, cudaStream_t s) {
+void launch_svd(const SvdDesc* d_desc, int nprob, const CopyDesc* packs, int max_smem_bytes,
+                cudaStream_t s) {
   if (nprob <= 0) return;
   if (max_smem_bytes > 0)
     cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          max_smem_bytes);
-  jacobi_svd_kernel<<<nprob, kThreads, max_smem_bytes, s>>>(d_desc, 2.220446049250313e-16);
+  jacobi_svd_kernel<<<nprob, kThreads, max_smem_bytes, s>>>(d_desc, packs, 2.220446049250313e-16);
 }
 
 void launch_dot(const DotDesc* d_desc, int ndesc, double2* partial, cudaStream_t s) {
   if (ndesc <= 0) return;
   dot_kernel<<<ndesc, kThreads, 0, s>>>(d_desc, partial);
+}
+
+void launch_dot_fused(const DotDesc* d_desc, int ndesc, double2* partial, const int* seg, int nout,
+                      double2* out, unsigned int* counter, cudaStream_t s) {
+  if (ndesc <= 0) return;
+  dot_fused_kernel<<<ndesc, kThreads, 0, s>>>(d_desc, partial, seg, nout, out, counter);
 }
 
 void launch_dot_reduce(const double2* partial, const int* seg_begin, int nout, double2* out,

@@ -31,6 +31,9 @@ struct CopyDesc {
   int accumulate;   // dst += alpha*v instead of dst = alpha*v
   int pad_;
   double2 alpha;
+  const double* w;  // optional per-index weight along dim `wdim` (singular values for U*S, S*Vd)
+  int wdim;
+  int pad2_;
   int dims[kMaxRank];
   int64_t sstr[kMaxRank];
   int64_t dstr[kMaxRank];
@@ -77,6 +80,7 @@ struct SvdDesc {
   int m, n;         // shape of M
   int trans;        // 1: work holds M^H (m < n)
   int use_smem;     // 1: the CTA copies work/vwork into shared memory
+  int pack_begin, pack_end;  // gather descriptors that assemble `work` from the tensor's blocks
 };
 
 struct DotDesc {
@@ -113,8 +117,11 @@ struct ScaleDesc {
 void launch_copy(const CopyDesc* d_desc, int ndesc, int64_t total, cudaStream_t s);
 void launch_gemm(const GemmOut* outs, const GemmPair* pairs, const GemmTile* tiles, int ntiles,
                  cudaStream_t s);
-void launch_svd(const SvdDesc* d_desc, int nprob, int max_smem_bytes, cudaStream_t s);
+void launch_svd(const SvdDesc* d_desc, int nprob, const CopyDesc* packs, int max_smem_bytes,
+                cudaStream_t s);
 void launch_dot(const DotDesc* d_desc, int ndesc, double2* partial, cudaStream_t s);
+void launch_dot_fused(const DotDesc* d_desc, int ndesc, double2* partial, const int* seg, int nout,
+                      double2* out, unsigned int* counter, cudaStream_t s);
 void launch_dot_reduce(const double2* partial, const int* seg_begin, int nout, double2* out,
                        cudaStream_t s);
 void launch_lincomb(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,

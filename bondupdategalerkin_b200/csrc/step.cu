@@ -151,20 +151,24 @@ struct Eng {
 inline int64_t dim(const T& t, int leg) { return t->legs[leg].total(); }
 
 struct SVDRes {
-  T U, Vd;
+  T U, Vd, Us, SVd_;  // Us = U*S and SVd_ = S*Vd when requested
   std::map<int, std::vector<double>> S;
   std::vector<std::pair<double, int>> kept, trunc;  // (sigma, charge), descending
 };
 
-SVDRes svd(const Eng& e, const T& t, std::vector<int> left, double cutoff, int nkeep = -1) {
-  TensorPtr U, V;
+// want: 1 = U, 2 = Vd, 4 = U*S, 8 = S*Vd (one unpack launch writes all requested factors)
+SVDRes svd(const Eng& e, const T& t, std::vector<int> left, double cutoff, int nkeep = -1,
+           int want = 3) {
+  TensorPtr U, V, US_, SV_;
   std::vector<double> sv;
   std::vector<int> q;
   int nk = 0;
-  svd_impl(e.c, *t, int(left.size()), left.data(), cutoff, nkeep, U, V, sv, q, nk);
+  svd_impl(e.c, *t, int(left.size()), left.data(), cutoff, nkeep, U, V, sv, q, nk, want, &US_, &SV_);
   SVDRes r;
-  r.U = Eng::sh(std::move(U));
-  r.Vd = Eng::sh(std::move(V));
+  if (U) r.U = Eng::sh(std::move(U));
+  if (V) r.Vd = Eng::sh(std::move(V));
+  if (US_) r.Us = Eng::sh(std::move(US_));
+  if (SV_) r.SVd_ = Eng::sh(std::move(SV_));
   for (size_t i = 0; i < sv.size(); ++i) {
     if (int(i) < nk) {
       r.kept.push_back({sv[i], q[i]});
@@ -176,8 +180,9 @@ SVDRes svd(const Eng& e, const T& t, std::vector<int> left, double cutoff, int n
   return r;
 }
 
-T US(const Eng& e, const SVDRes& r) { return e.scale_leg(r.U, r.U->rank - 1, r.S); }
-T SVd(const Eng& e, const SVDRes& r) { return e.scale_leg(r.Vd, 0, r.S); }
+T US(const Eng& e, const SVDRes& r) { return r.Us ? r.Us : e.scale_leg(r.U, r.U->rank - 1, r.S); }
+T SVd(const Eng& e, const SVDRes& r) { return r.SVd_ ? r.SVd_ : e.scale_leg(r.Vd, 0, r.S); }
+constexpr int W_U = 1, W_VD = 2, W_US = 4, W_SVD = 8;
 
 double sq_weight(const std::vector<std::pair<double, int>>& l) {
   double s = 0.0;
@@ -412,8 +417,8 @@ T reortho(const Eng& e, const T& frame, const T& block, bool left) {
   if (!block) return nullptr;
   T out = left ? perp_left(e, frame, block) : perp_right(e, frame, block);
   if (e.norm(out) <= CBE_EPS * std::max(e.norm(block), 1.0)) return nullptr;
-  if (left) return svd(e, out, {0, 1}, 1e-14).U;
-  return rows_from_u(e, svd(e, out, {1, 2}, 1e-14).U);
+  if (left) return svd(e, out, {0, 1}, 1e-14, -1, W_U).U;
+  return rows_from_u(e, svd(e, out, {1, 2}, 1e-14, -1, W_U).U);
 }
 
 // fused local space of a frame: charge -> list of (qa, qb) pairs, and per charge dims
@@ -564,17 +569,11 @@ double sample_residual(const Eng& e, const T& basis, const std::function<T(const
   const int rleg = left ? 2 : 0;
   double tot = 0.0;
   const Leg& rl = res->legs[rleg];
+  const std::vector<double> n2 = sector_norms2(e.c, *res, rleg);
   for (size_t s = 0; s < rl.q.size(); ++s) {
     auto it = cols.find(rl.q[s]);
     require(it != cols.end() && it->second > 0, "Test B: residual sector has no holdout column");
-    double n2;
-    if (rl.q.size() > 1) {
-      T rq = e.trim(res, rleg, {{rl.q[s], rl.d[s]}});
-      n2 = rq ? std::pow(e.norm(rq), 2) : 0.0;
-    } else {
-      n2 = std::pow(e.norm(res), 2);
-    }
-    tot += n2 / it->second;
+    tot += n2[s] / it->second;
   }
   return std::sqrt(tot);
 }
@@ -639,12 +638,12 @@ struct Step {
 
   // canonical form (canonical_form.jl)
   void move_right(MPS& psi, int site) {
-    SVDRes r = svd(e, psi[site], {0, 1}, 0.0);
+    SVDRes r = svd(e, psi[site], {0, 1}, 0.0, -1, W_U | W_SVD);
     psi[site + 1] = e.contract(SVd(e, r), {1}, psi[site + 1], {0});
     psi[site] = r.U;
   }
   void move_left(MPS& psi, int site) {
-    SVDRes r = svd(e, psi[site], {0}, 0.0);
+    SVDRes r = svd(e, psi[site], {0}, 0.0, -1, W_VD | W_US);
     psi[site - 1] = e.contract(psi[site - 1], {2}, US(e, r), {0});
     psi[site] = r.Vd;
   }
@@ -682,18 +681,18 @@ struct Step {
   }
 
   BondFrame frame_from(const T& left, const T& right) {
-    SVDRes rl = svd(e, left, {0, 1}, 0.0);
-    SVDRes rr = svd(e, right, {0}, 0.0);
+    SVDRes rl = svd(e, left, {0, 1}, 0.0, -1, W_U | W_SVD);
+    SVDRes rr = svd(e, right, {0}, 0.0, -1, W_US | W_VD);
     T core = e.contract(SVd(e, rl), {1}, US(e, rr), {0});
     return BondFrame{rl.U, core, rr.Vd, dim(rl.U, 2)};
   }
   BondFrame frame_onto_left(const T& liso, const T& carry, const T& right) {
-    SVDRes rr = svd(e, right, {0}, 0.0);
+    SVDRes rr = svd(e, right, {0}, 0.0, -1, W_US | W_VD);
     T ov = e.contract(liso, {0, 1}, carry, {0, 1}, true, false);
     return BondFrame{liso, e.contract(ov, {1}, US(e, rr), {0}), rr.Vd, dim(liso, 2)};
   }
   BondFrame frame_onto_right(const T& left, const T& carry, const T& riso) {
-    SVDRes rl = svd(e, left, {0, 1}, 0.0);
+    SVDRes rl = svd(e, left, {0, 1}, 0.0, -1, W_U | W_SVD);
     T ov = e.contract(carry, {1, 2}, riso, {1, 2}, false, true);
     return BondFrame{rl.U, e.contract(SVd(e, rl), {1}, ov, {0}), riso, dim(riso, 0)};
   }
@@ -749,7 +748,7 @@ struct Step {
           if (k <= 0) return nullptr;
           auto it = cache.find(k);
           if (it != cache.end()) return it->second;
-          SVDRes fac = svd(e, Y, legs, rank_cut(0.0, nY, nY), int(k));
+          SVDRes fac = svd(e, Y, legs, rank_cut(0.0, nY, nY), int(k), W_U);
           T res;
           if (!fac.kept.empty()) res = left ? reortho(e, frame, fac.U, true)
                                             : reortho(e, frame, rows_from_u(e, fac.U), false);
@@ -946,12 +945,12 @@ struct Step {
     std::vector<int> legs = left ? std::vector<int>{0, 1} : std::vector<int>{1, 2};
     const double nres = e.norm(residual);
     const double cut = rank_cut(0.0, e.norm(direction), nres);
-    SVDRes res = svd(e, residual, legs, cut);
+    SVDRes res = svd(e, residual, legs, cut, -1, W_U);
     const int nk = int(res.kept.size());
     auto tr = tail_rank(res.kept, weight, allowance, int(std::min<int64_t>(nk, room)), sq_weight(res.trunc));
     const bool fits = tr.second <= allowance;
     if (tr.first == 0) return {frame, 0, fits};
-    if (tr.first < nk) res = svd(e, residual, legs, cut, tr.first);
+    if (tr.first < nk) res = svd(e, residual, legs, cut, tr.first, W_U);
     T nb = left ? reortho(e, frame, res.U, true) : reortho(e, frame, rows_from_u(e, res.U), false);
     nb = cap_to_local_room(e, frame, nb, left);
     if (!nb) return {frame, 0, fits};
@@ -1091,7 +1090,7 @@ struct Step {
     std::vector<T> rfac(L + 2);
     for (int site = L; site >= 2; --site) {
       T carried = site == L ? psi[L] : e.contract(psi[site], {2}, rfac[site + 1], {0});
-      rfac[site] = US(e, svd(e, carried, {0}, 0.0));
+      rfac[site] = US(e, svd(e, carried, {0}, 0.0, -1, W_US));
     }
     double miss2 = 0.0;
     T AL;
@@ -1102,9 +1101,9 @@ struct Step {
       AL = e.contract(lf[site], {0, 1}, carried, {0, 1}, true, false);
     }
     std::vector<T> lfac(L + 1);
-    lfac[root_link] = SVd(e, svd(e, AL, {0}, 0.0));
+    lfac[root_link] = SVd(e, svd(e, AL, {0}, 0.0, -1, W_SVD));
     for (int bond = root_link + 1; bond <= L - 1; ++bond)
-      lfac[bond] = SVd(e, svd(e, e.contract(lfac[bond - 1], {1}, psi[bond], {0}), {0, 1}, 0.0));
+      lfac[bond] = SVd(e, svd(e, e.contract(lfac[bond - 1], {1}, psi[bond], {0}), {0, 1}, 0.0, -1, W_SVD));
     T AR;
     for (int bond = L - 1; bond >= root_link; --bond) {
       T carried = AR ? e.contract(psi[bond + 1], {2}, AR, {0}) : psi[bond + 1];
@@ -1526,13 +1525,14 @@ struct Step {
   // ── compression (truncation.jl) ──
   std::pair<SVDRes, bool> budget_svd(const T& t, std::vector<int> split, int maxdim,
                                      const std::function<double(double)>& share_of) {
-    SVDRes res = svd(e, t, split, 0.0, maxdim);
+    const int want = split.size() == 1 ? (W_VD | W_US) : (W_U | W_SVD);
+    SVDRes res = svd(e, t, split, 0.0, maxdim, want);
     const double share = share_of(sq_weight(res.kept) + sq_weight(res.trunc));
     const int nk = int(res.kept.size());
     auto tr = tail_rank(res.kept, 1.0, share, nk, sq_weight(res.trunc));
     const bool capped = tr.second > share && !res.trunc.empty();
     const int keep = std::max(tr.first, 1);
-    if (keep < nk) res = svd(e, t, split, 0.0, keep);
+    if (keep < nk) res = svd(e, t, split, 0.0, keep, want);
     return {res, capped};
   }
 
@@ -1729,7 +1729,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     ledger.expv_err = rep.err;
     ledger.expv_iters = rep.iters;
     if (rep.err > P.tol_expv * (1 + 1e-8)) ledger.unmet_(U_EXPV);
-    SVDRes res = svd(e, root_result, {0}, 0.0);
+    SVDRes res = svd(e, root_result, {0}, 0.0, -1, W_U | W_SVD);
     expanded[S.root_link - 1] = dim(lf[S.root_link], 2);
     const int64_t root_frame_width = dim(rf[S.root_link], 0);
     // assemble and compress (diagnostics.jl:269-337)
