@@ -56,6 +56,7 @@ SIGNATURES = {
     "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
     "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "bug_la_eigvals_hess": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
+    "bug_inner_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, _vp]),
 }
 # declared in native.py (structure arguments)
 NATIVE_ONLY = ("bug_mps_step",)

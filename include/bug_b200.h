@@ -222,6 +222,20 @@ int bug_la_eigh(int n, const double* a, double* vals, double* vecs);
 /* Eigenvalues of a complex upper-Hessenberg n x n matrix; replaces geev in _hess_coeffs. */
 int bug_la_eigvals_hess(int n, const double* a, double* vals_re_im);
 
+/* ── allocation-free inner product ──────────────────────────────────────────────────────── */
+/* No counterpart in the reference: added for callers that cannot allocate GPU memory at the call
+ * site -- a process whose device memory budget is fixed up front, a host callback or library hook
+ * where cudaMalloc is forbidden, or code that must not create or use an engine context (contexts
+ * allocate). Computes out[0] + i*out[1] = sum_i conj(a_i) * b_i for `n` interleaved complex
+ * doubles at device pointers `a` and `b`, writing the result to the device pointer `out`, on
+ * `stream` (a cudaStream_t; NULL is the default stream). The reduction scratch is a 64 KiB static
+ * device array held by every device that loads this library until the process exits; n may be at
+ * most 8,388,608 (larger n returns BUG_EINVAL). The first call on a device looks the array up with
+ * cudaGetSymbolAddress and should come before any stream capture. Calls on one device share the
+ * array: calls whose kernels overlap on the GPU race, so serialise them. No cudaMalloc, cudaFree
+ * or allocating library routine is called. */
+int bug_inner_noalloc(const double* a, const double* b, int64_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
