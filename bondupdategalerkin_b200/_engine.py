@@ -31,6 +31,8 @@ SIGNATURES = {
     "bug_ctx_kernel_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
                                             _c_double_p, _c_double_p, _c_double_p]),
     "bug_ctx_reset_stats": (ctypes.c_int, [_vp]),
+    "bug_ctx_host_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int64), _c_double_p,
+                                          _c_double_p, _c_double_p]),
     "bug_tensor_create": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, _c_int_p, _c_int_p, _c_int_p,
                                          ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_tensor_upload": (ctypes.c_int, [_vp, _vp, _c_double_p, ctypes.c_int64]),
@@ -62,8 +64,11 @@ SIGNATURES = {
 NATIVE_ONLY = ("bug_mps_step",)
 
 FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
-KERNEL_NAMES = {"copy": "copy_kernel", "gemm": "gemm_kernel", "svd": "jacobi_svd_kernel",
-                "dot": "dot_kernel", "lincomb": "lincomb_kernel", "scale": "scale_kernel"}
+# Where each family runs: the SVD is its own kernel; every other family is a stage kind of
+# stage_kernel (operations queued between two read-backs launch together as one stage list).
+KERNEL_NAMES = {"copy": "stage_kernel (copy stage)", "gemm": "stage_kernel (gemm stage)",
+                "svd": "jacobi_svd_kernel", "dot": "stage_kernel (dot stages)",
+                "lincomb": "stage_kernel (lincomb stage)", "scale": "stage_kernel (scale stage)"}
 
 STATUS = {0: "BUG_OK", 1: "BUG_EINVAL", 2: "BUG_ENONFINITE", 3: "BUG_ENOMEM", 4: "BUG_ETIMEOUT",
           5: "BUG_EDEVICE", 6: "BUG_ENOTCONV"}
@@ -132,6 +137,14 @@ class Context:
 
     def reset_stats(self) -> None:
         check(self.lib.bug_ctx_reset_stats(self.h))
+
+    def host_stats(self) -> dict:
+        """Host accounting since the last reset: read-back waits (count, seconds), seconds inside
+        kernel-launch calls and inside the stream-ordered allocator."""
+        n, w, la, al = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(self.lib.bug_ctx_host_stats(self.h, ctypes.byref(n), ctypes.byref(w), ctypes.byref(la),
+                                          ctypes.byref(al)))
+        return dict(syncs=int(n.value), wait_s=w.value, launch_s=la.value, alloc_s=al.value)
 
     def kernel_stats(self) -> dict:
         """Per kernel family: launches, algorithmic flops and bytes, device ms (profiling only)."""

@@ -15,9 +15,31 @@ thread_local bug_ctx* g_active_ctx = nullptr;
 
 Buffer::~Buffer() {
   if (ptr && ctx) {
-    cudaFreeAsync(ptr, ctx->stream);
+    ctx->dev_free(ptr);
     ctx->bytes -= n * int64_t(sizeof(double2));
   }
+}
+
+void run_copies(bug_ctx* c, std::vector<CopyDesc>& descs);
+
+// Zero n elements at p: a copy stage whose source is null.
+void zero_fill(bug_ctx* c, double2* p, int64_t n) {
+  std::vector<CopyDesc> d;
+  const int64_t chunk = int64_t(1) << 30;
+  for (int64_t off = 0; off < n; off += chunk) {
+    CopyDesc cd{};
+    cd.src = nullptr;
+    cd.dst = p + off;
+    cd.n = std::min(chunk, n - off);
+    cd.ndim = 1;
+    cd.dims[0] = int(cd.n);
+    cd.sstr[0] = 0;
+    cd.dstr[0] = 1;
+    cd.alpha = make_double2(1.0, 0.0);
+    cd.wdim = -1;
+    d.push_back(cd);
+  }
+  run_copies(c, d);
 }
 
 std::shared_ptr<Buffer> alloc_buffer(bug_ctx* c, int64_t n, bool zero) {
@@ -25,8 +47,8 @@ std::shared_ptr<Buffer> alloc_buffer(bug_ctx* c, int64_t n, bool zero) {
   b->n = n;
   b->ctx = c;
   if (n > 0) {
-    BUG_CUDA(cudaMallocAsync((void**)&b->ptr, size_t(n) * sizeof(double2), c->stream));
-    if (zero) BUG_CUDA(cudaMemsetAsync(b->ptr, 0, size_t(n) * sizeof(double2), c->stream));
+    b->ptr = static_cast<double2*>(c->dev_alloc(size_t(n) * sizeof(double2)));
+    if (zero) zero_fill(c, b->ptr, n);
     c->bytes += n * int64_t(sizeof(double2));
   }
   return b;
@@ -62,7 +84,6 @@ std::unique_ptr<bug_tensor> make_tensor(bug_ctx* c, int rank, std::vector<Leg> l
     b.size = block_size(*t, k, b.shape);
     b.off = off;
     off += b.size;
-    t->index[k] = int(t->blocks.size());
     t->blocks.push_back(b);
   }
   t->nelem = off;
@@ -116,9 +137,12 @@ void run_copies(bug_ctx* c, std::vector<CopyDesc>& descs) {
   }
   if (nz.empty()) return;
   CopyDesc* dd = c->push(nz);
-  c->begin();
-  bugk::launch_copy(dd, int(nz.size()), total, c->stream);
-  c->launched(BUG_K_COPY, 0.0, 32.0 * double(total));
+  bugk::Stage st{};
+  st.kind = bugk::kStageCopy;
+  st.n = int(nz.size());
+  st.total = total;
+  st.a = dd;
+  c->run_stage(st, BUG_K_COPY, 0.0, 32.0 * double(total));
 }
 
 CopyDesc plain_copy(const double2* src, double2* dst, int64_t n, bool conj, double2 alpha,
@@ -323,9 +347,13 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
       gbytes += 16.0 * (double(go.m) + double(go.n)) * double(pairs[p].k);
     }
   }
-  c->begin();
-  bugk::launch_gemm(d_outs, d_pairs, d_tiles, int(tiles.size()), c->stream);
-  c->launched(BUG_K_GEMM, flops, gbytes);
+  bugk::Stage st{};
+  st.kind = bugk::kStageGemm;
+  st.n = int(tiles.size());
+  st.a = d_outs;
+  st.b = d_pairs;
+  st.c = d_tiles;
+  c->run_stage(st, BUG_K_GEMM, flops, gbytes);
   return out;
 }
 
@@ -407,7 +435,10 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
   }
   double2* W = static_cast<double2*>(c->scratch(size_t(wtot) * sizeof(double2)));
   double* S = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
-  int* sweeps = static_cast<int*>(c->scratch(size_t(std::max(np, 1)) * sizeof(int)));
+  // singular values and sweep counts also go straight to host-mapped pinned memory
+  double* host = c->readback(size_t(stot) + size_t(np) + 1);
+  int* sweeps = reinterpret_cast<int*>(host + stot);
+  for (int s = 0; s < np; ++s) sweeps[s] = 0;
   // gather descriptors of the sector matrices (column-major M, or M^H when m < n), run inside the
   // Jacobi kernel itself
   std::vector<std::vector<CopyDesc>> packs_of(order.size());
@@ -471,6 +502,7 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
     d.U = W + uoff[s];
     d.V = W + voff[s];
     d.S = S + soff[s];
+    d.S_host = host + soff[s];
     d.sweeps = sweeps + s;
     d.m = int(p.m);
     d.n = int(p.n);
@@ -491,22 +523,14 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       sbytes += 16.0 * (2.0 * mm * r + r * r + (order[s2]->m + order[s2]->n) * r);
       sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
     }
-    c->begin();
-    bugk::launch_svd(dsd, np, dpk, max_smem, c->stream);
+    const bugk::Blob blob = c->begin();
+    bugk::launch_svd(blob, dsd, np, dpk, max_smem, c->stream);
     c->launched(BUG_K_SVD, sflops, sbytes);
   }
-  // read back singular values and sweep counts
-  const size_t nread = size_t(stot) + size_t(np);
-  double* host = c->readback(std::max<size_t>(nread, 1));
-  if (stot > 0) BUG_CUDA(cudaMemcpyAsync(host, S, size_t(stot) * sizeof(double),
-                                        cudaMemcpyDeviceToHost, c->stream));
-  std::vector<int> hsweeps(np);
-  if (np > 0) BUG_CUDA(cudaMemcpyAsync(host + stot, sweeps, size_t(np) * sizeof(int),
-                                      cudaMemcpyDeviceToHost, c->stream));
-  BUG_CUDA(cudaStreamSynchronize(c->stream));
-  if (np > 0) std::memcpy(hsweeps.data(), host + stot, size_t(np) * sizeof(int));
+  // the kernel wrote singular values and sweep counts into `host`
+  c->wait();
   for (int s = 0; s < np; ++s)
-    if (hsweeps[s] < 0) {
+    if (sweeps[s] < 0) {
       throw BugError(BUG_ENOTCONV, "Jacobi SVD did not converge within its sweep bound");
     }
   // selection (Telum): sigma > cutoff*smax, stable descending sort, Nkeep
@@ -653,22 +677,24 @@ void run_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<i
     for (int i = 0; i < 2 * nout; ++i) out_re_im[i] = 0.0;
     return;
   }
-  if (!c->dot_counter) {
-    BUG_CUDA(cudaMalloc((void**)&c->dot_counter, sizeof(unsigned int)));
-    BUG_CUDA(cudaMemsetAsync(c->dot_counter, 0, sizeof(unsigned int), c->stream));
-  }
   double2* partial = static_cast<double2*>(c->scratch(descs.size() * sizeof(double2)));
-  double2* res = static_cast<double2*>(c->scratch(size_t(nout) * sizeof(double2)));
+  double* host = c->readback(size_t(2 * nout));  // the kernel writes the sums here (host-mapped)
+  double2* res = reinterpret_cast<double2*>(host);
   DotDesc* dd = c->push(descs);
   int* dseg = c->push(seg);
   double dbytes = 0.0;
   for (auto& d : descs) dbytes += bytes_per_elem * double(d.n);
-  c->begin();
-  bugk::launch_dot_fused(dd, int(descs.size()), partial, dseg, nout, res, c->dot_counter, c->stream);
-  c->launched(BUG_K_DOT, 0.0, dbytes);
-  double* host = c->readback(size_t(2 * nout));
-  BUG_CUDA(cudaMemcpyAsync(host, res, size_t(nout) * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
-  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  bugk::Stage st{};
+  st.kind = bugk::kStageDot;
+  st.n = int(descs.size());
+  st.total = nout;
+  st.a = dd;
+  st.b = dseg;
+  st.p = partial;
+  st.q = res;
+  st.counter = c->counter();
+  c->run_stage(st, BUG_K_DOT, 0.0, dbytes);
+  c->wait();
   std::memcpy(out_re_im, host, size_t(nout) * sizeof(double2));
 }
 
@@ -766,9 +792,13 @@ std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
     LinSrc* dsrc = c->push(srcs);
     double lbytes = 0.0;
     for (auto& o : outs) lbytes += 16.0 * double(o.n) * double(o.src_end - o.src_begin + 1);
-    c->begin();
-    bugk::launch_lincomb(dout, int(outs.size()), dsrc, total, c->stream);
-    c->launched(BUG_K_LINCOMB, 0.0, lbytes);
+    bugk::Stage st{};
+    st.kind = bugk::kStageLincomb;
+    st.n = int(outs.size());
+    st.total = total;
+    st.a = dout;
+    st.b = dsrc;
+    c->run_stage(st, BUG_K_LINCOMB, 0.0, lbytes);
   }
   return out;
 }
@@ -780,7 +810,7 @@ int guard(const std::function<void()>& f) {
   struct Flush {
     ~Flush() {
       if (bug_ctx* c = g_active_ctx) {
-        for (void* p : c->deferred) cudaFreeAsync(p, c->stream);
+        for (void* p : c->deferred) c->dev_free(p);
         c->deferred.clear();
       }
       g_active_ctx = nullptr;
@@ -840,9 +870,12 @@ TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& tt, int leg, const double
     }
     if (!descs.empty()) {
       ScaleDesc* dd = c->push(descs);
-      c->begin();
-      bugk::launch_scale(dd, int(descs.size()), total, c->stream);
-      c->launched(BUG_K_SCALE, 0.0, 32.0 * double(total));
+      bugk::Stage st{};
+      st.kind = bugk::kStageScale;
+      st.n = int(descs.size());
+      st.total = total;
+      st.a = dd;
+      c->run_stage(st, BUG_K_SCALE, 0.0, 32.0 * double(total));
     }
     result = std::move(o);
     return result;
@@ -1056,15 +1089,19 @@ int bug_ctx_destroy(bug_ctx* c) {
     }
     if (c->pinned_out) cudaFreeHost(c->pinned_out);
     if (c->arena) cudaFreeAsync(c->arena, c->stream);
-    if (c->dot_counter) cudaFree(c->dot_counter);
+    c->release_cached();
     cudaStreamSynchronize(c->stream);
+    if (c->dot_counter) cudaFree(c->dot_counter);
     cudaStreamDestroy(c->stream);
     delete c;
   });
 }
 
 int bug_ctx_synchronize(bug_ctx* c) {
-  return guard([&] { BUG_CUDA(cudaStreamSynchronize(c->stream)); });
+  return guard([&] {
+    require(c != nullptr, "null context");
+    BUG_CUDA(cudaStreamSynchronize(c->stream));
+  });
 }
 
 int64_t bug_ctx_launches(const bug_ctx* c) { return c ? c->launches : 0; }
@@ -1099,6 +1136,19 @@ int bug_ctx_reset_stats(bug_ctx* c) {
       c->k_launches[f] = 0;
       c->k_flops[f] = c->k_bytes[f] = c->k_ms[f] = 0.0;
     }
+    c->syncs = 0;
+    c->sync_wait_s = c->launch_s = c->alloc_s = 0.0;
+  });
+}
+
+int bug_ctx_host_stats(bug_ctx* c, int64_t* syncs, double* wait_s, double* launch_s,
+                       double* alloc_s) {
+  return guard([&] {
+    require(c && syncs && wait_s && launch_s && alloc_s, "bad argument");
+    *syncs = c->syncs;
+    *wait_s = c->sync_wait_s;
+    *launch_s = c->launch_s;
+    *alloc_s = c->alloc_s;
   });
 }
 int64_t bug_ctx_bytes_in_use(const bug_ctx* c) { return c ? c->bytes : 0; }

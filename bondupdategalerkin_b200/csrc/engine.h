@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -22,6 +23,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 using bugk::CopyDesc;
@@ -93,6 +95,7 @@ namespace bugi {
 // when the call returns).
 extern thread_local bug_ctx* g_active_ctx;
 
+
 struct Buffer {
   double2* ptr = nullptr;
   int64_t n = 0;
@@ -106,13 +109,14 @@ struct bug_tensor {
   int rank = 0;
   std::vector<bugi::Leg> legs;
   std::vector<bugi::Block> blocks;  // ascending keys, payload laid out in this order
-  std::map<bugi::Key, int> index;
   int64_t nelem = 0;
   std::shared_ptr<bugi::Buffer> buf;
 
+  // index of the block with key k (binary search over the sorted keys), or -1
   int find(const bugi::Key& k) const {
-    auto it = index.find(k);
-    return it == index.end() ? -1 : it->second;
+    auto it = std::lower_bound(blocks.begin(), blocks.end(), k,
+                               [](const bugi::Block& b, const bugi::Key& key) { return b.key < key; });
+    return (it != blocks.end() && it->key == k) ? int(it - blocks.begin()) : -1;
   }
   const double2* data(int b) const { return buf->ptr + blocks[b].off; }
   double2* mdata(int b) { return buf->ptr + blocks[b].off; }
@@ -129,6 +133,79 @@ struct bug_ctx {
   double k_bytes[BUG_K_NFAMILIES] = {};
   double k_ms[BUG_K_NFAMILIES] = {};
   bool profiling = false;
+  // host-side accounting: synchronisations the host waited on and the time spent waiting, time
+  // inside kernel-launch calls, and time inside the stream-ordered allocator
+  int64_t syncs = 0;
+  double sync_wait_s = 0.0, launch_s = 0.0, alloc_s = 0.0;
+  std::chrono::steady_clock::time_point launch_t0;
+  static double since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  // Wait for everything issued so far (the host is about to read a result).
+  void wait() {
+    const auto t0 = std::chrono::steady_clock::now();
+    BUG_CUDA(cudaStreamSynchronize(stream));
+    sync_wait_s += since(t0);
+    ++syncs;
+  }
+  // Device memory: a caching allocator over the stream-ordered pool. Every kernel of the context
+  // runs in order on its one stream, so a block released after its last enqueued use may be handed
+  // to any later enqueued operation at once; released blocks wait in per-size-class free lists
+  // (classes 1.25x apart) instead of going back through cudaFreeAsync/cudaMallocAsync.
+  static constexpr size_t kCacheCap = size_t(8) << 30;  // bytes parked in free lists at most
+  std::unordered_map<void*, size_t> live_;                // allocation -> its size class
+  std::unordered_map<size_t, std::vector<void*>> free_;   // size class -> released blocks
+  size_t cached_bytes = 0;
+  static size_t size_class(size_t b) {
+    if (b <= 256) return 256;
+    const int e = 63 - __builtin_clzll(b - 1);  // 2^e < b <= 2^(e+1)
+    const size_t step = (size_t(1) << e) / 4;
+    return ((b + step - 1) / step) * step;
+  }
+  void* dev_alloc(size_t bytes) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const size_t cls = size_class(bytes);
+    void* p = nullptr;
+    auto it = free_.find(cls);
+    if (it != free_.end() && !it->second.empty()) {
+      p = it->second.back();
+      it->second.pop_back();
+      cached_bytes -= cls;
+    } else {
+      cudaError_t e = cudaMallocAsync(&p, cls, stream);
+      if (e == cudaErrorMemoryAllocation) {  // give the parked blocks back and retry once
+        cudaGetLastError();
+        release_cached();
+        e = cudaMallocAsync(&p, cls, stream);
+      }
+      BUG_CUDA(e);
+    }
+    live_[p] = cls;
+    alloc_s += since(t0);
+    return p;
+  }
+  void dev_free(void* p) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto it = live_.find(p);
+    size_t cls = 0;
+    if (it != live_.end()) {
+      cls = it->second;
+      live_.erase(it);
+    }
+    if (cls > 0 && cached_bytes + cls <= kCacheCap) {
+      free_[cls].push_back(p);
+      cached_bytes += cls;
+    } else {
+      cudaFreeAsync(p, stream);
+    }
+    alloc_s += since(t0);
+  }
+  void release_cached() {
+    for (auto& kv : free_)
+      for (void* p : kv.second) cudaFreeAsync(p, stream);
+    free_.clear();
+    cached_bytes = 0;
+  }
   struct Pending {
     int fam;
     cudaEvent_t a, b;
@@ -158,12 +235,22 @@ struct bug_ctx {
     }
     pending.clear();
   }
-  void begin() {
-    commit();
+  // Called right before a launch: hands the launch its descriptors, inline in the kernel
+  // parameters when they fit, else committed to the arena by one copy.
+  bugk::Blob begin() {
+    bugk::Blob b{nullptr, 0, arena};
+    if (!batch.empty() && batch.size() <= bugk::kInlineMax) {
+      b.host = batch.data();
+      b.bytes = batch.size();
+    } else {
+      commit();
+    }
     if (profiling) {
       cur_start = take_event();
       BUG_CUDA(cudaEventRecord(cur_start, stream));
     }
+    launch_t0 = std::chrono::steady_clock::now();
+    return b;
   }
   // pinned staging ring for descriptor uploads
   static constexpr int kSlots = 32;
@@ -173,7 +260,10 @@ struct bug_ctx {
   bool stage_used[kSlots] = {};
   int stage_next = 0;
   std::vector<void*> deferred;  // device scratch to free after the next launch
-  double* pinned_out = nullptr;  // small pinned buffer for results read back by the host
+  // Small pinned buffer for results the host reads. Pinned memory from cudaHostAlloc is mapped into
+  // the device's address space under unified addressing, so kernels write results here directly
+  // and the host reads them after a stream synchronisation, with no copy in between.
+  double* pinned_out = nullptr;
   size_t pinned_out_cap = 0;
 
   void* stage(size_t bytes) {
@@ -198,7 +288,6 @@ struct bug_ctx {
   // in one pinned copy + one H2D transfer (commit, run by begin() right before the launch). The
   // arena is reused by every launch: the next transfer into it is stream-ordered after the kernel
   // that read it.
-  unsigned int* dot_counter = nullptr;  // last-block counter of the fused reduction
   char* arena = nullptr;
   size_t arena_cap = 0;
   std::vector<char> batch;
@@ -207,14 +296,13 @@ struct bug_ctx {
     const size_t bytes = (std::max<size_t>(v.size() * sizeof(T), 16) + 15) & ~size_t(15);
     if (!arena) {
       arena_cap = size_t(64) << 20;
-      BUG_CUDA(cudaMallocAsync((void**)&arena, arena_cap, stream));
+      BUG_CUDA(cudaMallocAsync((void**)&arena, arena_cap, stream));  // lives until destroy
     }
     const size_t off = batch.size();
     if (off + bytes > arena_cap) {  // a launch larger than the arena: its own buffer
       void* h = stage(bytes);
       if (!v.empty()) std::memcpy(h, v.data(), v.size() * sizeof(T));
-      void* dptr = nullptr;
-      BUG_CUDA(cudaMallocAsync(&dptr, bytes, stream));
+      void* dptr = dev_alloc(bytes);
       BUG_CUDA(cudaMemcpyAsync(dptr, h, bytes, cudaMemcpyHostToDevice, stream));
       stage_done();
       deferred.push_back(dptr);
@@ -233,14 +321,30 @@ struct bug_ctx {
     stage_done();
     batch.clear();
   }
+  // ── launching one operation ──
+  unsigned int* dot_counter = nullptr;  // last-CTA counter of the dot stage (zero between launches)
+  unsigned int* counter() {
+    if (!dot_counter) {
+      BUG_CUDA(cudaMalloc((void**)&dot_counter, sizeof(unsigned int)));
+      BUG_CUDA(cudaMemsetAsync(dot_counter, 0, sizeof(unsigned int), stream));
+    }
+    return dot_counter;
+  }
+  // Launch one stage whose descriptor arrays were pushed since the last launch, and account it.
+  void run_stage(const bugk::Stage& st, int fam, double flops, double bytes_moved) {
+    const bugk::Blob b = begin();
+    bugk::launch_stage(b, st, stream);
+    launched(fam, flops, bytes_moved);
+  }
   void* scratch(size_t bytes) {
-    void* dptr = nullptr;
-    BUG_CUDA(cudaMallocAsync(&dptr, std::max<size_t>(bytes, 16), stream));
+    void* dptr = dev_alloc(std::max<size_t>(bytes, 16));
     deferred.push_back(dptr);
     bugi::g_active_ctx = this;
     return dptr;
   }
   void launched(int fam, double flops, double bytes_moved) {
+    launch_s += since(launch_t0);
+    batch.clear();  // an inline launch has copied its descriptors into the launch
     ++launches;
     BUG_CUDA(cudaGetLastError());
     k_launches[fam] += 1;
@@ -255,7 +359,7 @@ struct bug_ctx {
     }
   }
   void flush() {
-    for (void* p : deferred) BUG_CUDA(cudaFreeAsync(p, stream));
+    for (void* p : deferred) dev_free(p);
     deferred.clear();
   }
   double* readback(size_t n) {

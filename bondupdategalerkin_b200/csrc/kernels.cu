@@ -1,14 +1,17 @@
-// Device kernels of the B200 block-sparse engine. See kernels.cuh for the role of each family.
+// Device kernels of the B200 block-sparse engine. See kernels.cuh for the role of each kernel.
 #include "kernels.cuh"
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 
 namespace bugk {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = kStageThreads;
 constexpr int kSmCount = 148;  // B200: 2 dies x 74 SMs
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -38,18 +41,36 @@ __device__ __forceinline__ int find_desc(const D* d, int nd, int64_t e) {
   return lo;
 }
 
-inline int grid_for(int64_t total) {
-  int64_t g = (total + kThreads - 1) / kThreads;
-  int64_t cap = int64_t(kSmCount) * 16;
-  if (g > cap) g = cap;
-  if (g < 1) g = 1;
-  return int(g);
-}
+// Tensor payloads are read through L2 only (ld.global.cg): a stage may read a block that an
+// earlier stage of the same launch wrote on another SM, and a block may be reused for a new tensor
+// within one launch, so no SM-local L1 copy may serve a later stage.
+__device__ __forceinline__ double2 ldg2(const double2* p) { return __ldcg(p); }
 
-// ── batched strided copy ──────────────────────────────────────────────────────────────────────
+// The descriptor bytes of an inline launch, passed by value in the kernel parameters.
+template <int N>
+struct ParamBlock {
+  alignas(16) unsigned char b[N];
+};
 
-__global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restrict__ d, int nd,
-                                                        int64_t total) {
+// Moves descriptor pointers formed against the arena onto the parameter block when the launch
+// carried its descriptors inline (nb > 0); any other pointer is returned unchanged.
+struct Rebase {
+  const unsigned char* base;
+  const char* arena;
+  int64_t nb;
+  template <class T>
+  __device__ __forceinline__ const T* operator()(const T* p) const {
+    const char* c = reinterpret_cast<const char*>(p);
+    if (nb > 0 && c >= arena && c < arena + nb) return reinterpret_cast<const T*>(base + (c - arena));
+    return p;
+  }
+};
+
+#define BUG_BLOB_PARAMS(N) const __grid_constant__ ParamBlock<N> pb, const char* arena, int64_t nb
+
+// ── copy stage: batched strided gather/scatter ───────────────────────────────────────────────
+
+__device__ void copy_stage(const Rebase& rb, const CopyDesc* d, int nd, int64_t total) {
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
        e += int64_t(gridDim.x) * blockDim.x) {
     const CopyDesc& c = d[find_desc(d, nd, e)];
@@ -63,16 +84,16 @@ __global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restri
       dof += i * c.dstr[k];
       if (k == c.wdim) widx = i;
     }
-    double2 v = c.src[so];
+    double2 v = c.src ? ldg2(c.src + so) : make_double2(0.0, 0.0);
     if (c.conj) v.y = -v.y;
     if (c.w) {
-      const double s = c.w[widx];
+      const double s = __ldcg(rb(c.w) + widx);
       v.x *= s;
       v.y *= s;
     }
     double2 w = cmul(c.alpha, v);
     if (c.accumulate) {
-      double2 o = c.dst[dof];
+      double2 o = ldg2(c.dst + dof);
       w.x += o.x;
       w.y += o.y;
     }
@@ -80,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) copy_kernel(const CopyDesc* __restri
   }
 }
 
-// ── segmented grouped complex GEMM ────────────────────────────────────────────────────────────
+// ── gemm stage: segmented grouped complex GEMM ───────────────────────────────────────────────
 // Tile 32x32 per CTA, K chunks of 16, 256 threads each owning a 2x2 patch. Every output block is
 // covered by its own tiles, and each tile sums over all block pairs of that output block.
 
@@ -98,12 +119,13 @@ __device__ __forceinline__ int64_t group_off(int idx, int n, const int* d, const
   return off;
 }
 
-__global__ void __launch_bounds__(kThreads)
-gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs,
-            const GemmTile* __restrict__ tiles) {
-  __shared__ double2 As[TM][TK + 1];
-  __shared__ double2 Bs[TK][TN + 1];
-  const GemmTile t = tiles[blockIdx.x];
+struct GemmSmem {
+  double2 As[TM][TK + 1];
+  double2 Bs[TK][TN + 1];
+};
+
+__device__ void gemm_tile(const GemmOut* outs, const GemmPair* pairs, const GemmTile& t,
+                          GemmSmem& sm) {
   const GemmOut o = outs[t.out];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int row0 = t.tm * TM, col0 = t.tn * TN;
@@ -124,9 +146,9 @@ gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs
         const int gm = row0 + mm, gk = k0 + kk;
         double2 v = make_double2(0.0, 0.0);
         if (gm < o.m && gk < K)
-          v = A.p[group_off(gm, A.nr, A.rd, A.rs) + group_off(gk, A.nc, A.cd, A.cs)];
+          v = ldg2(A.p + group_off(gm, A.nr, A.rd, A.rs) + group_off(gk, A.nc, A.cd, A.cs));
         if (A.conj) v.y = -v.y;
-        As[mm][kk] = v;
+        sm.As[mm][kk] = v;
       }
       for (int i = threadIdx.x; i < TK * TN; i += kThreads) {
         int kk, nn;
@@ -134,15 +156,15 @@ gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs
         const int gk = k0 + kk, gn = col0 + nn;
         double2 v = make_double2(0.0, 0.0);
         if (gk < K && gn < o.n)
-          v = B.p[group_off(gk, B.nr, B.rd, B.rs) + group_off(gn, B.nc, B.cd, B.cs)];
+          v = ldg2(B.p + group_off(gk, B.nr, B.rd, B.rs) + group_off(gn, B.nc, B.cd, B.cs));
         if (B.conj) v.y = -v.y;
-        Bs[kk][nn] = v;
+        sm.Bs[kk][nn] = v;
       }
       __syncthreads();
 #pragma unroll
       for (int kk = 0; kk < TK; ++kk) {
-        const double2 a0 = As[ty * 2][kk], a1 = As[ty * 2 + 1][kk];
-        const double2 b0 = Bs[kk][tx * 2], b1 = Bs[kk][tx * 2 + 1];
+        const double2 a0 = sm.As[ty * 2][kk], a1 = sm.As[ty * 2 + 1][kk];
+        const double2 b0 = sm.Bs[kk][tx * 2], b1 = sm.Bs[kk][tx * 2 + 1];
         cfma(acc[0][0], a0, b0);
         cfma(acc[0][1], a0, b1);
         cfma(acc[1][0], a1, b0);
@@ -160,6 +182,120 @@ gemm_kernel(const GemmOut* __restrict__ outs, const GemmPair* __restrict__ pairs
       const int gn = col0 + tx * 2 + j;
       if (gn < o.n) o.C[int64_t(gm) * o.n + gn] = acc[i][j];
     }
+  }
+}
+
+// ── dot stages: deterministic two-phase inner products ──────────────────────────────────────
+
+__device__ void dot_partial(const DotDesc& c, double2* out, double* sr, double* si) {
+  double re = 0.0, im = 0.0;
+  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
+    const double2 a = ldg2(c.a + i), b = ldg2(c.b + i);
+    re = fma(a.x, b.x, fma(a.y, b.y, re));
+    im = fma(a.x, b.y, fma(-a.y, b.x, im));
+  }
+  re = warp_sum(re);
+  im = warp_sum(im);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sr[warp] = re;
+    si[warp] = im;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0, ti = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      tr += sr[w];
+      ti += si[w];
+    }
+    *out = make_double2(tr, ti);
+  }
+  __syncthreads();
+}
+
+__device__ void dot_reduce(const int* seg, int nout, const double2* partial, double2* out) {
+  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
+    double tr = 0.0, ti = 0.0;
+    for (int k = seg[o]; k < seg[o + 1]; ++k) {
+      const double2 p = ldg2(partial + k);
+      tr += p.x;
+      ti += p.y;
+    }
+    out[o] = make_double2(tr, ti);
+  }
+}
+
+// ── lincomb and scale stages ────────────────────────────────────────────────────────────────
+
+__device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const LinOut& o = outs[find_desc(outs, nout, e)];
+    const int64_t i = e - o.prefix;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int s = o.src_begin; s < o.src_end; ++s) cfma(acc, srcs[s].coef, ldg2(srcs[s].src + i));
+    o.dst[i] = acc;
+  }
+}
+
+__device__ void scale_stage(const Rebase& rb, const ScaleDesc* d, int nd, int64_t total) {
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(gridDim.x) * blockDim.x) {
+    const ScaleDesc& c = d[find_desc(d, nd, e)];
+    const int64_t i = e - c.prefix;
+    const int coord = int((i / c.leg_stride) % c.leg_dim);
+    const double w = __ldcg(rb(c.w) + coord);
+    const double2 v = ldg2(c.src + i);
+    c.dst[i] = make_double2(v.x * w, v.y * w);
+  }
+}
+
+// ── the stage kernel ─────────────────────────────────────────────────────────────────────────
+
+// One launch = one stage. The dot stage reduces in the same launch: every CTA adds its partial
+// sums, and the last CTA to finish (counted on a per-context counter that it resets) sums each
+// output's partials in index order, so the result is deterministic.
+template <int N>
+__global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), const Stage st) {
+  __shared__ GemmSmem gsm;
+  __shared__ double sr[kThreads / 32], si[kThreads / 32];
+  __shared__ bool last;
+  const Rebase rb{pb.b, arena, nb};
+  switch (st.kind) {
+    case kStageCopy:
+      copy_stage(rb, rb(static_cast<const CopyDesc*>(st.a)), st.n, st.total);
+      break;
+    case kStageGemm: {
+      const GemmOut* outs = rb(static_cast<const GemmOut*>(st.a));
+      const GemmPair* pairs = rb(static_cast<const GemmPair*>(st.b));
+      const GemmTile* tiles = rb(static_cast<const GemmTile*>(st.c));
+      for (int t = blockIdx.x; t < st.n; t += gridDim.x) gemm_tile(outs, pairs, tiles[t], gsm);
+      break;
+    }
+    case kStageDot: {
+      const DotDesc* d = rb(static_cast<const DotDesc*>(st.a));
+      for (int i = blockIdx.x; i < st.n; i += gridDim.x) dot_partial(d[i], st.p + i, sr, si);
+      unsigned int* counter = st.counter;
+      if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+      }
+      __syncthreads();
+      if (!last) break;
+      __threadfence();
+      dot_reduce(rb(static_cast<const int*>(st.b)), int(st.total), st.p, st.q);
+      if (threadIdx.x == 0) *counter = 0u;
+      break;
+    }
+    case kStageLincomb:
+      lincomb_stage(rb(static_cast<const LinOut*>(st.a)), st.n,
+                    rb(static_cast<const LinSrc*>(st.b)), st.total);
+      break;
+    case kStageScale:
+      scale_stage(rb, rb(static_cast<const ScaleDesc*>(st.a)), st.n, st.total);
+      break;
+    default:
+      break;
   }
 }
 
@@ -183,9 +319,14 @@ __device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b
   }
 }
 
-__global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __restrict__ descs,
-                                                              const CopyDesc* __restrict__ packs,
+template <int N>
+__global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N),
+                                                              const SvdDesc* descs,
+                                                              const CopyDesc* packs,
                                                               double tol_scale) {
+  const Rebase rb{pb.b, arena, nb};
+  descs = rb(descs);
+  packs = rb(packs);
   extern __shared__ double2 dyn[];
   __shared__ double sig[kMaxR];
   __shared__ int perm[kMaxR];
@@ -277,7 +418,7 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __r
     converged = (rotated == 0);
     __syncthreads();
   }
-  if (tid == 0) *d.sweeps = converged ? sweep : -1;
+  if (tid == 0) *d.sweeps = converged ? sweep : -1;  // host-mapped
   // singular values
   for (int j = warp; j < r; j += nwarps) {
     const double2* aj = A + int64_t(j) * mm;
@@ -326,180 +467,113 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(const SvdDesc* __r
       double2 v = d.trans ? make_double2(aj[i].x * inv, aj[i].y * inv) : vj[i];
       vo[i] = cmul(v, ph);
     }
-    if (lane == 0) d.S[o] = sj;
-  }
-}
-
-// ── deterministic reductions, linear combinations, leg scaling ───────────────────────────────
-
-__global__ void __launch_bounds__(kThreads) dot_kernel(const DotDesc* __restrict__ d,
-                                                       double2* __restrict__ partial) {
-  __shared__ double sr[kThreads / 32], si[kThreads / 32];
-  const DotDesc c = d[blockIdx.x];
-  double re = 0.0, im = 0.0;
-  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
-    const double2 a = c.a[i], b = c.b[i];
-    re = fma(a.x, b.x, fma(a.y, b.y, re));
-    im = fma(a.x, b.y, fma(-a.y, b.x, im));
-  }
-  re = warp_sum(re);
-  im = warp_sum(im);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    sr[warp] = re;
-    si[warp] = im;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double tr = 0.0, ti = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) {
-      tr += sr[w];
-      ti += si[w];
+    if (lane == 0) {
+      d.S[o] = sj;
+      d.S_host[o] = sj;
     }
-    partial[blockIdx.x] = make_double2(tr, ti);
-  }
-}
-
-// One-launch reduction: every block writes its partial, and the last block to finish (counted on
-// a persistent counter that it resets) sums each output's partials in index order, so the result
-// is deterministic.
-__global__ void __launch_bounds__(kThreads) dot_fused_kernel(const DotDesc* __restrict__ d,
-                                                             double2* __restrict__ partial,
-                                                             const int* __restrict__ seg, int nout,
-                                                             double2* __restrict__ out,
-                                                             unsigned int* counter) {
-  __shared__ double sr[kThreads / 32], si[kThreads / 32];
-  __shared__ bool last;
-  const DotDesc c = d[blockIdx.x];
-  double re = 0.0, im = 0.0;
-  for (int64_t i = threadIdx.x; i < c.n; i += blockDim.x) {
-    const double2 a = c.a[i], b = c.b[i];
-    re = fma(a.x, b.x, fma(a.y, b.y, re));
-    im = fma(a.x, b.y, fma(-a.y, b.x, im));
-  }
-  re = warp_sum(re);
-  im = warp_sum(im);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-    sr[warp] = re;
-    si[warp] = im;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double tr = 0.0, ti = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) {
-      tr += sr[w];
-      ti += si[w];
-    }
-    partial[blockIdx.x] = make_double2(tr, ti);
-    __threadfence();
-    const unsigned int t = atomicAdd(counter, 1u);
-    last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
-    double tr = 0.0, ti = 0.0;
-    for (int k = seg[o]; k < seg[o + 1]; ++k) {
-      const double2 p = __ldcg(&partial[k]);
-      tr += p.x;
-      ti += p.y;
-    }
-    out[o] = make_double2(tr, ti);
-  }
-  if (threadIdx.x == 0) *counter = 0u;
-}
-
-__global__ void dot_reduce_kernel(const double2* __restrict__ partial,
-                                  const int* __restrict__ seg, int nout, double2* __restrict__ out) {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= nout) return;
-  double tr = 0.0, ti = 0.0;
-  for (int k = seg[o]; k < seg[o + 1]; ++k) {
-    tr += partial[k].x;
-    ti += partial[k].y;
-  }
-  out[o] = make_double2(tr, ti);
-}
-
-__global__ void __launch_bounds__(kThreads) lincomb_kernel(const LinOut* __restrict__ outs, int nout,
-                                                           const LinSrc* __restrict__ srcs,
-                                                           int64_t total) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
-    const LinOut& o = outs[find_desc(outs, nout, e)];
-    const int64_t i = e - o.prefix;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int s = o.src_begin; s < o.src_end; ++s) {
-      const double2 v = srcs[s].src[i];
-      cfma(acc, srcs[s].coef, v);
-    }
-    o.dst[i] = acc;
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) scale_kernel(const ScaleDesc* __restrict__ d, int nd,
-                                                         int64_t total) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
-    const ScaleDesc& c = d[find_desc(d, nd, e)];
-    const int64_t i = e - c.prefix;
-    const int coord = int((i / c.leg_stride) % c.leg_dim);
-    const double w = c.w[coord];
-    const double2 v = c.src[i];
-    c.dst[i] = make_double2(v.x * w, v.y * w);
   }
 }
 
 }  // namespace
 
-void launch_copy(const CopyDesc* d_desc, int ndesc, int64_t total, cudaStream_t s) {
-  if (ndesc <= 0 || total <= 0) return;
-  copy_kernel<<<grid_for(total), kThreads, 0, s>>>(d_desc, ndesc, total);
+// Launch KERNEL<N> with the smallest parameter block that holds the launch's descriptors, or the
+// arena form (N = 16, nothing inline) when the descriptors were copied to the device. LAUNCH is a
+// macro taking (kernel instantiation, parameter block, inline byte count).
+#define BUG_WITH_BLOB(BLOB, LAUNCH)                                                        \
+  do {                                                                                   \
+    const Blob& b_ = (BLOB);                                                             \
+    const int64_t nb_ = b_.host ? int64_t(b_.bytes) : 0;                                  \
+    if (nb_ == 0) {                                                                      \
+      ParamBlock<16> p_{};                                                               \
+      LAUNCH(16, p_, 0);                                                                 \
+    } else if (nb_ <= 512) {                                                             \
+      ParamBlock<512> p_;                                                                \
+      std::memcpy(p_.b, b_.host, size_t(nb_));                                           \
+      LAUNCH(512, p_, nb_);                                                              \
+    } else if (nb_ <= 2048) {                                                            \
+      ParamBlock<2048> p_;                                                               \
+      std::memcpy(p_.b, b_.host, size_t(nb_));                                           \
+      LAUNCH(2048, p_, nb_);                                                             \
+    } else if (nb_ <= 8192) {                                                            \
+      ParamBlock<8192> p_;                                                               \
+      std::memcpy(p_.b, b_.host, size_t(nb_));                                           \
+      LAUNCH(8192, p_, nb_);                                                             \
+    } else {                                                                             \
+      ParamBlock<int(kInlineMax)> p_;                                                    \
+      std::memcpy(p_.b, b_.host, size_t(nb_));                                           \
+      LAUNCH(int(kInlineMax), p_, nb_);                                                  \
+    }                                                                                    \
+  } while (0)
+
+int stage_items(const Stage& s) {
+  switch (s.kind) {
+    case kStageCopy:
+    case kStageLincomb:
+    case kStageScale: {
+      const int64_t g = (s.total + kThreads - 1) / kThreads;
+      return int(std::min<int64_t>(std::max<int64_t>(g, 1), int64_t(kSmCount) * 16));
+    }
+    case kStageGemm:
+    case kStageDot:
+      return std::max(s.n, 1);
+    default:
+      return 1;
+  }
 }
 
-void launch_gemm(const GemmOut* outs, const GemmPair* pairs, const GemmTile* tiles, int ntiles,
-                 cudaStream_t s) {
-  if (ntiles <= 0) return;
-  gemm_kernel<<<ntiles, kThreads, 0, s>>>(outs, pairs, tiles);
+int stage_grid_limit() {
+  static int limit[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (limit[dev] == 0) {
+    int per_sm = 0, sms = kSmCount;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<int(kInlineMax)>, kThreads, 0);
+    limit[dev] = std::max(1, per_sm) * std::max(1, sms);
+  }
+  return limit[dev];
 }
 
-void launch_svd(const SvdDesc* d_desc, int nprob, const CopyDesc* packs, int max_smem_bytes,
-                cudaStream_t s) {
+void launch_stage(const Blob& b, const Stage& st, cudaStream_t s) {
+  const int grid = std::min(stage_items(st), stage_grid_limit());
+#define BUG_STAGE_LAUNCH(NB, P, NBYTES) \
+  stage_kernel<NB><<<grid, kThreads, 0, s>>>(P, b.arena, (NBYTES), st)
+  BUG_WITH_BLOB(b, BUG_STAGE_LAUNCH);
+#undef BUG_STAGE_LAUNCH
+}
+
+namespace {
+// Opt the SVD kernel's instantiations into large dynamic shared memory once per device.
+template <int N>
+void svd_smem_optin(int bytes) {
+  static int granted[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (bytes > granted[dev]) {
+    cudaFuncSetAttribute(jacobi_svd_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    granted[dev] = bytes;
+  }
+}
+}  // namespace
+
+void launch_svd(const Blob& b, const SvdDesc* d_desc, int nprob, const CopyDesc* packs,
+                int max_smem_bytes, cudaStream_t s) {
   if (nprob <= 0) return;
-  if (max_smem_bytes > 0)
-    cudaFuncSetAttribute(jacobi_svd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         max_smem_bytes);
-  jacobi_svd_kernel<<<nprob, kThreads, max_smem_bytes, s>>>(d_desc, packs, 2.220446049250313e-16);
-}
-
-void launch_dot(const DotDesc* d_desc, int ndesc, double2* partial, cudaStream_t s) {
-  if (ndesc <= 0) return;
-  dot_kernel<<<ndesc, kThreads, 0, s>>>(d_desc, partial);
-}
-
-void launch_dot_fused(const DotDesc* d_desc, int ndesc, double2* partial, const int* seg, int nout,
-                      double2* out, unsigned int* counter, cudaStream_t s) {
-  if (ndesc <= 0) return;
-  dot_fused_kernel<<<ndesc, kThreads, 0, s>>>(d_desc, partial, seg, nout, out, counter);
-}
-
-void launch_dot_reduce(const double2* partial, const int* seg_begin, int nout, double2* out,
-                       cudaStream_t s) {
-  if (nout <= 0) return;
-  dot_reduce_kernel<<<(nout + 127) / 128, 128, 0, s>>>(partial, seg_begin, nout, out);
-}
-
-void launch_lincomb(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,
-                    cudaStream_t s) {
-  if (nout <= 0 || total <= 0) return;
-  lincomb_kernel<<<grid_for(total), kThreads, 0, s>>>(outs, nout, srcs, total);
-}
-
-void launch_scale(const ScaleDesc* d_desc, int ndesc, int64_t total, cudaStream_t s) {
-  if (ndesc <= 0 || total <= 0) return;
-  scale_kernel<<<grid_for(total), kThreads, 0, s>>>(d_desc, ndesc, total);
+  if (max_smem_bytes > 0) {
+    const int64_t nb = b.host ? int64_t(b.bytes) : 0;
+    if (nb == 0) svd_smem_optin<16>(max_smem_bytes);
+    else if (nb <= 512) svd_smem_optin<512>(max_smem_bytes);
+    else if (nb <= 2048) svd_smem_optin<2048>(max_smem_bytes);
+    else if (nb <= 8192) svd_smem_optin<8192>(max_smem_bytes);
+    else svd_smem_optin<int(kInlineMax)>(max_smem_bytes);
+  }
+#define BUG_SVD_LAUNCH(NB, P, NBYTES)                                                           \
+  jacobi_svd_kernel<NB><<<nprob, kThreads, max_smem_bytes, s>>>(P, b.arena, (NBYTES), d_desc,  \
+                                                                 packs, 2.220446049250313e-16)
+  BUG_WITH_BLOB(b, BUG_SVD_LAUNCH);
+#undef BUG_SVD_LAUNCH
 }
 
 }  // namespace bugk

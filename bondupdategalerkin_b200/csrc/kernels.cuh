@@ -1,17 +1,22 @@
 // Device kernels of the B200 block-sparse engine (sm_100a, complex FP64).
 //
-// Four kernel families carry every block-sparse operation of the BUG step:
-//   * copy_kernel      -- batched strided gather/scatter (permutations, sector packing, direct
-//                         sums, trims, conjugation, scaling): the reference's HPTT transposes
-//                         (deps/Telum/src/contract.jl:27-167) folded into one launch per operation;
-//   * gemm_kernel      -- segmented grouped complex GEMM: every output block is owned by one CTA
-//                         tile that loops over all its contributing block pairs, so accumulation
-//                         is deterministic and needs no atomics (contract.jl:952-1005);
-//   * jacobi_svd_kernel-- batched one-sided (Hestenes) Jacobi SVD, one CTA per charge sector,
-//                         sorted, with the engine's phase convention (replaces gesdd,
-//                         deps/Telum/src/utils.jl:93-105);
-//   * dot/lincomb/scale kernels -- deterministic two-phase reductions and block-union linear
-//                         combinations (tensor_inner, norm, Telum's lazy +/-).
+// Two kernels carry every block-sparse operation of the BUG step.
+//
+// stage_kernel runs one operation per launch; its stage kind selects the body:
+//   * copy     -- batched strided gather/scatter (permutations, sector packing, direct sums, trims,
+//                 conjugation, scaling, zero fills): the reference's HPTT transposes
+//                 (deps/Telum/src/contract.jl:27-167) as one launch per operation;
+//   * gemm     -- segmented grouped complex GEMM: every output block is owned by tiles that loop
+//                 over all its contributing block pairs, so accumulation is deterministic and needs
+//                 no atomics (contract.jl:952-1005);
+//   * dot      -- deterministic inner products (tensor_inner, norm): partial sums per descriptor,
+//                 and the last CTA sums each output's partials in index order into host-mapped
+//                 memory;
+//   * lincomb, scale -- linear combinations over a union of blocks (Telum's lazy +/-), leg scaling.
+// The descriptors of a launch travel inside its kernel parameters when they fit (see Blob).
+//
+// jacobi_svd_kernel is the batched one-sided (Hestenes) Jacobi SVD, one CTA per charge sector,
+// sorted, with the engine's phase convention (replaces gesdd, deps/Telum/src/utils.jl:93-105).
 #pragma once
 
 #include <cuComplex.h>
@@ -27,7 +32,7 @@ struct CopyDesc {
   int64_t n;        // elements of this descriptor
   int64_t prefix;   // exclusive prefix sum of n over the launch
   int ndim;
-  int conj;         // conjugate the source value
+  int conj;         // conjugate the source value (a null src reads zeros: a fill)
   int accumulate;   // dst += alpha*v instead of dst = alpha*v
   int pad_;
   double2 alpha;
@@ -76,7 +81,8 @@ struct SvdDesc {
   double2* U;       // m x r column-major output (left vectors of M)
   double2* V;       // n x r column-major output (right vectors of M): M = U diag(S) V^H
   double* S;        // r singular values, descending
-  int* sweeps;      // sweeps used (or -1 if the bound was hit)
+  double* S_host;   // the same values written to host-mapped pinned memory (read after the sync)
+  int* sweeps;      // sweeps used (or -1 if the bound was hit), host-mapped pinned memory
   int m, n;         // shape of M
   int trans;        // 1: work holds M^H (m < n)
   int use_smem;     // 1: the CTA copies work/vwork into shared memory
@@ -114,18 +120,46 @@ struct ScaleDesc {
   const double* w;
 };
 
-void launch_copy(const CopyDesc* d_desc, int ndesc, int64_t total, cudaStream_t s);
-void launch_gemm(const GemmOut* outs, const GemmPair* pairs, const GemmTile* tiles, int ntiles,
-                 cudaStream_t s);
-void launch_svd(const SvdDesc* d_desc, int nprob, const CopyDesc* packs, int max_smem_bytes,
-                cudaStream_t s);
-void launch_dot(const DotDesc* d_desc, int ndesc, double2* partial, cudaStream_t s);
-void launch_dot_fused(const DotDesc* d_desc, int ndesc, double2* partial, const int* seg, int nout,
-                      double2* out, unsigned int* counter, cudaStream_t s);
-void launch_dot_reduce(const double2* partial, const int* seg_begin, int nout, double2* out,
-                       cudaStream_t s);
-void launch_lincomb(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,
-                    cudaStream_t s);
-void launch_scale(const ScaleDesc* d_desc, int ndesc, int64_t total, cudaStream_t s);
+// Where one launch finds its descriptor arrays. The engine forms every descriptor pointer against
+// the context's device arena. A launch whose arrays total at most kInlineMax bytes carries them
+// inside its kernel parameters (`host` set): no copy precedes the kernel, which rebases pointers
+// that fall in [arena, arena + bytes) onto its parameter block. A larger launch reads them from
+// the arena, filled by one host-to-device copy before the kernel (`host` null).
+struct Blob {
+  const void* host;
+  size_t bytes;
+  const char* arena;
+};
+constexpr size_t kInlineMax = 32000;  // kernel parameters are limited to 32764 bytes
+
+enum StageKind {
+  kStageCopy = 0,     // a: CopyDesc[n], total elements
+  kStageGemm = 1,     // a: GemmOut[], b: GemmPair[], c: GemmTile[n]
+  kStageDot = 2,      // a: DotDesc[n], b: int seg[total + 1]; p: n partials (scratch);
+                      // q[o] = sum of p[seg[o] .. seg[o+1]) in index order (host-mapped)
+  kStageLincomb = 4,  // a: LinOut[n], b: LinSrc[], total elements
+  kStageScale = 5,    // a: ScaleDesc[n], total elements
+};
+
+struct Stage {
+  int kind;
+  int n;
+  int64_t total;
+  const void* a;
+  const void* b;
+  const void* c;
+  double2* p;
+  double2* q;
+  unsigned int* counter;  // dot: the context's last-CTA counter (zero between launches)
+};
+
+constexpr int kStageThreads = 256;
+
+// Work items of one stage: its CTA count (capped at the co-resident limit; loops stride).
+int stage_items(const Stage& s);
+int stage_grid_limit();
+void launch_stage(const Blob& b, const Stage& st, cudaStream_t s);
+void launch_svd(const Blob& b, const SvdDesc* d_desc, int nprob, const CopyDesc* packs,
+                int max_smem_bytes, cudaStream_t s);
 
 }  // namespace bugk

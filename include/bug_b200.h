@@ -78,6 +78,12 @@ int bug_ctx_set_profiling(bug_ctx* ctx, int on);
 int bug_ctx_kernel_stats(bug_ctx* ctx, int family, int64_t* launches, double* flops, double* bytes,
                          double* device_ms);
 int bug_ctx_reset_stats(bug_ctx* ctx);
+/* Host-side accounting since the last reset: how many times the host waited for the stream to
+ * read a result back (norms, inner products, singular values), the seconds spent waiting, the
+ * seconds spent inside kernel-launch calls, and the seconds spent in the stream-ordered
+ * allocator. No reference counterpart (the reference runs on the CPU and waits for nothing). */
+int bug_ctx_host_stats(bug_ctx* ctx, int64_t* syncs, double* wait_s, double* launch_s,
+                       double* alloc_s);
 
 /* ── tensors: create / upload / download / inspect ────────────────────────────────────────── */
 /* A zero tensor with the given legs and block keys (TLArray construction,

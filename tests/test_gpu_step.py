@@ -121,3 +121,31 @@ def test_two_spin(dev, native):
     v /= np.linalg.norm(v)
     assert abs(abs(v[1]) - np.cos(t / 2)) < 1e-10
     assert abs(abs(v[2]) - np.sin(t / 2)) < 1e-10
+
+
+def test_profiled_step_identical(dev):
+    """Profiling launches every operation on its own; the fused stage lists of the normal run must
+    give bit-identical states (same arithmetic, same order)."""
+    DM, _ = dev
+    from bondupdategalerkin_b200 import _engine as E
+    from bondupdategalerkin_b200 import native as DN
+    from bondupdategalerkin_b200 import tensor as DT
+
+    ctx = E.context()
+    states = []
+    for profile in (False, True):
+        psi = DM.domain_wall_state(16)
+        mpo = DM.xxz_mpo(16, J=1.0, delta=0.5)
+        rng = np.random.default_rng(99)
+        ctx.set_profiling(profile)
+        try:
+            for _ in range(6):
+                DN.cbe_bug_step(psi, mpo, -0.05j, order=2, rng=rng, tol_basis=1e-4, maxdim=64)
+        finally:
+            ctx.set_profiling(False)
+        states.append([DT.to_blocks(t) for t in psi.tensors])
+    for (la, ba), (lb, bb) in zip(*states):
+        assert [(l.dir, l.sectors) for l in la] == [(l.dir, l.sectors) for l in lb]
+        assert ba.keys() == bb.keys()
+        for k in ba:
+            assert np.array_equal(ba[k], bb[k]), k
