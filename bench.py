@@ -35,16 +35,71 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(L=64, J=1.0, delta=0.5, tau=-0.05j, order=2, tol_basis=1e-4, maxdim=256,
                 bond_ceiling_factor=1.2, seed=1234)
 WORKLOAD_NAME = "xxz_quench_L64_delta0.5_domainwall_maxdim256_order2_tol1e-4"
+# The Heston PDE on a quantics grid: 10 + 10 bits (x in [-1, 1], v in [0, 0.5], end points on the
+# grid), r 0.03, q 0.01, kappa 2, theta 0.09, sigma 0.4, rho -0.7, start exp(0.5 x) exp(-v),
+# tau = 0.02 (real), Arnoldi (non-Hermitian), maxdim 64, order 1, 50 steps.
+HESTON = dict(nbits=10, params=(0.03, 0.01, 2.0, 0.09, 0.4, -0.7), tau=0.02, maxdim=64, seed=1234)
+HESTON_NAME = "heston_qtt_10x10bits_maxdim64_tau0.02_arnoldi"
+KIND = ["xxz"]
 L2_FLUSH_BYTES = 256 << 20
+_HESTON_DOMAIN = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
+
+
+def tau():
+    return HESTON["tau"] if KIND[0] == "heston" else WORKLOAD["tau"]
+
+
+def seed():
+    return HESTON["seed"] if KIND[0] == "heston" else WORKLOAD["seed"]
 
 
 def step_kwargs():
+    if KIND[0] == "heston":
+        return dict(maxdim=HESTON["maxdim"], hermitian=False)
     w = WORKLOAD
     return dict(order=w["order"], tol_basis=w["tol_basis"], maxdim=w["maxdim"],
                 bond_ceiling_factor=w["bond_ceiling_factor"])
 
 
+def device_inputs():
+    """(state, MPO) of the workload, built by the product's host builders and uploaded."""
+    if KIND[0] == "heston":
+        from bondupdategalerkin_b200 import qtt as P
+
+        g = P.qtt_grid(HESTON["nbits"], HESTON["nbits"], **_HESTON_DOMAIN)
+        psi = P.qtt_mps(P.qtt_separable(g, lambda x: np.exp(0.5 * x), lambda v: np.exp(-v)))
+        return psi, P.heston_mpo(g, P.HestonParams(*HESTON["params"]))
+    from bondupdategalerkin_b200 import models as DM
+
+    w = WORKLOAD
+    return DM.domain_wall_state(w["L"]), DM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
+
+
+def oracle_inputs():
+    """(state, MPO) of the workload in the CPU oracle."""
+    if KIND[0] == "heston":
+        from oracle import qtt as Q
+
+        g = Q.qtt_grid(HESTON["nbits"], HESTON["nbits"], **_HESTON_DOMAIN)
+        psi = Q.qtt_mps(Q.qtt_separable(g, lambda x: np.exp(0.5 * x), lambda v: np.exp(-v)))
+        return psi, Q.heston_mpo(g, Q.HestonParams(*HESTON["params"]))
+    from oracle import models as OM
+
+    w = WORKLOAD
+    return OM.domain_wall_state(w["L"]), OM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
+
+
 def config_dict(args, ws, max_bond=None):
+    if KIND[0] == "heston":
+        h = HESTON
+        cfg = {"workload": HESTON_NAME, "L": 2 * h["nbits"], "grid": "1024 x 1024", "tau": "0.02",
+               "order": 1, "maxdim": h["maxdim"], "hermitian": False,
+               "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+               "l2": "flushed before every step (256 MiB write)",
+               "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+        if max_bond is not None:
+            cfg["max_bond_dim_after"] = max_bond
+        return cfg
     w = WORKLOAD
     cfg = {"workload": WORKLOAD_NAME, "L": w["L"], "delta": w["delta"], "tau": "-0.05i",
            "order": w["order"], "tol_basis": w["tol_basis"], "maxdim": w["maxdim"],
@@ -149,18 +204,15 @@ def blas_threads():
 def oracle_steps(warmup, k):
     """Run the CPU oracle over the same trajectory: ``warmup`` untimed steps, then ``k`` timed.
     Returns (seconds for the k steps, bond dims after)."""
-    from oracle import models as OM
     from oracle import step as OS
 
-    w = WORKLOAD
-    psi = OM.domain_wall_state(w["L"])
-    mpo = OM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
-    rng = np.random.default_rng(w["seed"])
+    psi, mpo = oracle_inputs()
+    rng = np.random.default_rng(seed())
     for _ in range(warmup):
-        OS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
     t0 = time.perf_counter()
     for _ in range(k):
-        OS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
     return time.perf_counter() - t0, psi.bond_dims()
 
 
@@ -172,8 +224,7 @@ def oracle_sampled_steps(snaps, mpo_host=None):
     from oracle import step as OS
     from bondupdategalerkin_b200 import tensor as DT
 
-    w = WORKLOAD
-    mpo = mpo_host or OM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
+    mpo = mpo_host or oracle_inputs()[1]
     secs, which = 0.0, []
     for step_no, psi_d, rng_state in snaps:
         tensors = []
@@ -184,7 +235,7 @@ def oracle_sampled_steps(snaps, mpo_host=None):
         rng = np.random.default_rng()
         rng.bit_generator.state = rng_state
         t0 = time.perf_counter()
-        OS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
         secs += time.perf_counter() - t0
         which.append(step_no)
     return secs, which
@@ -233,7 +284,6 @@ def run_engine(args):
     if Bld.needs_build():
         Bld.build()
     E.set_default_device(local)
-    from bondupdategalerkin_b200 import models as DM
     from bondupdategalerkin_b200 import tensor as DT
 
     if args.host == "python":
@@ -244,12 +294,10 @@ def run_engine(args):
     ctx = E.context(local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    w = WORKLOAD
-    psi = DM.domain_wall_state(w["L"])
-    mpo = DM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
-    rng = np.random.default_rng(w["seed"])
+    psi, mpo = device_inputs()
+    rng = np.random.default_rng(seed())
     for _ in range(args.warmup):
-        DS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        DS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
     start_psi = psi.copy()
     start_rng = rng.bit_generator.state
 
@@ -278,7 +326,7 @@ def run_engine(args):
             flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        DS.cbe_bug_step(psi, mpo, w["tau"], rng=rng, **step_kwargs())
+        DS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
         e1.record(stream)
         evs.append((e0, e1))
     ctx.synchronize()
@@ -320,7 +368,7 @@ def run_engine(args):
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
-        DS.cbe_bug_step(psi_r, mpo, w["tau"], rng=rng_r, **step_kwargs())
+        DS.cbe_bug_step(psi_r, mpo, tau(), rng=rng_r, **step_kwargs())
     ctx.synchronize()
     stats = ctx.kernel_stats()
     ctx.set_profiling(False)
@@ -340,7 +388,7 @@ def run_engine(args):
             flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        host_state, center, io = step_host(host_state, center, host_mpo, w["tau"], rng=rng_e,
+        host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
                                            native=args.host == "native", **step_kwargs())
         e1.record(stream)
         ctx.synchronize()
@@ -419,7 +467,13 @@ def main():
                     help="time the steps only (for profiler runs)")
     ap.add_argument("--L", type=int, default=None,
                     help="chain length override (smaller cases for profiler captures only)")
+    ap.add_argument("--workload", default="xxz", choices=["xxz", "heston"],
+                    help="xxz: the L = 64 XXZ quench (the headline); heston: the 10 + 10-bit "
+                         "Heston QTT field (47 timed steps after 3 warm-up make its 50)")
     args = ap.parse_args()
+    KIND[0] = args.workload
+    if args.workload == "heston" and "--steps" not in sys.argv:
+        args.steps = 47
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.L is not None:

@@ -57,6 +57,8 @@ SIGNATURES = {
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
     "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
+    "bug_la_kry_weight": (ctypes.c_int, [ctypes.c_int, _c_double_p, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, _c_double_p]),
     "bug_la_eigvals_hess": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
     "bug_inner_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, _vp]),
 }

@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "kernels.cu", "step.cu", "noalloc.cu")]
 OUTPUT = os.path.join(HERE, "libbug_b200.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+              "-Xcompiler", "-fcx-limited-range",
               "-Xcompiler", "-fPIC", "-shared"]
 
 

@@ -1,0 +1,335 @@
+"""Quantics (QTT) inputs on device: grids, separable fields and the Heston generator.
+
+Host-side builders of the ``:none``-symmetry workloads (the Heston PDE on a quantics grid). Cores
+are formed with numpy once, on the host, and uploaded; the BUG step then runs on device. Follows
+the reference's conventions:
+
+* ``qtt_grid`` (``src/QTTS/Tooling/grid.jl:152-168``), the default GROUPED ordering with the least
+  significant bit first (``grid.jl:1-12``): site ``k + 1`` holds bit ``k`` of the x index and site
+  ``nx + k + 1`` bit ``k`` of the y index;
+* fields: ``tt_from_samples`` (TT-SVD with the ``_qtt_rank`` rule, ``src/QTTS/Tooling/
+  cores.jl:18-28,52-90``) and ``qtt_separable`` (``cores.jl:265-270``); ``qtt_mps``
+  (``src/QTTS/Tooling/state_adapter.jl:72-82``);
+* operators: cores ``(w_l, out, in, w_r)``; the shift ``(S psi)_i = psi_{i+1}`` as a binary carry
+  automaton with the carry on the bond (``src/QTTS/Tooling/derivatives.jl:21-36``), central
+  differences as sums of shifts, the ``:onesided`` boundary rows as rank-1 corrections
+  (``derivatives.jl:40-83``), coordinate diagonals of rank 2, products and sums of chains and
+  their compression (``src/QTTS/Tooling/mpo_algebra.jl``, ``cores.jl:92-128``);
+* ``heston_op`` / ``heston_mpo`` (``src/QTTS/Models/Heston/heston.jl:36-69``) and ``qtt_to_mpo``
+  (``state_adapter.jl:96-109``): the solver MPO stores ``(w_l, in, out, w_r)``.
+
+Nothing here forms an object of size ``2^n``: every operator is assembled core by core.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .models import MPO, MPS
+from .tensor import Leg, from_blocks
+
+
+@dataclass(frozen=True)
+class Grid:
+    nx: int
+    ny: int
+    x0: float
+    dx: float
+    y0: float
+    dy: float
+    periodic_x: bool
+    periodic_y: bool
+
+    @property
+    def length(self) -> int:
+        return self.nx + self.ny
+
+
+def qtt_grid(nx, ny, x=(-1.0, 1.0), y=(-1.0, 1.0), periodic_x=True, periodic_y=True) -> Grid:
+    """The grid on ``x[0] <= x < x[1]`` (periodic) or ``x[0] <= x <= x[1]`` (end points on the
+    grid), likewise in y."""
+    if nx < 1 or ny < 1:
+        raise ValueError("qtt_grid needs at least one bit per coordinate")
+    if not (x[1] > x[0] and y[1] > y[0]):
+        raise ValueError(f"empty domain {x} x {y}")
+    dx = (x[1] - x[0]) / (2 ** nx if periodic_x else 2 ** nx - 1)
+    dy = (y[1] - y[0]) / (2 ** ny if periodic_y else 2 ** ny - 1)
+    return Grid(nx, ny, float(x[0]), dx, float(y[0]), dy, periodic_x, periodic_y)
+
+
+def coords(g: Grid):
+    return g.x0 + g.dx * np.arange(2 ** g.nx), g.y0 + g.dy * np.arange(2 ** g.ny)
+
+
+@dataclass(frozen=True)
+class HestonParams:
+    """Rate, dividend yield, mean reversion, long-run variance, vol of vol, correlation."""
+
+    r: float
+    q: float
+    kappa: float
+    theta: float
+    sigma: float
+    rho: float
+
+    def feller(self) -> bool:
+        return 2 * self.kappa * self.theta >= self.sigma ** 2
+
+
+# ── fields ──────────────────────────────────────────────────────────────────────────────────
+
+def _tail_rank(S, delta):
+    r = len(S)
+    tail = 0.0
+    while r > 1 and tail + S[r - 1] ** 2 <= delta ** 2:
+        tail += S[r - 1] ** 2
+        r -= 1
+    return r
+
+
+def tt_from_samples(vals, tol=1e-14):
+    """1D quantics TT of ``vals[i] = f(x_i)``: cores ``(chi_l, 2, chi_r)``, bit 0 first."""
+    vals = np.asarray(vals, dtype=np.complex128)
+    n = int(round(np.log2(len(vals))))
+    if 2 ** n != len(vals):
+        raise ValueError(f"need 2^n samples, got {len(vals)}")
+    # row index = bit 0, the remaining bits along the columns
+    M = vals.reshape((2,) * n, order="F").reshape(2, -1)
+    delta = tol * np.linalg.norm(vals) / np.sqrt(max(n - 1, 1))
+    cores, chi = [], 1
+    for _ in range(n - 1):
+        M = M.reshape(chi * 2, -1)
+        U, S, Vh = np.linalg.svd(M, full_matrices=False)
+        r = _tail_rank(S, delta)
+        cores.append(U[:, :r].reshape(chi, 2, r))
+        M = S[:r, None] * Vh[:r]
+        chi = r
+    cores.append(M.reshape(chi, 2, 1))
+    return cores
+
+
+def qtt_separable(g: Grid, fx, fy, tol=1e-14):
+    """``fx(x) fy(y)``: two 1D TTs placed on the grouped ordering (x sites, then y sites)."""
+    xs, ys = coords(g)
+    return tt_from_samples([fx(x) for x in xs], tol) + tt_from_samples([fy(y) for y in ys], tol)
+
+
+def qtt_mps(cores, center=1) -> MPS:
+    """The device state of TT ``cores``: one dense block per site, uploaded, then gauged to site 1
+    and on to ``center`` by exact SVD moves on device."""
+    from .step import canonical
+
+    ts = []
+    for c in cores:
+        c = np.asarray(c, dtype=np.complex128)
+        legs = [Leg(-1, {0: c.shape[0]}), Leg(-1, {0: 2}), Leg(+1, {0: c.shape[2]})]
+        ts.append(from_blocks(legs, {(0, 0, 0): c}))
+    psi = MPS(ts, len(ts))
+    canonical(psi, 1)
+    canonical(psi, center)
+    return psi
+
+
+# ── operator chains: cores (w_l, out, in, w_r) ───────────────────────────────────────────────
+
+def op_identity(n):
+    return [np.eye(2, dtype=np.complex128).reshape(1, 2, 2, 1) for _ in range(n)]
+
+
+def op_shift(n, periodic=False):
+    """``(S psi)_i = psi_{i+1}``: bit k of the input is bit k of the output plus the carry from
+    bit k-1; the +1 enters at bit 0 and the carry out of the top bit wraps (periodic) or is lost."""
+    core = np.zeros((2, 2, 2, 2), dtype=np.complex128)  # [carry_in, out, in, carry_out]
+    for cin in range(2):
+        for o in range(2):
+            s = o + cin
+            core[cin, o, s % 2, s // 2] = 1.0
+    cores = [core.copy() for _ in range(n)]
+    cores[0] = cores[0][1:2]
+    cores[-1] = cores[-1].sum(axis=3, keepdims=True) if periodic else cores[-1][:, :, :, 0:1]
+    return cores
+
+
+def op_transpose(ch):
+    return [c.transpose(0, 2, 1, 3).copy() for c in ch]
+
+
+def op_scale(ch, a):
+    out = [c.copy() for c in ch]
+    out[0] = out[0] * a
+    return out
+
+
+def op_sum(chains):
+    """Direct sum: block-diagonal inner cores, boundary cores concatenated along the bond."""
+    L = len(chains[0])
+    out = []
+    for s in range(L):
+        parts = [ch[s] for ch in chains]
+        wl = 1 if s == 0 else sum(p.shape[0] for p in parts)
+        wr = 1 if s == L - 1 else sum(p.shape[3] for p in parts)
+        c = np.zeros((wl, 2, 2, wr), dtype=np.complex128)
+        ol = orr = 0
+        for p in parts:
+            a, b = p.shape[0], p.shape[3]
+            li = slice(0, 1) if s == 0 else slice(ol, ol + a)
+            ri = slice(0, 1) if s == L - 1 else slice(orr, orr + b)
+            c[li, :, :, ri] += p
+            if s != 0:
+                ol += a
+            if s != L - 1:
+                orr += b
+        out.append(c)
+    return out
+
+
+def op_compress(ch, tol=1e-14):
+    """Left QR sweep, right-to-left SVD sweep keeping each bond's smallest rank whose tail fits
+    ``tol * |chain| / sqrt(L - 1)`` (cores read as d = 4)."""
+    C = [c.reshape(c.shape[0], 4, c.shape[3]).astype(np.complex128) for c in ch]
+    L = len(C)
+    if L == 1:
+        return [c.reshape(c.shape[0], 2, 2, c.shape[2]) for c in C]
+    for k in range(L - 1):
+        chi, d, r = C[k].shape
+        Q, R = np.linalg.qr(C[k].reshape(chi * d, r))
+        C[k] = Q.reshape(chi, d, Q.shape[1])
+        C[k + 1] = np.tensordot(R, C[k + 1], axes=(1, 0))
+    delta = tol * np.linalg.norm(C[-1]) / np.sqrt(L - 1)
+    for k in range(L - 1, 0, -1):
+        chi, d, r = C[k].shape
+        U, S, Vh = np.linalg.svd(C[k].reshape(chi, d * r), full_matrices=False)
+        rr = _tail_rank(S, delta)
+        C[k] = Vh[:rr].reshape(rr, d, r)
+        C[k - 1] = np.tensordot(C[k - 1], U[:, :rr] * S[:rr], axes=(2, 0))
+    return [c.reshape(c.shape[0], 2, 2, c.shape[2]) for c in C]
+
+
+def op_lincomb(terms, tol=1e-14):
+    return op_compress(op_sum([op_scale(ch, a) for a, ch in terms]), tol)
+
+
+def op_compose(A, B, tol=1e-14):
+    """``A B`` (apply B first): bonds multiply, the inner index is summed."""
+    out = []
+    for a, b in zip(A, B):
+        c = np.einsum("aomr,bmis->aboirs", a, b)
+        out.append(c.reshape(a.shape[0] * b.shape[0], 2, 2, a.shape[3] * b.shape[3]))
+    return op_compress(out, tol)
+
+
+def op_ket_bra(n, row, col):
+    """``|row><col|`` on n bits (rank 1)."""
+    out = []
+    for k in range(n):
+        c = np.zeros((1, 2, 2, 1), dtype=np.complex128)
+        c[0, (row >> k) & 1, (col >> k) & 1, 0] = 1.0
+        out.append(c)
+    return out
+
+
+def op_coord_diag(n, x0, dx):
+    """``diag(x0 + dx i)``: rank 2, the bond carries (1, partial sum)."""
+    out = []
+    for k in range(n):
+        c = np.zeros((2, 2, 2, 2), dtype=np.complex128)
+        for b in range(2):
+            c[0, b, b, 0] = 1.0
+            c[0, b, b, 1] = dx * (2 ** k) * b
+            c[1, b, b, 1] = 1.0
+        out.append(c)
+    out[0] = out[0][0:1].copy()
+    out[0][0, :, :, 1] += x0 * np.eye(2)
+    out[-1] = out[-1][:, :, :, 1:2].copy()
+    return out
+
+
+_ONESIDED = {1: ([-3.0, 4.0, -1.0], [1.0, -4.0, 3.0]),
+             2: ([2.0, -5.0, 4.0, -1.0], [-1.0, 4.0, -5.0, 2.0])}
+
+
+def op_derivative(n, h, order=1, bc="onesided"):
+    """Second-order differences on ``2^n`` points of spacing h: the central ``(S+ - S-)/2h`` or
+    ``(S+ - 2I + S-)/h^2``. ``dirichlet0`` drops what leaves the box; ``onesided`` adds rank-1
+    corrections turning the first and last rows into the one-sided second-order stencils."""
+    if bc not in ("periodic", "dirichlet0", "onesided"):
+        raise ValueError(f"bad boundary condition {bc!r}")
+    fwd = op_shift(n, periodic=bc == "periodic")
+    bwd = op_transpose(fwd)
+    if order == 1:
+        central = op_lincomb([(1 / (2 * h), fwd), (-1 / (2 * h), bwd)])
+        crow = {1: 1 / (2 * h), -1: -1 / (2 * h)}
+        scale = 1 / (2 * h)
+    elif order == 2:
+        central = op_lincomb([(1 / h ** 2, fwd), (-2 / h ** 2, op_identity(n)), (1 / h ** 2, bwd)])
+        crow = {1: 1 / h ** 2, 0: -2 / h ** 2, -1: 1 / h ** 2}
+        scale = 1 / h ** 2
+    else:
+        raise ValueError(f"order must be 1 or 2, got {order}")
+    if bc != "onesided":
+        return central
+    N = 2 ** n
+    if N < 4:
+        raise ValueError(":onesided stencils need at least 4 points")
+    first, last = _ONESIDED[order]
+    patch = {}
+    for j, w in enumerate(first):            # row 0: the one-sided stencil minus the central row
+        patch[(0, j)] = patch.get((0, j), 0.0) + w * scale
+    for off, w in crow.items():
+        if 0 <= off < N:
+            patch[(0, off)] = patch.get((0, off), 0.0) - w
+    for j, w in enumerate(last):             # row N-1
+        col = N - len(last) + j
+        patch[(N - 1, col)] = patch.get((N - 1, col), 0.0) + w * scale
+    for off, w in crow.items():
+        col = N - 1 + off
+        if 0 <= col < N:
+            patch[(N - 1, col)] = patch.get((N - 1, col), 0.0) - w
+    terms = [(1.0, central)] + [(v, op_ket_bra(n, r, c)) for (r, c), v in sorted(patch.items())
+                                if v != 0.0]
+    return op_lincomb(terms)
+
+
+def heston_cores(g: Grid, p: HestonParams, adjoint=False, tol=1e-14):
+    """``A_H = v/2 d_xx + rho sigma v d_xv + sigma^2 v/2 d_vv + (r - q - v/2) d_x
+    + kappa (theta - v) d_v - r`` as operator cores on the grid's sites (``heston.jl:36-61``);
+    ``adjoint``: the forward-density operator (transpose, no discount)."""
+    if g.periodic_x or g.periodic_y:
+        raise ValueError("heston_op: build the grid with periodic_x = periodic_y = false")
+    if abs(g.y0) >= 1e-14:
+        raise ValueError("heston_op: the variance grid must start at v = 0")
+    d1x, d2x = op_derivative(g.nx, g.dx, 1), op_derivative(g.nx, g.dx, 2)
+    d1v, d2v = op_derivative(g.ny, g.dy, 1), op_derivative(g.ny, g.dy, 2)
+    var = op_coord_diag(g.ny, g.y0, g.dy)
+    var_d1v, var_d2v = op_compose(var, d1v), op_compose(var, d2v)
+    ix, iv = op_identity(g.nx), op_identity(g.ny)
+    terms = [
+        (0.5, d2x, var),
+        (p.rho * p.sigma, d1x, var_d1v),
+        (0.5 * p.sigma ** 2, ix, var_d2v),
+        (p.r - p.q, d1x, iv),
+        (-0.5, d1x, var),
+        (p.kappa * p.theta, ix, d1v),
+        (-p.kappa, ix, var_d1v),
+    ]
+    if not adjoint:
+        terms.append((-p.r, ix, iv))
+    chain = op_lincomb([(a, ax + av) for a, ax, av in terms], tol)
+    return op_transpose(chain) if adjoint else chain
+
+
+def cores_to_mpo(cores) -> MPO:
+    """The solver MPO of operator cores: stored as ``(w_l, in, out, w_r)`` with arrows
+    ``(w_l:-1, s_in:+1, s_out:-1, w_r:+1)``, one dense block per site."""
+    ts = []
+    for c in cores:
+        W = np.ascontiguousarray(np.asarray(c, dtype=np.complex128).transpose(0, 2, 1, 3))
+        legs = [Leg(-1, {0: W.shape[0]}), Leg(+1, {0: 2}), Leg(-1, {0: 2}), Leg(+1, {0: W.shape[3]})]
+        ts.append(from_blocks(legs, {(0, 0, 0, 0): W}))
+    return MPO(ts)
+
+
+def heston_mpo(g: Grid, p: HestonParams, adjoint=False) -> MPO:
+    return cores_to_mpo(heston_cores(g, p, adjoint))

@@ -227,6 +227,13 @@ int bug_la_expm(int n, const double* a, double* out);
 int bug_la_eigh(int n, const double* a, double* vals, double* vecs);
 /* Eigenvalues of a complex upper-Hessenberg n x n matrix; replaces geev in _hess_coeffs. */
 int bug_la_eigvals_hess(int n, const double* a, double* vals_re_im);
+/* The Krylov weight of v_{k+1} in exp(tau H) v_1 for the n x n Hessenberg matrix H (row-major,
+ * interleaved re/im): |H[k, k-1]| |tau| int_0^1 |(exp(s tau H_k) e_1)[k-1]| ds by composite Simpson
+ * in log space, normalised by the propagated seed's norm when state_seed (_kry_weight and
+ * _residual_integral, src/BUG/Core/RankAdaptation/krylov_enrichment.jl:58-120). k is 1-based,
+ * 1 <= k < n. */
+int bug_la_kry_weight(int n, const double* hm, int k, double tau_re, double tau_im, int state_seed,
+                      double* out);
 
 /* ── allocation-free inner product ──────────────────────────────────────────────────────── */
 /* No counterpart in the reference: added for callers that cannot allocate GPU memory at the call

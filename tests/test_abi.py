@@ -81,3 +81,31 @@ def test_small_matrix_routines_match_scipy():
         got = np.sort_complex(ev.view(np.complex128))
         want = np.sort_complex(np.linalg.eigvals(Hs))
         assert np.max(np.abs(got - want)) <= 1e-9 * max(1.0, np.max(np.abs(want)))
+
+
+def test_krylov_weight_matches_oracle():
+    """The native Krylov weight (nodes evaluated in blocks) against the oracle's node-by-node
+    evaluation, on Hessenberg matrices from mild to stiff (the 2 x 4096-panel cap reached)."""
+    import numpy as np
+
+    from bondupdategalerkin_b200 import _engine, build
+    from oracle import krylov as OK
+
+    build.build()
+    lib = _engine.load()
+    rng = np.random.default_rng(11)
+    for n, scale, tau, herm in [(6, 1.0, -0.05j, True), (20, 50.0, -0.05j, True),
+                                (33, 1e4, 0.02, False), (64, 3e5, 0.02, False)]:
+        A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        if herm:
+            A = A + A.conj().T
+        H = np.ascontiguousarray(np.triu(A, -1) * scale / n)
+        h = H.view(np.float64)
+        for k in (1, n // 2, n - 1):
+            for seed in (True, False):
+                out = np.zeros(1)
+                _engine.check(lib.bug_la_kry_weight(n, h.ctypes.data_as(_engine._c_double_p), k,
+                                                    tau.real, tau.imag, int(seed),
+                                                    out.ctypes.data_as(_engine._c_double_p)))
+                want = OK.kry_weight(H, k, tau, state_seed=seed)
+                assert abs(out[0] - want) <= 1e-9 * max(abs(want), 1e-300), (n, k, seed, out[0], want)

@@ -1,0 +1,126 @@
+"""The device BUG step on the Heston quantics workload against the CPU oracle (GPU).
+
+Symmetry ``:none`` (one dense block per tensor), a non-Hermitian generator (Arnoldi), real step
+tau = 0.02, the separable start exp(0.5 x) exp(-v). The device state is built by the product's
+builders (carry-automaton MPO, device canonical moves), the oracle's by its own route (dense
+TT-SVD); both draw their Gaussians from generators seeded alike. After every step: identical bond
+dimensions, ledger verdict and unmet checks, expv iterations; state infidelity <= 1e-12 (the
+normalised overlap; the generator does not conserve the norm, so the norms are compared too,
+to 1e-10 relative).
+
+On 10 + 10 bits the step is ill-conditioned in the state's NORM (the generator's spectrum
+reaches ~1e5, tau |A| ~ 1e3): perturbing the oracle's own input by 1e-15 moves its norm by ~1e-8
+after two steps and ~1e-5 after three, with bond dimensions and verdicts unchanged. No FP64
+implementation short of bit-identical arithmetic meets a fixed 1e-10 norm bar there, so the
+full-size cases run two perturbed oracle copies beside the reference one and hold the device to
+max(1e-10, 10x the oracle's own spread); dimensions, verdicts, expv iterations and the 1e-12
+infidelity bar stay exact. The product's MPO (carry automaton) and the oracle's (dense TT-SVD)
+are two compressions of one generator, so one full-size case uploads the oracle's MPO (its copies
+perturb the state) and one runs the product's (its copies perturb the MPO cores at 1e-14, another
+compression of the same generator).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import qtt as Q
+from oracle import step as OS
+from tests.gpu_util import mps_to_host, overlap
+
+pytestmark = pytest.mark.gpu
+
+HP = (0.03, 0.01, 2.0, 0.09, 0.4, -0.7)
+
+
+def _norm(psi):
+    t = psi[psi.center]
+    return np.sqrt(sum(np.vdot(b, b).real for b in t.blocks.values()))
+
+
+def _perturbed(psi, seed, eps=1e-15):
+    """A copy of the oracle state with its first site tensor perturbed by eps (relative)."""
+    from oracle.blocks import BT
+
+    q = psi.copy()
+    t = q[1]
+    r = np.random.default_rng(seed)
+    q[1] = BT(t.legs, {k: v * (1 + eps * r.standard_normal(v.shape)) for k, v in t.blocks.items()})
+    return q
+
+
+def _perturbed_mpo(mpo, seed, eps=1e-14):
+    """The oracle MPO with every core perturbed by eps (relative): another valid compression."""
+    from oracle.blocks import BT
+    from oracle.models import MPO
+
+    r = np.random.default_rng(seed)
+    return MPO([BT(t.legs, {k: v * (1 + eps * r.standard_normal(v.shape))
+                           for k, v in t.blocks.items()}) for t in mpo.tensors])
+
+
+def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10, spread=None,
+               **kw):
+    from bondupdategalerkin_b200 import build
+
+    build.build()
+    from bondupdategalerkin_b200 import native as DN
+    from bondupdategalerkin_b200 import qtt as P
+    from bondupdategalerkin_b200 import step as DS
+
+    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
+    dom = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
+    og, pg = Q.qtt_grid(nbits, nbits, **dom), P.qtt_grid(nbits, nbits, **dom)
+    fx, fv = (lambda x: np.exp(0.5 * x)), (lambda v: np.exp(-v))
+    opsi = Q.qtt_mps(Q.qtt_separable(og, fx, fv), center=1)
+    dpsi = P.qtt_mps(P.qtt_separable(pg, fx, fv), center=1)
+    ompo = Q.heston_mpo(og, Q.HestonParams(*HP))
+    if mpo_from == "product":
+        dmpo = P.heston_mpo(pg, P.HestonParams(*HP))
+    else:
+        from bondupdategalerkin_b200 import models as DM
+        from tests.gpu_util import to_dev
+
+        dmpo = DM.MPO([to_dev(t) for t in ompo.tensors])
+    orng, drng = np.random.default_rng(1234), np.random.default_rng(1234)
+    # the oracle's own spread: copies with the state (or the MPO) perturbed at roundoff level
+    copies = []
+    for s in ((1, 2) if spread else ()):
+        if spread == "state":
+            copies.append((_perturbed(opsi, s), ompo, np.random.default_rng(1234)))
+        else:
+            copies.append((opsi.copy(), _perturbed_mpo(ompo, s), np.random.default_rng(1234)))
+    for n in range(1, steps + 1):
+        oi = OS.cbe_bug_step(opsi, ompo, 0.02, maxdim=maxdim, hermitian=False, rng=orng, **kw)
+        tol = norm_tol
+        for cpsi, cmpo, crng in copies:
+            OS.cbe_bug_step(cpsi, cmpo, 0.02, maxdim=maxdim, hermitian=False, rng=crng, **kw)
+            tol = max(tol, 10.0 * abs(_norm(cpsi) - _norm(opsi)) / _norm(opsi))
+        di = dstep(dpsi, dmpo, 0.02, maxdim=maxdim, hermitian=False, rng=drng, **kw)
+        assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
+        assert di["status"] == oi["status"], n
+        assert di["ledger"].unmet == oi["ledger"].unmet, n
+        assert di["ledger"].expv_iters == oi["ledger"].expv_iters, n
+        h = mps_to_host(dpsi)
+        ab = overlap(h, opsi)
+        aa, bb = overlap(h, h).real, overlap(opsi, opsi).real
+        inf = 1.0 - abs(ab) ** 2 / (aa * bb)
+        assert inf <= 1e-12, (n, inf)
+        assert abs(np.sqrt(aa) - np.sqrt(bb)) <= tol * np.sqrt(bb), (n, tol)
+    return opsi, dpsi
+
+
+@pytest.mark.parametrize("native", [pytest.param(False, id="python-host"),
+                                    pytest.param(True, id="native-step")])
+def test_heston_4x4_bits(native):
+    run_heston(4, 4, 64, native, tol_basis=1e-8, tol_trunc=1e-12)
+
+
+def test_heston_10x10_bits_config():
+    """The config's grid (10 + 10 bits, maxdim 64), first steps (the oracle takes seconds each),
+    with the oracle's MPO on both sides."""
+    run_heston(10, 3, 64, True, mpo_from="oracle", spread="state")
+
+
+def test_heston_10x10_bits_product_mpo():
+    """The same with the product's own MPO on device."""
+    run_heston(10, 2, 64, True, spread="mpo")
