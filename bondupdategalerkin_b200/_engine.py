@@ -57,6 +57,14 @@ SIGNATURES = {
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
     "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
+    "bug_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.POINTER(_vp)]),
+    "bug_server_submit": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
+    "bug_server_cancel": (ctypes.c_int, [_vp, ctypes.c_int64]),
+    "bug_server_wait": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_double, _c_int_p]),
+    "bug_server_job_stats": (ctypes.c_int, [_vp, ctypes.c_int64, _vp]),
+    "bug_server_step_times": (ctypes.c_int, [_vp, ctypes.c_int64, _c_double_p, ctypes.c_int, _c_int_p]),
+    "bug_server_destroy": (ctypes.c_int, [_vp]),
+    "bug_projected_footprint": (ctypes.c_int64, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bug_la_kry_weight": (ctypes.c_int, [ctypes.c_int, _c_double_p, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, _c_double_p]),
     "bug_la_eigvals_hess": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),

@@ -6,7 +6,7 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "kernels.cu", "step.cu", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "kernels.cu", "step.cu", "noalloc.cu", "server.cu")]
 OUTPUT = os.path.join(HERE, "libbug_b200.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fcx-limited-range",

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace bugk {
 
@@ -521,11 +522,15 @@ int stage_items(const Stage& s) {
   }
 }
 
+// Per-device launch facts shared by every host thread that launches (server workers included).
+std::mutex g_launch_mu;
+
 int stage_grid_limit() {
   static int limit[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lk(g_launch_mu);
   if (limit[dev] == 0) {
     int per_sm = 0, sms = kSmCount;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -551,6 +556,7 @@ void svd_smem_optin(int bytes) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lk(g_launch_mu);  // the attribute only ever grows
   if (bytes > granted[dev]) {
     cudaFuncSetAttribute(jacobi_svd_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     granted[dev] = bytes;

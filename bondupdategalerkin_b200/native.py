@@ -80,16 +80,12 @@ def _lib():
     return lib
 
 
-def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
-                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
-                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
-                 root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
-                 closure_checks=False):
-    """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
-    HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields)."""
-    L = len(psi)
-    if len(mpo) != L:
-        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
+def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None, order=1,
+                maxdim=None, hermitian=True, expansion=None, root=None, reorth=True, truncate=True,
+                work_ceiling_rule="bond", bond_ceiling_factor=None, root_maxiter=30,
+                krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None, closure_checks=False):
+    """The keyword arguments of ``cbe_bug_step!`` as the C-ABI's ``bug_step_params`` (checked the
+    way the reference checks them, ``bug_step_stages.jl:15-142``)."""
     if L < 2:
         raise ValueError("cbe_bug_step needs at least two sites")
     if L - 1 > MAX_SITES:
@@ -107,7 +103,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         fixed_depth = expansion.krylov_fixed_depth
     if mode != "rank_tail":
         raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail")
-    p = StepParams(
+    return StepParams(
         tol_basis=tol_basis or 0.0, tol_trunc=-1.0 if tol_trunc is None else tol_trunc,
         tol_expv=tol_expv or 0.0, tol_krylov=tol_krylov or 0.0, order=order,
         maxdim=maxdim or 0, hermitian=int(hermitian),
@@ -116,6 +112,24 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         root=root or 0, reorth=int(reorth), truncate=int(truncate), root_maxiter=root_maxiter,
         fixed_width=width, tail_factor=tail_factor,
         krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth)
+
+
+def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
+                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
+                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
+                 root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
+                 closure_checks=False):
+    """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
+    HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields)."""
+    L = len(psi)
+    if len(mpo) != L:
+        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
+    p = step_params(L, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_expv=tol_expv,
+                    tol_krylov=tol_krylov, order=order, maxdim=maxdim, hermitian=hermitian,
+                    expansion=expansion, root=root, reorth=reorth, truncate=truncate,
+                    work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
+                    root_maxiter=root_maxiter, krylov_rank_tol=krylov_rank_tol,
+                    frontier_tol=frontier_tol, fold_omega=fold_omega, closure_checks=closure_checks)
     if rng is None:
         rng = np.random.default_rng(0x5EED)
 

@@ -218,6 +218,64 @@ int bug_mps_step(bug_ctx* ctx, int L, bug_tensor** psi_io, int* center_io,
                  const bug_step_params* params, bug_normal_fn draw, void* user,
                  bug_step_info* info, bug_bond_log* bond_log, int bond_log_cap, int* n_bond_log);
 
+/* ── serving: many jobs on one GPU ─────────────────────────────────────────────────────────
+ * No reference counterpart: the reference calls cbe_bug_step! one chain at a time. A server owns
+ * `workers` threads, each with its own context (stream, memory, staging); jobs wait in one FIFO
+ * queue and start when a worker is idle and the running jobs' projected footprints plus the new
+ * one fit `budget_bytes` (a job always starts when nothing runs). Running jobs overlap on the
+ * device (one stream each) and on the host cores; a job's result is the same as alone. */
+typedef struct bug_server bug_server;
+
+enum { BUG_JOB_QUEUED = 0, BUG_JOB_RUNNING = 1, BUG_JOB_DONE = 2, BUG_JOB_FAILED = 3,
+       BUG_JOB_CANCELLED = 4 };
+
+/* Build the job's state (L site handles, centre) and MPO (L handles) on `ctx`, the worker's
+ * context; the server owns the handles afterwards. Return BUG_OK or an error code. Called on the
+ * worker thread. `psi` and `mpo` have room for BUG_MAX_SITES + 1 handles. */
+typedef int (*bug_job_load_fn)(void* user, bug_ctx* ctx, int* L, bug_tensor** psi, int* center,
+                               bug_tensor** mpo);
+/* Read the job's final state (the handles stay the server's and are freed after the call).
+ * `status` is BUG_OK or the failing step's code. Called on the worker thread. */
+typedef void (*bug_job_done_fn)(void* user, bug_ctx* ctx, int status, int L,
+                                bug_tensor* const* psi, int center);
+
+typedef struct {
+  double tau_re, tau_im;     /* step size */
+  int nsteps;                /* steps of cbe_bug_step! */
+  bug_step_params params;
+  bug_normal_fn draw;        /* the job's own Gaussian stream */
+  void* draw_user;
+  bug_job_load_fn load;
+  bug_job_done_fn done;      /* may be NULL */
+  void* user;
+  int64_t footprint_bytes;   /* projected HBM need at maxdim (bug_projected_footprint) */
+} bug_job_spec;
+
+typedef struct {
+  int state;                 /* BUG_JOB_* */
+  int status;                /* BUG_OK or the failing call's code */
+  int worker;                /* the worker that ran it (-1: never started) */
+  int steps_done;
+  double t_submit, t_start, t_end;  /* seconds since the server started */
+  double step_s_sum, step_s_max;    /* per-step latency (stream drained), sum and maximum */
+} bug_job_stats;
+
+int bug_server_create(int device, int workers, int64_t budget_bytes, bug_server** out);
+int bug_server_submit(bug_server* s, const bug_job_spec* spec, int64_t* job_id);
+/* A queued job leaves the queue at once; a running one stops after its current step. */
+int bug_server_cancel(bug_server* s, int64_t job_id);
+/* Wait until job `job_id` (or every job, job_id <= 0) has finished, or `timeout_s` passes
+ * (negative: no limit). `finished` tells which. */
+int bug_server_wait(bug_server* s, int64_t job_id, double timeout_s, int* finished);
+int bug_server_job_stats(bug_server* s, int64_t job_id, bug_job_stats* out);
+/* The job's per-step latencies in seconds (up to cap; n = how many there are). */
+int bug_server_step_times(bug_server* s, int64_t job_id, double* out, int cap, int* n);
+/* Cancels queued jobs, lets running ones stop after their step, joins the workers. */
+int bug_server_destroy(bug_server* s);
+/* Projected HBM bytes of one chain at bond dimension maxdim: state, environment stacks, one
+ * bond's Krylov basis and probes and the two-site work tensors, doubled for temporaries. */
+int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim);
+
 /* ── host small-matrix routines of the step (no device work; usable without a GPU) ────────── */
 /* exp(A) for a complex n x n row-major matrix (Pade-13 scaling and squaring); replaces Julia's
  * matrix `exp` in _kry_weight/_hess_coeffs (krylov_enrichment.jl:89-120, root_methods.jl:136-141). */
