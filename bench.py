@@ -453,6 +453,151 @@ def run_engine(args):
         torch.distributed.destroy_process_group()
 
 
+# ── batched and served workloads (the native job server) ─────────────────────────────────────
+
+def _stream_oracle_inputs(spec):
+    """A job spec's inputs in the CPU oracle (the baseline leg)."""
+    if spec["kind"] == "xxz":
+        from oracle import models as OM
+
+        return OM.product_state(spec["spins"]), OM.xxz_mpo(spec["L"], J=1.0, delta=spec["delta"])
+    from oracle import qtt as Q
+
+    b = spec["bits"]
+    g = Q.qtt_grid(b, b, **_HESTON_DOMAIN)
+    psi = Q.qtt_mps(Q.qtt_separable(g, lambda x: np.exp(0.5 * x), lambda v: np.exp(-v)))
+    return psi, Q.heston_mpo(g, Q.HestonParams(*spec["params"]))
+
+
+def _oracle_from_blocks(blocks, center):
+    from oracle import blocks as OB
+    from oracle import models as OM
+
+    return OM.MPS([OB.BT([OB.Leg(l.dir, l.sectors) for l in legs], b) for legs, b in blocks], center)
+
+
+def stream_cpu_sample(specs, jobs, k=4):
+    """The oracle on a bounded sample: for k jobs, one step from the job's start and one from its
+    final state (so the sample spans the jobs' range of bond dimensions). Returns (steps, s)."""
+    from oracle import step as OS
+
+    secs, n = 0.0, 0
+    idx = np.linspace(0, len(specs) - 1, min(k, len(specs))).round().astype(int)
+    for i in idx:
+        spec, job = specs[i], jobs[i]
+        psi, mpo = _stream_oracle_inputs(spec)
+        starts = [psi]
+        if job is not None and job.result is not None:
+            starts.append(_oracle_from_blocks(job.result, job.result_center))
+        for st in starts:
+            rng = np.random.default_rng(spec["seed"])
+            t0 = time.perf_counter()
+            OS.cbe_bug_step(st, mpo, spec["tau"], rng=rng, **spec["kw"])
+            secs += time.perf_counter() - t0
+            n += 1
+    return n, secs
+
+
+def _block_bytes(blocks):
+    return sum(16 * v.size for _, b in blocks for v in b.values())
+
+
+def run_stream(args):
+    """``--workload batch`` (64 chains submitted at once) or ``served`` (Poisson arrivals)."""
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    from bondupdategalerkin_b200 import _engine as E
+    from bondupdategalerkin_b200 import build as Bld
+    from bondupdategalerkin_b200 import server as S
+    from bondupdategalerkin_b200 import workloads as WL
+
+    if Bld.needs_build():
+        Bld.build()
+    E.set_default_device(local)
+    workers = args.workers or min(16, os.cpu_count() or 1)
+    free, total = torch.cuda.mem_get_info(local)
+    budget = int(0.8 * free)
+    if KIND[0] == "batch":
+        specs = WL.batch_specs(args.jobs or 64)
+        name = f"batch_{len(specs)}_xxz_chains_L32-96_maxdim64-256_50steps_order2"
+    else:
+        specs = WL.served_specs(args.jobs or 48, rate=20.0, scale=args.scale)
+        name = (f"served_poisson20_{len(specs)}jobs_70xxz_30heston_scale{args.scale:g}")
+    inputs = [WL.job_inputs(sp) for sp in specs]  # host blocks, untimed
+    h2d = sum(_block_bytes(a) + _block_bytes(c) for a, _, c in inputs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    with S.Server(workers=workers, budget_bytes=budget, device=local) as srv:
+        t0 = time.perf_counter()
+        jobs = []
+        for sp, (st, cen, mp) in zip(specs, inputs):
+            if KIND[0] == "served":
+                delay = t0 + sp["arrival"] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+            jobs.append(srv.submit(st, cen, mp, sp["tau"], sp["nsteps"], sp["seed"], **sp["kw"]))
+        srv.wait()
+        wall = time.perf_counter() - t0
+        launches = srv.launches()
+        stats = [j.stats for j in jobs]
+        lat = S.latency_summary(jobs)
+    clk = clocks.stop()
+    failed = [s for s in stats if s["state"] != "done"]
+    steps = sum(s["steps_done"] for s in stats)
+    d2h = sum(_block_bytes(j.result) for j in jobs if j.result)
+    value = steps / wall
+    line = {
+        "metric": "chain_steps_per_s" if KIND[0] == "batch" else "served_steps_per_s",
+        "value": value, "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "ms_per_step": 1e3 * wall / max(steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128",
+        "data": "synthetic (seeded job stream: product/QTT starts, seeded Gaussian probes)",
+        "config": {"workload": name, "jobs": len(specs), "workers": workers,
+                   "hbm_budget_bytes": budget, "wall_s": wall,
+                   "timing": "host wall clock from the first submit to the last job's end, every "
+                             "worker stream drained (inputs uploaded and results downloaded by the "
+                             "jobs inside the timed region)"},
+        "gpu_launches": int(launches),
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": h2d // max(steps, 1),
+                "d2h_bytes_per_step": d2h // max(steps, 1)},
+        "latency": lat, "jobs_failed": len(failed),
+        "failures": [(s["steps_done"], s["status"], s["error"]) for s in failed[:3]], "clocks": clk,
+    }
+    if KIND[0] == "served":
+        line["config"]["arrivals"] = "Poisson, 20 jobs/s"
+        line["config"]["scale"] = (f"{args.scale:g}: L, maxdim, bits and steps ranges shrunk toward "
+                                   "their lower ends by this factor (1 = the stream as specified)")
+        line["throughput_jobs_per_s"] = len(specs) / wall
+    if not args.no_cpu_baseline:
+        n, secs = stream_cpu_sample(specs, jobs)
+        line["cpu_baseline"] = {"value": n / secs, "unit": "steps/s", "cores": blas_threads(),
+                                "kind": "port",
+                                "sample": f"CPU oracle, one step from the start and one from the end "
+                                          f"state of {n // 2} jobs spread over the stream (one at "
+                                          f"a time)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_stream_reference(args):
+    from bondupdategalerkin_b200 import workloads as WL
+
+    specs = WL.batch_specs(args.jobs or 64) if KIND[0] == "batch" else \
+        WL.served_specs(args.jobs or 48, rate=20.0, scale=args.scale)
+    n, secs = stream_cpu_sample(specs, [None] * len(specs), k=8)
+    value = n / secs
+    print(json.dumps({"impl": "reference", "metric": "chain_steps_per_s" if KIND[0] == "batch"
+                      else "served_steps_per_s", "value": value, "unit": "steps/s", "n_gpus": 1,
+                      "steps": n, "warmup": 0, "higher_is_better": True, "dtype": "c128",
+                      "cpu_baseline": {"value": value, "unit": "steps/s", "cores": blas_threads(),
+                                       "kind": "port",
+                                       "sample": f"CPU oracle, the first step of {n} jobs spread "
+                                                 "over the stream, one at a time"},
+                      "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,9 +612,14 @@ def main():
                     help="time the steps only (for profiler runs)")
     ap.add_argument("--L", type=int, default=None,
                     help="chain length override (smaller cases for profiler captures only)")
-    ap.add_argument("--workload", default="xxz", choices=["xxz", "heston"],
+    ap.add_argument("--workload", default="xxz", choices=["xxz", "heston", "batch", "served"],
                     help="xxz: the L = 64 XXZ quench (the headline); heston: the 10 + 10-bit "
-                         "Heston QTT field (47 timed steps after 3 warm-up make its 50)")
+                         "Heston QTT field (47 timed steps after 3 warm-up make its 50); batch: 64 "
+                         "chains at once on the job server; served: a Poisson job stream")
+    ap.add_argument("--workers", type=int, default=0, help="job server workers (0: min(16, cores))")
+    ap.add_argument("--jobs", type=int, default=0, help="batch/served: number of jobs")
+    ap.add_argument("--scale", type=float, default=0.25,
+                    help="served: shrink the stream's size ranges toward their lower ends")
     args = ap.parse_args()
     KIND[0] = args.workload
     if args.workload == "heston" and "--steps" not in sys.argv:
@@ -480,6 +630,13 @@ def main():
         WORKLOAD["L"] = args.L
         global WORKLOAD_NAME
         WORKLOAD_NAME = WORKLOAD_NAME.replace("L64", f"L{args.L}")
+    if args.workload in ("batch", "served"):
+        if args.impl == "reference":
+            if dist_env()[1] == 0:
+                run_stream_reference(args)
+        elif dist_env()[1] == 0:
+            run_stream(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -64,6 +64,8 @@ SIGNATURES = {
     "bug_server_job_stats": (ctypes.c_int, [_vp, ctypes.c_int64, _vp]),
     "bug_server_step_times": (ctypes.c_int, [_vp, ctypes.c_int64, _c_double_p, ctypes.c_int, _c_int_p]),
     "bug_server_destroy": (ctypes.c_int, [_vp]),
+    "bug_server_launches": (ctypes.c_int64, [_vp]),
+    "bug_server_job_error": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]),
     "bug_projected_footprint": (ctypes.c_int64, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "bug_la_kry_weight": (ctypes.c_int, [ctypes.c_int, _c_double_p, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, _c_double_p]),

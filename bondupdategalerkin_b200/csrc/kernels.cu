@@ -302,9 +302,10 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), con
 
 // ── batched one-sided Jacobi SVD ──────────────────────────────────────────────────────────────
 // Problem: work = A (mm x r, column-major, mm >= r). Columns are orthogonalised pairwise in a
-// round-robin order (r-1 rounds of disjoint pairs per sweep, one warp per pair) until no pair has
-// |a_p^H a_q| > tol*|a_p||a_q|. Then sigma_j = |a_j|, sorted descending (ties by index), and the
-// phase of each singular pair is fixed on the left vectors of M.
+// round-robin order (r-1 rounds of disjoint pairs per sweep, one warp per pair) until a sweep
+// rotates no pair by more than eps (a pair rotates while |a_p^H a_q| > m eps |a_p||a_q|). Then
+// sigma_j = |a_j|, sorted descending (ties by index), and the phase of each singular pair is fixed
+// on the left vectors of M.
 
 constexpr int kMaxSweeps = 60;
 constexpr int kMaxR = 1024;
@@ -364,7 +365,9 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
   for (int64_t i = tid; i < int64_t(r) * r; i += blockDim.x)
     V[i] = (i % (r + 1) == 0) ? make_double2(1.0, 0.0) : make_double2(0.0, 0.0);
   __syncthreads();
-  const double tol = tol_scale * sqrt(double(mm));
+  // m * eps: the rounding error of the computed a_p^H a_q is itself of order m * eps |a_p||a_q|,
+  // so a tighter test can keep near-degenerate or noise-level pairs rotating forever
+  const double tol = tol_scale * double(mm);
   const int re = r + (r & 1);
   int sweep = 0;
   bool converged = (r == 1);
@@ -393,9 +396,10 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
         gi = warp_sum(gi);
         const double g = sqrt(gr * gr + gi * gi);
         if (al > 0.0 && be > 0.0 && g > tol * sqrt(al) * sqrt(be)) {
-          if (lane == 0) rotated = 1;
           const double zeta = (be - al) / (2.0 * g);
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          // a rotation by an angle below eps leaves the pair as it was: not progress to wait for
+          if (lane == 0 && fabs(t) > tol_scale) rotated = 1;
           const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
           const double2 e = make_double2(gr / g, -gi / g);  // e^{-i phi}, gamma = g e^{i phi}
           for (int i = lane; i < mm; i += 32) {

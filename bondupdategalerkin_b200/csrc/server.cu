@@ -58,8 +58,6 @@ struct bug_server {
   std::map<int64_t, std::unique_ptr<Job>> jobs;
   std::vector<std::thread> threads;
   std::vector<bug_ctx*> ctxs;
-  std::string init_error;
-  int init_failed = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -302,6 +300,26 @@ extern "C" int bug_server_destroy(bug_server* s) {
     for (bug_ctx* c : s->ctxs) bug_ctx_destroy(c);
     delete s;
   });
+}
+
+extern "C" int bug_server_job_error(bug_server* s, int64_t job_id, char* buf, int cap) {
+  return guard([&] {
+    require(s && buf && cap > 0, "bad argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(job_id);
+    require(it != s->jobs.end(), "no such job");
+    const std::string& e = it->second->error;
+    const size_t n = std::min(e.size(), size_t(cap - 1));
+    std::memcpy(buf, e.data(), n);
+    buf[n] = 0;
+  });
+}
+
+extern "C" int64_t bug_server_launches(const bug_server* s) {
+  if (!s) return 0;
+  int64_t n = 0;
+  for (const bug_ctx* c : s->ctxs) n += bug_ctx_launches(c);
+  return n;
 }
 
 extern "C" int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim) {

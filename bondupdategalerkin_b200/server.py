@@ -134,9 +134,12 @@ class Job:
         E.check(lib.bug_server_step_times(self.server.h, self.id, None, 0, ctypes.byref(n)))
         buf = (ctypes.c_double * max(n.value, 1))()
         E.check(lib.bug_server_step_times(self.server.h, self.id, buf, n.value, ctypes.byref(n)))
+        msg = ctypes.create_string_buffer(512)
+        E.check(lib.bug_server_job_error(self.server.h, self.id, msg, 512))
         return dict(state=JOB_STATES[st.state], status=st.status, worker=st.worker,
                     steps_done=st.steps_done, t_submit=st.t_submit, t_start=st.t_start,
-                    t_end=st.t_end, step_s=list(buf[:n.value]), error=self.error)
+                    t_end=st.t_end, step_s=list(buf[:n.value]),
+                    error=self.error or (msg.value.decode(errors="replace") or None))
 
 
 class Server:
@@ -171,6 +174,10 @@ class Server:
                                          -1.0 if timeout is None else float(timeout),
                                          ctypes.byref(fin)))
         return bool(fin.value)
+
+    def launches(self) -> int:
+        """Kernel launches issued by all workers so far."""
+        return int(self.lib.bug_server_launches(self.h))
 
     def close(self) -> None:
         if self.h:

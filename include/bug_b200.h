@@ -272,6 +272,10 @@ int bug_server_job_stats(bug_server* s, int64_t job_id, bug_job_stats* out);
 int bug_server_step_times(bug_server* s, int64_t job_id, double* out, int cap, int* n);
 /* Cancels queued jobs, lets running ones stop after their step, joins the workers. */
 int bug_server_destroy(bug_server* s);
+/* The failing call's message of a failed job ("" otherwise), truncated to cap - 1 bytes. */
+int bug_server_job_error(bug_server* s, int64_t job_id, char* buf, int cap);
+/* Kernel launches issued by all workers so far. */
+int64_t bug_server_launches(const bug_server* s);
 /* Projected HBM bytes of one chain at bond dimension maxdim: state, environment stacks, one
  * bond's Krylov basis and probes and the two-site work tensors, doubled for temporaries. */
 int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim);

@@ -149,3 +149,27 @@ def test_profiled_step_identical(dev):
         assert ba.keys() == bb.keys()
         for k in ba:
             assert np.array_equal(ba[k], bb[k]), k
+
+
+@pytest.mark.parametrize("idx", [0, 3, 7])
+def test_random_sz0_chains_native_vs_oracle(dev, idx):
+    """Chains of the batched workload (seeded random product states with total S^z = 0, order 2,
+    tau = -0.02i): their first SVDs see many exactly degenerate and noise-level pairs."""
+    DM, _ = dev
+    from bondupdategalerkin_b200 import native as DN
+    from bondupdategalerkin_b200 import workloads as WL
+
+    sp = WL.batch_specs(64)[idx]
+    opsi = OM.product_state(sp["spins"])
+    ompo = OM.xxz_mpo(sp["L"], J=1.0, delta=sp["delta"])
+    dpsi = DM.product_state(sp["spins"])
+    dmpo = DM.xxz_mpo(sp["L"], J=1.0, delta=sp["delta"])
+    orng, drng = np.random.default_rng(sp["seed"]), np.random.default_rng(sp["seed"])
+    for n in range(1, 3):
+        oi = OS.cbe_bug_step(opsi, ompo, sp["tau"], rng=orng, **sp["kw"])
+        di = DN.cbe_bug_step(dpsi, dmpo, sp["tau"], rng=drng, **sp["kw"])
+        assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
+        assert di["status"] == oi["status"], n
+        h = mps_to_host(dpsi)
+        inf = 1.0 - fidelity(h, opsi)
+        assert inf <= 1e-12, (n, inf)
