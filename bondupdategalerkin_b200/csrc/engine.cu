@@ -493,6 +493,8 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
   // launch Jacobi
   std::vector<SvdDesc> sd(np);
   int max_smem = 0;
+  int64_t max_r = 0;
+  const int64_t smem_limit = bugk::svd_smem_limit();
   for (int s = 0; s < np; ++s) {
     auto& p = *order[s];
     int64_t mm = std::max(p.m, p.n), r = std::min(p.m, p.n);
@@ -507,9 +509,12 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
     d.m = int(p.m);
     d.n = int(p.n);
     d.trans = p.m < p.n ? 1 : 0;
-    int64_t bytes = (mm * r + r * r) * int64_t(sizeof(double2));
-    d.use_smem = bytes <= 200 * 1024 ? 1 : 0;
-    if (d.use_smem) max_smem = std::max<int>(max_smem, int(bytes));
+    // shared memory for A and V if both fit, else for A alone, else none
+    const int64_t both = (mm * r + r * r) * int64_t(sizeof(double2));
+    const int64_t a_only = mm * r * int64_t(sizeof(double2));
+    d.use_smem = both <= smem_limit ? 2 : (a_only <= smem_limit ? 1 : 0);
+    if (d.use_smem) max_smem = std::max<int>(max_smem, int(d.use_smem == 2 ? both : a_only));
+    max_r = std::max(max_r, r);
     d.pack_begin = int(packs.size());
     packs.insert(packs.end(), packs_of[s].begin(), packs_of[s].end());
     d.pack_end = int(packs.size());
@@ -524,7 +529,7 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
     }
     const bugk::Blob blob = c->begin();
-    bugk::launch_svd(blob, dsd, np, dpk, max_smem, c->stream);
+    bugk::launch_svd(blob, dsd, np, dpk, max_smem, max_r > 48 ? 1024 : 256, c->stream);
     c->launched(BUG_K_SVD, sflops, sbytes);
   }
   // the kernel wrote singular values and sweep counts into `host`

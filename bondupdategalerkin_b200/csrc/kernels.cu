@@ -302,13 +302,14 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), con
 
 // ── batched one-sided Jacobi SVD ──────────────────────────────────────────────────────────────
 // Problem: work = A (mm x r, column-major, mm >= r). Columns are orthogonalised pairwise in a
-// round-robin order (r-1 rounds of disjoint pairs per sweep, one warp per pair) until a sweep
-// rotates no pair by more than eps (a pair rotates while |a_p^H a_q| > m eps |a_p||a_q|). Then
-// sigma_j = |a_j|, sorted descending (ties by index), and the phase of each singular pair is fixed
-// on the left vectors of M.
+// round-robin order (r-1 rounds of disjoint pairs per sweep, one warp per pair) until no pair has
+// |a_p^H a_q| > m eps |a_p||a_q| -- relative to BOTH columns, so the singular vectors of tiny
+// singular values come out orthogonal too. Then sigma_j = |a_j|, sorted descending (ties by
+// index), and the phase of each singular pair is fixed on the left vectors of M.
 
 constexpr int kMaxSweeps = 60;
 constexpr int kMaxR = 1024;
+constexpr int kSvdThreads = 1024;  // wide sectors: one warp per column pair, 32 pairs per pass
 
 __device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b) {
   const int n1 = re - 1;
@@ -322,7 +323,7 @@ __device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b
 }
 
 template <int N>
-__global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N),
+__global__ void __launch_bounds__(kSvdThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N),
                                                               const SvdDesc* descs,
                                                               const CopyDesc* packs,
                                                               double tol_scale) {
@@ -332,6 +333,9 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
   extern __shared__ double2 dyn[];
   __shared__ double sig[kMaxR];
   __shared__ int perm[kMaxR];
+  __shared__ int zero_col[kMaxR];  // 1: numerically zero column, completed orthonormally
+  __shared__ double2 coef[kMaxR];
+  __shared__ double maxn2, wnorm2;
   __shared__ int rotated;
   const SvdDesc d = descs[blockIdx.x];
   const int mm = d.m > d.n ? d.m : d.n;
@@ -357,9 +361,9 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
   __syncthreads();
   double2* A = d.work;
   double2* V = d.vwork;
-  if (d.use_smem) {
+  if (d.use_smem) {  // 1: A in shared memory; 2: A and V
     A = dyn;
-    V = dyn + int64_t(mm) * r;
+    if (d.use_smem == 2) V = dyn + int64_t(mm) * r;
     for (int64_t i = tid; i < int64_t(mm) * r; i += blockDim.x) A[i] = d.work[i];
   }
   for (int64_t i = tid; i < int64_t(r) * r; i += blockDim.x)
@@ -368,6 +372,25 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
   // m * eps: the rounding error of the computed a_p^H a_q is itself of order m * eps |a_p||a_q|,
   // so a tighter test can keep near-degenerate or noise-level pairs rotating forever
   const double tol = tol_scale * double(mm);
+  // a column at most tol * (largest column norm) long is numerically zero: rotating it against
+  // the others only shrinks it further (its direction is rounding noise and never converges), so
+  // no pair with such a column is rotated, and afterwards it is replaced by a unit vector
+  // orthogonal to all other singular vectors (its singular value stays its tiny norm)
+  for (int j = warp; j < r; j += nwarps) {
+    const double2* aj = A + int64_t(j) * mm;
+    double s2 = 0.0;
+    for (int i = lane; i < mm; i += 32) s2 = fma(aj[i].x, aj[i].x, fma(aj[i].y, aj[i].y, s2));
+    s2 = warp_sum(s2);
+    if (lane == 0) sig[j] = s2;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double mx = 0.0;
+    for (int j = 0; j < r; ++j) mx = fmax(mx, sig[j]);
+    maxn2 = mx;
+  }
+  __syncthreads();
+  const double negl = tol * tol * maxn2;
   const int re = r + (r & 1);
   int sweep = 0;
   bool converged = (r == 1);
@@ -395,11 +418,10 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
         gr = warp_sum(gr);
         gi = warp_sum(gi);
         const double g = sqrt(gr * gr + gi * gi);
-        if (al > 0.0 && be > 0.0 && g > tol * sqrt(al) * sqrt(be)) {
+        if (al > negl && be > negl && g > tol * sqrt(al) * sqrt(be)) {
+          if (lane == 0) rotated = 1;
           const double zeta = (be - al) / (2.0 * g);
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          // a rotation by an angle below eps leaves the pair as it was: not progress to wait for
-          if (lane == 0 && fabs(t) > tol_scale) rotated = 1;
           const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
           const double2 e = make_double2(gr / g, -gi / g);  // e^{-i phi}, gamma = g e^{i phi}
           for (int i = lane; i < mm; i += 32) {
@@ -430,9 +452,74 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
     double s2 = 0.0;
     for (int i = lane; i < mm; i += 32) s2 = fma(aj[i].x, aj[i].x, fma(aj[i].y, aj[i].y, s2));
     s2 = warp_sum(s2);
-    if (lane == 0) sig[j] = sqrt(s2);
+    if (lane == 0) {
+      sig[j] = sqrt(s2);
+      zero_col[j] = s2 <= negl ? 1 : 0;
+    }
   }
   __syncthreads();
+  // complete the numerically zero columns: for each in turn, two classical Gram-Schmidt passes of
+  // a start vector (its own direction, else unit vectors e_k) against every other column's unit
+  // vector; accepted when at least half of it survives, stored as a unit vector
+  for (int j = 0; j < r; ++j) {
+    if (!zero_col[j]) continue;
+    double2* aj = A + int64_t(j) * mm;
+    for (int attempt = 0; attempt <= mm; ++attempt) {
+      const bool own = attempt == 0;
+      if (own && !(sig[j] > 0.0)) continue;
+      const double sc = own ? 1.0 / sig[j] : 0.0;
+      for (int i = tid; i < mm; i += blockDim.x)
+        aj[i] = own ? make_double2(aj[i].x * sc, aj[i].y * sc)
+                    : make_double2(i == attempt - 1 ? 1.0 : 0.0, 0.0);
+      __syncthreads();
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int k = warp; k < r; k += nwarps) {  // coef_k = u_k^H w (zero for unfinished columns)
+          double cr = 0.0, ci = 0.0;
+          if (k != j && (!zero_col[k] || zero_col[k] == 2)) {
+            const double2* ak = A + int64_t(k) * mm;
+            const double inv = zero_col[k] == 2 ? 1.0 : 1.0 / sig[k];
+            for (int i = lane; i < mm; i += 32) {
+              const double2 u = ak[i], w = aj[i];
+              cr = fma(u.x, w.x, fma(u.y, w.y, cr));
+              ci = fma(u.x, w.y, fma(-u.y, w.x, ci));
+            }
+            cr = warp_sum(cr) * inv;
+            ci = warp_sum(ci) * inv;
+          }
+          if (lane == 0) coef[k] = make_double2(cr, ci);
+        }
+        __syncthreads();
+        for (int i = tid; i < mm; i += blockDim.x) {  // w -= sum_k coef_k u_k
+          double2 w = aj[i];
+          for (int k = 0; k < r; ++k) {
+            const double2 c = coef[k];
+            if (c.x == 0.0 && c.y == 0.0) continue;
+            const double inv = zero_col[k] == 2 ? 1.0 : 1.0 / sig[k];
+            const double2 u = A[int64_t(k) * mm + i];
+            w.x -= inv * (c.x * u.x - c.y * u.y);
+            w.y -= inv * (c.x * u.y + c.y * u.x);
+          }
+          aj[i] = w;
+        }
+        __syncthreads();
+      }
+      if (warp == 0) {
+        double n2 = 0.0;
+        for (int i = lane; i < mm; i += 32) n2 = fma(aj[i].x, aj[i].x, fma(aj[i].y, aj[i].y, n2));
+        n2 = warp_sum(n2);
+        if (lane == 0) wnorm2 = n2;
+      }
+      __syncthreads();
+      if (wnorm2 >= 0.25) {
+        const double inv = 1.0 / sqrt(wnorm2);
+        for (int i = tid; i < mm; i += blockDim.x) aj[i] = make_double2(aj[i].x * inv, aj[i].y * inv);
+        __syncthreads();
+        if (tid == 0) zero_col[j] = 2;  // completed: a unit vector now
+        __syncthreads();
+        break;
+      }
+    }
+  }
   for (int j = tid; j < r; j += blockDim.x) {
     const double sj = sig[j];
     int pos = 0;
@@ -447,8 +534,8 @@ __global__ void __launch_bounds__(kThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS(N)
   for (int o = warp; o < r; o += nwarps) {
     const int j = perm[o];
     const double sj = sig[j];
-    const double inv = sj > 0.0 ? 1.0 / sj : 0.0;
-    const double2* aj = A + int64_t(j) * mm;  // left vector of work (times sigma)
+    const double inv = zero_col[j] == 2 ? 1.0 : (sj > 0.0 ? 1.0 / sj : 0.0);
+    const double2* aj = A + int64_t(j) * mm;  // left vector of work (times sigma, or completed)
     const double2* vj = V + int64_t(j) * r;   // right vector of work
     double2* uo = d.U + int64_t(o) * d.m;
     double2* vo = d.V + int64_t(o) * d.n;
@@ -568,8 +655,24 @@ void svd_smem_optin(int bytes) {
 }
 }  // namespace
 
+int svd_smem_limit() {
+  static int limit[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  if (limit[dev] == 0) {
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, jacobi_svd_kernel<int(kInlineMax)>);
+    limit[dev] = std::max(0, optin - int(fa.sharedSizeBytes) - 1024);
+  }
+  return limit[dev];
+}
+
 void launch_svd(const Blob& b, const SvdDesc* d_desc, int nprob, const CopyDesc* packs,
-                int max_smem_bytes, cudaStream_t s) {
+                int max_smem_bytes, int threads, cudaStream_t s) {
   if (nprob <= 0) return;
   if (max_smem_bytes > 0) {
     const int64_t nb = b.host ? int64_t(b.bytes) : 0;
@@ -580,7 +683,7 @@ void launch_svd(const Blob& b, const SvdDesc* d_desc, int nprob, const CopyDesc*
     else svd_smem_optin<int(kInlineMax)>(max_smem_bytes);
   }
 #define BUG_SVD_LAUNCH(NB, P, NBYTES)                                                           \
-  jacobi_svd_kernel<NB><<<nprob, kThreads, max_smem_bytes, s>>>(P, b.arena, (NBYTES), d_desc,  \
+  jacobi_svd_kernel<NB><<<nprob, threads, max_smem_bytes, s>>>(P, b.arena, (NBYTES), d_desc,    \
                                                                  packs, 2.220446049250313e-16)
   BUG_WITH_BLOB(b, BUG_SVD_LAUNCH);
 #undef BUG_SVD_LAUNCH

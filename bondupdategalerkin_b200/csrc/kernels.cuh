@@ -85,7 +85,7 @@ struct SvdDesc {
   int* sweeps;      // sweeps used (or -1 if the bound was hit), host-mapped pinned memory
   int m, n;         // shape of M
   int trans;        // 1: work holds M^H (m < n)
-  int use_smem;     // 1: the CTA copies work/vwork into shared memory
+  int use_smem;     // 1: the CTA keeps work in shared memory; 2: work and vwork
   int pack_begin, pack_end;  // gather descriptors that assemble `work` from the tensor's blocks
 };
 
@@ -159,7 +159,11 @@ constexpr int kStageThreads = 256;
 int stage_items(const Stage& s);
 int stage_grid_limit();
 void launch_stage(const Blob& b, const Stage& st, cudaStream_t s);
+// Dynamic shared memory the SVD kernel may use per CTA on this device (opt-in maximum minus its
+// static arrays).
+int svd_smem_limit();
+// `threads`: 256, or 1024 for wide sectors (one warp per column pair of a round).
 void launch_svd(const Blob& b, const SvdDesc* d_desc, int nprob, const CopyDesc* packs,
-                int max_smem_bytes, cudaStream_t s);
+                int max_smem_bytes, int threads, cudaStream_t s);
 
 }  // namespace bugk

@@ -132,3 +132,42 @@ def test_gaussian_matches_oracle_draws(D):
     want = OB.gaussian_fused(np.random.default_rng(9), OB.Leg(-1, la.sectors), OB.Leg(-1, lb.sectors),
                              cols, new_first=False)
     assert same(got, want) == 0.0
+
+
+def _isometry_err(U, cols):
+    """max |U^H U - I| over the sector matrices of an isometry whose columns are leg `cols`."""
+    err = 0.0
+    for c, (_, _, _, _, M) in OB.sector_matrix(U, tuple(i for i in range(len(U.legs)) if i != cols)).items():
+        err = max(err, float(np.max(np.abs(M.conj().T @ M - np.eye(M.shape[1])))))
+    return err
+
+
+def test_svd_rank_deficient(D):
+    """Numerically zero singular values (rank-deficient sectors, a column of rounding noise, an
+    exactly zero column): the Jacobi SVD converges, keeps U and V isometries, and matches the
+    non-negligible singular triples of LAPACK."""
+    # the 3 x 3 sector met in a random-product-state step: a singular value of 5e-168
+    legs = [OB.Leg(-1, {-3: 3}), OB.Leg(-1, {-1: 1, 1: 1}), OB.Leg(+1, {-4: 1, -2: 2})]
+    blk1 = np.array([0.01, 0.0, 0.0], dtype=np.complex128).reshape(3, 1, 1)
+    blk2 = np.array([[7.12816426e-2 - 4.22641607e-36j, 5.55681849e-3 + 1.20924481e-36j],
+                     [-1.85546035e-2 + 6.83848485e-36j, 2.13477560e-2 - 1.95659921e-36j],
+                     [7.20192925e-186 + 1.21465880e-151j, 3.04118525e-185 - 1.39750977e-151j]])
+    A = OB.BT(legs, {(-3, -1, -4): blk1, (-3, 1, -2): blk2.reshape(3, 1, 2)})
+    rng = np.random.default_rng(13)
+    left = rng.standard_normal((40, 6)) + 1j * rng.standard_normal((40, 6))
+    right = rng.standard_normal((6, 2, 25)) + 1j * rng.standard_normal((6, 2, 25))
+    lowrank = np.einsum("ak,kbc->abc", left, right)  # 40 x 50, rank 6
+    lowrank[:, :, 3] = 0.0                           # and an exactly zero column
+    B = OB.BT([OB.Leg(-1, {0: 40}), OB.Leg(-1, {0: 2}), OB.Leg(+1, {0: 25})], {(0, 0, 0): lowrank})
+    for T, split in ((A, (0,)), (B, (0,)), (B, (0, 1))):
+        want = OB.svd(T, split)
+        got = D.svd(to_dev(T), split)
+        gs = np.array([s for s, *_ in got.kept])
+        ws = np.array([s for s, *_ in want.kept])
+        big = ws > 1e-12 * ws[0]
+        assert np.allclose(gs[: big.sum()], ws[big], rtol=1e-12, atol=0)
+        assert np.all(gs[big.sum():] <= 1e-12 * ws[0])  # the numerically zero ones stay tiny
+        Uh, Vh = to_host(got.U), to_host(got.Vd)
+        assert _isometry_err(Uh, len(split)) < 1e-12
+        rec = OB.contract(to_host(got.US()), (len(split),), Vh, (0,))
+        assert same(rec, T) < 1e-13
