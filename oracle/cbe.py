@@ -24,7 +24,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import blocks as B
-from .budget import indicator
+from .budget import ADAPTIVE_GROWTH, indicator
 from .env import stream_left, stream_right
 
 EPS = 2.220446049250313e-16
@@ -123,13 +123,30 @@ def alloc_columns(dims: dict, budget: int) -> dict:
     return {q: min(d, math.ceil(d / tot * budget)) for q, d in dims.items()}
 
 
-def dd_probe(opp, oside, width, rng):
+def boost_columns(cols: dict, boost: dict, cap: dict) -> dict:
+    """``_boost!`` (``cbe.jl:206-216``): raise targeted sectors' columns, capped by ``cap``;
+    returns what did not fit."""
+    left = {}
+    for q, extra in boost.items():
+        if q not in cap:
+            continue
+        have = cols.get(q, 0)
+        add = min(max(extra, 0), max(cap[q] - have, 0))
+        cols[q] = have + add
+        if extra > add:
+            left[q] = extra - add
+    return left
+
+
+def dd_probe(opp, oside, width, rng, boost=None):
     """Sector-graded Gaussian probe in ``opp``'s discarded space (``dd_cbe.jl:132-161``)."""
     dfull, dT = fused_dims(opp, oside)
     dC = {c: max(dfull[c] - dT[c], 0) for c in dfull}
     if sum(dC.values()) == 0:
         return None
     cols = alloc_columns(dC, width)
+    if boost:
+        boost_columns(cols, boost, dC)
     if oside == "left":
         om = B.gaussian_fused(rng, opp.legs[0], opp.legs[1], cols, new_first=False)
     else:
@@ -181,6 +198,206 @@ def sample_residual(basis, project, sketch, Om, wleg, side):
         rq = B.trim_per_sector(residual, rleg, {q: d}) if len(residual.legs[rleg].sectors) > 1 else residual
         per[q] = (B.norm(rq) ** 2 if rq is not None else 0.0) / nq
     return math.sqrt(sum(per.values())), per, cols
+
+
+# ── the :adaptive controller: sectorwise thin pivoted QR, DD select, the incremental sketch ────
+
+REORTH_KEEP = 1.0 / math.sqrt(2.0)  # ``_REORTH_KEEP`` (dd_cbe.jl:273)
+DD_HOLDOUT = 4                      # ``_DD_HOLDOUT`` (dd_cbe_controller.jl:12)
+
+
+def thin_qr(sketch: B.BT, fl: int, ref_dir: int, thr: float):
+    """Orthonormal basis of the span of ``sketch``'s leg-``fl`` columns by column-pivoted
+    Householder QR per charge sector of leg ``fl`` (``_thin_qr``, ``dd_cbe.jl:184-259``; LAPACK
+    geqp3 through scipy, as Julia's ``qr(A, ColumnNorm())``). A direction is kept when its pivot
+    ``|R_kk|`` exceeds ``thr``. The new leg has the arrow ``ref_dir`` (``align_charge``); each kept
+    column's phase makes ``R_kk`` real positive (the gauge both implementations fix)."""
+    import scipy.linalg as sla
+
+    others = [i for i in range(sketch.rank) if i != fl]
+    ydir = sketch.legs[fl].dir
+    groups = {}
+    for key in sorted(sketch.blocks):
+        groups.setdefault(key[fl], []).append(key)
+    out_blocks, space = {}, {}
+    for charge in sorted(groups):
+        keys = groups[charge]
+        mats = [sketch.blocks[k].transpose(others + [fl]).reshape(-1, sketch.blocks[k].shape[fl])
+                for k in keys]
+        stacked = np.vstack(mats)
+        if stacked.shape[0] == 0:
+            continue
+        Q, R, _ = sla.qr(stacked, mode="economic", pivoting=True)
+        dg = np.diag(R)
+        kept = int(np.count_nonzero(np.abs(dg) > thr))
+        if kept == 0:
+            continue
+        ph = np.where(np.abs(dg[:kept]) > 0, dg[:kept] / np.where(dg[:kept] != 0, np.abs(dg[:kept]), 1), 1)
+        Qm = Q[:, :kept] * ph[None, :]
+        qn = charge if ydir == ref_dir else -charge
+        space[qn] = kept
+        row = 0
+        for k, M in zip(keys, mats):
+            nr = M.shape[0]
+            shp = [sketch.blocks[k].shape[i] for i in others] + [kept]
+            blk = Qm[row:row + nr].reshape(shp)
+            row += nr
+            inv = np.argsort(others + [fl])
+            nk = list(k)
+            nk[fl] = qn
+            out_blocks[tuple(nk)] = np.ascontiguousarray(blk.transpose(inv))
+    if not space:
+        return None
+    legs = list(sketch.legs)
+    legs[fl] = B.Leg(ref_dir, dict(sorted(space.items())))
+    return B.BT(legs, out_blocks)
+
+
+def dd_select(frame, sketch, side):
+    """``_dd_select`` (``dd_cbe.jl:290-321``): ``P^D sketch``, a first QR at the floor
+    ``CBE_EPS max(|sketch|, |projected|)``, then a QR of ``P^D`` of the first pass keeping
+    pivots ``>= REORTH_KEEP`` ("twice is enough")."""
+    left = side == "left"
+    fl = 2 if left else 0
+    perp = perp_left if left else perp_right
+    projected = perp(frame, sketch)
+    nz, ny = B.norm(sketch), B.norm(projected)
+    if ny <= CBE_EPS * max(nz, 1.0):
+        return None
+    ref_dir = frame.legs[fl].dir
+    first = thin_qr(projected, fl, ref_dir, CBE_EPS * max(nz, ny))
+    if first is None:
+        return None
+    return thin_qr(perp(frame, first), fl, ref_dir, REORTH_KEEP)
+
+
+def target_sectors(boost: dict, per: dict, Om, wleg: int, alloc) -> int:
+    """``_target_sectors!`` (``sketch.jl:188-201``)."""
+    if not per:
+        return 0
+    have = {} if Om is None else dict(Om.legs[wleg].sectors)
+    share = alloc.sample ** 2 / len(per)
+    n = 0
+    for q, r2 in per.items():
+        if not alloc.scale ** 2 * r2 > share:
+            continue
+        boost[q] = boost.get(q, 0) + max(have.get(q, 0), 1)
+        n += 1
+    return n
+
+
+def record_sample(ledger, side, ind, per, hcols, sketch, wleg, alloc):
+    """``_record_sample!`` (``sketch.jl:215-258``)."""
+    ledger.max_sample = max(ledger.max_sample, ind)
+    if side == "left":
+        ledger.max_sample_l = max(ledger.max_sample_l, ind)
+    else:
+        ledger.max_sample_r = max(ledger.max_sample_r, ind)
+    tot = sum(per.values())
+    relunc = 0.5 * math.sqrt(sum(r2 ** 2 / hcols[q] for q, r2 in per.items())) / tot if tot > 0 else 0.0
+    ledger.sample_log.append(dict(side=side, est=ind, relunc=relunc,
+                                  per={q: alloc.scale * math.sqrt(r2) for q, r2 in per.items()},
+                                  holdout=dict(hcols),
+                                  sketch={} if sketch is None else dict(sketch.legs[wleg].sectors)))
+
+
+def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap, alloc, ledger,
+                  holdout_width=DD_HOLDOUT):
+    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, ``batch_blocks = 1``,
+    ``cap_selection = :storage``, no audit, acceptance factor 1): grows the DD basis block by
+    block until an independent holdout finds the rest within ``alloc.sample``. Returns
+    ``(basis, status)``."""
+    left = side == "left"
+    fl, wleg = (2, 0) if left else (0, 2)
+    st = dict(aug=frame, basis=None, count=0, streamed=0, discovered=0)
+    boost = {}
+
+    def absorb(sketched):
+        nb = dd_select(st["aug"], sketched, side)
+        if nb is None:
+            return 0
+        current = 0 if st["basis"] is None else st["basis"].dim(fl)
+        room = ncap - current
+        if room <= 0:
+            return 0
+        if nb.dim(fl) > room:
+            nb = B.trim_total(nb, fl, room)
+            if nb is None:
+                return 0
+        st["basis"] = nb if st["basis"] is None else B.oplus([st["basis"], nb], fl)
+        st["aug"] = B.oplus([st["aug"], nb], fl)
+        return nb.dim(fl)
+
+    def stream(Om, field):
+        w = Om.dim(wleg)
+        st["streamed"] += w
+        if field == "n_probes":
+            st["discovered"] += w
+        if ledger is not None:
+            setattr(ledger, field, getattr(ledger, field) + w)
+        return sketch(Om)
+
+    def fresh(columns):
+        Om = draw(columns, None)
+        return None if Om is None else (Om, stream(Om, "n_holdout"))
+
+    def resid(check):
+        return sample_residual(st["basis"], project, lambda _: check[1], check[0], wleg, side)
+
+    def newsector():
+        b = st["basis"]
+        return b is not None and any(frame.legs[fl].sectors.get(q, 0) == 0
+                                     for q in b.legs[fl].sectors)
+
+    width = min(max(initial_width, 1), max(min(wcap, ncap), 1))
+    last = draw(width, None)
+    if last is None:
+        return None, "empty"
+    st["count"] += absorb(stream(last, "n_probes"))
+    check = fresh(holdout_width)
+    escalated = False
+    while True:
+        if check is None:
+            return st["basis"], "met"
+        est, per, hcols = resid(check)
+        ind = indicator(alloc, est)
+        ok = ind <= alloc.sample
+        if ok and not escalated and (ind > alloc.sample / 2 or newsector()):
+            escalated = True
+            wide = fresh(2 * holdout_width)
+            if wide is not None:
+                check = wide
+                continue
+        capped = st["discovered"] >= wcap or st["count"] >= ncap
+        if ok or capped:
+            if ledger is not None:
+                record_sample(ledger, side, ind, per, hcols, last, wleg, alloc)
+            if ok:
+                return st["basis"], "met"
+            if ledger is not None:
+                ledger.unmet_("sample")
+                ledger.workcap_reached = True
+            return st["basis"], "work_limited"
+        nt = target_sectors(boost, per, check[0], wleg, alloc)
+        if ledger is not None:
+            ledger.n_targeted += nt
+        next_check = fresh(holdout_width)
+        added = absorb(check[1])
+        if nt == 0:
+            width = min(2 * width, wcap)
+        remaining = ncap - (0 if st["basis"] is None else st["basis"].dim(fl))
+        if remaining > 0:
+            blk = draw(min(width, max(remaining + 2, 1)), boost if boost else None)
+            if blk is not None:
+                last = blk
+                added += absorb(stream(blk, "n_probes"))
+        check = next_check
+        st["count"] += added
+        if added == 0:
+            if ledger is not None:
+                record_sample(ledger, side, ind, per, hcols, last, wleg, alloc)
+                ledger.unmet_("sample")
+            return st["basis"], "basis_limited"
 
 
 @dataclass
@@ -240,10 +457,11 @@ class Expansion:
 
 def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
                   fixed_width=8, tail_factor=0.10, mode="rank_tail") -> Expansion:
-    """Grow one frame of the bond by the DD-projected sketch, rank by tail bisection
-    (``dd_cbe_expand.jl:19-301``)."""
-    if mode != "rank_tail":
-        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail is restated")
+    """Grow one frame of the bond by the DD-projected sketch (``dd_cbe_expand.jl:19-419``): rank
+    by tail bisection (``:rank_tail``, ``tail_dd``) or by the incremental controller
+    (``:adaptive``, ``_dd_controller``)."""
+    if mode not in ("rank_tail", "adaptive"):
+        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail and :adaptive are restated")
     if fixed_width < 1:
         raise ValueError("rank_tail requires positive fixed_width")
     if not 0 < tail_factor <= 1:
@@ -282,9 +500,19 @@ def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, wor
         def project(b):
             return perp_right(V0, b)
 
-    # tail_dd
-    Om = dd_probe(opp, oside, min(fixed_width, full_opp), rng)
     directions, direction_count = None, 0
+    if mode == "adaptive":
+        dmax = max(U0.dim(0), old_rank, V0.dim(2))
+        initial_width = math.ceil(1.2 * max(math.ceil(ADAPTIVE_GROWTH * dmax) - old_rank, 1))
+        wcap = full_opp
+        if alloc is not None and workcap > 0:
+            wcap = min(wcap, workcap)
+        directions, _ = dd_controller(frame, side, lambda w, bst: dd_probe(opp, oside, w, rng, bst),
+                                      sketch, project, initial_width, wcap, cap, alloc, ledger)
+        direction_count = 0 if directions is None else directions.dim(fl)
+        Om = None
+    else:  # tail_dd
+        Om = dd_probe(opp, oside, min(fixed_width, full_opp), rng)
     if Om is not None:
         if ledger is not None:
             ledger.n_probes += Om.dim(wleg)
