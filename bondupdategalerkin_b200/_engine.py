@@ -45,6 +45,8 @@ SIGNATURES = {
     "bug_svd": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.c_double, ctypes.c_int,
                                ctypes.POINTER(_vp), ctypes.POINTER(_vp), _c_double_p, _c_int_p,
                                ctypes.c_int, _c_int_p, _c_int_p]),
+    "bug_thin_qr": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                   ctypes.POINTER(_vp)]),
     "bug_scale_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_double_p, ctypes.POINTER(_vp)]),
     "bug_norm2": (ctypes.c_int, [_vp, _vp, _c_double_p]),
     "bug_inner": (ctypes.c_int, [_vp, _vp, _vp, _c_double_p]),

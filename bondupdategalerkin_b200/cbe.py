@@ -1,4 +1,4 @@
-"""DD-QR controlled bond expansion on device tensors (``mode = :rank_tail``).
+"""DD-QR controlled bond expansion on device tensors (``mode = :rank_tail`` and ``:adaptive``).
 
 The sketch, projections, SVD candidates and Test B estimates all run in the engine; only the
 Gaussian probe is drawn on the host (from the step's seeded generator, in a fixed order) and
@@ -11,7 +11,10 @@ uploaded. Follows:
   ``sector_graded_sketch(...; comp_ratio = nothing)`` (``sketch.jl:14-54``), ``_sample_residual``
   (``sketch.jl:141-180``), ``sampled_leak`` (``cbe.jl:355-391``), ``_fold_sketch_closures``
   (``cbe.jl:62-144``);
-* ``dd_cbe_expand`` with its default ``tail_dd`` branch (``dd_cbe_expand.jl:19-301,383-419``).
+* ``dd_cbe_expand`` with its default ``tail_dd`` branch (``dd_cbe_expand.jl:19-301,383-419``) and
+  its ``:adaptive`` branch: ``_dd_controller`` (``dd_cbe_controller.jl:26-212``), ``_dd_select`` and
+  ``_thin_qr`` (``dd_cbe.jl:184-321``, the pivoted QR on device: ``tensor.thin_qr``),
+  ``_target_sectors!`` / ``_record_sample!`` (``sketch.jl:188-258``), ``_boost!`` (``cbe.jl:206-216``).
 
 A right frame's bond leg is incoming; an SVD over ``(site, link_r)`` returns that leg outgoing, so
 the orthonormal rows are re-expressed on an incoming leg (:func:`rows_from_u`) before they join a
@@ -26,7 +29,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import tensor as B
-from .budget import indicator
+from .budget import ADAPTIVE_GROWTH, indicator
 from .env import stream_left, stream_right
 
 EPS = 2.220446049250313e-16
@@ -116,13 +119,31 @@ def alloc_columns(dims: dict, budget: int) -> dict:
     return {q: min(d, math.ceil(d / tot * budget)) for q, d in dims.items()}
 
 
-def dd_probe(opp, oside, width, rng):
-    """Sector-graded Gaussian probe in ``opp``'s discarded space (``dd_cbe.jl:132-161``)."""
+def boost_columns(cols: dict, boost: dict, cap: dict) -> dict:
+    """``_boost!`` (``cbe.jl:206-216``): raise targeted sectors' columns, capped by ``cap``;
+    returns what did not fit."""
+    left = {}
+    for q, extra in boost.items():
+        if q not in cap:
+            continue
+        have = cols.get(q, 0)
+        add = min(max(extra, 0), max(cap[q] - have, 0))
+        cols[q] = have + add
+        if extra > add:
+            left[q] = extra - add
+    return left
+
+
+def dd_probe(opp, oside, width, rng, boost=None):
+    """Sector-graded Gaussian probe in ``opp``'s discarded space (``dd_cbe.jl:132-161``), with the
+    targeted sectors' extra columns when ``boost`` is given."""
     dfull, dT = fused_dims(opp, oside)
     dC = {c: max(dfull[c] - dT[c], 0) for c in dfull}
     if sum(dC.values()) == 0:
         return None
     cols = alloc_columns(dC, width)
+    if boost:
+        boost_columns(cols, boost, dC)
     if oside == "left":
         om = B.gaussian_fused(rng, opp.legs[0], opp.legs[1], cols, new_first=False)
     else:
@@ -174,6 +195,159 @@ def sample_residual(basis, project, sketch, Om, wleg, side):
         rq = B.trim_per_sector(residual, rleg, {q: d}) if len(residual.legs[rleg].sectors) > 1 else residual
         per[q] = (B.norm(rq) ** 2 if rq is not None else 0.0) / nq
     return math.sqrt(sum(per.values())), per, cols
+
+
+DD_HOLDOUT = 4  # ``_DD_HOLDOUT`` (dd_cbe_controller.jl:12)
+
+
+def dd_select(frame, sketch, side):
+    """``_dd_select`` (``dd_cbe.jl:290-321``): ``P^D sketch``, a first pivoted QR at the floor
+    ``CBE_EPS max(|sketch|, |projected|)``, then a pivoted QR of ``P^D`` of the first pass keeping
+    pivots above ``REORTH_KEEP``."""
+    left = side == "left"
+    fl = 2 if left else 0
+    perp = perp_left if left else perp_right
+    projected = perp(frame, sketch)
+    nz, ny = B.norm(sketch), B.norm(projected)
+    if ny <= CBE_EPS * max(nz, 1.0):
+        return None
+    ref_dir = frame.legs[fl].dir
+    first = B.thin_qr(projected, fl, ref_dir, CBE_EPS * max(nz, ny))
+    if first is None:
+        return None
+    return B.thin_qr(perp(frame, first), fl, ref_dir, REORTH_KEEP)
+
+
+def target_sectors(boost: dict, per: dict, Om, wleg: int, alloc) -> int:
+    """``_target_sectors!`` (``sketch.jl:188-201``)."""
+    if not per:
+        return 0
+    have = {} if Om is None else dict(Om.legs[wleg].sectors)
+    share = alloc.sample ** 2 / len(per)
+    n = 0
+    for q, r2 in per.items():
+        if not alloc.scale ** 2 * r2 > share:
+            continue
+        boost[q] = boost.get(q, 0) + max(have.get(q, 0), 1)
+        n += 1
+    return n
+
+
+def record_sample(ledger, side, ind, per, hcols, sketch, wleg, alloc):
+    """``_record_sample!`` (``sketch.jl:215-258``)."""
+    ledger.max_sample = max(ledger.max_sample, ind)
+    if side == "left":
+        ledger.max_sample_l = max(ledger.max_sample_l, ind)
+    else:
+        ledger.max_sample_r = max(ledger.max_sample_r, ind)
+    tot = sum(per.values())
+    relunc = 0.5 * math.sqrt(sum(r2 ** 2 / hcols[q] for q, r2 in per.items())) / tot if tot > 0 else 0.0
+    ledger.sample_log.append(dict(side=side, est=ind, relunc=relunc,
+                                  per={q: alloc.scale * math.sqrt(r2) for q, r2 in per.items()},
+                                  holdout=dict(hcols),
+                                  sketch={} if sketch is None else dict(sketch.legs[wleg].sectors)))
+
+
+def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap, alloc, ledger,
+                  holdout_width=DD_HOLDOUT):
+    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, ``batch_blocks = 1``,
+    ``cap_selection = :storage``, no audit, acceptance factor 1): grows the DD basis block by
+    block until an independent holdout finds the rest within ``alloc.sample``. Returns
+    ``(basis, status)``; the probe draws come in the reference's order (first block, its holdout,
+    then per round the next holdout before the next block)."""
+    left = side == "left"
+    fl, wleg = (2, 0) if left else (0, 2)
+    aug, basis = frame, None
+    count = discovered = 0
+    boost = {}
+
+    def basis_dim():
+        return 0 if basis is None else basis.dim(fl)
+
+    def absorb(sketched):
+        nonlocal aug, basis
+        nb = dd_select(aug, sketched, side)
+        if nb is None:
+            return 0
+        room = ncap - basis_dim()
+        if room <= 0:
+            return 0
+        if nb.dim(fl) > room:
+            nb = B.trim_total(nb, fl, room)
+            if nb is None:
+                return 0
+        basis = nb if basis is None else B.oplus([basis, nb], fl)
+        aug = B.oplus([aug, nb], fl)
+        return nb.dim(fl)
+
+    def stream(Om, probe):
+        nonlocal discovered
+        w = Om.dim(wleg)
+        if probe:
+            discovered += w
+            if ledger is not None:
+                ledger.n_probes += w
+        elif ledger is not None:
+            ledger.n_holdout += w
+        return sketch(Om)
+
+    def fresh(columns):
+        Om = draw(columns, None)
+        return None if Om is None else (Om, stream(Om, False))
+
+    def newsector():
+        return basis is not None and any(frame.legs[fl].sectors.get(q, 0) == 0
+                                         for q in basis.legs[fl].sectors)
+
+    width = min(max(initial_width, 1), max(min(wcap, ncap), 1))
+    last = draw(width, None)
+    if last is None:
+        return None, "empty"
+    count += absorb(stream(last, True))
+    check = fresh(holdout_width)
+    escalated = False
+    while True:
+        if check is None:
+            return basis, "met"
+        est, per, hcols = sample_residual(basis, project, lambda _: check[1], check[0], wleg, side)
+        ind = indicator(alloc, est)
+        ok = ind <= alloc.sample
+        if ok and not escalated and (ind > alloc.sample / 2 or newsector()):
+            escalated = True
+            wide = fresh(2 * holdout_width)
+            if wide is not None:
+                check = wide
+                continue
+        capped = discovered >= wcap or count >= ncap
+        if ok or capped:
+            if ledger is not None:
+                record_sample(ledger, side, ind, per, hcols, last, wleg, alloc)
+            if ok:
+                return basis, "met"
+            if ledger is not None:
+                ledger.unmet_("sample")
+                ledger.workcap_reached = True
+            return basis, "work_limited"
+        nt = target_sectors(boost, per, check[0], wleg, alloc)
+        if ledger is not None:
+            ledger.n_targeted += nt
+        next_check = fresh(holdout_width)
+        added = absorb(check[1])
+        if nt == 0:
+            width = min(2 * width, wcap)
+        remaining = ncap - basis_dim()
+        if remaining > 0:
+            blk = draw(min(width, max(remaining + 2, 1)), boost if boost else None)
+            if blk is not None:
+                last = blk
+                added += absorb(stream(blk, True))
+        check = next_check
+        count += added
+        if added == 0:
+            if ledger is not None:
+                record_sample(ledger, side, ind, per, hcols, last, wleg, alloc)
+                ledger.unmet_("sample")
+            return basis, "basis_limited"
 
 
 @dataclass
@@ -233,10 +407,11 @@ class Expansion:
 
 def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
                   fixed_width=8, tail_factor=0.10, mode="rank_tail") -> Expansion:
-    """Grow one frame of the bond by the DD-projected sketch, rank by tail bisection
-    (``dd_cbe_expand.jl:19-301``)."""
-    if mode != "rank_tail":
-        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail is restated")
+    """Grow one frame of the bond by the DD-projected sketch (``dd_cbe_expand.jl:19-419``): rank
+    by tail bisection (``:rank_tail``, ``tail_dd``) or by the incremental controller
+    (``:adaptive``, ``_dd_controller``)."""
+    if mode not in ("rank_tail", "adaptive"):
+        raise NotImplementedError(f"DD mode {mode!r}: :rank_tail and :adaptive are built")
     if fixed_width < 1:
         raise ValueError("rank_tail requires positive fixed_width")
     if not 0 < tail_factor <= 1:
@@ -275,9 +450,19 @@ def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, wor
         def project(b):
             return perp_right(V0, b)
 
-    # tail_dd
-    Om = dd_probe(opp, oside, min(fixed_width, full_opp), rng)
     directions, direction_count = None, 0
+    if mode == "adaptive":
+        dmax = max(U0.dim(0), old_rank, V0.dim(2))
+        initial_width = math.ceil(1.2 * max(math.ceil(ADAPTIVE_GROWTH * dmax) - old_rank, 1))
+        wcap = full_opp
+        if alloc is not None and workcap > 0:
+            wcap = min(wcap, workcap)
+        directions, _ = dd_controller(frame, side, lambda w, bst: dd_probe(opp, oside, w, rng, bst),
+                                      sketch, project, initial_width, wcap, cap, alloc, ledger)
+        direction_count = 0 if directions is None else directions.dim(fl)
+        Om = None
+    else:  # tail_dd
+        Om = dd_probe(opp, oside, min(fixed_width, full_opp), rng)
     if Om is not None:
         if ledger is not None:
             ledger.n_probes += Om.dim(wleg)

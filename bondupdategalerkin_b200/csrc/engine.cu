@@ -669,6 +669,164 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
   return BUG_OK;
 }
 
+// ── column-pivoted thin QR per charge sector of one leg ────────────────────────────────────
+
+// Orthonormal basis of the span of `t`'s leg-`fl` columns (``_thin_qr``, dd_cbe.jl:184-259): per
+// charge sector of leg `fl`, the sector's blocks stacked row-wise (blocks in ascending key order,
+// rows = the other legs in C order, columns = leg `fl`), a column-pivoted Householder QR on
+// device, and the leading Q columns whose |R_kk| exceeds `thr`. The new leg has arrow `ref_dir`;
+// its charges keep the flux (negated when the arrow flips). nullptr when nothing is kept.
+TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, double thr) {
+  require(fl >= 0 && fl < t.rank && (ref_dir == 1 || ref_dir == -1), "thin_qr: bad leg or arrow");
+  const Leg& F = t.legs[fl];
+  std::map<int, std::vector<int>> groups;  // charge on fl -> block indices (ascending keys)
+  for (int bi = 0; bi < int(t.blocks.size()); ++bi) groups[t.blocks[bi].key[fl]].push_back(bi);
+  struct Sec {
+    int charge;
+    int64_t m = 0, n = 0, woff = 0, qoff = 0, roff = 0;
+    std::vector<int64_t> row_of;  // row offset of each block of the sector
+  };
+  std::vector<Sec> secs;
+  int64_t wtot = 0, rtot = 0;
+  for (auto& kv : groups) {
+    Sec sc;
+    sc.charge = kv.first;
+    sc.n = F.dim_of(kv.first);
+    for (int bi : kv.second) {
+      sc.row_of.push_back(sc.m);
+      sc.m += t.blocks[bi].size / std::max<int64_t>(sc.n, 1);
+    }
+    if (sc.m == 0 || sc.n == 0) continue;
+    require(sc.n <= 1024, "thin_qr: a sector wider than 1024 columns");
+    const int64_t kq = std::min(sc.m, sc.n);
+    sc.woff = wtot;
+    wtot += sc.m * sc.n;
+    sc.qoff = wtot;
+    wtot += sc.m * kq;
+    sc.roff = rtot;
+    rtot += kq;
+    secs.push_back(sc);
+  }
+  if (secs.empty()) return nullptr;
+  double2* W = static_cast<double2*>(c->scratch(size_t(wtot) * sizeof(double2)));
+  double* host = c->readback(size_t(rtot) + 1);
+  // strides of an element of a block inside its sector matrix (column-major m x n): the other
+  // legs in C order give the row, leg fl the column
+  auto matrix_strides = [&](const Block& b, int64_t m, std::array<int64_t, BUG_MAX_RANK>& st) {
+    int64_t acc = 1;
+    for (int l = t.rank - 1; l >= 0; --l) {
+      if (l == fl) continue;
+      st[l] = acc;
+      acc *= b.shape[l];
+    }
+    st[fl] = m;
+  };
+  std::vector<QrDesc> qd;
+  std::vector<CopyDesc> packs;
+  std::map<int, int> sec_of;
+  for (size_t s2 = 0; s2 < secs.size(); ++s2) {
+    Sec& sc = secs[s2];
+    sec_of[sc.charge] = int(s2);
+    QrDesc d{};
+    d.work = W + sc.woff;
+    d.Q = W + sc.qoff;
+    d.rdiag_host = host + sc.roff;
+    d.m = int(sc.m);
+    d.n = int(sc.n);
+    d.pack_begin = int(packs.size());
+    const auto& bis = groups[sc.charge];
+    for (size_t j = 0; j < bis.size(); ++j) {
+      const Block& b = t.blocks[bis[j]];
+      std::array<int64_t, BUG_MAX_RANK> ms{};
+      matrix_strides(b, sc.m, ms);
+      auto ss = c_strides(b.shape, t.rank);
+      CopyDesc cd{};
+      cd.src = t.data(bis[j]);
+      cd.dst = d.work + sc.row_of[j];
+      cd.n = b.size;
+      cd.ndim = t.rank;
+      cd.alpha = make_double2(1.0, 0.0);
+      cd.wdim = -1;
+      for (int l = 0; l < t.rank; ++l) {
+        cd.dims[l] = b.shape[l];
+        cd.sstr[l] = ss[l];
+        cd.dstr[l] = ms[l];
+      }
+      packs.push_back(cd);
+    }
+    d.pack_end = int(packs.size());
+    qd.push_back(d);
+  }
+  QrDesc* dq = c->push(qd);
+  CopyDesc* dp = c->push(packs);
+  const bugk::Blob blob = c->begin();
+  bugk::launch_qr(blob, dq, int(qd.size()), dp, c->stream);
+  double qflops = 0.0;
+  for (auto& sc : secs) qflops += 8.0 * 2.0 * double(sc.m) * double(sc.n) * double(std::min(sc.m, sc.n));
+  c->launched(BUG_K_SVD, qflops, 0.0);
+  c->wait();
+  // ranks, the new leg, the output tensor
+  Leg NL;
+  NL.dir = ref_dir;
+  std::vector<int> kept(secs.size(), 0);
+  std::map<int, int> dims;
+  for (size_t s2 = 0; s2 < secs.size(); ++s2) {
+    const Sec& sc = secs[s2];
+    const int64_t kq = std::min(sc.m, sc.n);
+    int k = 0;
+    for (int64_t j = 0; j < kq; ++j) k += host[sc.roff + j] > thr ? 1 : 0;
+    kept[s2] = k;
+    if (k > 0) dims[F.dir == ref_dir ? sc.charge : -sc.charge] = k;
+  }
+  if (dims.empty()) return nullptr;
+  for (auto& kv : dims) {
+    NL.q.push_back(kv.first);
+    NL.d.push_back(kv.second);
+  }
+  std::vector<Leg> legs = t.legs;
+  legs[fl] = NL;
+  std::vector<Key> keys;
+  for (auto& b : t.blocks) {
+    const int s2 = sec_of.count(b.key[fl]) ? sec_of[b.key[fl]] : -1;
+    if (s2 < 0 || kept[s2] == 0) continue;
+    Key k = b.key;
+    k[fl] = F.dir == ref_dir ? b.key[fl] : -b.key[fl];
+    keys.push_back(k);
+  }
+  auto out = make_tensor(c, t.rank, legs, keys, false);
+  std::vector<CopyDesc> copies;
+  for (size_t s2 = 0; s2 < secs.size(); ++s2) {
+    const Sec& sc = secs[s2];
+    if (kept[s2] == 0) continue;
+    const auto& bis = groups[sc.charge];
+    for (size_t j = 0; j < bis.size(); ++j) {
+      const Block& b = t.blocks[bis[j]];
+      Key k = b.key;
+      k[fl] = F.dir == ref_dir ? b.key[fl] : -b.key[fl];
+      const int ob = out->find(k);
+      const Block& o = out->blocks[ob];
+      std::array<int64_t, BUG_MAX_RANK> ms{};
+      matrix_strides(b, sc.m, ms);
+      auto ds = c_strides(o.shape, t.rank);
+      CopyDesc cd{};
+      cd.src = W + sc.qoff + sc.row_of[j];
+      cd.dst = out->mdata(ob);
+      cd.n = o.size;
+      cd.ndim = t.rank;
+      cd.alpha = make_double2(1.0, 0.0);
+      cd.wdim = -1;
+      for (int l = 0; l < t.rank; ++l) {
+        cd.dims[l] = o.shape[l];
+        cd.sstr[l] = ms[l];
+        cd.dstr[l] = ds[l];
+      }
+      copies.push_back(cd);
+    }
+  }
+  run_copies(c, copies);
+  return out;
+}
+
 // ── reductions and linear combinations ───────────────────────────────────────────────────────
 
 constexpr int64_t kDotChunk = 16384;
@@ -1247,6 +1405,13 @@ int bug_contract(bug_ctx* c, const bug_tensor* a, int n, const int* ia, const bu
   return guard([&] {
     require(c && a && b && out, "null argument");
     *out = contract_impl(c, *a, n, ia, *b, ib, conja != 0, conjb != 0).release();
+  });
+}
+
+int bug_thin_qr(bug_ctx* c, const bug_tensor* t, int leg, int ref_dir, double thr, bug_tensor** out) {
+  return guard([&] {
+    require(c && t && out, "null argument");
+    *out = thin_qr_impl(c, *t, leg, ref_dir, thr).release();
   });
 }
 

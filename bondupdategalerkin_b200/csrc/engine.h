@@ -33,6 +33,7 @@ using bugk::GemmPair;
 using bugk::GemmTile;
 using bugk::LinOut;
 using bugk::LinSrc;
+using bugk::QrDesc;
 using bugk::ScaleDesc;
 using bugk::SvdDesc;
 
@@ -392,6 +393,7 @@ void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_t
           double* out_re_im);
 TensorPtr lincomb_impl(bug_ctx* c, int n, const double* coef, const bug_tensor* const* ts);
 std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg);
+TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, double thr);
 TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& t, int leg, const double* w);
 TensorPtr conj_impl(bug_ctx* c, const bug_tensor& t);
 TensorPtr flip_leg_impl(bug_ctx* c, const bug_tensor& t, int leg);

@@ -566,6 +566,158 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS
   }
 }
 
+// ── column-pivoted Householder QR (thin, per charge sector) ────────────────────────────────
+// Step k: the remaining column (index >= k) with the largest norm over rows k..m-1 is swapped to
+// position k (ties: the lowest index); its Householder reflector H_k = I - tau v v^H (v_k = 1,
+// beta real, as LAPACK's zlarfg) zeroes it below the diagonal; H_k^H is applied to the columns
+// right of k. Q = H_0 ... H_{kq-1} restricted to its first kq columns, each column scaled by
+// sign(beta) so that R_kk >= 0.
+
+constexpr int kQrMaxN = 1024;
+
+template <int N>
+__global__ void __launch_bounds__(kThreads) qr_kernel(BUG_BLOB_PARAMS(N), const QrDesc* descs,
+                                                      const CopyDesc* packs) {
+  const Rebase rb{pb.b, arena, nb};
+  descs = rb(descs);
+  packs = rb(packs);
+  __shared__ double norms[kQrMaxN];
+  __shared__ double2 tau[kQrMaxN];
+  __shared__ double beta[kQrMaxN];
+  __shared__ int pivot;
+  __shared__ double xn2;
+  const QrDesc d = descs[blockIdx.x];
+  const int m = d.m, n = d.n, kq = m < n ? m : n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  if (kq <= 0 || n > kQrMaxN) return;
+  for (int pk = d.pack_begin; pk < d.pack_end; ++pk) {  // gather the sector matrix
+    const CopyDesc& c = packs[pk];
+    for (int64_t e = tid; e < c.n; e += blockDim.x) {
+      int64_t rr = e, so = 0, dof = 0;
+      for (int k = c.ndim - 1; k >= 0; --k) {
+        const int64_t i = rr % c.dims[k];
+        rr /= c.dims[k];
+        so += i * c.sstr[k];
+        dof += i * c.dstr[k];
+      }
+      c.dst[dof] = c.src[so];
+    }
+  }
+  __syncthreads();
+  double2* A = d.work;
+  for (int k = 0; k < kq; ++k) {
+    for (int j = k + warp; j < n; j += nwarps) {  // remaining column norms
+      const double2* aj = A + int64_t(j) * m;
+      double s2 = 0.0;
+      for (int i = k + lane; i < m; i += 32) s2 = fma(aj[i].x, aj[i].x, fma(aj[i].y, aj[i].y, s2));
+      s2 = warp_sum(s2);
+      if (lane == 0) norms[j] = s2;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int p = k;
+      for (int j = k + 1; j < n; ++j)
+        if (norms[j] > norms[p]) p = j;
+      pivot = p;
+    }
+    __syncthreads();
+    const int p = pivot;
+    if (p != k)
+      for (int i = tid; i < m; i += blockDim.x) {
+        const double2 t = A[int64_t(k) * m + i];
+        A[int64_t(k) * m + i] = A[int64_t(p) * m + i];
+        A[int64_t(p) * m + i] = t;
+      }
+    __syncthreads();
+    double2* ak = A + int64_t(k) * m;
+    if (warp == 0) {
+      double s2 = 0.0;
+      for (int i = k + 1 + lane; i < m; i += 32) s2 = fma(ak[i].x, ak[i].x, fma(ak[i].y, ak[i].y, s2));
+      s2 = warp_sum(s2);
+      if (lane == 0) xn2 = s2;
+    }
+    __syncthreads();
+    const double2 alpha = ak[k];
+    double bt, tr, ti;
+    double2 scale = make_double2(0.0, 0.0);
+    if (xn2 == 0.0 && alpha.y == 0.0) {
+      bt = alpha.x;
+      tr = 0.0;
+      ti = 0.0;
+    } else {
+      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+      bt = alpha.x >= 0.0 ? -nrm : nrm;
+      tr = (bt - alpha.x) / bt;
+      ti = -alpha.y / bt;
+      const double2 den = make_double2(alpha.x - bt, alpha.y);  // 1 / (alpha - beta)
+      const double dd = den.x * den.x + den.y * den.y;
+      scale = make_double2(den.x / dd, -den.y / dd);
+    }
+    __syncthreads();
+    if (!(tr == 0.0 && ti == 0.0)) {
+      for (int i = k + 1 + tid; i < m; i += blockDim.x) ak[i] = cmul(ak[i], scale);
+    }
+    if (tid == 0) {
+      tau[k] = make_double2(tr, ti);
+      beta[k] = bt;
+    }
+    __syncthreads();
+    if (!(tr == 0.0 && ti == 0.0)) {
+      // A_j -= conj(tau) v (v^H A_j), j > k
+      const double2 ctau = make_double2(tr, -ti);
+      for (int j = k + 1 + warp; j < n; j += nwarps) {
+        double2* aj = A + int64_t(j) * m;
+        double wr = 0.0, wi = 0.0;
+        for (int i = k + lane; i < m; i += 32) {
+          const double2 v = i == k ? make_double2(1.0, 0.0) : ak[i];
+          const double2 x = aj[i];
+          wr = fma(v.x, x.x, fma(v.y, x.y, wr));
+          wi = fma(v.x, x.y, fma(-v.y, x.x, wi));
+        }
+        wr = warp_sum(wr);
+        wi = warp_sum(wi);
+        const double2 f = cmul(ctau, make_double2(wr, wi));
+        for (int i = k + lane; i < m; i += 32) {
+          const double2 v = i == k ? make_double2(1.0, 0.0) : ak[i];
+          const double2 fv = cmul(v, f);
+          aj[i] = make_double2(aj[i].x - fv.x, aj[i].y - fv.y);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // Q columns: q_c = H_0 ... H_{kq-1} e_c, scaled by sign(beta_c)
+  for (int c = warp; c < kq; c += nwarps) {
+    double2* q = d.Q + int64_t(c) * m;
+    for (int i = lane; i < m; i += 32) q[i] = make_double2(i == c ? 1.0 : 0.0, 0.0);
+    __syncwarp();
+    for (int k = (c < kq - 1 ? c : kq - 1); k >= 0; --k) {  // H_k e_c = e_c for k > c
+      const double2 t = tau[k];
+      if (t.x == 0.0 && t.y == 0.0) continue;
+      const double2* vk = A + int64_t(k) * m;
+      double wr = 0.0, wi = 0.0;
+      for (int i = k + lane; i < m; i += 32) {
+        const double2 v = i == k ? make_double2(1.0, 0.0) : vk[i];
+        const double2 x = q[i];
+        wr = fma(v.x, x.x, fma(v.y, x.y, wr));
+        wi = fma(v.x, x.y, fma(-v.y, x.x, wi));
+      }
+      wr = warp_sum(wr);
+      wi = warp_sum(wi);
+      const double2 f = cmul(t, make_double2(wr, wi));
+      for (int i = k + lane; i < m; i += 32) {
+        const double2 v = i == k ? make_double2(1.0, 0.0) : vk[i];
+        const double2 fv = cmul(v, f);
+        q[i] = make_double2(q[i].x - fv.x, q[i].y - fv.y);
+      }
+      __syncwarp();
+    }
+    const double sg = beta[c] < 0.0 ? -1.0 : 1.0;
+    for (int i = lane; i < m; i += 32) q[i] = make_double2(q[i].x * sg, q[i].y * sg);
+    if (lane == 0) d.rdiag_host[c] = fabs(beta[c]);
+  }
+}
+
 }  // namespace
 
 // Launch KERNEL<N> with the smallest parameter block that holds the launch's descriptors, or the
@@ -637,6 +789,14 @@ void launch_stage(const Blob& b, const Stage& st, cudaStream_t s) {
   stage_kernel<NB><<<grid, kThreads, 0, s>>>(P, b.arena, (NBYTES), st)
   BUG_WITH_BLOB(b, BUG_STAGE_LAUNCH);
 #undef BUG_STAGE_LAUNCH
+}
+
+void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, cudaStream_t s) {
+  if (nprob <= 0) return;
+#define BUG_QR_LAUNCH(NB, P, NBYTES) \
+  qr_kernel<NB><<<nprob, kThreads, 0, s>>>(P, b.arena, (NBYTES), d_desc, packs)
+  BUG_WITH_BLOB(b, BUG_QR_LAUNCH);
+#undef BUG_QR_LAUNCH
 }
 
 namespace {

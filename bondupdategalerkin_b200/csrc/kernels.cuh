@@ -89,6 +89,18 @@ struct SvdDesc {
   int pack_begin, pack_end;  // gather descriptors that assemble `work` from the tensor's blocks
 };
 
+// One charge sector of a column-pivoted thin QR: `work` (m x n, column-major) is gathered from the
+// tensor's blocks by packs [pack_begin, pack_end), overwritten by the reflectors; `Q` receives the
+// first kq = min(m, n) columns of Q (column-major, m x kq), each with the phase that makes R_kk
+// real non-negative; `rdiag_host` (host-mapped) receives |R_kk|.
+struct QrDesc {
+  double2* work;
+  double2* Q;
+  double* rdiag_host;
+  int m, n;
+  int pack_begin, pack_end;
+};
+
 struct DotDesc {
   const double2* a;
   const double2* b;
@@ -159,6 +171,8 @@ constexpr int kStageThreads = 256;
 int stage_items(const Stage& s);
 int stage_grid_limit();
 void launch_stage(const Blob& b, const Stage& st, cudaStream_t s);
+// Column-pivoted Householder QR, one CTA per sector (see QrDesc).
+void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, cudaStream_t s);
 // Dynamic shared memory the SVD kernel may use per CTA on this device (opt-in maximum minus its
 // static arrays).
 int svd_smem_limit();

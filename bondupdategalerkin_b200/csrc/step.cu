@@ -6,7 +6,8 @@
 // rank decisions need, and no interpreter overhead. The step follows the reference in order:
 //   cbe_bug_step!            src/BUG/TimeEvolution/bug_step.jl:17-513
 //   _half_left!/_half_right! src/BUG/Core/Sweeps/half_sweeps.jl:218-410
-//   dd_cbe_expand (tail_dd)  src/BUG/Randomised/dd_cbe_expand.jl:19-301
+//   dd_cbe_expand            src/BUG/Randomised/dd_cbe_expand.jl:19-419 (:rank_tail, :adaptive)
+//   _dd_controller           src/BUG/Randomised/dd_cbe_controller.jl:26-212
 //   _krylov_enrich           src/BUG/Core/RankAdaptation/krylov_enrichment.jl:58-307
 //   lanczos/arnoldi chains   krylov_lanczos.jl:18-71, krylov_arnoldi.jl:13-58
 //   _single_pass_closure!    krylov_closure_loop.jl:203-281, frontier_closure.jl:42-222,
@@ -42,6 +43,9 @@ constexpr int TAIL_NODES = 8;
 constexpr double EXPV_SHIFT_TRIGGER = 30.0;
 constexpr double EXPV_MAX_NORM = 1e150;
 constexpr double FRONTIER_FLOOR = 1e-14;
+constexpr double REORTH_KEEP = 0.70710678118654752440;  // _REORTH_KEEP, dd_cbe.jl:273
+constexpr int DD_HOLDOUT = 4;                             // _DD_HOLDOUT, dd_cbe_controller.jl:12
+constexpr double ADAPTIVE_GROWTH = 1.2;                   // basis_budget.jl:565
 
 enum Unmet { U_SAMPLE = 0, U_TAIL, U_KRYLOV, U_TRUNC, U_PROJECTION, U_EXPV, U_CLOSURE };
 
@@ -137,6 +141,16 @@ struct Eng {
       data.insert(data.end(), kv.second.begin(), kv.second.end());
     }
     return sh(upload_impl(c, rank, legs, keys, reinterpret_cast<const double*>(data.data())));
+  }
+  // pivoted thin QR basis of the leg-`leg` columns per sector (engine: bug_thin_qr), or null
+  T thin_qr(const T& t, int leg, int ref_dir, double thr) const {
+    auto r = thin_qr_impl(c, *t, leg, ref_dir, thr);
+    return r ? sh(std::move(r)) : nullptr;
+  }
+  std::pair<double, double> norms(const T& a, const T& b) const {
+    double r[4];
+    dots(c, {{a.get(), a.get()}, {b.get(), b.get()}}, r);
+    return {std::sqrt(std::max(r[0], 0.0)), std::sqrt(std::max(r[2], 0.0))};
   }
   std::vector<cd> complex_normals(int64_t n) const {
     std::vector<double> x(static_cast<size_t>(2 * n));
@@ -527,7 +541,22 @@ T gaussian_fused(const Eng& e, const Leg& la, const Leg& lb, const std::map<int,
   return e.upload(3, legs, blocks);
 }
 
-T dd_probe(const Eng& e, const T& opp, bool oleft, int width) {
+// _boost! (cbe.jl:206-216): raise the targeted sectors' columns, capped by the room `cap`
+void boost_columns(std::map<int, int>& cols, const std::map<int, int64_t>& boost,
+                   const std::map<int, int64_t>& cap) {
+  for (auto& kv : boost) {
+    auto ci = cap.find(kv.first);
+    if (ci == cap.end()) continue;
+    const int64_t have = cols.count(kv.first) ? cols[kv.first] : 0;
+    const int64_t add = std::min<int64_t>(std::max<int64_t>(kv.second, 0),
+                                          std::max<int64_t>(ci->second - have, 0));
+    cols[kv.first] = int(have + add);
+  }
+}
+
+// sector-graded Gaussian probe in the opposite frame's discarded space (dd_cbe.jl:132-161)
+T dd_probe(const Eng& e, const T& opp, bool oleft, int width,
+           const std::map<int, int64_t>* boost = nullptr) {
   Fused f = fused_dims(opp, oleft);
   std::map<int, int64_t> dC;
   int64_t tot = 0;
@@ -537,6 +566,7 @@ T dd_probe(const Eng& e, const T& opp, bool oleft, int width) {
   }
   if (tot == 0) return nullptr;
   auto cols = alloc_columns(dC, width);
+  if (boost && !boost->empty()) boost_columns(cols, *boost, dC);
   T om = oleft ? gaussian_fused(e, opp->legs[0], opp->legs[1], cols, false)
                : gaussian_fused(e, opp->legs[1], opp->legs[2], cols, true);
   if (!om) return nullptr;
@@ -578,6 +608,71 @@ double sample_residual(const Eng& e, const T& basis, const std::function<T(const
   return std::sqrt(tot);
 }
 
+// Test B with one fixed, already sketched holdout (sketch.jl:141-180), per sector: `est`, the
+// per-sector residual share r2 = |residual_q|^2 / holdout columns_q, and the holdout columns.
+struct TestB {
+  double est = 0.0;
+  std::map<int, double> per;
+  std::map<int, int> cols;
+};
+
+TestB sample_residual_sectors(const Eng& e, const T& basis, const std::function<T(const T&)>& project,
+                              const T& sketched, const T& Om, int wleg, bool left) {
+  TestB r;
+  if (!Om) return r;
+  for (size_t s = 0; s < Om->legs[wleg].q.size(); ++s)
+    if (Om->legs[wleg].d[s] > 0) r.cols[Om->legs[wleg].q[s]] = Om->legs[wleg].d[s];
+  if (r.cols.empty() || !sketched) return r;
+  T res = project(sketched);
+  if (e.norm(res) <= CBE_EPS) return r;
+  if (basis) res = project(left ? perp_left(e, basis, res) : perp_right(e, basis, res));
+  const int rleg = left ? 2 : 0;
+  const Leg& rl = res->legs[rleg];
+  const std::vector<double> n2 = sector_norms2(e.c, *res, rleg);
+  double tot = 0.0;
+  for (size_t s = 0; s < rl.q.size(); ++s) {
+    if (rl.d[s] <= 0) continue;
+    auto it = r.cols.find(rl.q[s]);
+    require(it != r.cols.end() && it->second > 0, "Test B: residual sector has no holdout column");
+    r.per[rl.q[s]] = n2[s] / it->second;
+    tot += r.per[rl.q[s]];
+  }
+  r.est = std::sqrt(tot);
+  return r;
+}
+
+// _dd_select (dd_cbe.jl:290-321): P^D sketch, a first pivoted QR at the floor
+// CBE_EPS max(|sketch|, |projected|), then a pivoted QR of P^D of the first pass keeping pivots
+// above 1/sqrt(2) ("twice is enough"). Null when nothing survives.
+T dd_select(const Eng& e, const T& frame, const T& sketch, bool left) {
+  const int fl = left ? 2 : 0;
+  T projected = left ? perp_left(e, frame, sketch) : perp_right(e, frame, sketch);
+  const auto nn = e.norms(sketch, projected);
+  const double nz = nn.first, ny = nn.second;
+  if (ny <= CBE_EPS * std::max(nz, 1.0)) return nullptr;
+  const int ref_dir = frame->legs[fl].dir;
+  T first = e.thin_qr(projected, fl, ref_dir, CBE_EPS * std::max(nz, ny));
+  if (!first) return nullptr;
+  T again = left ? perp_left(e, frame, first) : perp_right(e, frame, first);
+  return e.thin_qr(again, fl, ref_dir, REORTH_KEEP);
+}
+
+// _target_sectors! (sketch.jl:188-201): sectors whose residual share exceeds an even split of
+// the sample allowance get max(holdout columns, 1) more probe columns; returns how many
+int target_sectors(std::map<int, int64_t>& boost, const TestB& tb, const T& Om, int wleg,
+                   double scale, double sample) {
+  if (tb.per.empty()) return 0;
+  const double share = sample * sample / double(tb.per.size());
+  int n = 0;
+  for (auto& kv : tb.per) {
+    if (!(scale * scale * kv.second > share)) continue;
+    const int have = Om ? Om->legs[wleg].dim_of(kv.first) : 0;
+    boost[kv.first] += std::max(have, 1);
+    ++n;
+  }
+  return n;
+}
+
 struct BondFrame {
   T U0, S0, V0;
   int64_t old_rank;
@@ -606,6 +701,7 @@ struct Params {
   int order, maxdim, hermitian, rule_maxdim, root, reorth, truncate, root_maxiter, fixed_width;
   double tail_factor, bond_ceiling_factor;
   int lanczos, fixed_depth;
+  int dd_mode;  // 0 :rank_tail, 1 :adaptive
 };
 
 struct MPS {
@@ -834,7 +930,123 @@ struct Step {
     return e.contract(r.U, {1}, r.Vd, {0});
   }
 
-  // DD-QR CBE, :rank_tail (dd_cbe_expand.jl:19-301)
+  // _record_sample! (sketch.jl:215-258): the ledger's sample maxima
+  static void record_sample(Ledger* ledger, bool left, double ind) {
+    if (!ledger) return;
+    ledger->max_sample = std::max(ledger->max_sample, ind);
+    if (left) ledger->max_sample_l = std::max(ledger->max_sample_l, ind);
+    else ledger->max_sample_r = std::max(ledger->max_sample_r, ind);
+  }
+
+  // _dd_controller (dd_cbe_controller.jl:26-212, batch_blocks = 1, cap_selection = :storage, no
+  // audit, acceptance factor 1): grows the DD basis block by block until an independent holdout
+  // of DD_HOLDOUT probe columns finds the rest within the sample allowance. Probe draws in the
+  // reference's order: the first block, its holdout, then per round the next holdout before the
+  // next block.
+  T dd_controller(const T& frame, const T& opp, bool left, const std::function<T(const T&)>& sketch,
+                  const std::function<T(const T&)>& project, int64_t initial_width, int64_t wcap,
+                  int64_t ncap, Ledger* ledger) {
+    const int fl = left ? 2 : 0, wleg = left ? 0 : 2;
+    T aug = frame, basis;
+    int64_t count = 0, discovered = 0;
+    std::map<int, int64_t> boost;
+    auto basis_dim = [&]() -> int64_t { return basis ? dim(basis, fl) : 0; };
+    auto draw = [&](int64_t w, bool boosted) {
+      return dd_probe(e, opp, !left, int(w), boosted && !boost.empty() ? &boost : nullptr);
+    };
+    auto absorb = [&](const T& sketched) -> int64_t {
+      if (!sketched) return 0;
+      T nb = dd_select(e, aug, sketched, left);
+      if (!nb) return 0;
+      const int64_t room = ncap - basis_dim();
+      if (room <= 0) return 0;
+      if (dim(nb, fl) > room) {
+        nb = e.trim_total(nb, fl, room);
+        if (!nb) return 0;
+      }
+      basis = basis ? e.oplus({basis, nb}, fl) : nb;
+      aug = e.oplus({aug, nb}, fl);
+      return dim(nb, fl);
+    };
+    auto stream = [&](const T& Om, bool probe) {
+      const int64_t w = dim(Om, wleg);
+      if (probe) {
+        discovered += w;
+        if (ledger) ledger->n_probes += w;
+      } else if (ledger) {
+        ledger->n_holdout += w;
+      }
+      return sketch(Om);
+    };
+    struct Check {
+      T Om, sk;
+    };
+    auto fresh = [&](int64_t columns) -> Check {
+      T Om = draw(columns, false);
+      if (!Om) return Check{};
+      return Check{Om, stream(Om, false)};
+    };
+    auto newsector = [&]() {
+      if (!basis) return false;
+      for (int q : basis->legs[fl].q)
+        if (frame->legs[fl].dim_of(q) == 0) return true;
+      return false;
+    };
+    int64_t width = std::min(std::max<int64_t>(initial_width, 1),
+                             std::max<int64_t>(std::min(wcap, ncap), 1));
+    T last = draw(width, false);
+    if (!last) return nullptr;
+    count += absorb(stream(last, true));
+    Check check = fresh(DD_HOLDOUT);
+    bool escalated = false;
+    while (true) {
+      if (!check.Om) return basis;
+      const TestB tb = sample_residual_sectors(e, basis, project, check.sk, check.Om, wleg, left);
+      const double ind = indicator(alloc, tb.est);
+      const bool ok = ind <= alloc.sample;
+      if (ok && !escalated && (ind > alloc.sample / 2 || newsector())) {
+        escalated = true;
+        Check wide = fresh(2 * DD_HOLDOUT);
+        if (wide.Om) {
+          check = wide;
+          continue;
+        }
+      }
+      const bool capped = discovered >= wcap || count >= ncap;
+      if (ok || capped) {
+        record_sample(ledger, left, ind);
+        if (ok) return basis;
+        if (ledger) {
+          ledger->unmet_(U_SAMPLE);
+          ledger->workcap_reached = true;
+        }
+        return basis;
+      }
+      const int nt = target_sectors(boost, tb, check.Om, wleg, alloc.scale, alloc.sample);
+      if (ledger) ledger->n_targeted += nt;
+      Check next_check = fresh(DD_HOLDOUT);
+      int64_t added = absorb(check.sk);
+      if (nt == 0) width = std::min(2 * width, wcap);
+      const int64_t remaining = ncap - basis_dim();
+      if (remaining > 0) {
+        T blk = draw(std::min(width, std::max<int64_t>(remaining + 2, 1)), true);
+        if (blk) {
+          last = blk;
+          added += absorb(stream(blk, true));
+        }
+      }
+      check = next_check;
+      count += added;
+      if (added == 0) {
+        record_sample(ledger, left, ind);
+        if (ledger) ledger->unmet_(U_SAMPLE);
+        return basis;
+      }
+    }
+  }
+
+  // DD-QR CBE (dd_cbe_expand.jl:19-419): rank by tail bisection (:rank_tail, tail_dd) or by the
+  // incremental controller (:adaptive, _dd_controller)
   Expansion dd_cbe_expand(const BondFrame& fr, int bond, const T& lenv, const T& renv, bool left,
                           Ledger* ledger, int64_t workcap) {
     const T& U0 = fr.U0;
@@ -862,9 +1074,19 @@ struct Step {
                   : env.stream_right(U0, core, Wl, Wr, lenv, renv, Om);
     };
     auto project = [&](const T& b) { return left ? perp_left(e, U0, b) : perp_right(e, V0, b); };
-    T Om = dd_probe(e, opp, !left, int(std::min<int64_t>(P.fixed_width, full_opp)));
-    T directions;
+    T Om, directions;
     int64_t direction_count = 0;
+    if (P.dd_mode == 1) {
+      const int64_t dmax = std::max({dim(U0, 0), old_rank, dim(V0, 2)});
+      const int64_t grow = int64_t(std::ceil(ADAPTIVE_GROWTH * double(dmax))) - old_rank;
+      const int64_t initial_width = int64_t(std::ceil(1.2 * double(std::max<int64_t>(grow, 1))));
+      int64_t wcap = full_opp;
+      if (workcap > 0) wcap = std::min(wcap, workcap);
+      directions = dd_controller(frame, opp, left, sketch, project, initial_width, wcap, cap, ledger);
+      direction_count = directions ? dim(directions, fl) : 0;
+    } else {
+      Om = dd_probe(e, opp, !left, int(std::min<int64_t>(P.fixed_width, full_opp)));
+    }
     if (Om) {
       if (ledger) ledger->n_probes += dim(Om, wleg);
       T Y = project(sketch(Om));
@@ -1689,6 +1911,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     P.bond_ceiling_factor = prm->bond_ceiling_factor;
     P.lanczos = prm->krylov_mode == 0 ? (P.hermitian ? 1 : 0) : (prm->krylov_mode == 1 ? 1 : 0);
     P.fixed_depth = prm->krylov_fixed_depth;
+    require(prm->dd_mode == 0 || prm->dd_mode == 1, "dd_mode must be 0 (:rank_tail) or 1 (:adaptive)");
+    P.dd_mode = prm->dd_mode;
     require(P.tail_factor > 0 && P.tail_factor <= 1, "tail_factor must lie in (0,1]");
 
     Eng e{c, draw, user};
@@ -1866,6 +2090,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     o.expv_err = ledger.expv_err;
     o.expv_iters = ledger.expv_iters;
     o.n_probes = ledger.n_probes;
+    o.n_holdout = ledger.n_holdout;
+    o.n_targeted = ledger.n_targeted;
     o.n_selected = ledger.n_selected;
     o.n_krylov = ledger.n_krylov;
     o.n_h1 = ledger.n_h1;

@@ -28,7 +28,7 @@ class StepParams(ctypes.Structure):
                 ("root", ctypes.c_int), ("reorth", ctypes.c_int), ("truncate", ctypes.c_int),
                 ("root_maxiter", ctypes.c_int), ("fixed_width", ctypes.c_int),
                 ("tail_factor", ctypes.c_double), ("krylov_mode", ctypes.c_int),
-                ("krylov_fixed_depth", ctypes.c_int)]
+                ("krylov_fixed_depth", ctypes.c_int), ("dd_mode", ctypes.c_int)]
 
 
 class BondLog(ctypes.Structure):
@@ -59,7 +59,8 @@ class StepInfo(ctypes.Structure):
                 ("defect", ctypes.c_double), ("n_root_frontier", ctypes.c_int64),
                 ("n_h1_closure", ctypes.c_int64), ("n_compress", ctypes.c_int64),
                 ("leak1", ctypes.c_double), ("expanded", ctypes.c_int * MAX_SITES),
-                ("n_new", ctypes.c_int * MAX_SITES), ("workcap", ctypes.c_int * MAX_SITES)]
+                ("n_new", ctypes.c_int * MAX_SITES), ("workcap", ctypes.c_int * MAX_SITES),
+                ("n_holdout", ctypes.c_int64), ("n_targeted", ctypes.c_int64)]
 
 
 DRAW_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double))
@@ -101,8 +102,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         mode, width = expansion.mode, expansion.fixed_width
         tail_factor, kmode = expansion.tail_factor, expansion.krylov_mode
         fixed_depth = expansion.krylov_fixed_depth
-    if mode != "rank_tail":
-        raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail")
+    if mode not in ("rank_tail", "adaptive"):
+        raise NotImplementedError(f"DD mode {mode!r}: :rank_tail and :adaptive are built")
     return StepParams(
         tol_basis=tol_basis or 0.0, tol_trunc=-1.0 if tol_trunc is None else tol_trunc,
         tol_expv=tol_expv or 0.0, tol_krylov=tol_krylov or 0.0, order=order,
@@ -111,7 +112,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         bond_ceiling_factor=-1.0 if bond_ceiling_factor is None else float(bond_ceiling_factor),
         root=root or 0, reorth=int(reorth), truncate=int(truncate), root_maxiter=root_maxiter,
         fixed_width=width, tail_factor=tail_factor,
-        krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth)
+        krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth,
+        dd_mode=1 if mode == "adaptive" else 0)
 
 
 def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
@@ -160,6 +162,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         expv_iters=info.expv_iters, discarded=info.ledger_discarded, max_sample=info.max_sample,
         max_tail=info.max_tail, max_krylov=info.max_krylov, max_krylov_c=info.max_krylov_c,
         max_krylov_d=info.max_krylov_d, n_probes=info.n_probes, n_selected=info.n_selected,
+        n_holdout=info.n_holdout, n_targeted=info.n_targeted,
         n_krylov=info.n_krylov, n_h1=info.n_h1, n_c_pass=info.n_c_pass, n_d_after_c=info.n_d_after_c,
         workcap_reached=bool(info.workcap_reached), maxdim_reached=bool(info.maxdim_reached),
         proj_err=info.proj_err, r_old=info.r_old, r_aug=info.r_aug, r_final=info.r_final,

@@ -20,7 +20,7 @@ step follows, in the reference's order:
 * ``truncate_recursive!`` / ``_budget_svd`` / ``_cut_divisor`` (``truncation.jl:49-158``) and
   ``_assemble_and_compress!`` (``diagnostics.jl:269-337``).
 
-Supported: ``mode = :rank_tail`` DD-QR expansion, Lanczos/Arnoldi local Krylov with the sequential
+Supported: ``mode = :rank_tail`` and ``:adaptive`` DD-QR expansion, Lanczos/Arnoldi local Krylov with the sequential
 rule, ``order >= 1`` with the single-pass closure (``closure_checks = false``) and folded leak
 estimates, root ``:exp`` only, no ``keep_states``/K-L-S/root report. Those keywords raise.
 """

@@ -233,6 +233,14 @@ def svd(t: DT, left, cutoff: float = 0.0, nkeep: int | None = None) -> SVDResult
     return SVDResult(DT(t.ctx, U), S, DT(t.ctx, V), kept, trunc)
 
 
+def thin_qr(t: DT, leg: int, ref_dir: int, thr: float):
+    """Pivoted thin QR basis of the leg-``leg`` columns per charge sector; see ``bug_thin_qr`` in
+    ``include/bug_b200.h``. None when no pivot exceeds ``thr``."""
+    h = _vp()
+    E.check(t.ctx.lib.bug_thin_qr(t.ctx.h, t.h, int(leg), int(ref_dir), float(thr), ctypes.byref(h)))
+    return DT(t.ctx, h) if h.value else None
+
+
 def scale_leg(t: DT, leg: int, w_by_charge: dict) -> DT:
     L = t.legs[leg]
     w = np.concatenate([np.asarray(w_by_charge[q], dtype=np.float64) for q in L.sectors]) if L.sectors else np.zeros(1)

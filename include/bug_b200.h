@@ -109,6 +109,15 @@ int bug_tensor_meta(const bug_tensor* t, int* dirs, int* nsec, int* charges, int
  * (contract.jl:952-1005 does one zgemm per pair; HPTT transposes become strided gathers). */
 int bug_contract(bug_ctx* ctx, const bug_tensor* a, int n, const int* ia, const bug_tensor* b,
                  const int* ib, int conja, int conjb, bug_tensor** out);
+/* Orthonormal basis of the span of the leg-`leg` columns of `t` (`_thin_qr`,
+ * src/BUG/Randomised/dd_cbe.jl:184-259): per charge sector of that leg, the sector's blocks stacked
+ * row-wise (ascending keys; rows = the other legs in C order) and a column-pivoted Householder QR
+ * (LAPACK geqp3's pivot rule, as Julia's qr(A, ColumnNorm())); the leading Q columns whose |R_kk|
+ * exceeds `thr` are kept, each with the phase that makes R_kk real positive. The new leg has arrow
+ * `ref_dir` and keeps the charge (negated when the arrow flips). A sector is at most 1024 columns
+ * wide (BUG_EINVAL otherwise). *out = NULL when nothing is kept. */
+int bug_thin_qr(bug_ctx* ctx, const bug_tensor* t, int leg, int ref_dir, double thr,
+                bug_tensor** out);
 /* Block-sparse SVD over the split `left | rest` with Telum's selection (svd.jl:1825-1921): keep
  * sigma > cutoff*sigma_max, stable descending sort over sectors (ascending charge), then the nkeep
  * largest (nkeep < 0: no limit). U = (left legs.., bond:+1), Vd = (bond:-1, right legs..).
@@ -167,6 +176,8 @@ typedef struct {
   double tail_factor;         /* :rank_tail acceptance share; <= 0: 0.10 */
   int krylov_mode;            /* 0 :auto, 1 :lanczos, 2 :arnoldi */
   int krylov_fixed_depth;     /* 0: residual-controlled stop */
+  int dd_mode;                /* DD expansion rule: 0 :rank_tail (tail_dd), 1 :adaptive
+                                 (_dd_controller, dd_cbe_controller.jl:26-212) */
 } bug_step_params;
 
 /* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
@@ -206,10 +217,11 @@ typedef struct {
   int expanded[BUG_MAX_SITES];
   int n_new[BUG_MAX_SITES];
   int workcap[BUG_MAX_SITES];
+  int64_t n_holdout, n_targeted; /* holdout probe columns; sectors targeted (:adaptive) */
 } bug_step_info;
 
 /* One rank-adaptive BUG step in place: `cbe_bug_step!(psi, mpo, tau; ...)`
- * (src/BUG/TimeEvolution/bug_step.jl:17-513), DD-QR :rank_tail expansion, Lanczos/Arnoldi local
+ * (src/BUG/TimeEvolution/bug_step.jl:17-513), DD-QR :rank_tail or :adaptive expansion, Lanczos/Arnoldi local
  * Krylov, order-p single-pass closure with folded leak estimates, :exp root. `psi_io[L]` holds the
  * state's site handles on entry; on return each slot holds a new handle owned by the caller, or
  * NULL where the caller's handle is unchanged. The MPO handles are only read. */

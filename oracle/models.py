@@ -240,6 +240,21 @@ def dense_xxz(L: int, J: float = 1.0, delta: float = 1.0) -> np.ndarray:
     return H
 
 
+def sparse_xxz(L: int, J: float = 1.0, delta: float = 1.0):
+    """``dense_xxz`` as a sparse matrix (same terms and ordering), for chains past dense size."""
+    import scipy.sparse as sp
+
+    def embed(o, i):
+        return sp.kron(sp.kron(sp.identity(2 ** i, format="csr"), sp.csr_matrix(o)),
+                       sp.identity(2 ** (L - i - 1), format="csr"), format="csr")
+
+    H = sp.csr_matrix((2 ** L, 2 ** L), dtype=np.complex128)
+    for i in range(L - 1):
+        H = H + J * (0.5 * (embed(SP, i) @ embed(SM, i + 1) + embed(SM, i) @ embed(SP, i + 1))
+                     + delta * embed(SZ, i) @ embed(SZ, i + 1))
+    return H.tocsr()
+
+
 def free_fermion_sz(L: int, t: float, J: float = 1.0, occupied=None) -> np.ndarray:
     """``<S^z_j(t)>`` of the XX chain from a Slater determinant (``test/common/free_fermion.jl:25-47``):
     ``sum_{k occ} |exp(-i h t)_{jk}|^2 - 1/2`` with ``h`` the ``J/2`` hopping matrix."""

@@ -171,3 +171,48 @@ def test_svd_rank_deficient(D):
         assert _isometry_err(Uh, len(split)) < 1e-12
         rec = OB.contract(to_host(got.US()), (len(split),), Vh, (0,))
         assert same(rec, T) < 1e-13
+
+
+def _qr_cases(rng):
+    """(tensor, leg, ref_dir, thr) cases for the pivoted thin QR."""
+    A = mps_like(rng)
+    # a sketch-like tensor whose column sectors are wider than their row space (m < n), with
+    # graded column norms so the pivot order is not the storage order
+    W = rand_bt(rng, (-1, -1, +1), ({0: 2, 2: 1}, SS, {-1: 9, 1: 7, 3: 5}), p_present=1.0)
+    for k, v in W.blocks.items():
+        W.blocks[k] = v * np.geomspace(1.0, 1e-3, v.shape[2])[None, None, :]
+    # rank-deficient sector: column 4 of sector +1 is twice column 0
+    legs = [OB.Leg(-1, {0: 6, 2: 4}), OB.Leg(-1, {-1: 1, 1: 1}), OB.Leg(+1, {-1: 3, 1: 5})]
+    blocks = {}
+    for key in [(0, -1, -1), (0, 1, 1), (2, -1, 1)]:
+        shp = tuple(l.sectors[q] for l, q in zip(legs, key))
+        blocks[key] = rng.standard_normal(shp) + 1j * rng.standard_normal(shp)
+    for key in [(0, 1, 1), (2, -1, 1)]:
+        blocks[key][..., 4] = blocks[key][..., 0] * 2.0
+    R = OB.BT(legs, blocks)
+    # columns of norm ~ 1 with some pivots below 1/sqrt(2): the second-pass keep rule
+    N = mps_like(rng)
+    for k, v in N.blocks.items():
+        N.blocks[k] = v / max(np.linalg.norm(v), 1e-300) * 0.9
+    return [(A, 2, +1, 1e-10), (A, 2, -1, 1e-10), (A, 0, -1, 1e-10), (A, 0, +1, 1e-3),
+            (W, 2, +1, 1e-10), (W, 2, +1, 1e-2), (R, 2, +1, 1e-10), (N, 2, +1, 1 / np.sqrt(2))]
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_thin_qr_matches_oracle(D, case):
+    """The device column-pivoted Householder QR against LAPACK geqp3 (scipy) with the phase that
+    makes R_kk real positive: same kept ranks per sector, same basis vectors."""
+    from oracle import cbe as OC
+
+    rng = np.random.default_rng(700 + case)
+    T, leg, ref, thr = _qr_cases(rng)[case]
+    want = OC.thin_qr(T, leg, ref, thr)
+    got = D.thin_qr(to_dev(T), leg, ref, thr)
+    if want is None:
+        assert got is None
+        return
+    got = to_host(got)
+    assert got.legs[leg].dir == want.legs[leg].dir
+    assert got.legs[leg].sectors == want.legs[leg].sectors
+    assert sorted(got.blocks) == sorted(want.blocks)
+    assert same(got, want) < 1e-11

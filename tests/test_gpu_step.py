@@ -55,6 +55,8 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
         assert di["ledger"].unmet == oi["ledger"].unmet, n
         assert di["ledger"].expv_iters == oi["ledger"].expv_iters, n
         assert di["expanded"] == oi["expanded"], n
+        for f in ("n_probes", "n_holdout", "n_targeted", "n_selected"):
+            assert getattr(di["ledger"], f) == getattr(oi["ledger"], f), (n, f)
         if n % check_every == 0 or n == steps:
             h = mps_to_host(dstate)
             inf = 1.0 - fidelity(h, ostate)
@@ -173,3 +175,59 @@ def test_random_sz0_chains_native_vs_oracle(dev, idx):
         h = mps_to_host(dpsi)
         inf = 1.0 - fidelity(h, opsi)
         assert inf <= 1e-12, (n, inf)
+
+
+ADAPTIVE = dict(work_ceiling_rule="maxdim", expansion=dict(krylov_mode="arnoldi", mode="adaptive"))
+
+
+@pytest.mark.parametrize("native", HOSTS)
+@pytest.mark.parametrize("order", [1, 2])
+def test_adaptive_fixture_setting(dev, order, native):
+    """The :adaptive DD controller (holdout-checked block growth, two-pass pivoted thin QR on
+    device) in the b155550 fixtures' setting, against the oracle's controller step by step."""
+    run_pair(dev, 10, 8, "neel_state", 0.0, order, native=native, **ADAPTIVE)
+
+
+@pytest.mark.parametrize("native", HOSTS)
+def test_adaptive_capped_vs_exact(dev, native):
+    """:adaptive with a binding work cap (every step ends work-limited, the sample check unmet).
+    A capped controller trims its basis to the room by column order, and the second-pass QR's
+    columns all have norm 1 to within a few ulps: its pivot order, and so the trimmed subset, is
+    decided by rounding (in LAPACK too). These runs are therefore compared through what does not
+    depend on that choice: the verdict per step, and the error against exact evolution (sparse
+    Krylov on the full 2^16 space), which must match the oracle's within half again."""
+    import scipy.sparse.linalg as ssl
+
+    DM, DS = dev
+    from bondupdategalerkin_b200 import native as DN
+
+    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
+    L, tau = 16, -0.1j
+    H = OM.sparse_xxz(L, 1.0, 0.5)
+    opsi, dpsi = OM.neel_state(L), DM.neel_state(L)
+    ompo, dmpo = OM.xxz_mpo(L, J=1.0, delta=0.5), DM.xxz_mpo(L, J=1.0, delta=0.5)
+    orng, drng = np.random.default_rng(1234), np.random.default_rng(1234)
+    v = OM.mps_to_dense(opsi)
+    kw = dict(order=2, tol_basis=1e-6, maxdim=16)
+
+    def err(w):
+        return 1.0 - abs(np.vdot(v, w)) ** 2 / (np.vdot(v, v).real * np.vdot(w, w).real)
+
+    for n in range(1, 7):
+        oi = OS.cbe_bug_step(opsi, ompo, tau, rng=orng, expansion=OS.DDQRExpansion(mode="adaptive"), **kw)
+        di = dstep(dpsi, dmpo, tau, rng=drng, expansion=DS.DDQRExpansion(mode="adaptive"), **kw)
+        v = ssl.expm_multiply(tau * H, v)
+        assert di["status"] == oi["status"] == "budget_unmet", n
+        assert di["ledger"].workcap_reached and oi["ledger"].workcap_reached, n
+        assert max(di["bond_dims"]) <= 16
+        eo, ed = err(OM.mps_to_dense(opsi)), err(OM.mps_to_dense(mps_to_host(dpsi)))
+        assert ed <= 1.5 * eo + 1e-10, (n, ed, eo)
+
+
+@pytest.mark.parametrize("native", HOSTS)
+def test_adaptive_targeted(dev, native):
+    """:adaptive at a tight tolerance: the holdout targets sectors (boosted probe columns) in
+    the last step."""
+    run_pair(dev, 14, 6, "neel_state", -0.5, 2, tau=-0.1j, tol_basis=1e-8, maxdim=32,
+             check_every=3, native=native, work_ceiling_rule="maxdim",
+             expansion=dict(mode="adaptive"))
