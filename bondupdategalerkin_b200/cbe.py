@@ -249,31 +249,53 @@ def record_sample(ledger, side, ind, per, hcols, sketch, wleg, alloc):
 
 
 def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap, alloc, ledger,
-                  holdout_width=DD_HOLDOUT):
-    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, ``batch_blocks = 1``,
-    ``cap_selection = :storage``, no audit, acceptance factor 1): grows the DD basis block by
-    block until an independent holdout finds the rest within ``alloc.sample``. Returns
-    ``(basis, status)``; the probe draws come in the reference's order (first block, its holdout,
-    then per round the next holdout before the next block)."""
+                  holdout_width=DD_HOLDOUT, batch_blocks=1, cap_selection="storage",
+                  acceptance_factor=1.0):
+    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, no audit): grows the DD basis block by
+    block until an independent holdout finds the rest within ``acceptance_factor * alloc.sample``.
+    Returns ``(basis, status)``; the probe draws come in the reference's order.
+
+    Streaming a block (probe or holdout) sets ``width`` to that block's column count, as the
+    reference's ``stream`` closure does by assigning the enclosing ``width``
+    (``dd_cbe_controller.jl:108-118``)."""
+    if not 0 < acceptance_factor <= 1:
+        raise ValueError("acceptance_factor must lie in (0,1]")
+    if not 1 <= batch_blocks <= 8:
+        raise ValueError("batch_blocks must lie in 1:8")
+    if cap_selection not in ("storage", "svd"):
+        raise ValueError("cap_selection must be :storage or :svd")
     left = side == "left"
     fl, wleg = (2, 0) if left else (0, 2)
     aug, basis = frame, None
-    count = discovered = 0
+    count = discovered = width = 0
     boost = {}
 
-    def basis_dim():
-        return 0 if basis is None else basis.dim(fl)
+    def remaining():
+        return ncap - (0 if basis is None else basis.dim(fl))
 
     def absorb(sketched):
         nonlocal aug, basis
         nb = dd_select(aug, sketched, side)
         if nb is None:
             return 0
-        room = ncap - basis_dim()
+        room = remaining()
         if room <= 0:
             return 0
         if nb.dim(fl) > room:
-            nb = B.trim_total(nb, fl, room)
+            if cap_selection == "svd":
+                # the strongest sampled directions across sectors (dd_cbe_controller.jl:67-96)
+                off = (perp_left if left else perp_right)(aug, sketched)
+                noff = B.norm(off)
+                fac = B.svd(off, (0, 1) if left else (1, 2), cutoff=rank_cut(0.0, noff, noff),
+                            nkeep=room)
+                if not fac.kept:
+                    nb = None
+                elif left:
+                    nb = reortho(aug, fac.U, "left")
+                else:
+                    nb = reortho(aug, rows_from_u(fac.U), "right")
+            else:
+                nb = B.trim_total(nb, fl, room)
             if nb is None:
                 return 0
         basis = nb if basis is None else B.oplus([basis, nb], fl)
@@ -281,14 +303,14 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         return nb.dim(fl)
 
     def stream(Om, probe):
-        nonlocal discovered
-        w = Om.dim(wleg)
+        nonlocal discovered, width
+        width = Om.dim(wleg)
         if probe:
-            discovered += w
+            discovered += width
             if ledger is not None:
-                ledger.n_probes += w
+                ledger.n_probes += width
         elif ledger is not None:
-            ledger.n_holdout += w
+            ledger.n_holdout += width
         return sketch(Om)
 
     def fresh(columns):
@@ -299,7 +321,10 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         return basis is not None and any(frame.legs[fl].sectors.get(q, 0) == 0
                                          for q in basis.legs[fl].sectors)
 
-    width = min(max(initial_width, 1), max(min(wcap, ncap), 1))
+    if cap_selection == "svd":
+        width = min(max(max(initial_width, ncap + min(4, ncap)), 1), max(wcap, 1))
+    else:
+        width = min(max(initial_width, 1), max(min(wcap, ncap), 1))
     last = draw(width, None)
     if last is None:
         return None, "empty"
@@ -311,7 +336,7 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
             return basis, "met"
         est, per, hcols = sample_residual(basis, project, lambda _: check[1], check[0], wleg, side)
         ind = indicator(alloc, est)
-        ok = ind <= alloc.sample
+        ok = ind <= acceptance_factor * alloc.sample
         if ok and not escalated and (ind > alloc.sample / 2 or newsector()):
             escalated = True
             wide = fresh(2 * holdout_width)
@@ -331,17 +356,32 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         nt = target_sectors(boost, per, check[0], wleg, alloc)
         if ledger is not None:
             ledger.n_targeted += nt
-        next_check = fresh(holdout_width)
-        added = absorb(check[1])
-        if nt == 0:
-            width = min(2 * width, wcap)
-        remaining = ncap - basis_dim()
-        if remaining > 0:
-            blk = draw(min(width, max(remaining + 2, 1)), boost if boost else None)
-            if blk is not None:
+        if batch_blocks == 1:
+            next_check = fresh(holdout_width)
+            added = absorb(check[1])
+            if nt == 0:
+                width = min(2 * width, wcap)
+            if remaining() > 0:
+                blk = draw(min(width, max(remaining() + 2, 1)), boost if boost else None)
+                if blk is not None:
+                    last = blk
+                    added += absorb(stream(blk, True))
+            check = next_check
+        else:
+            # the failed holdout is absorbed, then up to batch_blocks targeted blocks before the
+            # next holdout is drawn (dd_cbe_controller.jl:186-202)
+            added = absorb(check[1])
+            for _ in range(batch_blocks):
+                if remaining() <= 0:
+                    break
+                if nt == 0:
+                    width = min(2 * width, wcap)
+                blk = draw(min(width, max(remaining() + 2, 1)), boost if boost else None)
+                if blk is None:
+                    break
                 last = blk
                 added += absorb(stream(blk, True))
-        check = next_check
+            check = fresh(holdout_width)
         count += added
         if added == 0:
             if ledger is not None:
@@ -406,7 +446,8 @@ class Expansion:
 
 
 def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
-                  fixed_width=8, tail_factor=0.10, mode="rank_tail") -> Expansion:
+                  fixed_width=8, tail_factor=0.10, mode="rank_tail", holdout_width=DD_HOLDOUT,
+                  batch_blocks=1, cap_selection="storage", acceptance_factor=1.0) -> Expansion:
     """Grow one frame of the bond by the DD-projected sketch (``dd_cbe_expand.jl:19-419``): rank
     by tail bisection (``:rank_tail``, ``tail_dd``) or by the incremental controller
     (``:adaptive``, ``_dd_controller``)."""
@@ -458,7 +499,8 @@ def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, wor
         if alloc is not None and workcap > 0:
             wcap = min(wcap, workcap)
         directions, _ = dd_controller(frame, side, lambda w, bst: dd_probe(opp, oside, w, rng, bst),
-                                      sketch, project, initial_width, wcap, cap, alloc, ledger)
+                                      sketch, project, initial_width, wcap, cap, alloc, ledger,
+                                      holdout_width, batch_blocks, cap_selection, acceptance_factor)
         direction_count = 0 if directions is None else directions.dim(fl)
         Om = None
     else:  # tail_dd

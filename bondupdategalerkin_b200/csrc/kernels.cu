@@ -568,12 +568,15 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS
 
 // ── column-pivoted Householder QR (thin, per charge sector) ────────────────────────────────
 // Step k: the remaining column (index >= k) with the largest norm over rows k..m-1 is swapped to
-// position k (ties: the lowest index); its Householder reflector H_k = I - tau v v^H (v_k = 1,
+// position k, columns whose squared norm is within kPivotTie (relative) of the largest counting as
+// tied and the lowest index winning (the order of columns of numerically equal norm would
+// otherwise follow rounding); its Householder reflector H_k = I - tau v v^H (v_k = 1,
 // beta real, as LAPACK's zlarfg) zeroes it below the diagonal; H_k^H is applied to the columns
 // right of k. Q = H_0 ... H_{kq-1} restricted to its first kq columns, each column scaled by
 // sign(beta) so that R_kk >= 0.
 
 constexpr int kQrMaxN = 1024;
+constexpr double kPivotTie = 1e-10;
 
 template <int N>
 __global__ void __launch_bounds__(kThreads) qr_kernel(BUG_BLOB_PARAMS(N), const QrDesc* descs,
@@ -614,11 +617,14 @@ __global__ void __launch_bounds__(kThreads) qr_kernel(BUG_BLOB_PARAMS(N), const 
       if (lane == 0) norms[j] = s2;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0) {  // the lowest index whose squared norm is within kPivotTie of the largest
       int p = k;
       for (int j = k + 1; j < n; ++j)
         if (norms[j] > norms[p]) p = j;
-      pivot = p;
+      const double lim = norms[p] * (1.0 - kPivotTie);
+      int q = k;
+      while (q < p && !(norms[q] >= lim)) ++q;
+      pivot = q;
     }
     __syncthreads();
     const int p = pivot;

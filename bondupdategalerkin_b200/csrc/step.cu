@@ -702,6 +702,8 @@ struct Params {
   double tail_factor, bond_ceiling_factor;
   int lanczos, fixed_depth;
   int dd_mode;  // 0 :rank_tail, 1 :adaptive
+  int holdout_width, batch_blocks, cap_selection_svd;
+  double acceptance_factor;
 };
 
 struct MPS {
@@ -938,19 +940,20 @@ struct Step {
     else ledger->max_sample_r = std::max(ledger->max_sample_r, ind);
   }
 
-  // _dd_controller (dd_cbe_controller.jl:26-212, batch_blocks = 1, cap_selection = :storage, no
-  // audit, acceptance factor 1): grows the DD basis block by block until an independent holdout
-  // of DD_HOLDOUT probe columns finds the rest within the sample allowance. Probe draws in the
-  // reference's order: the first block, its holdout, then per round the next holdout before the
-  // next block.
+  // _dd_controller (dd_cbe_controller.jl:26-212, no audit): grows the DD basis block by block
+  // until an independent holdout of `holdout_width` probe columns finds the rest within
+  // acceptance_factor x the sample allowance. Probe draws in the reference's order. Streaming a
+  // block (probe or holdout) sets `width` to its column count: the reference's `stream` closure
+  // assigns the enclosing `width` (dd_cbe_controller.jl:108-118).
   T dd_controller(const T& frame, const T& opp, bool left, const std::function<T(const T&)>& sketch,
                   const std::function<T(const T&)>& project, int64_t initial_width, int64_t wcap,
                   int64_t ncap, Ledger* ledger) {
     const int fl = left ? 2 : 0, wleg = left ? 0 : 2;
+    const int64_t holdout_width = P.holdout_width;
     T aug = frame, basis;
-    int64_t count = 0, discovered = 0;
+    int64_t count = 0, discovered = 0, width = 0;
     std::map<int, int64_t> boost;
-    auto basis_dim = [&]() -> int64_t { return basis ? dim(basis, fl) : 0; };
+    auto remaining = [&]() -> int64_t { return ncap - (basis ? dim(basis, fl) : 0); };
     auto draw = [&](int64_t w, bool boosted) {
       return dd_probe(e, opp, !left, int(w), boosted && !boost.empty() ? &boost : nullptr);
     };
@@ -958,10 +961,22 @@ struct Step {
       if (!sketched) return 0;
       T nb = dd_select(e, aug, sketched, left);
       if (!nb) return 0;
-      const int64_t room = ncap - basis_dim();
+      const int64_t room = remaining();
       if (room <= 0) return 0;
       if (dim(nb, fl) > room) {
-        nb = e.trim_total(nb, fl, room);
+        if (P.cap_selection_svd) {
+          // the strongest sampled directions across sectors: an SVD of the thin projected
+          // sketch (dd_cbe_controller.jl:67-96)
+          T off = left ? perp_left(e, aug, sketched) : perp_right(e, aug, sketched);
+          const double noff = e.norm(off);
+          SVDRes fac = svd(e, off, left ? std::vector<int>{0, 1} : std::vector<int>{1, 2},
+                           rank_cut(0.0, noff, noff), int(room), W_U);
+          nb = fac.kept.empty() ? nullptr
+                                : (left ? reortho(e, aug, fac.U, true)
+                                        : reortho(e, aug, rows_from_u(e, fac.U), false));
+        } else {
+          nb = e.trim_total(nb, fl, room);
+        }
         if (!nb) return 0;
       }
       basis = basis ? e.oplus({basis, nb}, fl) : nb;
@@ -969,12 +984,12 @@ struct Step {
       return dim(nb, fl);
     };
     auto stream = [&](const T& Om, bool probe) {
-      const int64_t w = dim(Om, wleg);
+      width = dim(Om, wleg);
       if (probe) {
-        discovered += w;
-        if (ledger) ledger->n_probes += w;
+        discovered += width;
+        if (ledger) ledger->n_probes += width;
       } else if (ledger) {
-        ledger->n_holdout += w;
+        ledger->n_holdout += width;
       }
       return sketch(Om);
     };
@@ -992,21 +1007,24 @@ struct Step {
         if (frame->legs[fl].dim_of(q) == 0) return true;
       return false;
     };
-    int64_t width = std::min(std::max<int64_t>(initial_width, 1),
-                             std::max<int64_t>(std::min(wcap, ncap), 1));
+    if (P.cap_selection_svd)
+      width = std::min(std::max<int64_t>(std::max(initial_width, ncap + std::min<int64_t>(4, ncap)), 1),
+                       std::max<int64_t>(wcap, 1));
+    else
+      width = std::min(std::max<int64_t>(initial_width, 1), std::max<int64_t>(std::min(wcap, ncap), 1));
     T last = draw(width, false);
     if (!last) return nullptr;
     count += absorb(stream(last, true));
-    Check check = fresh(DD_HOLDOUT);
+    Check check = fresh(holdout_width);
     bool escalated = false;
     while (true) {
       if (!check.Om) return basis;
       const TestB tb = sample_residual_sectors(e, basis, project, check.sk, check.Om, wleg, left);
       const double ind = indicator(alloc, tb.est);
-      const bool ok = ind <= alloc.sample;
+      const bool ok = ind <= P.acceptance_factor * alloc.sample;
       if (ok && !escalated && (ind > alloc.sample / 2 || newsector())) {
         escalated = true;
-        Check wide = fresh(2 * DD_HOLDOUT);
+        Check wide = fresh(2 * holdout_width);
         if (wide.Om) {
           check = wide;
           continue;
@@ -1024,18 +1042,33 @@ struct Step {
       }
       const int nt = target_sectors(boost, tb, check.Om, wleg, alloc.scale, alloc.sample);
       if (ledger) ledger->n_targeted += nt;
-      Check next_check = fresh(DD_HOLDOUT);
-      int64_t added = absorb(check.sk);
-      if (nt == 0) width = std::min(2 * width, wcap);
-      const int64_t remaining = ncap - basis_dim();
-      if (remaining > 0) {
-        T blk = draw(std::min(width, std::max<int64_t>(remaining + 2, 1)), true);
-        if (blk) {
+      int64_t added = 0;
+      if (P.batch_blocks == 1) {
+        Check next_check = fresh(holdout_width);
+        added = absorb(check.sk);
+        if (nt == 0) width = std::min(2 * width, wcap);
+        if (remaining() > 0) {
+          T blk = draw(std::min(width, std::max<int64_t>(remaining() + 2, 1)), true);
+          if (blk) {
+            last = blk;
+            added += absorb(stream(blk, true));
+          }
+        }
+        check = next_check;
+      } else {
+        // the failed holdout is absorbed, then up to batch_blocks targeted blocks before the next
+        // holdout is drawn (dd_cbe_controller.jl:186-202)
+        added = absorb(check.sk);
+        for (int b = 0; b < P.batch_blocks; ++b) {
+          if (remaining() <= 0) break;
+          if (nt == 0) width = std::min(2 * width, wcap);
+          T blk = draw(std::min(width, std::max<int64_t>(remaining() + 2, 1)), true);
+          if (!blk) break;
           last = blk;
           added += absorb(stream(blk, true));
         }
+        check = fresh(holdout_width);
       }
-      check = next_check;
       count += added;
       if (added == 0) {
         record_sample(ledger, left, ind);
@@ -1913,6 +1946,13 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     P.fixed_depth = prm->krylov_fixed_depth;
     require(prm->dd_mode == 0 || prm->dd_mode == 1, "dd_mode must be 0 (:rank_tail) or 1 (:adaptive)");
     P.dd_mode = prm->dd_mode;
+    P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
+    P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
+    require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
+    require(prm->cap_selection == 0 || prm->cap_selection == 1, "cap_selection must be 0 (:storage) or 1 (:svd)");
+    P.cap_selection_svd = prm->cap_selection;
+    P.acceptance_factor = prm->acceptance_factor > 0 ? prm->acceptance_factor : 1.0;
+    require(P.acceptance_factor <= 1.0, "acceptance_factor must lie in (0,1]");
     require(P.tail_factor > 0 && P.tail_factor <= 1, "tail_factor must lie in (0,1]");
 
     Eng e{c, draw, user};

@@ -28,7 +28,9 @@ class StepParams(ctypes.Structure):
                 ("root", ctypes.c_int), ("reorth", ctypes.c_int), ("truncate", ctypes.c_int),
                 ("root_maxiter", ctypes.c_int), ("fixed_width", ctypes.c_int),
                 ("tail_factor", ctypes.c_double), ("krylov_mode", ctypes.c_int),
-                ("krylov_fixed_depth", ctypes.c_int), ("dd_mode", ctypes.c_int)]
+                ("krylov_fixed_depth", ctypes.c_int), ("dd_mode", ctypes.c_int),
+                ("holdout_width", ctypes.c_int), ("batch_blocks", ctypes.c_int),
+                ("cap_selection", ctypes.c_int), ("acceptance_factor", ctypes.c_double)]
 
 
 class BondLog(ctypes.Structure):
@@ -98,10 +100,23 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
     if fold_omega is False and order > 1:
         raise NotImplementedError("the exact (unfolded) closure leak")
     mode, width, tail_factor, kmode, fixed_depth = "rank_tail", 8, 0.10, "auto", 0
+    holdout, batch, capsel, accept = 4, 1, "storage", 1.0
     if expansion is not None:
         mode, width = expansion.mode, expansion.fixed_width
         tail_factor, kmode = expansion.tail_factor, expansion.krylov_mode
         fixed_depth = expansion.krylov_fixed_depth
+        holdout = getattr(expansion, "holdout_width", 4)
+        batch = getattr(expansion, "batch_blocks", 1)
+        capsel = getattr(expansion, "cap_selection", "storage")
+        accept = getattr(expansion, "acceptance_factor", 1.0)
+    if not 1 <= batch <= 8:
+        raise ValueError("batch_blocks must lie in 1:8")
+    if capsel not in ("storage", "svd"):
+        raise ValueError("cap_selection must be :storage or :svd")
+    if not 0 < accept <= 1:
+        raise ValueError("acceptance_factor must lie in (0,1]")
+    if holdout < 1:
+        raise ValueError("holdout_width must be positive")
     if mode not in ("rank_tail", "adaptive"):
         raise NotImplementedError(f"DD mode {mode!r}: :rank_tail and :adaptive are built")
     return StepParams(
@@ -113,7 +128,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         root=root or 0, reorth=int(reorth), truncate=int(truncate), root_maxiter=root_maxiter,
         fixed_width=width, tail_factor=tail_factor,
         krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth,
-        dd_mode=1 if mode == "adaptive" else 0)
+        dd_mode=1 if mode == "adaptive" else 0, holdout_width=holdout, batch_blocks=batch,
+        cap_selection=1 if capsel == "svd" else 0, acceptance_factor=accept)
 
 
 def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,

@@ -178,6 +178,10 @@ typedef struct {
   int krylov_fixed_depth;     /* 0: residual-controlled stop */
   int dd_mode;                /* DD expansion rule: 0 :rank_tail (tail_dd), 1 :adaptive
                                  (_dd_controller, dd_cbe_controller.jl:26-212) */
+  int holdout_width;          /* :adaptive holdout columns; <= 0: 4 */
+  int batch_blocks;           /* :adaptive blocks per holdout, 1..8; <= 0: 1 */
+  int cap_selection;          /* :adaptive past the cap: 0 :storage (first sectors), 1 :svd */
+  double acceptance_factor;   /* :adaptive acceptance, (0, 1]; <= 0: 1 */
 } bug_step_params;
 
 /* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by

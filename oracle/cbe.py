@@ -206,14 +206,61 @@ REORTH_KEEP = 1.0 / math.sqrt(2.0)  # ``_REORTH_KEEP`` (dd_cbe.jl:273)
 DD_HOLDOUT = 4                      # ``_DD_HOLDOUT`` (dd_cbe_controller.jl:12)
 
 
+PIVOT_TIE = 1e-10  # near-equal squared column norms (relative) count as a pivot tie
+
+
+def pivoted_qr(A: np.ndarray):
+    """Column-pivoted Householder QR of ``A`` (m x n), thin: ``(Q, |R_kk|)`` with Q's columns
+    scaled so that R_kk >= 0. LAPACK geqp3's factorisation (``qr(A, ColumnNorm())`` in Julia):
+    step k moves the remaining column of largest norm over rows k.. to position k and zeroes it
+    below the diagonal with a zlarfg reflector H = I - tau v v^H (v_k = 1, beta real), applying H^H
+    to the columns right of it. Two rules are this restatement's: the remaining norms are
+    recomputed at every step (geqp3 downdates them), and columns whose squared norm is within
+    ``PIVOT_TIE`` of the largest count as tied, the lowest index winning. Without the tie rule
+    the order of columns of (numerically) equal norm -- every column in ``_dd_select``'s second
+    pass, whose input is orthonormal columns projected once more -- is decided by rounding, in
+    LAPACK as well, and so are the subsets a capped controller keeps."""
+    A = np.array(A, dtype=np.complex128, copy=True)
+    m, n = A.shape
+    kq = min(m, n)
+    taus = np.zeros(kq, dtype=np.complex128)
+    betas = np.zeros(kq)
+    for k in range(kq):
+        nrm2 = np.sum(A[k:, k:].real ** 2 + A[k:, k:].imag ** 2, axis=0)
+        top = nrm2.max()
+        p = k + int(np.argmax(nrm2 >= top * (1.0 - PIVOT_TIE)))
+        if p != k:
+            A[:, [k, p]] = A[:, [p, k]]
+        alpha = A[k, k]
+        xn2 = float(np.sum(A[k + 1:, k].real ** 2 + A[k + 1:, k].imag ** 2))
+        if xn2 == 0.0 and alpha.imag == 0.0:
+            beta, tau = alpha.real, 0.0j
+        else:
+            nrm = math.sqrt(alpha.real ** 2 + alpha.imag ** 2 + xn2)
+            beta = -nrm if alpha.real >= 0.0 else nrm
+            tau = complex((beta - alpha.real) / beta, -alpha.imag / beta)
+            A[k + 1:, k] *= 1.0 / (alpha - beta)
+        taus[k], betas[k] = tau, beta
+        if tau != 0:
+            v = np.concatenate([[1.0 + 0j], A[k + 1:, k]])
+            w = v.conj() @ A[k:, k + 1:]
+            A[k:, k + 1:] -= np.conj(tau) * np.outer(v, w)
+    Q = np.eye(m, kq, dtype=np.complex128)
+    for k in reversed(range(kq)):
+        if taus[k] == 0:
+            continue
+        v = np.concatenate([[1.0 + 0j], A[k + 1:, k]])
+        Q[k:, :] -= taus[k] * np.outer(v, v.conj() @ Q[k:, :])
+    Q *= np.where(betas < 0.0, -1.0, 1.0)[None, :]
+    return Q, np.abs(betas)
+
+
 def thin_qr(sketch: B.BT, fl: int, ref_dir: int, thr: float):
     """Orthonormal basis of the span of ``sketch``'s leg-``fl`` columns by column-pivoted
-    Householder QR per charge sector of leg ``fl`` (``_thin_qr``, ``dd_cbe.jl:184-259``; LAPACK
-    geqp3 through scipy, as Julia's ``qr(A, ColumnNorm())``). A direction is kept when its pivot
-    ``|R_kk|`` exceeds ``thr``. The new leg has the arrow ``ref_dir`` (``align_charge``); each kept
-    column's phase makes ``R_kk`` real positive (the gauge both implementations fix)."""
-    import scipy.linalg as sla
-
+    Householder QR per charge sector of leg ``fl`` (``_thin_qr``, ``dd_cbe.jl:184-259``; the
+    factorisation of :func:`pivoted_qr`). A direction is kept when its pivot ``|R_kk|`` exceeds
+    ``thr``. The new leg has the arrow ``ref_dir`` (``align_charge``); each kept column's phase
+    makes ``R_kk`` real positive (the gauge both implementations fix)."""
     others = [i for i in range(sketch.rank) if i != fl]
     ydir = sketch.legs[fl].dir
     groups = {}
@@ -227,13 +274,11 @@ def thin_qr(sketch: B.BT, fl: int, ref_dir: int, thr: float):
         stacked = np.vstack(mats)
         if stacked.shape[0] == 0:
             continue
-        Q, R, _ = sla.qr(stacked, mode="economic", pivoting=True)
-        dg = np.diag(R)
-        kept = int(np.count_nonzero(np.abs(dg) > thr))
+        Q, rdiag = pivoted_qr(stacked)
+        kept = int(np.count_nonzero(rdiag > thr))
         if kept == 0:
             continue
-        ph = np.where(np.abs(dg[:kept]) > 0, dg[:kept] / np.where(dg[:kept] != 0, np.abs(dg[:kept]), 1), 1)
-        Qm = Q[:, :kept] * ph[None, :]
+        Qm = Q[:, :kept]
         qn = charge if ydir == ref_dir else -charge
         space[qn] = kept
         row = 0
@@ -302,14 +347,24 @@ def record_sample(ledger, side, ind, per, hcols, sketch, wleg, alloc):
 
 
 def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap, alloc, ledger,
-                  holdout_width=DD_HOLDOUT):
-    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, ``batch_blocks = 1``,
-    ``cap_selection = :storage``, no audit, acceptance factor 1): grows the DD basis block by
-    block until an independent holdout finds the rest within ``alloc.sample``. Returns
-    ``(basis, status)``."""
+                  holdout_width=DD_HOLDOUT, batch_blocks=1, cap_selection="storage",
+                  acceptance_factor=1.0):
+    """``_dd_controller`` (``dd_cbe_controller.jl:26-212``, no audit): grows the DD basis block by
+    block until an independent holdout finds the rest within ``acceptance_factor * alloc.sample``.
+    Returns ``(basis, status)``.
+
+    As in the reference, streaming a block (probe or holdout) sets the controller's ``width`` to
+    that block's column count: the reference's ``stream`` closure assigns the enclosing ``width``
+    (``dd_cbe_controller.jl:108-118``), so a widening doubles the last streamed block's width."""
+    if not 0 < acceptance_factor <= 1:
+        raise ValueError("acceptance_factor must lie in (0,1]")
+    if not 1 <= batch_blocks <= 8:
+        raise ValueError("batch_blocks must lie in 1:8")
+    if cap_selection not in ("storage", "svd"):
+        raise ValueError("cap_selection must be :storage or :svd")
     left = side == "left"
     fl, wleg = (2, 0) if left else (0, 2)
-    st = dict(aug=frame, basis=None, count=0, streamed=0, discovered=0)
+    st = dict(aug=frame, basis=None, count=0, streamed=0, discovered=0, width=0)
     boost = {}
 
     def absorb(sketched):
@@ -321,7 +376,21 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         if room <= 0:
             return 0
         if nb.dim(fl) > room:
-            nb = B.trim_total(nb, fl, room)
+            if cap_selection == "svd":
+                # the strongest sampled directions across sectors: an SVD of the thin projected
+                # sketch (dd_cbe_controller.jl:67-96)
+                off = (perp_left if left else perp_right)(st["aug"], sketched)
+                noff = B.norm(off)
+                fac = B.svd(off, (0, 1) if left else (1, 2), cutoff=rank_cut(0.0, noff, noff),
+                            nkeep=room)
+                if not fac.kept:
+                    nb = None
+                elif left:
+                    nb = reortho(st["aug"], fac.U, "left")
+                else:
+                    nb = reortho(st["aug"], rows_from_u(fac.U), "right")
+            else:
+                nb = B.trim_total(nb, fl, room)
             if nb is None:
                 return 0
         st["basis"] = nb if st["basis"] is None else B.oplus([st["basis"], nb], fl)
@@ -330,6 +399,7 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
 
     def stream(Om, field):
         w = Om.dim(wleg)
+        st["width"] = w
         st["streamed"] += w
         if field == "n_probes":
             st["discovered"] += w
@@ -349,8 +419,14 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         return b is not None and any(frame.legs[fl].sectors.get(q, 0) == 0
                                      for q in b.legs[fl].sectors)
 
-    width = min(max(initial_width, 1), max(min(wcap, ncap), 1))
-    last = draw(width, None)
+    def remaining():
+        return ncap - (0 if st["basis"] is None else st["basis"].dim(fl))
+
+    if cap_selection == "svd":
+        st["width"] = min(max(max(initial_width, ncap + min(4, ncap)), 1), max(wcap, 1))
+    else:
+        st["width"] = min(max(initial_width, 1), max(min(wcap, ncap), 1))
+    last = draw(st["width"], None)
     if last is None:
         return None, "empty"
     st["count"] += absorb(stream(last, "n_probes"))
@@ -361,7 +437,7 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
             return st["basis"], "met"
         est, per, hcols = resid(check)
         ind = indicator(alloc, est)
-        ok = ind <= alloc.sample
+        ok = ind <= acceptance_factor * alloc.sample
         if ok and not escalated and (ind > alloc.sample / 2 or newsector()):
             escalated = True
             wide = fresh(2 * holdout_width)
@@ -381,17 +457,32 @@ def dd_controller(frame, side, draw, sketch, project, initial_width, wcap, ncap,
         nt = target_sectors(boost, per, check[0], wleg, alloc)
         if ledger is not None:
             ledger.n_targeted += nt
-        next_check = fresh(holdout_width)
-        added = absorb(check[1])
-        if nt == 0:
-            width = min(2 * width, wcap)
-        remaining = ncap - (0 if st["basis"] is None else st["basis"].dim(fl))
-        if remaining > 0:
-            blk = draw(min(width, max(remaining + 2, 1)), boost if boost else None)
-            if blk is not None:
+        if batch_blocks == 1:
+            next_check = fresh(holdout_width)
+            added = absorb(check[1])
+            if nt == 0:
+                st["width"] = min(2 * st["width"], wcap)
+            if remaining() > 0:
+                blk = draw(min(st["width"], max(remaining() + 2, 1)), boost if boost else None)
+                if blk is not None:
+                    last = blk
+                    added += absorb(stream(blk, "n_probes"))
+            check = next_check
+        else:
+            # the failed holdout is absorbed, then up to batch_blocks targeted blocks before
+            # the next holdout is drawn (dd_cbe_controller.jl:186-202)
+            added = absorb(check[1])
+            for _ in range(batch_blocks):
+                if remaining() <= 0:
+                    break
+                if nt == 0:
+                    st["width"] = min(2 * st["width"], wcap)
+                blk = draw(min(st["width"], max(remaining() + 2, 1)), boost if boost else None)
+                if blk is None:
+                    break
                 last = blk
                 added += absorb(stream(blk, "n_probes"))
-        check = next_check
+            check = fresh(holdout_width)
         st["count"] += added
         if added == 0:
             if ledger is not None:
@@ -456,7 +547,8 @@ class Expansion:
 
 
 def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
-                  fixed_width=8, tail_factor=0.10, mode="rank_tail") -> Expansion:
+                  fixed_width=8, tail_factor=0.10, mode="rank_tail", holdout_width=DD_HOLDOUT,
+                  batch_blocks=1, cap_selection="storage", acceptance_factor=1.0) -> Expansion:
     """Grow one frame of the bond by the DD-projected sketch (``dd_cbe_expand.jl:19-419``): rank
     by tail bisection (``:rank_tail``, ``tail_dd``) or by the incremental controller
     (``:adaptive``, ``_dd_controller``)."""
@@ -508,7 +600,8 @@ def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, wor
         if alloc is not None and workcap > 0:
             wcap = min(wcap, workcap)
         directions, _ = dd_controller(frame, side, lambda w, bst: dd_probe(opp, oside, w, rng, bst),
-                                      sketch, project, initial_width, wcap, cap, alloc, ledger)
+                                      sketch, project, initial_width, wcap, cap, alloc, ledger,
+                                      holdout_width, batch_blocks, cap_selection, acceptance_factor)
         direction_count = 0 if directions is None else directions.dim(fl)
         Om = None
     else:  # tail_dd

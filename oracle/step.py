@@ -51,7 +51,14 @@ class DDQRExpansion:
 
     mode: str = "rank_tail"
     fixed_width: int = 8
+    fixed_rank: int = 0
+    rank_initial_width: int = 4
+    rank_floor: int = 0
     tail_factor: float = 0.10
+    holdout_width: int = 4
+    batch_blocks: int = 1
+    cap_selection: str = "storage"
+    acceptance_factor: float = 1.0
     krylov_mode: str = "auto"
     krylov_fixed_depth: int = 0
 
@@ -217,7 +224,11 @@ def cap_at(wcap, bond):
 def expand(cx: Ctx, fr, bond, lch, rch, side, ledger):
     return dd_cbe_expand(fr, cx.mpo, bond, lch, rch, side, cx.alloc, ledger, cap_at(cx.wcap, bond),
                          cx.rng, fixed_width=cx.expansion.fixed_width,
-                         tail_factor=cx.expansion.tail_factor, mode=cx.expansion.mode)
+                         tail_factor=cx.expansion.tail_factor, mode=cx.expansion.mode,
+                         holdout_width=cx.expansion.holdout_width,
+                         batch_blocks=cx.expansion.batch_blocks,
+                         cap_selection=cx.expansion.cap_selection,
+                         acceptance_factor=cx.expansion.acceptance_factor)
 
 
 def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
