@@ -47,6 +47,21 @@ SIGNATURES = {
                                ctypes.c_int, _c_int_p, _c_int_p]),
     "bug_thin_qr": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                    ctypes.POINTER(_vp)]),
+    "bug_env_boundary": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "bug_env_step": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "bug_apply_one_site": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "bug_apply_zero_site": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
+    "bug_sketch_stream": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                         ctypes.POINTER(_vp)]),
+    "bug_perp": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp)]),
+    "bug_root_expv": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_int64),
+                                     _c_double_p]),
+    "bug_site_populations": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
+                                            _c_double_p, ctypes.c_int, _c_int_p]),
+    "bug_observable_sz": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
+                                         _c_double_p]),
     "bug_scale_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_double_p, ctypes.POINTER(_vp)]),
     "bug_norm2": (ctypes.c_int, [_vp, _vp, _c_double_p]),
     "bug_inner": (ctypes.c_int, [_vp, _vp, _vp, _c_double_p]),

@@ -2162,6 +2162,194 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
   });
 }
 
+// ── kernel-granular entry points ───────────────────────────────────────────────────────────
+// The pieces of the step for a host that keeps the sweep logic itself: each takes borrowed
+// handles and returns a new handle owned by the caller (metadata copied, payload shared: tensors
+// are never mutated in place).
+
+namespace {
+
+T borrow(const bug_tensor* t) {
+  require(t != nullptr, "null tensor handle");
+  return T(const_cast<bug_tensor*>(t), [](bug_tensor*) {});
+}
+
+bug_tensor* hand_out(const T& t) { return t ? std::make_unique<bug_tensor>(*t).release() : nullptr; }
+
+// local populations of the site whose tensor is `t` (centre there; leg 1 the site leg): the
+// norm^2 of every local basis index, in leg order (sectors ascending, then index)
+std::vector<double> site_populations(bug_ctx* c, const bug_tensor& t) {
+  const Leg& sl = t.legs[1];
+  const std::vector<double> n2 = sector_norms2(c, t, 1);
+  std::vector<double> out;
+  for (size_t s = 0; s < sl.q.size(); ++s) {
+    if (sl.d[s] == 1) {
+      out.push_back(n2[s]);
+      continue;
+    }
+    double prev = 0.0;
+    for (int k = 1; k <= sl.d[s]; ++k) {
+      double cum = n2[s];
+      if (k < sl.d[s]) {
+        std::vector<int> counts(sl.q.size(), 0);
+        counts[s] = k;
+        auto tr = trim_impl(c, t, 1, counts.data());
+        double r[2] = {0.0, 0.0};
+        if (tr) dots(c, {{tr.get(), tr.get()}}, r);
+        cum = r[0];
+      }
+      out.push_back(cum - prev);
+      prev = cum;
+    }
+  }
+  return out;
+}
+
+// normalised local populations of every site (centre moved to each in turn), flattened
+std::vector<double> populations_impl(bug_ctx* c, int L, const bug_tensor* const* psi, int center) {
+  require(c && psi && L >= 1 && center >= 1 && center <= L, "bad argument");
+  Eng e{c, nullptr, nullptr};
+  MPOv none;
+  Step S(e, none, Params{}, cd(0.0), L);
+  MPS phi;
+  for (int i = 0; i < L; ++i) phi.s.push_back(borrow(psi[i]));
+  phi.center = center;
+  std::vector<double> out;
+  S.canonical(phi, 1);
+  for (int j = 1; j <= L; ++j) {
+    if (j > 1) S.canonical(phi, j);
+    std::vector<double> pop = site_populations(c, *phi[j]);
+    double tot = 0.0;
+    for (double x : pop) tot += x;
+    for (double x : pop) out.push_back(tot > 0 ? x / tot : 0.0);
+  }
+  return out;
+}
+
+}  // namespace
+
+extern "C" int bug_env_boundary(bug_ctx* c, int side, int charge, bug_tensor** out) {
+  return guard([&] {
+    require(c && out && (side == 0 || side == 1), "bad argument");
+    Eng e{c, nullptr, nullptr};
+    Env env{e};
+    *out = hand_out(side == 0 ? env.left_boundary() : env.right_boundary(charge));
+  });
+}
+
+extern "C" int bug_env_step(bug_ctx* c, int side, const bug_tensor* env_in, const bug_tensor* A,
+                            const bug_tensor* W, bug_tensor** out) {
+  return guard([&] {
+    require(c && out && (side == 0 || side == 1), "bad argument");
+    Eng e{c, nullptr, nullptr};
+    Env env{e};
+    *out = hand_out(side == 0 ? env.left_step(borrow(env_in), borrow(A), borrow(W))
+                              : env.right_step(borrow(env_in), borrow(A), borrow(W)));
+  });
+}
+
+extern "C" int bug_apply_one_site(bug_ctx* c, const bug_tensor* lenv, const bug_tensor* W,
+                                  const bug_tensor* renv, const bug_tensor* x, bug_tensor** out) {
+  return guard([&] {
+    require(c && out, "null argument");
+    Eng e{c, nullptr, nullptr};
+    Env env{e};
+    *out = hand_out(env.one_site(borrow(lenv), borrow(W), borrow(renv), borrow(x)));
+  });
+}
+
+extern "C" int bug_apply_zero_site(bug_ctx* c, const bug_tensor* lgen, const bug_tensor* rgen,
+                                   const bug_tensor* core, bug_tensor** out) {
+  return guard([&] {
+    require(c && out, "null argument");
+    Eng e{c, nullptr, nullptr};
+    ZeroSiteH h{borrow(lgen), borrow(rgen)};
+    *out = hand_out(h.apply(e, borrow(core)));
+  });
+}
+
+extern "C" int bug_sketch_stream(bug_ctx* c, int side, const bug_tensor* a, const bug_tensor* b,
+                                 const bug_tensor* Wl, const bug_tensor* Wr, const bug_tensor* lenv,
+                                 const bug_tensor* renv, const bug_tensor* probe, bug_tensor** out) {
+  return guard([&] {
+    require(c && out && (side == 0 || side == 1), "bad argument");
+    Eng e{c, nullptr, nullptr};
+    Env env{e};
+    *out = hand_out(side == 0 ? env.stream_left(borrow(a), borrow(b), borrow(Wl), borrow(Wr),
+                                                borrow(lenv), borrow(renv), borrow(probe))
+                              : env.stream_right(borrow(a), borrow(b), borrow(Wl), borrow(Wr),
+                                                 borrow(lenv), borrow(renv), borrow(probe)));
+  });
+}
+
+extern "C" int bug_perp(bug_ctx* c, int side, const bug_tensor* frame, const bug_tensor* K,
+                        bug_tensor** out) {
+  return guard([&] {
+    require(c && out && (side == 0 || side == 1), "bad argument");
+    Eng e{c, nullptr, nullptr};
+    *out = hand_out(side == 0 ? perp_left(e, borrow(frame), borrow(K))
+                              : perp_right(e, borrow(frame), borrow(K)));
+  });
+}
+
+extern "C" int bug_root_expv(bug_ctx* c, const bug_tensor* lgen, const bug_tensor* rgen,
+                             const bug_tensor* core, double tau_re, double tau_im, int hermitian,
+                             int maxiter, int reorth, double tol_expv, bug_tensor** out,
+                             int64_t* iters, double* err) {
+  return guard([&] {
+    require(c && out, "null argument");
+    require(maxiter >= 1, "maxiter must be positive");
+    Eng e{c, nullptr, nullptr};
+    MPOv none;
+    Params P{};
+    P.tol_expv = tol_expv;
+    Step S(e, none, P, cd(tau_re, tau_im), 2);
+    ZeroSiteH h{borrow(lgen), borrow(rgen)};
+    auto apply = [&](const T& v) { return h.apply(e, v); };
+    Step::ExpvRep rep;
+    T r = hermitian ? S.lanczos_expv(apply, borrow(core), maxiter, 1e-15, reorth != 0, tol_expv, rep)
+                    : S.arnoldi_expv(apply, borrow(core), maxiter, 1e-15, tol_expv, rep);
+    *out = hand_out(r);
+    if (iters) *iters = rep.iters;
+    if (err) *err = rep.err;
+  });
+}
+
+extern "C" int bug_site_populations(bug_ctx* c, int L, const bug_tensor* const* psi, int center,
+                                    double* out, int cap, int* n_out) {
+  return guard([&] {
+    require(n_out != nullptr, "null argument");
+    const std::vector<double> pop = populations_impl(c, L, psi, center);
+    for (int i = 0; i < int(pop.size()) && i < cap; ++i)
+      if (out) out[i] = pop[i];
+    *n_out = int(pop.size());
+  });
+}
+
+extern "C" int bug_observable_sz(bug_ctx* c, int L, const bug_tensor* const* psi, int center,
+                                 double* out) {
+  return guard([&] {
+    require(out != nullptr, "null argument");
+    const std::vector<double> pop = populations_impl(c, L, psi, center);
+    size_t k = 0;
+    for (int j = 0; j < L; ++j) {
+      const Leg& sl = psi[j]->legs[1];
+      double sz = 0.0;
+      if (sl.q.size() == 1) {  // :none -- one charge-0 sector, index 0 up, 1 down
+        require(sl.q[0] == 0 && sl.d[0] == 2, "S^z needs a spin-1/2 site");
+        sz = 0.5 * pop[k] - 0.5 * pop[k + 1];
+        k += 2;
+      } else {  // U(1) -- the charge is 2 S^z, one state per sector
+        for (size_t s = 0; s < sl.q.size(); ++s) {
+          require(sl.d[s] == 1, "S^z needs a spin-1/2 site");
+          sz += 0.5 * sl.q[s] * pop[k++];
+        }
+      }
+      out[j] = sz;
+    }
+  });
+}
+
 extern "C" int bug_la_expm(int n, const double* a, double* out) {
   return guard([&] {
     require(n >= 0, "bad size");

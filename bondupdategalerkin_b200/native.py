@@ -195,3 +195,89 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         ledger=ledger, status="met" if info.status == 0 else "budget_unmet",
         bond_dims=psi.bond_dims(), workcap=list(info.workcap[:L - 1]),
     )
+
+
+# ── kernel-granular entry points (``bug_env_step`` ... ``bug_observable_sz``) ──────────────────
+
+
+def _call(ctx, fn, *args):
+    h = ctypes.c_void_p()
+    E.check(getattr(ctx.lib, fn)(ctx.h, *args, ctypes.byref(h)))
+    return DT(ctx, h) if h.value else None
+
+
+def env_boundary(ctx, side: str, charge: int = 0) -> DT:
+    """Chain-end environment: ``side`` "left" or "right" (the latter carrying the total charge)."""
+    return _call(ctx, "bug_env_boundary", 0 if side == "left" else 1, int(charge))
+
+
+def env_step(env: DT, A: DT, W: DT, side: str) -> DT:
+    """``_mpo_left_step`` / ``_mpo_right_step`` (``mpo_environments.jl:65-108``)."""
+    return _call(env.ctx, "bug_env_step", 0 if side == "left" else 1, env.h, A.h, W.h)
+
+
+def apply_one_site(lenv: DT, W: DT, renv: DT, x: DT) -> DT:
+    """``apply_one_site`` (``effective_operators.jl:27-64``)."""
+    return _call(x.ctx, "bug_apply_one_site", lenv.h, W.h, renv.h, x.h)
+
+
+def apply_zero_site(lgen: DT, rgen: DT, core: DT) -> DT:
+    """``apply_zero_site`` (``effective_operators.jl:91-107``)."""
+    return _call(core.ctx, "bug_apply_zero_site", lgen.h, rgen.h, core.h)
+
+
+def sketch_stream(side: str, a: DT, b: DT, Wl: DT, Wr: DT, lenv: DT, renv: DT, probe: DT) -> DT:
+    """``_stream_left`` / ``_stream_right`` (``mpo_environments.jl:409-481``): side "left" with
+    ``a = U0 S0``, ``b = V0``; side "right" with ``a = U0``, ``b = S0 V0``."""
+    return _call(probe.ctx, "bug_sketch_stream", 0 if side == "left" else 1, a.h, b.h, Wl.h, Wr.h,
+                 lenv.h, renv.h, probe.h)
+
+
+def perp(side: str, frame: DT, K: DT) -> DT:
+    """``perp_component`` / ``perp_component_right`` (``sectors.jl:215-240``)."""
+    return _call(K.ctx, "bug_perp", 0 if side == "left" else 1, frame.h, K.h)
+
+
+def root_expv(lgen: DT, rgen: DT, core: DT, tau, hermitian=True, maxiter=30, reorth=True,
+              tol_expv=1e-10):
+    """``expv`` of the root (``root_methods.jl:359-402``): ``(exp(tau H0) core, H0 applications,
+    accumulated tail estimate)``."""
+    tau = complex(tau)
+    ctx = core.ctx
+    h = ctypes.c_void_p()
+    iters, err = ctypes.c_int64(), ctypes.c_double()
+    E.check(ctx.lib.bug_root_expv(ctx.h, lgen.h, rgen.h, core.h, tau.real, tau.imag, int(hermitian),
+                                  int(maxiter), int(reorth), float(tol_expv), ctypes.byref(h),
+                                  ctypes.byref(iters), ctypes.byref(err)))
+    return DT(ctx, h), int(iters.value), float(err.value)
+
+
+def _handles(psi):
+    return (ctypes.c_void_p * len(psi.tensors))(*[t.h.value for t in psi.tensors])
+
+
+def site_populations(psi) -> list:
+    """Normalised local populations per site, the site leg's indices in leg order."""
+    ctx = psi.tensors[0].ctx
+    n = ctypes.c_int()
+    E.check(ctx.lib.bug_site_populations(ctx.h, len(psi.tensors), _handles(psi), psi.center, None, 0,
+                                         ctypes.byref(n)))
+    buf = np.zeros(max(n.value, 1))
+    E.check(ctx.lib.bug_site_populations(ctx.h, len(psi.tensors), _handles(psi), psi.center,
+                                         buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n.value,
+                                         ctypes.byref(n)))
+    out, k = [], 0
+    for t in psi.tensors:
+        d = sum(t.legs[1].sectors.values())
+        out.append(buf[k:k + d].copy())
+        k += d
+    return out
+
+
+def observable_sz(psi) -> np.ndarray:
+    """``<S^z_j>`` for every site (``bug_observable_sz``)."""
+    ctx = psi.tensors[0].ctx
+    out = np.zeros(len(psi.tensors))
+    E.check(ctx.lib.bug_observable_sz(ctx.h, len(psi.tensors), _handles(psi), psi.center,
+                                      out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    return out

@@ -234,6 +234,54 @@ int bug_mps_step(bug_ctx* ctx, int L, bug_tensor** psi_io, int* center_io,
                  const bug_step_params* params, bug_normal_fn draw, void* user,
                  bug_step_info* info, bug_bond_log* bond_log, int bond_log_cap, int* n_bond_log);
 
+/* ── kernel-granular entry points ─────────────────────────────────────────────────────────
+ * The pieces of the step for a host that keeps the sweep logic itself (a Julia `ccall` shim).
+ * Inputs are borrowed; each output is a new handle owned by the caller. Layouts follow the
+ * engine's arrow conventions: MPS site (link_l:-1, site:-1, link_r:+1); MPO (w_l:-1, s_in:+1,
+ * s_out:-1, w_r:+1); left environment (bra:-1, w:+1, ket:+1); right environment (bra:+1, w:-1,
+ * ket:-1). */
+
+/* Chain-end environments (the `nothing` ends of mpo_environments.jl:141-175, explicit here):
+ * side 0 left (trivial), 1 right (carrying `charge`, the state's total charge). */
+int bug_env_boundary(bug_ctx* ctx, int side, int charge, bug_tensor** out);
+/* One environment push E -> A^dagger (E A W): side 0 `_mpo_left_step`, 1 `_mpo_right_step`
+ * (mpo_environments.jl:65-108). */
+int bug_env_step(bug_ctx* ctx, int side, const bug_tensor* env, const bug_tensor* A,
+                 const bug_tensor* W, bug_tensor** out);
+/* H1 x for the local Krylov (`apply_one_site`, effective_operators.jl:27-64). */
+int bug_apply_one_site(bug_ctx* ctx, const bug_tensor* lenv, const bug_tensor* W,
+                       const bug_tensor* renv, const bug_tensor* x, bug_tensor** out);
+/* H0 S = sum_w L[w] S R[w] (`apply_zero_site`, effective_operators.jl:91-107); `lgen`/`rgen` are
+ * the environments pushed through the bond's expanded left / right frames. */
+int bug_apply_zero_site(bug_ctx* ctx, const bug_tensor* lgen, const bug_tensor* rgen,
+                        const bug_tensor* core, bug_tensor** out);
+/* The streamed two-site sketch X Om with Theta never formed (`_stream_left`/`_stream_right`,
+ * mpo_environments.jl:409-481): side 0 with a = U0 S0 (l, s, b), b = V0 and a probe in V0's
+ * layout (g, s_r, l_r), out (l_l, s_l, g); side 1 with a = U0, b = S0 V0 and a probe
+ * (l_l, s_l, g), out (g, s_r, l_r). Wl, Wr: the bond's MPO sites. */
+int bug_sketch_stream(bug_ctx* ctx, int side, const bug_tensor* a, const bug_tensor* b,
+                      const bug_tensor* Wl, const bug_tensor* Wr, const bug_tensor* lenv,
+                      const bug_tensor* renv, const bug_tensor* probe, bug_tensor** out);
+/* (I - U U^dagger) K: side 0 `perp_component` (a left frame over legs 0, 1), 1
+ * `perp_component_right` (a right frame over legs 1, 2) (sectors.jl:215-240). */
+int bug_perp(bug_ctx* ctx, int side, const bug_tensor* frame, const bug_tensor* K,
+             bug_tensor** out);
+/* The root Galerkin exponential exp(tau H0) core (`expv`, root_methods.jl:359-402: `lanczos_expv`
+ * krylov.jl:128-263 when `hermitian`, else `arnoldi_expv` :343-442) with the Saad tail against
+ * `tol_expv` and adaptive substeps; `iters` = H0 applications, `err` = the accumulated tail. */
+int bug_root_expv(bug_ctx* ctx, const bug_tensor* lgen, const bug_tensor* rgen,
+                  const bug_tensor* core, double tau_re, double tau_im, int hermitian, int maxiter,
+                  int reorth, double tol_expv, bug_tensor** out, int64_t* iters, double* err);
+/* Normalised local populations of every site (`site_expval` of the diagonal projectors,
+ * local_observables.jl:11-24): per site, the site leg's indices in leg order (sectors
+ * ascending, then index); `n` = the total count (at most `cap` written). */
+int bug_site_populations(bug_ctx* ctx, int L, const bug_tensor* const* psi, int center,
+                         double* out, int cap, int* n);
+/* <S^z_j> for every site of a spin-1/2 chain (`sz_expectation`/`magnetisation`,
+ * local_observables.jl:11-24, bond_observables.jl:15): under U(1) the site charge is 2 S^z;
+ * under :none the one charge-0 sector holds up (index 0) and down (index 1). */
+int bug_observable_sz(bug_ctx* ctx, int L, const bug_tensor* const* psi, int center, double* out);
+
 /* ── serving: many jobs on one GPU ─────────────────────────────────────────────────────────
  * No reference counterpart: the reference calls cbe_bug_step! one chain at a time. A server owns
  * `workers` threads, each with its own context (stream, memory, staging); jobs wait in one FIFO
