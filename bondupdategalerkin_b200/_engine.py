@@ -62,6 +62,7 @@ SIGNATURES = {
                                             _c_double_p, ctypes.c_int, _c_int_p]),
     "bug_observable_sz": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int,
                                          _c_double_p]),
+    "bug_apply_two_site": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "bug_scale_leg": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_double_p, ctypes.POINTER(_vp)]),
     "bug_norm2": (ctypes.c_int, [_vp, _vp, _c_double_p]),
     "bug_inner": (ctypes.c_int, [_vp, _vp, _vp, _c_double_p]),
@@ -90,11 +91,11 @@ SIGNATURES = {
     "bug_inner_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, _vp]),
 }
 # declared in native.py (structure arguments)
-NATIVE_ONLY = ("bug_mps_step",)
+NATIVE_ONLY = ("bug_mps_step", "bug_tdvp2_step")  # bound in native.py with their structs
 
 FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
-# Where each family runs: the SVD is its own kernel; every other family is a stage kind of
-# stage_kernel (operations queued between two read-backs launch together as one stage list).
+# Where each family runs: the SVD (and the pivoted QR) is its own kernel; every other family is a
+# stage kind of stage_kernel, one launch per operation.
 KERNEL_NAMES = {"copy": "stage_kernel (copy stage)", "gemm": "stage_kernel (gemm stage)",
                 "svd": "jacobi_svd_kernel", "dot": "stage_kernel (dot stages)",
                 "lincomb": "stage_kernel (lincomb stage)", "scale": "stage_kernel (scale stage)"}

@@ -372,6 +372,13 @@ struct Env {
     t = e.contract(t, {1, 3}, A, {2, 1}, false, true);
     return e.permute(t, {2, 1, 0});
   }
+  // H Theta for a two-site tensor (l, s1, s2, r) (apply_h_two_site, mpo_environments.jl:316-344)
+  T two_site(const T& Le, const T& Wl, const T& Wr, const T& Re, const T& x) const {
+    T t = e.contract(Le, {2}, x, {0});
+    t = e.contract(t, {1, 2}, Wl, {0, 1});
+    t = e.contract(t, {4, 1}, Wr, {0, 1});
+    return e.contract(t, {4, 1}, Re, {1, 2});
+  }
   T one_site(const T& Le, const T& W, const T& Re, const T& x) const {
     T t = e.contract(Le, {2}, x, {0});
     t = e.contract(t, {1, 2}, W, {0, 1});
@@ -1729,14 +1736,18 @@ struct Step {
     double err = 0;
   };
 
+  // substeps: 1 one step of the whole tau, > 1 that many equal substeps, 0 the adaptive substep
+  // search (pick_tau)
   T lanczos_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
-                 bool reorth, double conv_tol, ExpvRep& rep) {
+                 bool reorth, double conv_tol, ExpvRep& rep, int substeps = 0) {
     const double beta0 = e.norm(vec);
     if (beta0 == 0) return vec;
     T cur = vec;
     cd tau_rem = tau, logscale = 0.0;
+    int nsub = 0;
     while (true) {
       rep.nsub += 1;
+      nsub += 1;
       const double cur_norm = e.norm(cur);
       if (cur_norm == 0) break;
       T v = e.scale(cur, 1.0 / cur_norm);
@@ -1775,13 +1786,15 @@ struct Step {
       Eig eg = tridiag_eigen(alpha, betas);
       auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
       const double betak = e.norm(residual);
-      const cd tau_s = pick_tau(ev, tau_rem, betak, conv_tol);
+      const cd tau_s = substeps == 1 ? tau_rem
+                       : substeps > 1 ? tau_rem / double(substeps - nsub + 1)
+                                      : pick_tau(ev, tau_rem, betak, conv_tol);
       auto cl = ev(tau_s);
       rep.err += tail_sup(ev, tau_s, betak) * cur_norm / beta0;
       cur = combine(cl.first, basis, cur_norm);
       logscale += cl.second;
       tau_rem -= tau_s;
-      if (std::abs(tau_rem) <= 1e-14 * std::max(std::abs(tau), 1.0)) break;
+      if (substeps == 1 || std::abs(tau_rem) <= 1e-14 * std::max(std::abs(tau), 1.0)) break;
       require(rep.nsub < 10000, "expv: substep search failed to advance");
     }
     return apply_scale(cur, logscale);
@@ -1801,13 +1814,15 @@ struct Step {
   }
 
   T arnoldi_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
-                 double conv_tol, ExpvRep& rep) {
+                 double conv_tol, ExpvRep& rep, int substeps = 0) {
     const double beta0 = e.norm(vec);
     if (beta0 == 0) return vec;
     T cur = vec;
     cd tau_rem = tau, logscale = 0.0;
+    int nsub = 0;
     while (true) {
       rep.nsub += 1;
+      nsub += 1;
       const double cur_norm = e.norm(cur);
       if (cur_norm == 0) break;
       std::vector<T> basis{e.scale(cur, 1.0 / cur_norm)};
@@ -1845,14 +1860,16 @@ struct Step {
       for (int i = 0; i < dimk; ++i)
         for (int j = 0; j < dimk; ++j) Hm(i, j) = H(i, j);
       auto ev = [&](cd s) { return hess_coeffs(Hm, s); };
-      const cd tau_s = pick_tau(ev, tau_rem, betak, conv_tol);
+      const cd tau_s = substeps == 1 ? tau_rem
+                       : substeps > 1 ? tau_rem / double(substeps - nsub + 1)
+                                      : pick_tau(ev, tau_rem, betak, conv_tol);
       auto cl = ev(tau_s);
       rep.err += tail_sup(ev, tau_s, betak) * cur_norm / beta0;
       basis.resize(dimk);
       cur = combine(cl.first, basis, cur_norm);
       logscale += cl.second;
       tau_rem -= tau_s;
-      if (std::abs(tau_rem) <= 1e-14 * std::max(std::abs(tau), 1.0)) break;
+      if (substeps == 1 || std::abs(tau_rem) <= 1e-14 * std::max(std::abs(tau), 1.0)) break;
       require(rep.nsub < 10000, "expv: substep search failed to advance");
     }
     return apply_scale(cur, logscale);
@@ -2347,6 +2364,136 @@ extern "C" int bug_observable_sz(bug_ctx* c, int L, const bug_tensor* const* psi
       }
       out[j] = sz;
     }
+  });
+}
+
+// ── two-site TDVP (src/Baselines/TDVP/tdvp2.jl) ────────────────────────────────────────────
+// One symmetric step: a forward sweep of two-site updates exp(tau/2 H2) with SVD splits and
+// backward one-site half-steps exp(-tau/2 H1), then the mirror sweep (tdvp2_step!, :229-297;
+// _tdvp2_bond!, :39-136; _tdvp2_backward, :145-173). The environments are carried bond to bond on
+// the sweep's own side and read from one prebuilt stack on the other.
+
+extern "C" int bug_tdvp2_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_io,
+                              const bug_tensor* const* mpo_in, double tau_re, double tau_im,
+                              const bug_tdvp2_params* prm, bug_tdvp2_info* info) {
+  return guard([&] {
+    require(c && psi_io && center_io && mpo_in && prm && info, "null argument");
+    require(L >= 2, "tdvp2_step needs at least two sites");
+    const int maxdim = prm->maxdim > 0 ? prm->maxdim : 200;
+    const double trunc_thresh = prm->trunc_thresh >= 0 ? prm->trunc_thresh : 1e-12;
+    const int maxiter = prm->maxiter > 0 ? prm->maxiter : 30;
+    const double tol = prm->tol > 0 ? prm->tol : 1e-15;
+    const bool hermitian = prm->hermitian != 0;
+    const double conv_tol = prm->conv_tol;
+    const int substeps = prm->substeps;
+    require(substeps >= 0, "substeps must be >= 0");
+    const double weight_tol = prm->weight_tol;
+    const double eshift = prm->eshift;
+    Eng e{c, nullptr, nullptr};
+    MPOv mpo;
+    for (int i = 0; i < L; ++i) mpo.W.push_back(borrow(mpo_in[i]));
+    MPS psi;
+    for (int i = 0; i < L; ++i) psi.s.push_back(borrow(psi_io[i]));
+    psi.center = *center_io;
+    require(psi.center >= 1 && psi.center <= L, "centre out of range");
+    const cd tau(tau_re, tau_im), half = tau / 2.0;
+    Step S(e, mpo, Params{}, half, L);
+    const int root = std::max(1, std::min(L - 1, L / 2)) + 1;
+    const double wdiv = std::sqrt(double(root - 1)) + std::sqrt(double(L - root));
+    int64_t apps = 0, theta_max = 0, peak = 0;
+    double worst = 0.0, wsum[2] = {0.0, 0.0}, total = 0.0;
+    auto stored = [&]() {
+      int64_t n = 0;
+      for (auto& t : psi.s) n += t->nelem;
+      return n;
+    };
+    auto expv = [&](const std::function<T(const T&)>& op, cd t, const T& v) {
+      S.tau = t;
+      Step::ExpvRep rep;
+      auto counted = [&](const T& x) {
+        apps += 1;
+        T y = op(x);
+        return eshift == 0.0 ? y : e.lin({{1.0, y}, {-eshift, x}});
+      };
+      return hermitian ? S.lanczos_expv(counted, v, maxiter, tol, false, conv_tol, rep, substeps)
+                       : S.arnoldi_expv(counted, v, maxiter, tol, conv_tol, rep, substeps);
+    };
+    auto split = [&](const T& theta, int want) {
+      if (weight_tol < 0) return svd(e, theta, {0, 1}, std::max(trunc_thresh, 1e-14), maxdim, want);
+      SVDRes res = svd(e, theta, {0, 1}, 0.0, maxdim, want);
+      const double share = weight_tol * std::sqrt(sq_weight(res.kept) + sq_weight(res.trunc)) / wdiv;
+      const int nk = int(res.kept.size());
+      const int keep = std::max(tail_rank(res.kept, 1.0, share, nk, sq_weight(res.trunc)).first, 1);
+      if (keep < nk) res = svd(e, theta, {0, 1}, 0.0, keep, want);
+      return res;
+    };
+    auto bond = [&](int i, bool right, const T& lch, const T& rch, int sweep) -> T {
+      T theta = e.contract(psi[i], {2}, psi[i + 1], {0});
+      theta_max = std::max(theta_max, theta->nelem);
+      peak = std::max(peak, stored() + theta->nelem);
+      const T& Wl = mpo[i];
+      const T& Wr = mpo[i + 1];
+      theta = expv([&](const T& x) { return S.env.two_site(lch, Wl, Wr, rch, x); }, half, theta);
+      SVDRes res = split(theta, right ? (W_U | W_SVD) : (W_VD | W_US));
+      worst = std::max(worst, trunc_weight(res));
+      wsum[sweep] += sq_weight(res.trunc);
+      total = std::max(total, sq_weight(res.kept) + sq_weight(res.trunc));
+      if (right) {
+        psi[i] = res.U;
+        T lnext = S.env.left_step(lch, psi[i], Wl);
+        T M = SVd(e, res);
+        if (i < L - 1) M = expv([&](const T& x) { return S.env.one_site(lnext, Wr, rch, x); }, -half, M);
+        psi[i + 1] = M;
+        psi.center = i + 1;
+        return lnext;
+      }
+      psi[i + 1] = res.Vd;
+      T rnext = S.env.right_step(rch, psi[i + 1], Wr);
+      T M = US(e, res);
+      if (i > 1) M = expv([&](const T& x) { return S.env.one_site(lch, Wl, rnext, x); }, -half, M);
+      psi[i] = M;
+      psi.center = i;
+      return rnext;
+    };
+    S.canonical(psi, 1);
+    std::vector<T> rstack = S.right_env_stack(psi, 3);
+    T lch = S.env.left_boundary();
+    for (int i = 1; i <= L - 1; ++i) lch = bond(i, true, lch, rstack[i + 2], 0);
+    std::vector<T> lstack = S.left_env_stack(psi, L - 2);
+    T rch = S.env.right_boundary(S.total_charge(psi));
+    for (int i = L - 1; i >= 1; --i) {
+      S.canonical(psi, i);
+      rch = bond(i, false, lstack[i], rch, 1);
+    }
+    // outputs: new site handles (the caller owns them); an unchanged slot returns NULL
+    for (int i = 0; i < L; ++i) {
+      bug_tensor* raw = psi.s[i].get();
+      if (raw == psi_io[i]) {
+        psi_io[i] = nullptr;
+        continue;
+      }
+      psi_io[i] = std::make_unique<bug_tensor>(*raw).release();
+    }
+    *center_io = psi.center;
+    int64_t mb = 0;
+    for (auto d : psi.bond_dims()) mb = std::max(mb, d);
+    info->max_bond = int(mb);
+    info->theta_elements = theta_max;
+    info->discarded = worst;
+    info->peak_elements = peak;
+    info->krylov_dims = apps;
+    info->cumulative = total > 0 ? (std::sqrt(wsum[0]) + std::sqrt(wsum[1])) / std::sqrt(total) : 0.0;
+  });
+}
+
+extern "C" int bug_apply_two_site(bug_ctx* c, const bug_tensor* lenv, const bug_tensor* Wl,
+                                  const bug_tensor* Wr, const bug_tensor* renv,
+                                  const bug_tensor* theta, bug_tensor** out) {
+  return guard([&] {
+    require(c && out, "null argument");
+    Eng e{c, nullptr, nullptr};
+    Env env{e};
+    *out = hand_out(env.two_site(borrow(lenv), borrow(Wl), borrow(Wr), borrow(renv), borrow(theta)));
   });
 }
 

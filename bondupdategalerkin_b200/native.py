@@ -281,3 +281,59 @@ def observable_sz(psi) -> np.ndarray:
     E.check(ctx.lib.bug_observable_sz(ctx.h, len(psi.tensors), _handles(psi), psi.center,
                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     return out
+
+
+def apply_two_site(lenv: DT, Wl: DT, Wr: DT, renv: DT, theta: DT) -> DT:
+    """``apply_h_two_site`` (``mpo_environments.jl:316-344``) on a two-site tensor ``(l, s1, s2, r)``."""
+    return _call(theta.ctx, "bug_apply_two_site", lenv.h, Wl.h, Wr.h, renv.h, theta.h)
+
+
+# ── two-site TDVP baseline (``bug_tdvp2_step``) ───────────────────────────────────────────────
+
+
+class TDVP2Params(ctypes.Structure):
+    _fields_ = [("maxdim", ctypes.c_int), ("trunc_thresh", ctypes.c_double), ("maxiter", ctypes.c_int),
+                ("tol", ctypes.c_double), ("hermitian", ctypes.c_int), ("conv_tol", ctypes.c_double),
+                ("substeps", ctypes.c_int), ("weight_tol", ctypes.c_double), ("eshift", ctypes.c_double)]
+
+
+class TDVP2Info(ctypes.Structure):
+    _fields_ = [("max_bond", ctypes.c_int), ("theta_elements", ctypes.c_int64),
+                ("discarded", ctypes.c_double), ("peak_elements", ctypes.c_int64),
+                ("krylov_dims", ctypes.c_int64), ("cumulative", ctypes.c_double)]
+
+
+def tdvp2_step(psi, mpo, tau, *, maxdim=200, trunc_thresh=1e-12, maxiter=30, tol=1e-15,
+               hermitian=True, conv_tol=0.0, substeps=1, weight_tol=None, eshift=0.0) -> dict:
+    """``tdvp2_step!(psi, h, tau; ...)`` (``src/Baselines/TDVP/tdvp2.jl:229-297``): one symmetric
+    two-site TDVP step on an HBM-resident state, in place. Returns the ``TDVP2Info`` fields."""
+    L = len(psi)
+    if L < 2:
+        raise ValueError("tdvp2_step needs at least two sites")
+    if len(mpo) != L:
+        raise ValueError(f"chain has {len(mpo)} sites, state has {L}")
+    if weight_tol is not None and weight_tol < 0:
+        raise ValueError(f"weight_tol must be non-negative, got {weight_tol}")
+    lib = E.load()
+    lib.bug_tdvp2_step.restype = ctypes.c_int
+    lib.bug_tdvp2_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p),
+                                   ctypes.c_double, ctypes.c_double, ctypes.POINTER(TDVP2Params),
+                                   ctypes.POINTER(TDVP2Info)]
+    p = TDVP2Params(maxdim=int(maxdim), trunc_thresh=float(trunc_thresh), maxiter=int(maxiter),
+                    tol=float(tol), hermitian=int(hermitian), conv_tol=float(conv_tol),
+                    substeps=int(substeps), weight_tol=-1.0 if weight_tol is None else float(weight_tol),
+                    eshift=float(eshift))
+    ctx = psi.tensors[0].ctx
+    tau = complex(tau)
+    arr = (ctypes.c_void_p * L)(*[t.h.value for t in psi.tensors])
+    warr = (ctypes.c_void_p * L)(*[w.h.value for w in mpo.tensors])
+    center = ctypes.c_int(psi.center)
+    info = TDVP2Info()
+    E.check(lib.bug_tdvp2_step(ctx.h, L, arr, ctypes.byref(center), warr, tau.real, tau.imag,
+                               ctypes.byref(p), ctypes.byref(info)))
+    for i in range(L):
+        if arr[i]:
+            psi.tensors[i] = DT(ctx, ctypes.c_void_p(arr[i]))
+    psi.center = center.value
+    return {f: getattr(info, f) for f, _ in TDVP2Info._fields_}

@@ -282,6 +282,45 @@ int bug_site_populations(bug_ctx* ctx, int L, const bug_tensor* const* psi, int 
  * under :none the one charge-0 sector holds up (index 0) and down (index 1). */
 int bug_observable_sz(bug_ctx* ctx, int L, const bug_tensor* const* psi, int center, double* out);
 
+/* H Theta for a two-site tensor (l, s1, s2, r) (`apply_h_two_site`, mpo_environments.jl:316-344). */
+int bug_apply_two_site(bug_ctx* ctx, const bug_tensor* lenv, const bug_tensor* Wl,
+                       const bug_tensor* Wr, const bug_tensor* renv, const bug_tensor* theta,
+                       bug_tensor** out);
+
+/* ── two-site TDVP, the reference's matched-accuracy baseline ─────────────────────────────
+ * `tdvp2_step!(psi, h, tau; ...)` (src/Baselines/TDVP/tdvp2.jl:229-297). Keyword defaults in
+ * brackets are the reference's; a zero-initialised struct gets them except `substeps` and
+ * `hermitian`, which the caller sets (the reference's defaults: 1 and 1). */
+typedef struct {
+  int maxdim;          /* <= 0: 200 */
+  double trunc_thresh; /* Telum relative cutoff of each split (at least 1e-14); < 0: 1e-12 */
+  int maxiter;         /* Krylov dimension per exponential; <= 0: 30 */
+  double tol;          /* Krylov breakdown; <= 0: 1e-15 */
+  int hermitian;       /* 1 Lanczos, 0 Arnoldi */
+  double conv_tol;     /* Saad tail stop; 0: none */
+  int substeps;        /* 1 one step of each tau, > 1 equal substeps, 0 adaptive */
+  double weight_tol;   /* < 0: cut by trunc_thresh; >= 0: the BUG's budgeted cut
+                          weight_tol ||Theta|| / (sqrt(r - 1) + sqrt(L - r)), r = root link + 1 */
+  double eshift;       /* integrate H - eshift (imaginary time) */
+} bug_tdvp2_params;
+
+/* TDVP2Info (tdvp2.jl:17-24). */
+typedef struct {
+  int max_bond;
+  int64_t theta_elements; /* largest two-site tensor formed (stored elements) */
+  double discarded;       /* largest relative weight one split discarded */
+  int64_t peak_elements;  /* state + largest two-site tensor */
+  int64_t krylov_dims;    /* operator applications */
+  double cumulative;      /* relative discarded norm, accounted as in truncate_recursive! */
+} bug_tdvp2_info;
+
+/* One symmetric two-site TDVP step of `tau` in place (forward sweep of exp(tau/2 H2) updates with
+ * backward exp(-tau/2 H1) half-steps, then the mirror sweep). Handles as in bug_mps_step: each
+ * slot of `psi_io` returns a new handle owned by the caller, or NULL where unchanged. */
+int bug_tdvp2_step(bug_ctx* ctx, int L, bug_tensor** psi_io, int* center_io,
+                   const bug_tensor* const* mpo, double tau_re, double tau_im,
+                   const bug_tdvp2_params* params, bug_tdvp2_info* info);
+
 /* ── serving: many jobs on one GPU ─────────────────────────────────────────────────────────
  * No reference counterpart: the reference calls cbe_bug_step! one chain at a time. A server owns
  * `workers` threads, each with its own context (stream, memory, staging); jobs wait in one FIFO

@@ -212,3 +212,24 @@ def test_pivoted_qr_tie_rule():
     assert np.allclose(r, 1.0, atol=1e-14)
     ph = np.array([np.vdot(Q[:, j], X[:, j]) for j in range(6)])
     assert np.allclose(np.abs(ph), 1.0, atol=1e-13)
+
+
+def test_tdvp2_baseline_fixture():
+    """The two-site TDVP restatement against the reference's frozen ``baseline_tdvp2_xx`` run
+    (L = 10 XX from Neel, dt 0.05, maxdim 64, trunc_thresh 1e-12), with the bars of
+    ``test/Baselines/test_baselines.jl`` (S^z within 1e-5 of the frozen run and within
+    2 err_exact + 1e-6 of free fermions) and, tighter, the frozen bond dimensions and S^z to
+    1e-12."""
+    from oracle import tdvp as T
+
+    fz = GOLDEN["baseline_tdvp2_xx"]
+    L, dt = fz["L"], fz["dt"]
+    psi = M.neel_state(L)
+    mpo = M.xxz_mpo(L, J=1.0, delta=0.0)
+    for step, row in enumerate(fz["trajectory"][:4], start=1):
+        T.tdvp2_step(psi, mpo, -1j * dt, maxdim=64, trunc_thresh=1e-12)
+        sz = M.sz_profile(psi)
+        exact = M.free_fermion_sz(L, step * dt, occupied=range(0, L, 2))
+        assert np.max(np.abs(sz - np.array(row["sz"]))) <= 1e-12
+        assert np.max(np.abs(sz - exact)) <= 2 * row["err_exact"] + 1e-6
+        assert psi.bond_dims() == row["bond_dims"]
