@@ -14,6 +14,10 @@ through host buffers: the state and MPO uploaded and the new state downloaded ev
 ``cpu_baseline`` (the CPU oracle over a bounded sample of the same steps), ``clocks``.
 ``--impl reference`` times the CPU oracle (the restatement of the reference's CPU path) on the
 same steps. Under torchrun each rank runs an independent replica (the step does not shard).
+
+``--workload tdvp2`` measures the reference's matched-accuracy comparator, two-site TDVP
+(``tdvp2_step!``, maxdim 256, per-cut allowance ``weight_tol`` 1e-7, Lanczos with 30 iterations),
+over the same chain and 100-step trajectory (metric TDVP2 steps/s).
 """
 
 from __future__ import annotations
@@ -40,6 +44,10 @@ WORKLOAD_NAME = "xxz_quench_L64_delta0.5_domainwall_maxdim256_order2_tol1e-4"
 # tau = 0.02 (real), Arnoldi (non-Hermitian), maxdim 64, order 1, 50 steps.
 HESTON = dict(nbits=10, params=(0.03, 0.01, 2.0, 0.09, 0.4, -0.7), tau=0.02, maxdim=64, seed=1234)
 HESTON_NAME = "heston_qtt_10x10bits_maxdim64_tau0.02_arnoldi"
+# The reference's matched-accuracy comparator on the headline chain: two-site TDVP with the BUG's
+# per-cut allowance (weight_tol = the step's default tol_trunc 1e-7), maxdim 256, Lanczos.
+TDVP2 = dict(maxdim=256, weight_tol=1e-7)
+TDVP2_NAME = "tdvp2_xxz_quench_L64_delta0.5_domainwall_maxdim256_wtol1e-7"
 KIND = ["xxz"]
 L2_FLUSH_BYTES = 256 << 20
 _HESTON_DOMAIN = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
@@ -51,6 +59,30 @@ def tau():
 
 def seed():
     return HESTON["seed"] if KIND[0] == "heston" else WORKLOAD["seed"]
+
+
+def dev_step(mod, psi, mpo, rng):
+    """One step of the workload through the product module ``mod`` (native or Python host)."""
+    if KIND[0] == "tdvp2":
+        from bondupdategalerkin_b200 import native as N
+
+        return N.tdvp2_step(psi, mpo, tau(), **TDVP2)
+    return mod.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+
+
+def oracle_step(psi, mpo, rng):
+    """The same step in the CPU oracle."""
+    if KIND[0] == "tdvp2":
+        from oracle import tdvp as OT
+
+        return OT.tdvp2_step(psi, mpo, tau(), **TDVP2)
+    from oracle import step as OS
+
+    return OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+
+
+def metric_name():
+    return "tdvp2_steps_per_s" if KIND[0] == "tdvp2" else "bug_steps_per_s"
 
 
 def step_kwargs():
@@ -101,6 +133,15 @@ def config_dict(args, ws, max_bond=None):
             cfg["max_bond_dim_after"] = max_bond
         return cfg
     w = WORKLOAD
+    if KIND[0] == "tdvp2":
+        cfg = {"workload": TDVP2_NAME, "L": w["L"], "delta": w["delta"], "tau": "-0.05i",
+               "maxdim": TDVP2["maxdim"], "weight_tol": TDVP2["weight_tol"], "krylov": "lanczos, maxiter 30",
+               "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+               "l2": "flushed before every step (256 MiB write)",
+               "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+        if max_bond is not None:
+            cfg["max_bond_dim_after"] = max_bond
+        return cfg
     cfg = {"workload": WORKLOAD_NAME, "L": w["L"], "delta": w["delta"], "tau": "-0.05i",
            "order": w["order"], "tol_basis": w["tol_basis"], "maxdim": w["maxdim"],
            "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
@@ -204,15 +245,13 @@ def blas_threads():
 def oracle_steps(warmup, k):
     """Run the CPU oracle over the same trajectory: ``warmup`` untimed steps, then ``k`` timed.
     Returns (seconds for the k steps, bond dims after)."""
-    from oracle import step as OS
-
     psi, mpo = oracle_inputs()
     rng = np.random.default_rng(seed())
     for _ in range(warmup):
-        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+        oracle_step(psi, mpo, rng)
     t0 = time.perf_counter()
     for _ in range(k):
-        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+        oracle_step(psi, mpo, rng)
     return time.perf_counter() - t0, psi.bond_dims()
 
 
@@ -221,7 +260,6 @@ def oracle_sampled_steps(snaps, mpo_host=None):
     the generator state the device step started from. Returns (seconds, step numbers)."""
     from oracle import blocks as OB
     from oracle import models as OM
-    from oracle import step as OS
     from bondupdategalerkin_b200 import tensor as DT
 
     mpo = mpo_host or oracle_inputs()[1]
@@ -235,7 +273,7 @@ def oracle_sampled_steps(snaps, mpo_host=None):
         rng = np.random.default_rng()
         rng.bit_generator.state = rng_state
         t0 = time.perf_counter()
-        OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+        oracle_step(psi, mpo, rng)
         secs += time.perf_counter() - t0
         which.append(step_no)
     return secs, which
@@ -250,7 +288,7 @@ def run_reference(args):
     value = k / secs
     cores = blas_threads()
     line = {
-        "impl": "reference", "metric": "bug_steps_per_s", "value": value, "unit": "steps/s",
+        "impl": "reference", "metric": metric_name(), "value": value, "unit": "steps/s",
         "n_gpus": ws, "steps": k, "warmup": args.warmup, "ms_per_step": 1e3 * secs / k,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
@@ -297,7 +335,7 @@ def run_engine(args):
     psi, mpo = device_inputs()
     rng = np.random.default_rng(seed())
     for _ in range(args.warmup):
-        DS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+        dev_step(DS, psi, mpo, rng)
     start_psi = psi.copy()
     start_rng = rng.bit_generator.state
 
@@ -326,7 +364,7 @@ def run_engine(args):
             flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        DS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
+        dev_step(DS, psi, mpo, rng)
         e1.record(stream)
         evs.append((e0, e1))
     ctx.synchronize()
@@ -349,7 +387,7 @@ def run_engine(args):
     final_dims = psi.bond_dims()
     if args.no_replay:
         if rank == 0:
-            print(json.dumps({"metric": "bug_steps_per_s", "value": value, "unit": "steps/s",
+            print(json.dumps({"metric": metric_name(), "value": value, "unit": "steps/s",
                               "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
                               "ms_per_step": total_ms / args.steps, "gpu_launches": int(launches),
                               "host_waits": host_line,
@@ -368,14 +406,14 @@ def run_engine(args):
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()
-        DS.cbe_bug_step(psi_r, mpo, tau(), rng=rng_r, **step_kwargs())
+        dev_step(DS, psi_r, mpo, rng_r)
     ctx.synchronize()
     stats = ctx.kernel_stats()
     ctx.set_profiling(False)
     assert psi_r.bond_dims() == final_dims, "profiled replay diverged from the timed steps"
 
     # ── end to end through host buffers: upload state+MPO, step, download the new state ──
-    from bondupdategalerkin_b200.api import step_host
+    from bondupdategalerkin_b200.api import step_host, tdvp2_step_host
 
     host_state = [DT.to_blocks(t) for t in start_psi.tensors]
     host_mpo = [DT.to_blocks(t) for t in mpo.tensors]
@@ -388,8 +426,11 @@ def run_engine(args):
             flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
-                                           native=args.host == "native", **step_kwargs())
+        if KIND[0] == "tdvp2":
+            host_state, center, io = tdvp2_step_host(host_state, center, host_mpo, tau(), **TDVP2)
+        else:
+            host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
+                                               native=args.host == "native", **step_kwargs())
         e1.record(stream)
         ctx.synchronize()
         e2e_ms += e0.elapsed_time(e1)
@@ -426,7 +467,7 @@ def run_engine(args):
     roof["families"] = {f: {"launches": s["launches"], "ms": round(s["ms"], 3)} for f, s in stats.items()}
 
     line = {
-        "metric": "bug_steps_per_s", "value": value, "unit": "steps/s", "n_gpus": ws,
+        "metric": metric_name(), "value": value, "unit": "steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
@@ -612,10 +653,12 @@ def main():
                     help="time the steps only (for profiler runs)")
     ap.add_argument("--L", type=int, default=None,
                     help="chain length override (smaller cases for profiler captures only)")
-    ap.add_argument("--workload", default="xxz", choices=["xxz", "heston", "batch", "served"],
+    ap.add_argument("--workload", default="xxz",
+                    choices=["xxz", "heston", "tdvp2", "batch", "served"],
                     help="xxz: the L = 64 XXZ quench (the headline); heston: the 10 + 10-bit "
-                         "Heston QTT field (47 timed steps after 3 warm-up make its 50); batch: 64 "
-                         "chains at once on the job server; served: a Poisson job stream")
+                         "Heston QTT field (47 timed steps after 3 warm-up make its 50); tdvp2: the "
+                         "two-site TDVP baseline over the headline's 100-step trajectory; batch: 64 chains at once on the job server; served: a Poisson "
+                         "job stream")
     ap.add_argument("--workers", type=int, default=0, help="job server workers (0: min(16, cores))")
     ap.add_argument("--jobs", type=int, default=0, help="batch/served: number of jobs")
     ap.add_argument("--scale", type=float, default=0.25,

@@ -50,3 +50,27 @@ def step_host(host_state, center, host_mpo, tau, native=True, **kwargs):
     out = [to_blocks(t) for t in psi.tensors]
     d2h = sum(16 * t.nelem for t in psi.tensors)
     return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)
+
+
+def tdvp2_step_host(host_state, center, host_mpo, tau, **kwargs):
+    """One two-site TDVP step (``tdvp2_step!``) on host-resident data, as :func:`step_host` does
+    for the BUG step: upload, step on the device, download. Returns ``(new_host_state,
+    new_center, io)``."""
+    from .native import tdvp2_step
+
+    h2d = 0
+    sites = []
+    for legs, blocks in host_state:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        sites.append(t)
+    ws = []
+    for legs, blocks in host_mpo:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        ws.append(t)
+    psi = MPS(sites, center)
+    info = tdvp2_step(psi, MPO(ws), tau, **kwargs)
+    out = [to_blocks(t) for t in psi.tensors]
+    d2h = sum(16 * t.nelem for t in psi.tensors)
+    return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)

@@ -833,16 +833,10 @@ constexpr int64_t kDotChunk = 16384;
 
 // Run a descriptor list whose descriptors are grouped by output slot (seg[o]..seg[o+1]) through
 // the one-launch reduction; returns nout complex sums (read back, synchronising).
-void run_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<int>& seg, int nout,
-              double* out_re_im, double bytes_per_elem) {
-  if (nout <= 0) return;
-  if (descs.empty()) {
-    for (int i = 0; i < 2 * nout; ++i) out_re_im[i] = 0.0;
-    return;
-  }
+// The dot launch itself: sums of every output (re, im) written to `q` (device or host-mapped).
+void launch_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<int>& seg,
+                 int nout, double2* q, double bytes_per_elem) {
   double2* partial = static_cast<double2*>(c->scratch(descs.size() * sizeof(double2)));
-  double* host = c->readback(size_t(2 * nout));  // the kernel writes the sums here (host-mapped)
-  double2* res = reinterpret_cast<double2*>(host);
   DotDesc* dd = c->push(descs);
   int* dseg = c->push(seg);
   double dbytes = 0.0;
@@ -854,17 +848,28 @@ void run_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<i
   st.a = dd;
   st.b = dseg;
   st.p = partial;
-  st.q = res;
+  st.q = q;
   st.counter = c->counter();
   c->run_stage(st, BUG_K_DOT, 0.0, dbytes);
+}
+
+void run_dots(bug_ctx* c, const std::vector<DotDesc>& descs, const std::vector<int>& seg, int nout,
+              double* out_re_im, double bytes_per_elem) {
+  if (nout <= 0) return;
+  if (descs.empty()) {
+    for (int i = 0; i < 2 * nout; ++i) out_re_im[i] = 0.0;
+    return;
+  }
+  double* host = c->readback(size_t(2 * nout));  // the kernel writes the sums here (host-mapped)
+  launch_dots(c, descs, seg, nout, reinterpret_cast<double2*>(host), bytes_per_elem);
   c->wait();
   std::memcpy(out_re_im, host, size_t(nout) * sizeof(double2));
 }
 
-void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
-          double* out_re_im) {
-  std::vector<DotDesc> descs;
-  std::vector<int> seg(pairs.size() + 1, 0);
+// descriptors of <a_o, b_o> for every pair o: matching blocks in chunks of kDotChunk
+void dot_descs(const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
+               std::vector<DotDesc>& descs, std::vector<int>& seg) {
+  seg.assign(pairs.size() + 1, 0);
   for (size_t o = 0; o < pairs.size(); ++o) {
     seg[o] = int(descs.size());
     const bug_tensor& a = *pairs[o].first;
@@ -884,7 +889,26 @@ void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_t
     }
   }
   seg[pairs.size()] = int(descs.size());
+}
+
+void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
+          double* out_re_im) {
+  std::vector<DotDesc> descs;
+  std::vector<int> seg;
+  dot_descs(pairs, descs, seg);
   run_dots(c, descs, seg, int(pairs.size()), out_re_im, 32.0);
+}
+
+void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
+                 double2* q) {
+  std::vector<DotDesc> descs;
+  std::vector<int> seg;
+  dot_descs(pairs, descs, seg);
+  if (descs.empty()) {
+    BUG_CUDA(cudaMemsetAsync(q, 0, pairs.size() * sizeof(double2), c->stream));
+    return;
+  }
+  launch_dots(c, descs, seg, int(pairs.size()), q, 32.0);
 }
 
 // sum of |x|^2 over the blocks of `t` whose charge on `leg` is sector s, for every sector s of
@@ -920,7 +944,8 @@ std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg) {
 }
 
 std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
-                                         const bug_tensor* const* ts) {
+                                         const bug_tensor* const* ts, const double* const* cref,
+                                         const int* cmode) {
   require(n >= 1, "lincomb needs at least one tensor");
   const int rank = ts[0]->rank;
   std::vector<Leg> legs = ts[0]->legs;
@@ -945,7 +970,14 @@ std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
     for (int i = 0; i < n; ++i) {
       int b = ts[i]->find(out->blocks[j].key);
       if (b < 0) continue;
-      srcs.push_back(LinSrc{ts[i]->data(b), make_double2(coef[2 * i], coef[2 * i + 1])});
+      LinSrc ls{};
+      ls.src = ts[i]->data(b);
+      ls.coef = make_double2(coef[2 * i], coef[2 * i + 1]);
+      if (cmode && cmode[i]) {
+        ls.cref = cref[i];
+        ls.cmode = cmode[i];
+      }
+      srcs.push_back(ls);
     }
     o.src_end = int(srcs.size());
     outs.push_back(o);

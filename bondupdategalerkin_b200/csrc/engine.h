@@ -391,7 +391,13 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
              int& nkept, int want = 3, TensorPtr* US = nullptr, TensorPtr* SVd = nullptr);
 void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
           double* out_re_im);
-TensorPtr lincomb_impl(bug_ctx* c, int n, const double* coef, const bug_tensor* const* ts);
+// sum_i coef_i t_i; with cmode[i] != 0 the coefficient of t_i is computed on the device from the
+// dot product at cref[i] (bugk::LinSrc)
+TensorPtr lincomb_impl(bug_ctx* c, int n, const double* coef, const bug_tensor* const* ts,
+                       const double* const* cref = nullptr, const int* cmode = nullptr);
+// <a_o, b_o> for every pair written (re, im) to device memory `q`, no host wait
+void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
+                 double2* q);
 std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg);
 TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, double thr);
 TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& t, int leg, const double* w);

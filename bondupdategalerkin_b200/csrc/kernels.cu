@@ -234,7 +234,15 @@ __device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, 
     const LinOut& o = outs[find_desc(outs, nout, e)];
     const int64_t i = e - o.prefix;
     double2 acc = make_double2(0.0, 0.0);
-    for (int s = o.src_begin; s < o.src_end; ++s) cfma(acc, srcs[s].coef, ldg2(srcs[s].src + i));
+    for (int s = o.src_begin; s < o.src_end; ++s) {
+      double2 cf = srcs[s].coef;
+      if (srcs[s].cmode) {
+        const double x = __ldcg(srcs[s].cref);
+        const double r = sqrt(fmax(x, 0.0));
+        cf = make_double2(srcs[s].cmode == 1 ? -x : (srcs[s].cmode == 2 ? 1.0 / r : -r), 0.0);
+      }
+      cfma(acc, cf, ldg2(srcs[s].src + i));
+    }
     o.dst[i] = acc;
   }
 }

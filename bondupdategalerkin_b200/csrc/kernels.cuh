@@ -116,9 +116,16 @@ struct LinOut {
   int src_begin, src_end;
 };
 
+// One source of a linear combination: coef * src, or with `cmode` != 0 a coefficient computed in
+// the kernel from the real part x of a dot product the device wrote at `cref` (the recurrence
+// coefficients of a Krylov chain that the host has not read back): 1 -> -x, 2 -> 1/sqrt(max(x,0)),
+// 3 -> -sqrt(max(x,0)).
 struct LinSrc {
   const double2* src;
   double2 coef;
+  const double* cref;
+  int cmode;
+  int pad_;
 };
 
 struct ScaleDesc {

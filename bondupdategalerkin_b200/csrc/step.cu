@@ -1732,14 +1732,114 @@ struct Step {
   }
 
   struct ExpvRep {
-    int64_t iters = 0, nsub = 0;
+    int64_t iters = 0, nsub = 0, wasted = 0;  // wasted: applications past a deferred chain's cut
     double err = 0;
   };
+
+  // A linear combination whose coefficients may be device-resident dot products (bugk::LinSrc):
+  // mode 0 uses `coef`; 1, 2, 3 give -x, 1/sqrt(max(x, 0)), -sqrt(max(x, 0)) of the real part x
+  // at `ref`.
+  struct DevTerm {
+    cd coef;
+    int mode;
+    const double* ref;
+    T t;
+  };
+  T lin_dev(const std::vector<DevTerm>& terms) {
+    std::vector<double> coef;
+    std::vector<const bug_tensor*> ts;
+    std::vector<const double*> refs;
+    std::vector<int> modes;
+    for (auto& x : terms) {
+      coef.push_back(x.coef.real());
+      coef.push_back(x.coef.imag());
+      ts.push_back(x.t.get());
+      refs.push_back(x.ref);
+      modes.push_back(x.mode);
+    }
+    return Eng::sh(lincomb_impl(e.c, int(ts.size()), coef.data(), ts.data(), refs.data(), modes.data()));
+  }
+
+  // The Lanczos chain (no reorthogonalisation, no convergence test) with its coefficients left on
+  // the device: alpha_k and |r_k|^2 are written by the dot launches into device memory, and the
+  // combinations that need them compute -alpha, 1/|r| and -|r| in the kernel. The host reads the
+  // coefficients back once per chunk of iterations and replays the host-driven chain's stop (the
+  // first |r| below `tol`) on them: the arithmetic is the host-driven chain's, launch for launch,
+  // with one read-back per chunk instead of two per iteration. The first chunk is at most the
+  // vector's dimension long (a Krylov chain breaks down by then), later chunks kDeferredChunk; the
+  // iterations of the last chunk past the stop are discarded. Returns their applications.
+  static constexpr int kDeferredChunk = 8;
+  int64_t deferred_chain(const std::function<T(const T&)>& apply, const T& v0, int maxiter,
+                         double tol, std::vector<T>& basis, std::vector<double>& alpha,
+                         std::vector<double>& betas, double& betak) {
+    double2* A = static_cast<double2*>(e.c->scratch(size_t(2 * maxiter) * sizeof(double2)));
+    double2* N = A + maxiter;  // N[k] = |r|^2 after iteration k + 1
+    auto re = [](const double2* q) { return reinterpret_cast<const double*>(q); };
+    basis.assign(1, v0);
+    T residual = apply(v0);
+    dots_device(e.c, {{v0.get(), residual.get()}}, A);
+    residual = lin_dev({{1.0, 0, nullptr, residual}, {0.0, 1, re(A), v0}});
+    dots_device(e.c, {{residual.get(), residual.get()}}, N);
+    int ran = 1;  // iterations run on the device
+    int chunk = int(std::max<int64_t>(1, std::min<int64_t>(kDeferredChunk, v0->nelem)));
+    alpha.clear();
+    betas.clear();
+    betak = -1.0;
+    int used = -1;
+    int tested = 1;  // iterations whose continuation has been replayed on the host
+    while (true) {
+      const int target = std::min(maxiter, ran + chunk - (ran == 1 ? 1 : 0));
+      for (int it = ran + 1; it <= target; ++it) {
+        T v = lin_dev({{0.0, 2, re(N + (it - 2)), residual}});
+        basis.push_back(v);
+        residual = apply(v);
+        dots_device(e.c, {{v.get(), residual.get()}}, A + (it - 1));
+        residual = lin_dev({{1.0, 0, nullptr, residual},
+                            {0.0, 1, re(A + (it - 1)), v},
+                            {0.0, 3, re(N + (it - 2)), basis[basis.size() - 2]}});
+        dots_device(e.c, {{residual.get(), residual.get()}}, N + (it - 1));
+      }
+      ran = target;
+      double* host = e.c->readback(size_t(4 * maxiter));
+      BUG_CUDA(cudaMemcpyAsync(host, A, size_t(maxiter) * sizeof(double2), cudaMemcpyDeviceToHost,
+                               e.c->stream));
+      BUG_CUDA(cudaMemcpyAsync(host + 2 * maxiter, N, size_t(maxiter) * sizeof(double2),
+                               cudaMemcpyDeviceToHost, e.c->stream));
+      e.c->wait();
+      auto nrm = [&](int k) { return std::sqrt(std::max(host[2 * (maxiter + k)], 0.0)); };
+      if (alpha.empty()) alpha.push_back(host[0]);
+      // replay the stop test of iterations tested+1 .. ran+1 (the test of `it` reads N[it-2])
+      for (int it = tested + 1; it <= std::min(maxiter, ran + 1); ++it) {
+        const double off = nrm(it - 2);
+        if (off < tol) {
+          used = it - 1;
+          betak = off;
+          break;
+        }
+        if (it > ran) break;  // continues: the next chunk runs it
+        betas.push_back(off);
+        alpha.push_back(host[2 * (it - 1)]);
+        tested = it;
+      }
+      if (used > 0) break;
+      if (ran == maxiter) {
+        used = maxiter;
+        betak = nrm(maxiter - 1);
+        break;
+      }
+      tested = ran;
+      chunk = kDeferredChunk;
+    }
+    basis.resize(size_t(used));
+    alpha.resize(size_t(used));
+    betas.resize(size_t(used - 1));
+    return int64_t(ran - used);
+  }
 
   // substeps: 1 one step of the whole tau, > 1 that many equal substeps, 0 the adaptive substep
   // search (pick_tau)
   T lanczos_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
-                 bool reorth, double conv_tol, ExpvRep& rep, int substeps = 0) {
+                 bool reorth, double conv_tol, ExpvRep& rep, int substeps = 0, bool deferred = false) {
     const double beta0 = e.norm(vec);
     if (beta0 == 0) return vec;
     T cur = vec;
@@ -1751,41 +1851,48 @@ struct Step {
       const double cur_norm = e.norm(cur);
       if (cur_norm == 0) break;
       T v = e.scale(cur, 1.0 / cur_norm);
-      std::vector<T> basis{v};
+      std::vector<T> basis;
       std::vector<double> alpha, betas;
-      T residual = apply(v);
-      rep.iters += 1;
-      double a = e.inner(v, residual).real();
-      alpha.push_back(a);
-      residual = e.lin({{1.0, residual}, {-a, v}});
-      for (int it = 2; it <= maxiter; ++it) {
-        const double off = e.norm(residual);
-        if (off < tol) break;
-        if (conv_tol > 0) {
-          Eig eg = tridiag_eigen(alpha, betas);
-          auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
-          if (tail_sup(ev, tau_rem, off, conv_tol) < conv_tol) break;
-        }
-        betas.push_back(off);
-        v = e.scale(residual, 1.0 / off);
+      double betak = 0.0;
+      if (deferred && !reorth && conv_tol <= 0) {
+        rep.wasted += deferred_chain(apply, v, maxiter, tol, basis, alpha, betas, betak);
+        rep.iters += int64_t(basis.size());
+      } else {
         basis.push_back(v);
-        residual = apply(v);
+        T residual = apply(v);
         rep.iters += 1;
-        a = e.inner(v, residual).real();
+        double a = e.inner(v, residual).real();
         alpha.push_back(a);
-        residual = e.lin({{1.0, residual}, {-a, v}, {-off, basis[basis.size() - 2]}});
-        if (reorth) {
-          for (int pass = 0; pass < 2; ++pass) {
-            auto cs = e.inner_many(basis, residual);
-            std::vector<std::pair<cd, T>> terms{{1.0, residual}};
-            for (size_t i = 0; i < basis.size(); ++i) terms.push_back({-cs[i], basis[i]});
-            residual = e.lin(terms);
+        residual = e.lin({{1.0, residual}, {-a, v}});
+        for (int it = 2; it <= maxiter; ++it) {
+          const double off = e.norm(residual);
+          if (off < tol) break;
+          if (conv_tol > 0) {
+            Eig eg = tridiag_eigen(alpha, betas);
+            auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
+            if (tail_sup(ev, tau_rem, off, conv_tol) < conv_tol) break;
+          }
+          betas.push_back(off);
+          v = e.scale(residual, 1.0 / off);
+          basis.push_back(v);
+          residual = apply(v);
+          rep.iters += 1;
+          a = e.inner(v, residual).real();
+          alpha.push_back(a);
+          residual = e.lin({{1.0, residual}, {-a, v}, {-off, basis[basis.size() - 2]}});
+          if (reorth) {
+            for (int pass = 0; pass < 2; ++pass) {
+              auto cs = e.inner_many(basis, residual);
+              std::vector<std::pair<cd, T>> terms{{1.0, residual}};
+              for (size_t i = 0; i < basis.size(); ++i) terms.push_back({-cs[i], basis[i]});
+              residual = e.lin(terms);
+            }
           }
         }
+        betak = e.norm(residual);
       }
       Eig eg = tridiag_eigen(alpha, betas);
       auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
-      const double betak = e.norm(residual);
       const cd tau_s = substeps == 1 ? tau_rem
                        : substeps > 1 ? tau_rem / double(substeps - nsub + 1)
                                       : pick_tau(ev, tau_rem, betak, conv_tol);
@@ -1799,6 +1906,7 @@ struct Step {
     }
     return apply_scale(cur, logscale);
   }
+
 
   std::pair<std::vector<cd>, cd> hess_coeffs(const CMat& Hm, cd t) {
     const int n = Hm.n;
@@ -2415,8 +2523,12 @@ extern "C" int bug_tdvp2_step(bug_ctx* c, int L, bug_tensor** psi_io, int* cente
         T y = op(x);
         return eshift == 0.0 ? y : e.lin({{1.0, y}, {-eshift, x}});
       };
-      return hermitian ? S.lanczos_expv(counted, v, maxiter, tol, false, conv_tol, rep, substeps)
-                       : S.arnoldi_expv(counted, v, maxiter, tol, conv_tol, rep, substeps);
+      // Lanczos keeps its recurrence coefficients on the device (one read-back per chunk of
+      // iterations); applications past the host-driven chain's stop are not counted
+      T r = hermitian ? S.lanczos_expv(counted, v, maxiter, tol, false, conv_tol, rep, substeps, true)
+                      : S.arnoldi_expv(counted, v, maxiter, tol, conv_tol, rep, substeps);
+      apps -= rep.wasted;
+      return r;
     };
     auto split = [&](const T& theta, int want) {
       if (weight_tol < 0) return svd(e, theta, {0, 1}, std::max(trunc_thresh, 1e-14), maxdim, want);
