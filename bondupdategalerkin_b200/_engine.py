@@ -75,6 +75,8 @@ SIGNATURES = {
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
     "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
+    "bug_la_eigh_tridiag": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p,
+                                           _c_double_p]),
     "bug_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.POINTER(_vp)]),
     "bug_server_submit": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
     "bug_server_cancel": (ctypes.c_int, [_vp, ctypes.c_int64]),

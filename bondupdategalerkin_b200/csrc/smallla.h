@@ -4,6 +4,10 @@
 // eigenvalues; src/BUG/Core/LocalSolvers/krylov.jl:77-98, root_methods.jl:136-141) and Julia's
 // matrix `exp` for these. This file holds the engine's own implementations:
 //   * eigh_jacobi   -- cyclic Jacobi eigen-decomposition of a real symmetric matrix;
+//   * eigh_tridiag  -- eigen-decomposition of a symmetric tridiagonal matrix (the Lanczos
+//                      tridiagonal) by the implicit symmetric QR step with Wilkinson shift and
+//                      deflation (Golub & Van Loan, "Matrix Computations", Algorithms 8.3.2/8.3.3),
+//                      the rotations chased down the diagonal and off-diagonal directly;
 //   * expm          -- scaling and squaring with the degree-13 Pade approximant (Higham, "The
 //                      scaling and squaring method for the matrix exponential revisited", SIAM J.
 //                      Matrix Anal. Appl. 26 (2005)); the Pade coefficients are computed from
@@ -108,6 +112,70 @@ inline void eigh_jacobi(const RMat& A0, std::vector<double>& vals, RMat& V) {
   RMat W(n, n);
   for (int j = 0; j < n; ++j) {
     vals[j] = A(order[j], order[j]);
+    for (int i = 0; i < n; ++i) W(i, j) = V(i, order[j]);
+  }
+  V = W;
+}
+
+// Symmetric tridiagonal eigen-decomposition: diagonal `d` (n), off-diagonal `e` (n - 1). Returns
+// eigenvalues ascending and eigenvectors as columns of V. Each implicit QR step on an unreduced
+// block [lo, hi] starts with the rotation that takes (d_lo - mu, e_lo) to (r, 0), mu the
+// eigenvalue of the trailing 2 x 2 nearer its last entry, and chases the bulge down: the rotation
+// in plane (k, k+1) is G = [[c, s], [-s, c]], T <- G^T T G, V <- V G. Off-diagonals below
+// eps (|d_i| + |d_i+1|) are set to zero (deflation).
+inline void eigh_tridiag(std::vector<double> d, std::vector<double> e, std::vector<double>& vals,
+                         RMat& V) {
+  const int n = int(d.size());
+  V = RMat(n, n);
+  for (int i = 0; i < n; ++i) V(i, i) = 1.0;
+  e.resize(std::max(n - 1, 0));
+  const double eps = 2.220446049250313e-16;
+  auto negligible = [&](int i) { return std::fabs(e[i]) <= eps * (std::fabs(d[i]) + std::fabs(d[i + 1])); };
+  int hi = n - 1, steps = 0;
+  while (hi > 0) {
+    if (negligible(hi - 1)) {
+      e[hi - 1] = 0.0;
+      --hi;
+      continue;
+    }
+    int lo = hi - 1;
+    while (lo > 0 && !negligible(lo - 1)) --lo;
+    if (lo > 0) e[lo - 1] = 0.0;
+    if (++steps > 60 * n) throw std::runtime_error("eigh_tridiag: QR iteration did not converge");
+    // Wilkinson shift from the trailing 2 x 2 of the block
+    const double a = d[hi - 1], b = e[hi - 1], m = d[hi];
+    const double delta = 0.5 * (a - m);
+    const double den = delta + (delta >= 0.0 ? 1.0 : -1.0) * std::hypot(delta, b);
+    const double mu = den != 0.0 ? m - b * b / den : m;
+    double x = d[lo] - mu, z = e[lo], bulge = 0.0;
+    for (int k = lo; k < hi; ++k) {
+      const double r = std::hypot(x, z);
+      const double c = r != 0.0 ? x / r : 1.0, s = r != 0.0 ? -z / r : 0.0;
+      if (k > lo) e[k - 1] = c * e[k - 1] - s * bulge;  // the previous bulge is zeroed
+      const double dk = d[k], dk1 = d[k + 1], ek = e[k];
+      d[k] = c * c * dk - 2.0 * c * s * ek + s * s * dk1;
+      d[k + 1] = s * s * dk + 2.0 * c * s * ek + c * c * dk1;
+      e[k] = c * s * (dk - dk1) + (c * c - s * s) * ek;
+      if (k + 1 < hi) {
+        bulge = -s * e[k + 1];
+        e[k + 1] = c * e[k + 1];
+        x = e[k];
+        z = bulge;
+      }
+      for (int row = 0; row < n; ++row) {
+        const double vk = V(row, k), vk1 = V(row, k + 1);
+        V(row, k) = c * vk - s * vk1;
+        V(row, k + 1) = s * vk + c * vk1;
+      }
+    }
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return d[p] < d[q]; });
+  vals.resize(n);
+  RMat W(n, n);
+  for (int j = 0; j < n; ++j) {
+    vals[j] = d[order[j]];
     for (int i = 0; i < n; ++i) W(i, j) = V(i, order[j]);
   }
   V = W;

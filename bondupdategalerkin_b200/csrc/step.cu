@@ -1682,12 +1682,9 @@ struct Step {
   static Eig tridiag_eigen(const std::vector<double>& a, const std::vector<double>& b) {
     for (double x : a) require(std::isfinite(x), "Lanczos tridiagonal has non-finite entries");
     for (double x : b) require(std::isfinite(x), "Lanczos tridiagonal has non-finite entries");
-    const int n = int(a.size());
-    RMat Tm(n, n);
-    for (int i = 0; i < n; ++i) Tm(i, i) = a[i];
-    for (int i = 0; i + 1 < n; ++i) Tm(i, i + 1) = Tm(i + 1, i) = b[i];
     Eig eg;
-    smallla::eigh_jacobi(Tm, eg.vals, eg.vecs);
+    smallla::eigh_tridiag(a, std::vector<double>(b.begin(), b.begin() + std::max<ptrdiff_t>(ptrdiff_t(a.size()) - 1, 0)),
+                          eg.vals, eg.vecs);
     return eg;
   }
   static double tail(const std::vector<cd>& c, double betak) { return c.empty() ? 0.0 : betak * std::abs(c.back()); }
@@ -2619,6 +2616,20 @@ extern "C" int bug_la_expm(int n, const double* a, double* out) {
       out[2 * i] = R.a[i].real();
       out[2 * i + 1] = R.a[i].imag();
     }
+  });
+}
+
+extern "C" int bug_la_eigh_tridiag(int n, const double* d, const double* e, double* vals,
+                                   double* vecs) {
+  return guard([&] {
+    require(n >= 0, "bad size");
+    std::vector<double> dd(d, d + n), ee;
+    if (n > 1) ee.assign(e, e + n - 1);
+    std::vector<double> v;
+    smallla::RMat V;
+    smallla::eigh_tridiag(dd, ee, v, V);
+    for (int i = 0; i < n; ++i) vals[i] = v[i];
+    for (int i = 0; i < n * n; ++i) vecs[i] = V.a[i];
   });
 }
 

@@ -388,8 +388,13 @@ int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim);
  * matrix `exp` in _kry_weight/_hess_coeffs (krylov_enrichment.jl:89-120, root_methods.jl:136-141). */
 int bug_la_expm(int n, const double* a, double* out);
 /* Eigen-decomposition of a real symmetric n x n matrix (cyclic Jacobi): ascending eigenvalues and
- * eigenvectors as columns; replaces syevr in _tridiag_eigen (krylov.jl:77-98). */
+ * eigenvectors as columns (row-major n x n). */
 int bug_la_eigh(int n, const double* a, double* vals, double* vecs);
+/* Eigen-decomposition of the symmetric tridiagonal matrix with diagonal d (n) and off-diagonal e
+ * (n - 1) by implicit QR steps with Wilkinson shifts: ascending eigenvalues and eigenvectors as
+ * columns (row-major n x n); replaces syevr in _tridiag_eigen (krylov.jl:77-98), the step's
+ * Lanczos tridiagonal. */
+int bug_la_eigh_tridiag(int n, const double* d, const double* e, double* vals, double* vecs);
 /* Eigenvalues of a complex upper-Hessenberg n x n matrix; replaces geev in _hess_coeffs. */
 int bug_la_eigvals_hess(int n, const double* a, double* vals_re_im);
 /* The Krylov weight of v_{k+1} in exp(tau H) v_1 for the n x n Hessenberg matrix H (row-major,
