@@ -8,19 +8,27 @@
 * ``step_host(...)`` -- the same step for a caller whose state lives in host memory: the site
   tensors and the MPO are uploaded, the step runs on the device, and the new site tensors come back
   (the shape of a ``ccall`` from a Julia host that keeps its own containers);
-* ``magnetisation(psi)`` -- ``<S^z_j>`` for every site (``src/QMB/Observables/bond_observables.jl:15``).
+* ``magnetisation(psi)`` -- ``<S^z_j>`` for every site (``src/QMB/Observables/bond_observables.jl:15``);
+* ``tdvp2_step(psi, mpo, tau; ...)`` -- the two-site TDVP baseline (``src/Baselines/TDVP/tdvp2.jl``),
+  ``tdvp2_step_host`` its host-buffer form;
+* ``ite_step`` / ``ite_evolve`` and the step schedules -- normalised imaginary time
+  (``src/BUG/ITE/ite_step.jl``, ``schedules.jl``).
 """
 
 from __future__ import annotations
 
 from .models import MPO, MPS, domain_wall_state, neel_state, product_state, sz_profile, xxz_mpo
-from .native import cbe_bug_step
+from .ite import (beta_grid, geometric_schedule, ite_energy, ite_evolve, ite_step, log_panel_steps,
+                  uniform_beta_steps, uniform_schedule)
+from .native import cbe_bug_step, tdvp2_step
 from .step import DDQRExpansion
 from .step import cbe_bug_step as cbe_bug_step_python_host
 from .tensor import from_blocks, to_blocks
 
 __all__ = ["cbe_bug_step", "cbe_bug_step_python_host", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
-           "domain_wall_state", "neel_state", "product_state", "xxz_mpo"]
+           "domain_wall_state", "neel_state", "product_state", "xxz_mpo", "tdvp2_step",
+           "tdvp2_step_host", "ite_step", "ite_evolve", "ite_energy", "log_panel_steps",
+           "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule"]
 
 
 def magnetisation(psi):

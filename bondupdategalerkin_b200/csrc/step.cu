@@ -406,11 +406,14 @@ struct Env {
   }
 };
 
+// H0 - shift (apply_zero_site, effective_operators.jl:91-107; shift_h, :110-129)
 struct ZeroSiteH {
   T l, r;
+  double shift = 0.0;
   T apply(const Eng& e, const T& core) const {
     T t = e.contract(l, {2}, core, {0});
-    return e.contract(t, {1, 2}, r, {1, 2});
+    T y = e.contract(t, {1, 2}, r, {1, 2});
+    return shift == 0.0 ? y : e.lin({{1.0, y}, {-shift, core}});
   }
 };
 
@@ -861,6 +864,7 @@ struct Step {
   const MPOv& mpo;
   Params P;
   cd tau;
+  double eshift = 0.0;  // the generators are H - eshift
   int L, root_link;
   Alloc alloc{};
   std::vector<int64_t> wcap;
@@ -1363,7 +1367,7 @@ struct Step {
       const T& W = mpo[bond];
       auto applyH = [&](const T& v) {
         nmv += 1;
-        return env.one_site(lch, W, rch1, v);
+        return h1(lch, W, rch1, v);
       };
       auto kr = krylov_enrich(Kex, applyH, ex.U_ex, true, cap_at(bond), 1.0, true);
       record_krylov(bl, kr.second);
@@ -1397,7 +1401,7 @@ struct Step {
       const T& W = mpo[bond + 1];
       auto applyH = [&](const T& v) {
         nmv += 1;
-        return env.one_site(lch1, W, rch, v);
+        return h1(lch1, W, rch, v);
       };
       auto kr = krylov_enrich(Bex, applyH, ex.V_ex, false, cap_at(bond), 1.0, true);
       record_krylov(bl, kr.second);
@@ -1465,7 +1469,12 @@ struct Step {
   };
   ZeroSiteH root_generator(KL& fr) {
     return ZeroSiteH{env.left_step(fr.lenv, fr.lf[root_link], mpo[root_link]),
-                     env.right_step(fr.renv, fr.rf[root_link], mpo[root_link + 1])};
+                     env.right_step(fr.renv, fr.rf[root_link], mpo[root_link + 1]), eshift};
+  }
+  // H1 - eshift on a site tensor (shift_h: eshift = 0 is the unshifted action itself)
+  T h1(const T& lch, const T& W, const T& rch, const T& v) const {
+    T y = env.one_site(lch, W, rch, v);
+    return eshift == 0.0 ? y : e.lin({{1.0, y}, {-eshift, v}});
   }
   T project_root(const MPS& psi, KL& fr) {
     return e.contract(overlap_left(psi, fr.lf), {1}, overlap_right(psi, fr.rf), {0});
@@ -1520,14 +1529,25 @@ struct Step {
     int64_t added = 0, n_h1 = 0;
   };
 
-  FrontierHalf frontier_left(MPS Fm, KL& fr, double amp) {
+  // enrich = false measures only (estimate_global_complement_action): the frames stay, the
+  // environments are the frames' own
+  FrontierHalf frontier_left(MPS Fm, KL& fr, double amp, bool enrich = true) {
     FrontierHalf out;
     canonical(Fm, 1);
     auto rstack = right_env_stack(Fm, 3);
     T lch = env.left_boundary();
     T lenv = lch;
     T carry, Pm;
+    std::map<int, T> chain;
+    if (!enrich) {
+      T ch = env.left_boundary();
+      for (int bond = 1; bond <= root_link; ++bond) {
+        chain[bond] = ch;
+        if (bond < root_link) ch = env.left_step(ch, fr.lf[bond], mpo[bond]);
+      }
+    }
     for (int bond = 1; bond <= root_link; ++bond) {
+      if (!enrich) lch = chain[bond];
       T old = Pm ? e.contract(Pm, {1}, fr.lf[bond], {0}) : fr.lf[bond];
       T site_core = carry ? e.contract(carry, {1}, Fm[bond], {0}) : Fm[bond];
       BondFrame tsf = frame_onto_left(old, site_core, Fm[bond + 1]);
@@ -1537,7 +1557,7 @@ struct Step {
       Ledger bl;
       const bool quiet = indicator(alloc, lk) <= alloc.per_bond;
       T Wi;
-      if (!quiet) {
+      if (enrich && !quiet) {
         Expansion ex = dd_cbe_expand(tsf, bond, lch, rch, true, &bl, cap_at(bond));
         T rp = e.contract(Fm[bond + 1], {1, 2}, ex.V_ex, {1, 2}, false, true);
         T Kex = e.contract(site_core, {2}, rp, {0});
@@ -1545,7 +1565,7 @@ struct Step {
         const T& W = mpo[bond];
         auto applyH = [&](const T& v) {
           out.n_h1 += 1;
-          return env.one_site(lch, W, rch1, v);
+          return h1(lch, W, rch1, v);
         };
         auto kr = krylov_enrich(Kex, applyH, ex.U_ex, true, cap_at(bond), amp, false);
         record_krylov(bl, kr.second);
@@ -1553,20 +1573,20 @@ struct Step {
       } else {
         Wi = old;
       }
-      T Wn = polar_frame(Wi, true);
+      T Wn = enrich ? polar_frame(Wi, true) : old;
       out.frames[bond] = Wn;
       out.added += dim(Wn, 2) - dim(old, 2);
       log_bond(out.ledger, bl, bond, 0, int(dim(Wn, 2)));
-      Pm = e.contract(Wn, {0, 1}, old, {0, 1}, true, false);
+      if (enrich) Pm = e.contract(Wn, {0, 1}, old, {0, 1}, true, false);
       carry = e.contract(Wn, {0, 1}, site_core, {0, 1}, true, false);
       if (bond == root_link) lenv = lch;
-      if (bond < root_link) lch = env.left_step(lch, Wn, mpo[bond]);
+      if (enrich && bond < root_link) lch = env.left_step(lch, Wn, mpo[bond]);
     }
     out.env = lenv;
     return out;
   }
 
-  FrontierHalf frontier_right(MPS Fm, KL& fr, double amp) {
+  FrontierHalf frontier_right(MPS Fm, KL& fr, double amp, bool enrich = true) {
     FrontierHalf out;
     canonical(Fm, L);
     auto lstack = left_env_stack(Fm, L - 2);
@@ -1574,7 +1594,16 @@ struct Step {
     T renv = rch;
     T carry, Pm;
     std::vector<double> leak(L + 1, 0.0);
+    std::map<int, T> chain;
+    if (!enrich) {
+      T ch = env.right_boundary(total_charge(Fm));
+      for (int bond = L - 1; bond >= root_link; --bond) {
+        chain[bond] = ch;
+        if (bond > root_link) ch = env.right_step(ch, fr.rf[bond], mpo[bond + 1]);
+      }
+    }
     for (int bond = L - 1; bond >= root_link; --bond) {
+      if (!enrich) rch = chain[bond];
       T old = Pm ? e.contract(fr.rf[bond], {2}, Pm, {0}) : fr.rf[bond];
       T site_core = carry ? e.contract(Fm[bond + 1], {2}, carry, {0}) : Fm[bond + 1];
       BondFrame tsf = frame_onto_right(Fm[bond], site_core, old);
@@ -1584,7 +1613,7 @@ struct Step {
       Ledger bl;
       const bool quiet = indicator(alloc, lk) <= alloc.per_bond;
       T Zj;
-      if (!quiet) {
+      if (enrich && !quiet) {
         Expansion ex = dd_cbe_expand(tsf, bond, lch, rch, false, &bl, cap_at(bond));
         T lp = e.contract(ex.U_ex, {0, 1}, Fm[bond], {0, 1}, true, false);
         T Bex = e.contract(lp, {1}, site_core, {0});
@@ -1592,7 +1621,7 @@ struct Step {
         const T& W = mpo[bond + 1];
         auto applyH = [&](const T& v) {
           out.n_h1 += 1;
-          return env.one_site(lch1, W, rch, v);
+          return h1(lch1, W, rch, v);
         };
         auto kr = krylov_enrich(Bex, applyH, ex.V_ex, false, cap_at(bond), amp, false);
         record_krylov(bl, kr.second);
@@ -1600,14 +1629,14 @@ struct Step {
       } else {
         Zj = old;
       }
-      T Zn = polar_frame(Zj, false);
+      T Zn = enrich ? polar_frame(Zj, false) : old;
       out.frames[bond] = Zn;
       out.added += dim(Zn, 0) - dim(old, 0);
       log_bond(out.ledger, bl, bond, 1, int(dim(Zn, 0)));
-      Pm = e.contract(old, {1, 2}, Zn, {1, 2}, false, true);
+      if (enrich) Pm = e.contract(old, {1, 2}, Zn, {1, 2}, false, true);
       carry = e.contract(site_core, {1, 2}, Zn, {1, 2}, false, true);
       if (bond == root_link) renv = rch;
-      if (bond > root_link) rch = env.right_step(rch, Zn, mpo[bond + 1]);
+      if (enrich && bond > root_link) rch = env.right_step(rch, Zn, mpo[bond + 1]);
     }
     for (int b = root_link; b < L; ++b) out.leak.push_back(leak[b]);
     out.env = renv;
@@ -1619,16 +1648,19 @@ struct Step {
     double leak = 0;
     bool met = true, capped = false;
     Ledger ledger;
+    std::vector<double> leaks_left, leaks_right;  // per bond: 1..root, root..L-1
   };
 
-  Sweep frontier_sweep(KL& fr, const MPS& psi, const T& core, double nrm) {
+  Sweep frontier_sweep(KL& fr, const MPS& psi, const T& core, double nrm, bool enrich = true) {
     Sweep sw;
     const double nF = e.norm(core);
     if (nF <= FRONTIER_FLOOR * std::max(nrm, EPS)) return sw;
     MPS Fm = frontier_mps(psi, fr, core);
     const double amp = nF / std::max(nrm, EPS);
-    FrontierHalf rl = frontier_left(Fm, fr, amp);
-    FrontierHalf rr = frontier_right(Fm, fr, amp);
+    FrontierHalf rl = frontier_left(Fm, fr, amp, enrich);
+    FrontierHalf rr = frontier_right(Fm, fr, amp, enrich);
+    sw.leaks_left = rl.leak;
+    sw.leaks_right = rr.leak;
     sw.ledger.merge(rl.ledger);
     sw.ledger.merge(rr.ledger);
     double lL = 0, lR = 0;
@@ -2088,6 +2120,10 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     psi.center = *center_io;
     const cd tau(tau_re, tau_im);
     Step S(e, mpo, P, tau, L);
+    S.eshift = prm->eshift;
+    require(!prm->outside_residual || prm->root_report, "outside_residual needs root_report");
+    require(!prm->outside_residual || prm->rng_ctl, "outside_residual needs rng_ctl (a copy of the draw stream)");
+    require(!prm->outside_residual || P.order > 1, "the outside residual with the exact (unfolded) leak is not built");
     S.root_link = P.root > 0 ? P.root : std::max(1, std::min(L - 1, L / 2));
     require(S.root_link >= 1 && S.root_link <= L - 1, "root must be a bond in 1:L-1");
 
@@ -2183,16 +2219,92 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     ledger.proj_err = npsi > 0 ? S.projection_miss(psi, lf, rf) / npsi : 0.0;
     if (ledger.proj_err > P.tol_basis) ledger.unmet_(U_PROJECTION);
     ZeroSiteH gen{S.env.left_step(lenv_root, lf[S.root_link], mpo[S.root_link]),
-                  S.env.right_step(renv_root, rf[S.root_link], mpo[S.root_link + 1])};
+                  S.env.right_step(renv_root, rf[S.root_link], mpo[S.root_link + 1]), S.eshift};
     int64_t nroot_apps = 0;
     auto apply_root = [&](const T& v) {
       nroot_apps += 1;
       return gen.apply(e, v);
     };
+    auto solve_root = [&](const T& start, Step::ExpvRep& r) {
+      return P.hermitian ? S.lanczos_expv(apply_root, start, P.root_maxiter, 1e-15, P.reorth != 0, P.tol_expv, r)
+                         : S.arnoldi_expv(apply_root, start, P.root_maxiter, 1e-15, P.tol_expv, r);
+    };
     Step::ExpvRep rep;
-    T root_result = P.hermitian
-                        ? S.lanczos_expv(apply_root, root_start, P.root_maxiter, 1e-15, P.reorth != 0, P.tol_expv, rep)
-                        : S.arnoldi_expv(apply_root, root_start, P.root_maxiter, 1e-15, P.tol_expv, rep);
+    T root_result = solve_root(root_start, rep);
+    // the root report (_report_root!, bug_step_stages.jl:243-390)
+    const double NaN = std::numeric_limits<double>::quiet_NaN();
+    double r_e_pre = NaN, r_e_root = NaN, r_resid = NaN, r_init = NaN, r_out = NaN, r_outl = NaN,
+           r_outr = NaN;
+    int r_passes = 0, r_added = 0;
+    if (prm->root_report) {
+      auto rayleigh = [&](const T& v) {
+        const double n2 = std::pow(e.norm(v), 2);
+        if (!(n2 > 0)) return NaN;
+        return e.inner(v, gen.apply(e, v)).real() / n2 + S.eshift;
+      };
+      // estimate_global_complement_action (frontier_closure.jl:238-277, nsample = 0): the
+      // per-bond two-site misses of a non-enriching frontier sweep, drawn from a copy of the stream
+      struct Action {
+        double left = 0, right = 0, bound = 0;
+        bool have = false;
+      };
+      auto outside_of = [&](const T& core) {
+        Action a;
+        Step::KL kf{lf, rf, lenv_root, renv_root, 0};
+        prm->rng_ctl(prm->rng_ctl_user, 0);
+        auto sw = S.frontier_sweep(kf, psi, core, std::max(e.norm(core), EPS), false);
+        prm->rng_ctl(prm->rng_ctl_user, 1);
+        for (double x : sw.leaks_left) a.left += x * x;
+        for (double x : sw.leaks_right) a.right += x * x;
+        a.bound = std::sqrt(a.left + a.right);
+        a.left = std::sqrt(a.left);
+        a.right = std::sqrt(a.right);
+        a.have = true;
+        return a;
+      };
+      auto residual_of = [&](const Action& a, const T& v) {
+        return a.have ? std::abs(tau) * a.bound / std::max(e.norm(v), EPS) : NaN;
+      };
+      r_e_pre = rayleigh(root_start);
+      Action outside;
+      if (prm->outside_residual) outside = outside_of(root_result);
+      r_init = residual_of(outside, root_result);
+      if (prm->outside_residual) {
+        while (!(residual_of(outside, root_result) <= P.tol_basis) && r_passes < 2 * P.order + 2) {
+          Step::KL kf{lf, rf, lenv_root, renv_root, 0};
+          r_passes += 1;
+          auto sw = S.frontier_sweep(kf, psi, root_result, nrm, true);
+          ledger.merge(sw.ledger);
+          if (sw.added == 0) break;
+          r_added += int(sw.added);
+          lf = kf.lf;
+          rf = kf.rf;
+          lenv_root = kf.lenv;
+          renv_root = kf.renv;
+          root_start = S.project_root(psi, kf);
+          gen = S.root_generator(kf);
+          rep = Step::ExpvRep{};
+          root_result = solve_root(root_start, rep);
+          outside = outside_of(root_result);
+          if (sw.capped) break;
+        }
+        if (r_added > 0) {
+          for (int b = 1; b < S.root_link; ++b) expanded[b - 1] = dim(lf[b], 2);
+          for (int b = S.root_link + 1; b < L; ++b) expanded[b - 1] = dim(rf[b], 0);
+          int64_t mx = 0;
+          for (auto x : expanded) mx = std::max(mx, x);
+          ledger.r_aug = std::max(mx, dim(rf[S.root_link], 0));
+        }
+      }
+      r_e_root = rayleigh(root_result);
+      if (outside.have) {
+        const double rn = std::max(e.norm(root_result), EPS);
+        r_out = outside.bound / rn;
+        r_outl = outside.left / rn;
+        r_outr = outside.right / rn;
+        r_resid = std::abs(tau) * outside.bound / rn;
+      }
+    }
     ledger.expv_err = rep.err;
     ledger.expv_iters = rep.iters;
     if (rep.err > P.tol_expv * (1 + 1e-8)) ledger.unmet_(U_EXPV);
@@ -2253,6 +2365,15 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     o.expv_iters = ledger.expv_iters;
     o.n_probes = ledger.n_probes;
     o.n_holdout = ledger.n_holdout;
+    o.e_pre = r_e_pre;
+    o.e_root = r_e_root;
+    o.resid = r_resid;
+    o.resid_initial = r_init;
+    o.outside = r_out;
+    o.outside_left = r_outl;
+    o.outside_right = r_outr;
+    o.outside_passes = r_passes;
+    o.outside_added = r_added;
     o.n_targeted = ledger.n_targeted;
     o.n_selected = ledger.n_selected;
     o.n_krylov = ledger.n_krylov;

@@ -20,6 +20,9 @@ MAX_SITES = 1024
 UNMET_NAMES = {1: "sample", 2: "tail", 3: "krylov", 4: "trunc", 5: "projection", 6: "expv", 7: "closure"}
 
 
+RNG_CTL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int)
+
+
 class StepParams(ctypes.Structure):
     _fields_ = [("tol_basis", ctypes.c_double), ("tol_trunc", ctypes.c_double),
                 ("tol_expv", ctypes.c_double), ("tol_krylov", ctypes.c_double),
@@ -30,7 +33,10 @@ class StepParams(ctypes.Structure):
                 ("tail_factor", ctypes.c_double), ("krylov_mode", ctypes.c_int),
                 ("krylov_fixed_depth", ctypes.c_int), ("dd_mode", ctypes.c_int),
                 ("holdout_width", ctypes.c_int), ("batch_blocks", ctypes.c_int),
-                ("cap_selection", ctypes.c_int), ("acceptance_factor", ctypes.c_double)]
+                ("cap_selection", ctypes.c_int), ("acceptance_factor", ctypes.c_double),
+                ("eshift", ctypes.c_double), ("root_report", ctypes.c_int),
+                ("outside_residual", ctypes.c_int), ("rng_ctl", RNG_CTL_FN),
+                ("rng_ctl_user", ctypes.c_void_p)]
 
 
 class BondLog(ctypes.Structure):
@@ -62,7 +68,11 @@ class StepInfo(ctypes.Structure):
                 ("n_h1_closure", ctypes.c_int64), ("n_compress", ctypes.c_int64),
                 ("leak1", ctypes.c_double), ("expanded", ctypes.c_int * MAX_SITES),
                 ("n_new", ctypes.c_int * MAX_SITES), ("workcap", ctypes.c_int * MAX_SITES),
-                ("n_holdout", ctypes.c_int64), ("n_targeted", ctypes.c_int64)]
+                ("n_holdout", ctypes.c_int64), ("n_targeted", ctypes.c_int64),
+                ("e_pre", ctypes.c_double), ("e_root", ctypes.c_double), ("resid", ctypes.c_double),
+                ("resid_initial", ctypes.c_double), ("outside", ctypes.c_double),
+                ("outside_left", ctypes.c_double), ("outside_right", ctypes.c_double),
+                ("outside_passes", ctypes.c_int), ("outside_added", ctypes.c_int)]
 
 
 DRAW_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double))
@@ -136,9 +146,14 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
                  order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
                  reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
                  root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
-                 closure_checks=False):
+                 closure_checks=False, eshift=0.0, root_report=None, outside_residual=False):
     """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
-    HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields)."""
+    HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields). The
+    generators are ``H - eshift``; a dict passed as ``root_report`` receives the root's energies
+    and, with ``outside_residual``, the outside-Galerkin defect after its re-enrichment
+    (``_report_root!``, ``bug_step_stages.jl:243-390``)."""
+    if outside_residual and root_report is None:
+        raise ValueError("outside_residual needs root_report")
     L = len(psi)
     if len(mpo) != L:
         raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
@@ -155,6 +170,20 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     def draw(user, n, out):
         x = rng.standard_normal(int(n))
         ctypes.memmove(out, x.ctypes.data, 8 * int(n))
+
+    saved = []
+
+    @RNG_CTL_FN
+    def rng_ctl(user, op):
+        if op == 0:
+            saved.append(rng.bit_generator.state)
+        else:
+            rng.bit_generator.state = saved.pop()
+
+    p.eshift = float(eshift)
+    p.root_report = int(root_report is not None)
+    p.outside_residual = int(bool(outside_residual))
+    p.rng_ctl = rng_ctl
 
     ctx = psi.tensors[0].ctx
     tau = complex(tau)
@@ -188,6 +217,12 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         bond_log=[{f: getattr(logs[i], f) for f, _ in BondLog._fields_} for i in range(min(nlog.value, cap))],
     )
     ledger.status = lambda: "met" if ledger.tolerance_met else "budget_unmet"
+    if root_report is not None:
+        root_report.update(
+            eshift=float(eshift), e_pre=info.e_pre, e_root=info.e_root,
+            resid_initial=info.resid_initial, outside_passes=info.outside_passes,
+            outside_added=info.outside_added, outside=info.outside, outside_left=info.outside_left,
+            outside_right=info.outside_right, resid=info.resid)
     return dict(
         expanded=list(info.expanded[:L - 1]), n_new=list(info.n_new[:L - 1]),
         root_link=info.root_link, root_rank=info.root_rank, err_pre=0.0, err_fnl=0.0,

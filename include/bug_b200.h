@@ -158,6 +158,11 @@ int bug_trim(bug_ctx* ctx, const bug_tensor* t, int leg, const int* counts, bug_
 /* Keyword arguments of `cbe_bug_step!` (bug_step.jl:17-148); a non-positive value selects the
  * reference default noted beside it (TOL_DEFAULTS, basis_budget.jl:568; DDQRExpansion,
  * src/BUG/Randomised/cbe.jl:254-290). */
+/* Saves (op 0) or restores (op 1) the caller's Gaussian stream: the outside-residual
+ * measurement draws from a copy of the stream (the reference measures with `copy(rng)`,
+ * bug_step_stages.jl:309-317), so the step's own draws continue from the saved state. */
+typedef void (*bug_rng_ctl_fn)(void* user, int op);
+
 typedef struct {
   double tol_basis;           /* <= 0: 1e-5 */
   double tol_trunc;           /* < 0: 1e-7 */
@@ -182,6 +187,12 @@ typedef struct {
   int batch_blocks;           /* :adaptive blocks per holdout, 1..8; <= 0: 1 */
   int cap_selection;          /* :adaptive past the cap: 0 :storage (first sectors), 1 :svd */
   double acceptance_factor;   /* :adaptive acceptance, (0, 1]; <= 0: 1 */
+  double eshift;              /* the generators are H - eshift (shift_h, effective_operators.jl:110-129) */
+  int root_report;            /* fill the info's root report (_report_root!, bug_step_stages.jl:243-390) */
+  int outside_residual;       /* with root_report: measure |tau| ||(I-P) H psi_1|| / ||psi_1|| and
+                                 re-enrich on it (at most 2 order + 2 passes); needs rng_ctl */
+  bug_rng_ctl_fn rng_ctl;
+  void* rng_ctl_user;
 } bug_step_params;
 
 /* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
@@ -222,6 +233,11 @@ typedef struct {
   int n_new[BUG_MAX_SITES];
   int workcap[BUG_MAX_SITES];
   int64_t n_holdout, n_targeted; /* holdout probe columns; sectors targeted (:adaptive) */
+  /* root report (NaN where not measured): Rayleigh-quotient energies of the root start and
+   * result (+ eshift), the outside defect before and after re-enrichment, its left/right parts
+   * and bound relative to ||psi_1||, the re-enrichment passes and directions added */
+  double e_pre, e_root, resid, resid_initial, outside, outside_left, outside_right;
+  int outside_passes, outside_added;
 } bug_step_info;
 
 /* One rank-adaptive BUG step in place: `cbe_bug_step!(psi, mpo, tau; ...)`

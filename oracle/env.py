@@ -89,13 +89,19 @@ def apply_one_site(Lenv: BT, W: BT, Renv: BT, x: BT) -> BT:
 class ZeroSiteH:
     """``H0 S = sum_w L[w] S R[w]`` through the expanded frames (``effective_operators.jl:78-107``)."""
 
-    def __init__(self, mpo, bond, lenv, renv, U_ex, V_ex):
+    def __init__(self, mpo, bond, lenv, renv, U_ex, V_ex, eshift=0.0):
         self.l = left_step(lenv, U_ex, mpo[bond])
         self.r = right_step(renv, V_ex, mpo[bond + 1])
+        self.eshift = float(eshift)  # applies H0 - eshift (shift_h)
 
     def apply(self, core: BT) -> BT:
         t = contract(self.l, (2,), core, (0,))     # (bra_l, w, b_r)
-        return contract(t, (1, 2), self.r, (1, 2))  # (bra_l, bra_r)
+        y = contract(t, (1, 2), self.r, (1, 2))    # (bra_l, bra_r)
+        if self.eshift == 0.0:
+            return y
+        from .blocks import add
+
+        return add(y, core, 1.0, -self.eshift)
 
 
 def stream_left(left_amplitude: BT, right_isometry: BT, mpo, bond, lenv, renv, Om: BT) -> BT:

@@ -1,0 +1,219 @@
+"""CPU restatement of normalised imaginary-time CBE-BUG (test infrastructure: the checker of the
+product's ``ite.py``, never part of the product).
+
+Follows ``src/BUG/ITE/ite_step.jl`` (``ite_step!`` ``:129-231``, ``_ite_attempt!`` ``:62-126``,
+``_ite_nsplit`` ``:40-44``, ``_ite_capped`` ``:53``, ``_ite_result`` ``:238-262``, ``ite_evolve!``
+``:273-301``, ``_ite_energy``/``_ite_normalise!`` ``:4-17``) and ``src/BUG/ITE/schedules.jl``. One
+branch is not restated: a step whose order-p closure is unmet is re-attempted by the reference
+with ``closure_checks = true`` (the multi-pass closure loop), which this restatement does not
+have; such a step goes straight to the split.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import blocks as B
+from .env import left_env_stack
+from .step import cbe_bug_step
+
+ITE_MAXSPLIT = 64  # _ITE_MAXSPLIT
+
+
+def mpo_energy(psi, mpo) -> complex:
+    """``<psi|H|psi>`` by pushing the left environment through every site."""
+    E = left_env_stack(psi, mpo, upto=len(psi))[len(psi) + 1]
+    (v,) = E.blocks.values()
+    return complex(v.reshape(-1)[0])
+
+
+def ite_energy(psi, mpo) -> float:
+    """``_ite_energy``: ``<psi|H|psi> / <psi|psi>``."""
+    n2 = B.norm(psi[psi.center]) ** 2
+    return mpo_energy(psi, mpo).real / max(n2, np.finfo(float).eps)
+
+
+def ite_normalise(psi) -> float:
+    """``_ite_normalise!``: renormalise through the centre tensor; returns the old norm."""
+    n = B.norm(psi[psi.center])
+    if not (math.isfinite(n) and n > 0):
+        raise ArithmeticError(f"imaginary-time step produced a state of norm {n} -- not representable")
+    psi[psi.center] = B.scale(psi[psi.center], 1.0 / n)
+    return n
+
+
+def nsplit(attempt, tol_basis, order) -> int:
+    """``_ite_nsplit``: sub-steps of a rejected attempt."""
+    r = attempt["resid"]
+    if not ("outside" in attempt["unmet"] and math.isfinite(r) and r > tol_basis):
+        return 2
+    return min(max(math.ceil(1.2 * (r / tol_basis) ** (1.0 / (order + 1))), 2), ITE_MAXSPLIT)
+
+
+def capped(attempt) -> bool:
+    """``_ite_capped``: a resource-capped failure (maxdim or the work ceiling)."""
+    lg = attempt["info"]["ledger"]
+    return bool(lg.maxdim_reached or lg.workcap_reached)
+
+
+def attempt_step(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxdim, eshift,
+                 outside_residual, rng, step=cbe_bug_step, energy=ite_energy,
+                 normalise=ite_normalise, **kwargs):
+    """``_ite_attempt!``: one step at ``tau = -dbeta`` with the shifted generators and the root
+    report, renormalisation, the energies and the verdicts."""
+    t0 = time.perf_counter()
+    e_before = energy(psi, mpo)
+    es = e_before if eshift == "energy" else float(eshift)
+    rep = {}
+    info = step(psi, mpo, complex(-dbeta), order=order, eshift=es, tol_basis=tol_basis,
+                tol_trunc=tol_trunc, tol_expv=tol_root, maxdim=maxdim, root_report=rep,
+                outside_residual=outside_residual, rng=rng, **kwargs)
+    growth = normalise(psi)
+    e_after = energy(psi, mpo)
+    unmet = list(info["ledger"].unmet)
+    if outside_residual and not (rep["resid"] <= tol_basis):
+        unmet.append("outside")
+    return dict(
+        dbeta=dbeta, ok=not unmet, unmet=unmet, eshift=es, e_before=e_before,
+        e_pre_root=rep["e_pre"], e_root=rep["e_root"], e_after=e_after,
+        de_root=rep["e_root"] - rep["e_pre"], de_compression=e_after - rep["e_root"],
+        outside=rep["outside"], resid=rep["resid"], resid_initial=rep["resid_initial"],
+        outside_passes=rep["outside_passes"], outside_added=rep["outside_added"],
+        root_err=info["ledger"].expv_err, root_iters=info["ledger"].expv_iters,
+        discarded=info["ledger"].discarded, growth=growth, chi=max(psi.bond_dims(), default=0),
+        r_aug=info["ledger"].r_aug, closure_checks=False, wall=time.perf_counter() - t0, info=info)
+
+
+def result(status, pieces, attempts, t0):
+    """``_ite_result``: fold the accepted pieces of a step into one record."""
+    unmet = []
+    for piece in pieces:
+        for u in piece["unmet"]:
+            if u not in unmet:
+                unmet.append(u)
+    return dict(
+        status=status, unmet=unmet, dbeta=sum(p["dbeta"] for p in pieces),
+        e_before=pieces[0]["e_before"], e_pre_root=pieces[0]["e_pre_root"],
+        e_root=pieces[-1]["e_root"], e_after=pieces[-1]["e_after"],
+        de_root=sum(p["de_root"] for p in pieces),
+        de_compression=sum(p["de_compression"] for p in pieces),
+        resid=max(p["resid"] for p in pieces), outside=max(p["outside"] for p in pieces),
+        root_err=max(p["root_err"] for p in pieces), discarded=max(p["discarded"] for p in pieces),
+        chi=pieces[-1]["chi"], nsub=sum(p.get("nsub", 1) for p in pieces), attempts=attempts,
+        wall=time.perf_counter() - t0)
+
+
+def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol_trunc=1e-6,
+             tol_root=1e-6, maxdim=128, eshift="energy", outside_residual=True, retries=2,
+             on_fail="flag", parallel=False, rng=None, step=cbe_bug_step, energy=ite_energy,
+             normalise=ite_normalise, **kwargs):
+    """``ite_step!``: one normalised imaginary-time step over ``dbeta`` in place, accepted when the
+    ledger is met and the outside defect is within ``tol_basis``; otherwise re-done as sub-steps
+    while ``retries`` last (resource-capped failures are not split)."""
+    if not dbeta > 0:
+        raise ValueError(f"dbeta must be positive, got {dbeta}")
+    if root_method != "exp":
+        raise NotImplementedError(f"root_method {root_method!r}: only :exp is built")
+    if on_fail not in ("flag", "error"):
+        raise ValueError("on_fail must be flag or error")
+    if retries < 0:
+        raise ValueError(f"retries must be >= 0, got {retries}")
+    if parallel:
+        raise NotImplementedError("parallel half-sweeps are not built")
+    if rng is None:
+        rng = np.random.default_rng(0x5EED)
+    t0 = time.perf_counter()
+    normalise(psi)
+    saved = psi.copy()
+    akw = dict(order=order, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_root=tol_root,
+               maxdim=maxdim, eshift=eshift, outside_residual=outside_residual, rng=rng,
+               step=step, energy=energy, normalise=normalise)
+
+    def restore():
+        for site in range(1, len(psi) + 1):
+            psi[site] = saved[site]
+        psi.center = saved.center
+
+    attempts = []
+    attempt = attempt_step(psi, mpo, float(dbeta), **akw, **kwargs)
+    attempts.append(attempt)
+    if attempt["ok"]:
+        return result("met", [attempt], attempts, t0)
+    if retries > 0 and not capped(attempt):
+        restore()
+        count = nsplit(attempt, tol_basis, order)
+        halves = []
+        for _ in range(count):
+            sub = ite_step(psi, mpo, dbeta / count, root_method=root_method, retries=retries - 1,
+                           on_fail="flag", **akw, **kwargs)
+            attempts += sub["attempts"]
+            halves.append(sub)
+        ok = all(h["status"] != "failed" for h in halves)
+        res = result("retried" if ok else "failed", halves, attempts, t0)
+        if not ok and on_fail == "error":
+            raise ArithmeticError(f"imaginary-time step dbeta={dbeta} failed after retries: "
+                                  f"unmet {res['unmet']}")
+        return res
+    if on_fail == "error":
+        raise ArithmeticError(f"imaginary-time step dbeta={dbeta} failed: unmet {attempt['unmet']}")
+    return result("failed", [attempt], attempts, t0)
+
+
+def ite_evolve(psi, mpo, steps, observe=None, **kwargs):
+    """``ite_evolve!``: one ``ite_step`` per entry of ``steps``; one record per step with the
+    ``beta`` reached (and ``obs`` when ``observe`` is given)."""
+    log = []
+    beta = 0.0
+    for db in steps:
+        rec = ite_step(psi, mpo, db, **kwargs)
+        beta += db
+        rec = dict(beta=beta, **rec)
+        if observe is not None:
+            rec["obs"] = observe(psi)
+        log.append(rec)
+    return log
+
+
+# ── schedules (schedules.jl) ──────────────────────────────────────────────────────────────────
+
+
+def log_panel_steps(beta_max, panel_count, per_panel=4):
+    """``log_panel_steps``: ``panel_count`` dyadic panels with endpoints ``0, beta_max /
+    2^(P-1), ..., beta_max``, each split into ``per_panel`` uniform steps."""
+    if not beta_max > 0:
+        raise ValueError(f"beta_max must be positive, got {beta_max}")
+    if panel_count < 1:
+        raise ValueError(f"log_panel_steps needs panel_count >= 1, got {panel_count}")
+    if per_panel < 1:
+        raise ValueError(f"per_panel must be >= 1, got {per_panel}")
+    edges = [0.0] + [float(beta_max) / 2.0 ** (panel_count - p) for p in range(1, panel_count + 1)]
+    out = []
+    for p in range(panel_count):
+        out += [(edges[p + 1] - edges[p]) / per_panel] * per_panel
+    return out
+
+
+def uniform_beta_steps(beta_max, step_count):
+    """``uniform_beta_steps``: ``step_count`` equal steps reaching ``beta_max``."""
+    if not beta_max > 0:
+        raise ValueError(f"beta_max must be positive, got {beta_max}")
+    if step_count < 1:
+        raise ValueError(f"step_count must be >= 1, got {step_count}")
+    return [float(beta_max) / step_count] * step_count
+
+
+def beta_grid(steps):
+    """The grid points ``0, b_1, ..., beta_max`` a step list reaches."""
+    return [0.0] + list(np.cumsum(np.asarray(steps, dtype=float)))
+
+
+def uniform_schedule(step_size, step_count):
+    return [float(step_size)] * step_count
+
+
+def geometric_schedule(first_step, ratio, hmax, step_count):
+    """``dtau_k = min(hmax, first_step * ratio^k)``, ``k = 0..step_count-1``."""
+    return [min(float(hmax), first_step * ratio ** k) for k in range(step_count)]

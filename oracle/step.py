@@ -209,6 +209,12 @@ class Ctx:
     recurrence: str
     wcap: list
     rng: object
+    eshift: float = 0.0  # the generators are H - eshift (shift_h, effective_operators.jl:110-129)
+
+
+def shifted(y, x, s):
+    """``(H - s) x`` from ``y = H x`` (``shift_h``); ``s = 0`` returns ``y`` itself."""
+    return y if s == 0.0 else B.add(y, x, 1.0, -s)
 
 
 @dataclass
@@ -251,7 +257,7 @@ def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
 
         def applyH(v, lch=lch, W=W, rch1=rch1):
             acc.nmv += 1
-            return apply_one_site(lch, W, rch1, v)
+            return shifted(apply_one_site(lch, W, rch1, v), v, cx.eshift)
 
         Wk, st = krylov_enrich(Kex, applyH, ex.U_ex, "left", cx.tau, cx.alloc,
                                workcap=cap_at(cx.wcap, bond), recurrence=cx.recurrence,
@@ -289,7 +295,7 @@ def half_right(psiR, right_frames, expanded, nn, acc, hledger, cx: Ctx):
 
         def applyH(v, lch1=lch1, W=W, rch=rch):
             acc.nmv += 1
-            return apply_one_site(lch1, W, rch, v)
+            return shifted(apply_one_site(lch1, W, rch, v), v, cx.eshift)
 
         Zk, st = krylov_enrich(Bex, applyH, ex.V_ex, "right", cx.tau, cx.alloc,
                                workcap=cap_at(cx.wcap, bond), recurrence=cx.recurrence,
@@ -366,11 +372,13 @@ class KLFrames:
     lenv: object
     renv: object
     gen: int = 0
+    eshift: float = 0.0
 
 
 def root_generator(mpo, fr: KLFrames):
+    """``B = P H P - eshift`` at the root (``_root_generator``, ``krylov_closure_frames.jl:291-303``)."""
     return ZeroSiteH(mpo, fr.root_link, fr.lenv, fr.renv, fr.left_frames[fr.root_link],
-                     fr.right_frames[fr.root_link])
+                     fr.right_frames[fr.root_link], eshift=fr.eshift)
 
 
 def project_root(psi, fr: KLFrames):
@@ -433,7 +441,7 @@ def frontier_left(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
 
             def applyH(v, lch=lch, W=W, rch1=rch1):
                 out["n_h1"] += 1
-                return apply_one_site(lch, W, rch1, v)
+                return shifted(apply_one_site(lch, W, rch1, v), v, cx.eshift)
 
             Wi, st = krylov_enrich(Kex, applyH, ex.U_ex, "left", cx.tau, cx.alloc,
                                    workcap=cap_at(cx.wcap, bond), amp=amp, state_seed=False,
@@ -494,7 +502,7 @@ def frontier_right(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
 
             def applyH(v, lch1=lch1, W=W, rch=rch):
                 out["n_h1"] += 1
-                return apply_one_site(lch1, W, rch, v)
+                return shifted(apply_one_site(lch1, W, rch, v), v, cx.eshift)
 
             Zj, st = krylov_enrich(Bex, applyH, ex.V_ex, "right", cx.tau, cx.alloc,
                                    workcap=cap_at(cx.wcap, bond), amp=amp, state_seed=False,
@@ -547,7 +555,8 @@ def frontier_sweep(fr: KLFrames, psi, mpo, core, degree, cx: Ctx, nrm, enrich=Tr
         fr.lenv, fr.renv, fr.gen = rl["env"], rr["env"], gen
     lg.n_closure_sweeps = 1
     lg.n_h1_closure = rl["n_h1"] + rr["n_h1"]
-    return dict(added=added, leak=leak, met=met, capped=enrich and lg.workcap_reached, ledger=lg)
+    return dict(added=added, leak=leak, met=met, capped=enrich and lg.workcap_reached, ledger=lg,
+                leaks_left=rl["leak"], leaks_right=rr["leak"])
 
 
 def single_pass_closure(fr: KLFrames, psi, mpo, root_start, cx: Ctx, order, nrm, ledger):
@@ -681,13 +690,110 @@ def local_dim(psi):
     return max(psi[s].dim(1) for s in range(1, len(psi) + 1))
 
 
+def closure_maxpass(order):
+    return 2 * order + 2  # _closure_maxpass, krylov_closure_frames.jl:12
+
+
+def complement_action(psi, mpo, fr: KLFrames, core, cx: Ctx):
+    """``estimate_global_complement_action`` (``frontier_closure.jl:238-277``, ``nsample = 0``): the
+    per-bond two-site misses of a non-enriching frontier sweep of ``core`` on the frames ``fr``,
+    measured with a copy of the step's generator so its stream is left untouched."""
+    rng = np.random.default_rng()
+    rng.bit_generator.state = cx.rng.bit_generator.state
+    L = len(psi)
+    alloc = basis_allocation(Budget(1.0, 0.0, 1.0), L - 1)  # scale 1: raw norms
+    mcx = Ctx(cx.mpo, 0j, cx.root_link, alloc, cx.expansion, cx.recurrence, cx.wcap, rng, cx.eshift)
+    frames = KLFrames(dict(fr.left_frames), dict(fr.right_frames), fr.root_link, fr.lenv, fr.renv,
+                      fr.gen, fr.eshift)
+    sw = frontier_sweep(frames, psi, mpo, core, 0, mcx, max(B.norm(core), np.finfo(float).eps),
+                        enrich=False)
+    pl, pr = sw.get("leaks_left", []), sw.get("leaks_right", [])
+    left = math.sqrt(sum(x * x for x in pl))
+    right = math.sqrt(sum(x * x for x in pr))
+    return dict(left=left, right=right, bound=math.sqrt(left * left + right * right),
+                per_left=list(pl), per_right=list(pr))
+
+
+def report_root(report, psi, mpo, left_frames, right_frames, root_link, lenv_root, renv_root,
+                root_operator, root_start, root_result, solve_with, *, cx, nrm, ledger, expanded,
+                outside_residual, tol_basis, order):
+    """``_report_root!`` (``bug_step_stages.jl:243-390``): the Rayleigh-quotient energies before and
+    after the root solve and, with ``outside_residual``, the defect ``|tau| ||(I - P) H psi_1|| /
+    ||psi_1||``; while it fails ``tol_basis`` the frames are re-enriched by the evolved state's own
+    frontier sweep and the root re-solved (at most ``2 order + 2`` passes)."""
+    state = dict(op=root_operator, lenv=lenv_root, renv=renv_root, rep=None)
+
+    def rayleigh(v):
+        n2 = B.norm(v) ** 2
+        if not n2 > 0:
+            return float("nan")
+        return B.inner(v, state["op"].apply(v)).real / n2 + cx.eshift
+
+    def frames():
+        return KLFrames(left_frames, right_frames, root_link, state["lenv"], state["renv"], 0, cx.eshift)
+
+    def outside_of(v):
+        return complement_action(psi, mpo, frames(), v, cx)
+
+    def residual_of(action, v):
+        if action is None:
+            return float("nan")
+        return abs(cx.tau) * action["bound"] / max(B.norm(v), np.finfo(float).eps)
+
+    e_pre = rayleigh(root_start)
+    outside = outside_of(root_result) if outside_residual else None
+    initial = residual_of(outside, root_result)
+    passes = added = 0
+    if outside_residual:
+        while not (residual_of(outside, root_result) <= tol_basis) and passes < closure_maxpass(order):
+            fr = frames()
+            passes += 1
+            sw = frontier_sweep(fr, psi, mpo, root_result, 0, cx, nrm, enrich=True)
+            ledger.merge(sw["ledger"])
+            if sw["added"] == 0:
+                break
+            added += sw["added"]
+            state["lenv"], state["renv"] = fr.lenv, fr.renv
+            root_start = project_root(psi, fr)
+            state["op"] = root_generator(mpo, fr)
+            root_result, state["rep"] = solve_with(state["op"], root_start)
+            outside = outside_of(root_result)
+            if sw["capped"]:
+                break
+        if added > 0:
+            L = len(psi)
+            for b in range(1, root_link):
+                expanded[b - 1] = left_frames[b].dim(2)
+            for b in range(root_link + 1, L):
+                expanded[b - 1] = right_frames[b].dim(0)
+            ledger.r_aug = max(max(expanded, default=0), right_frames[root_link].dim(0))
+    e_root = rayleigh(root_result)
+    rn = max(B.norm(root_result), np.finfo(float).eps)
+    nan = float("nan")
+    report.update(
+        eshift=cx.eshift, e_pre=e_pre, e_root=e_root, n_root=None, resid_initial=initial,
+        outside_passes=passes, outside_added=added,
+        outside=nan if outside is None else outside["bound"] / rn,
+        outside_left=nan if outside is None else outside["left"] / rn,
+        outside_right=nan if outside is None else outside["right"] / rn,
+        per_left=[] if outside is None else [x / rn for x in outside["per_left"]],
+        per_right=[] if outside is None else [x / rn for x in outside["per_right"]],
+        resid=nan if outside is None else abs(cx.tau) * outside["bound"] / rn,
+    )
+    return dict(root_start=root_start, root_result=root_result, lenv=state["lenv"],
+                renv=state["renv"], rep=state["rep"])
+
+
 def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
                  order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
                  reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
                  root_maxiter=K.ROOT_MAXITER, krylov_rank_tol=0.0, frontier_tol=0.0,
-                 fold_omega=None, closure_checks=False):
+                 fold_omega=None, closure_checks=False, eshift=0.0, root_report=None,
+                 outside_residual=False):
     """One rank-adaptive BUG step in place; returns the step info dict
-    (``bug_step.jl:17-513``)."""
+    (``bug_step.jl:17-513``). The generators are ``H - eshift``; with ``root_report`` (a dict) the
+    root's energies and, with ``outside_residual``, the outside-Galerkin defect and its
+    re-enrichment are filled in (``_report_root!``, ``bug_step_stages.jl:243-390``)."""
     tau = complex(tau)
     L = len(psi)
     if len(mpo) != L:
@@ -709,6 +815,11 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         raise NotImplementedError("the exact (unfolded) closure leak is not restated")
     if closure_checks:
         raise NotImplementedError("closure_checks = true is not restated")
+    if outside_residual and root_report is None:
+        raise ValueError("outside_residual needs root_report")
+    if outside_residual and not fold:
+        raise NotImplementedError("the outside residual with the exact (unfolded) leak is not restated")
+    eshift = float(eshift)
     if frontier_tol != 0.0 or krylov_rank_tol != 0.0:
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
     if work_ceiling_rule not in ("maxdim", "bond"):
@@ -740,7 +851,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     nL = [0] * (L - 1)
     nR = [0] * (L - 1)
     accL, accR = HalfAcc(), HalfAcc()
-    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng)
+    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift)
     ledgerL, ledgerR = Ledger(), Ledger()
     left_frames, right_frames = {}, {}
     psiL = psi.copy()
@@ -753,7 +864,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     AL = overlap_left(psi, left_frames, root_link)
     root_start = B.contract(AL, (1,), AR, (0,))
     nclose = 0
-    fr = KLFrames(left_frames, right_frames, root_link, lenv_root, renv_root, 0)
+    fr = KLFrames(left_frames, right_frames, root_link, lenv_root, renv_root, 0, eshift)
     if order > 1:
         cl = single_pass_closure(fr, psi, mpo, root_start, cx, order, nrm, ledger)
         for b in range(1, root_link):
@@ -768,16 +879,26 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     if ledger.proj_err > budget.basis:
         ledger.unmet_("projection")
     gen = ZeroSiteH(mpo, root_link, lenv_root, renv_root, left_frames[root_link],
-                    right_frames[root_link])
+                    right_frames[root_link], eshift=eshift)
     nroot = [0]
 
-    def apply_root(v):
-        nroot[0] += 1
-        return gen.apply(v)
+    def solve_with(op, start):
+        def apply_root(v):
+            nroot[0] += 1
+            return op.apply(v)
 
-    root_result, rep = K.expv(VOPS, apply_root, tau, root_start, hermitian=hermitian,
-                              maxiter=root_maxiter, tol=1e-15, reorth=reorth,
-                              conv_tol=budget.expv, substeps=0)
+        return K.expv(VOPS, apply_root, tau, start, hermitian=hermitian, maxiter=root_maxiter,
+                      tol=1e-15, reorth=reorth, conv_tol=budget.expv, substeps=0)
+
+    root_result, rep = solve_with(gen, root_start)
+    if root_report is not None:
+        rr = report_root(root_report, psi, mpo, left_frames, right_frames, root_link, lenv_root,
+                         renv_root, gen, root_start, root_result, solve_with, cx=cx, nrm=nrm,
+                         ledger=ledger, expanded=expanded, outside_residual=outside_residual,
+                         tol_basis=budget.basis, order=order)
+        root_start, root_result = rr["root_start"], rr["root_result"]
+        if rr["rep"] is not None:
+            rep = rr["rep"]
     ledger.expv_err = rep[2]
     ledger.expv_iters = rep[0]
     if rep[2] > budget.expv * (1 + 1e-8):

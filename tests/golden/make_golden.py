@@ -8,7 +8,8 @@ It copies numbers only (S^z profiles, bond dimensions, statuses, errors against 
 the discarded weight, norms and the no-symmetry final state) from
 ``test/fixtures/b155550/{xx_u1_bug_order1,xx_u1_bug_order2,xx_none_bug_order2}.json`` (read by the
 reference's ``test/BUG/TimeEvolution/test_fixtures_b155550.jl``) and the two-site TDVP baseline's
-``baseline_tdvp2_xx.json`` (read by ``test/Baselines/test_baselines.jl``).
+``baseline_tdvp2_xx.json`` (read by ``test/Baselines/test_baselines.jl``) and the imaginary-time
+``heisenberg_ite.json`` (read by ``test_fixtures_b155550.jl`` as well).
 """
 
 import json
@@ -19,7 +20,8 @@ import sys
 def main(ref_root: str) -> None:
     src = pathlib.Path(ref_root) / "test" / "fixtures" / "b155550"
     out = {"source": "test/fixtures/b155550", "versions": json.load(open(src / "versions.json"))}
-    for name in ("xx_u1_bug_order1", "xx_u1_bug_order2", "xx_none_bug_order2", "baseline_tdvp2_xx"):
+    for name in ("xx_u1_bug_order1", "xx_u1_bug_order2", "xx_none_bug_order2", "baseline_tdvp2_xx",
+                 "heisenberg_ite"):
         d = json.load(open(src / f"{name}.json"))
         d.pop("wall_s", None)
         out[name] = d

@@ -233,3 +233,39 @@ def test_tdvp2_baseline_fixture():
         assert np.max(np.abs(sz - np.array(row["sz"]))) <= 1e-12
         assert np.max(np.abs(sz - exact)) <= 2 * row["err_exact"] + 1e-6
         assert psi.bond_dims() == row["bond_dims"]
+
+
+def test_ite_heisenberg_fixture():
+    """Normalised imaginary time (``ite_evolve!``, two steps of dbeta 0.125 per row) on the
+    Heisenberg chain from Neel, under the defaults the reference froze ``heisenberg_ite`` with
+    (``:adaptive`` DD, Arnoldi, the ``:maxdim`` ceiling): the frozen energies to 1e-12 at
+    beta 0.25 and 0.5 and 1e-8 at 0.75 and 1, the frozen statuses, monotone decrease and never
+    below the ground state (the reference test's bars)."""
+    from oracle import ite as I
+
+    fz = GOLDEN["heisenberg_ite"]
+    L = fz["L"]
+    mpo = M.xxz_mpo(L, J=1.0, delta=1.0)
+    psi = M.neel_state(L)
+    rng = np.random.default_rng(1234)
+    kw = dict(work_ceiling_rule="maxdim", expansion=S.DDQRExpansion(mode="adaptive", krylov_mode="arnoldi"))
+    prev = np.inf
+    for i, row in enumerate(fz["trajectory"][:4]):
+        hist = I.ite_evolve(psi, mpo, I.uniform_beta_steps(0.25, 2), order=2, rng=rng, **kw)
+        e = I.ite_energy(psi, mpo)
+        assert abs(e - row["energy"]) <= (1e-12 if i < 2 else 1e-8), (row["beta"], e, row["energy"])
+        assert [h["status"] for h in hist] == row["status"]
+        assert e < prev and e >= fz["e_exact_ground"] - 1e-10
+        prev = e
+
+
+def test_ite_schedules():
+    """``log_panel_steps`` / ``uniform_beta_steps`` / ``geometric_schedule`` (``schedules.jl``)."""
+    from oracle import ite as I
+
+    s = I.log_panel_steps(8.0, 3, per_panel=4)
+    assert len(s) == 12 and abs(sum(s) - 8.0) < 1e-12
+    assert s[:4] == [0.5] * 4 and s[4:8] == [0.5] * 4 and s[8:] == [1.0] * 4
+    assert I.beta_grid([0.5, 0.25])[-1] == 0.75
+    assert I.uniform_beta_steps(2.0, 8) == [0.25] * 8
+    assert I.geometric_schedule(0.1, 2.0, 0.5, 4) == [0.1, 0.2, 0.4, 0.5]
