@@ -714,6 +714,7 @@ struct Params {
   int dd_mode;  // 0 :rank_tail, 1 :adaptive
   int holdout_width, batch_blocks, cap_selection_svd;
   double acceptance_factor;
+  int closure_checks = 0;  // the measured, multi-pass closure (_krylov_closure!, checks = true)
 };
 
 struct MPS {
@@ -1667,7 +1668,13 @@ struct Step {
     for (double x : rl.leak) lL += x * x;
     for (double x : rr.leak) lR += x * x;
     sw.leak = indicator(alloc, std::sqrt(lL + lR));
-    sw.met = sw.ledger.tolerance_met;
+    if (enrich) {
+      sw.met = sw.ledger.tolerance_met;
+    } else {  // a measurement meets its shares when every bond's action is within per_bond
+      sw.met = true;
+      for (double x : rl.leak) sw.met &= indicator(alloc, x) <= alloc.per_bond;
+      for (double x : rr.leak) sw.met &= indicator(alloc, x) <= alloc.per_bond;
+    }
     sw.added = rl.added + rr.added;
     if (sw.added > 0) {
       for (int b = 1; b <= root_link; ++b) fr.lf[b] = rl.frames[b];
@@ -1680,6 +1687,94 @@ struct Step {
     sw.ledger.n_h1_closure = rl.n_h1 + rr.n_h1;
     sw.capped = sw.ledger.workcap_reached;
     return sw;
+  }
+
+  // _krylov_closure! with checks = true (krylov_closure_loop.jl:18-194; serial, include_zero =
+  // false): every frontier is first measured on the incoming frames (_measure_frontiers,
+  // frontier_closure.jl:289-359), which stay untouched if all close; otherwise the closure loop
+  // (_closure_loop!, :370-409) sweeps degrees 1..order-1 until a pass adds nothing (converged if
+  // every share is met), a capped pass misses a share, or 2 order + 2 passes; degree 0 is then
+  // measured again on the final frames.
+  struct ClosureOut {
+    T root;
+    Ledger lg;
+    int64_t nroot = 0;
+  };
+  ClosureOut checked_closure(KL& fr, const MPS& psi, const T& root_start, double nrm) {
+    ClosureOut out;
+    Ledger& lg = out.lg;
+    lg.order = P.order;
+    T current = root_start;
+    ZeroSiteH op = root_generator(fr);
+    auto projected = [&](const T& root, int count) {
+      std::vector<T> Fs;
+      T F = root;
+      for (int d = 1; d <= count; ++d) {
+        out.nroot += 1;
+        F = e.scale(op.apply(e, F), tau / double(d));
+        Fs.push_back(F);
+      }
+      return Fs;
+    };
+    std::vector<T> cores{root_start};
+    for (auto& F : projected(root_start, P.order - 1)) cores.push_back(F);
+    std::vector<double> final_leak(P.order, 0.0);
+    bool met = true;
+    for (int d = 0; d < P.order; ++d) {
+      auto sw = frontier_sweep(fr, psi, cores[d], nrm, false);
+      lg.merge(sw.ledger);
+      final_leak[d] = sw.leak;
+      if (d >= 1) met &= sw.met;
+    }
+    const int gen0 = fr.gen;
+    int passes = 0;
+    bool converged = true;
+    if (!met) {
+      op = root_generator(fr);
+      auto frontier = [&](int degree) { return degree == 0 ? current : projected(current, degree).back(); };
+      const int maxpass = 2 * P.order + 2;
+      passes = maxpass;
+      converged = false;
+      for (int pass = 1; pass <= maxpass; ++pass) {
+        bool grew = false, allmet = true, capped = false;
+        for (int degree = 1; degree < P.order; ++degree) {
+          T F = frontier(degree);
+          auto sw = frontier_sweep(fr, psi, F, nrm, true);
+          lg.merge(sw.ledger);
+          final_leak[degree] = sw.leak;
+          if (sw.added > 0) {
+            op = root_generator(fr);
+            current = project_root(psi, fr);
+          }
+          grew |= sw.added > 0;
+          allmet &= sw.met;
+          capped |= sw.capped;
+        }
+        if (!grew) {
+          passes = pass;
+          converged = allmet;
+          break;
+        }
+        if (capped && !allmet) {
+          passes = pass;
+          break;
+        }
+      }
+      if (fr.gen != gen0) {
+        auto sw = frontier_sweep(fr, psi, frontier(0), nrm, false);
+        lg.merge(sw.ledger);
+        final_leak[0] = sw.leak;
+      }
+    }
+    lg.n_passes = passes;
+    lg.leak = final_leak;
+    double defect = 0.0;
+    for (int d = 0; d < P.order; ++d) defect += final_leak[d] / (d + 1);
+    lg.defect = defect;
+    lg.n_root_frontier = out.nroot;
+    if (!converged) lg.unmet_(U_CLOSURE);
+    out.root = current;
+    return out;
   }
 
   // ── root exponential (krylov.jl, root_methods.jl) ──
@@ -2100,6 +2195,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     P.fixed_depth = prm->krylov_fixed_depth;
     require(prm->dd_mode == 0 || prm->dd_mode == 1, "dd_mode must be 0 (:rank_tail) or 1 (:adaptive)");
     P.dd_mode = prm->dd_mode;
+    P.closure_checks = prm->closure_checks != 0;
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
@@ -2171,7 +2267,18 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     T root_start = e.contract(AL, {1}, AR, {0});
     int64_t nclose = 0;
     Step::KL fr{lf, rf, lenv_root, renv_root, 0};
-    if (P.order > 1) {
+    if (P.order > 1 && P.closure_checks) {
+      auto cl = S.checked_closure(fr, psi, root_start, nrm);
+      ledger.merge(cl.lg);
+      lf = fr.lf;
+      rf = fr.rf;
+      for (int b = 1; b < S.root_link; ++b) expanded[b - 1] = dim(lf[b], 2);
+      for (int b = S.root_link + 1; b < L; ++b) expanded[b - 1] = dim(rf[b], 0);
+      lenv_root = fr.lenv;
+      renv_root = fr.renv;
+      root_start = cl.root;
+      nclose = cl.lg.n_h1_closure + cl.nroot;
+    } else if (P.order > 1) {
       Ledger lg;
       lg.order = P.order;
       int64_t nroot = 0;

@@ -7,9 +7,7 @@ then renormalisation through the centre tensor. A rejected step is redone from t
 sub-steps (their number from the defect's scaling, ``(resid / tol_basis)^(1/(p+1))``, else two)
 while ``retries`` last; resource-capped failures are flagged at once. The step runs in the library
 (``native.cbe_bug_step``); energies are ``<psi|H|psi> / <psi|psi>`` from a device environment
-sweep. Not built: ``root_method`` other than ``:exp``, ``parallel`` half-sweeps, and the
-reference's re-attempt of a step whose closure is unmet with ``closure_checks = true`` (the step
-has no multi-pass closure loop); such a step goes straight to the split.
+sweep. Not built: ``root_method`` other than ``:exp`` and ``parallel`` half-sweeps.
 """
 
 from __future__ import annotations
@@ -66,7 +64,7 @@ def _capped(attempt) -> bool:
 
 
 def _attempt(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxdim, eshift,
-             outside_residual, rng, **kwargs):
+             outside_residual, rng, closure_checks=False, **kwargs):
     """``_ite_attempt!`` (``ite_step.jl:62-126``)."""
     t0 = time.perf_counter()
     e_before = ite_energy(psi, mpo)
@@ -74,7 +72,8 @@ def _attempt(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxdim, 
     rep = {}
     info = N.cbe_bug_step(psi, mpo, complex(-dbeta), order=order, eshift=es, tol_basis=tol_basis,
                           tol_trunc=tol_trunc, tol_expv=tol_root, maxdim=maxdim, root_report=rep,
-                          outside_residual=outside_residual, rng=rng, **kwargs)
+                          outside_residual=outside_residual, closure_checks=closure_checks,
+                          rng=rng, **kwargs)
     growth = ite_normalise(psi)
     e_after = ite_energy(psi, mpo)
     unmet = list(info["ledger"].unmet)
@@ -89,7 +88,7 @@ def _attempt(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxdim, 
         root_err=info["ledger"].expv_err, root_iters=info["ledger"].expv_iters,
         discarded=info["ledger"].discarded, growth=growth, chi=max(psi.bond_dims(), default=0),
         r_aug=info["ledger"].r_aug,
-        closure_checks=False, wall=time.perf_counter() - t0, info=info)
+        closure_checks=closure_checks, wall=time.perf_counter() - t0, info=info)
 
 
 def _result(status, pieces, attempts, t0):
@@ -141,10 +140,15 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
         psi.center = saved.center
 
     attempts = []
-    attempt = _attempt(psi, mpo, float(dbeta), **akw, **kwargs)
+    attempt = _attempt(psi, mpo, float(dbeta), **akw, closure_checks=False, **kwargs)
     attempts.append(attempt)
+    # an unclosed closure is re-attempted with the measured, multi-pass closure
+    if not attempt["ok"] and order > 1 and "closure" in attempt["unmet"]:
+        restore()
+        attempt = _attempt(psi, mpo, float(dbeta), **akw, closure_checks=True, **kwargs)
+        attempts.append(attempt)
     if attempt["ok"]:
-        return _result("met", [attempt], attempts, t0)
+        return _result("met" if len(attempts) == 1 else "retried", [attempt], attempts, t0)
     if retries > 0 and not _capped(attempt):
         restore()
         count = _nsplit(attempt, tol_basis, order)

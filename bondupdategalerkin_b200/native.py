@@ -36,7 +36,7 @@ class StepParams(ctypes.Structure):
                 ("cap_selection", ctypes.c_int), ("acceptance_factor", ctypes.c_double),
                 ("eshift", ctypes.c_double), ("root_report", ctypes.c_int),
                 ("outside_residual", ctypes.c_int), ("rng_ctl", RNG_CTL_FN),
-                ("rng_ctl_user", ctypes.c_void_p)]
+                ("rng_ctl_user", ctypes.c_void_p), ("closure_checks", ctypes.c_int)]
 
 
 class BondLog(ctypes.Structure):
@@ -105,8 +105,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         raise ValueError(f"at most {MAX_SITES + 1} sites")
     if work_ceiling_rule not in ("bond", "maxdim"):
         raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r}")
-    if closure_checks or frontier_tol or krylov_rank_tol:
-        raise NotImplementedError("closure_checks / frontier_tol / krylov_rank_tol > 0")
+    if frontier_tol or krylov_rank_tol:
+        raise NotImplementedError("frontier_tol / krylov_rank_tol > 0")
     if fold_omega is False and order > 1:
         raise NotImplementedError("the exact (unfolded) closure leak")
     mode, width, tail_factor, kmode, fixed_depth = "rank_tail", 8, 0.10, "auto", 0
@@ -139,7 +139,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         fixed_width=width, tail_factor=tail_factor,
         krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth,
         dd_mode=1 if mode == "adaptive" else 0, holdout_width=holdout, batch_blocks=batch,
-        cap_selection=1 if capsel == "svd" else 0, acceptance_factor=accept)
+        cap_selection=1 if capsel == "svd" else 0, acceptance_factor=accept,
+        closure_checks=int(bool(closure_checks)))
 
 
 def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,

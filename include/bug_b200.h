@@ -193,6 +193,9 @@ typedef struct {
                                  re-enrich on it (at most 2 order + 2 passes); needs rng_ctl */
   bug_rng_ctl_fn rng_ctl;
   void* rng_ctl_user;
+  int closure_checks;         /* order > 1: measure every frontier first and close them in passes
+                                 (_krylov_closure! with checks = true,
+                                 krylov_closure_loop.jl:18-194) instead of the single pass */
 } bug_step_params;
 
 /* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by

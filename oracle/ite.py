@@ -3,10 +3,7 @@ product's ``ite.py``, never part of the product).
 
 Follows ``src/BUG/ITE/ite_step.jl`` (``ite_step!`` ``:129-231``, ``_ite_attempt!`` ``:62-126``,
 ``_ite_nsplit`` ``:40-44``, ``_ite_capped`` ``:53``, ``_ite_result`` ``:238-262``, ``ite_evolve!``
-``:273-301``, ``_ite_energy``/``_ite_normalise!`` ``:4-17``) and ``src/BUG/ITE/schedules.jl``. One
-branch is not restated: a step whose order-p closure is unmet is re-attempted by the reference
-with ``closure_checks = true`` (the multi-pass closure loop), which this restatement does not
-have; such a step goes straight to the split.
+``:273-301``, ``_ite_energy``/``_ite_normalise!`` ``:4-17``) and ``src/BUG/ITE/schedules.jl``.
 """
 
 from __future__ import annotations
@@ -60,7 +57,7 @@ def capped(attempt) -> bool:
 
 
 def attempt_step(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxdim, eshift,
-                 outside_residual, rng, step=cbe_bug_step, energy=ite_energy,
+                 outside_residual, rng, closure_checks=False, step=cbe_bug_step, energy=ite_energy,
                  normalise=ite_normalise, **kwargs):
     """``_ite_attempt!``: one step at ``tau = -dbeta`` with the shifted generators and the root
     report, renormalisation, the energies and the verdicts."""
@@ -70,7 +67,7 @@ def attempt_step(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxd
     rep = {}
     info = step(psi, mpo, complex(-dbeta), order=order, eshift=es, tol_basis=tol_basis,
                 tol_trunc=tol_trunc, tol_expv=tol_root, maxdim=maxdim, root_report=rep,
-                outside_residual=outside_residual, rng=rng, **kwargs)
+                outside_residual=outside_residual, closure_checks=closure_checks, rng=rng, **kwargs)
     growth = normalise(psi)
     e_after = energy(psi, mpo)
     unmet = list(info["ledger"].unmet)
@@ -84,7 +81,7 @@ def attempt_step(psi, mpo, dbeta, *, order, tol_basis, tol_trunc, tol_root, maxd
         outside_passes=rep["outside_passes"], outside_added=rep["outside_added"],
         root_err=info["ledger"].expv_err, root_iters=info["ledger"].expv_iters,
         discarded=info["ledger"].discarded, growth=growth, chi=max(psi.bond_dims(), default=0),
-        r_aug=info["ledger"].r_aug, closure_checks=False, wall=time.perf_counter() - t0, info=info)
+        r_aug=info["ledger"].r_aug, closure_checks=closure_checks, wall=time.perf_counter() - t0, info=info)
 
 
 def result(status, pieces, attempts, t0):
@@ -138,10 +135,15 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
         psi.center = saved.center
 
     attempts = []
-    attempt = attempt_step(psi, mpo, float(dbeta), **akw, **kwargs)
+    attempt = attempt_step(psi, mpo, float(dbeta), **akw, closure_checks=False, **kwargs)
     attempts.append(attempt)
+    # an unclosed closure is re-attempted with the measured, multi-pass closure
+    if not attempt["ok"] and order > 1 and "closure" in attempt["unmet"]:
+        restore()
+        attempt = attempt_step(psi, mpo, float(dbeta), **akw, closure_checks=True, **kwargs)
+        attempts.append(attempt)
     if attempt["ok"]:
-        return result("met", [attempt], attempts, t0)
+        return result("met" if len(attempts) == 1 else "retried", [attempt], attempts, t0)
     if retries > 0 and not capped(attempt):
         restore()
         count = nsplit(attempt, tol_basis, order)

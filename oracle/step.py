@@ -590,6 +590,98 @@ def single_pass_closure(fr: KLFrames, psi, mpo, root_start, cx: Ctx, order, nrm,
     return dict(root_start=state["root"], n_h1=lg.n_h1_closure, n_root=state["nroot"])
 
 
+def projected_frontiers(applyB, root, tau, count):
+    """``_projected_frontiers`` (``krylov_closure_frames.jl:315-323``): ``F_j = (tau / j) B F_{j-1}``."""
+    out, F = [], root
+    for d in range(1, count + 1):
+        F = B.scale(applyB(F), tau / d)
+        out.append(F)
+    return out
+
+
+def closure_loop(frontier, sweep, order, maxpass, include_zero=False):
+    """``_closure_loop!`` (``frontier_closure.jl:370-409``): pass 1 sweeps the initial degrees,
+    later passes ``1..order-1``; converged when a pass adds nothing and meets every share; a pass
+    with a share unmet and a sweep at the work ceiling stops capped."""
+    later = list(range(1, order))
+    initial = list(range(order)) if include_zero else later
+    if not initial:
+        return dict(passes=0, converged=True, exhausted=False, capped=False)
+    ok0 = True
+    for p in range(1, maxpass + 1):
+        grew, allmet, capped = False, True, False
+        for degree in (initial if p == 1 else later):
+            r = sweep(frontier(degree), degree, p)
+            grew |= r["added"] > 0
+            allmet &= r["met"]
+            capped |= r["capped"]
+            if degree == 0:
+                ok0 = r["met"]
+        if not grew or not later:
+            return dict(passes=p, converged=allmet and ok0, exhausted=False, capped=False)
+        if capped and not allmet:
+            return dict(passes=p, converged=False, exhausted=False, capped=True)
+    return dict(passes=maxpass, converged=False, exhausted=True, capped=False)
+
+
+def checked_closure(fr: KLFrames, psi, mpo, root_start, cx: Ctx, order, nrm, ledger):
+    """``_krylov_closure!`` with ``checks = true`` (``krylov_closure_loop.jl:18-194``, serial,
+    ``include_zero = false``): measure every frontier on the incoming frames first
+    (``_measure_frontiers``, ``frontier_closure.jl:289-359``) and leave them untouched if all
+    close; otherwise run the closure loop and measure degree 0 on the final frames."""
+    lg = Ledger(order=order)
+    state = dict(nroot=0, root=root_start, op=root_generator(mpo, fr))
+
+    def applyB(v):
+        state["nroot"] += 1
+        return state["op"].apply(v)
+
+    cores = [root_start] + projected_frontiers(applyB, root_start, cx.tau, order - 1)
+    final_leak = {}
+    met, met0 = True, True
+    for d, core in enumerate(cores):
+        sw = frontier_sweep(fr, psi, mpo, core, d, cx, nrm, enrich=False)
+        lg.merge(sw["ledger"])
+        final_leak[d] = sw["leak"]
+        if d >= 1:
+            met &= sw["met"]
+        else:
+            met0 = sw["met"]
+    gen0 = fr.gen
+    if met:
+        res = dict(passes=0, converged=True)
+    else:
+        state["op"] = root_generator(mpo, fr)
+
+        def frontier(degree):
+            if degree == 0:
+                return state["root"]
+            return projected_frontiers(applyB, state["root"], cx.tau, degree)[degree - 1]
+
+        def sweep(F, degree, pass_):
+            sw = frontier_sweep(fr, psi, mpo, F, degree, cx, nrm, enrich=True)
+            lg.merge(sw["ledger"])
+            final_leak[degree] = sw["leak"]
+            if sw["added"] > 0:
+                state["op"] = root_generator(mpo, fr)
+                state["root"] = project_root(psi, fr)
+            return sw
+
+        res = closure_loop(frontier, sweep, order, closure_maxpass(order))
+        if fr.gen != gen0:
+            sw = frontier_sweep(fr, psi, mpo, frontier(0), 0, cx, nrm, enrich=False)
+            lg.merge(sw["ledger"])
+            final_leak[0] = sw["leak"]
+    lg.n_passes = res["passes"]
+    lg.leak = [final_leak[d] for d in range(order)]
+    lg.defect = sum(lg.leak[d] / (d + 1) for d in range(order))
+    lg.n_root_frontier = state["nroot"]
+    if not res["converged"]:
+        lg.unmet_("closure")
+    ledger.merge(lg)
+    return dict(root_start=state["root"], n_h1=lg.n_h1_closure, n_root=state["nroot"])
+
+
 # ── compression ──────────────────────────────────────────────────────────────────────────────
 
 
@@ -813,8 +905,6 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     fold = (order > 1) if fold_omega is None else fold_omega
     if order > 1 and not fold:
         raise NotImplementedError("the exact (unfolded) closure leak is not restated")
-    if closure_checks:
-        raise NotImplementedError("closure_checks = true is not restated")
     if outside_residual and root_report is None:
         raise ValueError("outside_residual needs root_report")
     if outside_residual and not fold:
@@ -866,7 +956,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     nclose = 0
     fr = KLFrames(left_frames, right_frames, root_link, lenv_root, renv_root, 0, eshift)
     if order > 1:
-        cl = single_pass_closure(fr, psi, mpo, root_start, cx, order, nrm, ledger)
+        closure = checked_closure if closure_checks else single_pass_closure
+        cl = closure(fr, psi, mpo, root_start, cx, order, nrm, ledger)
         for b in range(1, root_link):
             expanded[b - 1] = left_frames[b].dim(2)
         for b in range(root_link + 1, L):

@@ -254,3 +254,15 @@ def test_adaptive_batch_blocks(dev, native):
     run_pair(dev, 14, 6, "neel_state", -0.5, 2, tau=-0.1j, tol_basis=1e-8, maxdim=32,
              check_every=3, native=native, work_ceiling_rule="maxdim", widths=False,
              expansion=dict(mode="adaptive", batch_blocks=3, holdout_width=6, acceptance_factor=0.5))
+
+
+@pytest.mark.parametrize("native", [pytest.param(True, id="native-step")])
+def test_closure_checks(dev, native):
+    """``closure_checks = true``: every frontier measured first, then the closure loop in passes
+    and degree 0 measured again (``_krylov_closure!`` with checks), against the oracle: the
+    Heisenberg chain from Neel in imaginary time (the closure unmet in the first steps) and an
+    XXZ quench in real time."""
+    run_pair(dev, 10, 3, "neel_state", 1.0, 2, tau=-0.125, maxdim=64, native=native,
+             closure_checks=True)
+    run_pair(dev, 12, 4, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=32, check_every=2,
+             native=native, closure_checks=True)
