@@ -715,6 +715,8 @@ struct Params {
   int holdout_width, batch_blocks, cap_selection_svd;
   double acceptance_factor;
   int closure_checks = 0;  // the measured, multi-pass closure (_krylov_closure!, checks = true)
+  int root_method = 0;     // 0 exp, 1 trapezoid, 2 radau2, 3 radau3
+  bool root_shift = true;  // the implicit roots' imaginary-time spectral shift
 };
 
 struct MPS {
@@ -1963,7 +1965,9 @@ struct Step {
   // substeps: 1 one step of the whole tau, > 1 that many equal substeps, 0 the adaptive substep
   // search (pick_tau)
   T lanczos_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
-                 bool reorth, double conv_tol, ExpvRep& rep, int substeps = 0, bool deferred = false) {
+                 bool reorth, double conv_tol, ExpvRep& rep, int substeps = 0, bool deferred = false,
+                 int rmethod = 0, bool rshift = true) {
+    if (rmethod) substeps = 1;  // an implicit root takes the whole step in one stage
     const double beta0 = e.norm(vec);
     if (beta0 == 0) return vec;
     T cur = vec;
@@ -1993,7 +1997,7 @@ struct Step {
           if (off < tol) break;
           if (conv_tol > 0) {
             Eig eg = tridiag_eigen(alpha, betas);
-            auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
+            auto ev = [&](cd s) { return rmethod ? rational_coeffs(eg, s, rmethod, rshift) : coeffs_from_eigen(eg, s); };
             if (tail_sup(ev, tau_rem, off, conv_tol) < conv_tol) break;
           }
           betas.push_back(off);
@@ -2016,7 +2020,7 @@ struct Step {
         betak = e.norm(residual);
       }
       Eig eg = tridiag_eigen(alpha, betas);
-      auto ev = [&](cd s) { return coeffs_from_eigen(eg, s); };
+      auto ev = [&](cd s) { return rmethod ? rational_coeffs(eg, s, rmethod, rshift) : coeffs_from_eigen(eg, s); };
       const cd tau_s = substeps == 1 ? tau_rem
                        : substeps > 1 ? tau_rem / double(substeps - nsub + 1)
                                       : pick_tau(ev, tau_rem, betak, conv_tol);
@@ -2032,6 +2036,65 @@ struct Step {
   }
 
 
+  // ── implicit roots (root_methods.jl:12-75, 143-168): R(z) = N(z) / D(z) of one implicit RK
+  // step, the (k, k+1) Pade approximants of exp (coefficients constant term first): 1 trapezoid,
+  // 2 Radau IIA with two stages, 3 with three. The spectrum is shifted to the Ritz value that
+  // maximises Re(tau lambda) (none in real time or without `shift`); no scale is carried.
+  static cd root_stability(int m, cd z) {
+    static const std::vector<double> num[4] = {{}, {1.0, 0.5}, {1.0, 1.0 / 3.0}, {1.0, 0.4, 0.05}};
+    static const std::vector<double> den[4] = {
+        {}, {1.0, -0.5}, {1.0, -2.0 / 3.0, 1.0 / 6.0}, {1.0, -0.6, 0.15, -1.0 / 60.0}};
+    auto horner = [&](const std::vector<double>& c) {
+      cd r = c.back();
+      for (int k = int(c.size()) - 2; k >= 0; --k) r = r * z + c[k];
+      return r;
+    };
+    return horner(num[m]) / horner(den[m]);
+  }
+  static cd rational_shift(const std::vector<cd>& vals, cd t, bool shift) {
+    if (!shift || vals.empty() || t.real() == 0) return 0.0;
+    size_t top = 0;
+    for (size_t i = 1; i < vals.size(); ++i)
+      if ((t * vals[i]).real() > (t * vals[top]).real()) top = i;
+    return vals[top];
+  }
+  static std::pair<std::vector<cd>, cd> rational_coeffs(const Eig& eg, cd t, int m, bool shift) {
+    std::vector<cd> cv(eg.vals.begin(), eg.vals.end());
+    const cd sigma = rational_shift(cv, t, shift);
+    const int n = int(eg.vals.size());
+    std::vector<cd> w(n), c(n, 0.0);
+    for (int j = 0; j < n; ++j) w[j] = root_stability(m, t * (cd(eg.vals[j]) - sigma)) * eg.vecs(0, j);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) c[i] += eg.vecs(i, j) * w[j];
+    return {c, 0.0};
+  }
+  std::pair<std::vector<cd>, cd> hess_rational(const CMat& Hm, cd t, int m, bool shift) {
+    const int n = Hm.n;
+    if (n == 0) return {{}, 0.0};
+    const cd sigma = rational_shift(smallla::eigvals_hess(Hm), t, shift);
+    CMat M(n, n);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) M(i, j) = t * (Hm(i, j) - (i == j ? sigma : cd(0)));
+    static const std::vector<double> num[4] = {{}, {1.0, 0.5}, {1.0, 1.0 / 3.0}, {1.0, 0.4, 0.05}};
+    static const std::vector<double> den[4] = {
+        {}, {1.0, -0.5}, {1.0, -2.0 / 3.0, 1.0 / 6.0}, {1.0, -0.6, 0.15, -1.0 / 60.0}};
+    auto poly = [&](const std::vector<double>& c) {
+      CMat r(n, n);
+      for (int i = 0; i < n; ++i) r(i, i) = c.back();
+      for (int k = int(c.size()) - 2; k >= 0; --k) {
+        r = smallla::matmul(r, M);
+        for (int i = 0; i < n; ++i) r(i, i) += c[k];
+      }
+      return r;
+    };
+    CMat N = poly(num[m]), e1(n, 1);
+    for (int i = 0; i < n; ++i) e1(i, 0) = N(i, 0);
+    CMat x = smallla::solve(poly(den[m]), e1);
+    std::vector<cd> c(n);
+    for (int i = 0; i < n; ++i) c[i] = x(i, 0);
+    return {c, 0.0};
+  }
+
   std::pair<std::vector<cd>, cd> hess_coeffs(const CMat& Hm, cd t) {
     const int n = Hm.n;
     if (n == 0) return {{}, 0.0};
@@ -2046,7 +2109,8 @@ struct Step {
   }
 
   T arnoldi_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
-                 double conv_tol, ExpvRep& rep, int substeps = 0) {
+                 double conv_tol, ExpvRep& rep, int substeps = 0, int rmethod = 0, bool rshift = true) {
+    if (rmethod) substeps = 1;
     const double beta0 = e.norm(vec);
     if (beta0 == 0) return vec;
     T cur = vec;
@@ -2081,7 +2145,7 @@ struct Step {
           CMat lead(dimk, dimk);
           for (int i = 0; i < dimk; ++i)
             for (int j = 0; j < dimk; ++j) lead(i, j) = H(i, j);
-          auto ev = [&](cd s) { return hess_coeffs(lead, s); };
+          auto ev = [&](cd s) { return rmethod ? hess_rational(lead, s, rmethod, rshift) : hess_coeffs(lead, s); };
           if (tail_sup(ev, tau_rem, rn, conv_tol) < conv_tol) break;
         }
         H(k + 1, k) = rn;
@@ -2091,7 +2155,7 @@ struct Step {
       CMat Hm(dimk, dimk);
       for (int i = 0; i < dimk; ++i)
         for (int j = 0; j < dimk; ++j) Hm(i, j) = H(i, j);
-      auto ev = [&](cd s) { return hess_coeffs(Hm, s); };
+      auto ev = [&](cd s) { return rmethod ? hess_rational(Hm, s, rmethod, rshift) : hess_coeffs(Hm, s); };
       const cd tau_s = substeps == 1 ? tau_rem
                        : substeps > 1 ? tau_rem / double(substeps - nsub + 1)
                                       : pick_tau(ev, tau_rem, betak, conv_tol);
@@ -2196,6 +2260,9 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     require(prm->dd_mode == 0 || prm->dd_mode == 1, "dd_mode must be 0 (:rank_tail) or 1 (:adaptive)");
     P.dd_mode = prm->dd_mode;
     P.closure_checks = prm->closure_checks != 0;
+    require(prm->root_method >= 0 && prm->root_method <= 3, "root_method must be 0 (exp), 1 (trapezoid), 2 (radau2) or 3 (radau3)");
+    P.root_method = prm->root_method;
+    P.root_shift = prm->root_noshift == 0;
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
@@ -2333,8 +2400,10 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
       return gen.apply(e, v);
     };
     auto solve_root = [&](const T& start, Step::ExpvRep& r) {
-      return P.hermitian ? S.lanczos_expv(apply_root, start, P.root_maxiter, 1e-15, P.reorth != 0, P.tol_expv, r)
-                         : S.arnoldi_expv(apply_root, start, P.root_maxiter, 1e-15, P.tol_expv, r);
+      return P.hermitian ? S.lanczos_expv(apply_root, start, P.root_maxiter, 1e-15, P.reorth != 0, P.tol_expv, r,
+                                          0, false, P.root_method, P.root_shift)
+                         : S.arnoldi_expv(apply_root, start, P.root_maxiter, 1e-15, P.tol_expv, r, 0,
+                                          P.root_method, P.root_shift);
     };
     Step::ExpvRep rep;
     T root_result = solve_root(root_start, rep);

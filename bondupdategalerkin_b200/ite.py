@@ -118,8 +118,8 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
     ``nsub`` and ``attempts``. ``kwargs`` go to ``cbe_bug_step``."""
     if not dbeta > 0:
         raise ValueError(f"dbeta must be positive, got {dbeta}")
-    if root_method != "exp":
-        raise NotImplementedError(f"root_method {root_method!r}: only :exp is built")
+    if root_method not in ("exp", "trapezoid", "radau2", "radau3"):
+        raise NotImplementedError(f"root_method {root_method!r}: exp, trapezoid, radau2, radau3 are built")
     if on_fail not in ("flag", "error"):
         raise ValueError("on_fail must be flag or error")
     if retries < 0:
@@ -132,7 +132,8 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
     ite_normalise(psi)
     saved = psi.copy()  # the step replaces tensors and never mutates them: a stable snapshot
     akw = dict(order=order, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_root=tol_root,
-               maxdim=maxdim, eshift=eshift, outside_residual=outside_residual, rng=rng)
+               maxdim=maxdim, eshift=eshift, outside_residual=outside_residual, rng=rng,
+               root_method=root_method)
 
     def restore():
         for site in range(1, len(psi) + 1):
@@ -154,7 +155,7 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
         count = _nsplit(attempt, tol_basis, order)
         halves = []
         for _ in range(count):
-            sub = ite_step(psi, mpo, dbeta / count, root_method=root_method, retries=retries - 1,
+            sub = ite_step(psi, mpo, dbeta / count, retries=retries - 1,
                            on_fail="flag", **akw, **kwargs)
             attempts += sub["attempts"]
             halves.append(sub)

@@ -36,7 +36,8 @@ class StepParams(ctypes.Structure):
                 ("cap_selection", ctypes.c_int), ("acceptance_factor", ctypes.c_double),
                 ("eshift", ctypes.c_double), ("root_report", ctypes.c_int),
                 ("outside_residual", ctypes.c_int), ("rng_ctl", RNG_CTL_FN),
-                ("rng_ctl_user", ctypes.c_void_p), ("closure_checks", ctypes.c_int)]
+                ("rng_ctl_user", ctypes.c_void_p), ("closure_checks", ctypes.c_int),
+                ("root_method", ctypes.c_int), ("root_noshift", ctypes.c_int)]
 
 
 class BondLog(ctypes.Structure):
@@ -147,7 +148,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
                  order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
                  reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
                  root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
-                 closure_checks=False, eshift=0.0, root_report=None, outside_residual=False):
+                 closure_checks=False, eshift=0.0, root_report=None, outside_residual=False,
+                 root_method="exp", root_shift=True):
     """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
     HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields). The
     generators are ``H - eshift``; a dict passed as ``root_report`` receives the root's energies
@@ -181,6 +183,11 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         else:
             rng.bit_generator.state = saved.pop()
 
+    methods = {"exp": 0, "trapezoid": 1, "radau2": 2, "radau3": 3}
+    if root_method not in methods:
+        raise NotImplementedError(f"root_method {root_method!r}: {tuple(methods)} are built")
+    p.root_method = methods[root_method]
+    p.root_noshift = 0 if root_shift else 1
     p.eshift = float(eshift)
     p.root_report = int(root_report is not None)
     p.outside_residual = int(bool(outside_residual))

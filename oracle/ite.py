@@ -112,8 +112,8 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
     while ``retries`` last (resource-capped failures are not split)."""
     if not dbeta > 0:
         raise ValueError(f"dbeta must be positive, got {dbeta}")
-    if root_method != "exp":
-        raise NotImplementedError(f"root_method {root_method!r}: only :exp is built")
+    if root_method not in ("exp", "trapezoid", "radau2", "radau3"):
+        raise NotImplementedError(f"root_method {root_method!r}: exp, trapezoid, radau2, radau3 are built")
     if on_fail not in ("flag", "error"):
         raise ValueError("on_fail must be flag or error")
     if retries < 0:
@@ -127,6 +127,7 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
     saved = psi.copy()
     akw = dict(order=order, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_root=tol_root,
                maxdim=maxdim, eshift=eshift, outside_residual=outside_residual, rng=rng,
+               root_method=root_method,
                step=step, energy=energy, normalise=normalise)
 
     def restore():
@@ -149,7 +150,7 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
         count = nsplit(attempt, tol_basis, order)
         halves = []
         for _ in range(count):
-            sub = ite_step(psi, mpo, dbeta / count, root_method=root_method, retries=retries - 1,
+            sub = ite_step(psi, mpo, dbeta / count, retries=retries - 1,
                            on_fail="flag", **akw, **kwargs)
             attempts += sub["attempts"]
             halves.append(sub)

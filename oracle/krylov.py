@@ -102,6 +102,60 @@ def hess_coeffs(Hm, tau):
     return P[:, 0].copy(), tau * sigma
 
 
+# ── implicit roots (root_methods.jl:12-75, 143-168) ─────────────────────────────────────────────
+# The stability functions R(z) = N(z) / D(z) of one implicit Runge-Kutta step (coefficients constant
+# term first): the trapezoid rule and Radau IIA with two and three stages, the (k, k+1) Pade
+# approximants of exp(z).
+ROOT_PADE = {
+    "trapezoid": ([1.0, 1 / 2], [1.0, -1 / 2]),
+    "radau2": ([1.0, 1 / 3], [1.0, -2 / 3, 1 / 6]),
+    "radau3": ([1.0, 2 / 5, 1 / 20], [1.0, -3 / 5, 3 / 20, -1 / 60]),
+}
+ROOT_METHODS = ("exp",) + tuple(ROOT_PADE)
+
+
+def root_stability(method, z):
+    """``root_stability``: ``R(z)`` (``exp(z)`` for ``"exp"``)."""
+    z = complex(z)
+    if method == "exp":
+        return np.exp(z)
+    num, den = ROOT_PADE[method]
+    return np.polyval(num[::-1], z) / np.polyval(den[::-1], z)
+
+
+def rational_shift(vals, tau, shift=True):
+    """``_rational_shift``: the Ritz value maximising ``Re(tau lambda)`` (none in real time)."""
+    if not shift or len(vals) == 0 or tau.real == 0:
+        return 0j
+    return complex(vals[int(np.argmax([(tau * complex(v)).real for v in vals]))])
+
+
+def rational_coeffs(vals, vecs, tau, method, shift=True):
+    """``_rational_coeffs``: ``R(tau (T - sigma)) e_1`` on the tridiagonal's eigenpairs, no scale."""
+    sigma = rational_shift(vals, tau, shift)
+    w = np.array([root_stability(method, tau * (complex(v) - sigma)) for v in vals])
+    return vecs.astype(np.complex128) @ (w * vecs[0, :].astype(np.complex128)), 0j
+
+
+def hess_rational(Hm, tau, method, shift=True):
+    """``_hess_rational``: ``R(tau (H - sigma)) e_1`` on the Arnoldi Hessenberg, no scale."""
+    if Hm.size == 0:
+        return np.zeros(0, dtype=np.complex128), 0j
+    sigma = rational_shift(np.linalg.eigvals(Hm), tau, shift)
+    M = tau * (Hm - sigma * np.eye(Hm.shape[0]))
+    num, den = ROOT_PADE[method]
+
+    def poly(c):
+        out = c[-1] * np.eye(M.shape[0], dtype=np.complex128)
+        for k in range(len(c) - 2, -1, -1):
+            out = out @ M + c[k] * np.eye(M.shape[0])
+        return out
+
+    e1 = np.zeros(M.shape[0], dtype=np.complex128)
+    e1[0] = 1.0
+    return np.linalg.solve(poly(den), poly(num) @ e1), 0j
+
+
 def tail(coeff, betak):
     return 0.0 if len(coeff) == 0 else betak * abs(coeff[-1])
 
@@ -151,9 +205,20 @@ def apply_scale(ops, cur, logscale):
 
 
 def lanczos_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, reorth=False, conv_tol=0.0,
-                 substeps=1):
-    """``exp(tau*A) vector`` for Hermitian ``A`` (``krylov.jl:128-263``). Returns
-    ``(result, report)`` with ``report = (iterations, substeps, err)``."""
+                 substeps=1, root_method="exp", rational_shift=True):
+    """``exp(tau*A) vector`` for Hermitian ``A`` (``krylov.jl:128-263``); with an implicit
+    ``root_method`` its stability function instead, in one stage. Returns ``(result, report)``
+    with ``report = (iterations, substeps, err)``."""
+    if root_method not in ROOT_METHODS:
+        raise NotImplementedError(f"root_method {root_method!r}: {ROOT_METHODS} are built")
+    if root_method != "exp":
+        substeps = 1
+
+    def coeffs(vals, vecs, s):
+        if root_method == "exp":
+            return coeffs_from_eigen(vals, vecs, s)
+        return rational_coeffs(vals, vecs, s, root_method, rational_shift)
+
     tau = complex(tau)
     beta0 = ops.norm(vector)
     if beta0 == 0:
@@ -182,7 +247,7 @@ def lanczos_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, reorth=False, c
                 break
             if conv_tol > 0:
                 vals, vecs = tridiag_eigen(alpha, betas)
-                tt = tail_sup(lambda s: coeffs_from_eigen(vals, vecs, s), tau_rem, off, above=conv_tol)
+                tt = tail_sup(lambda s: coeffs(vals, vecs, s), tau_rem, off, above=conv_tol)
                 if tt < conv_tol:
                     break
             betas.append(off)
@@ -198,7 +263,7 @@ def lanczos_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, reorth=False, c
                     corr = [(ops.inner(prev, residual), prev) for prev in basis]
                     residual = ops.lin([(1.0, residual)] + [(-c, p) for c, p in corr])
         vals, vecs = tridiag_eigen(alpha, betas)
-        evalcoeff = lambda s: coeffs_from_eigen(vals, vecs, complex(s))
+        evalcoeff = lambda s: coeffs(vals, vecs, complex(s))
         betak = ops.norm(residual)
         if substeps == 1:
             tau_s = tau_rem
@@ -229,8 +294,20 @@ def cgs2(ops, H, column, basis, vector):
     return vector
 
 
-def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, substeps=1):
-    """``exp(tau*A) vector`` for any ``A`` by Arnoldi with CGS2 (``krylov.jl:343-442``)."""
+def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, substeps=1,
+                 root_method="exp", rational_shift=True):
+    """``exp(tau*A) vector`` for any ``A`` by Arnoldi with CGS2 (``krylov.jl:343-442``); with an
+    implicit ``root_method`` its stability function instead, in one stage."""
+    if root_method not in ROOT_METHODS:
+        raise NotImplementedError(f"root_method {root_method!r}: {ROOT_METHODS} are built")
+    if root_method != "exp":
+        substeps = 1
+
+    def hcoeffs(Hm, s):
+        if root_method == "exp":
+            return hess_coeffs(Hm, s)
+        return hess_rational(Hm, s, root_method, rational_shift)
+
     tau = complex(tau)
     beta0 = ops.norm(vector)
     if beta0 == 0:
@@ -259,7 +336,7 @@ def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, s
                 break
             if conv_tol > 0:
                 lead = H[:dim, :dim].copy()
-                tt = tail_sup(lambda s: hess_coeffs(lead, s), tau_rem, rn, above=conv_tol)
+                tt = tail_sup(lambda s: hcoeffs(lead, s), tau_rem, rn, above=conv_tol)
                 if tt < conv_tol:
                     break
             H[k + 1, k] = rn
@@ -267,7 +344,7 @@ def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, s
                 break
             basis.append(ops.lin([(1.0 / rn, residual)]))
         Hm = H[:dim, :dim].copy()
-        evalcoeff = lambda s: hess_coeffs(Hm, complex(s))
+        evalcoeff = lambda s: hcoeffs(Hm, complex(s))
         if substeps == 1:
             tau_s = tau_rem
         elif substeps > 1:
@@ -287,7 +364,8 @@ def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, s
 
 
 def expv(ops, apply, tau, vector, hermitian=True, **kw):
-    """``expv`` dispatcher (``root_methods.jl:359-402``), ``root_method = :exp`` only."""
+    """``expv`` dispatcher (``root_methods.jl:359-402``): ``root_method`` ``"exp"`` or one of the
+    implicit roots ``"trapezoid"``, ``"radau2"``, ``"radau3"`` (``"radau2_gmres"`` is not built)."""
     if hermitian:
         return lanczos_expv(ops, apply, tau, vector, **kw)
     kw.pop("reorth", None)

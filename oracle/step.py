@@ -881,7 +881,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
                  reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
                  root_maxiter=K.ROOT_MAXITER, krylov_rank_tol=0.0, frontier_tol=0.0,
                  fold_omega=None, closure_checks=False, eshift=0.0, root_report=None,
-                 outside_residual=False):
+                 outside_residual=False, root_method="exp", root_shift=True):
     """One rank-adaptive BUG step in place; returns the step info dict
     (``bug_step.jl:17-513``). The generators are ``H - eshift``; with ``root_report`` (a dict) the
     root's energies and, with ``outside_residual``, the outside-Galerkin defect and its
@@ -979,7 +979,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
             return op.apply(v)
 
         return K.expv(VOPS, apply_root, tau, start, hermitian=hermitian, maxiter=root_maxiter,
-                      tol=1e-15, reorth=reorth, conv_tol=budget.expv, substeps=0)
+                      tol=1e-15, reorth=reorth, conv_tol=budget.expv, substeps=0,
+                      root_method=root_method, rational_shift=root_shift)
 
     root_result, rep = solve_with(gen, root_start)
     if root_report is not None:

@@ -92,3 +92,19 @@ def test_ite_heisenberg_fixture_on_device(dev):
         assert dpsi.bond_dims() == opsi.bond_dims()
         assert e < prev and e >= fz["e_exact_ground"] - 1e-10
         prev = e
+
+
+def test_ite_radau3_matches_oracle(dev):
+    """``ite_evolve`` with the Radau IIA(3) root: the device driver against the oracle's, energies
+    to 1e-12, the same statuses and bond dimensions."""
+    DM, N, DS, DI = dev
+    L = 10
+    dpsi, opsi = DM.neel_state(L), OM.neel_state(L)
+    dmpo, ompo = DM.xxz_mpo(L, J=1.0, delta=1.0), OM.xxz_mpo(L, J=1.0, delta=1.0)
+    drng, orng = np.random.default_rng(5), np.random.default_rng(5)
+    steps = DI.uniform_beta_steps(0.5, 4)
+    dh = DI.ite_evolve(dpsi, dmpo, steps, order=2, rng=drng, root_method="radau3", maxdim=32)
+    oh = OI.ite_evolve(opsi, ompo, steps, order=2, rng=orng, root_method="radau3", maxdim=32)
+    assert [h["status"] for h in dh] == [h["status"] for h in oh]
+    assert dpsi.bond_dims() == opsi.bond_dims()
+    assert abs(DI.ite_energy(dpsi, dmpo) - OI.ite_energy(opsi, ompo)) <= 1e-12

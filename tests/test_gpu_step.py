@@ -266,3 +266,13 @@ def test_closure_checks(dev, native):
              closure_checks=True)
     run_pair(dev, 12, 4, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=32, check_every=2,
              native=native, closure_checks=True)
+
+
+@pytest.mark.parametrize("method", ["trapezoid", "radau2", "radau3"])
+def test_implicit_root_methods(dev, method):
+    """The implicit root integrators (one stage of the Pade stability function on the root's
+    Krylov basis) against the oracle, in real time and, with the spectral shift, imaginary time."""
+    run_pair(dev, 12, 3, "domain_wall_state", 0.5, 2, tau=-0.05j, tol_basis=1e-4, maxdim=32,
+             native=True, root_method=method)
+    run_pair(dev, 10, 3, "neel_state", 1.0, 2, tau=-0.1, maxdim=32, native=True,
+             root_method=method)

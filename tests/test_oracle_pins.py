@@ -269,3 +269,25 @@ def test_ite_schedules():
     assert I.beta_grid([0.5, 0.25])[-1] == 0.75
     assert I.uniform_beta_steps(2.0, 8) == [0.25] * 8
     assert I.geometric_schedule(0.1, 2.0, 0.5, 4) == [0.1, 0.2, 0.4, 0.5]
+
+
+@pytest.mark.parametrize("method", ["trapezoid", "radau2", "radau3"])
+@pytest.mark.parametrize("tau", [-0.7j, -0.4 + 0j])
+def test_implicit_roots_closed_form(method, tau):
+    """The implicit roots apply their stability function R(z) exactly when the Krylov space is
+    complete: R(tau A) x in real time, R(tau (A - sigma)) x in imaginary time with sigma the
+    eigenvalue maximising Re(tau lambda) (the reference's spectral shift), for Lanczos and
+    Arnoldi; R is the (k, k+1) Pade approximant (R(z) - exp(z) = O(z^(2k+2)))."""
+    x = _multi_sector()
+    scale = lambda q: 0.5 * q + 1.0
+    lam = {k: scale(k[2]) for k in x.blocks}
+    sigma = max(lam.values(), key=lambda v: (tau * v).real) if tau.real != 0 else 0.0
+    want = B.BT(x.legs, {k: K.root_stability(method, tau * (lam[k] - sigma)) * v
+                         for k, v in x.blocks.items()})
+    for herm in (True, False):
+        y, _ = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=herm,
+                      root_method=method)
+        assert B.norm(B.sub(y, want)) < 1e-12 * B.norm(want)
+    order = {"trapezoid": 2, "radau2": 3, "radau3": 5}[method]
+    z = 1e-2
+    assert abs(K.root_stability(method, z) - np.exp(z)) < 10 * z ** (order + 1)
