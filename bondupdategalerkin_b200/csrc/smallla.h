@@ -181,6 +181,42 @@ inline void eigh_tridiag(std::vector<double> d, std::vector<double> e, std::vect
   V = W;
 }
 
+// Least-squares solution of A x = b (A m x n, m >= n) by Householder QR: each reflector
+// I - 2 v v^H / (v^H v), v = a + e^{i arg a_kk} |a| e_k, zeroes column k below the diagonal; then
+// R x = (Q^H b)[0..n). A zero column leaves its unknown zero.
+inline std::vector<cd> lstsq(CMat A, std::vector<cd> b) {
+  const int m = A.n, n = A.m;
+  for (int k = 0; k < n && k < m; ++k) {
+    double nrm2 = 0.0;
+    for (int i = k; i < m; ++i) nrm2 += std::norm(A(i, k));
+    const double nrm = std::sqrt(nrm2);
+    if (nrm == 0.0) continue;
+    const cd alpha = A(k, k);
+    const cd ph = std::abs(alpha) > 0.0 ? alpha / std::abs(alpha) : cd(1.0);
+    std::vector<cd> v(size_t(m - k));
+    v[0] = alpha + ph * nrm;
+    for (int i = k + 1; i < m; ++i) v[size_t(i - k)] = A(i, k);
+    double vv = 0.0;
+    for (auto& x : v) vv += std::norm(x);
+    auto reflect = [&](auto&& get) {
+      cd sdot = 0.0;
+      for (int i = k; i < m; ++i) sdot += std::conj(v[size_t(i - k)]) * get(i);
+      sdot *= 2.0 / vv;
+      for (int i = k; i < m; ++i) get(i) -= v[size_t(i - k)] * sdot;
+    };
+    for (int j = k; j < n; ++j) reflect([&](int i) -> cd& { return A(i, j); });
+    reflect([&](int i) -> cd& { return b[size_t(i)]; });
+  }
+  std::vector<cd> x(size_t(n), 0.0);
+  for (int k = std::min(n, m) - 1; k >= 0; --k) {
+    if (A(k, k) == cd(0.0)) continue;
+    cd s = b[size_t(k)];
+    for (int j = k + 1; j < n; ++j) s -= A(k, j) * x[size_t(j)];
+    x[size_t(k)] = s / A(k, k);
+  }
+  return x;
+}
+
 // Solve X from P X = Q (complex, partial pivoting); P is overwritten.
 inline CMat solve(CMat P, CMat Q) {
   const int n = P.n;

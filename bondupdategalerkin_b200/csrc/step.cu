@@ -2095,6 +2095,140 @@ struct Step {
     return {c, 0.0};
   }
 
+  // ── radau2_gmres (root_methods.jl:170-345): one Radau IIA(2) step, the coupled stages
+  // (I - tau A (x) B) Y = 1 (x) x decoupled by A = P Lambda P^-1 into (I - tau lambda_k (B - sigma))
+  // Z_k = d_k x, d = P^-1 1, solved on ONE Arnoldi basis of B (a Krylov space is shift
+  // invariant), then Y = (P (x) I) Z; restarted on the true stage residual at most 4 times. The
+  // method is stiffly accurate: the result is Y_2.
+  struct Gmres {
+    std::vector<T> Z;
+    double res = 0.0;
+    int64_t nmv = 0;
+    cd sigma = 0.0;
+  };
+  // _shifted_gmres: the systems (I - z_k (B - sigma)) Z_k = d_k rhs on one basis; Wt[s][k] the
+  // entry of P the solution of system k enters stage s with
+  Gmres shifted_gmres(const std::function<T(const T&)>& apply, const T& rhs, const std::vector<cd>& zs,
+                      const std::vector<cd>& ds, const std::vector<std::vector<cd>>& Wt,
+                      bool have_sigma, cd sigma_in, double target, int maxiter, double tol) {
+    Gmres g;
+    const double beta = e.norm(rhs);
+    std::vector<T> basis{e.scale(rhs, 1.0 / beta)};
+    CMat H(maxiter + 1, maxiter);
+    std::vector<std::vector<cd>> ys;
+    for (int k = 1; k <= maxiter; ++k) {
+      T nv = apply(basis[size_t(k - 1)]);
+      for (int pass = 0; pass < 2; ++pass) {  // CGS2 (krylov.jl:321-332)
+        auto cs = e.inner_many(basis, nv);
+        std::vector<std::pair<cd, T>> terms{{1.0, nv}};
+        for (size_t i = 0; i < basis.size(); ++i) {
+          H(int(i), k - 1) += cs[i];
+          terms.push_back({-cs[i], basis[i]});
+        }
+        nv = e.lin(terms);
+      }
+      g.nmv += 1;
+      const double nn = e.norm(nv);
+      H(k, k - 1) = nn;
+      CMat lead(k, k);
+      for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) lead(i, j) = H(i, j);
+      g.sigma = have_sigma ? sigma_in : rational_shift(smallla::eigvals_hess(lead), tau, true);
+      ys.assign(zs.size(), {});
+      std::vector<std::vector<cd>> sres(zs.size());
+      for (size_t sidx = 0; sidx < zs.size(); ++sidx) {
+        CMat M(k + 1, k);
+        for (int i = 0; i <= k; ++i)
+          for (int j = 0; j < k; ++j)
+            M(i, j) = (i == j ? cd(1.0) : cd(0.0)) - zs[sidx] * (H(i, j) - (i == j ? g.sigma : cd(0.0)));
+        std::vector<cd> rhs_k(size_t(k + 1), 0.0);
+        rhs_k[0] = ds[sidx] * beta;
+        ys[sidx] = smallla::lstsq(M, rhs_k);
+        sres[sidx] = rhs_k;
+        for (int i = 0; i <= k; ++i)
+          for (int j = 0; j < k; ++j) sres[sidx][size_t(i)] -= M(i, j) * ys[sidx][size_t(j)];
+      }
+      double r2 = 0.0;  // |SR Wt^T|_F
+      for (size_t st = 0; st < Wt.size(); ++st)
+        for (int i = 0; i <= k; ++i) {
+          cd acc = 0.0;
+          for (size_t sidx = 0; sidx < zs.size(); ++sidx) acc += sres[sidx][size_t(i)] * Wt[st][sidx];
+          r2 += std::norm(acc);
+        }
+      g.res = std::sqrt(r2);
+      if (nn < tol || g.res <= target || k == maxiter) break;
+      basis.push_back(e.scale(nv, 1.0 / nn));
+    }
+    for (auto& c : ys) {
+      std::vector<T> b(basis.begin(), basis.begin() + long(c.size()));
+      g.Z.push_back(combine(c, b, 1.0));
+    }
+    return g;
+  }
+
+  T radau2_gmres_expv(const std::function<T(const T&)>& apply, const T& vec, int maxiter, double tol,
+                      double conv_tol, bool rshift, ExpvRep& rep) {
+    const double beta0 = e.norm(vec);
+    if (beta0 == 0) return vec;
+    const double A[2][2] = {{5.0 / 12.0, -1.0 / 12.0}, {0.75, 0.25}};
+    const cd half_tr = 0.5 * (A[0][0] + A[1][1]);
+    const cd disc = std::sqrt(half_tr * half_tr - cd(A[0][0] * A[1][1] - A[0][1] * A[1][0]));
+    const cd lam[2] = {half_tr + disc, half_tr - disc};
+    cd Pm[2][2];
+    for (int k = 0; k < 2; ++k) {  // eigenvector (A12, lambda - A11), unit norm
+      const cd v0 = A[0][1], v1 = lam[k] - A[0][0];
+      const double nv = std::sqrt(std::norm(v0) + std::norm(v1));
+      Pm[0][k] = v0 / nv;
+      Pm[1][k] = v1 / nv;
+    }
+    const cd det = Pm[0][0] * Pm[1][1] - Pm[0][1] * Pm[1][0];
+    const cd Pi[2][2] = {{Pm[1][1] / det, -Pm[0][1] / det}, {-Pm[1][0] / det, Pm[0][0] / det}};
+    const std::vector<cd> zs{tau * lam[0], tau * lam[1]};
+    const double target = conv_tol > 0 ? conv_tol * beta0 : 0.0;
+    const std::vector<cd> ds{Pi[0][0] + Pi[0][1], Pi[1][0] + Pi[1][1]};
+    const std::vector<std::vector<cd>> W2{{Pm[0][0], Pm[0][1]}, {Pm[1][0], Pm[1][1]}};
+    Gmres g = shifted_gmres(apply, vec, zs, ds, W2, !rshift, 0.0, target, maxiter, tol);
+    int64_t nmv = g.nmv;
+    const cd sigma = g.sigma;
+    auto stage = [&](const std::vector<T>& Z, int i) { return e.lin({{Pm[i][0], Z[0]}, {Pm[i][1], Z[1]}}); };
+    std::vector<T> Y{stage(g.Z, 0), stage(g.Z, 1)};
+    std::vector<T> R(2);
+    auto residual = [&]() {
+      std::vector<T> BY;
+      for (auto& y : Y) {
+        T img = apply(y);
+        BY.push_back(sigma == cd(0.0) ? img : e.lin({{1.0, img}, {-sigma, y}}));
+      }
+      nmv += 2;
+      for (int i = 0; i < 2; ++i)
+        R[i] = e.lin({{1.0, vec}, {-1.0, Y[i]}, {tau * A[i][0], BY[0]}, {tau * A[i][1], BY[1]}});
+      return std::sqrt(std::pow(e.norm(R[0]), 2) + std::pow(e.norm(R[1]), 2));
+    };
+    double res = residual();
+    int cycles = 1;
+    while (target > 0 && res > target && cycles < 4) {
+      cycles += 1;
+      std::vector<T> dZ;
+      for (int i = 0; i < 2; ++i) {
+        T rho = e.lin({{Pi[i][0], R[0]}, {Pi[i][1], R[1]}});
+        if (e.norm(rho) == 0) {
+          dZ.push_back(rho);
+          continue;
+        }
+        Gmres gk = shifted_gmres(apply, rho, {zs[size_t(i)]}, {1.0}, {{Pm[0][i]}, {Pm[1][i]}}, true,
+                                 sigma, target / std::sqrt(2.0), maxiter, tol);
+        nmv += gk.nmv;
+        dZ.push_back(gk.Z[0]);
+      }
+      for (int i = 0; i < 2; ++i) Y[i] = e.lin({{1.0, Y[i]}, {1.0, stage(dZ, i)}});
+      res = residual();
+    }
+    rep.iters += nmv;
+    rep.nsub += 1;
+    rep.err += res / beta0;
+    return Y[1];
+  }
+
   std::pair<std::vector<cd>, cd> hess_coeffs(const CMat& Hm, cd t) {
     const int n = Hm.n;
     if (n == 0) return {{}, 0.0};
@@ -2260,7 +2394,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     require(prm->dd_mode == 0 || prm->dd_mode == 1, "dd_mode must be 0 (:rank_tail) or 1 (:adaptive)");
     P.dd_mode = prm->dd_mode;
     P.closure_checks = prm->closure_checks != 0;
-    require(prm->root_method >= 0 && prm->root_method <= 3, "root_method must be 0 (exp), 1 (trapezoid), 2 (radau2) or 3 (radau3)");
+    require(prm->root_method >= 0 && prm->root_method <= 4,
+            "root_method must be 0 (exp), 1 (trapezoid), 2 (radau2), 3 (radau3) or 4 (radau2_gmres)");
     P.root_method = prm->root_method;
     P.root_shift = prm->root_noshift == 0;
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
@@ -2400,6 +2535,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
       return gen.apply(e, v);
     };
     auto solve_root = [&](const T& start, Step::ExpvRep& r) {
+      if (P.root_method == 4)
+        return S.radau2_gmres_expv(apply_root, start, P.root_maxiter, 1e-15, P.tol_expv, P.root_shift, r);
       return P.hermitian ? S.lanczos_expv(apply_root, start, P.root_maxiter, 1e-15, P.reorth != 0, P.tol_expv, r,
                                           0, false, P.root_method, P.root_shift)
                          : S.arnoldi_expv(apply_root, start, P.root_maxiter, 1e-15, P.tol_expv, r, 0,

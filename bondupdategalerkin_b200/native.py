@@ -183,7 +183,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         else:
             rng.bit_generator.state = saved.pop()
 
-    methods = {"exp": 0, "trapezoid": 1, "radau2": 2, "radau3": 3}
+    methods = {"exp": 0, "trapezoid": 1, "radau2": 2, "radau3": 3, "radau2_gmres": 4}
     if root_method not in methods:
         raise NotImplementedError(f"root_method {root_method!r}: {tuple(methods)} are built")
     p.root_method = methods[root_method]

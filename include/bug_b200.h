@@ -196,8 +196,9 @@ typedef struct {
   int closure_checks;         /* order > 1: measure every frontier first and close them in passes
                                  (_krylov_closure! with checks = true,
                                  krylov_closure_loop.jl:18-194) instead of the single pass */
-  int root_method;            /* root integrator (root_methods.jl:12-75): 0 exp, 1 trapezoid,
-                                 2 radau2, 3 radau3 (one implicit stage on the Krylov basis) */
+  int root_method;            /* root integrator (root_methods.jl:12-345): 0 exp, 1 trapezoid,
+                                 2 radau2, 3 radau3 (one implicit stage on the Krylov basis),
+                                 4 radau2_gmres (the coupled stages by shifted GMRES) */
   int root_noshift;           /* 1: no imaginary-time spectral shift of the implicit roots
                                  (`root_shift = false`) */
 } bug_step_params;

@@ -112,8 +112,8 @@ def ite_step(psi, mpo, dbeta, *, order=2, root_method="exp", tol_basis=1e-5, tol
     while ``retries`` last (resource-capped failures are not split)."""
     if not dbeta > 0:
         raise ValueError(f"dbeta must be positive, got {dbeta}")
-    if root_method not in ("exp", "trapezoid", "radau2", "radau3"):
-        raise NotImplementedError(f"root_method {root_method!r}: exp, trapezoid, radau2, radau3 are built")
+    if root_method not in ("exp", "trapezoid", "radau2", "radau3", "radau2_gmres"):
+        raise ValueError(f"root_method must be exp, trapezoid, radau2, radau3 or radau2_gmres, got {root_method!r}")
     if on_fail not in ("flag", "error"):
         raise ValueError("on_fail must be flag or error")
     if retries < 0:

@@ -111,7 +111,7 @@ ROOT_PADE = {
     "radau2": ([1.0, 1 / 3], [1.0, -2 / 3, 1 / 6]),
     "radau3": ([1.0, 2 / 5, 1 / 20], [1.0, -3 / 5, 3 / 20, -1 / 60]),
 }
-ROOT_METHODS = ("exp",) + tuple(ROOT_PADE)
+ROOT_METHODS = ("exp",) + tuple(ROOT_PADE) + ("radau2_gmres",)
 
 
 def root_stability(method, z):
@@ -211,6 +211,9 @@ def lanczos_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, reorth=False, c
     with ``report = (iterations, substeps, err)``."""
     if root_method not in ROOT_METHODS:
         raise NotImplementedError(f"root_method {root_method!r}: {ROOT_METHODS} are built")
+    if root_method == "radau2_gmres":
+        return radau2_gmres_expv(ops, apply, tau, vector, tol=tol, maxiter=maxiter,
+                                 conv_tol=conv_tol, rational_shift_on=rational_shift)
     if root_method != "exp":
         substeps = 1
 
@@ -300,6 +303,9 @@ def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, s
     implicit ``root_method`` its stability function instead, in one stage."""
     if root_method not in ROOT_METHODS:
         raise NotImplementedError(f"root_method {root_method!r}: {ROOT_METHODS} are built")
+    if root_method == "radau2_gmres":
+        return radau2_gmres_expv(ops, apply, tau, vector, tol=tol, maxiter=maxiter,
+                                 conv_tol=conv_tol, rational_shift_on=rational_shift)
     if root_method != "exp":
         substeps = 1
 
@@ -363,9 +369,106 @@ def arnoldi_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0, s
     return apply_scale(ops, cur, logscale), (total, nsub, err)
 
 
+# ── radau2_gmres: Radau IIA(2) coupled stages by matrix-free shifted GMRES (root_methods.jl:170-345)
+RADAU2_A = np.array([[5 / 12, -1 / 12], [3 / 4, 1 / 4]])
+RADAU_MAXCYCLE = 4  # _RADAU_MAXCYCLE
+
+
+def _radau2_eig():
+    lam, P = np.linalg.eig(RADAU2_A.astype(np.complex128))
+    return lam, P, np.linalg.inv(P)
+
+
+def shifted_gmres(ops, apply, rhs, tau, zs, ds, Wt, sigma, target, maxiter, tol):
+    """``_shifted_gmres``: one GMRES cycle for ``(I - z_k (B - sigma)) Z_k = d_k rhs`` on one Arnoldi
+    basis of ``B``; stops when the stage residual ``|sum_k Wt[:, k] g_k|`` reaches ``target``, at
+    breakdown or at ``maxiter``. ``sigma = None`` takes the shift from the current Ritz values."""
+    beta = ops.norm(rhs)
+    basis = [ops.lin([(1.0 / beta, rhs)])]
+    H = np.zeros((maxiter + 1, maxiter), dtype=np.complex128)
+    ys, res, sig, nmv = [], math.inf, 0j, 0
+    for k in range(1, maxiter + 1):
+        nv = cgs2(ops, H, k - 1, basis, apply(basis[k - 1]))
+        nmv += 1
+        nn = ops.norm(nv)
+        H[k, k - 1] = nn
+        Hb = H[:k + 1, :k]
+        Ib = np.eye(k + 1, k, dtype=np.complex128)
+        sig = rational_shift(np.linalg.eigvals(H[:k, :k]), tau) if sigma is None else sigma
+        be1 = np.zeros(k + 1, dtype=np.complex128)
+        be1[0] = beta
+        SR = np.zeros((k + 1, len(zs)), dtype=np.complex128)
+        ys = []
+        for i, z in enumerate(zs):
+            M = Ib - z * (Hb - sig * Ib)
+            c = np.linalg.lstsq(M, ds[i] * be1, rcond=None)[0]
+            ys.append(c)
+            SR[:, i] = ds[i] * be1 - M @ c
+        res = float(np.linalg.norm(SR @ Wt.T))
+        if nn < tol or res <= target or k == maxiter:
+            break
+        basis.append(ops.lin([(1.0 / nn, nv)]))
+    return [combine(ops, c, basis[:len(c)], 1.0) for c in ys], res, nmv, sig
+
+
+def radau2_gmres_expv(ops, apply, tau, vector, tol=1e-13, maxiter=60, conv_tol=0.0,
+                      rational_shift_on=True):
+    """``radau2_gmres_expv``: one Radau IIA(2) step of ``dx/dt = B x`` over ``tau``, the coupled
+    stages decoupled by the eigenvectors of the Butcher matrix and solved on one Krylov basis,
+    restarted on the true stage residual at most ``RADAU_MAXCYCLE`` times. Returns ``(Y_2,
+    (applications, 1, relative stage residual))``."""
+    tau = complex(tau)
+    beta0 = ops.norm(vector)
+    if beta0 == 0:
+        return vector, (0, 0, 0.0)
+    lam, P, Pinv = _radau2_eig()
+    zs = tau * lam
+    target = conv_tol * beta0 if conv_tol > 0 else 0.0
+    Zs, _, nmv, sigma = shifted_gmres(ops, apply, vector, tau, zs, Pinv @ np.ones(2), P,
+                                      None if rational_shift_on else 0j, target, maxiter, tol)
+
+    def stage(Z, i):
+        return ops.lin([(P[i, 0], Z[0]), (P[i, 1], Z[1])])
+
+    Y = [stage(Zs, 0), stage(Zs, 1)]
+
+    def residual(Y):
+        nonlocal nmv
+        BY = []
+        for y in Y:
+            img = apply(y)
+            BY.append(img if sigma == 0 else ops.lin([(1.0, img), (-sigma, y)]))
+        nmv += 2
+        R = [ops.lin([(1.0, vector), (-1.0, Y[i]), (tau * RADAU2_A[i, 0], BY[0]),
+                      (tau * RADAU2_A[i, 1], BY[1])]) for i in range(2)]
+        return R, math.sqrt(ops.norm(R[0]) ** 2 + ops.norm(R[1]) ** 2)
+
+    R, res = residual(Y)
+    cycles = 1
+    while target > 0 and res > target and cycles < RADAU_MAXCYCLE:
+        cycles += 1
+        dZ = []
+        for i in range(2):
+            rho = ops.lin([(Pinv[i, 0], R[0]), (Pinv[i, 1], R[1])])
+            if ops.norm(rho) == 0:
+                dZ.append(rho)
+                continue
+            Zk, _, m, _ = shifted_gmres(ops, apply, rho, tau, zs[i:i + 1], np.ones(1, dtype=np.complex128),
+                                        P[:, i:i + 1], sigma, target / math.sqrt(2), maxiter, tol)
+            nmv += m
+            dZ.append(Zk[0])
+        Y = [ops.lin([(1.0, Y[i]), (1.0, stage(dZ, i))]) for i in range(2)]
+        R, res = residual(Y)
+    return Y[1], (nmv, 1, res / beta0)
+
+
 def expv(ops, apply, tau, vector, hermitian=True, **kw):
-    """``expv`` dispatcher (``root_methods.jl:359-402``): ``root_method`` ``"exp"`` or one of the
-    implicit roots ``"trapezoid"``, ``"radau2"``, ``"radau3"`` (``"radau2_gmres"`` is not built)."""
+    """``expv`` dispatcher (``root_methods.jl:359-402``): ``root_method`` ``"exp"``, one of the
+    implicit roots ``"trapezoid"``, ``"radau2"``, ``"radau3"``, or ``"radau2_gmres"``."""
+    if kw.get("root_method") == "radau2_gmres":
+        return radau2_gmres_expv(ops, apply, tau, vector, tol=kw.get("tol", 1e-13),
+                                 maxiter=kw.get("maxiter", 60), conv_tol=kw.get("conv_tol", 0.0),
+                                 rational_shift_on=kw.get("rational_shift", True))
     if hermitian:
         return lanczos_expv(ops, apply, tau, vector, **kw)
     kw.pop("reorth", None)

@@ -268,7 +268,7 @@ def test_closure_checks(dev, native):
              native=native, closure_checks=True)
 
 
-@pytest.mark.parametrize("method", ["trapezoid", "radau2", "radau3"])
+@pytest.mark.parametrize("method", ["trapezoid", "radau2", "radau3", "radau2_gmres"])
 def test_implicit_root_methods(dev, method):
     """The implicit root integrators (one stage of the Pade stability function on the root's
     Krylov basis) against the oracle, in real time and, with the spectral shift, imaginary time."""

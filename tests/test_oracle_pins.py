@@ -291,3 +291,20 @@ def test_implicit_roots_closed_form(method, tau):
     order = {"trapezoid": 2, "radau2": 3, "radau3": 5}[method]
     z = 1e-2
     assert abs(K.root_stability(method, z) - np.exp(z)) < 10 * z ** (order + 1)
+
+
+@pytest.mark.parametrize("tau", [-0.7j, -0.4 + 0j])
+def test_radau2_gmres_is_radau2(tau):
+    """The coupled-stage Radau IIA(2) solved by shifted GMRES converges to the same step as the
+    rational ``radau2`` root: R(tau (A - sigma)) x on a diagonal operator, with the stage residual
+    it reports at rounding level."""
+    x = _multi_sector()
+    scale = lambda q: 0.5 * q + 1.0
+    lam = {k: scale(k[2]) for k in x.blocks}
+    sigma = max(lam.values(), key=lambda v: (tau * v).real) if tau.real != 0 else 0.0
+    want = B.BT(x.legs, {k: K.root_stability("radau2", tau * (lam[k] - sigma)) * v
+                         for k, v in x.blocks.items()})
+    y, rep = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=True,
+                    root_method="radau2_gmres", conv_tol=1e-12)
+    assert B.norm(B.sub(y, want)) < 1e-12 * B.norm(want)
+    assert rep[2] < 1e-12
