@@ -17,7 +17,9 @@ same steps. Under torchrun each rank runs an independent replica (the step does 
 
 ``--workload tdvp2`` measures the reference's matched-accuracy comparator, two-site TDVP
 (``tdvp2_step!``, maxdim 256, per-cut allowance ``weight_tol`` 1e-7, Lanczos with 30 iterations),
-over the same chain and 100-step trajectory (metric TDVP2 steps/s).
+over the same chain and 100-step trajectory (metric TDVP2 steps/s). ``--workload ite`` measures
+normalised imaginary time (``ite_step!`` with its energy shift, outside residual and retries) on the
+L = 32 Heisenberg chain from Neel, dbeta 0.125 to beta 4 (metric ITE steps/s).
 """
 
 from __future__ import annotations
@@ -48,6 +50,11 @@ HESTON_NAME = "heston_qtt_10x10bits_maxdim64_tau0.02_arnoldi"
 # per-cut allowance (weight_tol = the step's default tol_trunc 1e-7), maxdim 256, Lanczos.
 TDVP2 = dict(maxdim=256, weight_tol=1e-7)
 TDVP2_NAME = "tdvp2_xxz_quench_L64_delta0.5_domainwall_maxdim256_wtol1e-7"
+# Normalised imaginary time (ite_step!) on the Heisenberg chain from Neel, the setting of the
+# reference's heisenberg_ite fixture at L = 32: dbeta 0.125, order 2, maxdim 128, the ite_step!
+# defaults (tol_basis 1e-5, tol_trunc 1e-6, tol_root 1e-6, energy shift, outside residual).
+ITE = dict(L=32, delta=1.0, dbeta=0.125, kw=dict(order=2, maxdim=128))
+ITE_NAME = "ite_heisenberg_L32_neel_dbeta0.125_order2_maxdim128"
 KIND = ["xxz"]
 L2_FLUSH_BYTES = 256 << 20
 _HESTON_DOMAIN = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
@@ -67,6 +74,10 @@ def dev_step(mod, psi, mpo, rng):
         from bondupdategalerkin_b200 import native as N
 
         return N.tdvp2_step(psi, mpo, tau(), **TDVP2)
+    if KIND[0] == "ite":
+        from bondupdategalerkin_b200 import ite as DI
+
+        return DI.ite_step(psi, mpo, ITE["dbeta"], rng=rng, **ITE["kw"])
     return mod.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
 
 
@@ -76,13 +87,17 @@ def oracle_step(psi, mpo, rng):
         from oracle import tdvp as OT
 
         return OT.tdvp2_step(psi, mpo, tau(), **TDVP2)
+    if KIND[0] == "ite":
+        from oracle import ite as OI
+
+        return OI.ite_step(psi, mpo, ITE["dbeta"], rng=rng, **ITE["kw"])
     from oracle import step as OS
 
     return OS.cbe_bug_step(psi, mpo, tau(), rng=rng, **step_kwargs())
 
 
 def metric_name():
-    return "tdvp2_steps_per_s" if KIND[0] == "tdvp2" else "bug_steps_per_s"
+    return {"tdvp2": "tdvp2_steps_per_s", "ite": "ite_steps_per_s"}.get(KIND[0], "bug_steps_per_s")
 
 
 def step_kwargs():
@@ -103,6 +118,8 @@ def device_inputs():
         return psi, P.heston_mpo(g, P.HestonParams(*HESTON["params"]))
     from bondupdategalerkin_b200 import models as DM
 
+    if KIND[0] == "ite":
+        return DM.neel_state(ITE["L"]), DM.xxz_mpo(ITE["L"], J=1.0, delta=ITE["delta"])
     w = WORKLOAD
     return DM.domain_wall_state(w["L"]), DM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
 
@@ -117,6 +134,8 @@ def oracle_inputs():
         return psi, Q.heston_mpo(g, Q.HestonParams(*HESTON["params"]))
     from oracle import models as OM
 
+    if KIND[0] == "ite":
+        return OM.neel_state(ITE["L"]), OM.xxz_mpo(ITE["L"], J=1.0, delta=ITE["delta"])
     w = WORKLOAD
     return OM.domain_wall_state(w["L"]), OM.xxz_mpo(w["L"], J=w["J"], delta=w["delta"])
 
@@ -133,6 +152,16 @@ def config_dict(args, ws, max_bond=None):
             cfg["max_bond_dim_after"] = max_bond
         return cfg
     w = WORKLOAD
+    if KIND[0] == "ite":
+        cfg = {"workload": ITE_NAME, "L": ITE["L"], "delta": ITE["delta"], "dbeta": ITE["dbeta"],
+               "order": 2, "maxdim": 128, "tol_basis": 1e-5, "eshift": "energy",
+               "outside_residual": True,
+               "timed_steps": f"{args.warmup + 1}..{args.warmup + args.steps}",
+               "l2": "flushed before every step (256 MiB write)",
+               "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+        if max_bond is not None:
+            cfg["max_bond_dim_after"] = max_bond
+        return cfg
     if KIND[0] == "tdvp2":
         cfg = {"workload": TDVP2_NAME, "L": w["L"], "delta": w["delta"], "tau": "-0.05i",
                "maxdim": TDVP2["maxdim"], "weight_tol": TDVP2["weight_tol"], "krylov": "lanczos, maxiter 30",
@@ -413,7 +442,7 @@ def run_engine(args):
     assert psi_r.bond_dims() == final_dims, "profiled replay diverged from the timed steps"
 
     # ── end to end through host buffers: upload state+MPO, step, download the new state ──
-    from bondupdategalerkin_b200.api import step_host, tdvp2_step_host
+    from bondupdategalerkin_b200.api import ite_step_host, step_host, tdvp2_step_host
 
     host_state = [DT.to_blocks(t) for t in start_psi.tensors]
     host_mpo = [DT.to_blocks(t) for t in mpo.tensors]
@@ -428,6 +457,9 @@ def run_engine(args):
         e0.record(stream)
         if KIND[0] == "tdvp2":
             host_state, center, io = tdvp2_step_host(host_state, center, host_mpo, tau(), **TDVP2)
+        elif KIND[0] == "ite":
+            host_state, center, io = ite_step_host(host_state, center, host_mpo, ITE["dbeta"],
+                                                   rng=rng_e, **ITE["kw"])
         else:
             host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
                                                native=args.host == "native", **step_kwargs())
@@ -654,10 +686,12 @@ def main():
     ap.add_argument("--L", type=int, default=None,
                     help="chain length override (smaller cases for profiler captures only)")
     ap.add_argument("--workload", default="xxz",
-                    choices=["xxz", "heston", "tdvp2", "batch", "served"],
+                    choices=["xxz", "heston", "tdvp2", "ite", "batch", "served"],
                     help="xxz: the L = 64 XXZ quench (the headline); heston: the 10 + 10-bit "
                          "Heston QTT field (47 timed steps after 3 warm-up make its 50); tdvp2: the "
-                         "two-site TDVP baseline over the headline's 100-step trajectory; batch: 64 chains at once on the job server; served: a Poisson "
+                         "two-site TDVP baseline over the headline's 100-step trajectory; ite: normalised "
+                         "imaginary time on the L = 32 Heisenberg chain (29 timed steps of dbeta "
+                         "0.125 after 3 warm-up reach beta 4); batch: 64 chains at once on the job server; served: a Poisson "
                          "job stream")
     ap.add_argument("--workers", type=int, default=0, help="job server workers (0: min(16, cores))")
     ap.add_argument("--jobs", type=int, default=0, help="batch/served: number of jobs")
@@ -667,6 +701,8 @@ def main():
     KIND[0] = args.workload
     if args.workload == "heston" and "--steps" not in sys.argv:
         args.steps = 47
+    if args.workload == "ite" and "--steps" not in sys.argv:
+        args.steps = 29
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.L is not None:

@@ -27,7 +27,7 @@ from .tensor import from_blocks, to_blocks
 
 __all__ = ["cbe_bug_step", "cbe_bug_step_python_host", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
            "domain_wall_state", "neel_state", "product_state", "xxz_mpo", "tdvp2_step",
-           "tdvp2_step_host", "ite_step", "ite_evolve", "ite_energy", "log_panel_steps",
+           "tdvp2_step_host", "ite_step", "ite_step_host", "ite_evolve", "ite_energy", "log_panel_steps",
            "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule"]
 
 
@@ -82,3 +82,24 @@ def tdvp2_step_host(host_state, center, host_mpo, tau, **kwargs):
     out = [to_blocks(t) for t in psi.tensors]
     d2h = sum(16 * t.nelem for t in psi.tensors)
     return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)
+
+
+def ite_step_host(host_state, center, host_mpo, dbeta, **kwargs):
+    """One normalised imaginary-time step (``ite_step!``) on host-resident data: upload, step on
+    the device, download. Returns ``(new_host_state, new_center, io)``."""
+    h2d = 0
+    sites = []
+    for legs, blocks in host_state:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        sites.append(t)
+    ws = []
+    for legs, blocks in host_mpo:
+        t = from_blocks(legs, blocks)
+        h2d += 16 * t.nelem
+        ws.append(t)
+    psi = MPS(sites, center)
+    rec = ite_step(psi, MPO(ws), dbeta, **kwargs)
+    out = [to_blocks(t) for t in psi.tensors]
+    d2h = sum(16 * t.nelem for t in psi.tensors)
+    return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=rec)
