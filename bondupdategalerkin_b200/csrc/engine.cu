@@ -528,8 +528,12 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
       sbytes += 16.0 * (2.0 * mm * r + r * r + (order[s2]->m + order[s2]->n) * r);
       sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
     }
+    // one warp per column pair of a round (8 to 32 warps): a round's pairs run side by side
+    // instead of in turns. Which warp takes a pair or a column changes no reduction order, so
+    // the factors are the same bits for any warp count.
+    const int warps = int(std::min<int64_t>(32, std::max<int64_t>(8, (max_r + 1) / 2)));
     const bugk::Blob blob = c->begin();
-    bugk::launch_svd(blob, dsd, np, dpk, max_smem, max_r > 48 ? 1024 : 256, c->stream);
+    bugk::launch_svd(blob, dsd, np, dpk, max_smem, 32 * warps, c->stream);
     c->launched(BUG_K_SVD, sflops, sbytes);
   }
   // the kernel wrote singular values and sweep counts into `host`
@@ -759,8 +763,14 @@ TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, dou
   }
   QrDesc* dq = c->push(qd);
   CopyDesc* dp = c->push(packs);
+  // one warp per column of the widest sector (8 to 32 warps): a reflector reaches the remaining
+  // columns side by side. Which warp takes a column changes no reduction order, so Q and R are the
+  // same bits for any warp count.
+  int64_t max_n = 0;
+  for (auto& sc : secs) max_n = std::max<int64_t>(max_n, sc.n);
+  const int qwarps = int(std::min<int64_t>(32, std::max<int64_t>(8, max_n)));
   const bugk::Blob blob = c->begin();
-  bugk::launch_qr(blob, dq, int(qd.size()), dp, c->stream);
+  bugk::launch_qr(blob, dq, int(qd.size()), dp, 32 * qwarps, c->stream);
   double qflops = 0.0;
   for (auto& sc : secs) qflops += 8.0 * 2.0 * double(sc.m) * double(sc.n) * double(std::min(sc.m, sc.n));
   c->launched(BUG_K_SVD, qflops, 0.0);

@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), con
 
 constexpr int kMaxSweeps = 60;
 constexpr int kMaxR = 1024;
-constexpr int kSvdThreads = 1024;  // wide sectors: one warp per column pair, 32 pairs per pass
+constexpr int kSvdThreads = 1024;  // launched with one warp per column pair, 8 to 32 warps
 
 __device__ __forceinline__ void rr_pair(int i, int round, int re, int& a, int& b) {
   const int n1 = re - 1;
@@ -584,10 +584,11 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS
 // sign(beta) so that R_kk >= 0.
 
 constexpr int kQrMaxN = 1024;
+constexpr int kQrThreads = 1024;  // launched with one warp per column of the widest sector, 8 to 32 warps
 constexpr double kPivotTie = 1e-10;
 
 template <int N>
-__global__ void __launch_bounds__(kThreads) qr_kernel(BUG_BLOB_PARAMS(N), const QrDesc* descs,
+__global__ void __launch_bounds__(kQrThreads) qr_kernel(BUG_BLOB_PARAMS(N), const QrDesc* descs,
                                                       const CopyDesc* packs) {
   const Rebase rb{pb.b, arena, nb};
   descs = rb(descs);
@@ -805,10 +806,11 @@ void launch_stage(const Blob& b, const Stage& st, cudaStream_t s) {
 #undef BUG_STAGE_LAUNCH
 }
 
-void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, cudaStream_t s) {
+void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, int threads,
+               cudaStream_t s) {
   if (nprob <= 0) return;
 #define BUG_QR_LAUNCH(NB, P, NBYTES) \
-  qr_kernel<NB><<<nprob, kThreads, 0, s>>>(P, b.arena, (NBYTES), d_desc, packs)
+  qr_kernel<NB><<<nprob, threads, 0, s>>>(P, b.arena, (NBYTES), d_desc, packs)
   BUG_WITH_BLOB(b, BUG_QR_LAUNCH);
 #undef BUG_QR_LAUNCH
 }

@@ -179,7 +179,8 @@ int stage_items(const Stage& s);
 int stage_grid_limit();
 void launch_stage(const Blob& b, const Stage& st, cudaStream_t s);
 // Column-pivoted Householder QR, one CTA per sector (see QrDesc).
-void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, cudaStream_t s);
+void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, int threads,
+               cudaStream_t s);
 // Dynamic shared memory the SVD kernel may use per CTA on this device (opt-in maximum minus its
 // static arrays).
 int svd_smem_limit();
