@@ -425,13 +425,19 @@ __global__ void __launch_bounds__(kSvdThreads) jacobi_svd_kernel(BUG_BLOB_PARAMS
         be = warp_sum(be);
         gr = warp_sum(gr);
         gi = warp_sum(gi);
-        const double g = sqrt(gr * gr + gi * gi);
-        if (al > negl && be > negl && g > tol * sqrt(al) * sqrt(be)) {
+        // |a_p^H a_q| > tol |a_p| |a_q| tested on squares, so a pair that does not rotate (every
+        // pair of the last sweep) costs no square root; the rotation then takes two reciprocal
+        // square roots, one square root and one division in sequence. (tol^2 al) be is infinite
+        // only where the threshold exceeds every finite g2, so the test is exact wherever g2 is
+        // finite and normal, the range in which |a_p^H a_q| itself was computable before.
+        const double g2 = gr * gr + gi * gi;
+        if (al > negl && be > negl && g2 > (tol * tol * al) * be) {
           if (lane == 0) rotated = 1;
-          const double zeta = (be - al) / (2.0 * g);
+          const double ig = rsqrt(g2);  // 1 / |gamma|
+          const double zeta = (be - al) * (0.5 * ig);
           const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-          const double2 e = make_double2(gr / g, -gi / g);  // e^{-i phi}, gamma = g e^{i phi}
+          const double c = rsqrt(1.0 + t * t), s = c * t;
+          const double2 e = make_double2(gr * ig, -gi * ig);  // e^{-i phi}, gamma = |gamma| e^{i phi}
           for (int i = lane; i < mm; i += 32) {
             const double2 x = ap[i];
             const double2 ey = cmul(e, aq[i]);

@@ -7,7 +7,8 @@ then renormalisation through the centre tensor. A rejected step is redone from t
 sub-steps (their number from the defect's scaling, ``(resid / tol_basis)^(1/(p+1))``, else two)
 while ``retries`` last; resource-capped failures are flagged at once. The step runs in the library
 (``native.cbe_bug_step``); energies are ``<psi|H|psi> / <psi|psi>`` from a device environment
-sweep. Not built: ``root_method`` other than ``:exp`` and ``parallel`` half-sweeps.
+sweep. ``root_method`` is ``exp``, ``trapezoid``, ``radau2``, ``radau3`` or ``radau2_gmres``. Not
+built: ``parallel`` half-sweeps.
 """
 
 from __future__ import annotations
