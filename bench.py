@@ -182,10 +182,9 @@ def config_dict(args, ws, max_bond=None):
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from bondupdategalerkin_b200.replicas import world
+
+    return world()
 
 
 class ClockSampler:
@@ -337,14 +336,12 @@ def mps_bytes(psi):
 def run_engine(args):
     import torch
 
-    ws, rank, local = dist_env()
-    if ws > 1:
-        import datetime
+    from bondupdategalerkin_b200.replicas import Replicas
 
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                             device_id=torch.device("cuda", local))
+    ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    reps = Replicas("nccl", device=dev)  # N independent replicas: timing collectives only
     from bondupdategalerkin_b200 import _engine as E
     from bondupdategalerkin_b200 import build as Bld
 
@@ -368,14 +365,10 @@ def run_engine(args):
     start_psi = psi.copy()
     start_rng = rng.bit_generator.state
 
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
-
     # ── timed region ──
     ctx.synchronize()
     torch.cuda.synchronize(dev)
-    barrier()
+    reps.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = ctx.launches()
@@ -404,15 +397,10 @@ def run_engine(args):
                  "sync_wait_ms_per_step": 1e3 * hstats["wait_s"] / args.steps,
                  "launch_call_ms_per_step": 1e3 * hstats["launch_s"] / args.steps,
                  "alloc_call_ms_per_step": 1e3 * hstats["alloc_s"] / args.steps}
-    barrier()
+    reps.barrier()
     clk = clocks.stop()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = float(sum(step_ms))
-    if ws > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = ws * args.steps / (total_ms / 1e3)
+    value, total_ms = reps.rate(args.steps, float(sum(step_ms)))  # max over ranks
     final_dims = psi.bond_dims()
     if args.no_replay:
         if rank == 0:
@@ -422,8 +410,7 @@ def run_engine(args):
                               "host_waits": host_line,
                               "note": "--no-replay: timing run only (no e2e, roofline or baseline)"}),
                   flush=True)
-        if ws > 1:
-            torch.distributed.destroy_process_group()
+        reps.close()
         return
 
     # ── profiled replay of the same steps (kernel durations on the engine stream) ──
@@ -468,11 +455,7 @@ def run_engine(args):
         e2e_ms += e0.elapsed_time(e1)
         h2d += io["h2d_bytes"]
         d2h += io["d2h_bytes"]
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = ws * args.steps / (e2e_ms / 1e3)
+    e2e_value, e2e_ms = reps.rate(args.steps, e2e_ms)  # max over ranks
 
     # ── roofline of the dominant kernel family ──
     hbm_peak, hbm_src = measured_peaks()
@@ -522,8 +505,7 @@ def run_engine(args):
         line["fp64_zgemm_tflops_measured"] = zgemm
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        torch.distributed.destroy_process_group()
+    reps.close()
 
 
 # ── batched and served workloads (the native job server) ─────────────────────────────────────
