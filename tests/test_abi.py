@@ -33,6 +33,13 @@ def test_python_binding_covers_the_header():
     assert lib.bug_version().decode().startswith("bug_b200")
 
 
+def test_integration_guide_names_every_entry_point():
+    """The binding guide for the reference's host lists every function the header declares."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in declared() if not re.search(rf"\b{n}\b", guide)]
+    assert not missing, missing
+
+
 def test_context_creation_fails_loudly_without_a_device():
     import pytest
     import torch
