@@ -59,7 +59,7 @@ def _perturbed_mpo(mpo, seed, eps=1e-14):
 
 
 def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10, spread=None,
-               **kw):
+               dom=None, hp=HP, fx=None, fv=None, **kw):
     from bondupdategalerkin_b200 import build
 
     build.build()
@@ -68,14 +68,15 @@ def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10,
     from bondupdategalerkin_b200 import step as DS
 
     dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
-    dom = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
+    dom = dom or dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
     og, pg = Q.qtt_grid(nbits, nbits, **dom), P.qtt_grid(nbits, nbits, **dom)
-    fx, fv = (lambda x: np.exp(0.5 * x)), (lambda v: np.exp(-v))
+    fx = fx or (lambda x: np.exp(0.5 * x))
+    fv = fv or (lambda v: np.exp(-v))
     opsi = Q.qtt_mps(Q.qtt_separable(og, fx, fv), center=1)
     dpsi = P.qtt_mps(P.qtt_separable(pg, fx, fv), center=1)
-    ompo = Q.heston_mpo(og, Q.HestonParams(*HP))
+    ompo = Q.heston_mpo(og, Q.HestonParams(*hp))
     if mpo_from == "product":
-        dmpo = P.heston_mpo(pg, P.HestonParams(*HP))
+        dmpo = P.heston_mpo(pg, P.HestonParams(*hp))
     else:
         from bondupdategalerkin_b200 import models as DM
         from tests.gpu_util import to_dev
@@ -124,3 +125,29 @@ def test_heston_10x10_bits_config():
 def test_heston_10x10_bits_product_mpo():
     """The same with the product's own MPO on device."""
     run_heston(10, 2, 64, True, spread="mpo")
+
+
+def test_heston_backward_fixture():
+    """The reference's frozen Heston backward pricing run (5 + 5 bits, x in [-3, 3], v in [0, 1],
+    r 0.03 q 0 kappa 1.5 theta 0.09 sigma 0.5 rho -0.7, softplus payoff, ten steps of 0.02):
+    the native step on the product's builders follows the oracle step by step (dimensions,
+    verdicts, iterations, infidelity <= 1e-12) and ends within 1e-4 of the frozen final state,
+    as the oracle does (2.8e-5)."""
+    import json
+    import os
+
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "b155550.json")))
+    d = d["qtt_heston_backward"]
+    ref = np.array(d["final_state"]["re"]) + 1j * np.array(d["final_state"]["im"])
+
+    def payoff(x):
+        z = (np.exp(x) - 1.0) / 0.02
+        return 0.02 * (z if z > 30 else np.log1p(np.exp(z)))
+
+    dom = dict(x=(-3.0, 3.0), y=(0.0, 1.0), periodic_x=False, periodic_y=False)
+    opsi, dpsi = run_heston(d["N"], d["steps"], 64, True, dom=dom,
+                            hp=(0.03, 0.0, 1.5, 0.09, 0.5, -0.7), fx=payoff, fv=lambda v: 1.0,
+                            order=2, tol_basis=1e-8, tol_trunc=1e-10)
+    dense = Q.qtt_dense(mps_to_host(dpsi))
+    err = np.linalg.norm(dense - ref) / np.linalg.norm(ref)
+    assert err < 1e-4, err
