@@ -35,6 +35,20 @@ using smallla::RMat;
 
 constexpr double EPS = 2.220446049250313e-16;
 constexpr double CBE_EPS = 100 * EPS;
+
+// _tridiag_eigen's check (krylov.jl:77-86): a non-finite Lanczos coefficient comes from the input
+// vector or the operator, not from the eigensolver, and is reported as such (BUG_ENONFINITE)
+// instead of as a convergence failure.
+inline void require_finite_tridiag(const double* alpha, size_t na, const double* beta, size_t nb) {
+  size_t ca = 0, cb = 0;
+  for (size_t i = 0; i < na; ++i) ca += !std::isfinite(alpha[i]);
+  for (size_t i = 0; i < nb; ++i) cb += !std::isfinite(beta[i]);
+  if (ca || cb)
+    throw BugError(BUG_ENONFINITE, "Lanczos tridiagonal has non-finite entries (" + std::to_string(ca) +
+                                       " of " + std::to_string(na) + " alpha, " + std::to_string(cb) +
+                                       " of " + std::to_string(nb) +
+                                       " beta): the input vector or the operator is not finite");
+}
 constexpr double KRY_BREAKDOWN = 1e-13;
 constexpr int KRY_MAXDEPTH = 64;
 constexpr double KRY_SKEW_TOL = 1e-12;
@@ -1809,8 +1823,7 @@ struct Step {
     return {c, t * sigma};
   }
   static Eig tridiag_eigen(const std::vector<double>& a, const std::vector<double>& b) {
-    for (double x : a) require(std::isfinite(x), "Lanczos tridiagonal has non-finite entries");
-    for (double x : b) require(std::isfinite(x), "Lanczos tridiagonal has non-finite entries");
+    require_finite_tridiag(a.data(), a.size(), b.data(), b.size());
     Eig eg;
     smallla::eigh_tridiag(a, std::vector<double>(b.begin(), b.begin() + std::max<ptrdiff_t>(ptrdiff_t(a.size()) - 1, 0)),
                           eg.vals, eg.vecs);
@@ -3059,6 +3072,7 @@ extern "C" int bug_la_eigh_tridiag(int n, const double* d, const double* e, doub
     require(n >= 0, "bad size");
     std::vector<double> dd(d, d + n), ee;
     if (n > 1) ee.assign(e, e + n - 1);
+    require_finite_tridiag(dd.data(), dd.size(), ee.data(), ee.size());
     std::vector<double> v;
     smallla::RMat V;
     smallla::eigh_tridiag(dd, ee, v, V);

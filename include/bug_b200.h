@@ -417,7 +417,7 @@ int bug_la_eigh(int n, const double* a, double* vals, double* vecs);
 /* Eigen-decomposition of the symmetric tridiagonal matrix with diagonal d (n) and off-diagonal e
  * (n - 1) by implicit QR steps with Wilkinson shifts: ascending eigenvalues and eigenvectors as
  * columns (row-major n x n); replaces syevr in _tridiag_eigen (krylov.jl:77-98), the step's
- * Lanczos tridiagonal. */
+ * Lanczos tridiagonal. A non-finite entry returns BUG_ENONFINITE, as _tridiag_eigen throws. */
 int bug_la_eigh_tridiag(int n, const double* d, const double* e, double* vals, double* vecs);
 /* Eigenvalues of a complex upper-Hessenberg n x n matrix; replaces geev in _hess_coeffs. */
 int bug_la_eigvals_hess(int n, const double* a, double* vals_re_im);

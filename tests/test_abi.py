@@ -156,3 +156,60 @@ def test_tridiagonal_eigensolver_matches_lapack():
         assert np.max(np.abs(vals - want)) <= 1e-13 * scale, (n, np.max(np.abs(vals - want)))
         assert np.max(np.abs(vecs.T @ vecs - np.eye(n))) <= 1e-13
         assert np.max(np.abs(vecs @ np.diag(vals) @ vecs.T - T)) <= 1e-13 * scale
+
+
+def _tridiag(lib, d, e):
+    import numpy as np
+
+    from bondupdategalerkin_b200 import _engine
+
+    n = len(d)
+    vals, vecs = np.zeros(n), np.zeros((n, n))
+    dp = np.ascontiguousarray(d, float)
+    ep = np.ascontiguousarray(e if n > 1 else [0.0], float)
+    code = lib.bug_la_eigh_tridiag(n, dp.ctypes.data_as(_engine._c_double_p),
+                                   ep.ctypes.data_as(_engine._c_double_p),
+                                   vals.ctypes.data_as(_engine._c_double_p),
+                                   vecs.ctypes.data_as(_engine._c_double_p))
+    return code, vals, vecs
+
+
+def test_tridiagonal_eigensolver_reference_case_and_non_finite_input():
+    """The reference's own case for ``_tridiag_eigen`` (``test_krylov_weights.jl:105-116``): exact
+    to 1e-12 on finite input; NaN or Inf is named (BUG_ENONFINITE, the entries counted) instead of
+    surfacing as a convergence failure."""
+    import numpy as np
+
+    from bondupdategalerkin_b200 import _engine, build
+
+    build.build()
+    lib = _engine.load()
+    d, e = [0.3, -1.2, 2.5, 0.0, 1e-9], [1.0, 1e-12, 0.7, 2.0]
+    code, vals, vecs = _tridiag(lib, d, e)
+    assert code == 0
+    T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    assert np.linalg.norm(T @ vecs - vecs @ np.diag(vals)) < 1e-12
+    assert np.linalg.norm(vecs.T @ vecs - np.eye(5)) < 1e-12
+    enonfinite = [k for k, v in _engine.STATUS.items() if v == "BUG_ENONFINITE"][0]
+    for d, e, counts in (([0.0, np.nan], [1.0], "1 of 2 alpha, 0 of 1 beta"),
+                         ([0.0, 1.0], [np.inf], "0 of 2 alpha, 1 of 1 beta")):
+        code, _, _ = _tridiag(lib, d, e)
+        assert code == enonfinite
+        msg = lib.bug_last_error().decode()
+        assert "non-finite" in msg and counts in msg, msg
+
+
+def test_krylov_weight_two_by_two_known_answer():
+    """The native weight on the reference's 2 x 2 (``test_krylov_weights.jl:44-56``): H_1 = [2 pi],
+    beta = 1, tau = -i gives |tau| beta int_0^1 |exp(-2 pi i s)| ds = 1."""
+    import numpy as np
+
+    from bondupdategalerkin_b200 import _engine, build
+
+    build.build()
+    lib = _engine.load()
+    H = np.ascontiguousarray([[2 * np.pi, 0.0], [1.0, 0.0]], dtype=np.complex128)
+    out = np.zeros(1)
+    _engine.check(lib.bug_la_kry_weight(2, H.view(np.float64).ctypes.data_as(_engine._c_double_p),
+                                        1, 0.0, -1.0, 1, out.ctypes.data_as(_engine._c_double_p)))
+    assert abs(out[0] - 1.0) <= 1e-10

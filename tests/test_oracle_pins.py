@@ -3,6 +3,10 @@
 * Test A lists: ``test/BUG/Randomised/test_expansion.jl:15-88``.
 * The two-spin entangling step: ``test_expansion.jl:90-109``.
 * ``expv`` against sector-diagonal closed forms: ``test/BUG/Core/LocalSolvers/test_krylov.jl:21-168``.
+* The Krylov stopping weights (``test/BUG/Core/LocalSolvers/test_krylov_weights.jl:44-117``): the
+  residual integral on the 2 x 2 where Saad's scalar cancels (weight 1), its bound on random
+  Hermitian generators, the root's tail guarded over the step, ``_tridiag_eigen`` exact and naming
+  non-finite input.
 * The b155550 frozen trajectories, with the reference's own tolerances and settings
   (``test/BUG/TimeEvolution/test_fixtures_b155550.jl:23-97``): S^z within 1e-5 of the frozen
   profile and within ``2 err_exact + 1e-6`` of free fermions, status as frozen; the frozen runs used
@@ -308,3 +312,96 @@ def test_radau2_gmres_is_radau2(tau):
                     root_method="radau2_gmres", conv_tol=1e-12)
     assert B.norm(B.sub(y, want)) < 1e-12 * B.norm(want)
     assert rep[2] < 1e-12
+
+
+# ── the Krylov stopping weights (test_krylov_weights.jl) ─────────────────────────────────────
+
+
+def _arnoldi(H, seed, depth):
+    """Plain Arnoldi with two Gram-Schmidt passes, the test's own recurrence (not the oracle's)."""
+    basis = np.zeros((len(seed), depth + 1), dtype=np.complex128)
+    hess = np.zeros((depth + 1, depth + 1), dtype=np.complex128)
+    basis[:, 0] = seed / np.linalg.norm(seed)
+    for step in range(depth):
+        image = H @ basis[:, step]
+        for _ in range(2):
+            proj = basis[:, : step + 1].conj().T @ image
+            hess[: step + 1, step] += proj
+            image = image - basis[:, : step + 1] @ proj
+        hess[step + 1, step] = np.linalg.norm(image)
+        basis[:, step + 1] = image / hess[step + 1, step]
+    return basis, hess
+
+
+def _krylov_error(H, seed, tau, basis, hess, depth):
+    exact = scipy.linalg.expm(tau * H) @ seed
+    reduced = scipy.linalg.expm(tau * hess[:depth, :depth])[:, 0]
+    return np.linalg.norm(exact - basis[:, :depth] @ reduced)
+
+
+def test_kry_weight_does_not_cancel_on_two_by_two():
+    """|tau| beta int_0^1 |exp(-2 pi i s)| ds = 1 where one direction leaves an O(1) error."""
+    H = np.array([[2 * np.pi, 1], [1, 0]], dtype=np.complex128)
+    seed = np.array([1, 0], dtype=np.complex128)
+    basis, hess = _arnoldi(H, seed, 1)
+    err = _krylov_error(H, seed, -1j, basis, hess, 1)
+    w = K.kry_weight(hess, 1, -1j)
+    assert err > 0.1
+    assert w == pytest.approx(1.0, rel=1e-10)
+    assert w >= err
+
+
+def test_kry_weight_bounds_random_hermitian_errors():
+    rng = np.random.default_rng(11)
+    dim, depth, checked = 30, 16, 0
+    for _ in range(3):
+        for tau in (-0.1j, -1j, -3j):
+            raw = rng.standard_normal((dim, dim)) + 1j * rng.standard_normal((dim, dim))
+            H = (raw + raw.conj().T) / 2
+            seed = rng.standard_normal(dim) + 1j * rng.standard_normal(dim)
+            seed /= np.linalg.norm(seed)
+            basis, hess = _arnoldi(H, seed, depth)
+            for step in range(1, depth):
+                err = _krylov_error(H, seed, tau, basis, hess, step)
+                if err < 1e-13:
+                    break
+                checked += 1
+                assert err <= (1 + 1e-3) * K.kry_weight(hess, step, tau) + 1e-14, (tau, step)
+    assert checked > 30
+
+
+def test_root_tail_is_guarded_over_the_step():
+    """T_2 = [0 pi; pi 0] from e_1 on [0 pi 0; pi 0 1; 0 1 0]: [exp(-i T_2)]_{2,1} = -i sin(pi) = 0,
+    so the endpoint tail vanishes with an O(1) error; the guarded tail samples |sin(pi s)|."""
+    chain = np.array([[0, np.pi, 0], [np.pi, 0, 1], [0, 1, 0]], dtype=np.complex128)
+    tau = -1j
+    vals, vecs = K.tridiag_eigen([0.0, 0.0], [np.pi])
+
+    def evalcoeff(step):
+        return K.coeffs_from_eigen(vals, vecs, complex(step))
+
+    endpoint = K.tail(evalcoeff(tau)[0], 1.0)
+    guarded = K.tail_sup(evalcoeff, complex(tau), 1.0)
+    true_err = np.linalg.norm(scipy.linalg.expm(tau * chain) @ np.array([1, 0, 0])
+                              - np.concatenate([evalcoeff(tau)[0], [0]]))
+    assert true_err > 0.1
+    assert endpoint < 1e-12
+    assert guarded >= 0.9
+    assert abs(tau) * guarded >= true_err
+    for step in (-0.3j, -2.7j):
+        assert K.tail_sup(evalcoeff, step, 1.0) >= K.tail(evalcoeff(step)[0], 1.0)
+    for step in (-0.5 + 0j, -0.5 - 1j):  # imaginary time and loss keep the endpoint value
+        assert K.tail_sup(evalcoeff, step, 1.0) == K.tail(evalcoeff(step)[0], 1.0)
+
+
+def test_tridiag_eigen_exact_and_names_non_finite_input():
+    d = [0.3, -1.2, 2.5, 0.0, 1e-9]
+    e = [1.0, 1e-12, 0.7, 2.0]
+    vals, vecs = K.tridiag_eigen(d, e)
+    T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    assert np.linalg.norm(T @ vecs - vecs @ np.diag(vals)) < 1e-12
+    assert np.linalg.norm(vecs.T @ vecs - np.eye(5)) < 1e-12
+    with pytest.raises(ValueError, match="non-finite"):
+        K.tridiag_eigen([0.0, np.nan], [1.0])
+    with pytest.raises(ValueError, match="non-finite"):
+        K.tridiag_eigen([0.0, 1.0], [np.inf])
