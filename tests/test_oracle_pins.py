@@ -2,7 +2,8 @@
 
 * Test A lists: ``test/BUG/Randomised/test_expansion.jl:15-88``.
 * The two-spin entangling step: ``test_expansion.jl:90-109``.
-* ``expv`` against sector-diagonal closed forms: ``test/BUG/Core/LocalSolvers/test_krylov.jl:21-168``.
+* ``expv`` against sector-diagonal closed forms, its degenerate generators, reorthogonalisation, zero
+  input and the root stability functions: ``test/BUG/Core/LocalSolvers/test_krylov.jl:21-216``.
 * The Krylov stopping weights (``test/BUG/Core/LocalSolvers/test_krylov_weights.jl:44-117``): the
   residual integral on the 2 x 2 where Saad's scalar cancels (weight 1), its bound on random
   Hermitian generators, the root's tail guarded over the step, ``_tridiag_eigen`` exact and naming
@@ -110,6 +111,63 @@ def test_arnoldi_terminates_at_true_krylov_dimension():
     assert rep[0] == 2
     y, rep = K.expv(K.VecOps(), lambda v: _diag(v, scale), tau, x, hermitian=True, maxiter=60)
     assert rep[0] == 60
+
+
+def test_expv_degenerate_generators():
+    """``test_krylov.jl:38-58,175-179``: the identity generator gives exp(tau) x, the zero generator
+    the identity, a Hermitian generator keeps the norm in real time, Arnoldi matches Lanczos on it,
+    and a zero input returns zero on both paths."""
+    x = _multi_sector()
+    ops = K.VecOps()
+    y, _ = K.expv(ops, lambda v: v, -1.0 + 0j, x, hermitian=True)
+    assert B.norm(B.sub(y, B.scale(x, np.exp(-1.0)))) < 1e-12
+    y, _ = K.expv(ops, lambda v: B.scale(v, 0.0), -0.1j, x, hermitian=True)
+    assert B.norm(B.sub(y, x)) < 1e-14
+    y, _ = K.expv(ops, lambda v: B.scale(v, 2.0), -0.3j, x, hermitian=True)
+    assert abs(B.norm(y) - B.norm(x)) < 1e-12
+    yl, _ = K.expv(ops, lambda v: B.scale(v, 2.0), -0.2j, x, hermitian=True)
+    ya, _ = K.expv(ops, lambda v: B.scale(v, 2.0), -0.2j, x, hermitian=False)
+    assert B.norm(B.sub(yl, ya)) < 1e-11
+    z = B.scale(x, 0.0)
+    for herm in (True, False):
+        y, _ = K.expv(ops, lambda v: B.scale(v, 2.0), -0.1j, z, hermitian=herm)
+        assert B.norm(y) < 1e-15
+
+
+def test_lanczos_reorthogonalisation_spans_the_same_space():
+    """``test_krylov.jl:126-131``: full reorthogonalisation changes nothing on a diagonal generator."""
+    x = _multi_sector()
+    scale = lambda q: 0.5 * q + 1.0
+    y0, _ = K.expv(K.VecOps(), lambda v: _diag(v, scale), -0.5j, x, hermitian=True, reorth=False)
+    y1, _ = K.expv(K.VecOps(), lambda v: _diag(v, scale), -0.5j, x, hermitian=True, reorth=True)
+    assert B.norm(B.sub(y0, y1)) < 1e-11
+
+
+def test_inner_is_zero_when_no_blocks_match():
+    """``test_krylov.jl:181-191``: stored sectors disjoint on equal spaces give 0, not an error."""
+    x = _multi_sector()
+    a = B.BT(x.legs, {k: v for k, v in x.blocks.items() if k[2] == -1})
+    b = B.BT(x.legs, {k: v for k, v in x.blocks.items() if k[2] == 1})
+    assert B.inner(a, b) == 0
+    assert B.inner(a, a) != 0
+
+
+def test_root_stability_functions():
+    """``test_krylov.jl:194-216``: A-stability on the negative axis and the imaginary axis, the
+    classical order from the error ratio, L-stability of the Radau roots, the trapezoid's -1 limit,
+    damping of stiff scalars."""
+    zs = list(-(10.0 ** np.linspace(-3, 8, 60))) + [0.0]
+    for m, q in (("trapezoid", 2), ("radau2", 3), ("radau3", 5)):
+        assert all(abs(K.root_stability(m, z)) <= 1 + 1e-14 for z in zs)
+        assert all(abs(K.root_stability(m, 1j * y)) <= 1 + 1e-12 for y in np.arange(-50, 50.5, 0.5))
+        err = lambda z: abs(K.root_stability(m, z) - np.exp(z))
+        assert abs(math.log2(err(-0.1) / err(-0.05)) - (q + 1)) < 0.25
+        for lh in (0.1, 10.0, 1e4):
+            assert abs(K.root_stability(m, -lh)) < 1
+    assert abs(K.root_stability("radau2", -1e8)) < 1e-6
+    assert abs(K.root_stability("radau3", -1e8)) < 1e-6
+    assert abs(K.root_stability("trapezoid", -1e8) + 1) < 1e-6
+    assert K.root_stability("exp", -0.3) == pytest.approx(math.exp(-0.3))
 
 
 FROZEN = dict(work_ceiling_rule="maxdim", expansion=S.DDQRExpansion(krylov_mode="arnoldi"))
