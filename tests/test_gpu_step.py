@@ -276,3 +276,30 @@ def test_implicit_root_methods(dev, method):
              native=True, root_method=method)
     run_pair(dev, 10, 3, "neel_state", 1.0, 2, tau=-0.1, maxdim=32, native=True,
              root_method=method)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_native_step_converges_at_order_p_plus_one(dev, order):
+    """The native step on the interacting L = 10 quench (delta 0.5, domain wall, to t = 1, tight
+    tolerances) against the dense exponential: global order p + 1 in tau, as the oracle's
+    (error ratios 4.0 and 8.0 when tau halves; 4.4e-4 and 3.7e-6 at tau = 0.05)."""
+    import scipy.linalg
+
+    DM, _ = dev
+    from bondupdategalerkin_b200 import native as DN
+
+    L, T = 10, 1.0
+    exact = scipy.linalg.expm(-1j * T * OM.dense_xxz(L, 1.0, 0.5)) @ \
+        OM.mps_to_dense(OM.domain_wall_state(L))
+    errs = []
+    for dt in (0.1, 0.05):
+        psi, mpo = DM.domain_wall_state(L), DM.xxz_mpo(L, J=1.0, delta=0.5)
+        rng = np.random.default_rng(1234)
+        for _ in range(int(round(T / dt))):
+            info = DN.cbe_bug_step(psi, mpo, -1j * dt, order=order, tol_basis=1e-8,
+                                   tol_trunc=1e-12, maxdim=256, rng=rng)
+            assert info["status"] == "met"
+        dense = OM.mps_to_dense(mps_to_host(psi))
+        errs.append(np.linalg.norm(dense - exact) / np.linalg.norm(exact))
+    assert errs[0] / errs[1] > 0.85 * 2 ** (order + 1), errs
+    assert errs[1] < (1e-3 if order == 1 else 1e-5), errs
