@@ -14,6 +14,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _engine as E
+from .options import check_step_options
 from .tensor import DT
 
 MAX_SITES = 1024
@@ -144,22 +145,31 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         closure_checks=int(bool(closure_checks)))
 
 
-def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
-                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
-                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
+def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=None,
+                 tol_krylov=None, order=1, closure_probe=0, maxdim=None, hermitian=True,
+                 expansion=None, rng=None, root=None, reorth=True, truncate=True,
+                 work_ceiling_rule="bond", bond_ceiling_factor=None, root_ceiling_factor=1.2,
                  root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
                  closure_checks=False, eshift=0.0, root_report=None, outside_residual=False,
-                 root_method="exp", root_shift=True):
+                 root_method="exp", root_shift=True, frames_report=None, keep_states=(),
+                 keep_tols=(), frames_only=False, exact=False, parallel=False, kls=None):
     """``cbe_bug_step!(psi, mpo, tau; ...)`` (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on an
     HBM-resident state, in place. Returns the step info (``CBEBugSweepInfo`` fields). The
     generators are ``H - eshift``; a dict passed as ``root_report`` receives the root's energies
     and, with ``outside_residual``, the outside-Galerkin defect after its re-enrichment
-    (``_report_root!``, ``bug_step_stages.jl:243-390``)."""
+    (``_report_root!``, ``bug_step_stages.jl:243-390``). Every keyword of the reference is taken;
+    the options it refuses raise ``ValueError``, the ones not built here ``NotImplementedError``
+    (``options.check_step_options``)."""
+    L = len(psi)
+    tol_expv = check_step_options(
+        L, len(mpo), root=root, parallel=parallel, kls=kls, tol_expv=tol_expv, tol_root=tol_root,
+        order=order, work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
+        root_ceiling_factor=root_ceiling_factor, frontier_tol=frontier_tol,
+        krylov_rank_tol=krylov_rank_tol, closure_probe=closure_probe, keep_states=keep_states,
+        keep_tols=keep_tols, frames_only=frames_only, frames_report=frames_report, exact=exact,
+        root_report=root_report, truncate=truncate, outside_residual=outside_residual)
     if outside_residual and root_report is None:
         raise ValueError("outside_residual needs root_report")
-    L = len(psi)
-    if len(mpo) != L:
-        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
     p = step_params(L, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_expv=tol_expv,
                     tol_krylov=tol_krylov, order=order, maxdim=maxdim, hermitian=hermitian,
                     expansion=expansion, root=root, reorth=reorth, truncate=truncate,

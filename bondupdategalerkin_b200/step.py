@@ -35,6 +35,7 @@ import numpy as np
 
 from . import tensor as B
 from . import krylov as K
+from .options import check_step_options
 from .budget import (ADAPTIVE_GROWTH, DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
                      basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
                      work_ceiling)
@@ -683,22 +684,33 @@ def local_dim(psi):
     return max(psi[s].dim(1) for s in range(1, len(psi) + 1))
 
 
-def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
-                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
-                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
+def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=None,
+                 tol_krylov=None, order=1, closure_probe=0, maxdim=None, hermitian=True,
+                 expansion=None, rng=None, root=None, reorth=True, truncate=True,
+                 work_ceiling_rule="bond", bond_ceiling_factor=None, root_ceiling_factor=1.2,
                  root_maxiter=K.ROOT_MAXITER, krylov_rank_tol=0.0, frontier_tol=0.0,
-                 fold_omega=None, closure_checks=False):
+                 fold_omega=None, closure_checks=False, eshift=0.0, root_report=None,
+                 outside_residual=False, root_method="exp", root_shift=True, frames_report=None,
+                 keep_states=(), keep_tols=(), frames_only=False, exact=False, parallel=False,
+                 kls=None):
     """One rank-adaptive BUG step in place; returns the step info dict
-    (``bug_step.jl:17-513``)."""
+    (``bug_step.jl:17-513``). The reference's keywords are checked as it checks them
+    (``options.check_step_options``). This host leaves the imaginary-time options (``eshift``,
+    ``root_report``, ``outside_residual``), the implicit roots and ``closure_checks`` to the native
+    step (``native.cbe_bug_step``) and says so."""
     tau = complex(tau)
     L = len(psi)
-    if len(mpo) != L:
-        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
-    if L < 2:
-        raise ValueError("cbe_bug_step needs at least two sites")
+    tol_expv = check_step_options(
+        L, len(mpo), root=root, parallel=parallel, kls=kls, tol_expv=tol_expv, tol_root=tol_root,
+        order=order, work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
+        root_ceiling_factor=root_ceiling_factor, frontier_tol=frontier_tol,
+        krylov_rank_tol=krylov_rank_tol, closure_probe=closure_probe, keep_states=keep_states,
+        keep_tols=keep_tols, frames_only=frames_only, frames_report=frames_report, exact=exact,
+        root_report=root_report, truncate=truncate, outside_residual=outside_residual)
+    if eshift != 0.0 or root_report is not None or outside_residual or root_method != "exp":
+        raise NotImplementedError("eshift, root_report, outside_residual and the implicit roots run "
+                                  "in the native step (native.cbe_bug_step)")
     root_link = bug_root_link(L) if root is None else root
-    if not 1 <= root_link <= L - 1:
-        raise ValueError(f"root must be a bond in 1:{L - 1}, got {root_link}")
     budget = Budget(TOL_DEFAULTS["basis"] if tol_basis is None else tol_basis,
                     TOL_DEFAULTS["trunc"] if tol_trunc is None else tol_trunc,
                     TOL_DEFAULTS["expv"] if tol_expv is None else tol_expv)

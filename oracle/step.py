@@ -876,25 +876,97 @@ def report_root(report, psi, mpo, left_frames, right_frames, root_link, lenv_roo
                 renv=state["renv"], rep=state["rep"])
 
 
-def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None,
-                 order=1, maxdim=None, hermitian=True, expansion=None, rng=None, root=None,
-                 reorth=True, truncate=True, work_ceiling_rule="bond", bond_ceiling_factor=None,
+KLS_SCHEDULES = ("sequential", "kl_then_s", "concurrent")  # parallel_kls.jl:7
+
+
+def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, work_ceiling_rule,
+                 bond_ceiling_factor, root_ceiling_factor, frontier_tol, krylov_rank_tol,
+                 closure_probe, keep_states, keep_tols, frames_only, frames_report, exact,
+                 root_report, truncate, outside_residual):
+    """``_step_options`` (``bug_step_stages.jl:40-142``): the reference's refusals (``ValueError``)
+    in its order, then the options this restatement leaves out (``NotImplementedError``). Returns
+    ``(root_link, tol_expv)``."""
+    if mpo_len != L:
+        raise ValueError(f"MPO has {mpo_len} sites, state has {L}")
+    if L < 2:
+        raise ValueError("cbe_bug_step needs at least two sites")
+    root_link = bug_root_link(L) if root is None else root
+    if not 1 <= root_link <= L - 1:
+        raise ValueError(f"root must be a bond in 1:{L - 1}, got {root_link}")
+    if isinstance(parallel, bool):
+        mode, run_parallel = ("half_sweeps" if parallel else "serial"), parallel
+    elif parallel in ("serial", "half_sweeps", "full"):
+        mode, run_parallel = parallel, parallel != "serial"
+    else:
+        raise ValueError(f"parallel must be :serial, :half_sweeps, :full or a Bool, got {parallel!r}")
+    if mode == "full" and kls is None:
+        kls = "concurrent"
+    if tol_root is not None and tol_expv is not None:
+        raise ValueError("tol_root and tol_expv name the same tolerance; pass one")
+    if tol_root is not None:
+        tol_expv = tol_root
+    if order < 1:
+        raise ValueError(f"order must be >= 1, got {order}")
+    if bond_ceiling_factor is None:
+        bond_ceiling_factor = DEFAULT_BOND_CEILING_FACTOR if work_ceiling_rule == "bond" else 0.0
+    if frontier_tol < 0:
+        raise ValueError(f"frontier_tol must be >= 0, got {frontier_tol}")
+    if work_ceiling_rule not in ("maxdim", "bond", "bond_strict", "frame_root"):
+        raise ValueError(f"work_ceiling_rule must be :maxdim, :bond, :bond_strict or :frame_root, "
+                         f"got {work_ceiling_rule!r}")
+    if not (bond_ceiling_factor == 0 or (bond_ceiling_factor > 1 and work_ceiling_rule != "maxdim")):
+        raise ValueError("bond_ceiling_factor must be 0, or > 1 with work_ceiling_rule = bond")
+    if not root_ceiling_factor > 1:
+        raise ValueError("root_ceiling_factor must exceed one")
+    frame_factor = 2.0 if bond_ceiling_factor == 0 else bond_ceiling_factor
+    if work_ceiling_rule == "frame_root" and root_ceiling_factor > frame_factor:
+        raise ValueError("root_ceiling_factor must not exceed frame factor")
+    if closure_probe < 0:
+        raise ValueError(f"closure_probe must be a non-negative count, got {closure_probe}")
+    if len(keep_tols) and len(keep_tols) != len(keep_states):
+        raise ValueError(f"keep_tols has {len(keep_tols)} entries for {len(keep_states)} keep_states")
+    if any(t < 0 for t in keep_tols):
+        raise ValueError(f"keep_tols must be >= 0, got {list(keep_tols)}")
+    if frames_only and (root_report is not None or kls is not None or truncate):
+        raise ValueError("frames_only needs root_report = nothing, kls = nothing and truncate = false")
+    if kls is not None and kls not in KLS_SCHEDULES:
+        raise ValueError(f"the K/L/S schedule must be one of {KLS_SCHEDULES}, got {kls!r}")
+    if kls is not None and outside_residual:
+        raise ValueError("the parallel K/L/S step does not combine with the outside-residual "
+                         "re-enrichment")
+    if run_parallel or kls is not None:
+        raise NotImplementedError("parallel half-sweeps and the K/L/S step are not restated")
+    if work_ceiling_rule not in ("maxdim", "bond"):
+        raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
+    if frontier_tol > 0 or krylov_rank_tol > 0:
+        raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
+    if closure_probe > 0:
+        raise NotImplementedError("closure_probe > 0 is not restated")
+    if len(keep_states) or frames_only or frames_report is not None or exact:
+        raise NotImplementedError("keep_states, frames_only, frames_report and exact are not restated")
+    return root_link, tol_expv
+
+
+def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=None,
+                 tol_krylov=None, order=1, closure_probe=0, maxdim=None, hermitian=True,
+                 expansion=None, rng=None, root=None, reorth=True, truncate=True,
+                 work_ceiling_rule="bond", bond_ceiling_factor=None, root_ceiling_factor=1.2,
                  root_maxiter=K.ROOT_MAXITER, krylov_rank_tol=0.0, frontier_tol=0.0,
                  fold_omega=None, closure_checks=False, eshift=0.0, root_report=None,
-                 outside_residual=False, root_method="exp", root_shift=True):
+                 outside_residual=False, root_method="exp", root_shift=True, frames_report=None,
+                 keep_states=(), keep_tols=(), frames_only=False, exact=False, parallel=False,
+                 kls=None):
     """One rank-adaptive BUG step in place; returns the step info dict
     (``bug_step.jl:17-513``). The generators are ``H - eshift``; with ``root_report`` (a dict) the
     root's energies and, with ``outside_residual``, the outside-Galerkin defect and its
     re-enrichment are filled in (``_report_root!``, ``bug_step_stages.jl:243-390``)."""
     tau = complex(tau)
     L = len(psi)
-    if len(mpo) != L:
-        raise ValueError(f"MPO has {len(mpo)} sites, state has {L}")
-    if L < 2:
-        raise ValueError("cbe_bug_step needs at least two sites")
-    root_link = bug_root_link(L) if root is None else root
-    if not 1 <= root_link <= L - 1:
-        raise ValueError(f"root must be a bond in 1:{L - 1}, got {root_link}")
+    root_link, tol_expv = step_options(
+        L, len(mpo), root, parallel, kls, tol_expv, tol_root, order, work_ceiling_rule,
+        bond_ceiling_factor, root_ceiling_factor, frontier_tol, krylov_rank_tol, closure_probe,
+        keep_states, keep_tols, frames_only, frames_report, exact, root_report, truncate,
+        outside_residual)
     budget = Budget(TOL_DEFAULTS["basis"] if tol_basis is None else tol_basis,
                     TOL_DEFAULTS["trunc"] if tol_trunc is None else tol_trunc,
                     TOL_DEFAULTS["expv"] if tol_expv is None else tol_expv)
@@ -910,12 +982,6 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     if outside_residual and not fold:
         raise NotImplementedError("the outside residual with the exact (unfolded) leak is not restated")
     eshift = float(eshift)
-    if frontier_tol != 0.0 or krylov_rank_tol != 0.0:
-        raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
-    if work_ceiling_rule not in ("maxdim", "bond"):
-        raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
-    if not (bond_ceiling_factor == 0 or (bond_ceiling_factor > 1 and work_ceiling_rule == "bond")):
-        raise ValueError("bond_ceiling_factor must be 0, or > 1 with work_ceiling_rule = bond")
     maxdim = 128 if maxdim is None else maxdim
     bond_ranks = psi.bond_dims()
     if work_ceiling_rule == "bond":
