@@ -357,9 +357,12 @@ class TDVP2Info(ctypes.Structure):
 
 
 def tdvp2_step(psi, mpo, tau, *, maxdim=200, trunc_thresh=1e-12, maxiter=30, tol=1e-15,
-               hermitian=True, conv_tol=0.0, substeps=1, weight_tol=None, eshift=0.0) -> dict:
+               hermitian=True, conv_tol=0.0, substeps=1, weight_tol=None, eshift=0.0,
+               backward_report=None, backward_norms=None) -> dict:
     """``tdvp2_step!(psi, h, tau; ...)`` (``src/Baselines/TDVP/tdvp2.jl:229-297``): one symmetric
-    two-site TDVP step on an HBM-resident state, in place. Returns the ``TDVP2Info`` fields."""
+    two-site TDVP step on an HBM-resident state, in place. Returns the ``TDVP2Info`` fields. The
+    backward-substep amplification reports (``backward_report``, ``backward_norms``) are not
+    built and raise ``NotImplementedError`` when asked for."""
     L = len(psi)
     if L < 2:
         raise ValueError("tdvp2_step needs at least two sites")
@@ -367,6 +370,8 @@ def tdvp2_step(psi, mpo, tau, *, maxdim=200, trunc_thresh=1e-12, maxiter=30, tol
         raise ValueError(f"chain has {len(mpo)} sites, state has {L}")
     if weight_tol is not None and weight_tol < 0:
         raise ValueError(f"weight_tol must be non-negative, got {weight_tol}")
+    if backward_report is not None or backward_norms is not None:
+        raise NotImplementedError("backward_report / backward_norms are not built")
     lib = E.load()
     lib.bug_tdvp2_step.restype = ctypes.c_int
     lib.bug_tdvp2_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),

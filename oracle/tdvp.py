@@ -39,7 +39,8 @@ def _expv(apply, tau, vector, kw):
 
 
 def tdvp2_step(psi, mpo, tau, maxdim=200, trunc_thresh=1e-12, maxiter=30, tol=1e-15,
-               hermitian=True, conv_tol=0.0, substeps=1, weight_tol=None, eshift=0.0):
+               hermitian=True, conv_tol=0.0, substeps=1, weight_tol=None, eshift=0.0,
+               backward_report=None, backward_norms=None):
     """One symmetric two-site TDVP step of ``tau`` in place (``tdvp2_step!``); returns the
     ``TDVP2Info`` fields as a dict."""
     L = len(psi)
@@ -49,6 +50,8 @@ def tdvp2_step(psi, mpo, tau, maxdim=200, trunc_thresh=1e-12, maxiter=30, tol=1e
         raise ValueError(f"chain has {len(mpo)} sites, state has {L}")
     if weight_tol is not None and weight_tol < 0:
         raise ValueError("weight_tol must be non-negative")
+    if backward_report is not None or backward_norms is not None:
+        raise NotImplementedError("backward_report / backward_norms are not restated")
     tau = complex(tau)
     half = tau / 2
     eshift = float(eshift)

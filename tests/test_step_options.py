@@ -106,3 +106,19 @@ def test_root_ceiling_factor_alone_is_accepted():
     from bondupdategalerkin_b200.options import check_step_options
 
     assert check_step_options(L, L, root_ceiling_factor=1.5) is None
+
+
+def test_tdvp2_keywords_checked_as_the_reference_does():
+    """``tdvp2_step!`` (``tdvp2.jl:182-228``): two sites at least, matching chain lengths, a
+    non-negative ``weight_tol``; the backward amplification reports are named as not built."""
+    from bondupdategalerkin_b200 import native as N
+    from oracle import tdvp as T
+
+    for step in (T.tdvp2_step, N.tdvp2_step):
+        psi = M.domain_wall_state(L)
+        with pytest.raises(ValueError):
+            step(psi, M.xxz_mpo(L - 1), -0.05j)
+        with pytest.raises(ValueError):
+            step(psi, M.xxz_mpo(L), -0.05j, weight_tol=-1.0)
+        with pytest.raises(NotImplementedError):
+            step(psi, M.xxz_mpo(L), -0.05j, backward_norms=[])
