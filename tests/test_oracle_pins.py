@@ -498,3 +498,139 @@ def test_step_converges_at_order_p_plus_one(order):
         errs.append(np.linalg.norm(M.mps_to_dense(psi) - exact) / np.linalg.norm(exact))
     assert errs[0] / errs[1] > 0.85 * 2 ** (order + 1), errs
     assert errs[1] < (1e-3 if order == 1 else 1e-5), errs
+
+
+# ── per-bond work ceilings (test/BUG/Core/RankAdaptation/test_bond_work_ceiling.jl) ─────────
+
+
+def test_bond_work_ceilings_known_answers():
+    """``test_bond_work_ceiling.jl:23-30``, in the oracle and in the product's host bookkeeping."""
+    from bondupdategalerkin_b200 import budget as PB
+    from oracle import budget as OB
+
+    for bwc in (OB.bond_work_ceilings, PB.bond_work_ceilings):
+        assert bwc([1, 3, 8], 2, 1024) == [4, 12, 32]
+        assert bwc([0, 5], 4, 1024) == [1, 40]  # never 0, which admits nothing
+        assert bwc([1, 3, 8, 40], 2, 16) == [4, 12, 16, 16]
+        assert bwc([1, 5, 10, 65], 2, 1024, factor=1.2) == [3, 12, 24, 156]
+        assert bwc([1, 5, 10], 3, 1024, factor=1.2) == [4, 18, 36]
+        assert bwc([1, 5, 10], 4, 1024, factor=1.2) == [5, 24, 48]
+        assert bwc([0, 65], 2, 70, factor=1.2) == [1, 70]
+
+
+def test_work_ceilings_bound_every_frame():
+    """``test_bond_work_ceiling.jl:36-119`` on the Heisenberg chain L = 8 (U(1), tau = -0.2i): from
+    the Neel state and from an entangled start, orders 2 and 3, every frame width and every bond
+    stays within its ceiling under the default (1.2), the older 2 d D_b rule and a binding maxdim;
+    the explicit default is the default bit for bit. (The reference runs these with the exact DD
+    probe, which is not built; the bounds hold for the randomised probe the same way.)"""
+    from oracle.budget import bond_work_ceilings
+
+    L, d = 8, 2
+    mpo = M.xxz_mpo(L, J=1.0, delta=1.0)
+    settings = dict(tol_basis=1e-8, tol_expv=1e-12, tol_trunc=1e-12, maxdim=64)
+
+    def step(state, **kw):
+        return S.cbe_bug_step(state, mpo, -0.2j, rng=np.random.default_rng(7), **settings, **kw)
+
+    for factor, kw in ((1.2, {}), (0.0, dict(work_ceiling_rule="bond", bond_ceiling_factor=0.0))):
+        psi = M.neel_state(L)
+        start = psi.bond_dims()
+        assert all(b == 1 for b in start)
+        info = step(psi, order=2, **kw)
+        ceil = bond_work_ceilings(start, d, 64, factor=factor)
+        assert all(e <= c for e, c in zip(info["expanded"], ceil))
+        assert all(b <= c for b, c in zip(psi.bond_dims(), ceil))
+
+    start_state = M.neel_state(L)
+    for _ in range(2):
+        step(start_state, order=2)
+    start = start_state.bond_dims()
+    twice = dict(work_ceiling_rule="bond", bond_ceiling_factor=0.0)
+    ceil2 = bond_work_ceilings(start, d, 64)
+    tight = bond_work_ceilings(start, d, 64, factor=1.2)
+    assert all(t < c for t, c in zip(tight, ceil2))
+    for order in (2, 3):
+        a, b = start_state.copy(), start_state.copy()
+        step(a, order=order)
+        step(b, order=order, work_ceiling_rule="bond", bond_ceiling_factor=1.2)
+        assert np.array_equal(M.mps_to_dense(a), M.mps_to_dense(b))
+        for kw, ceil in ((twice, ceil2), (dict(work_ceiling_rule="bond", bond_ceiling_factor=1.2),
+                                          tight)):
+            s = start_state.copy()
+            info = step(s, order=order, **kw)
+            assert all(e <= c for e, c in zip(info["expanded"], ceil)), (order, kw)
+            assert all(x <= c for x, c in zip(s.bond_dims(), ceil)), (order, kw)
+    small = max(max(start), 2)
+    capped = bond_work_ceilings(start, d, small)
+    assert any(c < x for c, x in zip(capped, ceil2))
+    s = start_state.copy()
+    info = S.cbe_bug_step(s, mpo, -0.2j, rng=np.random.default_rng(7), order=2,
+                          **dict(settings, maxdim=small), **twice)
+    assert all(e <= c for e, c in zip(info["expanded"], capped))
+    assert all(x <= small for x in s.bond_dims())
+
+
+# ── the tolerance budget (test/BUG/Core/RankAdaptation/test_basis_budget.jl) ─────────────────
+
+
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_basis_budget_known_answers(which):
+    """``test_basis_budget.jl:21-97``: the budget's validation, the RSS allocation rule, tau = 0 as
+    a basis question, the indicator's one scaling, the work ceiling and the conservative ledger
+    merge, in the oracle and in the product's host bookkeeping."""
+    if which == "oracle":
+        from oracle import budget as BB
+    else:
+        from bondupdategalerkin_b200 import budget as BB
+    b = BB.Budget(1e-5, 1e-7, 1e-10)
+    assert (b.basis, b.trunc, b.expv) == (1e-5, 1e-7, 1e-10)
+    for bad in ((0.0, 1e-7, 1e-10), (-1e-5, 1e-7, 1e-10), (1e-5, 1e-7, 0.0), (1e-5, -1e-7, 1e-10)):
+        with pytest.raises(ValueError):
+            BB.Budget(*bad)
+    assert BB.Budget(1e-5, 0.0, 1e-10).trunc == 0.0  # "discard nothing" is meaningful
+
+    bb = BB.Budget(1e-4, 1e-7, 1e-10)
+    a = BB.basis_allocation(bb, 19, tau=0.05, nrm=1.0)
+    assert a.per_bond == pytest.approx(1e-4 / math.sqrt(19))
+    for share in (a.sample, a.tail, a.krylov):
+        assert share == pytest.approx(a.per_bond / 2)
+    assert a.scale == pytest.approx(0.05)
+    assert BB.basis_allocation(bb, 76, tau=0.05, nrm=1.0).per_bond == pytest.approx(a.per_bond / 2)
+    assert BB.basis_allocation(bb, 19, tau=0.05, nrm=2.0).scale == pytest.approx(0.025)
+
+    a0 = BB.basis_allocation(BB.Budget(1e-5, 1e-7, 1e-10), 11, tau=0, nrm=1.0)
+    assert a0.scale == 1.0 and BB.indicator(a0, 0.25) == 0.25
+    a1 = BB.basis_allocation(BB.Budget(1e-5, 1e-7, 1e-10), 9, tau=0.1, nrm=4.0)
+    assert a1.scale == pytest.approx(0.025) and BB.indicator(a1, 8.0) == pytest.approx(0.2)
+
+    assert BB.work_ceiling(128, 10) == 256
+    assert BB.work_ceiling(128, 200) == 400  # r > maxdim: the floor governs
+    assert BB.work_ceiling(0, 0) == 1  # never zero
+    assert BB.work_ceiling(128, 10, 4) == 512
+    assert BB.work_ceiling(128, 200, 4) == 800
+
+    x, y = BB.Ledger(), BB.Ledger()
+    assert x.tolerance_met and not x.workcap_reached
+    x.max_sample, x.n_probes = 1e-6, 12
+    y.max_sample, y.n_probes = 3e-6, 7
+    y.workcap_reached, y.tolerance_met = True, False
+    x.merge(y)
+    assert x.max_sample == 3e-6 and x.n_probes == 19
+    assert x.workcap_reached and not x.tolerance_met
+
+
+def test_retired_knobs_are_refused_before_the_state_is_touched():
+    """``test_basis_budget.jl:8-19``: a retired fixed-width knob is no keyword of the step (the
+    reference's MethodError is a TypeError here), refused before any evolution, in the oracle
+    and both product hosts."""
+    from bondupdategalerkin_b200 import native as N
+    from bondupdategalerkin_b200 import step as P
+
+    for step in (S.cbe_bug_step, N.cbe_bug_step, P.cbe_bug_step):
+        psi, mpo = M.neel_state(6), M.xxz_mpo(6, J=1.0, delta=0.0)
+        dims0 = psi.bond_dims()
+        for kw in (dict(tol_basis=1e-5, dex=4), dict(trunc_thresh=1e-10)):
+            with pytest.raises(TypeError):
+                step(psi, mpo, -0.05j, **kw)
+        assert psi.bond_dims() == dims0
