@@ -14,7 +14,7 @@ from types import SimpleNamespace
 import numpy as np
 
 from . import _engine as E
-from .options import check_step_options
+from .options import check_step_options, resolve_krylov_recurrence
 from .tensor import DT
 
 MAX_SITES = 1024
@@ -129,6 +129,7 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         raise ValueError("acceptance_factor must lie in (0,1]")
     if holdout < 1:
         raise ValueError("holdout_width must be positive")
+    resolve_krylov_recurrence(kmode, hermitian)  # refuses an unknown recurrence by name
     if mode not in ("rank_tail", "adaptive"):
         raise NotImplementedError(f"DD mode {mode!r}: :rank_tail and :adaptive are built")
     return StepParams(

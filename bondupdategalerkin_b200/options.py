@@ -101,3 +101,16 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
     if unbuilt:
         raise NotImplementedError("not built: " + "; ".join(unbuilt))
     return tol_expv
+
+
+KRYLOV_MODES = ("auto", "lanczos", "arnoldi")
+
+
+def resolve_krylov_recurrence(mode, hermitian):
+    """``resolve_krylov_recurrence`` (``src/BUG/Randomised/cbe.jl:299``): ``auto`` is Lanczos on a
+    Hermitian step and Arnoldi otherwise, an explicit recurrence is kept, another name is refused."""
+    if mode not in KRYLOV_MODES:
+        raise ValueError(f"krylov_mode must be :auto, :lanczos or :arnoldi, got {mode!r}")
+    if mode == "auto":
+        return "lanczos" if hermitian else "arnoldi"
+    return mode

@@ -35,7 +35,7 @@ import numpy as np
 
 from . import tensor as B
 from . import krylov as K
-from .options import check_step_options
+from .options import check_step_options, resolve_krylov_recurrence
 from .budget import (ADAPTIVE_GROWTH, DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
                      basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
                      work_ceiling)
@@ -736,9 +736,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     else:
         wcap = work_ceiling(maxdim, max(bond_ranks, default=0), local_dim(psi))
     expansion = DDQRExpansion() if expansion is None else expansion
-    recurrence = expansion.krylov_mode
-    if recurrence == "auto":
-        recurrence = "lanczos" if hermitian else "arnoldi"
+    recurrence = resolve_krylov_recurrence(expansion.krylov_mode, hermitian)
     if rng is None:
         rng = np.random.default_rng(0x5EED)
 

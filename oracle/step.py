@@ -990,6 +990,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         wcap = work_ceiling(maxdim, max(bond_ranks, default=0), local_dim(psi))
     expansion = DDQRExpansion() if expansion is None else expansion
     recurrence = expansion.krylov_mode
+    if recurrence not in ("auto", "lanczos", "arnoldi"):  # resolve_krylov_recurrence refuses it
+        raise ValueError(f"krylov_mode must be :auto, :lanczos or :arnoldi, got {recurrence!r}")
     if recurrence == "auto":
         recurrence = "lanczos" if hermitian else "arnoldi"
     if rng is None:

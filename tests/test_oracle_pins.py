@@ -375,6 +375,15 @@ def test_radau2_gmres_is_radau2(tau):
 # ── the Krylov stopping weights (test_krylov_weights.jl) ─────────────────────────────────────
 
 
+def _krylov_module(which):
+    """The oracle's Krylov routines, or the product's (the Python host's) under the same names."""
+    if which == "product":
+        from bondupdategalerkin_b200 import krylov
+    else:
+        from oracle import krylov
+    return krylov
+
+
 def _arnoldi(H, seed, depth):
     """Plain Arnoldi with two Gram-Schmidt passes, the test's own recurrence (not the oracle's)."""
     basis = np.zeros((len(seed), depth + 1), dtype=np.complex128)
@@ -397,8 +406,10 @@ def _krylov_error(H, seed, tau, basis, hess, depth):
     return np.linalg.norm(exact - basis[:, :depth] @ reduced)
 
 
-def test_kry_weight_does_not_cancel_on_two_by_two():
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_kry_weight_does_not_cancel_on_two_by_two(which):
     """|tau| beta int_0^1 |exp(-2 pi i s)| ds = 1 where one direction leaves an O(1) error."""
+    K = _krylov_module(which)
     H = np.array([[2 * np.pi, 1], [1, 0]], dtype=np.complex128)
     seed = np.array([1, 0], dtype=np.complex128)
     basis, hess = _arnoldi(H, seed, 1)
@@ -409,7 +420,9 @@ def test_kry_weight_does_not_cancel_on_two_by_two():
     assert w >= err
 
 
-def test_kry_weight_bounds_random_hermitian_errors():
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_kry_weight_bounds_random_hermitian_errors(which):
+    K = _krylov_module(which)
     rng = np.random.default_rng(11)
     dim, depth, checked = 30, 16, 0
     for _ in range(3):
@@ -428,9 +441,11 @@ def test_kry_weight_bounds_random_hermitian_errors():
     assert checked > 30
 
 
-def test_root_tail_is_guarded_over_the_step():
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_root_tail_is_guarded_over_the_step(which):
     """T_2 = [0 pi; pi 0] from e_1 on [0 pi 0; pi 0 1; 0 1 0]: [exp(-i T_2)]_{2,1} = -i sin(pi) = 0,
     so the endpoint tail vanishes with an O(1) error; the guarded tail samples |sin(pi s)|."""
+    K = _krylov_module(which)
     chain = np.array([[0, np.pi, 0], [np.pi, 0, 1], [0, 1, 0]], dtype=np.complex128)
     tau = -1j
     vals, vecs = K.tridiag_eigen([0.0, 0.0], [np.pi])
@@ -452,7 +467,9 @@ def test_root_tail_is_guarded_over_the_step():
         assert K.tail_sup(evalcoeff, step, 1.0) == K.tail(evalcoeff(step)[0], 1.0)
 
 
-def test_tridiag_eigen_exact_and_names_non_finite_input():
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_tridiag_eigen_exact_and_names_non_finite_input(which):
+    K = _krylov_module(which)
     d = [0.3, -1.2, 2.5, 0.0, 1e-9]
     e = [1.0, 1e-12, 0.7, 2.0]
     vals, vecs = K.tridiag_eigen(d, e)
@@ -634,3 +651,122 @@ def test_retired_knobs_are_refused_before_the_state_is_touched():
             with pytest.raises(TypeError):
                 step(psi, mpo, -0.05j, **kw)
         assert psi.bond_dims() == dims0
+
+
+# ── the XX defaults and the local Krylov recurrence (test_krylov_defaults.jl,
+#    test_local_lanczos.jl) ───────────────────────────────────────────────────────────────────
+
+
+def test_expansion_defaults_and_recurrence_resolution():
+    """``test_krylov_defaults.jl:21-48``: the DDQRExpansion defaults (oracle and product), the
+    recurrence ``auto`` resolves to, an unknown recurrence refused, and the shared stop rule."""
+    from bondupdategalerkin_b200 import krylov as PK
+    from bondupdategalerkin_b200 import step as P
+    from bondupdategalerkin_b200.options import resolve_krylov_recurrence
+
+    for cls in (S.DDQRExpansion, P.DDQRExpansion):
+        e = cls()
+        assert (e.mode, e.fixed_width, e.tail_factor, e.krylov_mode, e.krylov_fixed_depth) == \
+            ("rank_tail", 8, 0.10, "auto", 0)
+    assert resolve_krylov_recurrence("auto", True) == "lanczos"
+    assert resolve_krylov_recurrence("auto", False) == "arnoldi"
+    assert resolve_krylov_recurrence("arnoldi", True) == "arnoldi"
+    with pytest.raises(ValueError):
+        resolve_krylov_recurrence("gmres", True)
+    psi, mpo = M.domain_wall_state(6), M.xxz_mpo(6, J=1.0, delta=0.0)
+    with pytest.raises(ValueError):
+        S.cbe_bug_step(psi, mpo, -0.1j, expansion=S.DDQRExpansion(krylov_mode="gmres"))
+    for stop in (K.krylov_stop, PK.krylov_stop):
+        assert stop(1e-3, 1e-2, 1, 0) == (True, True)     # adaptive: within the allowance
+        assert stop(1e-1, 1e-2, 1, 0) == (False, False)   # adaptive: go on
+        assert stop(1e-3, 1e-2, 2, 4) == (False, False)   # fixed depth not reached yet
+        assert stop(1e-3, 1e-2, 4, 4) == (True, True)
+        assert stop(1e-1, 1e-2, 4, 4) == (True, False)    # never claims a missed tolerance
+
+
+def test_defaults_reach_the_step():
+    """``test_krylov_defaults.jl:50-90``: on an entangled XX start (L = 8, U(1)), the default step
+    is bit for bit the explicit-Lanczos step, with ``hermitian = false`` the explicit-Arnoldi step,
+    and every frame and bond stays within ``min(ceil(1.2 d D_b), maxdim)``."""
+    from oracle.budget import bond_work_ceilings
+
+    mpo = M.xxz_mpo(8, J=1.0, delta=0.0)
+    start = M.domain_wall_state(8)
+    for _ in range(3):
+        S.cbe_bug_step(start, mpo, -0.1j, order=2)
+
+    def one(**kw):
+        s = start.copy()
+        info = S.cbe_bug_step(s, mpo, -0.1j, order=2, tol_basis=1e-4,
+                              rng=np.random.default_rng(7), **kw)
+        return s, info
+
+    d, info = one()
+    lz, _ = one(expansion=S.DDQRExpansion(krylov_mode="lanczos"))
+    assert np.array_equal(M.mps_to_dense(d), M.mps_to_dense(lz))
+    nh, _ = one(hermitian=False)
+    ar, _ = one(hermitian=False, expansion=S.DDQRExpansion(krylov_mode="arnoldi"))
+    assert np.array_equal(M.mps_to_dense(nh), M.mps_to_dense(ar))
+    ceil = bond_work_ceilings(start.bond_dims(), 2, 128, factor=1.2)
+    assert all(e <= c for e, c in zip(info["expanded"], ceil))
+    assert all(b <= c for b, c in zip(d.bond_dims(), ceil))
+
+
+class _ArrayOps:
+    """The chains' vector operations on plain arrays (the reference test's vectors)."""
+
+    @staticmethod
+    def inner(a, b):
+        return complex(np.vdot(a, b))
+
+    @staticmethod
+    def norm(a):
+        return float(np.linalg.norm(a))
+
+    @staticmethod
+    def lin(terms):
+        return sum(c * v for c, v in terms)
+
+    @staticmethod
+    def inner_many(vs, x):
+        return [complex(np.vdot(v, x)) for v in vs]
+
+
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_local_lanczos_and_arnoldi_chains(which):
+    """``test_local_lanczos.jl``: on random Hermitian generators (n = 24, 40; |tau| = 0.1, 1, 4)
+    both chains close, their bases capture exp(tau H) seed to 2e-7, the Lanczos basis is
+    orthonormal to 1e-7 and its depth within 4 of Arnoldi's; a fixed depth that misses the
+    tolerance reports itself capped, not closed. The product's chains (the Python host's) run on
+    the same plain vectors."""
+    if which == "product":
+        from bondupdategalerkin_b200 import krylov as K  # noqa: N811
+    else:
+        from oracle import krylov as K  # noqa: N811
+    rng = np.random.default_rng(45912)
+    ops = _ArrayOps()
+    for n in (24, 40):
+        for t in (0.1, 1.0, 4.0):
+            A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+            H = (A + A.conj().T) / 2
+            seed = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+            seed /= np.linalg.norm(seed)
+            tau = -1j * t
+            score = lambda *_: True
+            ar = K.arnoldi_chain(ops, seed, lambda x: H @ x, tau, 1e-9, score, maxdepth=n)
+            la = K.lanczos_chain(ops, seed, lambda x: H @ x, tau, 1e-9, score, maxdepth=n)
+            ref = scipy.linalg.expm(tau * H) @ seed
+            QA, QL = np.column_stack(ar["basis"]), np.column_stack(la["basis"])
+            assert ar["closed"] and la["closed"]
+            assert np.linalg.norm(ref - QA @ (QA.conj().T @ ref)) <= 2e-7
+            assert np.linalg.norm(ref - QL @ (QL.conj().T @ ref)) <= 2e-7
+            assert abs(la["n_h1"] - ar["n_h1"]) <= 4
+            assert all(np.isfinite(la["weights"]))
+            assert np.linalg.norm(QL.conj().T @ QL - np.eye(QL.shape[1])) <= 1e-7
+    n = 20
+    H = np.diag(np.ones(n - 1), 1) + np.diag(np.ones(n - 1), -1)
+    seed = np.zeros(n, dtype=np.complex128)
+    seed[0] = 1
+    r = K.lanczos_chain(ops, seed, lambda x: H @ x, -2j, 1e-12, lambda *_: True, maxdepth=n,
+                        fixed_depth=4)
+    assert r["n_h1"] == 4 and r["capped"] and not r["closed"]
