@@ -770,3 +770,41 @@ def test_local_lanczos_and_arnoldi_chains(which):
     r = K.lanczos_chain(ops, seed, lambda x: H @ x, -2j, 1e-12, lambda *_: True, maxdepth=n,
                         fixed_depth=4)
     assert r["n_h1"] == 4 and r["capped"] and not r["closed"]
+
+
+# ── bond frames and the discarded-space projection (test_frames.jl, test_sectors.jl) ────────
+
+
+def _frame_checks(psi, bond):
+    from oracle.cbe import frame_theta, perp_left
+
+    S.canonical(psi, bond)
+    f = S.frame_from(psi[bond], psi[bond + 1])
+    gl = B.contract(f.U0, (0, 1), f.U0, (0, 1), conja=True)
+    gr = B.contract(f.V0, (1, 2), f.V0, (1, 2), conjb=True)
+    assert np.allclose(B.to_dense(gl), np.eye(f.U0.dim(2)), atol=1e-12)  # left isometry
+    assert np.allclose(B.to_dense(gr), np.eye(f.V0.dim(0)), atol=1e-12)  # right isometry
+    two_site = B.contract(psi[bond], (2,), psi[bond + 1], (0,))
+    assert B.norm(B.sub(frame_theta(f), two_site)) < 1e-12
+    assert f.old_rank == psi[bond].dim(2)
+    nrm = B.norm(psi[psi.center])
+    assert abs(B.norm(f.S0) - nrm) < 1e-12 and abs(B.norm(frame_theta(f)) - nrm) < 1e-12
+    # a vector inside U0's range has no component outside it
+    K1 = B.contract(f.U0, (2,), f.S0, (0,))
+    assert B.norm(perp_left(f.U0, K1)) < 1e-12
+    return f
+
+
+def test_bond_frames_are_exact_canonical_snapshots():
+    """``test_frames.jl:8-99`` and ``test_sectors.jl:61-69``: U0 a left and V0 a right isometry,
+    U0 S0 V0 the two-site block exactly, the old rank the link dimension, the snapshot
+    norm-preserving, and perp(U0, K) = 0 for K in U0's range; on a product state and on every
+    interior bond of an entangled state whose bonds carry several charge sectors."""
+    _frame_checks(M.domain_wall_state(6), 2)
+    psi = M.domain_wall_state(6)
+    mpo = M.xxz_mpo(6, J=1.0, delta=0.5)
+    for _ in range(2):
+        S.cbe_bug_step(psi, mpo, -0.3j, order=2, rng=np.random.default_rng(5))
+    assert max(len(psi[i].legs[2].sectors) for i in range(1, 6)) > 1  # multi-sector bonds
+    for bond in range(1, 6):
+        _frame_checks(psi, bond)
