@@ -808,3 +808,64 @@ def test_bond_frames_are_exact_canonical_snapshots():
     assert max(len(psi[i].legs[2].sectors) for i in range(1, 6)) > 1  # multi-sector bonds
     for bond in range(1, 6):
         _frame_checks(psi, bond)
+
+
+# ── the symmetric MPS and its canonical moves (test_symmetric_mps.jl,
+#    test_state_conformance.jl) ───────────────────────────────────────────────────────────────
+
+
+def _inner(a, b):
+    """<a|b> of two oracle MPS by transfer contraction (charges that do not meet give no block)."""
+    E = None
+    for i in range(1, len(a) + 1):
+        if E is None:
+            E = B.contract(a[i], (0, 1), b[i], (0, 1), conja=True)
+        else:
+            t = B.contract(E, (0,), a[i], (0,), conjb=True)
+            E = B.contract(t, (0, 1), b[i], (0, 1))
+    return complex(sum(np.sum(v) for v in E.blocks.values()))
+
+
+def test_symmetric_mps_layout_and_canonical_moves():
+    """``test_symmetric_mps.jl:9-70``: the domain wall is a normalised product state with the
+    documented leg layout (link, site of dimension 2, link; opposite arrows across every bond);
+    canonical moves keep the norm and the arrows, move the centre, and leave left isometries
+    left of the centre and right isometries right of it."""
+    psi = M.domain_wall_state(6)
+    assert len(psi) == 6 and abs(abs(_inner(psi, psi)) - 1.0) < 1e-14
+    assert all(b == 1 for b in psi.bond_dims())
+    for i in range(1, 7):
+        assert len(psi[i].legs) == 3 and psi[i].dim(1) == 2
+    for i in range(1, 6):
+        assert psi[i].legs[2].dir != psi[i + 1].legs[0].dir
+    n0 = abs(_inner(psi, psi))
+    for centre in (3, 6):
+        S.canonical(psi, centre)
+        assert psi.center == centre and abs(abs(_inner(psi, psi)) - n0) < 1e-13
+    psi = M.neel_state(6)
+    S.canonical(psi, 2)
+    for i in range(1, 6):
+        assert psi[i].legs[2].dir != psi[i + 1].legs[0].dir
+    # an entangled state, so the isometries are not trivially product tensors
+    mpo = M.xxz_mpo(6, J=1.0, delta=0.5)
+    S.cbe_bug_step(psi, mpo, -0.3j, order=2, rng=np.random.default_rng(2))
+    S.canonical(psi, 4)
+    for i in range(1, 4):
+        g = B.contract(psi[i], (0, 1), psi[i], (0, 1), conja=True)
+        assert np.allclose(B.to_dense(g), np.eye(psi[i].dim(2)), atol=1e-12)
+    for i in range(5, 7):
+        g = B.contract(psi[i], (1, 2), psi[i], (1, 2), conjb=True)
+        assert np.allclose(B.to_dense(g), np.eye(psi[i].dim(0)), atol=1e-12)
+
+
+def test_inner_products_against_dense_and_across_charges():
+    """``test_state_conformance.jl:81-94``: <a|b> matches the dense vectors' product and is
+    Hermitian; states of different total S^z give an exact zero."""
+    a = M.neel_state(6)
+    b2 = M.neel_state(6)
+    S.cbe_bug_step(b2, M.xxz_mpo(6, J=1.0, delta=0.5), -0.4j, order=2, rng=np.random.default_rng(4))
+    ab = _inner(a, b2)
+    assert abs(ab - np.vdot(M.mps_to_dense(a), M.mps_to_dense(b2))) < 1e-12
+    assert abs(_inner(b2, a) - np.conj(ab)) < 1e-12
+    c = M.product_state(["up", "up", "up", "up", "down", "down"])
+    assert _inner(a, c) == 0
