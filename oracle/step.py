@@ -27,16 +27,16 @@ from __future__ import annotations
 
 import math
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
 from . import blocks as B
 from . import krylov as K
-from .budget import (ADAPTIVE_GROWTH, DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
+from .budget import (DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
                      basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
                      work_ceiling)
-from .cbe import (CBE_EPS, BondFrame, cap_to_local_room, dd_cbe_expand, folded_closures, perp_left,
+from .cbe import (BondFrame, cap_to_local_room, dd_cbe_expand, folded_closures, perp_left,
                   perp_right, rank_cut, reortho, rows_from_u, sampled_leak)
 from .env import (ZeroSiteH, apply_one_site, left_boundary, left_env_stack, left_step,
                   right_boundary, right_env_stack, right_step, total_charge)
