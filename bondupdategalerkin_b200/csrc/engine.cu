@@ -1409,7 +1409,7 @@ int bug_tensor_download(bug_ctx* c, const bug_tensor* t, double* host, int64_t n
   });
 }
 
-int bug_tensor_free(bug_ctx* c, bug_tensor* t) {
+int bug_tensor_free(bug_ctx* /*ctx: the ABI names the owner; the handle frees itself*/, bug_tensor* t) {
   return guard([&] { delete t; });
 }
 

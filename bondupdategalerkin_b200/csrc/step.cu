@@ -1496,7 +1496,7 @@ struct Step {
   T project_root(const MPS& psi, KL& fr) {
     return e.contract(overlap_left(psi, fr.lf), {1}, overlap_right(psi, fr.rf), {0});
   }
-  MPS frontier_mps(const MPS& psi, KL& fr, const T& core) {
+  MPS frontier_mps(const MPS& /*psi*/, KL& fr, const T& core) {
     MPS m;
     for (int s = 1; s < root_link; ++s) m.s.push_back(fr.lf[s]);
     m.s.push_back(e.contract(fr.lf[root_link], {2}, core, {0}));
