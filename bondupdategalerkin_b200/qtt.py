@@ -47,13 +47,21 @@ class Grid:
         return self.nx + self.ny
 
 
-def qtt_grid(nx, ny, x=(-1.0, 1.0), y=(-1.0, 1.0), periodic_x=True, periodic_y=True) -> Grid:
+def qtt_grid(nx, ny, x=(-1.0, 1.0), y=(-1.0, 1.0), periodic_x=True, periodic_y=True,
+             order="grouped", endian="lsb_first") -> Grid:
     """The grid on ``x[0] <= x < x[1]`` (periodic) or ``x[0] <= x <= x[1]`` (end points on the
     grid), likewise in y."""
     if nx < 1 or ny < 1:
         raise ValueError("qtt_grid needs at least one bit per coordinate")
     if not (x[1] > x[0] and y[1] > y[0]):
         raise ValueError(f"empty domain {x} x {y}")
+    if order not in ("grouped", "interleaved"):  # QTTOrdering, grid.jl:43-46
+        raise ValueError(f"order must be :grouped or :interleaved, got :{order}")
+    if endian not in ("lsb_first", "msb_first"):
+        raise ValueError(f"endian must be :lsb_first or :msb_first, got :{endian}")
+    if (order, endian) != ("grouped", "lsb_first"):
+        raise NotImplementedError("only the default ordering (grouped, least significant bit first) "
+                                  "is built; the others are the reference's diagnostics")
     dx = (x[1] - x[0]) / (2 ** nx if periodic_x else 2 ** nx - 1)
     dy = (y[1] - y[0]) / (2 ** ny if periodic_y else 2 ** ny - 1)
     return Grid(nx, ny, float(x[0]), dx, float(y[0]), dy, periodic_x, periodic_y)

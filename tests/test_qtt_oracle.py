@@ -190,3 +190,26 @@ def test_heston_backward_bug_steps_reach_the_fixture():
     assert statuses[3:] == ["met"] * (d["steps"] - 3)
     assert relerr(Q.qtt_dense(psi), ref) < 1e-4
     assert abs(max(psi.bond_dims()) - d["trajectory"][-1]["chi"]) <= 2
+
+
+def test_grid_orderings_checked_as_the_reference_does():
+    """``qtt_grid`` / ``QTTOrdering`` (``grid.jl:35-46,152-168``): at least one bit per coordinate,
+    a non-empty domain, ``order`` grouped or interleaved and ``endian`` lsb_first or msb_first
+    (refused otherwise); only the default ordering is built, the others are named."""
+    import pytest
+
+    from bondupdategalerkin_b200 import qtt as P
+
+    for grid in (Q.qtt_grid, P.qtt_grid):
+        with pytest.raises(ValueError):
+            grid(0, 3)
+        with pytest.raises(ValueError):
+            grid(3, 3, x=(1.0, 1.0))
+        with pytest.raises(ValueError):
+            grid(3, 3, order="spiral")
+        with pytest.raises(ValueError):
+            grid(3, 3, endian="middle")
+        for kw in (dict(order="interleaved"), dict(endian="msb_first")):
+            with pytest.raises(NotImplementedError):
+                grid(3, 3, **kw)
+        assert grid(3, 3, order="grouped", endian="lsb_first").nx == 3
