@@ -12,7 +12,10 @@
 * ``tdvp2_step(psi, mpo, tau; ...)`` -- the two-site TDVP baseline (``src/Baselines/TDVP/tdvp2.jl``),
   ``tdvp2_step_host`` its host-buffer form;
 * ``ite_step`` / ``ite_evolve`` and the step schedules -- normalised imaginary time
-  (``src/BUG/ITE/ite_step.jl``, ``schedules.jl``).
+  (``src/BUG/ITE/ite_step.jl``, ``schedules.jl``);
+* the quantics builders under the reference's names: ``qtt_grid``, ``qtt_separable``, ``qtt_mps``,
+  ``qtt_shift``, ``qtt_derivative``, ``qtt_to_mpo``, ``HestonParams``, ``heston_op``,
+  ``heston_mpo`` (``src/QTTS/Tooling``, ``src/QTTS/Models/Heston``).
 """
 
 from __future__ import annotations
@@ -21,6 +24,8 @@ from .models import MPO, MPS, domain_wall_state, neel_state, product_state, sz_p
 from .ite import (beta_grid, geometric_schedule, ite_energy, ite_evolve, ite_step, log_panel_steps,
                   uniform_beta_steps, uniform_schedule)
 from .native import cbe_bug_step, tdvp2_step
+from .qtt import (HestonParams, heston_mpo, heston_op, qtt_derivative, qtt_grid, qtt_mps,
+                  qtt_separable, qtt_shift, qtt_to_mpo)
 from .step import DDQRExpansion
 from .step import cbe_bug_step as cbe_bug_step_python_host
 from .tensor import from_blocks, to_blocks
@@ -28,7 +33,9 @@ from .tensor import from_blocks, to_blocks
 __all__ = ["cbe_bug_step", "cbe_bug_step_python_host", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
            "domain_wall_state", "neel_state", "product_state", "xxz_mpo", "tdvp2_step",
            "tdvp2_step_host", "ite_step", "ite_step_host", "ite_evolve", "ite_energy", "log_panel_steps",
-           "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule"]
+           "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule",
+           "qtt_grid", "qtt_separable", "qtt_mps", "qtt_shift", "qtt_derivative", "qtt_to_mpo",
+           "HestonParams", "heston_op", "heston_mpo"]
 
 
 def magnetisation(psi):

@@ -160,6 +160,29 @@ def op_shift(n, periodic=False):
     return cores
 
 
+QTT_BCS = ("periodic", "dirichlet0", "onesided")  # derivatives.jl:15
+
+
+def qtt_shift(n, bc="periodic"):
+    """``qtt_shift(n; bc = :periodic)`` (``derivatives.jl:23-40``): ``(S psi)_i = psi_{i+1}`` on
+    ``n`` bits; ``periodic`` wraps ``2^n - 1`` onto 0, any other boundary leaves the last row zero.
+    The backward shift is ``op_transpose(qtt_shift(n, bc))``."""
+    if n < 1:
+        raise ValueError("qtt_shift needs n >= 1")
+    return op_shift(n, periodic=bc == "periodic")
+
+
+def qtt_derivative(n, h, order=1, bc="periodic"):
+    """``qtt_derivative(n, h; order = 1, bc = :periodic)`` (``derivatives.jl:53-83``): the
+    second-order central difference of ``order`` 1 or 2 with boundary ``bc`` (one of ``QTT_BCS``);
+    ``onesided`` needs at least four points."""
+    if bc not in QTT_BCS:
+        raise ValueError(f"bc must be one of {QTT_BCS}, got :{bc}")
+    if order not in (1, 2):
+        raise ValueError(f"order must be 1 or 2, got {order}")
+    return op_derivative(n, h, order=order, bc=bc)
+
+
 def op_transpose(ch):
     return [c.transpose(0, 2, 1, 3).copy() for c in ch]
 
@@ -340,4 +363,15 @@ def cores_to_mpo(cores) -> MPO:
 
 
 def heston_mpo(g: Grid, p: HestonParams, adjoint=False) -> MPO:
+    """``heston_mpo(g, params)`` (``heston.jl:69``): the generator as the solver MPO on device."""
     return cores_to_mpo(heston_cores(g, p, adjoint))
+
+
+def heston_op(g: Grid, p: HestonParams, adjoint=False):
+    """``heston_op(g, params)`` (``heston.jl:36-61``): the generator as host operator cores."""
+    return heston_cores(g, p, adjoint)
+
+
+def qtt_to_mpo(cores) -> MPO:
+    """``qtt_to_mpo`` (``state_adapter.jl:96-109``): operator cores as the solver MPO on device."""
+    return cores_to_mpo(cores)

@@ -213,3 +213,45 @@ def test_grid_orderings_checked_as_the_reference_does():
             with pytest.raises(NotImplementedError):
                 grid(3, 3, **kw)
         assert grid(3, 3, order="grouped", endian="lsb_first").nx == 3
+
+
+def test_reference_named_shift_and_derivative():
+    """``qtt_shift`` / ``qtt_derivative`` under the reference's names and defaults (periodic):
+    every boundary (periodic, dirichlet0, onesided) and order against the dense stencils, the
+    shift against the dense forward shift, and the reference's refusals."""
+    import pytest
+
+    from bondupdategalerkin_b200 import qtt as P
+
+    for n in (3, 4):
+        N = 2 ** n
+        for bc in P.QTT_BCS:
+            for order in (1, 2):
+                want = Q.derivative_dense(N, 0.3, order, bc=bc)
+                assert relerr(Q.mpo_dense(P.qtt_derivative(n, 0.3, order=order, bc=bc)), want) < 1e-12
+        assert relerr(Q.mpo_dense(P.qtt_derivative(n, 0.3)),
+                      Q.derivative_dense(N, 0.3, 1, bc="periodic")) < 1e-12
+        fwd = np.eye(N, k=1)
+        assert np.allclose(Q.mpo_dense(P.qtt_shift(n, bc="dirichlet0")), fwd)
+        wrap = fwd.copy()
+        wrap[N - 1, 0] = 1.0
+        assert np.allclose(Q.mpo_dense(P.qtt_shift(n)), wrap)
+    with pytest.raises(ValueError):
+        P.qtt_derivative(3, 0.1, bc="neumann")
+    with pytest.raises(ValueError):
+        P.qtt_derivative(3, 0.1, order=3)
+    with pytest.raises(ValueError):
+        P.qtt_derivative(1, 0.1, bc="onesided")  # two points: the stencils need four
+    with pytest.raises(ValueError):
+        P.qtt_shift(0)
+
+
+def test_public_api_names_the_quantics_builders():
+    """The public module exports every name it lists, and the quantics builders under the
+    reference's names build the same generator as the oracle."""
+    from bondupdategalerkin_b200 import api
+
+    assert not [n for n in api.__all__ if not hasattr(api, n)]
+    dom = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
+    op = api.heston_op(api.qtt_grid(4, 4, **dom), api.HestonParams(*HP_FIELDS))
+    assert relerr(Q.mpo_dense(op), Q.heston_dense(heston_grid(4, 4), HP)) < 1e-11
