@@ -869,3 +869,36 @@ def test_inner_products_against_dense_and_across_charges():
     assert abs(_inner(b2, a) - np.conj(ab)) < 1e-12
     c = M.product_state(["up", "up", "up", "up", "down", "down"])
     assert _inner(a, c) == 0
+
+
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_ite_schedule_grids(which):
+    """``test_schedules.jl`` (IT-U1): log-panel grids reach beta_max without gaps, uniform inside a
+    panel, the first two panels equal and then doubling, the first step beta_max / (2^(P-1) k),
+    the coarsest (beta_max / 2) / k, reproducible; uniform steps; the refusals."""
+    if which == "product":
+        from bondupdategalerkin_b200 import ite as I
+    else:
+        from oracle import ite as I
+    for bmax, P, k in ((8.0, 5, 4), (1.0, 1, 4), (30.0, 7, 2)):
+        s = I.log_panel_steps(bmax, P, per_panel=k)
+        g = I.beta_grid(s)
+        assert len(s) == P * k and all(x > 0 for x in s)
+        assert g[0] == 0.0 and g[-1] == pytest.approx(bmax, rel=1e-14)
+        assert all(b > a for a, b in zip(g, g[1:]))
+        panels = [s[j * k:(j + 1) * k] for j in range(P)]
+        assert all(all(x == pytest.approx(p[0]) for x in p) for p in panels)
+        widths = [sum(p) for p in panels]
+        if P >= 2:
+            assert widths[1] == pytest.approx(widths[0])
+        if P >= 3:
+            assert all(widths[j + 1] == pytest.approx(2 * widths[j]) for j in range(1, P - 1))
+        assert s[0] == pytest.approx(bmax / (2.0 ** (P - 1) * k))
+        assert max(s) == pytest.approx((bmax if P == 1 else bmax / 2) / k)
+        assert I.log_panel_steps(bmax, P, per_panel=k) == s
+    u = I.uniform_beta_steps(2.0, 8)
+    assert all(x == 0.25 for x in u) and I.beta_grid(u)[-1] == pytest.approx(2.0)
+    for bad in (lambda: I.log_panel_steps(1.0, 0), lambda: I.log_panel_steps(-1.0, 3),
+                lambda: I.uniform_beta_steps(1.0, 0)):
+        with pytest.raises(ValueError):
+            bad()
