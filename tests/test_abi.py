@@ -213,3 +213,24 @@ def test_krylov_weight_two_by_two_known_answer():
     _engine.check(lib.bug_la_kry_weight(2, H.view(np.float64).ctypes.data_as(_engine._c_double_p),
                                         1, 0.0, -1.0, 1, out.ctypes.data_as(_engine._c_double_p)))
     assert abs(out[0] - 1.0) <= 1e-10
+
+
+def test_projected_footprint_is_the_documented_bound():
+    """The job server's admission size (``bug_projected_footprint``, host arithmetic: no device):
+    state, two environment stacks, one bond's Krylov basis and probes (64 + 16 vectors) and the
+    two-site work tensors at bond dimension maxdim, in complex FP64, doubled for temporaries; zero
+    for a degenerate chain; monotone in every argument."""
+    import ctypes
+
+    from bondupdategalerkin_b200 import _engine
+
+    lib = _engine.load()
+    f = lib.bug_projected_footprint
+    f.restype, f.argtypes = ctypes.c_int64, [ctypes.c_int] * 4
+    for L, d, D, w in ((64, 2, 256, 5), (20, 2, 64, 12), (8, 4, 32, 3)):
+        D2 = D * D
+        want = 2 * 16 * (L * d * D2 + 2 * L * w * D2 + 80 * d * D2 + 4 * d * d * D2)
+        assert f(L, d, D, w) == want
+        assert f(L + 1, d, D, w) > want and f(L, d, D + 1, w) > want and f(L, d, D, w + 1) > want
+    assert f(0, 2, 64, 5) == 0 and f(8, 2, 0, 5) == 0
+    assert f(64, 2, 256, 5) < 2 ** 31  # the headline chain at maxdim 256: ~1.8 GiB of 180 GB
