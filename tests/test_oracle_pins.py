@@ -902,3 +902,28 @@ def test_ite_schedule_grids(which):
                 lambda: I.uniform_beta_steps(1.0, 0)):
         with pytest.raises(ValueError):
             bad()
+
+
+def test_fused_sectors_cover_the_frames_charges():
+    """``test_sectors.jl:18-59``: the fused space link (x) site of every bond frame's U0 has the
+    full dimension with no duplicate charge, U0's new-leg charges are among the fused charges and
+    every stored block conserves charge; links with a non-zero charge are covered (a vacuum link is
+    its own dual and would hide a sign error)."""
+    mpo = M.xxz_mpo(6, J=1.0, delta=0.5)
+    ent = M.neel_state(6)
+    S.cbe_bug_step(ent, mpo, -0.3j, order=2, rng=np.random.default_rng(9))
+    saw_charged = False
+    for psi in (M.domain_wall_state(4), M.neel_state(6), ent):
+        for bond in range(1, len(psi)):
+            S.canonical(psi, bond)
+            U0 = S.frame_from(psi[bond], psi[bond + 1]).U0
+            la, lb, lc = U0.legs
+            fused = B.fused_sectors(la, lb, lc.dir)
+            assert sum(la.sectors[qa] * lb.sectors[qb] for v in fused.values() for qa, qb in v) \
+                == U0.dim(0) * U0.dim(1)
+            assert len(set(fused)) == len(fused)
+            assert set(lc.sectors) <= set(fused)
+            for qa, qb, qc in U0.blocks:
+                assert la.dir * qa + lb.dir * qb + lc.dir * qc == 0
+            saw_charged |= any(q != 0 for q in la.sectors)
+    assert saw_charged
