@@ -133,3 +133,13 @@ def test_reference_arm_prints_one_line_on_rank_zero_only():
     r1 = _bench(["--impl", "reference", "--steps", "1", "--warmup", "3"],
                 WORLD_SIZE="2", RANK="1", LOCAL_RANK="1")
     assert r1.returncode == 0 and r1.stdout.strip() == ""
+
+
+@pytest.mark.parametrize("workload,metric", [("tdvp2", "tdvp2_steps_per_s"), ("ite", "ite_steps_per_s")])
+def test_reference_arm_other_workloads(workload, metric):
+    """The reference arm keeps the same contract on the TDVP2 and imaginary-time workloads."""
+    r = _bench(["--impl", "reference", "--workload", workload, "--steps", "1", "--warmup", "3"])
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.strip()][-1])
+    assert line["impl"] == "reference" and line["metric"] == metric and line["value"] > 0
+    assert line["config"]["workload"].startswith(workload) and line["higher_is_better"] is True
