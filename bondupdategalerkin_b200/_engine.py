@@ -112,6 +112,29 @@ class EngineError(RuntimeError):
         self.code = code
 
 
+# The status codes as the exceptions a caller of the reference catches: an ArgumentError or
+# DimensionMismatch is a ValueError here, a non-finite or unconverged computation an
+# ArithmeticError, an allocation failure a MemoryError. Each is still an EngineError.
+class EngineArgumentError(EngineError, ValueError):
+    """BUG_EINVAL: a bad argument, shape or arrow."""
+
+
+class EngineNonFiniteError(EngineError, ArithmeticError):
+    """BUG_ENONFINITE: non-finite data where the reference throws."""
+
+
+class EngineMemoryError(EngineError, MemoryError):
+    """BUG_ENOMEM: a device or host allocation failed."""
+
+
+class EngineConvergenceError(EngineError, ArithmeticError):
+    """BUG_ENOTCONV: an iterative kernel hit its iteration bound."""
+
+
+_ERRORS = {1: EngineArgumentError, 2: EngineNonFiniteError, 3: EngineMemoryError,
+           6: EngineConvergenceError}
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -137,7 +160,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
 
 def check(code: int) -> None:
     if code != 0:
-        raise EngineError(code, load().bug_last_error().decode(errors="replace"))
+        raise _ERRORS.get(code, EngineError)(code, load().bug_last_error().decode(errors="replace"))
 
 
 class Context:

@@ -234,3 +234,23 @@ def test_projected_footprint_is_the_documented_bound():
         assert f(L + 1, d, D, w) > want and f(L, d, D + 1, w) > want and f(L, d, D, w + 1) > want
     assert f(0, 2, 64, 5) == 0 and f(8, 2, 0, 5) == 0
     assert f(64, 2, 256, 5) < 2 ** 31  # the headline chain at maxdim 256: ~1.8 GiB of 180 GB
+
+
+def test_status_codes_raise_the_reference_exception_kinds():
+    """A refused argument raises a ValueError (the reference's ArgumentError), non-finite data an
+    ArithmeticError, each still an EngineError carrying its status code."""
+    import numpy as np
+    import pytest
+
+    from bondupdategalerkin_b200 import _engine
+
+    lib = _engine.load()
+    v = np.zeros(4)
+    p = v.ctypes.data_as(_engine._c_double_p)
+    with pytest.raises(ValueError) as e:
+        _engine.check(lib.bug_la_eigh_tridiag(-1, p, p, p, p))
+    assert isinstance(e.value, _engine.EngineError) and e.value.code == 1
+    d = np.array([0.0, np.nan])
+    with pytest.raises(ArithmeticError) as e:
+        _engine.check(lib.bug_la_eigh_tridiag(2, d.ctypes.data_as(_engine._c_double_p), p, p, p))
+    assert isinstance(e.value, _engine.EngineError) and e.value.code == 2
