@@ -927,3 +927,30 @@ def test_fused_sectors_cover_the_frames_charges():
                 assert la.dir * qa + lb.dir * qb + lc.dir * qc == 0
             saw_charged |= any(q != 0 for q in la.sectors)
     assert saw_charged
+
+
+def test_probe_column_rules_agree_with_the_oracle():
+    """The DD probe's column allocation (proportional, ceiling, capped by the sector), the targeted
+    boost (``_boost!``, ``cbe.jl:206-216``: capped, the remainder returned) and the rank cut, in
+    the Python host's ``cbe.py`` against the oracle on random sector layouts."""
+    from bondupdategalerkin_b200 import cbe as PC
+    from oracle import cbe as OC
+
+    rng = np.random.default_rng(17)
+    for _ in range(300):
+        dims = {int(q): int(d) for q, d in zip(rng.choice(np.arange(-6, 7), 5, replace=False),
+                                               rng.integers(0, 40, 5))}
+        budget = int(rng.integers(-2, 120))
+        a = OC.alloc_columns(dims, budget)
+        assert a == PC.alloc_columns(dims, budget)
+        assert all(0 <= a[q] <= dims[q] for q in dims)
+        if budget > 0 and sum(dims.values()) > 0:
+            assert sum(a.values()) >= min(budget, sum(dims.values()))
+        boost = {q: int(rng.integers(-3, 20)) for q in list(dims)[:3]}
+        boost[99] = 5  # a sector with no cap is skipped
+        ca, cb = dict(a), dict(a)
+        la, lb = OC.boost_columns(ca, boost, dims), PC.boost_columns(cb, boost, dims)
+        assert (ca, la) == (cb, lb)
+        assert all(ca[q] <= max(dims[q], a[q]) for q in dims)
+    for args in ((1e-6, 2.0, 0.5), (0.0, 2.0, 0.5), (0.0, 1e-3, 1e-3)):
+        assert OC.rank_cut(*args) == PC.rank_cut(*args)
