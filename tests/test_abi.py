@@ -254,3 +254,19 @@ def test_status_codes_raise_the_reference_exception_kinds():
     with pytest.raises(ArithmeticError) as e:
         _engine.check(lib.bug_la_eigh_tridiag(2, d.ctypes.data_as(_engine._c_double_p), p, p, p))
     assert isinstance(e.value, _engine.EngineError) and e.value.code == 2
+
+
+def test_smoke_fails_loudly_without_a_device():
+    """No CPU fallback: the smoke check of the device path raises where there is no GPU."""
+    import pytest
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import sys
+
+    sys.path.insert(0, ROOT)
+    import __graft_entry__ as g
+
+    with pytest.raises(Exception):
+        g.smoke()
