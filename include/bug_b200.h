@@ -204,8 +204,9 @@ typedef struct {
 } bug_step_params;
 
 /* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
- * sqrt(1/2), in the probe order documented in DESIGN.md (the caller's seeded generator stands in
- * for the reference's `rng`, bug_step.jl:147). */
+ * sqrt(1/2), probe by probe: sectors in ascending charge, one C-ordered matrix over the fused
+ * space per sector (the caller's seeded generator stands in for the reference's `rng`,
+ * bug_step.jl:147). */
 typedef void (*bug_normal_fn)(void* user, int64_t n, double* out);
 
 #define BUG_MAX_SITES 1024
