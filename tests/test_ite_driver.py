@@ -22,7 +22,7 @@ class _Ledger:
 
 
 class _Chain:
-    """A chain of scalars standing in for site tensors (the driver only copies and restores)."""
+    """A chain of scalars standing in for site tensors (ite_step only copies and restores them)."""
 
     def __init__(self, n=4):
         self.sites = [1.0] * n
