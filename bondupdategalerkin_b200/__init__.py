@@ -1,8 +1,9 @@
 """B200-native engine for the rank-adaptive BUG step of madhavmen/BondUpdateGalerkin.
 
-``cbe_bug_step`` (``step.py``) is the drop-in for ``cbe_bug_step!``
-(``src/BUG/TimeEvolution/bug_step.jl:17-513``); its tensors live in HBM as engine handles
-(``tensor.py``) and every contraction, factorisation and reduction runs in ``libbug_b200.so``.
+``native.cbe_bug_step`` (exported by ``api``) is the drop-in for ``cbe_bug_step!``
+(``src/BUG/TimeEvolution/bug_step.jl:17-513``): the whole step runs in ``libbug_b200.so`` (the
+sweep logic in C++, ``csrc/step.cu``; every contraction, factorisation and reduction as sm_100a
+kernels) on tensors that live in HBM as engine handles (``tensor.py``).
 """
 
-__version__ = "0.1.0"
+__version__ = "0.2.0"

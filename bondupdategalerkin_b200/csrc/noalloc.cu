@@ -15,7 +15,12 @@
 //     is rejected with BUG_EINVAL and nothing runs.
 //   * The first call on a device looks up the array's device address with cudaGetSymbolAddress
 //     (a host-side lookup, once per device, made with that device current). Make that first call
-//     before any stream capture.
+//     before any stream capture. The address is kept for the life of the process, so the entry
+//     point assumes the device's primary context (the runtime's default) and no cudaDeviceReset
+//     between calls; a caller that resets the device or makes another context current must not
+//     use it afterwards.
+//   * a, b and out must be 16-byte aligned (the kernel moves whole complex doubles); a misaligned
+//     pointer is rejected with BUG_EINVAL before anything runs.
 //   * All calls on a device share its one array, and the array keeps the last call's contents:
 //     each call clears the counter that must start at zero, but two calls whose kernels overlap on
 //     the GPU (issued on different streams of one device with nothing ordering them) race on the
@@ -119,6 +124,12 @@ extern "C" int bug_inner_noalloc(const double* a, const double* b, int64_t n, do
                                       " exceeds the no-alloc limit of " + std::to_string(kMaxElems) +
                                       " complex elements");
     bugi::require(n == 0 || (a != nullptr && b != nullptr), "bug_inner_noalloc: null input pointer");
+    // the kernel reads and writes whole complex doubles (16-byte loads and stores)
+    bugi::require(reinterpret_cast<uintptr_t>(out) % 16 == 0,
+                  "bug_inner_noalloc: out is not 16-byte aligned");
+    bugi::require(n == 0 || (reinterpret_cast<uintptr_t>(a) % 16 == 0 &&
+                             reinterpret_cast<uintptr_t>(b) % 16 == 0),
+                  "bug_inner_noalloc: a or b is not 16-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* scratch = scratch_address();
     double2* o = reinterpret_cast<double2*>(out);

@@ -436,12 +436,14 @@ int bug_la_kry_weight(int n, const double* hm, int k, double tau_re, double tau_
  * where cudaMalloc is forbidden, or code that must not create or use an engine context (contexts
  * allocate). Computes out[0] + i*out[1] = sum_i conj(a_i) * b_i for `n` interleaved complex
  * doubles at device pointers `a` and `b`, writing the result to the device pointer `out`, on
- * `stream` (a cudaStream_t; NULL is the default stream). The reduction scratch is a 64 KiB static
- * device array held by every device that loads this library until the process exits; n may be at
- * most 8,388,608 (larger n returns BUG_EINVAL). The first call on a device looks the array up with
- * cudaGetSymbolAddress and should come before any stream capture. Calls on one device share the
- * array: calls whose kernels overlap on the GPU race, so serialise them. No cudaMalloc, cudaFree
- * or allocating library routine is called. */
+ * `stream` (a cudaStream_t; NULL is the default stream). a, b and out must be 16-byte aligned
+ * (BUG_EINVAL otherwise, before anything runs). The reduction scratch is a static device array of
+ * 64 KiB + 256 B (65,792 bytes) held by every device that loads this library until the process
+ * exits; n may be at most 8,388,608 (larger n returns BUG_EINVAL). The first call on a device looks
+ * the array up with cudaGetSymbolAddress and should come before any stream capture; the address is
+ * kept for the process, so calls assume the device's primary context and no cudaDeviceReset in
+ * between. Calls on one device share the array: calls whose kernels overlap on the GPU race, so
+ * serialise them. No cudaMalloc, cudaFree or allocating library routine is called. */
 int bug_inner_noalloc(const double* a, const double* b, int64_t n, double* out, void* stream);
 
 #ifdef __cplusplus

@@ -1,8 +1,8 @@
 """Extract the reference's frozen b155550 trajectories into ``tests/golden/b155550.json``.
 
-Run once in a container where the reference tree is mounted:
+Run once where the reference tree is present, naming its root:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference-root>
 
 It copies numbers only (S^z profiles, bond dimensions, statuses, errors against the exact answer,
 the discarded weight, norms and the no-symmetry final state) from
@@ -33,4 +33,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference-root>")
+    main(sys.argv[1])

@@ -56,6 +56,43 @@ def test_contract(D, case):
     assert same(got, want) < 1e-13
 
 
+def _big_cases(rng):
+    """Contractions at the block sizes maxdim 256-512 allows: sector dims 33-256, contracted
+    extents 17, 100 and 512, and 3- and 4-dim strided index groups on either operand."""
+    SS2 = {-1: 1, 1: 1}
+    A = rand_bt(rng, (-1, -1, +1), ({0: 64, 2: 33}, SS2, {-1: 64, 1: 128, 3: 33}), 1.0)
+    E = rand_bt(rng, (-1, +1, +1), ({q: 128 for q in (-2, 0, 2, 4)}, {-2: 1, 0: 3, 2: 1},
+                                    {0: 64, 2: 33}), 1.0)
+    M = rand_bt(rng, (-1, +1), ({0: 256, 2: 128, 4: 64}, {0: 17, 2: 100, 4: 512}), 1.0)
+    N = rand_bt(rng, (-1, +1), ({0: 17, 2: 100, 4: 512}, {0: 64, 2: 33, 4: 256}), 1.0)
+    sec = {-2: 3, 0: 5, 2: 2}
+    P = rand_bt(rng, (+1, -1, +1, -1, +1), (sec,) * 5, 1.0)
+    Q = rand_bt(rng, (-1, +1, -1, +1, -1), (sec,) * 5, 1.0)
+    S = rand_bt(rng, (+1, -1, +1), (sec, {0: 33, 2: 64}, {-2: 4, 0: 5, 2: 6}), 1.0)
+    R4 = rand_bt(rng, (-1, +1, -1, +1), ({0: 33, 2: 40}, {0: 2, 2: 3}, {0: 4, 2: 5}, {0: 66, 2: 70, 4: 9}),
+                 1.0)
+    return [
+        (A, (0, 1), A, (0, 1), True, False),      # K = 33/64, outputs up to 128 x 128
+        (E, (2,), A, (0,), False, False),          # env x site, K = 33/64, 128-row outputs
+        (M, (1,), N, (0,), False, False),          # K = 17, 100, 512 on 256/128/64 x 64/33/256
+        (N, (0,), M, (1,), True, True),            # the same pairs transposed and conjugated
+        (P, (0, 2, 3, 4), Q, (4, 0, 1, 2), False, False),  # 4-dim strided contracted groups
+        (P, (1,), S, (0,), False, False),          # a 4-dim free group (rows) x 2 free legs
+        (R4, (0, 3), R4, (0, 3), True, False),     # split contracted legs, 2-dim free group
+        (R4, (3,), R4, (3,), False, True),         # 3-dim free groups, K up to 70
+    ]
+
+
+@pytest.mark.parametrize("case", range(8))
+def test_contract_large_blocks(D, case):
+    rng = np.random.default_rng(500 + case)
+    a, ia, b, ib, ca, cb = _big_cases(rng)[case]
+    want = OB.contract(a, ia, b, ib, conja=ca, conjb=cb)
+    got = to_host(D.contract(to_dev(a), ia, to_dev(b), ib, conja=ca, conjb=cb))
+    assert sorted(got.blocks) == sorted(want.blocks)
+    assert same(got, want) < 1e-13
+
+
 @pytest.mark.parametrize("left,cutoff,nkeep", [((0, 1), 0.0, None), ((0,), 0.0, None),
                                                 ((0, 1), 1e-1, None), ((0, 1), 0.0, 5),
                                                 ((1, 2), 0.0, None), ((0, 2), 1e-3, 7)])

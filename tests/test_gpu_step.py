@@ -105,9 +105,19 @@ def test_xxz_quench(dev, native):
 
 @pytest.mark.parametrize("native", HOSTS)
 def test_xxz_quench_l64_native_vs_oracle(dev, native):
-    """The benchmark workload's first steps (L = 64, delta = 0.5, maxdim 256, tol 1e-4)."""
-    run_pair(dev, 64, 6, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=256, check_every=3,
+    """The benchmark workload (L = 64, delta = 0.5, maxdim 256, tol 1e-4) over its first 25 steps,
+    which include every step the default benchmark times (6..25): dimensions, verdicts, widths and
+    iterations every step, the state and S^z every 5 steps."""
+    run_pair(dev, 64, 25, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=256, check_every=5,
              native=native)
+
+
+def test_xxz_quench_l64_full_trajectory(dev):
+    """The whole 100-step trajectory of the benchmark workload on the native step (chi reaches
+    39): dimensions, verdicts, widths and iterations every step, the state and S^z every 10."""
+    _, _, worst = run_pair(dev, 64, 100, "domain_wall_state", 0.5, 2, tol_basis=1e-4, maxdim=256,
+                           check_every=10, native=True)
+    assert worst[0] <= 1e-12 and worst[1] <= 1e-10
 
 
 @pytest.mark.parametrize("native", HOSTS)
