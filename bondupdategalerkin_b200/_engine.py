@@ -28,6 +28,10 @@ SIGNATURES = {
     "bug_ctx_bytes_in_use": (ctypes.c_int64, [_vp]),
     "bug_ctx_stream": (_vp, [_vp]),
     "bug_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "bug_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "bug_batch_context": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "bug_batch_launches": (ctypes.c_int64, [_vp]),
+    "bug_batch_destroy": (ctypes.c_int, [_vp]),
     "bug_ctx_kernel_stats": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
                                             _c_double_p, _c_double_p, _c_double_p]),
     "bug_ctx_reset_stats": (ctypes.c_int, [_vp]),
@@ -93,7 +97,7 @@ SIGNATURES = {
     "bug_inner_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, _vp]),
 }
 # declared in native.py (structure arguments)
-NATIVE_ONLY = ("bug_mps_step", "bug_tdvp2_step")  # bound in native.py with their structs
+NATIVE_ONLY = ("bug_mps_step", "bug_tdvp2_step", "bug_step_batch")  # bound in native.py with their structs
 
 FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
 # Where each family runs: the SVD (and the pivoted QR) is its own kernel; every other family is a
@@ -173,6 +177,15 @@ class Context:
         self.h = h
         self.lib = lib
         self.device = device
+
+    @classmethod
+    def borrow(cls, h, device: int = 0) -> "Context":
+        """A context owned elsewhere (a batch's): usable for tensors, never destroyed here."""
+        c = cls.__new__(cls)
+        c.h = h
+        c.lib = load()
+        c.device = device
+        return c
 
     def synchronize(self):
         check(self.lib.bug_ctx_synchronize(self.h))

@@ -915,7 +915,7 @@ void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, cons
   std::vector<int> seg;
   dot_descs(pairs, descs, seg);
   if (descs.empty()) {
-    BUG_CUDA(cudaMemsetAsync(q, 0, pairs.size() * sizeof(double2), c->stream));
+    zero_fill(c, q, int64_t(pairs.size()));  // a (queued) stage: stays in order with the others
     return;
   }
   launch_dots(c, descs, seg, int(pairs.size()), q, 32.0);
@@ -1011,16 +1011,24 @@ std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,
 }  // namespace bugi
 
 namespace bugi {
+int guard_body(const std::function<void()>& f);
+
+// Runs one C-ABI call. When it returns, the stages the call queued on its context are launched
+// (or dropped if the call failed) and the call's scratch is released, so every call leaves all of
+// its work enqueued on the context stream, in order.
 int guard(const std::function<void()>& f) {
-  struct Flush {
-    ~Flush() {
-      if (bug_ctx* c = g_active_ctx) {
-        for (void* p : c->deferred) c->dev_free(p);
-        c->deferred.clear();
-      }
-      g_active_ctx = nullptr;
-    }
-  } fl;
+  int rc = guard_body(f);
+  if (bug_ctx* c = g_active_ctx) {
+    if (rc == BUG_OK) rc = guard_body([c] { c->drain(); });
+    if (rc != BUG_OK) c->discard_queue();
+    for (void* p : c->deferred) c->dev_free(p);
+    c->deferred.clear();
+  }
+  g_active_ctx = nullptr;
+  return rc;
+}
+
+int guard_body(const std::function<void()>& f) {
   try {
     f();
     return BUG_OK;
@@ -1246,10 +1254,15 @@ TensorPtr upload_impl(bug_ctx* c, int rank, const std::vector<Leg>& legs, const 
                       const double* data) {
   auto t = make_tensor(c, rank, legs, keys, false);
   require(int(t->blocks.size()) == int(keys.size()), "duplicate block keys");
-  if (t->nelem > 0)
-    BUG_CUDA(cudaMemcpyAsync(t->buf->ptr, data, size_t(t->nelem) * sizeof(double2),
-                             cudaMemcpyHostToDevice, c->stream));
-  BUG_CUDA(cudaStreamSynchronize(c->stream));
+  if (t->nelem > 0) {
+    // through the pinned staging ring: no wait, and `data` may be reused at once. The payload is
+    // a new allocation that no queued stage reads, so the copy may precede them in the stream.
+    const size_t bytes = size_t(t->nelem) * sizeof(double2);
+    void* h = c->stage(bytes);
+    std::memcpy(h, data, bytes);
+    BUG_CUDA(cudaMemcpyAsync(t->buf->ptr, h, bytes, cudaMemcpyHostToDevice, c->stream));
+    c->stage_done();
+  }
   return t;
 }
 
@@ -1274,6 +1287,10 @@ int bug_ctx_create(int device, bug_ctx** out) {
     auto c = std::make_unique<bug_ctx>();
     c->device = device;
     BUG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->list_cluster = bugk::stage_list_cluster();
+    // BUG_STAGE_LISTS=0 launches every stage on its own (same results; for comparisons)
+    const char* lists = std::getenv("BUG_STAGE_LISTS");
+    c->queue_enabled = !(lists && std::string(lists) == "0");
     for (int i = 0; i < bug_ctx::kSlots; ++i)
       BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
     cudaMemPool_t pool;
@@ -1293,11 +1310,13 @@ int bug_ctx_destroy(bug_ctx* c) {
       cudaEventDestroy(c->stage_ev[i]);
     }
     if (c->pinned_out) cudaFreeHost(c->pinned_out);
+    if (c->tc_err_host) cudaFreeHost(c->tc_err_host);
     if (c->arena) cudaFreeAsync(c->arena, c->stream);
     c->release_cached();
     cudaStreamSynchronize(c->stream);
     if (c->dot_counter) cudaFree(c->dot_counter);
-    cudaStreamDestroy(c->stream);
+    if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+    if (c->owns_stream) cudaStreamDestroy(c->stream);
     delete c;
   });
 }
@@ -1305,7 +1324,8 @@ int bug_ctx_destroy(bug_ctx* c) {
 int bug_ctx_synchronize(bug_ctx* c) {
   return guard([&] {
     require(c != nullptr, "null context");
-    BUG_CUDA(cudaStreamSynchronize(c->stream));
+    c->sync_stream();
+    c->check_tc_error();
   });
 }
 
@@ -1394,7 +1414,7 @@ int bug_tensor_upload(bug_ctx* c, bug_tensor* t, const double* host, int64_t nel
     if (nelem > 0)
       BUG_CUDA(cudaMemcpyAsync(t->buf->ptr, host, size_t(nelem) * sizeof(double2),
                                cudaMemcpyHostToDevice, c->stream));
-    BUG_CUDA(cudaStreamSynchronize(c->stream));
+    c->sync_stream();
   });
 }
 
@@ -1405,7 +1425,7 @@ int bug_tensor_download(bug_ctx* c, const bug_tensor* t, double* host, int64_t n
     if (nelem > 0)
       BUG_CUDA(cudaMemcpyAsync(host, t->buf->ptr, size_t(nelem) * sizeof(double2),
                                cudaMemcpyDeviceToHost, c->stream));
-    BUG_CUDA(cudaStreamSynchronize(c->stream));
+    c->sync_stream();
   });
 }
 

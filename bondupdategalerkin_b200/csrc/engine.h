@@ -15,12 +15,14 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <functional>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -92,6 +94,87 @@ struct bug_ctx;
 
 namespace bugi {
 
+// Merges the stage lists of several contexts that share one stream into single launches (one
+// cluster per list, bugk::launch_stage_lists). A context hands over its drained list and waits
+// until a launch holding it has been issued: at once when every context that could still submit
+// has submitted, else after a short spin. Contexts that are waiting on the device (a read-back) or
+// have no job do not hold a launch back. Stream order keeps each context's operations in its own
+// program order, because a context issues nothing else while its list is pending.
+struct Combiner {
+  cudaStream_t stream = nullptr;
+  int cluster = 0;
+  std::mutex mu;
+  std::vector<std::pair<const bugk::Stage*, int>> pending;
+  std::atomic<uint64_t> launched_upto{0};  // tickets below this were launched
+  uint64_t next_ticket = 0;
+  int active = 0;   // contexts running a job
+  int blocked = 0;  // of those, waiting on the device
+  int64_t launches = 0, lists = 0;
+  cudaError_t err = cudaSuccess;
+  static constexpr double kSpinSeconds = 25e-6;
+
+  // caller holds mu
+  void flush_locked() {
+    if (pending.empty()) return;
+    bugk::ListTable lt{};
+    const int n = int(pending.size());
+    for (int i = 0; i < n; ++i) {
+      lt.stages[i] = pending[i].first;
+      lt.n[i] = pending[i].second;
+    }
+    const cudaError_t e = bugk::launch_stage_lists(lt, n, cluster, stream);
+    if (e != cudaSuccess && err == cudaSuccess) err = e;
+    ++launches;
+    lists += n;
+    pending.clear();
+    launched_upto.store(next_ticket, std::memory_order_release);
+  }
+  void maybe_flush_locked() {
+    if (!pending.empty() && int(pending.size()) >= std::max(1, active - blocked)) flush_locked();
+  }
+  void submit(const bugk::Stage* st, int n) {
+    uint64_t ticket;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      ticket = next_ticket++;
+      pending.push_back({st, n});
+      if (int(pending.size()) >= bugk::kMaxLists) flush_locked();
+      else maybe_flush_locked();
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    while (launched_upto.load(std::memory_order_acquire) <= ticket) {
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > kSpinSeconds) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (launched_upto.load(std::memory_order_relaxed) <= ticket) flush_locked();
+      }
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (err != cudaSuccess) {
+      const cudaError_t e = err;
+      err = cudaSuccess;
+      throw BugError(BUG_EDEVICE, std::string("stage-list launch: ") + cudaGetErrorString(e));
+    }
+  }
+  void job_begin() {
+    std::lock_guard<std::mutex> lk(mu);
+    ++active;
+  }
+  void job_end() {
+    std::lock_guard<std::mutex> lk(mu);
+    --active;
+    maybe_flush_locked();
+  }
+  void block_begin() {
+    std::lock_guard<std::mutex> lk(mu);
+    ++blocked;
+    maybe_flush_locked();
+  }
+  void block_end() {
+    std::lock_guard<std::mutex> lk(mu);
+    --blocked;
+  }
+};
+
 // The context whose scratch the current C-ABI call queued for release (freed, stream-ordered,
 // when the call returns).
 extern thread_local bug_ctx* g_active_ctx;
@@ -144,10 +227,47 @@ struct bug_ctx {
   }
   // Wait for everything issued so far (the host is about to read a result).
   void wait() {
+    drain();
     const auto t0 = std::chrono::steady_clock::now();
-    BUG_CUDA(cudaStreamSynchronize(stream));
+    sync_stream();
     sync_wait_s += since(t0);
     ++syncs;
+    check_tc_error();
+  }
+  // Contexts of a job server or batch share one stream and a Combiner; a context then waits for
+  // its own work by an event (recorded after it), not for the whole shared stream.
+  bugi::Combiner* combiner = nullptr;
+  cudaEvent_t sync_ev = nullptr;
+  bool owns_stream = true;
+  void sync_stream() {
+    if (!combiner) {
+      BUG_CUDA(cudaStreamSynchronize(stream));
+      return;
+    }
+    combiner->block_begin();
+    cudaError_t e = cudaEventRecord(sync_ev, stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(sync_ev);
+    combiner->block_end();
+    BUG_CUDA(e);
+  }
+  // Mixed precision: output blocks with both extents >= mixed_min_dim go to the tensor-core GEMM
+  // (0: off). Its kernels report a timed-out pipeline wait in a host-mapped flag.
+  int mixed_min_dim = 0;
+  int* tc_err_host = nullptr;
+  int* tc_err_dev = nullptr;
+  int* tc_error_flag() {
+    if (!tc_err_host) {
+      BUG_CUDA(cudaHostAlloc((void**)&tc_err_host, sizeof(int), cudaHostAllocMapped));
+      *tc_err_host = 0;
+      BUG_CUDA(cudaHostGetDevicePointer((void**)&tc_err_dev, tc_err_host, 0));
+    }
+    return tc_err_dev;
+  }
+  void check_tc_error() {
+    if (tc_err_host && *tc_err_host) {
+      *tc_err_host = 0;
+      throw bugi::BugError(BUG_ETIMEOUT, "tensor-core GEMM: a pipeline wait ran out its bound");
+    }
   }
   // Device memory: a caching allocator over the stream-ordered pool. Every kernel of the context
   // runs in order on its one stream, so a block released after its last enqueued use may be handed
@@ -186,6 +306,10 @@ struct bug_ctx {
     return p;
   }
   void dev_free(void* p) {
+    if (!queue.empty()) {  // a queued stage may still read it: reusable once the queue is launched
+      pending_free.push_back(p);
+      return;
+    }
     const auto t0 = std::chrono::steady_clock::now();
     auto it = live_.find(p);
     size_t cls = 0;
@@ -239,6 +363,7 @@ struct bug_ctx {
   // Called right before a launch: hands the launch its descriptors, inline in the kernel
   // parameters when they fit, else committed to the arena by one copy.
   bugk::Blob begin() {
+    drain(true);  // queued stages come first in stream order (their descriptors share the batch)
     bugk::Blob b{nullptr, 0, arena};
     if (!batch.empty() && batch.size() <= bugk::kInlineMax) {
       b.host = batch.data();
@@ -331,8 +456,92 @@ struct bug_ctx {
     }
     return dot_counter;
   }
+  // ── deferred stages ──
+  // A small stage is not launched on its own: it joins the queue, and the queue runs as ONE
+  // launch of one thread-block cluster (bugk::launch_stage_list) when the host next needs the
+  // device: a read-back, any other launch or stream operation, a full queue, or the end of the
+  // C-ABI call. The queued stages' descriptors stay in `batch` (their arena offsets are final),
+  // and memory released while stages are queued is parked in `pending_free` until the queue is
+  // launched, so no later operation can be handed a block a queued stage still reads.
+  bool queue_enabled = true;
+  int list_cluster = 0;  // CTAs of the stage-list cluster (0: no cluster launch; never queue)
+  std::vector<bugk::Stage> queue;
+  std::vector<void*> pending_free;
+  int64_t list_launches = 0, queued_stages = 0;
+  static constexpr size_t kQueueMaxStages = 256;
+  static constexpr size_t kQueueMaxBytes = size_t(2) << 20;
+  static constexpr int64_t kQueueMaxElems = 65536;   // copy / lincomb / scale elements
+  static constexpr int kQueueMaxItems = 128;          // gemm tiles, dot descriptors
+  static constexpr double kQueueMaxFlops = 2e7;       // gemm algorithmic flops
+  bool queueable(const bugk::Stage& st, double flops) const {
+    if (!queue_enabled || profiling || list_cluster <= 0) return false;
+    switch (st.kind) {
+      case bugk::kStageCopy:
+      case bugk::kStageLincomb:
+      case bugk::kStageScale:
+        return st.total <= kQueueMaxElems;
+      case bugk::kStageGemm:
+        return st.n <= kQueueMaxItems && flops <= kQueueMaxFlops;
+      case bugk::kStageDot:
+        return st.n <= kQueueMaxItems;
+      default:
+        return false;
+    }
+  }
+  // Launch the queued stages (in order) as one cluster launch. keep_batch: the caller has pushed
+  // descriptors of its own launch after the queued ones and launches next (begin()).
+  void drain(bool keep_batch = false) {
+    if (queue.empty()) return;
+    launch_t0 = std::chrono::steady_clock::now();
+    bugk::Stage* d = push(queue);
+    const int n = int(queue.size());
+    cudaError_t e = cudaSuccess;
+    if (combiner) {
+      // descriptors to this context's arena (a merged launch carries nothing inline), then one
+      // launch with the other contexts' lists
+      commit();
+      queue.clear();
+      combiner->submit(d, n);
+    } else {
+      bugk::Blob b{nullptr, 0, arena};
+      if (batch.size() <= bugk::kInlineMax) {
+        b.host = batch.data();
+        b.bytes = batch.size();
+      } else {
+        commit();  // copies every descriptor pushed so far (the caller's too) into the arena
+      }
+      e = bugk::launch_stage_list(b, d, n, list_cluster, stream);
+      queue.clear();
+      if (!keep_batch) batch.clear();
+      ++launches;
+    }
+    launch_s += since(launch_t0);
+    ++list_launches;
+    std::vector<void*> freed;
+    freed.swap(pending_free);
+    for (void* p : freed) dev_free(p);
+    BUG_CUDA(e);
+  }
+  // Drop the queue without launching it (the C-ABI call failed; its results are not used).
+  void discard_queue() {
+    queue.clear();
+    batch.clear();
+    std::vector<void*> freed;
+    freed.swap(pending_free);
+    for (void* p : freed) dev_free(p);
+  }
   // Launch one stage whose descriptor arrays were pushed since the last launch, and account it.
   void run_stage(const bugk::Stage& st, int fam, double flops, double bytes_moved) {
+    if (queueable(st, flops)) {
+      queue.push_back(st);
+      ++queued_stages;
+      k_launches[fam] += 1;
+      k_flops[fam] += flops;
+      k_bytes[fam] += bytes_moved;
+      bugi::g_active_ctx = this;  // the C-ABI call drains the queue when it returns
+      if (queue.size() >= kQueueMaxStages || batch.size() >= kQueueMaxBytes) drain();
+      return;
+    }
     const bugk::Blob b = begin();
     bugk::launch_stage(b, st, stream);
     launched(fam, flops, bytes_moved);

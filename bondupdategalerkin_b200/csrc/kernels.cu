@@ -1,6 +1,7 @@
 // Device kernels of the B200 block-sparse engine. See kernels.cuh for the role of each kernel.
 #include "kernels.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -71,9 +72,12 @@ struct Rebase {
 
 // ── copy stage: batched strided gather/scatter ───────────────────────────────────────────────
 
-__device__ void copy_stage(const Rebase& rb, const CopyDesc* d, int nd, int64_t total) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
+// `cta` / `ncta`: this CTA's rank among the CTAs that share the stage, and their number (the grid of
+// a single-stage launch, or one cluster of a stage list).
+__device__ void copy_stage(const Rebase& rb, const CopyDesc* d, int nd, int64_t total, int cta,
+                           int ncta) {
+  for (int64_t e = cta * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(ncta) * blockDim.x) {
     const CopyDesc& c = d[find_desc(d, nd, e)];
     int64_t r = e - c.prefix;
     int64_t so = 0, dof = 0;
@@ -228,9 +232,10 @@ __device__ void dot_reduce(const int* seg, int nout, const double2* partial, dou
 
 // ── lincomb and scale stages ────────────────────────────────────────────────────────────────
 
-__device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
+__device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,
+                              int cta, int ncta) {
+  for (int64_t e = cta * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(ncta) * blockDim.x) {
     const LinOut& o = outs[find_desc(outs, nout, e)];
     const int64_t i = e - o.prefix;
     double2 acc = make_double2(0.0, 0.0);
@@ -247,9 +252,10 @@ __device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, 
   }
 }
 
-__device__ void scale_stage(const Rebase& rb, const ScaleDesc* d, int nd, int64_t total) {
-  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(gridDim.x) * blockDim.x) {
+__device__ void scale_stage(const Rebase& rb, const ScaleDesc* d, int nd, int64_t total, int cta,
+                            int ncta) {
+  for (int64_t e = cta * int64_t(blockDim.x) + threadIdx.x; e < total;
+       e += int64_t(ncta) * blockDim.x) {
     const ScaleDesc& c = d[find_desc(d, nd, e)];
     const int64_t i = e - c.prefix;
     const int coord = int((i / c.leg_stride) % c.leg_dim);
@@ -272,7 +278,7 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), con
   const Rebase rb{pb.b, arena, nb};
   switch (st.kind) {
     case kStageCopy:
-      copy_stage(rb, rb(static_cast<const CopyDesc*>(st.a)), st.n, st.total);
+      copy_stage(rb, rb(static_cast<const CopyDesc*>(st.a)), st.n, st.total, blockIdx.x, gridDim.x);
       break;
     case kStageGemm: {
       const GemmOut* outs = rb(static_cast<const GemmOut*>(st.a));
@@ -298,14 +304,79 @@ __global__ void __launch_bounds__(kThreads) stage_kernel(BUG_BLOB_PARAMS(N), con
     }
     case kStageLincomb:
       lincomb_stage(rb(static_cast<const LinOut*>(st.a)), st.n,
-                    rb(static_cast<const LinSrc*>(st.b)), st.total);
+                    rb(static_cast<const LinSrc*>(st.b)), st.total, blockIdx.x, gridDim.x);
       break;
     case kStageScale:
-      scale_stage(rb, rb(static_cast<const ScaleDesc*>(st.a)), st.n, st.total);
+      scale_stage(rb, rb(static_cast<const ScaleDesc*>(st.a)), st.n, st.total, blockIdx.x, gridDim.x);
       break;
     default:
       break;
   }
+}
+
+// ── stage lists: small stages in order, one cluster each, hardware barriers between them ─────
+
+// One list on the CTAs of this cluster: `cta` is the CTA's rank in the cluster and `ncta` the
+// cluster size, so the stage bodies stride over the cluster's CTAs. No CTA leaves early, so every
+// CTA reaches every barrier. The barrier (barrier.cluster arrive.release / wait.acquire) orders
+// each stage's global writes before the next stage's reads, which go through L2 (ld.global.cg).
+__device__ void run_list(const Rebase& rb, const Stage* list, int nstages, int cta, int ncta,
+                         GemmSmem& gsm, double* sr, double* si) {
+  cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+  for (int k = 0; k < nstages; ++k) {
+    const Stage st = list[k];
+    switch (st.kind) {
+      case kStageCopy:
+        copy_stage(rb, rb(static_cast<const CopyDesc*>(st.a)), st.n, st.total, cta, ncta);
+        break;
+      case kStageGemm: {
+        const GemmOut* outs = rb(static_cast<const GemmOut*>(st.a));
+        const GemmPair* pairs = rb(static_cast<const GemmPair*>(st.b));
+        const GemmTile* tiles = rb(static_cast<const GemmTile*>(st.c));
+        for (int t = cta; t < st.n; t += ncta) gemm_tile(outs, pairs, tiles[t], gsm);
+        break;
+      }
+      case kStageDot: {
+        const DotDesc* d = rb(static_cast<const DotDesc*>(st.a));
+        for (int i = cta; i < st.n; i += ncta) dot_partial(d[i], st.p + i, sr, si);
+        cluster.sync();  // every partial written before any is summed
+        if (cta == 0) dot_reduce(rb(static_cast<const int*>(st.b)), int(st.total), st.p, st.q);
+        break;
+      }
+      case kStageLincomb:
+        lincomb_stage(rb(static_cast<const LinOut*>(st.a)), st.n,
+                      rb(static_cast<const LinSrc*>(st.b)), st.total, cta, ncta);
+        break;
+      case kStageScale:
+        scale_stage(rb, rb(static_cast<const ScaleDesc*>(st.a)), st.n, st.total, cta, ncta);
+        break;
+      default:
+        break;
+    }
+    cluster.sync();
+  }
+}
+
+// One list: the grid is exactly one cluster.
+template <int N>
+__global__ void __launch_bounds__(kThreads) stage_list_kernel(BUG_BLOB_PARAMS(N),
+                                                              const Stage* stages, int nstages) {
+  __shared__ GemmSmem gsm;
+  __shared__ double sr[kThreads / 32], si[kThreads / 32];
+  const Rebase rb{pb.b, arena, nb};
+  run_list(rb, rb(stages), nstages, int(blockIdx.x), int(gridDim.x), gsm, sr, si);
+}
+
+// Several independent lists (of different contexts) in one launch: cluster i runs list i. The
+// lists' descriptors are in their contexts' arenas (nothing inline, nothing to rebase).
+__global__ void __launch_bounds__(kThreads) stage_lists_kernel(const __grid_constant__ ListTable lt) {
+  __shared__ GemmSmem gsm;
+  __shared__ double sr[kThreads / 32], si[kThreads / 32];
+  cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
+  const int ncta = int(cluster.num_blocks());
+  const int li = int(blockIdx.x) / ncta;
+  const Rebase rb{nullptr, nullptr, 0};
+  run_list(rb, lt.stages[li], lt.n[li], int(cluster.block_rank()), ncta, gsm, sr, si);
 }
 
 // ── batched one-sided Jacobi SVD ──────────────────────────────────────────────────────────────
@@ -810,6 +881,78 @@ void launch_stage(const Blob& b, const Stage& st, cudaStream_t s) {
   stage_kernel<NB><<<grid, kThreads, 0, s>>>(P, b.arena, (NBYTES), st)
   BUG_WITH_BLOB(b, BUG_STAGE_LAUNCH);
 #undef BUG_STAGE_LAUNCH
+}
+
+namespace {
+cudaLaunchConfig_t cluster_config(int cluster, int nclusters, cudaStream_t s, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(cluster * nclusters), 1, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = unsigned(cluster);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <int N>
+cudaError_t list_launch_n(const ParamBlock<N>& p, const char* arena, int64_t nb, const Stage* st,
+                          int n, int cluster, cudaStream_t s) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = cluster_config(cluster, 1, s, attr);
+  return cudaLaunchKernelEx(&cfg, stage_list_kernel<N>, p, arena, nb, st, n);
+}
+
+// Largest cluster (16, else 8) of which at least one can be resident, for one kernel.
+template <class K>
+int cluster_for(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  for (int c : {16, 8}) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config(c, 1, nullptr, attr);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kernel, &cfg) == cudaSuccess && n >= 1) return c;
+    cudaGetLastError();
+  }
+  return 0;
+}
+}  // namespace
+
+int stage_list_cluster() {
+  static int cl[64];
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  std::lock_guard<std::mutex> lk(g_launch_mu);
+  if (!done[dev]) {
+    // every list kernel must allow the size used (they share one code path)
+    cl[dev] = std::min({cluster_for(stage_list_kernel<16>), cluster_for(stage_list_kernel<512>),
+                        cluster_for(stage_list_kernel<2048>), cluster_for(stage_list_kernel<8192>),
+                        cluster_for(stage_list_kernel<int(kInlineMax)>), cluster_for(stage_lists_kernel)});
+    done[dev] = true;
+  }
+  return cl[dev];
+}
+
+cudaError_t launch_stage_list(const Blob& b, const Stage* stages, int nstages, int cluster,
+                              cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+#define BUG_LIST_LAUNCH(NB, P, NBYTES) \
+  e = list_launch_n<NB>(P, b.arena, (NBYTES), stages, nstages, cluster, s)
+  BUG_WITH_BLOB(b, BUG_LIST_LAUNCH);
+#undef BUG_LIST_LAUNCH
+  return e;
+}
+
+cudaError_t launch_stage_lists(const ListTable& lt, int nlists, int cluster, cudaStream_t s) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = cluster_config(cluster, nlists, s, attr);
+  return cudaLaunchKernelEx(&cfg, stage_lists_kernel, lt);
 }
 
 void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, int threads,

@@ -178,6 +178,29 @@ constexpr int kStageThreads = 256;
 int stage_items(const Stage& s);
 int stage_grid_limit();
 void launch_stage(const Blob& b, const Stage& st, cudaStream_t s);
+
+// A list of small stages run in order by ONE launch of one thread-block cluster: every CTA of the
+// cluster takes part in every stage (the stage bodies stride over the cluster's CTAs exactly as a
+// single-stage launch strides over its grid), and a hardware cluster barrier (release/acquire at
+// cluster scope) separates consecutive stages, so each stage sees every earlier stage's writes.
+// The arithmetic of every element, tile and partial sum is the single-stage launch's, so results
+// are bit-identical; the dot stage reduces its partials after a barrier instead of by a last-CTA
+// counter. `stages` is an array in the descriptor blob.
+cudaError_t launch_stage_list(const Blob& b, const Stage* stages, int nstages, int cluster,
+                              cudaStream_t s);
+// CTAs per cluster for stage lists on the current device (16 where the device allows the
+// non-portable size, else 8; 0 if no cluster launch is possible).
+int stage_list_cluster();
+
+// Stage lists of several contexts launched together: cluster i (of `cluster` CTAs) runs the n[i]
+// stages at stages[i], in order, with barriers as above. Their descriptors live in device memory
+// (each context's arena), so the kernel rebases nothing.
+constexpr int kMaxLists = 128;
+struct ListTable {
+  const Stage* stages[kMaxLists];
+  int n[kMaxLists];
+};
+cudaError_t launch_stage_lists(const ListTable& lt, int nlists, int cluster, cudaStream_t s);
 // Column-pivoted Householder QR, one CTA per sector (see QrDesc).
 void launch_qr(const Blob& b, const QrDesc* d_desc, int nprob, const CopyDesc* packs, int threads,
                cudaStream_t s);

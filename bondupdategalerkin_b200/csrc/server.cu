@@ -22,6 +22,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <functional>
 #include <mutex>
 #include <thread>
 
@@ -58,6 +59,10 @@ struct bug_server {
   std::map<int64_t, std::unique_ptr<Job>> jobs;
   std::vector<std::thread> threads;
   std::vector<bug_ctx*> ctxs;
+  // The workers' contexts share one stream, and their stage lists go through one combiner: the
+  // lists the running jobs drain at about the same time become one launch (a cluster per job).
+  bugi::Combiner combiner;
+  cudaStream_t shared = nullptr;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -75,6 +80,13 @@ struct bug_server {
 void bug_server::run_job(int w, int64_t id, Job& job) {
   (void)id;
   bug_ctx* ctx = ctxs[w];
+  if (shared) combiner.job_begin();
+  struct End {
+    bug_server* s;
+    ~End() {
+      if (s->shared) s->combiner.job_end();
+    }
+  } end_{this};
   std::vector<bug_tensor*> psi(BUG_MAX_SITES + 1, nullptr), mpo(BUG_MAX_SITES + 1, nullptr);
   std::vector<bug_tensor*> io(BUG_MAX_SITES + 1, nullptr);
   int L = 0, center = 0;
@@ -158,6 +170,23 @@ void bug_server::worker(int w) {
 using bugi::guard;
 using bugi::require;
 
+// Puts the contexts on one new stream with one combiner (their own streams are destroyed).
+static void share_stream(int device, std::vector<bug_ctx*>& ctxs, bugi::Combiner& comb,
+                         cudaStream_t& shared) {
+  BUG_CUDA(cudaSetDevice(device));
+  BUG_CUDA(cudaStreamCreateWithFlags(&shared, cudaStreamNonBlocking));
+  comb.stream = shared;
+  comb.cluster = ctxs[0]->list_cluster;
+  for (bug_ctx* c : ctxs) {
+    BUG_CUDA(cudaStreamSynchronize(c->stream));
+    BUG_CUDA(cudaStreamDestroy(c->stream));
+    c->stream = shared;
+    c->owns_stream = false;
+    c->combiner = &comb;
+    BUG_CUDA(cudaEventCreateWithFlags(&c->sync_ev, cudaEventDisableTiming));
+  }
+}
+
 extern "C" int bug_server_create(int device, int workers, int64_t budget_bytes, bug_server** out) {
   return guard([&] {
     require(out != nullptr && workers >= 1 && workers <= 256 && budget_bytes > 0, "bad argument");
@@ -173,6 +202,11 @@ extern "C" int bug_server_create(int device, int workers, int64_t budget_bytes, 
       }
       s->ctxs.push_back(c);
     }
+    // BUG_SERVER_COMBINE=0 keeps one stream per worker and one launch per list (for comparisons)
+    const char* comb = std::getenv("BUG_SERVER_COMBINE");
+    const bool combine = !(comb && std::string(comb) == "0") && workers <= bugk::kMaxLists &&
+                         s->ctxs[0]->list_cluster > 0 && s->ctxs[0]->queue_enabled;
+    if (combine) share_stream(device, s->ctxs, s->combiner, s->shared);
     bug_server* raw = s.get();
     for (int w = 0; w < workers; ++w) raw->threads.emplace_back([raw, w] { raw->worker(w); });
     *out = s.release();
@@ -298,6 +332,7 @@ extern "C" int bug_server_destroy(bug_server* s) {
     s->done_cv.notify_all();
     for (auto& t : s->threads) t.join();
     for (bug_ctx* c : s->ctxs) bug_ctx_destroy(c);
+    if (s->shared) cudaStreamDestroy(s->shared);
     delete s;
   });
 }
@@ -319,7 +354,135 @@ extern "C" int64_t bug_server_launches(const bug_server* s) {
   if (!s) return 0;
   int64_t n = 0;
   for (const bug_ctx* c : s->ctxs) n += bug_ctx_launches(c);
-  return n;
+  return n + const_cast<bug_server*>(s)->combiner.launches;
+}
+
+// ── batched steps ─────────────────────────────────────────────────────────────────────────────
+// n chains stepped together: n contexts on one shared stream with one combiner (their stage
+// lists merge into shared launches) and n persistent host threads, one per chain.
+
+struct bug_batch {
+  int device = 0;
+  std::vector<bug_ctx*> ctxs;
+  bugi::Combiner combiner;
+  cudaStream_t shared = nullptr;
+  std::vector<std::thread> threads;
+  std::mutex mu;
+  std::condition_variable go_cv, done_cv;
+  uint64_t gen = 0;
+  int nrun = 0, remaining = 0;
+  bool stop = false;
+  std::function<void(int)> task;
+
+  void worker(int i) {
+    cudaSetDevice(device);
+    uint64_t seen = 0;
+    for (;;) {
+      std::function<void(int)> t;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        go_cv.wait(lk, [&] { return stop || gen != seen; });
+        if (stop) return;
+        seen = gen;
+        if (i >= nrun) continue;
+        t = task;
+      }
+      if (shared) combiner.job_begin();
+      t(i);
+      if (shared) combiner.job_end();
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (--remaining == 0) done_cv.notify_all();
+      }
+    }
+  }
+};
+
+extern "C" int bug_batch_create(int device, int n, bug_batch** out) {
+  return guard([&] {
+    require(out != nullptr && n >= 1 && n <= bugk::kMaxLists, "bug_batch_create: bad argument");
+    auto b = std::make_unique<bug_batch>();
+    b->device = device;
+    for (int i = 0; i < n; ++i) {
+      bug_ctx* c = nullptr;
+      const int rc = bug_ctx_create(device, &c);
+      if (rc != BUG_OK) {
+        for (bug_ctx* x : b->ctxs) bug_ctx_destroy(x);
+        throw bugi::BugError(rc, std::string("bug_batch_create: ") + bug_last_error());
+      }
+      b->ctxs.push_back(c);
+    }
+    if (b->ctxs[0]->list_cluster > 0 && b->ctxs[0]->queue_enabled)
+      share_stream(device, b->ctxs, b->combiner, b->shared);
+    bug_batch* raw = b.get();
+    for (int i = 0; i < n; ++i) raw->threads.emplace_back([raw, i] { raw->worker(i); });
+    *out = b.release();
+  });
+}
+
+extern "C" int bug_batch_context(bug_batch* b, int i, bug_ctx** out) {
+  return guard([&] {
+    require(b && out && i >= 0 && i < int(b->ctxs.size()), "bug_batch_context: bad argument");
+    *out = b->ctxs[size_t(i)];
+  });
+}
+
+extern "C" int bug_step_batch(bug_batch* b, int n, const int* L, bug_tensor** const* psi_io,
+                              int* center_io, const bug_tensor* const* const* mpo,
+                              const double* tau_re, const double* tau_im,
+                              const bug_step_params* params, bug_normal_fn draw,
+                              void* const* draw_user, bug_step_info* info, int* status) {
+  int first_rc = BUG_OK;
+  std::string first_err;
+  const int rc0 = guard([&] {
+    require(b && n >= 1 && n <= int(b->ctxs.size()) && L && psi_io && center_io && mpo && tau_re &&
+                tau_im && params && draw && draw_user && info && status,
+            "bug_step_batch: bad argument");
+    std::vector<std::string> chain_err(static_cast<size_t>(n));
+    std::unique_lock<std::mutex> lk(b->mu);
+    b->task = [&](int i) {
+      int nlog = 0;
+      status[i] = bug_mps_step(b->ctxs[size_t(i)], L[i], psi_io[i], &center_io[i], mpo[i], tau_re[i],
+                               tau_im[i], &params[i], draw, draw_user[i], &info[i], nullptr, 0, &nlog);
+      if (status[i] != BUG_OK) chain_err[static_cast<size_t>(i)] = bug_last_error();
+    };
+    b->nrun = n;
+    b->remaining = n;
+    ++b->gen;
+    b->go_cv.notify_all();
+    b->done_cv.wait(lk, [&] { return b->remaining == 0; });
+    b->task = nullptr;
+    for (int i = 0; i < n; ++i)
+      if (status[i] != BUG_OK && first_rc == BUG_OK) {
+        first_rc = status[i];
+        first_err = "chain " + std::to_string(i) + ": " + chain_err[static_cast<size_t>(i)];
+      }
+  });
+  if (rc0 != BUG_OK) return rc0;
+  if (first_rc != BUG_OK) bugi::g_err = first_err;
+  return first_rc;
+}
+
+extern "C" int64_t bug_batch_launches(const bug_batch* b) {
+  if (!b) return 0;
+  int64_t n = 0;
+  for (const bug_ctx* c : b->ctxs) n += bug_ctx_launches(c);
+  return n + const_cast<bug_batch*>(b)->combiner.launches;
+}
+
+extern "C" int bug_batch_destroy(bug_batch* b) {
+  return guard([&] {
+    if (!b) return;
+    {
+      std::lock_guard<std::mutex> lk(b->mu);
+      b->stop = true;
+    }
+    b->go_cv.notify_all();
+    for (auto& t : b->threads) t.join();
+    for (bug_ctx* c : b->ctxs) bug_ctx_destroy(c);
+    if (b->shared) cudaStreamDestroy(b->shared);
+    delete b;
+  });
 }
 
 extern "C" int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim) {

@@ -1940,6 +1940,7 @@ struct Step {
       }
       ran = target;
       double* host = e.c->readback(size_t(4 * maxiter));
+      e.c->drain();  // the queued recurrence writes A and N: it runs before the copies
       BUG_CUDA(cudaMemcpyAsync(host, A, size_t(maxiter) * sizeof(double2), cudaMemcpyDeviceToHost,
                                e.c->stream));
       BUG_CUDA(cudaMemcpyAsync(host + 2 * maxiter, N, size_t(maxiter) * sizeof(double2),

@@ -85,6 +85,12 @@ _declared = [False]
 def _lib():
     lib = E.load()
     if not _declared[0]:
+        lib.bug_step_batch.restype = ctypes.c_int
+        lib.bug_step_batch.argtypes = [
+            ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p,
+            ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(StepParams), DRAW_FN, ctypes.c_void_p,
+            ctypes.POINTER(StepInfo), ctypes.POINTER(ctypes.c_int)]
         lib.bug_mps_step.restype = ctypes.c_int
         lib.bug_mps_step.argtypes = [
             ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int),
@@ -162,6 +168,51 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     the options it refuses raise ``ValueError``, the ones not built here ``NotImplementedError``
     (``options.check_step_options``)."""
     L = len(psi)
+    p, keep = _step_setup(psi, mpo, rng, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_expv=tol_expv,
+                          tol_root=tol_root, tol_krylov=tol_krylov, order=order,
+                          closure_probe=closure_probe, maxdim=maxdim, hermitian=hermitian,
+                          expansion=expansion, root=root, reorth=reorth, truncate=truncate,
+                          work_ceiling_rule=work_ceiling_rule,
+                          bond_ceiling_factor=bond_ceiling_factor,
+                          root_ceiling_factor=root_ceiling_factor, root_maxiter=root_maxiter,
+                          krylov_rank_tol=krylov_rank_tol, frontier_tol=frontier_tol,
+                          fold_omega=fold_omega, closure_checks=closure_checks, eshift=eshift,
+                          root_report=root_report, outside_residual=outside_residual,
+                          root_method=root_method, root_shift=root_shift,
+                          frames_report=frames_report, keep_states=keep_states, keep_tols=keep_tols,
+                          frames_only=frames_only, exact=exact, parallel=parallel, kls=kls)
+    rng = keep["rng"]
+
+    @DRAW_FN
+    def draw(user, n, out):
+        x = rng.standard_normal(int(n))
+        ctypes.memmove(out, x.ctypes.data, 8 * int(n))
+
+    ctx = psi.tensors[0].ctx
+    tau = complex(tau)
+    arr = (ctypes.c_void_p * L)(*[t.h.value for t in psi.tensors])
+    warr = (ctypes.c_void_p * L)(*[w.h.value for w in mpo.tensors])
+    center = ctypes.c_int(psi.center)
+    info = StepInfo()
+    cap = 8 * L
+    logs = (BondLog * cap)()
+    nlog = ctypes.c_int()
+    E.check(_lib().bug_mps_step(ctx.h, L, arr, ctypes.byref(center), warr, tau.real, tau.imag,
+                                ctypes.byref(p), draw, None, ctypes.byref(info), logs, cap,
+                                ctypes.byref(nlog)))
+    return _step_result(psi, ctx, arr, center, info, logs, min(nlog.value, cap), order, eshift,
+                        root_report)
+
+
+def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_krylov, order,
+                closure_probe, maxdim, hermitian, expansion, root, reorth, truncate,
+                work_ceiling_rule, bond_ceiling_factor, root_ceiling_factor, root_maxiter,
+                krylov_rank_tol, frontier_tol, fold_omega, closure_checks, eshift, root_report,
+                outside_residual, root_method, root_shift, frames_report, keep_states, keep_tols,
+                frames_only, exact, parallel, kls):
+    """The step's keyword checks and its ``bug_step_params`` (with the generator save/restore
+    callback); returns the struct and the objects that must outlive the call."""
+    L = len(psi)
     tol_expv = check_step_options(
         L, len(mpo), root=root, parallel=parallel, kls=kls, tol_expv=tol_expv, tol_root=tol_root,
         order=order, work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
@@ -179,12 +230,6 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
                     frontier_tol=frontier_tol, fold_omega=fold_omega, closure_checks=closure_checks)
     if rng is None:
         rng = np.random.default_rng(0x5EED)
-
-    @DRAW_FN
-    def draw(user, n, out):
-        x = rng.standard_normal(int(n))
-        ctypes.memmove(out, x.ctypes.data, 8 * int(n))
-
     saved = []
 
     @RNG_CTL_FN
@@ -203,19 +248,12 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     p.root_report = int(root_report is not None)
     p.outside_residual = int(bool(outside_residual))
     p.rng_ctl = rng_ctl
+    return p, {"rng": rng, "rng_ctl": rng_ctl, "saved": saved}
 
-    ctx = psi.tensors[0].ctx
-    tau = complex(tau)
-    arr = (ctypes.c_void_p * L)(*[t.h.value for t in psi.tensors])
-    warr = (ctypes.c_void_p * L)(*[w.h.value for w in mpo.tensors])
-    center = ctypes.c_int(psi.center)
-    info = StepInfo()
-    cap = 8 * L
-    logs = (BondLog * cap)()
-    nlog = ctypes.c_int()
-    E.check(_lib().bug_mps_step(ctx.h, L, arr, ctypes.byref(center), warr, tau.real, tau.imag,
-                                ctypes.byref(p), draw, None, ctypes.byref(info), logs, cap,
-                                ctypes.byref(nlog)))
+
+def _step_result(psi, ctx, arr, center, info, logs, nlog, order, eshift, root_report):
+    """Installs the step's new site handles in ``psi`` and returns the step info dict."""
+    L = len(psi)
     for i in range(L):
         if arr[i]:
             psi.tensors[i] = DT(ctx, ctypes.c_void_p(arr[i]))
@@ -233,7 +271,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         order=order, n_passes=info.n_passes, n_closure_sweeps=info.n_closure_sweeps,
         defect=info.defect, n_root_frontier=info.n_root_frontier, n_h1_closure=info.n_h1_closure,
         n_compress=info.n_compress,
-        bond_log=[{f: getattr(logs[i], f) for f, _ in BondLog._fields_} for i in range(min(nlog.value, cap))],
+        bond_log=[{f: getattr(logs[i], f) for f, _ in BondLog._fields_} for i in range(nlog)]
+        if logs is not None else [],
     )
     ledger.status = lambda: "met" if ledger.tolerance_met else "budget_unmet"
     if root_report is not None:
@@ -249,6 +288,88 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         ledger=ledger, status="met" if info.status == 0 else "budget_unmet",
         bond_dims=psi.bond_dims(), workcap=list(info.workcap[:L - 1]),
     )
+
+
+_STEP_DEFAULTS = dict(tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=None, tol_krylov=None,
+                      order=1, closure_probe=0, maxdim=None, hermitian=True, expansion=None,
+                      root=None, reorth=True, truncate=True, work_ceiling_rule="bond",
+                      bond_ceiling_factor=None, root_ceiling_factor=1.2, root_maxiter=30,
+                      krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
+                      closure_checks=False, eshift=0.0, root_report=None, outside_residual=False,
+                      root_method="exp", root_shift=True, frames_report=None, keep_states=(),
+                      keep_tols=(), frames_only=False, exact=False, parallel=False, kls=None)
+
+
+class Batch:
+    """Chains stepped together (``bug_step_batch``): ``n`` engine contexts on one shared stream,
+    one host thread per chain, and the small stages the chains queue between their read-backs
+    merged into shared launches (a thread-block cluster per chain). Build chain ``i``'s state and
+    MPO on ``contexts[i]`` (``tensor.from_blocks(..., ctx)``) and free them before ``close()``;
+    each chain's result is the same as its own ``cbe_bug_step``."""
+
+    def __init__(self, n: int, device: int = 0):
+        lib = _lib()
+        h = ctypes.c_void_p()
+        E.check(lib.bug_batch_create(int(device), int(n), ctypes.byref(h)))
+        self.h, self.n, self.lib = h, int(n), lib
+        self.contexts = []
+        for i in range(self.n):
+            c = ctypes.c_void_p()
+            E.check(lib.bug_batch_context(h, i, ctypes.byref(c)))
+            self.contexts.append(E.Context.borrow(c, device))
+
+    def launches(self) -> int:
+        return int(self.lib.bug_batch_launches(self.h))
+
+    def step(self, states, mpos, taus, rngs, **kw) -> list:
+        """One ``cbe_bug_step`` of every chain (``states[i]``, ``mpos[i]``, ``taus[i]``, drawing
+        from ``rngs[i]``), the same keywords for all; returns the per-chain info dicts."""
+        n = len(states)
+        if not (len(mpos) == len(taus) == len(rngs) == n) or n < 1 or n > self.n:
+            raise ValueError("Batch.step: one state, MPO, tau and generator per chain")
+        opts = dict(_STEP_DEFAULTS)
+        unknown = set(kw) - set(opts)
+        if unknown:
+            raise TypeError(f"unknown keywords {sorted(unknown)}")
+        opts.update(kw)
+        params = (StepParams * n)()
+        keeps = []
+        for i in range(n):
+            p, keep = _step_setup(states[i], mpos[i], rngs[i], **opts)
+            params[i] = p
+            keeps.append(keep)
+        gens = [k["rng"] for k in keeps]
+
+        @DRAW_FN
+        def draw(user, count, out):
+            x = gens[int(user or 0)].standard_normal(int(count))
+            ctypes.memmove(out, x.ctypes.data, 8 * int(count))
+
+        Ls = (ctypes.c_int * n)(*[len(s) for s in states])
+        arrs = [(ctypes.c_void_p * len(s))(*[t.h.value for t in s.tensors]) for s in states]
+        warrs = [(ctypes.c_void_p * len(m))(*[w.h.value for w in m.tensors]) for m in mpos]
+        psi_io = (ctypes.c_void_p * n)(*[ctypes.cast(a, ctypes.c_void_p).value for a in arrs])
+        mpo_p = (ctypes.c_void_p * n)(*[ctypes.cast(a, ctypes.c_void_p).value for a in warrs])
+        centers = (ctypes.c_int * n)(*[s.center for s in states])
+        tr = (ctypes.c_double * n)(*[complex(t).real for t in taus])
+        ti = (ctypes.c_double * n)(*[complex(t).imag for t in taus])
+        users = (ctypes.c_void_p * n)(*range(n))
+        infos = (StepInfo * n)()
+        status = (ctypes.c_int * n)()
+        E.check(self.lib.bug_step_batch(self.h, n, Ls, ctypes.cast(psi_io, ctypes.c_void_p), centers,
+                                        ctypes.cast(mpo_p, ctypes.c_void_p), tr, ti, params, draw,
+                                        ctypes.cast(users, ctypes.c_void_p), infos, status))
+        out = []
+        for i in range(n):
+            center = ctypes.c_int(centers[i])
+            out.append(_step_result(states[i], states[i].tensors[0].ctx, arrs[i], center, infos[i],
+                                    None, 0, opts["order"], opts["eshift"], opts["root_report"]))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            E.check(self.lib.bug_batch_destroy(self.h))
+            self.h = None
 
 
 # ── kernel-granular entry points (``bug_env_step`` ... ``bug_observable_sz``) ──────────────────

@@ -408,6 +408,30 @@ int64_t bug_server_launches(const bug_server* s);
  * bond's Krylov basis and probes and the two-site work tensors, doubled for temporaries. */
 int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim);
 
+/* ── batched steps ──────────────────────────────────────────────────────────────────────────
+ * Many independent chains stepped together (the batched caller of `cbe_bug_step!`,
+ * src/BUG/TimeEvolution/bug_step.jl:17-513, which the reference runs one chain at a time). A batch
+ * owns n engine contexts on ONE shared stream and n host threads; each chain's sweep logic runs on
+ * its own thread and context, and the small stages each chain queues between its read-backs are
+ * merged with the other chains' into one launch (a thread-block cluster per chain), so the device
+ * sees one launch per round of all chains' stage lists. Every chain's result is bit-identical to
+ * its own bug_mps_step (the kernels are deterministic, each chain draws from its own generator).
+ * Build chain i's state and MPO on bug_batch_context(b, i); a chain's tensors must stay on its
+ * context and be freed before bug_batch_destroy. Up to 128 chains. */
+typedef struct bug_batch bug_batch;
+int bug_batch_create(int device, int n, bug_batch** out);
+int bug_batch_context(bug_batch* b, int i, bug_ctx** out);
+/* One step of chains 0..n-1 (n <= the batch's size), each argument indexed by chain as
+ * bug_mps_step's; status[i] is chain i's return code, and the call returns the first failing code
+ * (bug_last_error names the chain). */
+int bug_step_batch(bug_batch* b, int n, const int* L, bug_tensor** const* psi_io, int* center_io,
+                   const bug_tensor* const* const* mpo, const double* tau_re, const double* tau_im,
+                   const bug_step_params* params, bug_normal_fn draw, void* const* draw_user,
+                   bug_step_info* info, int* status);
+/* Kernel launches issued for the batch so far (merged stage-list launches counted once). */
+int64_t bug_batch_launches(const bug_batch* b);
+int bug_batch_destroy(bug_batch* b);
+
 /* ── host small-matrix routines of the step (no device work; usable without a GPU) ────────── */
 /* exp(A) for a complex n x n row-major matrix (Pade-13 scaling and squaring); replaces Julia's
  * matrix `exp` in _kry_weight/_hess_coeffs (krylov_enrichment.jl:89-120, root_methods.jl:136-141). */
