@@ -366,182 +366,108 @@ struct SectorPlan {
   int64_t m = 0, n = 0;
 };
 
-int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
-             std::unique_ptr<bug_tensor>& U, std::unique_ptr<bug_tensor>& Vd,
-             std::vector<double>& sv_sorted, std::vector<int>& sv_q, int& nkept, int want,
-             std::unique_ptr<bug_tensor>* USo, std::unique_ptr<bug_tensor>* SVdo) {
+// One tensor's SVD inside a multi-tensor launch: its sector plans and its offsets into the shared
+// workspace, singular values and read-back arrays.
+struct SvdJob {
+  const bug_tensor* t = nullptr;
+  std::vector<int> L, R;
+  std::map<int, SectorPlan> plans;
+  std::vector<SectorPlan*> order;
+  std::vector<int64_t> woff, vwoff, uoff, voff, soff;
+  int64_t wtot = 0, stot = 0;
+  int np = 0;
+};
+
+void svd_plan(SvdJob& j, const bug_tensor& t, int nleft, const int* left) {
   require(nleft >= 0 && nleft <= t.rank, "bad split");
+  j.t = &t;
   std::vector<bool> isl(t.rank, false);
-  std::vector<int> L(left, left + nleft), R;
-  for (int i : L) {
+  j.L.assign(left, left + nleft);
+  for (int i : j.L) {
     require(i >= 0 && i < t.rank && !isl[i], "bad left leg");
     isl[i] = true;
   }
   for (int i = 0; i < t.rank; ++i)
-    if (!isl[i]) R.push_back(i);
-  std::map<int, SectorPlan> plans;
+    if (!isl[i]) j.R.push_back(i);
+  const std::vector<int>& L = j.L;
+  const std::vector<int>& R = j.R;
   for (auto& b : t.blocks) {
     int cq = 0;
     for (int i : L) cq -= t.legs[i].dir * b.key[i];
     std::vector<int> rk, ck;
     for (int i : L) rk.push_back(b.key[i]);
     for (int i : R) ck.push_back(b.key[i]);
-    auto& p = plans[cq];
+    auto& p = j.plans[cq];
     p.charge = cq;
     p.rows.push_back(rk);
     p.cols.push_back(ck);
   }
-  std::vector<SectorPlan*> order;
-  for (auto& kv : plans) {
+  for (auto& kv : j.plans) {
     auto& p = kv.second;
     std::sort(p.rows.begin(), p.rows.end());
     p.rows.erase(std::unique(p.rows.begin(), p.rows.end()), p.rows.end());
     std::sort(p.cols.begin(), p.cols.end());
     p.cols.erase(std::unique(p.cols.begin(), p.cols.end()), p.cols.end());
     for (auto& rk : p.rows) {
-      int64_t s = 1;
-      for (size_t j = 0; j < L.size(); ++j) s *= t.legs[L[j]].dim_of(rk[j]);
+      int64_t sz = 1;
+      for (size_t q = 0; q < L.size(); ++q) sz *= t.legs[L[q]].dim_of(rk[q]);
       p.roff.push_back(p.m);
-      p.rdim.push_back(s);
-      p.m += s;
+      p.rdim.push_back(sz);
+      p.m += sz;
     }
     for (auto& ck : p.cols) {
-      int64_t s = 1;
-      for (size_t j = 0; j < R.size(); ++j) s *= t.legs[R[j]].dim_of(ck[j]);
+      int64_t sz = 1;
+      for (size_t q = 0; q < R.size(); ++q) sz *= t.legs[R[q]].dim_of(ck[q]);
       p.coff.push_back(p.n);
-      p.cdim.push_back(s);
-      p.n += s;
+      p.cdim.push_back(sz);
+      p.n += sz;
     }
-    order.push_back(&p);
+    j.order.push_back(&p);
   }
-  const int np = int(order.size());
+  j.np = int(j.order.size());
   // workspace per sector: work (mm*r), vwork (r*r), U (m*r), V (n*r), S (r)
-  std::vector<int64_t> woff(np), vwoff(np), uoff(np), voff(np), soff(np);
-  int64_t wtot = 0, stot = 0;
-  for (int s = 0; s < np; ++s) {
-    auto& p = *order[s];
+  j.woff.resize(j.np);
+  j.vwoff.resize(j.np);
+  j.uoff.resize(j.np);
+  j.voff.resize(j.np);
+  j.soff.resize(j.np);
+  for (int q = 0; q < j.np; ++q) {
+    auto& p = *j.order[q];
     int64_t mm = std::max(p.m, p.n), r = std::min(p.m, p.n);
     require(r <= 1024, "SVD sector wider than the engine's 1024-column limit");
-    woff[s] = wtot;
-    wtot += mm * r;
-    vwoff[s] = wtot;
-    wtot += r * r;
-    uoff[s] = wtot;
-    wtot += p.m * r;
-    voff[s] = wtot;
-    wtot += p.n * r;
-    soff[s] = stot;
-    stot += r;
+    j.woff[q] = j.wtot;
+    j.wtot += mm * r;
+    j.vwoff[q] = j.wtot;
+    j.wtot += r * r;
+    j.uoff[q] = j.wtot;
+    j.wtot += p.m * r;
+    j.voff[q] = j.wtot;
+    j.wtot += p.n * r;
+    j.soff[q] = j.stot;
+    j.stot += r;
   }
-  double2* W = static_cast<double2*>(c->scratch(size_t(wtot) * sizeof(double2)));
-  double* S = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
-  // singular values and sweep counts also go straight to host-mapped pinned memory
-  double* host = c->readback(size_t(stot) + size_t(np) + 1);
-  int* sweeps = reinterpret_cast<int*>(host + stot);
-  for (int s = 0; s < np; ++s) sweeps[s] = 0;
-  // gather descriptors of the sector matrices (column-major M, or M^H when m < n), run inside the
-  // Jacobi kernel itself
-  std::vector<std::vector<CopyDesc>> packs_of(order.size());
-  for (int bi = 0; bi < int(t.blocks.size()); ++bi) {
-    const Block& b = t.blocks[bi];
-    int cq = 0;
-    for (int i : L) cq -= t.legs[i].dir * b.key[i];
-    auto& p = plans[cq];
-    int s = int(std::find(order.begin(), order.end(), &p) - order.begin());
-    std::vector<int> rk, ck;
-    for (int i : L) rk.push_back(b.key[i]);
-    for (int i : R) ck.push_back(b.key[i]);
-    int ri = int(std::lower_bound(p.rows.begin(), p.rows.end(), rk) - p.rows.begin());
-    int ci = int(std::lower_bound(p.cols.begin(), p.cols.end(), ck) - p.cols.begin());
-    const bool trans = p.m < p.n;
-    auto ss = c_strides(b.shape, t.rank);
-    CopyDesc d{};
-    d.src = t.data(bi);
-    d.dst = W + woff[s];
-    d.n = b.size;
-    d.ndim = t.rank;
-    d.conj = trans ? 1 : 0;
-    d.alpha = make_double2(1.0, 0.0);
-    // element multi-index in (L..., R...) order; row = C-order over L dims, col over R dims
-    int p_i = 0;
-    int64_t rs = 1, cs = 1;
-    std::array<int64_t, BUG_MAX_RANK> rstr{}, cstr{};
-    for (int j = int(L.size()) - 1; j >= 0; --j) {
-      rstr[j] = rs;
-      rs *= b.shape[L[j]];
-    }
-    for (int j = int(R.size()) - 1; j >= 0; --j) {
-      cstr[j] = cs;
-      cs *= b.shape[R[j]];
-    }
-    const int64_t ldw = trans ? p.n : p.m;  // leading dimension of the column-major work
-    for (size_t j = 0; j < L.size(); ++j, ++p_i) {
-      d.dims[p_i] = b.shape[L[j]];
-      d.sstr[p_i] = ss[L[j]];
-      d.dstr[p_i] = trans ? rstr[j] * ldw : rstr[j];
-    }
-    for (size_t j = 0; j < R.size(); ++j, ++p_i) {
-      d.dims[p_i] = b.shape[R[j]];
-      d.sstr[p_i] = ss[R[j]];
-      d.dstr[p_i] = trans ? cstr[j] : cstr[j] * ldw;
-    }
-    const int64_t base = trans ? (p.coff[ci] + p.roff[ri] * ldw) : (p.roff[ri] + p.coff[ci] * ldw);
-    d.dst = W + woff[s] + base;
-    packs_of[s].push_back(d);
-  }
-  std::vector<CopyDesc> packs;
-  // launch Jacobi
-  std::vector<SvdDesc> sd(np);
-  int max_smem = 0;
-  int64_t max_r = 0;
-  const int64_t smem_limit = bugk::svd_smem_limit();
-  for (int s = 0; s < np; ++s) {
-    auto& p = *order[s];
-    int64_t mm = std::max(p.m, p.n), r = std::min(p.m, p.n);
-    SvdDesc& d = sd[s];
-    d.work = W + woff[s];
-    d.vwork = W + vwoff[s];
-    d.U = W + uoff[s];
-    d.V = W + voff[s];
-    d.S = S + soff[s];
-    d.S_host = host + soff[s];
-    d.sweeps = sweeps + s;
-    d.m = int(p.m);
-    d.n = int(p.n);
-    d.trans = p.m < p.n ? 1 : 0;
-    // shared memory for A and V if both fit, else for A alone, else none
-    const int64_t both = (mm * r + r * r) * int64_t(sizeof(double2));
-    const int64_t a_only = mm * r * int64_t(sizeof(double2));
-    d.use_smem = both <= smem_limit ? 2 : (a_only <= smem_limit ? 1 : 0);
-    if (d.use_smem) max_smem = std::max<int>(max_smem, int(d.use_smem == 2 ? both : a_only));
-    max_r = std::max(max_r, r);
-    d.pack_begin = int(packs.size());
-    packs.insert(packs.end(), packs_of[s].begin(), packs_of[s].end());
-    d.pack_end = int(packs.size());
-  }
-  if (np > 0) {
-    SvdDesc* dsd = c->push(sd);
-    CopyDesc* dpk = c->push(packs);
-    double sbytes = 0.0, sflops = 0.0;
-    for (int s2 = 0; s2 < np; ++s2) {
-      double mm = double(std::max(order[s2]->m, order[s2]->n)), r = double(std::min(order[s2]->m, order[s2]->n));
-      sbytes += 16.0 * (2.0 * mm * r + r * r + (order[s2]->m + order[s2]->n) * r);
-      sflops += 8.0 * 2.0 * mm * r * r;  // one QR-equivalent pass: the algorithmic floor of an SVD
-    }
-    // one warp per column pair of a round (8 to 32 warps): a round's pairs run side by side
-    // instead of in turns. Which warp takes a pair or a column changes no reduction order, so
-    // the factors are the same bits for any warp count.
-    const int warps = int(std::min<int64_t>(32, std::max<int64_t>(8, (max_r + 1) / 2)));
-    const bugk::Blob blob = c->begin();
-    bugk::launch_svd(blob, dsd, np, dpk, max_smem, 32 * warps, c->stream);
-    c->launched(BUG_K_SVD, sflops, sbytes);
-  }
-  // the kernel wrote singular values and sweep counts into `host`
-  c->wait();
-  for (int s = 0; s < np; ++s)
-    if (sweeps[s] < 0) {
-      throw BugError(BUG_ENOTCONV, "Jacobi SVD did not converge within its sweep bound");
-    }
+}
+
+// Selection and factors of one job after the launch's read-back.
+void svd_finish(bug_ctx* c, SvdJob& job, const SvdReq& q, double2* W, double* S, const double* host) {
+  const bug_tensor& t = *job.t;
+  const std::vector<int>& L = job.L;
+  const std::vector<int>& R = job.R;
+  const int np = job.np;
+  auto& order = job.order;
+  auto& uoff = job.uoff;
+  auto& voff = job.voff;
+  auto& soff = job.soff;
+  const double cutoff = q.cutoff;
+  const int nkeep = q.nkeep;
+  const int want = q.want;
+  std::vector<double>& sv_sorted = *q.sv_sorted;
+  std::vector<int>& sv_q = *q.sv_q;
+  int& nkept = *q.nkept;
+  std::unique_ptr<bug_tensor>& U = *q.U;
+  std::unique_ptr<bug_tensor>& Vd = *q.Vd;
+  std::unique_ptr<bug_tensor>* USo = q.USo;
+  std::unique_ptr<bug_tensor>* SVdo = q.SVdo;
   // selection (Telum): sigma > cutoff*smax, stable descending sort, Nkeep
   struct Entry {
     double sv;
@@ -670,6 +596,149 @@ int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double
     }
   }
   run_copies(c, out);
+}
+
+
+// The SVDs of several tensors: one Jacobi launch over all their sectors and one read-back; then
+// each tensor's Telum selection and its factors, exactly as one call per tensor would give them
+// (a sector's arithmetic does not depend on the other sectors of the launch).
+void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs) {
+  std::vector<SvdJob> jobs(reqs.size());
+  int64_t wtot = 0, stot = 0, nptot = 0;
+  std::vector<int64_t> wbase(reqs.size()), sbase(reqs.size()), pbase(reqs.size());
+  for (size_t r = 0; r < reqs.size(); ++r) {
+    svd_plan(jobs[r], *reqs[r].t, reqs[r].nleft, reqs[r].left);
+    wbase[r] = wtot;
+    sbase[r] = stot;
+    pbase[r] = nptot;
+    wtot += jobs[r].wtot;
+    stot += jobs[r].stot;
+    nptot += jobs[r].np;
+  }
+  double2* W0 = static_cast<double2*>(c->scratch(size_t(std::max<int64_t>(wtot, 1)) * sizeof(double2)));
+  double* S0 = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
+  // singular values and sweep counts also go straight to host-mapped pinned memory
+  double* host0 = c->readback(size_t(stot) + size_t(nptot) + 1);
+  int* sweeps0 = reinterpret_cast<int*>(host0 + stot);
+  for (int64_t q = 0; q < nptot; ++q) sweeps0[q] = 0;
+  const int smem_limit = bugk::svd_smem_limit();
+  std::vector<SvdDesc> sd;
+  std::vector<CopyDesc> packs;
+  int max_smem = 0;
+  int64_t max_r = 0;
+  double sbytes = 0.0, sflops = 0.0;
+  for (size_t r = 0; r < reqs.size(); ++r) {
+    SvdJob& j = jobs[r];
+    const bug_tensor& t = *j.t;
+    const std::vector<int>& L = j.L;
+    const std::vector<int>& R = j.R;
+    double2* W = W0 + wbase[r];
+    double* S = S0 + sbase[r];
+    double* host = host0 + sbase[r];
+    // gather descriptors of the sector matrices (column-major M, or M^H when m < n), run inside
+    // the Jacobi kernel itself
+    std::vector<std::vector<CopyDesc>> packs_of(j.order.size());
+    for (int bi = 0; bi < int(t.blocks.size()); ++bi) {
+      const Block& b = t.blocks[bi];
+      int cq = 0;
+      for (int i : L) cq -= t.legs[i].dir * b.key[i];
+      auto& p = j.plans[cq];
+      int sec = int(std::find(j.order.begin(), j.order.end(), &p) - j.order.begin());
+      std::vector<int> rk, ck;
+      for (int i : L) rk.push_back(b.key[i]);
+      for (int i : R) ck.push_back(b.key[i]);
+      int ri = int(std::lower_bound(p.rows.begin(), p.rows.end(), rk) - p.rows.begin());
+      int ci = int(std::lower_bound(p.cols.begin(), p.cols.end(), ck) - p.cols.begin());
+      const bool trans = p.m < p.n;
+      auto ss = c_strides(b.shape, t.rank);
+      CopyDesc d{};
+      d.src = t.data(bi);
+      d.dst = W + j.woff[sec];
+      d.n = b.size;
+      d.ndim = t.rank;
+      d.conj = trans ? 1 : 0;
+      d.alpha = make_double2(1.0, 0.0);
+      // element multi-index in (L..., R...) order; row = C-order over L dims, col over R dims
+      int p_i = 0;
+      int64_t rs = 1, cs = 1;
+      std::array<int64_t, BUG_MAX_RANK> rstr{}, cstr{};
+      for (int q = int(L.size()) - 1; q >= 0; --q) {
+        rstr[q] = rs;
+        rs *= b.shape[L[q]];
+      }
+      for (int q = int(R.size()) - 1; q >= 0; --q) {
+        cstr[q] = cs;
+        cs *= b.shape[R[q]];
+      }
+      const int64_t ldw = trans ? p.n : p.m;  // leading dimension of the column-major work
+      for (size_t q = 0; q < L.size(); ++q, ++p_i) {
+        d.dims[p_i] = b.shape[L[q]];
+        d.sstr[p_i] = ss[L[q]];
+        d.dstr[p_i] = trans ? rstr[q] * ldw : rstr[q];
+      }
+      for (size_t q = 0; q < R.size(); ++q, ++p_i) {
+        d.dims[p_i] = b.shape[R[q]];
+        d.sstr[p_i] = ss[R[q]];
+        d.dstr[p_i] = trans ? cstr[q] : cstr[q] * ldw;
+      }
+      const int64_t base = trans ? (p.coff[ci] + p.roff[ri] * ldw) : (p.roff[ri] + p.coff[ci] * ldw);
+      d.dst += base;
+      packs_of[sec].push_back(d);
+    }
+    for (int sec = 0; sec < j.np; ++sec) {
+      auto& p = *j.order[sec];
+      int64_t mm = std::max(p.m, p.n), rr = std::min(p.m, p.n);
+      SvdDesc d{};
+      d.work = W + j.woff[sec];
+      d.vwork = W + j.vwoff[sec];
+      d.U = W + j.uoff[sec];
+      d.V = W + j.voff[sec];
+      d.S = S + j.soff[sec];
+      d.S_host = host + j.soff[sec];
+      d.sweeps = sweeps0 + pbase[r] + sec;
+      d.m = int(p.m);
+      d.n = int(p.n);
+      d.trans = p.m < p.n ? 1 : 0;
+      // shared memory for A and V if both fit, else for A alone, else none
+      const int64_t both = (mm * rr + rr * rr) * int64_t(sizeof(double2));
+      const int64_t a_only = mm * rr * int64_t(sizeof(double2));
+      d.use_smem = both <= smem_limit ? 2 : (a_only <= smem_limit ? 1 : 0);
+      if (d.use_smem) max_smem = std::max<int>(max_smem, int(d.use_smem == 2 ? both : a_only));
+      max_r = std::max(max_r, rr);
+      d.pack_begin = int(packs.size());
+      packs.insert(packs.end(), packs_of[sec].begin(), packs_of[sec].end());
+      d.pack_end = int(packs.size());
+      sd.push_back(d);
+      sbytes += 16.0 * (2.0 * double(mm) * double(rr) + double(rr) * double(rr) + double(p.m + p.n) * double(rr));
+      sflops += 8.0 * 2.0 * double(mm) * double(rr) * double(rr);  // one QR-equivalent pass
+    }
+  }
+  const int np = int(sd.size());
+  if (np > 0) {
+    SvdDesc* dsd = c->push(sd);
+    CopyDesc* dpk = c->push(packs);
+    // one warp per column pair of a round (8 to 32 warps): a round's pairs run side by side
+    // instead of in turns. Which warp takes a pair or a column changes no reduction order, so
+    // the factors are the same bits for any warp count.
+    const int warps = int(std::min<int64_t>(32, std::max<int64_t>(8, (max_r + 1) / 2)));
+    const bugk::Blob blob = c->begin();
+    bugk::launch_svd(blob, dsd, np, dpk, max_smem, 32 * warps, c->stream);
+    c->launched(BUG_K_SVD, sflops, sbytes);
+  }
+  // the kernel wrote singular values and sweep counts into `host`
+  c->wait();
+  for (int64_t q = 0; q < nptot; ++q)
+    if (sweeps0[q] < 0) throw BugError(BUG_ENOTCONV, "Jacobi SVD did not converge within its sweep bound");
+  for (size_t r = 0; r < reqs.size(); ++r)
+    svd_finish(c, jobs[r], reqs[r], W0 + wbase[r], S0 + sbase[r], host0 + sbase[r]);
+}
+
+int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
+             std::unique_ptr<bug_tensor>& U, std::unique_ptr<bug_tensor>& Vd,
+             std::vector<double>& sv_sorted, std::vector<int>& sv_q, int& nkept, int want,
+             std::unique_ptr<bug_tensor>* USo, std::unique_ptr<bug_tensor>* SVdo) {
+  svd_many(c, {SvdReq{&t, nleft, left, cutoff, nkeep, want, &U, &Vd, &sv_sorted, &sv_q, &nkept, USo,
+                      SVdo}});
   return BUG_OK;
 }
 

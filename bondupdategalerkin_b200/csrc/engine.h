@@ -598,6 +598,24 @@ TensorPtr contract_impl(bug_ctx* c, const bug_tensor& A, int n, const int* ia, c
 int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
              TensorPtr& U, TensorPtr& Vd, std::vector<double>& sv_sorted, std::vector<int>& sv_q,
              int& nkept, int want = 3, TensorPtr* US = nullptr, TensorPtr* SVd = nullptr);
+// One tensor's SVD request for svd_many (svd_impl's arguments).
+struct SvdReq {
+  const bug_tensor* t;
+  int nleft;
+  const int* left;
+  double cutoff;
+  int nkeep;
+  int want;
+  TensorPtr* U;
+  TensorPtr* Vd;
+  std::vector<double>* sv_sorted;
+  std::vector<int>* sv_q;
+  int* nkept;
+  TensorPtr* USo;
+  TensorPtr* SVdo;
+};
+// Several tensors' SVDs (each as svd_impl) in one launch and one read-back.
+void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs);
 void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
           double* out_re_im);
 // sum_i coef_i t_i; with cmode[i] != 0 the coefficient of t_i is computed on the device from the

@@ -208,6 +208,39 @@ SVDRes svd(const Eng& e, const T& t, std::vector<int> left, double cutoff, int n
   return r;
 }
 
+// Two independent SVDs (cutoff 0, no Nkeep) in one launch and one read-back, each result as svd()
+// gives it.
+std::pair<SVDRes, SVDRes> svd2(const Eng& e, const T& t1, std::vector<int> left1, int want1,
+                               const T& t2, std::vector<int> left2, int want2) {
+  struct Raw {
+    TensorPtr U, V, US_, SV_;
+    std::vector<double> sv;
+    std::vector<int> q;
+    int nk = 0;
+  } a, b;
+  svd_many(e.c, {SvdReq{t1.get(), int(left1.size()), left1.data(), 0.0, -1, want1, &a.U, &a.V,
+                        &a.sv, &a.q, &a.nk, &a.US_, &a.SV_},
+                 SvdReq{t2.get(), int(left2.size()), left2.data(), 0.0, -1, want2, &b.U, &b.V,
+                        &b.sv, &b.q, &b.nk, &b.US_, &b.SV_}});
+  auto conv = [](Raw& x) {
+    SVDRes r;
+    if (x.U) r.U = Eng::sh(std::move(x.U));
+    if (x.V) r.Vd = Eng::sh(std::move(x.V));
+    if (x.US_) r.Us = Eng::sh(std::move(x.US_));
+    if (x.SV_) r.SVd_ = Eng::sh(std::move(x.SV_));
+    for (size_t i = 0; i < x.sv.size(); ++i) {
+      if (int(i) < x.nk) {
+        r.kept.push_back({x.sv[i], x.q[i]});
+        r.S[x.q[i]].push_back(x.sv[i]);
+      } else {
+        r.trunc.push_back({x.sv[i], x.q[i]});
+      }
+    }
+    return r;
+  };
+  return {conv(a), conv(b)};
+}
+
 T US(const Eng& e, const SVDRes& r) { return r.Us ? r.Us : e.scale_leg(r.U, r.U->rank - 1, r.S); }
 T SVd(const Eng& e, const SVDRes& r) { return r.SVd_ ? r.SVd_ : e.scale_leg(r.Vd, 0, r.S); }
 constexpr int W_U = 1, W_VD = 2, W_US = 4, W_SVD = 8;
@@ -936,8 +969,9 @@ struct Step {
   }
 
   BondFrame frame_from(const T& left, const T& right) {
-    SVDRes rl = svd(e, left, {0, 1}, 0.0, -1, W_U | W_SVD);
-    SVDRes rr = svd(e, right, {0}, 0.0, -1, W_US | W_VD);
+    auto both = svd2(e, left, {0, 1}, W_U | W_SVD, right, {0}, W_US | W_VD);
+    SVDRes& rl = both.first;
+    SVDRes& rr = both.second;
     T core = e.contract(SVd(e, rl), {1}, US(e, rr), {0});
     return BondFrame{rl.U, core, rr.Vd, dim(rl.U, 2)};
   }
