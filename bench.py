@@ -653,6 +653,115 @@ def run_stream_reference(args):
                               "d2h_bytes_per_step": 0}}), flush=True)
 
 
+def _rand_device_tensor(DT, rng, dirs, sectors):
+    """A device tensor with every charge-conserving block present and Gaussian entries."""
+    import itertools
+
+    legs = [DT.Leg(d, s) for d, s in zip(dirs, sectors)]
+    blocks = {}
+    for key in itertools.product(*[sorted(s) for s in sectors]):
+        if sum(d * q for d, q in zip(dirs, key)) != 0:
+            continue
+        shape = tuple(s[q] for s, q in zip(sectors, key))
+        blocks[key] = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    return DT.from_blocks(legs, blocks)
+
+
+def envpush_inputs(DT, rng, kind, D=256):
+    """E (bra, w, ket), A (l, s, r), W (w_l, s_in, s_out, w_r) of a chi = D environment push: one
+    dense block per tensor (no symmetry), or U(1) with 33 link sectors of a Gaussian profile summing
+    to D and the XXZ MPO's sectors (w = 5: charges -2, 0 x 3, +2)."""
+    if kind == "dense":
+        link, wl, sl = {0: D}, {0: 5}, {0: 2}
+        rlink = link
+    else:
+        qs = list(range(-32, 33, 2))
+        wts = np.exp(-np.array(qs, float) ** 2 / (2 * 12.0 ** 2))
+        dims = np.maximum(1, np.floor(wts / wts.sum() * D)).astype(int)
+        dims[len(qs) // 2] += D - dims.sum()
+        link, wl, sl = {q: int(d) for q, d in zip(qs, dims)}, {-2: 1, 0: 3, 2: 1}, {-1: 1, 1: 1}
+        rlink = {q + 1: d for q, d in link.items()}
+    E = _rand_device_tensor(DT, rng, (-1, +1, +1), (link, wl, link))
+    A = _rand_device_tensor(DT, rng, (-1, -1, +1), (link, sl, rlink))
+    W = _rand_device_tensor(DT, rng, (-1, +1, -1, +1), (wl, sl, sl, wl))
+    return E, A, W
+
+
+def run_envpush(args):
+    """The environment push E' = A^dag (E A W) (bug_env_step) at chi = 256 on the FP64 stage kernel
+    and on the tensor-core 3xTF32 path (blocks of at least 64 x 64), timed with CUDA events on the
+    engine stream after an L2 flush; TFLOP/s counts the algorithmic 8 m n k per block pair."""
+    import torch
+
+    from bondupdategalerkin_b200 import _engine as E
+    from bondupdategalerkin_b200 import build as Bld
+    from bondupdategalerkin_b200 import native as N
+    from bondupdategalerkin_b200 import tensor as DT
+
+    if Bld.needs_build():
+        Bld.build()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    ctx = E.context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    peaks = {}
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        peaks = json.load(open(p))
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    tf32_peak = bf16 / 2.0  # dense TF32 issues at half the BF16 rate
+    zgemm = measure_zgemm_tflops(torch, dev)
+    out = {"metric": "env_push_tflops", "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": True, "dtype": "c128 (fp64) / 3xtf32 (mixed)",
+           "data": "synthetic (Gaussian blocks)", "l2": "flushed before every push (256 MiB write)",
+           "cases": {},
+           "peaks": {"fp64_zgemm_tflops_measured": zgemm,
+                     "tf32_dense_tflops": tf32_peak,
+                     "tf32_source": ("MEASURED_PEAKS.json bf16_tflops / 2" if "bf16_tflops" in peaks
+                                     else "fallback 1590 bf16 / 2")}}
+    for kind in ("dense", "u1"):
+        rng = np.random.default_rng(5)
+        Et, At, Wt = envpush_inputs(DT, rng, kind)
+        res = {}
+        results = {}
+        for mode, min_dim in (("fp64", 0), ("mixed", 64)):
+            ctx.set_mixed(min_dim)
+            for _ in range(args.warmup):
+                N.env_step(Et, At, Wt, "left")
+            ctx.synchronize()
+            ctx.reset_stats()
+            times = []
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = N.env_step(Et, At, Wt, "left")
+                e1.record(stream)
+                times.append((e0, e1))
+            ctx.synchronize()
+            torch.cuda.synchronize(dev)
+            ms = statistics.median(a.elapsed_time(b) for a, b in times)
+            st = ctx.kernel_stats()
+            flops = (st["gemm"]["flops"] + st["mixed"]["flops"]) / args.steps
+            results[mode] = DT.to_blocks(r)[1]
+            res[mode] = {"ms_per_push": ms, "tflops": flops / (ms / 1e3) / 1e12,
+                         "gflop_per_push": flops / 1e9,
+                         "mixed_share_of_flops": st["mixed"]["flops"] / max(st["gemm"]["flops"] + st["mixed"]["flops"], 1.0),
+                         "launches_per_push": (st["gemm"]["launches"] + st["mixed"]["launches"]) / args.steps}
+        ctx.set_mixed(0)
+        num = max(float(np.max(np.abs(results["mixed"][k] - v))) for k, v in results["fp64"].items())
+        den = max(float(np.max(np.abs(v))) for v in results["fp64"].values())
+        res["mixed_rel_err_vs_fp64"] = num / den
+        res["fp64_frac_of_zgemm"] = res["fp64"]["tflops"] / zgemm
+        # the tensor pipe does three TF32 products per algorithmic one
+        res["mixed_tensor_frac_of_tf32_peak"] = 3.0 * res["mixed"]["tflops"] / tf32_peak
+        res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_push"] / res["mixed"]["ms_per_push"]
+        out["cases"][kind] = res
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -668,7 +777,7 @@ def main():
     ap.add_argument("--L", type=int, default=None,
                     help="chain length override (smaller cases for profiler captures only)")
     ap.add_argument("--workload", default="xxz",
-                    choices=["xxz", "heston", "tdvp2", "ite", "batch", "served"],
+                    choices=["xxz", "heston", "tdvp2", "ite", "batch", "served", "envpush"],
                     help="xxz: the L = 64 XXZ quench (the headline); heston: the 10 + 10-bit "
                          "Heston QTT field (47 timed steps after 3 warm-up make its 50); tdvp2: the "
                          "two-site TDVP baseline over the headline's 100-step trajectory; ite: normalised "
@@ -691,6 +800,9 @@ def main():
         WORKLOAD["L"] = args.L
         global WORKLOAD_NAME
         WORKLOAD_NAME = WORKLOAD_NAME.replace("L64", f"L{args.L}")
+    if args.workload == "envpush":
+        run_envpush(args)
+        return
     if args.workload in ("batch", "served"):
         if args.impl == "reference":
             if dist_env()[1] == 0:

@@ -28,6 +28,7 @@ SIGNATURES = {
     "bug_ctx_bytes_in_use": (ctypes.c_int64, [_vp]),
     "bug_ctx_stream": (_vp, [_vp]),
     "bug_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "bug_ctx_set_mixed": (ctypes.c_int, [_vp, ctypes.c_int]),
     "bug_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
     "bug_batch_context": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "bug_batch_launches": (ctypes.c_int64, [_vp]),
@@ -99,7 +100,7 @@ SIGNATURES = {
 # declared in native.py (structure arguments)
 NATIVE_ONLY = ("bug_mps_step", "bug_tdvp2_step", "bug_step_batch")  # bound in native.py with their structs
 
-FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale")
+FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale", "mixed")
 # Where each family runs: the SVD (and the pivoted QR) is its own kernel; every other family is a
 # stage kind of stage_kernel, one launch per operation.
 KERNEL_NAMES = {"copy": "stage_kernel (copy stage)", "gemm": "stage_kernel (gemm stage)",
@@ -179,12 +180,14 @@ class Context:
         self.device = device
 
     @classmethod
-    def borrow(cls, h, device: int = 0) -> "Context":
-        """A context owned elsewhere (a batch's): usable for tensors, never destroyed here."""
+    def borrow(cls, h, device: int = 0, owner=None) -> "Context":
+        """A context owned elsewhere (a batch's): usable for tensors, never destroyed here. It keeps
+        `owner` alive, so tensors on it (which hold their context) outlive the owner's teardown."""
         c = cls.__new__(cls)
         c.h = h
         c.lib = load()
         c.device = device
+        c._owner = owner
         return c
 
     def synchronize(self):
@@ -202,6 +205,10 @@ class Context:
 
     def set_profiling(self, on: bool) -> None:
         check(self.lib.bug_ctx_set_profiling(self.h, int(on)))
+
+    def set_mixed(self, min_dim: int) -> None:
+        """Tensor-core 3xTF32 contractions for output blocks with both extents >= min_dim (0: off)."""
+        check(self.lib.bug_ctx_set_mixed(self.h, int(min_dim)))
 
     def reset_stats(self) -> None:
         check(self.lib.bug_ctx_reset_stats(self.h))

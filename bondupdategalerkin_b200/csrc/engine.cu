@@ -7,6 +7,7 @@
 // ring, and launches a handful of kernels on the context stream; only operations whose result
 // the host must read (norms, inner products, singular values, downloads) synchronise.
 #include "engine.h"
+#include "tcgemm.cuh"
 
 namespace bugi {
 
@@ -308,6 +309,7 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   std::vector<GemmOut> outs;
   std::vector<GemmPair> pairs;
   std::vector<GemmTile> tiles;
+  std::vector<int> mixed;  // outputs the tensor-core path computes
   for (auto& kv : outmap) {
     int oj = out->find(kv.first);
     const Block& ob = out->blocks[oj];
@@ -333,14 +335,24 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
     go.pair_end = int(pairs.size());
     int o = int(outs.size());
     outs.push_back(go);
+    if (c->mixed_min_dim > 0 && bugtc::mixed_block(int(m), int(nn), c->mixed_min_dim)) {
+      mixed.push_back(o);
+      continue;
+    }
     for (int tm = 0; tm * 32 < m; ++tm)
       for (int tn = 0; tn * 32 < nn; ++tn) tiles.push_back(GemmTile{o, tm, tn});
   }
+  if (!mixed.empty()) bugtc::run_mixed(c, outs, pairs, mixed);
+  if (tiles.empty()) return out;
   GemmOut* d_outs = c->push(outs);
   GemmPair* d_pairs = c->push(pairs);
   GemmTile* d_tiles = c->push(tiles);
   double flops = 0.0, gbytes = 0.0;
-  for (auto& go : outs) {
+  std::vector<char> is_mixed(outs.size(), 0);
+  for (int o : mixed) is_mixed[size_t(o)] = 1;
+  for (size_t o = 0; o < outs.size(); ++o) {
+    if (is_mixed[o]) continue;
+    const GemmOut& go = outs[o];
     gbytes += 16.0 * double(go.m) * double(go.n);
     for (int p = go.pair_begin; p < go.pair_end; ++p) {
       flops += 8.0 * double(go.m) * double(go.n) * double(pairs[p].k);
@@ -1360,6 +1372,10 @@ int bug_ctx_create(int device, bug_ctx** out) {
     // BUG_STAGE_LISTS=0 launches every stage on its own (same results; for comparisons)
     const char* lists = std::getenv("BUG_STAGE_LISTS");
     c->queue_enabled = !(lists && std::string(lists) == "0");
+    if (const char* qm = std::getenv("BUG_STAGE_LIST_MAX")) {
+      const long v = std::strtol(qm, nullptr, 10);
+      if (v >= 1 && v <= 4096) c->queue_max_stages = size_t(v);
+    }
     for (int i = 0; i < bug_ctx::kSlots; ++i)
       BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
     cudaMemPool_t pool;
@@ -1401,6 +1417,13 @@ int bug_ctx_synchronize(bug_ctx* c) {
 int64_t bug_ctx_launches(const bug_ctx* c) { return c ? c->launches : 0; }
 
 void* bug_ctx_stream(bug_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int bug_ctx_set_mixed(bug_ctx* c, int min_dim) {
+  return guard([&] {
+    require(c != nullptr, "null context");
+    c->mixed_min_dim = min_dim > 0 ? min_dim : 0;
+  });
+}
 
 int bug_ctx_set_profiling(bug_ctx* c, int on) {
   return guard([&] {

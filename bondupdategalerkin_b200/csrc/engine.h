@@ -468,7 +468,10 @@ struct bug_ctx {
   std::vector<bugk::Stage> queue;
   std::vector<void*> pending_free;
   int64_t list_launches = 0, queued_stages = 0;
-  static constexpr size_t kQueueMaxStages = 256;
+  // Stages a queue holds before it is launched: small enough that the device starts on them while
+  // the host plans the next ones (a queue held back until a read-back leaves the device idle
+  // meanwhile), large enough to save most launches.
+  size_t queue_max_stages = 8;
   static constexpr size_t kQueueMaxBytes = size_t(2) << 20;
   static constexpr int64_t kQueueMaxElems = 65536;   // copy / lincomb / scale elements
   static constexpr int kQueueMaxItems = 128;          // gemm tiles, dot descriptors
@@ -539,7 +542,7 @@ struct bug_ctx {
       k_flops[fam] += flops;
       k_bytes[fam] += bytes_moved;
       bugi::g_active_ctx = this;  // the C-ABI call drains the queue when it returns
-      if (queue.size() >= kQueueMaxStages || batch.size() >= kQueueMaxBytes) drain();
+      if (queue.size() >= queue_max_stages || batch.size() >= kQueueMaxBytes) drain();
       return;
     }
     const bugk::Blob b = begin();

@@ -304,19 +304,30 @@ class Batch:
     """Chains stepped together (``bug_step_batch``): ``n`` engine contexts on one shared stream,
     one host thread per chain, and the small stages the chains queue between their read-backs
     merged into shared launches (a thread-block cluster per chain). Build chain ``i``'s state and
-    MPO on ``contexts[i]`` (``tensor.from_blocks(..., ctx)``) and free them before ``close()``;
-    each chain's result is the same as its own ``cbe_bug_step``."""
+    MPO on ``contexts[i]`` (``tensor.from_blocks(..., ctx)``); each chain's result is the same as
+    its own ``cbe_bug_step``. The batch is torn down when the last reference to it or to a tensor
+    on its contexts goes away (tensors hold their context, which holds the batch)."""
+
+    class _Handle:
+        def __init__(self, lib, h):
+            self.lib, self.h = lib, h
+
+        def __del__(self):
+            if self.h:
+                self.lib.bug_batch_destroy(self.h)
+                self.h = None
 
     def __init__(self, n: int, device: int = 0):
         lib = _lib()
         h = ctypes.c_void_p()
         E.check(lib.bug_batch_create(int(device), int(n), ctypes.byref(h)))
+        self._handle = Batch._Handle(lib, h)
         self.h, self.n, self.lib = h, int(n), lib
         self.contexts = []
         for i in range(self.n):
             c = ctypes.c_void_p()
             E.check(lib.bug_batch_context(h, i, ctypes.byref(c)))
-            self.contexts.append(E.Context.borrow(c, device))
+            self.contexts.append(E.Context.borrow(c, device, owner=self._handle))
 
     def launches(self) -> int:
         return int(self.lib.bug_batch_launches(self.h))
@@ -365,11 +376,6 @@ class Batch:
             out.append(_step_result(states[i], states[i].tensors[0].ctx, arrs[i], center, infos[i],
                                     None, 0, opts["order"], opts["eshift"], opts["root_report"]))
         return out
-
-    def close(self) -> None:
-        if self.h:
-            E.check(self.lib.bug_batch_destroy(self.h))
-            self.h = None
 
 
 # ── kernel-granular entry points (``bug_env_step`` ... ``bug_observable_sz``) ──────────────────

@@ -71,13 +71,22 @@ enum {
   BUG_K_DOT = 3,      /* inner products and norms */
   BUG_K_LINCOMB = 4,  /* linear combinations */
   BUG_K_SCALE = 5,    /* leg scaling (U*S, S*Vd) */
-  BUG_K_NFAMILIES = 6
+  BUG_K_MIXED = 6,    /* tensor-core (tcgen05, 3xTF32) grouped complex GEMM and its operand pack */
+  BUG_K_NFAMILIES = 7
 };
 /* Profiling on: every launch is bracketed by CUDA events on the context stream. */
 int bug_ctx_set_profiling(bug_ctx* ctx, int on);
 int bug_ctx_kernel_stats(bug_ctx* ctx, int family, int64_t* launches, double* flops, double* bytes,
                          double* device_ms);
 int bug_ctx_reset_stats(bug_ctx* ctx);
+/* Mixed precision (the BUG step's contractions, bug_contract and everything built on them): an
+ * output block whose row and column extents are both at least `min_dim` is computed on the tensor
+ * cores as a 3xTF32 split product with FP32 accumulation (relative error about 1e-7 of
+ * sum |a||b| instead of FP64's 1e-16); smaller blocks, the SVD/QR factorisations, the Krylov
+ * recurrences' inner products and every reduction stay in FP64. min_dim <= 0 turns it off (the
+ * default: everything in FP64). No reference counterpart (the reference computes in FP64 only,
+ * deps/Telum/src/contract.jl:952-1005). */
+int bug_ctx_set_mixed(bug_ctx* ctx, int min_dim);
 /* Host-side accounting since the last reset: how many times the host waited for the stream to
  * read a result back (norms, inner products, singular values), the seconds spent waiting, the
  * seconds spent inside kernel-launch calls, and the seconds spent in the stream-ordered
