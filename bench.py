@@ -141,6 +141,13 @@ def oracle_inputs():
 
 
 def config_dict(args, ws, max_bond=None):
+    cfg = _config_dict(args, ws, max_bond)
+    if getattr(args, "mixed", 0) > 0:
+        cfg["precision"] = f"3xTF32 tensor cores for contraction blocks >= {args.mixed} x {args.mixed}"
+    return cfg
+
+
+def _config_dict(args, ws, max_bond=None):
     if KIND[0] == "heston":
         h = HESTON
         cfg = {"workload": HESTON_NAME, "L": 2 * h["nbits"], "grid": "1024 x 1024", "tau": "0.02",
@@ -356,6 +363,7 @@ def run_engine(args):
         from bondupdategalerkin_b200 import native as DS
 
     ctx = E.context(local)
+    ctx.set_mixed(args.mixed)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     psi, mpo = device_inputs()
@@ -784,6 +792,9 @@ def main():
                          "imaginary time on the L = 32 Heisenberg chain (29 timed steps of dbeta "
                          "0.125 after 3 warm-up reach beta 4); batch: 64 chains at once on the job server; served: a Poisson "
                          "job stream")
+    ap.add_argument("--mixed", type=int, default=0,
+                    help="contraction blocks with both extents >= this run on the tensor cores "
+                         "(3xTF32); 0 (default): everything in FP64")
     ap.add_argument("--workers", type=int, default=0, help="job server workers (0: min(16, cores))")
     ap.add_argument("--jobs", type=int, default=0, help="batch/served: number of jobs")
     ap.add_argument("--scale", type=float, default=0.25,

@@ -1376,6 +1376,10 @@ int bug_ctx_create(int device, bug_ctx** out) {
       const long v = std::strtol(qm, nullptr, 10);
       if (v >= 1 && v <= 4096) c->queue_max_stages = size_t(v);
     }
+    if (const char* qr = std::getenv("BUG_STAGE_LIST_ROUNDS")) {
+      const long v = std::strtol(qr, nullptr, 10);
+      if (v >= 1 && v <= 64) c->queue_rounds = int(v);
+    }
     for (int i = 0; i < bug_ctx::kSlots; ++i)
       BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
     cudaMemPool_t pool;

@@ -471,22 +471,25 @@ struct bug_ctx {
   // Stages a queue holds before it is launched: small enough that the device starts on them while
   // the host plans the next ones (a queue held back until a read-back leaves the device idle
   // meanwhile), large enough to save most launches.
-  size_t queue_max_stages = 8;
+  size_t queue_max_stages = 4;
   static constexpr size_t kQueueMaxBytes = size_t(2) << 20;
-  static constexpr int64_t kQueueMaxElems = 65536;   // copy / lincomb / scale elements
-  static constexpr int kQueueMaxItems = 128;          // gemm tiles, dot descriptors
+  // Only stages the cluster finishes in `queue_rounds` rounds are queued (a gemm tile or dot
+  // descriptor per CTA per round; 4 elements per thread per round for the element-wise kinds):
+  // a larger stage runs faster as its own full-grid launch than on one cluster.
+  int queue_rounds = 1;
   static constexpr double kQueueMaxFlops = 2e7;       // gemm algorithmic flops
   bool queueable(const bugk::Stage& st, double flops) const {
     if (!queue_enabled || profiling || list_cluster <= 0) return false;
+    const int64_t items = int64_t(queue_rounds) * list_cluster;
     switch (st.kind) {
       case bugk::kStageCopy:
       case bugk::kStageLincomb:
       case bugk::kStageScale:
-        return st.total <= kQueueMaxElems;
+        return st.total <= items * bugk::kStageThreads * 4;
       case bugk::kStageGemm:
-        return st.n <= kQueueMaxItems && flops <= kQueueMaxFlops;
+        return st.n <= items && flops <= kQueueMaxFlops;
       case bugk::kStageDot:
-        return st.n <= kQueueMaxItems;
+        return st.n <= items;
       default:
         return false;
     }

@@ -487,7 +487,8 @@ double rank_cut(double stol, double sketch_norm, double outside_norm) {
 T reortho(const Eng& e, const T& frame, const T& block, bool left) {
   if (!block) return nullptr;
   T out = left ? perp_left(e, frame, block) : perp_right(e, frame, block);
-  if (e.norm(out) <= CBE_EPS * std::max(e.norm(block), 1.0)) return nullptr;
+  const auto nb = e.norms(out, block);  // one read-back for both
+  if (nb.first <= CBE_EPS * std::max(nb.second, 1.0)) return nullptr;
   if (left) return svd(e, out, {0, 1}, 1e-14, -1, W_U).U;
   return rows_from_u(e, svd(e, out, {1, 2}, 1e-14, -1, W_U).U);
 }
@@ -1341,8 +1342,9 @@ struct Step {
   std::tuple<T, int64_t, bool> extend_frame(const T& frame, const T& residual, const T& direction,
                                             bool left, double weight, double allowance, int64_t room) {
     std::vector<int> legs = left ? std::vector<int>{0, 1} : std::vector<int>{1, 2};
-    const double nres = e.norm(residual);
-    const double cut = rank_cut(0.0, e.norm(direction), nres);
+    const auto nrd = e.norms(residual, direction);  // one read-back for both
+    const double nres = nrd.first;
+    const double cut = rank_cut(0.0, nrd.second, nres);
     SVDRes res = svd(e, residual, legs, cut, -1, W_U);
     const int nk = int(res.kept.size());
     auto tr = tail_rank(res.kept, weight, allowance, int(std::min<int64_t>(nk, room)), sq_weight(res.trunc));
@@ -2250,7 +2252,8 @@ struct Step {
       nmv += 2;
       for (int i = 0; i < 2; ++i)
         R[i] = e.lin({{1.0, vec}, {-1.0, Y[i]}, {tau * A[i][0], BY[0]}, {tau * A[i][1], BY[1]}});
-      return std::sqrt(std::pow(e.norm(R[0]), 2) + std::pow(e.norm(R[1]), 2));
+      const auto nR = e.norms(R[0], R[1]);
+      return std::sqrt(std::pow(nR.first, 2) + std::pow(nR.second, 2));
     };
     double res = residual();
     int cycles = 1;

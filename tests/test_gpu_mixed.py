@@ -56,7 +56,7 @@ def test_mixed_contract_matches_oracle(D, mixed_ctx, case):
     rng = np.random.default_rng(700 + case)
     a, ia, b, ib, ca, cb = _big_cases(rng)[case]
     want = OB.contract(a, ia, b, ib, conja=ca, conjb=cb)
-    scale = OB.contract(_abs(a), ia, _abs(b), ib)
+    scale = OB.contract(_abs(a), ia, _abs(b), ib, conja=ca, conjb=cb)  # conj only flips arrows
     mixed_ctx.set_mixed(1)
     got = to_host(D.contract(to_dev(a), ia, to_dev(b), ib, conja=ca, conjb=cb))
     assert sorted(got.blocks) == sorted(want.blocks)
