@@ -268,6 +268,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic():
+    """DRAM bytes per launch of each kernel family from a committed ncu capture
+    (profiles/dram_traffic.json: family -> {dram_bytes_per_launch, source}), or {}."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
 def blas_threads():
     try:
         from threadpoolctl import threadpool_info
@@ -482,12 +491,27 @@ def run_engine(args):
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": None,
                 "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
+    traffic = measured_traffic().get(fam)
+    if traffic:
+        roof["traffic"] = traffic["dram_bytes_per_launch"]
+        roof["traffic_source"] = traffic["source"]
     tot_ms = sum(s["ms"] for s in stats.values())
     roof["kernel"] = E.KERNEL_NAMES[fam]
     roof["launches"] = st["launches"]
     roof["avg_launch_us"] = 1e3 * per_launch_ms
     roof["share_of_device_time"] = st["ms"] / tot_ms if tot_ms > 0 else None
     roof["families"] = {f: {"launches": s["launches"], "ms": round(s["ms"], 3)} for f, s in stats.items()}
+
+    # the bandwidth-bound families (copies, inner products, combinations, leg scaling): the one
+    # with the most device time, its algorithmic bytes per launch over its average launch time
+    bw = {f: x for f, x in stats.items() if f in ("copy", "dot", "lincomb", "scale") and x["launches"]}
+    if bw:
+        bf = max(bw, key=lambda f: bw[f]["ms"])
+        b_ms = bw[bf]["ms"] / bw[bf]["launches"]
+        b_ach = bw[bf]["bytes"] / bw[bf]["launches"] / (b_ms / 1e3) / 1e9
+        roof["hbm_family"] = {"family": bf, "bound": "hbm", "achieved": b_ach, "peak": hbm_peak,
+                              "unit": "GB/s", "frac": b_ach / hbm_peak, "avg_launch_us": 1e3 * b_ms,
+                              "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
 
     line = {
         "metric": metric_name(), "value": value, "unit": "steps/s", "n_gpus": ws,
