@@ -65,10 +65,62 @@ enum Unmet { U_SAMPLE = 0, U_TAIL, U_KRYLOV, U_TRUNC, U_PROJECTION, U_EXPV, U_CL
 
 // ── engine wrappers ──────────────────────────────────────────────────────────────────────────
 
+// The step's Gaussian draws, fetched from the caller's stream in chunks instead of one callback per
+// probe. The caller's generator is saved when the step starts (rng_ctl op 0); values are handed out
+// in stream order from the buffer; a save/restore pair inside the step (a measurement drawing from
+// a copy of the stream) becomes a mark on the buffer position; when the step ends, the caller's
+// generator is restored (op 1) and advanced by exactly the values handed out, so it ends where
+// one draw per probe would have left it. Needs a normal stream that splits freely (a draw of a + b
+// values equals a draw of a then b, as numpy's standard_normal does).
+struct DrawBuf {
+  bug_normal_fn draw = nullptr;
+  void* user = nullptr;
+  bug_rng_ctl_fn ctl = nullptr;
+  void* ctl_user = nullptr;
+  std::vector<double> x;      // values drawn from the caller's stream; x[0] is at position `base`
+  int64_t base = 0, pos = 0;  // pos: stream position of the next value handed out
+  std::vector<int64_t> marks;
+  bool open = false;
+  static constexpr int64_t kChunk = 4096;
+  void begin() {
+    ctl(ctl_user, 0);
+    open = true;
+  }
+  void take(int64_t n, double* out) {
+    const int64_t have = base + int64_t(x.size()) - pos;
+    if (have < n) {
+      const int64_t keep_from = marks.empty() ? pos : std::min(pos, marks.front());
+      x.erase(x.begin(), x.begin() + (keep_from - base));
+      base = keep_from;
+      const int64_t get = std::max(n - have, kChunk);
+      const size_t old = x.size();
+      x.resize(old + size_t(get));
+      draw(user, get, x.data() + old);
+    }
+    std::memcpy(out, x.data() + (pos - base), size_t(n) * sizeof(double));
+    pos += n;
+  }
+  void save() { marks.push_back(pos); }
+  void restore() {
+    pos = marks.back();
+    marks.pop_back();
+  }
+  // the caller's generator back to the step's start, then forward by the values handed out
+  void finish() {
+    if (!open) return;
+    open = false;
+    ctl(ctl_user, 1);
+    std::vector<double> tmp(size_t(std::max<int64_t>(pos, 1)));
+    if (pos > 0) draw(user, pos, tmp.data());
+  }
+  ~DrawBuf() { finish(); }
+};
+
 struct Eng {
   bug_ctx* c;
   bug_normal_fn draw;
   void* user;
+  DrawBuf* buf = nullptr;  // when set, draws come from the buffer
 
   static T sh(TensorPtr p) { return T(p.release()); }
 
@@ -168,7 +220,10 @@ struct Eng {
   }
   std::vector<cd> complex_normals(int64_t n) const {
     std::vector<double> x(static_cast<size_t>(2 * n));
-    if (n > 0) draw(user, 2 * n, x.data());
+    if (n > 0) {
+      if (buf) buf->take(2 * n, x.data());
+      else draw(user, 2 * n, x.data());
+    }
     std::vector<cd> z(static_cast<size_t>(n));
     const double s = std::sqrt(0.5);
     for (int64_t i = 0; i < n; ++i) z[i] = cd(x[2 * i] * s, x[2 * i + 1] * s);
@@ -2458,7 +2513,16 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     require(P.acceptance_factor <= 1.0, "acceptance_factor must lie in (0,1]");
     require(P.tail_factor > 0 && P.tail_factor <= 1, "tail_factor must lie in (0,1]");
 
+    DrawBuf dbuf;
     Eng e{c, draw, user};
+    if (prm->rng_ctl && draw) {
+      dbuf.draw = draw;
+      dbuf.user = user;
+      dbuf.ctl = prm->rng_ctl;
+      dbuf.ctl_user = prm->rng_ctl_user;
+      dbuf.begin();
+      e.buf = &dbuf;
+    }
     MPOv mpo;
     for (int i = 0; i < L; ++i) {
       // the MPO handles stay owned by the caller: alias them without taking ownership
@@ -2615,9 +2679,11 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
       auto outside_of = [&](const T& core) {
         Action a;
         Step::KL kf{lf, rf, lenv_root, renv_root, 0};
-        prm->rng_ctl(prm->rng_ctl_user, 0);
+        if (e.buf) e.buf->save();
+        else prm->rng_ctl(prm->rng_ctl_user, 0);
         auto sw = S.frontier_sweep(kf, psi, core, std::max(e.norm(core), EPS), false);
-        prm->rng_ctl(prm->rng_ctl_user, 1);
+        if (e.buf) e.buf->restore();
+        else prm->rng_ctl(prm->rng_ctl_user, 1);
         for (double x : sw.leaks_left) a.left += x * x;
         for (double x : sw.leaks_right) a.right += x * x;
         a.bound = std::sqrt(a.left + a.right);
