@@ -69,7 +69,7 @@ def seed():
 
 
 def dev_step(mod, psi, mpo, rng):
-    """One step of the workload through the product module ``mod`` (native or Python host)."""
+    """One step of the workload through the product module ``mod`` (the native step)."""
     if KIND[0] == "tdvp2":
         from bondupdategalerkin_b200 import native as N
 
@@ -366,10 +366,7 @@ def run_engine(args):
     E.set_default_device(local)
     from bondupdategalerkin_b200 import tensor as DT
 
-    if args.host == "python":
-        from bondupdategalerkin_b200 import step as DS
-    else:
-        from bondupdategalerkin_b200 import native as DS
+    from bondupdategalerkin_b200 import native as DS
 
     ctx = E.context(local)
     ctx.set_mixed(args.mixed)
@@ -466,7 +463,7 @@ def run_engine(args):
                                                    rng=rng_e, **ITE["kw"])
         else:
             host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
-                                               native=args.host == "native", **step_kwargs())
+                                               **step_kwargs())
         e1.record(stream)
         ctx.synchronize()
         e2e_ms += e0.elapsed_time(e1)
@@ -518,7 +515,7 @@ def run_engine(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (deterministic product-state start, seeded Gaussian probes)",
-        "config": dict(config_dict(args, ws, max(final_dims)), host=args.host),
+        "config": config_dict(args, ws, max(final_dims)),
         "gpu_launches": int(launches),
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps},
@@ -802,8 +799,6 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--host", default="native", choices=["native", "python"],
-                    help="native: the step runs inside libbug_b200.so; python: the Python host")
     ap.add_argument("--no-replay", action="store_true",
                     help="time the steps only (for profiler runs)")
     ap.add_argument("--L", type=int, default=None,

@@ -2,9 +2,7 @@
 
 * ``cbe_bug_step(psi, mpo, tau; ...)`` -- the drop-in for ``cbe_bug_step!``
   (``src/BUG/TimeEvolution/bug_step.jl:17-513``) on HBM-resident states, run as one call into the
-  library (``native.py``); ``cbe_bug_step_python_host`` is the same step with the sweep logic in
-  Python over the kernel-granular C-ABI (``step.py``), the shape of a Julia host that keeps its
-  sweeps;
+  library (``native.py``); ``Batch`` steps many chains together (``bug_step_batch``);
 * ``step_host(...)`` -- the same step for a caller whose state lives in host memory: the site
   tensors and the MPO are uploaded, the step runs on the device, and the new site tensors come back
   (the shape of a ``ccall`` from a Julia host that keeps its own containers);
@@ -23,14 +21,13 @@ from __future__ import annotations
 from .models import MPO, MPS, domain_wall_state, neel_state, product_state, sz_profile, xxz_mpo
 from .ite import (beta_grid, geometric_schedule, ite_energy, ite_evolve, ite_step, log_panel_steps,
                   uniform_beta_steps, uniform_schedule)
-from .native import cbe_bug_step, tdvp2_step
+from .native import Batch, cbe_bug_step, tdvp2_step
+from .options import DDQRExpansion
 from .qtt import (HestonParams, heston_mpo, heston_op, qtt_derivative, qtt_grid, qtt_mps,
                   qtt_separable, qtt_shift, qtt_to_mpo)
-from .step import DDQRExpansion
-from .step import cbe_bug_step as cbe_bug_step_python_host
 from .tensor import from_blocks, to_blocks
 
-__all__ = ["cbe_bug_step", "cbe_bug_step_python_host", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
+__all__ = ["cbe_bug_step", "Batch", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
            "domain_wall_state", "neel_state", "product_state", "xxz_mpo", "tdvp2_step",
            "tdvp2_step_host", "ite_step", "ite_step_host", "ite_evolve", "ite_energy", "log_panel_steps",
            "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule",
@@ -42,7 +39,7 @@ def magnetisation(psi):
     return sz_profile(psi)
 
 
-def step_host(host_state, center, host_mpo, tau, native=True, **kwargs):
+def step_host(host_state, center, host_mpo, tau, **kwargs):
     """One BUG step on host-resident data.
 
     ``host_state`` / ``host_mpo``: per site ``(legs, {key: ndarray})`` as ``tensor.to_blocks``
@@ -60,8 +57,7 @@ def step_host(host_state, center, host_mpo, tau, native=True, **kwargs):
         h2d += 16 * t.nelem
         ws.append(t)
     psi = MPS(sites, center)
-    step = cbe_bug_step if native else cbe_bug_step_python_host
-    info = step(psi, MPO(ws), tau, **kwargs)
+    info = cbe_bug_step(psi, MPO(ws), tau, **kwargs)
     out = [to_blocks(t) for t in psi.tensors]
     d2h = sum(16 * t.nelem for t in psi.tensors)
     return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)

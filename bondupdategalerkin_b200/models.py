@@ -202,12 +202,42 @@ def xxz_mpo(L: int, J: float = 1.0, delta: float = 1.0, symmetry: str = "U1") ->
     return mpo_from_entries(L, ls, wstates, entries)
 
 
+def move_right(psi, site):
+    """``move_right!`` (``canonical_form.jl:10-54``): site = U, S Vd absorbed into site + 1."""
+    from . import tensor as B
+
+    res = B.svd(psi[site], (0, 1), cutoff=0.0)
+    psi[site + 1] = B.contract(res.SVd(), (1,), psi[site + 1], (0,))
+    psi[site] = res.U
+
+
+def move_left(psi, site):
+    """``move_left!``: site = Vd, U S absorbed into site - 1."""
+    from . import tensor as B
+
+    res = B.svd(psi[site], (0,), cutoff=0.0)
+    psi[site - 1] = B.contract(psi[site - 1], (2,), res.US(), (0,))
+    psi[site] = res.Vd
+
+
+def canonical(psi, site):
+    """``canonical!(psi, site)``: gauge moves (block SVDs on the device) to centre ``site``."""
+    if not 1 <= site <= len(psi):
+        raise IndexError(site)
+    while psi.center < site:
+        move_right(psi, psi.center)
+        psi.center += 1
+    while psi.center > site:
+        move_left(psi, psi.center)
+        psi.center -= 1
+    return psi
+
+
 def sz_profile(psi) -> np.ndarray:
     """``<S^z_j>`` for every site of a normalised or unnormalised state
     (``magnetisation`` -> ``site_expval``, ``src/QMB/Observables/bond_observables.jl:15``,
     ``local_observables.jl:11-24``): the centre is moved to each site in turn and the site's
     weight read off, which is exact because every other tensor is then an isometry."""
-    from .step import canonical
     from .tensor import to_blocks
 
     phi = psi.copy()

@@ -3,13 +3,35 @@
 Every keyword of the reference step is accepted under its own name. A value the reference refuses
 raises ``ValueError`` (its ``ArgumentError`` / ``DimensionMismatch``) with the reference's reason,
 in the reference's order; a valid value of an option this engine does not build raises
-``NotImplementedError`` naming it. The checks are pure host logic: both hosts run them before any
-device work.
+``NotImplementedError`` naming it. The checks are pure host logic, run before any device work.
 """
 
 from __future__ import annotations
 
-from .budget import DEFAULT_BOND_CEILING_FACTOR
+from dataclasses import dataclass
+
+# the per-bond work ceiling's factor under `:bond` (basis_budget.jl:484-494): frames at most
+# ceil(factor d D_b)
+DEFAULT_BOND_CEILING_FACTOR = 1.2
+
+
+@dataclass
+class DDQRExpansion:
+    """``DDQRExpansion`` defaults (``src/BUG/Randomised/cbe.jl:254-290``): the expansion settings
+    the step passes to the native library (``bug_step_params``)."""
+
+    mode: str = "rank_tail"
+    fixed_width: int = 8
+    fixed_rank: int = 0
+    rank_initial_width: int = 4
+    rank_floor: int = 0
+    tail_factor: float = 0.10
+    holdout_width: int = 4
+    batch_blocks: int = 1
+    cap_selection: str = "storage"
+    acceptance_factor: float = 1.0
+    krylov_mode: str = "auto"
+    krylov_fixed_depth: int = 0
 
 KLS_SCHEDULES = ("sequential", "kl_then_s", "concurrent")  # parallel_kls.jl:7
 WORK_CEILING_RULES = ("maxdim", "bond", "bond_strict", "frame_root")

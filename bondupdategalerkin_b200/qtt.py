@@ -127,7 +127,7 @@ def qtt_separable(g: Grid, fx, fy, tol=1e-14):
 def qtt_mps(cores, center=1) -> MPS:
     """The device state of TT ``cores``: one dense block per site, uploaded, then gauged to site 1
     and on to ``center`` by exact SVD moves on device."""
-    from .step import canonical
+    from .models import canonical
 
     ts = []
     for c in cores:

@@ -27,7 +27,7 @@ def dev():
     from bondupdategalerkin_b200 import ite as DI
     from bondupdategalerkin_b200 import models as DM
     from bondupdategalerkin_b200 import native as N
-    from bondupdategalerkin_b200 import step as DS
+    from bondupdategalerkin_b200 import options as DS
 
     return DM, N, DS, DI
 

@@ -65,9 +65,8 @@ def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10,
     build.build()
     from bondupdategalerkin_b200 import native as DN
     from bondupdategalerkin_b200 import qtt as P
-    from bondupdategalerkin_b200 import step as DS
 
-    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
+    dstep = DN.cbe_bug_step
     dom = dom or dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
     og, pg = Q.qtt_grid(nbits, nbits, **dom), P.qtt_grid(nbits, nbits, **dom)
     fx = fx or (lambda x: np.exp(0.5 * x))
@@ -110,8 +109,7 @@ def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10,
     return opsi, dpsi
 
 
-@pytest.mark.parametrize("native", [pytest.param(False, id="python-host"),
-                                    pytest.param(True, id="native-step")])
+@pytest.mark.parametrize("native", [pytest.param(True, id="native-step")])
 def test_heston_4x4_bits(native):
     run_heston(4, 4, 64, native, tol_basis=1e-8, tol_trunc=1e-12)
 

@@ -24,7 +24,7 @@ def dev():
 
     build.build()
     from bondupdategalerkin_b200 import models as DM
-    from bondupdategalerkin_b200 import step as DS
+    from bondupdategalerkin_b200 import options as DS
 
     return DM, DS
 
@@ -34,7 +34,7 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
     DM, DS = dev
     from bondupdategalerkin_b200 import native as DN
 
-    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
+    dstep = DN.cbe_bug_step
     ostate = getattr(OM, start)(L, symmetry=sym)
     dstate = getattr(DM, start)(L, symmetry=sym)
     ompo = OM.xxz_mpo(L, J=1.0, delta=delta, symmetry=sym)
@@ -73,7 +73,7 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
 FROZEN = dict(work_ceiling_rule="maxdim", expansion=dict(krylov_mode="arnoldi"))
 
 
-HOSTS = [pytest.param(False, id="python-host"), pytest.param(True, id="native-step")]
+HOSTS = [pytest.param(True, id="native-step")]
 
 
 @pytest.mark.parametrize("native", HOSTS)
@@ -125,7 +125,7 @@ def test_two_spin(dev, native):
     DM, DS = dev
     from bondupdategalerkin_b200 import native as DN
 
-    step = DN.cbe_bug_step if native else DS.cbe_bug_step
+    step = DN.cbe_bug_step
     mpo = DM.xxz_mpo(2, J=1.0, delta=0.0)
     psi = DM.product_state(["up", "down"])
     t = 0.3
@@ -212,7 +212,7 @@ def test_adaptive_capped_vs_exact(dev, native):
     DM, DS = dev
     from bondupdategalerkin_b200 import native as DN
 
-    dstep = DN.cbe_bug_step if native else DS.cbe_bug_step
+    dstep = DN.cbe_bug_step
     L, tau = 16, -0.1j
     H = OM.sparse_xxz(L, 1.0, 0.5)
     opsi, dpsi = OM.neel_state(L), DM.neel_state(L)

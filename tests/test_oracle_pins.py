@@ -376,11 +376,9 @@ def test_radau2_gmres_is_radau2(tau):
 
 
 def _krylov_module(which):
-    """The oracle's Krylov routines, or the product's (the Python host's) under the same names."""
-    if which == "product":
-        from bondupdategalerkin_b200 import krylov
-    else:
-        from oracle import krylov
+    """The oracle's Krylov routines."""
+    from oracle import krylov
+
     return krylov
 
 
@@ -406,7 +404,7 @@ def _krylov_error(H, seed, tau, basis, hess, depth):
     return np.linalg.norm(exact - basis[:, :depth] @ reduced)
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_kry_weight_does_not_cancel_on_two_by_two(which):
     """|tau| beta int_0^1 |exp(-2 pi i s)| ds = 1 where one direction leaves an O(1) error."""
     K = _krylov_module(which)
@@ -420,7 +418,7 @@ def test_kry_weight_does_not_cancel_on_two_by_two(which):
     assert w >= err
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_kry_weight_bounds_random_hermitian_errors(which):
     K = _krylov_module(which)
     rng = np.random.default_rng(11)
@@ -441,7 +439,7 @@ def test_kry_weight_bounds_random_hermitian_errors(which):
     assert checked > 30
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_root_tail_is_guarded_over_the_step(which):
     """T_2 = [0 pi; pi 0] from e_1 on [0 pi 0; pi 0 1; 0 1 0]: [exp(-i T_2)]_{2,1} = -i sin(pi) = 0,
     so the endpoint tail vanishes with an O(1) error; the guarded tail samples |sin(pi s)|."""
@@ -467,7 +465,7 @@ def test_root_tail_is_guarded_over_the_step(which):
         assert K.tail_sup(evalcoeff, step, 1.0) == K.tail(evalcoeff(step)[0], 1.0)
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_tridiag_eigen_exact_and_names_non_finite_input(which):
     K = _krylov_module(which)
     d = [0.3, -1.2, 2.5, 0.0, 1e-9]
@@ -521,11 +519,11 @@ def test_step_converges_at_order_p_plus_one(order):
 
 
 def test_bond_work_ceilings_known_answers():
-    """``test_bond_work_ceiling.jl:23-30``, in the oracle and in the product's host bookkeeping."""
-    from bondupdategalerkin_b200 import budget as PB
+    """``test_bond_work_ceiling.jl:23-30`` in the oracle (the native step's ceilings are held to the
+    oracle's by the device parity tests: identical widths and dimensions every step)."""
     from oracle import budget as OB
 
-    for bwc in (OB.bond_work_ceilings, PB.bond_work_ceilings):
+    for bwc in (OB.bond_work_ceilings,):
         assert bwc([1, 3, 8], 2, 1024) == [4, 12, 32]
         assert bwc([0, 5], 4, 1024) == [1, 40]  # never 0, which admits nothing
         assert bwc([1, 3, 8, 40], 2, 16) == [4, 12, 16, 16]
@@ -591,15 +589,12 @@ def test_work_ceilings_bound_every_frame():
 # ── the tolerance budget (test/BUG/Core/RankAdaptation/test_basis_budget.jl) ─────────────────
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_basis_budget_known_answers(which):
     """``test_basis_budget.jl:21-97``: the budget's validation, the RSS allocation rule, tau = 0 as
     a basis question, the indicator's one scaling, the work ceiling and the conservative ledger
-    merge, in the oracle and in the product's host bookkeeping."""
-    if which == "oracle":
-        from oracle import budget as BB
-    else:
-        from bondupdategalerkin_b200 import budget as BB
+    merge, in the oracle (the native step's budget is held to it by the device parity tests)."""
+    from oracle import budget as BB
     b = BB.Budget(1e-5, 1e-7, 1e-10)
     assert (b.basis, b.trunc, b.expv) == (1e-5, 1e-7, 1e-10)
     for bad in ((0.0, 1e-7, 1e-10), (-1e-5, 1e-7, 1e-10), (1e-5, 1e-7, 0.0), (1e-5, -1e-7, 1e-10)):
@@ -640,11 +635,10 @@ def test_basis_budget_known_answers(which):
 def test_retired_knobs_are_refused_before_the_state_is_touched():
     """``test_basis_budget.jl:8-19``: a retired fixed-width knob is no keyword of the step (the
     reference's MethodError is a TypeError here), refused before any evolution, in the oracle
-    and both product hosts."""
+    and the native step."""
     from bondupdategalerkin_b200 import native as N
-    from bondupdategalerkin_b200 import step as P
 
-    for step in (S.cbe_bug_step, N.cbe_bug_step, P.cbe_bug_step):
+    for step in (S.cbe_bug_step, N.cbe_bug_step):
         psi, mpo = M.neel_state(6), M.xxz_mpo(6, J=1.0, delta=0.0)
         dims0 = psi.bond_dims()
         for kw in (dict(tol_basis=1e-5, dex=4), dict(trunc_thresh=1e-10)):
@@ -660,11 +654,9 @@ def test_retired_knobs_are_refused_before_the_state_is_touched():
 def test_expansion_defaults_and_recurrence_resolution():
     """``test_krylov_defaults.jl:21-48``: the DDQRExpansion defaults (oracle and product), the
     recurrence ``auto`` resolves to, an unknown recurrence refused, and the shared stop rule."""
-    from bondupdategalerkin_b200 import krylov as PK
-    from bondupdategalerkin_b200 import step as P
-    from bondupdategalerkin_b200.options import resolve_krylov_recurrence
+    from bondupdategalerkin_b200.options import DDQRExpansion, resolve_krylov_recurrence
 
-    for cls in (S.DDQRExpansion, P.DDQRExpansion):
+    for cls in (S.DDQRExpansion, DDQRExpansion):
         e = cls()
         assert (e.mode, e.fixed_width, e.tail_factor, e.krylov_mode, e.krylov_fixed_depth) == \
             ("rank_tail", 8, 0.10, "auto", 0)
@@ -676,7 +668,7 @@ def test_expansion_defaults_and_recurrence_resolution():
     psi, mpo = M.domain_wall_state(6), M.xxz_mpo(6, J=1.0, delta=0.0)
     with pytest.raises(ValueError):
         S.cbe_bug_step(psi, mpo, -0.1j, expansion=S.DDQRExpansion(krylov_mode="gmres"))
-    for stop in (K.krylov_stop, PK.krylov_stop):
+    for stop in (K.krylov_stop,):
         assert stop(1e-3, 1e-2, 1, 0) == (True, True)     # adaptive: within the allowance
         assert stop(1e-1, 1e-2, 1, 0) == (False, False)   # adaptive: go on
         assert stop(1e-3, 1e-2, 2, 4) == (False, False)   # fixed depth not reached yet
@@ -732,17 +724,13 @@ class _ArrayOps:
         return [complex(np.vdot(v, x)) for v in vs]
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_local_lanczos_and_arnoldi_chains(which):
     """``test_local_lanczos.jl``: on random Hermitian generators (n = 24, 40; |tau| = 0.1, 1, 4)
     both chains close, their bases capture exp(tau H) seed to 2e-7, the Lanczos basis is
     orthonormal to 1e-7 and its depth within 4 of Arnoldi's; a fixed depth that misses the
-    tolerance reports itself capped, not closed. The product's chains (the Python host's) run on
-    the same plain vectors."""
-    if which == "product":
-        from bondupdategalerkin_b200 import krylov as K  # noqa: N811
-    else:
-        from oracle import krylov as K  # noqa: N811
+    tolerance reports itself capped, not closed."""
+    from oracle import krylov as K  # noqa: N811
     rng = np.random.default_rng(45912)
     ops = _ArrayOps()
     for n in (24, 40):
@@ -871,7 +859,7 @@ def test_inner_products_against_dense_and_across_charges():
     assert _inner(a, c) == 0
 
 
-@pytest.mark.parametrize("which", ["oracle", "product"])
+@pytest.mark.parametrize("which", ["oracle"])
 def test_ite_schedule_grids(which):
     """``test_schedules.jl`` (IT-U1): log-panel grids reach beta_max without gaps, uniform inside a
     panel, the first two panels equal and then doubling, the first step beta_max / (2^(P-1) k),
@@ -928,29 +916,3 @@ def test_fused_sectors_cover_the_frames_charges():
             saw_charged |= any(q != 0 for q in la.sectors)
     assert saw_charged
 
-
-def test_probe_column_rules_agree_with_the_oracle():
-    """The DD probe's column allocation (proportional, ceiling, capped by the sector), the targeted
-    boost (``_boost!``, ``cbe.jl:206-216``: capped, the remainder returned) and the rank cut, in
-    the Python host's ``cbe.py`` against the oracle on random sector layouts."""
-    from bondupdategalerkin_b200 import cbe as PC
-    from oracle import cbe as OC
-
-    rng = np.random.default_rng(17)
-    for _ in range(300):
-        dims = {int(q): int(d) for q, d in zip(rng.choice(np.arange(-6, 7), 5, replace=False),
-                                               rng.integers(0, 40, 5))}
-        budget = int(rng.integers(-2, 120))
-        a = OC.alloc_columns(dims, budget)
-        assert a == PC.alloc_columns(dims, budget)
-        assert all(0 <= a[q] <= dims[q] for q in dims)
-        if budget > 0 and sum(dims.values()) > 0:
-            assert sum(a.values()) >= min(budget, sum(dims.values()))
-        boost = {q: int(rng.integers(-3, 20)) for q in list(dims)[:3]}
-        boost[99] = 5  # a sector with no cap is skipped
-        ca, cb = dict(a), dict(a)
-        la, lb = OC.boost_columns(ca, boost, dims), PC.boost_columns(cb, boost, dims)
-        assert (ca, la) == (cb, lb)
-        assert all(ca[q] <= max(dims[q], a[q]) for q in dims)
-    for args in ((1e-6, 2.0, 0.5), (0.0, 2.0, 0.5), (0.0, 1e-3, 1e-3)):
-        assert OC.rank_cut(*args) == PC.rank_cut(*args)

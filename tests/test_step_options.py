@@ -1,7 +1,7 @@
 """The step's keyword checks against the reference's (``bug_step_stages.jl:40-142``), on CPU.
 
-Every keyword of ``cbe_bug_step!`` is accepted by name. The oracle and both product hosts (the
-native step's Python entry and the Python host) must refuse what the reference refuses
+Every keyword of ``cbe_bug_step!`` is accepted by name. The oracle and the native step's Python
+entry must refuse what the reference refuses
 (``ArgumentError`` / ``DimensionMismatch`` -> ``ValueError``) and name what they do not build
 (``NotImplementedError``), with the same outcome for the same keywords. The checks run before any
 device work, so the product hosts are called here with the oracle's chain objects and never reach
@@ -61,9 +61,8 @@ def _args(kw):
 
 def _hosts():
     from bondupdategalerkin_b200 import native as N
-    from bondupdategalerkin_b200 import step as P
 
-    return [("oracle", S.cbe_bug_step), ("native", N.cbe_bug_step), ("python-host", P.cbe_bug_step)]
+    return [("oracle", S.cbe_bug_step), ("native", N.cbe_bug_step)]
 
 
 @pytest.mark.parametrize("kw,exc", BAD, ids=[repr(k) for k, _ in BAD])
