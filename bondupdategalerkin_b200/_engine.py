@@ -29,7 +29,7 @@ SIGNATURES = {
     "bug_ctx_stream": (_vp, [_vp]),
     "bug_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
     "bug_ctx_set_mixed": (ctypes.c_int, [_vp, ctypes.c_int]),
-    "bug_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _vp]),
+    "bug_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp]),
     "bug_batch_context": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "bug_batch_launches": (ctypes.c_int64, [_vp]),
     "bug_batch_destroy": (ctypes.c_int, [_vp]),

@@ -301,9 +301,10 @@ _STEP_DEFAULTS = dict(tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=No
 
 
 class Batch:
-    """Chains stepped together (``bug_step_batch``): ``n`` engine contexts on one shared stream,
-    one host thread per chain, and the small stages the chains queue between their read-backs
-    merged into shared launches (a thread-block cluster per chain). Build chain ``i``'s state and
+    """Chains stepped together (``bug_step_batch``): ``n`` engine contexts and one host thread per
+    chain, so the chains' host work and kernels overlap; with ``combine`` the contexts share one
+    stream and the small stages the chains queue between their read-backs are merged into shared
+    launches (a thread-block cluster per chain). Build chain ``i``'s state and
     MPO on ``contexts[i]`` (``tensor.from_blocks(..., ctx)``); each chain's result is the same as
     its own ``cbe_bug_step``. The batch is torn down when the last reference to it or to a tensor
     on its contexts goes away (tensors hold their context, which holds the batch)."""
@@ -317,10 +318,10 @@ class Batch:
                 self.lib.bug_batch_destroy(self.h)
                 self.h = None
 
-    def __init__(self, n: int, device: int = 0):
+    def __init__(self, n: int, device: int = 0, combine: bool = False):
         lib = _lib()
         h = ctypes.c_void_p()
-        E.check(lib.bug_batch_create(int(device), int(n), ctypes.byref(h)))
+        E.check(lib.bug_batch_create(int(device), int(n), int(bool(combine)), ctypes.byref(h)))
         self._handle = Batch._Handle(lib, h)
         self.h, self.n, self.lib = h, int(n), lib
         self.contexts = []

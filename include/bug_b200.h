@@ -420,15 +420,17 @@ int64_t bug_projected_footprint(int L, int d, int maxdim, int mpo_dim);
 /* ── batched steps ──────────────────────────────────────────────────────────────────────────
  * Many independent chains stepped together (the batched caller of `cbe_bug_step!`,
  * src/BUG/TimeEvolution/bug_step.jl:17-513, which the reference runs one chain at a time). A batch
- * owns n engine contexts on ONE shared stream and n host threads; each chain's sweep logic runs on
- * its own thread and context, and the small stages each chain queues between its read-backs are
- * merged with the other chains' into one launch (a thread-block cluster per chain), so the device
- * sees one launch per round of all chains' stage lists. Every chain's result is bit-identical to
- * its own bug_mps_step (the kernels are deterministic, each chain draws from its own generator).
- * Build chain i's state and MPO on bug_batch_context(b, i); a chain's tensors must stay on its
- * context and be freed before bug_batch_destroy. Up to 128 chains. */
+ * owns n engine contexts and n host threads; each chain's sweep logic runs on its own thread and
+ * context, so the chains' host work and their kernels overlap. With `combine` != 0 the contexts
+ * share ONE stream and the small stages each chain queues between its read-backs are merged with
+ * the other chains' into one launch (a thread-block cluster per chain); with 0 (recommended: on
+ * B200 a stream per chain measured 3x the throughput) each context keeps its own stream. Every
+ * chain's result is bit-identical to its own bug_mps_step either way (the kernels are
+ * deterministic, each chain draws from its own generator). Build chain i's state and MPO on
+ * bug_batch_context(b, i); a chain's tensors must stay on its context and be freed before
+ * bug_batch_destroy. Up to 128 chains. */
 typedef struct bug_batch bug_batch;
-int bug_batch_create(int device, int n, bug_batch** out);
+int bug_batch_create(int device, int n, int combine, bug_batch** out);
 int bug_batch_context(bug_batch* b, int i, bug_ctx** out);
 /* One step of chains 0..n-1 (n <= the batch's size), each argument indexed by chain as
  * bug_mps_step's; status[i] is chain i's return code, and the call returns the first failing code

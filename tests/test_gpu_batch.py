@@ -1,8 +1,8 @@
 """Chains stepped together (``bug_step_batch``) against the same chains stepped one at a time (GPU).
 
-A batch runs every chain's sweep logic on its own host thread and context, with all contexts on
-one stream and the chains' queued stages merged into shared launches (one thread-block cluster per
-chain). The kernels are deterministic and each chain draws from its own generator, so every chain
+A batch runs every chain's sweep logic on its own host thread and context: each with its own
+stream, or (``combine``) all on one stream with the chains' queued stages merged into shared
+launches (one thread-block cluster per chain). The kernels are deterministic and each chain draws from its own generator, so every chain
 must come out bit-identical to its own ``cbe_bug_step``: the same bond dimensions, verdicts and
 site tensors to the last bit, at every step. The chains differ in length, anisotropy, start state
 and maxdim, so their stage lists differ in length and shape within each merged launch.
@@ -30,14 +30,15 @@ def _on_ctx(t, ctx):
     return DT.from_blocks(legs, blocks, ctx)
 
 
-def test_batch_matches_solo_steps():
+@pytest.mark.parametrize("combine", [False, True], ids=["stream-per-chain", "merged-launches"])
+def test_batch_matches_solo_steps(combine):
     from bondupdategalerkin_b200 import build
     from bondupdategalerkin_b200 import models as DM
     from bondupdategalerkin_b200 import native as DN
     from bondupdategalerkin_b200 import tensor as DT
 
     build.build()
-    batch = DN.Batch(len(CHAINS))
+    batch = DN.Batch(len(CHAINS), combine=combine)
     bat, bat_mpo = [], []
     solo, solo_mpo, srng, brng = [], [], [], []
     for i, (L, delta, start, maxdim, seed) in enumerate(CHAINS):
