@@ -11,6 +11,8 @@
   ``tdvp2_step_host`` its host-buffer form;
 * ``ite_step`` / ``ite_evolve`` and the step schedules -- normalised imaginary time
   (``src/BUG/ITE/ite_step.jl``, ``schedules.jl``);
+* ``qtt_bug_step`` -- ``qtt_bug_step!`` for a linear flow (the rational-root BUG step,
+  ``src/QTTS/Tooling/nonlinear_step.jl``);
 * the quantics builders under the reference's names: ``qtt_grid``, ``qtt_separable``, ``qtt_mps``,
   ``qtt_shift``, ``qtt_derivative``, ``qtt_to_mpo``, ``HestonParams``, ``heston_op``,
   ``heston_mpo`` (``src/QTTS/Tooling``, ``src/QTTS/Models/Heston``).
@@ -23,8 +25,8 @@ from .ite import (beta_grid, geometric_schedule, ite_energy, ite_evolve, ite_ste
                   uniform_beta_steps, uniform_schedule)
 from .native import Batch, cbe_bug_step, tdvp2_step
 from .options import DDQRExpansion
-from .qtt import (HestonParams, heston_mpo, heston_op, qtt_derivative, qtt_grid, qtt_mps,
-                  qtt_separable, qtt_shift, qtt_to_mpo)
+from .qtt import (HestonParams, heston_mpo, heston_op, qtt_bug_step, qtt_derivative, qtt_grid, qtt_mps,
+                  qtt_separable, qtt_shift, qtt_step_tolerance, qtt_to_mpo)
 from .tensor import from_blocks, to_blocks
 
 __all__ = ["cbe_bug_step", "Batch", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
@@ -32,7 +34,7 @@ __all__ = ["cbe_bug_step", "Batch", "step_host", "magnetisation", "DDQRExpansion
            "tdvp2_step_host", "ite_step", "ite_step_host", "ite_evolve", "ite_energy", "log_panel_steps",
            "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule",
            "qtt_grid", "qtt_separable", "qtt_mps", "qtt_shift", "qtt_derivative", "qtt_to_mpo",
-           "HestonParams", "heston_op", "heston_mpo"]
+           "HestonParams", "heston_op", "heston_mpo", "qtt_bug_step", "qtt_step_tolerance"]
 
 
 def magnetisation(psi):

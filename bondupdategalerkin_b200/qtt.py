@@ -375,3 +375,74 @@ def heston_op(g: Grid, p: HestonParams, adjoint=False):
 def qtt_to_mpo(cores) -> MPO:
     """``qtt_to_mpo`` (``state_adapter.jl:96-109``): operator cores as the solver MPO on device."""
     return cores_to_mpo(cores)
+
+
+# ── the QTT BUG step of a linear flow (src/QTTS/Tooling/nonlinear_step.jl) ───────────────────
+
+QTT_KRYLOV_MARGIN = 0.5       # _QTT_KRYLOV_MARGIN, nonlinear_step.jl:8
+QTT_RATIONAL_MAXITER = 200    # _QTT_RATIONAL_MAXITER, nonlinear_step.jl:17
+QTT_TOL_FLOOR = 1e-14         # _QTT_TOL_FLOOR, nonlinear_step.jl:23
+_QTT_ROOTS = {2: "trapezoid", 3: "radau2", 4: "radau3"}  # qtt_root_for_order, stage_solvers.jl:161-165
+
+
+def qtt_step_tolerance(tol, h, order, scaling="order", h_ref=0.1):
+    """``qtt_step_tolerance`` (``nonlinear_step.jl:25-47``): the per-step value of a tolerance,
+    ``tol (|h| / h_ref)^(order + 1)`` (never looser than ``tol``) floored at 1e-14 unless ``tol``
+    is already below it; ``scaling = "fixed"`` returns ``tol``."""
+    if scaling not in ("order", "fixed"):
+        raise ValueError(f"tol_scaling must be :order or :fixed, got :{scaling}")
+    if not h_ref > 0:
+        raise ValueError(f"tol_h_ref must be positive, got {h_ref}")
+    if scaling == "fixed" or tol == 0:
+        return float(tol)
+    factor = min(1.0, (abs(float(h)) / float(h_ref)) ** (order + 1))
+    return max(float(tol) * factor, min(float(tol), QTT_TOL_FLOOR))
+
+
+def qtt_root_for_order(order):
+    """The rational root of BUG order 2, 3, 4: trapezoid, Radau IIA (2 stages), Radau IIA (3)."""
+    if order not in _QTT_ROOTS:
+        raise ValueError(f"nonlinear BUG orders are 2, 3, 4; got {order}")
+    return _QTT_ROOTS[order]
+
+
+def qtt_bug_step(psi, mpo, t, h, *, pref=1.0, order=2, root=None, tol_stage=1e-10, tol_basis=1e-6,
+                 tol_trunc=1e-8, maxdim=128, stage_solver="auto", tol_scaling="order",
+                 tol_h_ref=0.1, tol_krylov=None, rng=None, **kwargs):
+    """``qtt_bug_step!(psi, fl, t, h; ...)`` (``src/QTTS/Tooling/nonlinear_step.jl:102-371``) for a
+    linear flow ``F = pref H psi`` with ``H`` the operator of ``mpo`` (``LinearFlow``,
+    ``src/BUG/TimeEvolution/flows.jl:20-31``), in place on the device. For a linear flow
+    ``stage_solver = "auto"`` is ``krylov_rational``: one native BUG step (``bug_mps_step``) at
+    ``order`` whose root is the rational stability function ``root`` (trapezoid / Radau IIA) of
+    the Galerkin operator on its Arnoldi basis, applied unshifted (``root_shift = False``, at most
+    200 Arnoldi vectors), then compressed; the tolerances are ``qtt_step_tolerance`` values. The
+    Newton-GMRES stage equations of nonlinear flows (``stage_solver = "newton_gmres"``) are not built.
+    ``t`` is the start time (a linear flow does not depend on it). Returns the step report:
+    ``converged`` (the root's Krylov error within the stage tolerance), ``residual``, ``krylov``,
+    ``discarded``, ``chi``, ``rank_capped``, ``tol_step`` and the step's ``info``."""
+    if stage_solver not in ("auto", "krylov_rational", "newton_gmres"):
+        raise ValueError("stage_solver must be :auto, :newton_gmres or :krylov_rational, "
+                         f"got :{stage_solver}")
+    if stage_solver == "newton_gmres":
+        raise NotImplementedError("stage_solver = :newton_gmres (the nonlinear stage equations)")
+    from .native import cbe_bug_step
+
+    root = qtt_root_for_order(order) if root is None else root
+
+    def st(tol):
+        return qtt_step_tolerance(tol, h, order, scaling=tol_scaling, h_ref=tol_h_ref)
+
+    tol_step = dict(basis=st(tol_basis), trunc=st(tol_trunc), stage=st(tol_stage),
+                    scaling=tol_scaling, h_ref=float(tol_h_ref))
+    tol_kry = st(QTT_KRYLOV_MARGIN * tol_basis if tol_krylov is None else tol_krylov)
+    info = cbe_bug_step(psi, mpo, complex(pref * h), order=order, tol_basis=tol_step["basis"],
+                        tol_trunc=tol_step["trunc"], maxdim=maxdim, hermitian=False, eshift=0.0,
+                        tol_krylov=tol_kry, root_method=root, tol_root=tol_step["stage"],
+                        root_shift=False, root_maxiter=QTT_RATIONAL_MAXITER, truncate=True,
+                        rng=rng, **kwargs)
+    err = info["ledger"].expv_err
+    chi = max(psi.bond_dims())
+    return dict(solver="krylov_rational", root=root, order=order, converged=err <= tol_step["stage"],
+                residual=err, krylov=info["ledger"].expv_iters, discarded=info["discarded"],
+                chi=chi, rank_capped=chi >= maxdim, tol_step=tol_step, bond_dims=info["bond_dims"],
+                status=info["status"], info=info)

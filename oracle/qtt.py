@@ -334,3 +334,68 @@ def mpo_dense(cores) -> np.ndarray:
             M = np.einsum("OIw,woir->oOiIr", M, c)
             M = M.reshape(M.shape[0] * M.shape[1], M.shape[2] * M.shape[3], M.shape[4])
     return M[:, :, 0]
+
+
+# ── the QTT BUG step of a linear flow (src/QTTS/Tooling/nonlinear_step.jl) ───────────────────
+
+QTT_KRYLOV_MARGIN = 0.5       # _QTT_KRYLOV_MARGIN, nonlinear_step.jl:8
+QTT_RATIONAL_MAXITER = 200    # _QTT_RATIONAL_MAXITER, nonlinear_step.jl:17
+QTT_TOL_FLOOR = 1e-14         # _QTT_TOL_FLOOR, nonlinear_step.jl:23
+
+
+def qtt_step_tolerance(tol, h, order, scaling="order", h_ref=0.1):
+    """``qtt_step_tolerance`` (``nonlinear_step.jl:25-47``): ``tol (|h| / h_ref)^(order + 1)``
+    (never looser than ``tol``), floored at 1e-14 unless ``tol`` is already below it; ``fixed``
+    returns ``tol``."""
+    if scaling not in ("order", "fixed"):
+        raise ValueError(f"tol_scaling must be :order or :fixed, got :{scaling}")
+    if not h_ref > 0:
+        raise ValueError(f"tol_h_ref must be positive, got {h_ref}")
+    if scaling == "fixed" or tol == 0:
+        return float(tol)
+    factor = min(1.0, (abs(float(h)) / float(h_ref)) ** (order + 1))
+    return max(float(tol) * factor, min(float(tol), QTT_TOL_FLOOR))
+
+
+def qtt_root_for_order(order):
+    """``qtt_root_for_order`` (``stage_solvers.jl:161-165``): 2 trapezoid, 3 Radau IIA (2 stages),
+    4 Radau IIA (3 stages)."""
+    roots = {2: "trapezoid", 3: "radau2", 4: "radau3"}
+    if order not in roots:
+        raise ValueError(f"nonlinear BUG orders are 2, 3, 4; got {order}")
+    return roots[order]
+
+
+def qtt_bug_step(psi, mpo, t, h, *, pref=1.0, order=2, root=None, tol_stage=1e-10, tol_basis=1e-6,
+                 tol_trunc=1e-8, maxdim=128, stage_solver="auto", tol_scaling="order",
+                 tol_h_ref=0.1, tol_krylov=None, rng=None, **kwargs):
+    """``qtt_bug_step!`` (``nonlinear_step.jl:102-371``) for a linear flow ``F = pref H psi``
+    (``LinearFlow``, ``flows.jl:20-31``, with ``H`` the operator of ``mpo``): ``stage_solver =
+    :auto`` is ``:krylov_rational`` there, i.e. ``cbe_bug_step!`` at ``order`` with the rational root
+    ``root`` (trapezoid / Radau IIA stability function on the Arnoldi basis of the Galerkin operator)
+    applied unshifted, capped at 200 Arnoldi vectors, then compressed (``nonlinear_step.jl:238-250,
+    327-371``). The tolerances are per-step ``qtt_step_tolerance`` values. The Newton-GMRES stage path
+    of nonlinear flows is not restated. Returns the step report (``converged``: the root's Krylov
+    error within the stage tolerance)."""
+    if stage_solver not in ("auto", "krylov_rational", "newton_gmres"):
+        raise ValueError("stage_solver must be :auto, :newton_gmres or :krylov_rational, "
+                         f"got :{stage_solver}")
+    if stage_solver == "newton_gmres":
+        raise NotImplementedError("stage_solver = :newton_gmres (the nonlinear stage equations)")
+    root = qtt_root_for_order(order) if root is None else root
+    st = lambda tol: qtt_step_tolerance(tol, h, order, scaling=tol_scaling, h_ref=tol_h_ref)  # noqa: E731
+    tol_step = dict(basis=st(tol_basis), trunc=st(tol_trunc), stage=st(tol_stage),
+                    scaling=tol_scaling, h_ref=float(tol_h_ref))
+    tol_kry = st(QTT_KRYLOV_MARGIN * tol_basis if tol_krylov is None else tol_krylov)
+    from oracle import step as S
+
+    info = S.cbe_bug_step(psi, mpo, complex(pref * h), order=order, tol_basis=tol_step["basis"],
+                          tol_trunc=tol_step["trunc"], maxdim=maxdim, hermitian=False, eshift=0.0,
+                          tol_krylov=tol_kry, root_method=root, tol_root=tol_step["stage"],
+                          root_shift=False, root_maxiter=QTT_RATIONAL_MAXITER, truncate=True,
+                          rng=rng, **kwargs)
+    err = info["ledger"].expv_err
+    return dict(solver="krylov_rational", root=root, order=order, converged=err <= tol_step["stage"],
+                residual=err, krylov=info["ledger"].expv_iters, discarded=info["discarded"],
+                chi=max(psi.bond_dims()), rank_capped=max(psi.bond_dims()) >= maxdim,
+                tol_step=tol_step, bond_dims=info["bond_dims"], status=info["status"], info=info)

@@ -149,3 +149,50 @@ def test_heston_backward_fixture():
     dense = Q.qtt_dense(mps_to_host(dpsi))
     err = np.linalg.norm(dense - ref) / np.linalg.norm(ref)
     assert err < 1e-4, err
+
+
+def test_qtt_bug_step_linear_flow_on_device():
+    """``qtt_bug_step!`` on the Heston linear flow (the rational Radau IIA(2) root, unshifted) on the
+    device from the reference's frozen Heston backward start (5 + 5 bits, ten steps of 0.02,
+    tol_basis 1e-8, work ceiling at maxdim): step for step the oracle's dimensions, verdicts, root
+    iterations and state (infidelity <= 1e-12, norm within 1e-10), and the final state within 5e-8
+    of the frozen one (the oracle: 7.1e-9)."""
+    import json
+    import os
+
+    from bondupdategalerkin_b200 import build
+
+    build.build()
+    from bondupdategalerkin_b200 import qtt as P
+
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "b155550.json")))
+    d = d["qtt_heston_backward"]
+    ref = np.array(d["final_state"]["re"]) + 1j * np.array(d["final_state"]["im"])
+
+    def payoff(x):
+        z = (np.exp(x) - 1.0) / 0.02
+        return 0.02 * (z if z > 30 else np.log1p(np.exp(z)))
+
+    dom = dict(x=(-3.0, 3.0), y=(0.0, 1.0), periodic_x=False, periodic_y=False)
+    hp = (0.03, 0.0, 1.5, 0.09, 0.5, -0.7)
+    og, pg = Q.qtt_grid(d["N"], d["N"], **dom), P.qtt_grid(d["N"], d["N"], **dom)
+    opsi = Q.qtt_mps(Q.qtt_separable(og, payoff, lambda v: 1.0, tol=1e-12))
+    dpsi = P.qtt_mps(P.qtt_separable(pg, payoff, lambda v: 1.0, tol=1e-12))
+    ompo, dmpo = Q.heston_mpo(og, Q.HestonParams(*hp)), P.heston_mpo(pg, P.HestonParams(*hp))
+    orng, drng = np.random.default_rng(1234), np.random.default_rng(1234)
+    kw = dict(order=d["order"], maxdim=64, tol_trunc=1e-10, tol_stage=1e-9, tol_basis=1e-8,
+              tol_scaling="fixed", work_ceiling_rule="maxdim")
+    h = d["h"]
+    for k in range(d["steps"]):
+        orep = Q.qtt_bug_step(opsi, ompo, k * h, h, rng=orng, **kw)
+        drep = P.qtt_bug_step(dpsi, dmpo, k * h, h, rng=drng, **kw)
+        assert drep["bond_dims"] == orep["bond_dims"], k
+        assert drep["status"] == orep["status"] and drep["converged"], k
+        assert drep["krylov"] == orep["krylov"], k
+        hst = mps_to_host(dpsi)
+        ab = overlap(hst, opsi)
+        aa, bb = overlap(hst, hst).real, overlap(opsi, opsi).real
+        assert 1.0 - abs(ab) ** 2 / (aa * bb) <= 1e-12, k
+        assert abs(np.sqrt(aa) - np.sqrt(bb)) <= 1e-10 * np.sqrt(bb), k
+    dense = Q.qtt_dense(mps_to_host(dpsi))
+    assert np.linalg.norm(dense - ref) / np.linalg.norm(ref) < 5e-8

@@ -15,6 +15,7 @@ import json
 import os
 
 import numpy as np
+import pytest
 import scipy.linalg as sl
 
 from oracle import qtt as Q
@@ -255,3 +256,51 @@ def test_public_api_names_the_quantics_builders():
     dom = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
     op = api.heston_op(api.qtt_grid(4, 4, **dom), api.HestonParams(*HP_FIELDS))
     assert relerr(Q.mpo_dense(op), Q.heston_dense(heston_grid(4, 4), HP)) < 1e-11
+
+
+def test_qtt_step_tolerance_known_answers():
+    """``qtt_step_tolerance`` (``nonlinear_step.jl:25-47``): the order-scaled per-step tolerance,
+    never looser than the passed one, floored at 1e-14, ``fixed`` untouched; bad settings refused."""
+    for mod in (Q, __import__("bondupdategalerkin_b200.qtt", fromlist=["qtt"])):
+        assert mod.qtt_step_tolerance(1e-6, 0.05, 2) == pytest.approx(1e-6 * 0.5 ** 3)
+        assert mod.qtt_step_tolerance(1e-6, 0.2, 2) == 1e-6          # a longer step keeps tol
+        assert mod.qtt_step_tolerance(1e-6, 1e-4, 3) == 1e-14        # the floor
+        assert mod.qtt_step_tolerance(1e-16, 1e-4, 3) == 1e-16       # already below the floor
+        assert mod.qtt_step_tolerance(1e-6, 0.01, 2, scaling="fixed") == 1e-6
+        assert mod.qtt_step_tolerance(0.0, 0.01, 2) == 0.0
+        with pytest.raises(ValueError):
+            mod.qtt_step_tolerance(1e-6, 0.01, 2, scaling="none")
+        with pytest.raises(ValueError):
+            mod.qtt_step_tolerance(1e-6, 0.01, 2, h_ref=0.0)
+        assert [mod.qtt_root_for_order(p) for p in (2, 3, 4)] == ["trapezoid", "radau2", "radau3"]
+        with pytest.raises(ValueError):
+            mod.qtt_root_for_order(5)
+
+
+def test_qtt_bug_step_linear_flow_reaches_the_fixture():
+    """``qtt_bug_step!`` on the Heston linear flow (``krylov_rational``: the order-3 step's root is
+    the Radau IIA(2) stability function, unshifted) from the fixture's start: with tol_basis 1e-8
+    and the work ceiling at maxdim, each step stays within 1e-8 of the dense Radau IIA(2) step and
+    the tenth lands within 5e-8 of the frozen final state (7.1e-9 measured; the frozen state itself
+    is 7.2e-9 from the dense Radau run); every step meets its tolerances and converges. The stage
+    solver of nonlinear flows is refused as not built."""
+    d, ref, g = _heston_backward_fixture()
+    h = d["h"]
+    mpo = Q.heston_mpo(g, HESTON_BACKWARD)
+    psi = Q.qtt_mps(Q.qtt_separable(g, _payoff, lambda v: 1.0, tol=1e-12))
+    H = Q.heston_dense(g, HESTON_BACKWARD)
+    hH, eye = h * H, np.eye(H.shape[0])
+    R = np.linalg.solve(eye - 2 * hH / 3 + hH @ hH / 6, eye + hH / 3)
+    v = Q.qtt_dense(psi)
+    rng = np.random.default_rng(1234)
+    for k in range(d["steps"]):
+        rep = Q.qtt_bug_step(psi, mpo, k * h, h, order=d["order"], maxdim=64, tol_trunc=1e-10,
+                             tol_stage=1e-9, tol_basis=1e-8, tol_scaling="fixed",
+                             work_ceiling_rule="maxdim", rng=rng)
+        v = R @ v
+        assert rep["solver"] == "krylov_rational" and rep["root"] == "radau2"
+        assert rep["converged"] and rep["status"] == "met", (k, rep["residual"], rep["status"])
+        assert relerr(Q.qtt_dense(psi), v) < 1e-8, k
+    assert relerr(Q.qtt_dense(psi), ref) < 5e-8
+    with pytest.raises(NotImplementedError):
+        Q.qtt_bug_step(psi, mpo, 0.0, h, order=3, stage_solver="newton_gmres")
