@@ -15,6 +15,7 @@ namespace {
 
 constexpr int kThreads = kStageThreads;
 constexpr int kSmCount = 148;  // B200: 2 dies x 74 SMs
+constexpr int kElemUnroll = 4;  // elements per thread and pass of the element-wise stages
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -76,33 +77,53 @@ struct Rebase {
 // a single-stage launch, or one cluster of a stage list).
 __device__ void copy_stage(const Rebase& rb, const CopyDesc* d, int nd, int64_t total, int cta,
                            int ncta) {
-  for (int64_t e = cta * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(ncta) * blockDim.x) {
-    const CopyDesc& c = d[find_desc(d, nd, e)];
-    int64_t r = e - c.prefix;
-    int64_t so = 0, dof = 0;
-    int64_t widx = 0;
-    for (int k = c.ndim - 1; k >= 0; --k) {
-      int64_t i = r % c.dims[k];
-      r /= c.dims[k];
-      so += i * c.sstr[k];
-      dof += i * c.dstr[k];
-      if (k == c.wdim) widx = i;
+  // a thread takes up to kElemUnroll elements per pass (a stride apart) and issues all their loads
+  // before any store, so a small grid (one cluster of a stage list) waits for one L2 round trip per
+  // pass instead of one per element; each element's arithmetic is unchanged
+  const int64_t step = int64_t(ncta) * blockDim.x;
+  for (int64_t e0 = cta * int64_t(blockDim.x) + threadIdx.x; e0 < total; e0 += step * kElemUnroll) {
+    double2 v[kElemUnroll], o[kElemUnroll];
+    double2* dp[kElemUnroll];
+    bool acc[kElemUnroll];
+#pragma unroll
+    for (int u = 0; u < kElemUnroll; ++u) {
+      const int64_t e = e0 + u * step;
+      dp[u] = nullptr;
+      acc[u] = false;
+      if (e >= total) continue;
+      const CopyDesc& c = d[find_desc(d, nd, e)];
+      int64_t r = e - c.prefix;
+      int64_t so = 0, dof = 0;
+      int64_t widx = 0;
+      for (int k = c.ndim - 1; k >= 0; --k) {
+        int64_t i = r % c.dims[k];
+        r /= c.dims[k];
+        so += i * c.sstr[k];
+        dof += i * c.dstr[k];
+        if (k == c.wdim) widx = i;
+      }
+      double2 x = c.src ? ldg2(c.src + so) : make_double2(0.0, 0.0);
+      if (c.conj) x.y = -x.y;
+      if (c.w) {
+        const double sc = __ldcg(rb(c.w) + widx);
+        x.x *= sc;
+        x.y *= sc;
+      }
+      v[u] = cmul(c.alpha, x);
+      dp[u] = c.dst + dof;
+      acc[u] = c.accumulate != 0;
+      if (acc[u]) o[u] = ldg2(dp[u]);
     }
-    double2 v = c.src ? ldg2(c.src + so) : make_double2(0.0, 0.0);
-    if (c.conj) v.y = -v.y;
-    if (c.w) {
-      const double s = __ldcg(rb(c.w) + widx);
-      v.x *= s;
-      v.y *= s;
+#pragma unroll
+    for (int u = 0; u < kElemUnroll; ++u) {
+      if (!dp[u]) continue;
+      double2 w = v[u];
+      if (acc[u]) {
+        w.x += o[u].x;
+        w.y += o[u].y;
+      }
+      *dp[u] = w;
     }
-    double2 w = cmul(c.alpha, v);
-    if (c.accumulate) {
-      double2 o = ldg2(c.dst + dof);
-      w.x += o.x;
-      w.y += o.y;
-    }
-    c.dst[dof] = w;
   }
 }
 
@@ -234,21 +255,34 @@ __device__ void dot_reduce(const int* seg, int nout, const double2* partial, dou
 
 __device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, int64_t total,
                               int cta, int ncta) {
-  for (int64_t e = cta * int64_t(blockDim.x) + threadIdx.x; e < total;
-       e += int64_t(ncta) * blockDim.x) {
-    const LinOut& o = outs[find_desc(outs, nout, e)];
-    const int64_t i = e - o.prefix;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int s = o.src_begin; s < o.src_end; ++s) {
-      double2 cf = srcs[s].coef;
-      if (srcs[s].cmode) {
-        const double x = __ldcg(srcs[s].cref);
-        const double r = sqrt(fmax(x, 0.0));
-        cf = make_double2(srcs[s].cmode == 1 ? -x : (srcs[s].cmode == 2 ? 1.0 / r : -r), 0.0);
+  // as copy_stage: up to kElemUnroll elements per thread and pass, loads before stores
+  const int64_t step = int64_t(ncta) * blockDim.x;
+  for (int64_t e0 = cta * int64_t(blockDim.x) + threadIdx.x; e0 < total; e0 += step * kElemUnroll) {
+    double2 res[kElemUnroll];
+    double2* dp[kElemUnroll];
+#pragma unroll
+    for (int u = 0; u < kElemUnroll; ++u) {
+      const int64_t e = e0 + u * step;
+      dp[u] = nullptr;
+      if (e >= total) continue;
+      const LinOut& o = outs[find_desc(outs, nout, e)];
+      const int64_t i = e - o.prefix;
+      double2 acc = make_double2(0.0, 0.0);
+      for (int s = o.src_begin; s < o.src_end; ++s) {
+        double2 cf = srcs[s].coef;
+        if (srcs[s].cmode) {
+          const double x = __ldcg(srcs[s].cref);
+          const double r = sqrt(fmax(x, 0.0));
+          cf = make_double2(srcs[s].cmode == 1 ? -x : (srcs[s].cmode == 2 ? 1.0 / r : -r), 0.0);
+        }
+        cfma(acc, cf, ldg2(srcs[s].src + i));
       }
-      cfma(acc, cf, ldg2(srcs[s].src + i));
+      res[u] = acc;
+      dp[u] = o.dst + i;
     }
-    o.dst[i] = acc;
+#pragma unroll
+    for (int u = 0; u < kElemUnroll; ++u)
+      if (dp[u]) *dp[u] = res[u];
   }
 }
 
