@@ -154,9 +154,15 @@ def test_heston_backward_fixture():
 def test_qtt_bug_step_linear_flow_on_device():
     """``qtt_bug_step!`` on the Heston linear flow (the rational Radau IIA(2) root, unshifted) on the
     device from the reference's frozen Heston backward start (5 + 5 bits, ten steps of 0.02,
-    tol_basis 1e-8, work ceiling at maxdim): step for step the oracle's dimensions, verdicts, root
-    iterations and state (infidelity <= 1e-12, norm within 1e-10), and the final state within 5e-8
-    of the frozen one (the oracle: 7.1e-9)."""
+    tol_basis 1e-8, work ceiling at maxdim), the product's MPO against the oracle's.
+
+    The root's Arnoldi stop on this generator is a near tie: the oracle's own iteration count moves
+    between 7 and 11 (steps 8, 9) or 11 and 12 (step 6) when its MPO cores are perturbed at 1e-14
+    (another compression of the same generator), and the enrichment widths move with it, which
+    parts the Gaussian streams from there on. So every step holds the device to the oracle's
+    bond dimensions exactly, to its verdict and Arnoldi count or those of one of six perturbed
+    oracle copies, to a converged root, and to the oracle's state (infidelity <= 1e-12, norm
+    within 1e-10); the final state lies within 5e-8 of the frozen one (the oracle: 7.1e-9)."""
     import json
     import os
 
@@ -176,19 +182,25 @@ def test_qtt_bug_step_linear_flow_on_device():
     dom = dict(x=(-3.0, 3.0), y=(0.0, 1.0), periodic_x=False, periodic_y=False)
     hp = (0.03, 0.0, 1.5, 0.09, 0.5, -0.7)
     og, pg = Q.qtt_grid(d["N"], d["N"], **dom), P.qtt_grid(d["N"], d["N"], **dom)
-    opsi = Q.qtt_mps(Q.qtt_separable(og, payoff, lambda v: 1.0, tol=1e-12))
-    dpsi = P.qtt_mps(P.qtt_separable(pg, payoff, lambda v: 1.0, tol=1e-12))
     ompo, dmpo = Q.heston_mpo(og, Q.HestonParams(*hp)), P.heston_mpo(pg, P.HestonParams(*hp))
-    orng, drng = np.random.default_rng(1234), np.random.default_rng(1234)
     kw = dict(order=d["order"], maxdim=64, tol_trunc=1e-10, tol_stage=1e-9, tol_basis=1e-8,
               tol_scaling="fixed", work_ceiling_rule="maxdim")
     h = d["h"]
+
+    def start(mod, grid):
+        return mod.qtt_mps(mod.qtt_separable(grid, payoff, lambda v: 1.0, tol=1e-12))
+
+    # the oracle and six copies with the MPO perturbed at 1e-14: the decisions each step admits
+    runs = [(start(Q, og), mpo, np.random.default_rng(1234))
+            for mpo in [ompo] + [_perturbed_mpo(ompo, s) for s in range(1, 7)]]
+    opsi = runs[0][0]
+    dpsi, drng = start(P, pg), np.random.default_rng(1234)
     for k in range(d["steps"]):
-        orep = Q.qtt_bug_step(opsi, ompo, k * h, h, rng=orng, **kw)
+        reps = [Q.qtt_bug_step(psi, mpo, k * h, h, rng=rng, **kw) for psi, mpo, rng in runs]
         drep = P.qtt_bug_step(dpsi, dmpo, k * h, h, rng=drng, **kw)
-        assert drep["bond_dims"] == orep["bond_dims"], k
-        assert drep["status"] == orep["status"] and drep["converged"], k
-        assert drep["krylov"] == orep["krylov"], k
+        assert drep["bond_dims"] == reps[0]["bond_dims"], k
+        assert drep["status"] in {r["status"] for r in reps} and drep["converged"], k
+        assert drep["krylov"] in {r["krylov"] for r in reps}, (k, drep["krylov"], reps[0]["krylov"])
         hst = mps_to_host(dpsi)
         ab = overlap(hst, opsi)
         aa, bb = overlap(hst, hst).real, overlap(opsi, opsi).real
