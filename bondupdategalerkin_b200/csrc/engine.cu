@@ -1004,7 +1004,8 @@ void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, cons
 
 // sum of |x|^2 over the blocks of `t` whose charge on `leg` is sector s, for every sector s of
 // that leg (ascending), in one launch and one read-back.
-std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg) {
+static void sector_descs(const bug_tensor& t, int leg, std::vector<DotDesc>& descs,
+                         std::vector<int>& seg) {
   const Leg& L = t.legs[leg];
   const int nout = int(L.q.size());
   std::vector<std::vector<DotDesc>> per(nout);
@@ -1019,19 +1020,40 @@ std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg) {
       per[s].push_back(d);
     }
   }
-  std::vector<DotDesc> descs;
-  std::vector<int> seg(nout + 1, 0);
+  descs.clear();
+  seg.assign(nout + 1, 0);
   for (int s = 0; s < nout; ++s) {
     seg[s] = int(descs.size());
     descs.insert(descs.end(), per[s].begin(), per[s].end());
   }
   seg[nout] = int(descs.size());
+}
+
+std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg) {
+  const int nout = int(t.legs[leg].q.size());
+  std::vector<DotDesc> descs;
+  std::vector<int> seg;
+  sector_descs(t, leg, descs, seg);
   std::vector<double> out(nout, 0.0);
   if (nout == 0) return out;
   std::vector<double> tmp(2 * size_t(nout));
   run_dots(c, descs, seg, nout, tmp.data(), 16.0);
   for (int s = 0; s < nout; ++s) out[s] = tmp[2 * s];
   return out;
+}
+
+// The same sums (re, im) written to device memory `q` (one slot per sector of `leg`), no read-back.
+void sector_norms2_device(bug_ctx* c, const bug_tensor& t, int leg, double2* q) {
+  const int nout = int(t.legs[leg].q.size());
+  if (nout == 0) return;
+  std::vector<DotDesc> descs;
+  std::vector<int> seg;
+  sector_descs(t, leg, descs, seg);
+  if (descs.empty()) {
+    zero_fill(c, q, int64_t(nout));
+    return;
+  }
+  launch_dots(c, descs, seg, nout, q, 16.0);
 }
 
 std::unique_ptr<bug_tensor> lincomb_impl(bug_ctx* c, int n, const double* coef,

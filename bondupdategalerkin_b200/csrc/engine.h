@@ -632,6 +632,7 @@ TensorPtr lincomb_impl(bug_ctx* c, int n, const double* coef, const bug_tensor* 
 void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
                  double2* q);
 std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg);
+void sector_norms2_device(bug_ctx* c, const bug_tensor& t, int leg, double2* q);
 TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, double thr);
 TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& t, int leg, const double* w);
 TensorPtr conj_impl(bug_ctx* c, const bug_tensor& t);

@@ -270,7 +270,9 @@ __device__ void lincomb_stage(const LinOut* outs, int nout, const LinSrc* srcs, 
       double2 acc = make_double2(0.0, 0.0);
       for (int s = o.src_begin; s < o.src_end; ++s) {
         double2 cf = srcs[s].coef;
-        if (srcs[s].cmode) {
+        if (srcs[s].cmode == 4) {
+          cf = make_double2(-__ldcg(srcs[s].cref), -__ldcg(srcs[s].cref + 1));
+        } else if (srcs[s].cmode) {
           const double x = __ldcg(srcs[s].cref);
           const double r = sqrt(fmax(x, 0.0));
           cf = make_double2(srcs[s].cmode == 1 ? -x : (srcs[s].cmode == 2 ? 1.0 / r : -r), 0.0);

@@ -612,7 +612,8 @@ std::map<int, int> alloc_columns(const std::map<int, int64_t>& dims, int budget)
 
 // Gaussian on the fused space; layout (la, lb, g:+1) or (g:-1, la, lb)
 T gaussian_fused(const Eng& e, const Leg& la, const Leg& lb, const std::map<int, int>& cols,
-                 bool new_first) {
+                 bool new_first, bool* nonzero = nullptr) {
+  if (nonzero) *nonzero = false;
   const int gdir = new_first ? -1 : +1;
   Fused f = fused_of(la, lb, gdir);
   Leg g;
@@ -634,6 +635,8 @@ T gaussian_fused(const Eng& e, const Leg& la, const Leg& lb, const std::map<int,
     int64_t n = 0;
     for (auto& pr : kv.second) n += int64_t(la.dim_of(pr.first)) * lb.dim_of(pr.second);
     std::vector<cd> M = e.complex_normals(n * k);  // (n, k) C order
+    if (nonzero && !*nonzero)
+      *nonzero = std::any_of(M.begin(), M.end(), [](const cd& z) { return z != cd(0); });
     int64_t off = 0;
     for (auto& pr : kv.second) {
       const int da = la.dim_of(pr.first), db = lb.dim_of(pr.second);
@@ -667,9 +670,11 @@ void boost_columns(std::map<int, int>& cols, const std::map<int, int64_t>& boost
   }
 }
 
-// sector-graded Gaussian probe in the opposite frame's discarded space (dd_cbe.jl:132-161)
+// sector-graded Gaussian probe in the opposite frame's discarded space (dd_cbe.jl:132-161). With
+// `norm_slot` the probe's |.|^2 is queued into that device slot and the probe returned unchecked:
+// the caller reads the slot back with its own next result and treats |probe| = 0 as no probe.
 T dd_probe(const Eng& e, const T& opp, bool oleft, int width,
-           const std::map<int, int64_t>* boost = nullptr) {
+           const std::map<int, int64_t>* boost = nullptr, double2* norm_slot = nullptr) {
   Fused f = fused_dims(opp, oleft);
   std::map<int, int64_t> dC;
   int64_t tot = 0;
@@ -684,16 +689,46 @@ T dd_probe(const Eng& e, const T& opp, bool oleft, int width,
                : gaussian_fused(e, opp->legs[1], opp->legs[2], cols, true);
   if (!om) return nullptr;
   T pr = oleft ? perp_left(e, opp, om) : perp_right(e, opp, om);
+  if (norm_slot) {
+    dots_device(e.c, {{pr.get(), pr.get()}}, norm_slot);
+    return pr;
+  }
   return e.norm(pr) > 0 ? pr : nullptr;
 }
 
 T graded_sketch(const Eng& e, const T& frame, bool left, int npre) {
   Fused f = fused_dims(frame, left);
   auto cols = alloc_columns(f.dfull, npre);
-  T r = left ? gaussian_fused(e, frame->legs[0], frame->legs[1], cols, false)
-             : gaussian_fused(e, frame->legs[1], frame->legs[2], cols, true);
+  // the drawn values are on the host: |r| > 0 exactly when one of them is not zero (a Gaussian
+  // value whose square underflows, |x| < 1e-161, does not occur)
+  bool nonzero = false;
+  T r = left ? gaussian_fused(e, frame->legs[0], frame->legs[1], cols, false, &nonzero)
+             : gaussian_fused(e, frame->legs[1], frame->legs[2], cols, true, &nonzero);
   if (!r) return nullptr;
-  return e.norm(r) > 0 ? r : nullptr;
+  return nonzero ? r : nullptr;
+}
+
+// Test B's two read-backs in one: |res| (returned) and the per-sector squared norms `n2` of the
+// residual the test measures, `fin` (res itself, or res projected off `basis` once more), the
+// latter formed and measured ahead of the |res| <= CBE_EPS test and unused when that test returns
+// early.
+double residual_norms(const Eng& e, const T& res, const T& basis,
+                      const std::function<T(const T&)>& project, bool left, std::vector<double>& n2,
+                      T& fin) {
+  const int rleg = left ? 2 : 0;
+  fin = basis ? project(left ? perp_left(e, basis, res) : perp_right(e, basis, res)) : res;
+  const int ns = int(fin->legs[rleg].q.size());
+  double2* q = static_cast<double2*>(e.c->scratch(size_t(1 + ns) * sizeof(double2)));
+  dots_device(e.c, {{res.get(), res.get()}}, q);
+  sector_norms2_device(e.c, *fin, rleg, q + 1);
+  double* host = e.c->readback(size_t(2 * (1 + ns)));
+  e.c->drain();  // the queued dot stages write the slots: they run before the copy
+  BUG_CUDA(cudaMemcpyAsync(host, q, size_t(1 + ns) * sizeof(double2), cudaMemcpyDeviceToHost,
+                           e.c->stream));
+  e.c->wait();
+  n2.resize(size_t(ns));
+  for (int s = 0; s < ns; ++s) n2[size_t(s)] = host[2 * (1 + s)];
+  return std::sqrt(std::max(host[0], 0.0));
 }
 
 // Test B with one fixed probe (sketch.jl:141-180)
@@ -707,12 +742,13 @@ double sample_residual(const Eng& e, const T& basis, const std::function<T(const
   T sk = sketch(Om);
   if (!sk) return 0.0;
   T res = project(sk);
-  if (e.norm(res) <= CBE_EPS) return 0.0;
-  if (basis) res = project(left ? perp_left(e, basis, res) : perp_right(e, basis, res));
   const int rleg = left ? 2 : 0;
+  std::vector<double> n2;
+  T fin;
+  if (residual_norms(e, res, basis, project, left, n2, fin) <= CBE_EPS) return 0.0;
+  res = fin;
   double tot = 0.0;
   const Leg& rl = res->legs[rleg];
-  const std::vector<double> n2 = sector_norms2(e.c, *res, rleg);
   for (size_t s = 0; s < rl.q.size(); ++s) {
     auto it = cols.find(rl.q[s]);
     require(it != cols.end() && it->second > 0, "Test B: residual sector has no holdout column");
@@ -737,11 +773,12 @@ TestB sample_residual_sectors(const Eng& e, const T& basis, const std::function<
     if (Om->legs[wleg].d[s] > 0) r.cols[Om->legs[wleg].q[s]] = Om->legs[wleg].d[s];
   if (r.cols.empty() || !sketched) return r;
   T res = project(sketched);
-  if (e.norm(res) <= CBE_EPS) return r;
-  if (basis) res = project(left ? perp_left(e, basis, res) : perp_right(e, basis, res));
+  std::vector<double> n2;
+  T fin;
+  if (residual_norms(e, res, basis, project, left, n2, fin) <= CBE_EPS) return r;
+  res = fin;
   const int rleg = left ? 2 : 0;
   const Leg& rl = res->legs[rleg];
-  const std::vector<double> n2 = sector_norms2(e.c, *res, rleg);
   double tot = 0.0;
   for (size_t s = 0; s < rl.q.size(); ++s) {
     if (rl.d[s] <= 0) continue;
@@ -1225,7 +1262,8 @@ struct Step {
                   : env.stream_right(U0, core, Wl, Wr, lenv, renv, Om);
     };
     auto project = [&](const T& b) { return left ? perp_left(e, U0, b) : perp_right(e, V0, b); };
-    T Om, directions;
+    T Om, directions, Y;
+    double nY = 0.0;
     int64_t direction_count = 0;
     if (P.dd_mode == 1) {
       const int64_t dmax = std::max({dim(U0, 0), old_rank, dim(V0, 2)});
@@ -1236,12 +1274,22 @@ struct Step {
       directions = dd_controller(frame, opp, left, sketch, project, initial_width, wcap, cap, ledger);
       direction_count = directions ? dim(directions, fl) : 0;
     } else {
-      Om = dd_probe(e, opp, !left, int(std::min<int64_t>(P.fixed_width, full_opp)));
+      // the probe's non-zero test and |Y| come back together: Y is formed before the test is known
+      double2* q = static_cast<double2*>(e.c->scratch(2 * sizeof(double2)));
+      Om = dd_probe(e, opp, !left, int(std::min<int64_t>(P.fixed_width, full_opp)), nullptr, q);
+      if (Om) {
+        Y = project(sketch(Om));
+        dots_device(e.c, {{Y.get(), Y.get()}}, q + 1);
+        double* host = e.c->readback(4);
+        e.c->drain();  // the queued dot stages write the slots: they run before the copy
+        BUG_CUDA(cudaMemcpyAsync(host, q, 2 * sizeof(double2), cudaMemcpyDeviceToHost, e.c->stream));
+        e.c->wait();
+        if (!(std::sqrt(std::max(host[0], 0.0)) > 0)) Om = nullptr;
+        nY = std::sqrt(std::max(host[2], 0.0));
+      }
     }
     if (Om) {
       if (ledger) ledger->n_probes += dim(Om, wleg);
-      T Y = project(sketch(Om));
-      const double nY = e.norm(Y);
       if (!(nY <= CBE_EPS)) {
         std::vector<int> legs = left ? std::vector<int>{0, 1} : std::vector<int>{1, 2};
         const int64_t rmax = std::min(cap, dim(Om, wleg));
@@ -1314,35 +1362,38 @@ struct Step {
     bool closed = false, capped = false;
   };
 
+  // The chain's scalars stay on the device until ONE read-back per step: the Lanczos alpha
+  // (slot 0), |image|^2 (slot 1), the score residual's |r|^2 (slot 2), the seed's |s|^2 (slot 3,
+  // step 1) and, for Arnoldi, the two CGS passes' coefficients (slots 4 .. 4 + 2k). The
+  // combinations that need them read them from device memory (DevTerm modes), so every value is
+  // the one a chain with host scalars computes. Work whose need the read-back decides runs ahead
+  // of it and is dropped when not needed: the first application before the seed is known to be
+  // non-zero (not counted then), the score residual before the breakdown test. `applyH` must not
+  // count its applications: `n_h1` holds the chain's. `prep` forms the score residual of a new
+  // direction and queues its squared norm into a slot; `decide` takes the read-back norm and
+  // returns false to cap.
   Chain krylov_basis(const T& seed, const std::function<T(const T&)>& applyH, double allowance,
-                     const std::function<bool(const T&, double, bool)>& score, double amp,
-                     bool state_seed, bool lanczos) {
+                     const std::function<T(const T&, double2*)>& prep,
+                     const std::function<bool(const T&, const T&, double, double, bool)>& decide,
+                     double amp, bool state_seed, bool lanczos) {
     Chain ch;
-    const double sn = e.norm(seed);
-    if (!(sn > 0)) {
-      ch.closed = true;
-      return ch;
-    }
     tau_eff = tau == cd(0) ? cd(1.0) : tau;
-    T unit = e.scale(seed, 1.0 / sn);
     const int maxdepth = KRY_MAXDEPTH;
     CMat Hm(maxdepth + 1, maxdepth + 1);
-    ch.basis.push_back(unit);
+    double2* slot = static_cast<double2*>(e.c->scratch(size_t(4 + 2 * maxdepth) * sizeof(double2)));
+    auto re = [](const double2* q) { return reinterpret_cast<const double*>(q); };
+    dots_device(e.c, {{seed.get(), seed.get()}}, slot + 3);
+    ch.basis.push_back(lin_dev({{0.0, 2, re(slot + 3), seed}}));  // seed / |seed|
     std::vector<T>& vs = ch.basis;
     double prev_beta = 0.0;
     for (int step = 1; step <= maxdepth; ++step) {
       T image = applyH(lanczos ? vs[step - 1] : vs.back());
       ch.n_h1 += 1;
+      const int k = int(vs.size());
       if (lanczos) {
         if (step > 1) image = e.lin({{1.0, image}, {-prev_beta, vs[step - 2]}});
-        const cd alpha = e.inner(vs[step - 1], image);
-        // with tensor-core contractions the matvec carries FP32-level error (about 1e-7 relative),
-        // so the Hermiticity test allows that much instead of FP64 rounding
-        const double herm_tol = e.c->mixed_min_dim > 0 ? 1e-5 : 1e-9;
-        require(std::abs(alpha.imag()) <= herm_tol * std::max(std::abs(alpha), 1.0),
-                "Lanczos needs a Hermitian one-site generator");
-        Hm(step - 1, step - 1) = alpha.real();
-        image = e.lin({{1.0, image}, {-alpha.real(), vs[step - 1]}});
+        dots_device(e.c, {{vs[step - 1].get(), image.get()}}, slot);
+        image = lin_dev({{1.0, 0, nullptr, image}, {0.0, 1, re(slot), vs[step - 1]}});
         if (step >= 20 && step % 2 == 0) {
           auto cs = e.inner_many(vs, image);
           std::vector<std::pair<cd, T>> terms{{1.0, image}};
@@ -1351,26 +1402,54 @@ struct Step {
         }
       } else {
         for (int pass = 0; pass < 2; ++pass) {
-          auto cs = e.inner_many(vs, image);
-          std::vector<std::pair<cd, T>> terms{{1.0, image}};
-          for (size_t i = 0; i < vs.size(); ++i) {
-            Hm(int(i), step - 1) += cs[i];
-            terms.push_back({-cs[i], vs[i]});
-          }
-          image = e.lin(terms);
+          double2* cs = slot + 4 + pass * k;
+          std::vector<std::pair<const bug_tensor*, const bug_tensor*>> ps;
+          for (auto& v : vs) ps.push_back({v.get(), image.get()});
+          dots_device(e.c, ps, cs);
+          std::vector<DevTerm> terms{{1.0, 0, nullptr, image}};
+          for (int i = 0; i < k; ++i) terms.push_back({0.0, 4, re(cs + i), vs[size_t(i)]});
+          image = lin_dev(terms);
         }
       }
-      const double beta = e.norm(image);
+      dots_device(e.c, {{image.get(), image.get()}}, slot + 1);
+      T nv = lin_dev({{0.0, 2, re(slot + 1), image}});
+      T residual = prep(nv, slot + 2);
+      const int nread = lanczos ? 4 : 4 + 2 * k;
+      double* host = e.c->readback(size_t(2 * nread));
+      e.c->drain();  // the queued stages write the slots: they run before the copy
+      BUG_CUDA(cudaMemcpyAsync(host, slot, size_t(nread) * sizeof(double2), cudaMemcpyDeviceToHost,
+                               e.c->stream));
+      e.c->wait();
+      if (step == 1 && !(std::sqrt(std::max(host[6], 0.0)) > 0)) {
+        ch = Chain{};  // a zero seed: no basis and no application
+        ch.closed = true;
+        return ch;
+      }
+      if (lanczos) {
+        const cd alpha(host[0], host[1]);
+        // with tensor-core contractions the matvec carries FP32-level error (about 1e-7 relative),
+        // so the Hermiticity test allows that much instead of FP64 rounding
+        const double herm_tol = e.c->mixed_min_dim > 0 ? 1e-5 : 1e-9;
+        require(std::abs(alpha.imag()) <= herm_tol * std::max(std::abs(alpha), 1.0),
+                "Lanczos needs a Hermitian one-site generator");
+        Hm(step - 1, step - 1) = alpha.real();
+      } else {
+        for (int pass = 0; pass < 2; ++pass)
+          for (int i = 0; i < k; ++i) {
+            const double* c2 = host + 2 * (4 + pass * k + i);
+            Hm(i, step - 1) += cd(c2[0], c2[1]);
+          }
+      }
+      const double beta = std::sqrt(std::max(host[2], 0.0));
       if (beta <= KRY_BREAKDOWN) {
         ch.closed = true;
         break;
       }
       Hm(step, step - 1) = beta;
       if (lanczos) Hm(step - 1, step) = beta;
-      T nv = e.scale(image, 1.0 / beta);
       vs.push_back(nv);
       const double w = amp * kry_weight(Hm, step, state_seed);
-      if (!score(nv, w, step == 1)) {
+      if (!decide(residual, nv, w, std::sqrt(std::max(host[4], 0.0)), step == 1)) {
         ch.capped = true;
         break;
       }
@@ -1424,9 +1503,13 @@ struct Step {
     T frame = start_frame;
     KStats st;
     int64_t added_d = 0;
-    auto score = [&](const T& dir, double w, bool first) {
+    auto prep = [&](const T& dir, double2* slot) {
       T residual = left ? perp_left(e, frame, dir) : perp_right(e, frame, dir);
-      const double eta = w * e.norm(residual);
+      dots_device(e.c, {{residual.get(), residual.get()}}, slot);
+      return residual;
+    };
+    auto decide = [&](const T& residual, const T& dir, double w, double rnorm, bool first) {
+      const double eta = w * rnorm;
       if (first) st.eta_c = eta;
       else st.eta_d = std::max(st.eta_d, eta);
       if (!(eta > allow)) return true;
@@ -1438,7 +1521,8 @@ struct Step {
       if (!first) added_d += std::get<1>(r);
       return std::get<2>(r);
     };
-    Chain ch = krylov_basis(seed, applyH, alloc.krylov, score, amp, state_seed, P.lanczos != 0);
+    Chain ch = krylov_basis(seed, applyH, alloc.krylov, prep, decide, amp, state_seed,
+                            P.lanczos != 0);
     st.n_h1 = ch.n_h1;
     st.capped = ch.capped;
     st.d_after_c = st.eta_c <= alloc.krylov && added_d > 0;
@@ -1476,11 +1560,9 @@ struct Step {
       T Kex = e.contract(carried, {2}, rp, {0});
       T rch1 = env.right_step(rstack[bond + 2], ex.V_ex, mpo[bond + 1]);
       const T& W = mpo[bond];
-      auto applyH = [&](const T& v) {
-        nmv += 1;
-        return h1(lch, W, rch1, v);
-      };
+      auto applyH = [&](const T& v) { return h1(lch, W, rch1, v); };
       auto kr = krylov_enrich(Kex, applyH, ex.U_ex, true, cap_at(bond), 1.0, true);
+      nmv += kr.second.n_h1;
       record_krylov(bl, kr.second);
       T Wk = kr.first;
       lf[bond] = Wk;
@@ -1510,11 +1592,9 @@ struct Step {
       T Bex = e.contract(lp, {1}, carried, {0});
       T lch1 = env.left_step(lstack[bond], ex.U_ex, mpo[bond]);
       const T& W = mpo[bond + 1];
-      auto applyH = [&](const T& v) {
-        nmv += 1;
-        return h1(lch1, W, rch, v);
-      };
+      auto applyH = [&](const T& v) { return h1(lch1, W, rch, v); };
       auto kr = krylov_enrich(Bex, applyH, ex.V_ex, false, cap_at(bond), 1.0, true);
+      nmv += kr.second.n_h1;
       record_krylov(bl, kr.second);
       T Zk = kr.first;
       rf[bond] = Zk;
@@ -1544,7 +1624,12 @@ struct Step {
     }
     return AR;
   }
+  // The outside components' squared norms go to device slots and come back in one read-back at
+  // the end, summed in the order the terms arise.
   double projection_miss(const MPS& psi, std::map<int, T>& lf, std::map<int, T>& rf) {
+    double2* n2 = static_cast<double2*>(e.c->scratch(size_t(L + 1) * sizeof(double2)));
+    int nterm = 0;
+    auto miss_term = [&](const T& x) { dots_device(e.c, {{x.get(), x.get()}}, n2 + nterm++); };
     std::vector<T> rfac(L + 2);
     for (int site = L; site >= 2; --site) {
       T carried = site == L ? psi[L] : e.contract(psi[site], {2}, rfac[site + 1], {0});
@@ -1555,7 +1640,7 @@ struct Step {
     for (int site = 1; site <= root_link; ++site) {
       T carried = AL ? e.contract(AL, {1}, psi[site], {0}) : psi[site];
       T outside = perp_left(e, lf[site], carried);
-      miss2 += std::pow(e.norm(e.contract(outside, {2}, rfac[site + 1], {0})), 2);
+      miss_term(e.contract(outside, {2}, rfac[site + 1], {0}));
       AL = e.contract(lf[site], {0, 1}, carried, {0, 1}, true, false);
     }
     std::vector<T> lfac(L + 1);
@@ -1566,8 +1651,16 @@ struct Step {
     for (int bond = L - 1; bond >= root_link; --bond) {
       T carried = AR ? e.contract(psi[bond + 1], {2}, AR, {0}) : psi[bond + 1];
       T outside = perp_right(e, rf[bond], carried);
-      miss2 += std::pow(e.norm(e.contract(lfac[bond], {1}, outside, {0})), 2);
+      miss_term(e.contract(lfac[bond], {1}, outside, {0}));
       AR = e.contract(carried, {1, 2}, rf[bond], {1, 2}, false, true);
+    }
+    if (nterm > 0) {
+      double* host = e.c->readback(size_t(2 * nterm));
+      e.c->drain();  // the queued dot stages write the slots: they run before the copy
+      BUG_CUDA(cudaMemcpyAsync(host, n2, size_t(nterm) * sizeof(double2), cudaMemcpyDeviceToHost,
+                               e.c->stream));
+      e.c->wait();
+      for (int i = 0; i < nterm; ++i) miss2 += std::pow(std::sqrt(std::max(host[2 * i], 0.0)), 2);
     }
     return std::sqrt(miss2);
   }
@@ -1674,11 +1767,9 @@ struct Step {
         T Kex = e.contract(site_core, {2}, rp, {0});
         T rch1 = env.right_step(rch, ex.V_ex, mpo[bond + 1]);
         const T& W = mpo[bond];
-        auto applyH = [&](const T& v) {
-          out.n_h1 += 1;
-          return h1(lch, W, rch1, v);
-        };
+        auto applyH = [&](const T& v) { return h1(lch, W, rch1, v); };
         auto kr = krylov_enrich(Kex, applyH, ex.U_ex, true, cap_at(bond), amp, false);
+        out.n_h1 += kr.second.n_h1;
         record_krylov(bl, kr.second);
         Wi = kr.first;
       } else {
@@ -1730,11 +1821,9 @@ struct Step {
         T Bex = e.contract(lp, {1}, site_core, {0});
         T lch1 = env.left_step(lch, ex.U_ex, mpo[bond]);
         const T& W = mpo[bond + 1];
-        auto applyH = [&](const T& v) {
-          out.n_h1 += 1;
-          return h1(lch1, W, rch, v);
-        };
+        auto applyH = [&](const T& v) { return h1(lch1, W, rch, v); };
         auto kr = krylov_enrich(Bex, applyH, ex.V_ex, false, cap_at(bond), amp, false);
+        out.n_h1 += kr.second.n_h1;
         record_krylov(bl, kr.second);
         Zj = kr.first;
       } else {
@@ -1971,7 +2060,7 @@ struct Step {
 
   // A linear combination whose coefficients may be device-resident dot products (bugk::LinSrc):
   // mode 0 uses `coef`; 1, 2, 3 give -x, 1/sqrt(max(x, 0)), -sqrt(max(x, 0)) of the real part x
-  // at `ref`.
+  // at `ref`; 4 gives -(x + iy) of the complex value (x, y) at `ref`.
   struct DevTerm {
     cd coef;
     int mode;
