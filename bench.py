@@ -56,6 +56,7 @@ TDVP2_NAME = "tdvp2_xxz_quench_L64_delta0.5_domainwall_maxdim256_wtol1e-7"
 ITE = dict(L=32, delta=1.0, dbeta=0.125, kw=dict(order=2, maxdim=128))
 ITE_NAME = "ite_heisenberg_L32_neel_dbeta0.125_order2_maxdim128"
 KIND = ["xxz"]
+PARALLEL = [False]  # parallel = true: half-sweeps and frontier halves on two streams
 L2_FLUSH_BYTES = 256 << 20
 _HESTON_DOMAIN = dict(x=(-1.0, 1.0), y=(0.0, 0.5), periodic_x=False, periodic_y=False)
 
@@ -101,11 +102,12 @@ def metric_name():
 
 
 def step_kwargs():
+    extra = dict(parallel=True) if PARALLEL[0] else {}
     if KIND[0] == "heston":
-        return dict(maxdim=HESTON["maxdim"], hermitian=False)
+        return dict(maxdim=HESTON["maxdim"], hermitian=False, **extra)
     w = WORKLOAD
     return dict(order=w["order"], tol_basis=w["tol_basis"], maxdim=w["maxdim"],
-                bond_ceiling_factor=w["bond_ceiling_factor"])
+                bond_ceiling_factor=w["bond_ceiling_factor"], **extra)
 
 
 def device_inputs():
@@ -144,6 +146,8 @@ def config_dict(args, ws, max_bond=None):
     cfg = _config_dict(args, ws, max_bond)
     if getattr(args, "mixed", 0) > 0:
         cfg["precision"] = f"3xTF32 tensor cores for contraction blocks >= {args.mixed} x {args.mixed}"
+    if PARALLEL[0]:
+        cfg["half_sweeps"] = "parallel = true: the two halves on two streams and two host threads"
     return cfg
 
 
@@ -811,6 +815,8 @@ def main():
                          "imaginary time on the L = 32 Heisenberg chain (29 timed steps of dbeta "
                          "0.125 after 3 warm-up reach beta 4); batch: 64 chains at once on the job server; served: a Poisson "
                          "job stream")
+    ap.add_argument("--parallel", action="store_true",
+                    help="parallel = true: the half-sweeps and frontier halves on two streams")
     ap.add_argument("--mixed", type=int, default=0,
                     help="contraction blocks with both extents >= this run on the tensor cores "
                          "(3xTF32); 0 (default): everything in FP64")
@@ -820,6 +826,7 @@ def main():
                     help="served: shrink the stream's size ranges toward their lower ends")
     args = ap.parse_args()
     KIND[0] = args.workload
+    PARALLEL[0] = args.parallel
     if args.workload == "heston" and "--steps" not in sys.argv:
         args.steps = 47
     if args.workload == "ite" and "--steps" not in sys.argv:

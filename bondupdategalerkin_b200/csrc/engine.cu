@@ -46,11 +46,11 @@ void zero_fill(bug_ctx* c, double2* p, int64_t n) {
 std::shared_ptr<Buffer> alloc_buffer(bug_ctx* c, int64_t n, bool zero) {
   auto b = std::make_shared<Buffer>();
   b->n = n;
-  b->ctx = c;
+  b->ctx = c->allocator();  // a second stream's tensors are returned to the allocator they came from
   if (n > 0) {
     b->ptr = static_cast<double2*>(c->dev_alloc(size_t(n) * sizeof(double2)));
     if (zero) zero_fill(c, b->ptr, n);
-    c->bytes += n * int64_t(sizeof(double2));
+    b->ctx->bytes += n * int64_t(sizeof(double2));
   }
   return b;
 }
@@ -1388,26 +1388,7 @@ int bug_ctx_create(int device, bug_ctx** out) {
     require(device >= 0 && device < count, "no such CUDA device");
     BUG_CUDA(cudaSetDevice(device));
     auto c = std::make_unique<bug_ctx>();
-    c->device = device;
-    BUG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    c->list_cluster = bugk::stage_list_cluster();
-    // BUG_STAGE_LISTS=0 launches every stage on its own (same results; for comparisons)
-    const char* lists = std::getenv("BUG_STAGE_LISTS");
-    c->queue_enabled = !(lists && std::string(lists) == "0");
-    if (const char* qm = std::getenv("BUG_STAGE_LIST_MAX")) {
-      const long v = std::strtol(qm, nullptr, 10);
-      if (v >= 1 && v <= 4096) c->queue_max_stages = size_t(v);
-    }
-    if (const char* qr = std::getenv("BUG_STAGE_LIST_ROUNDS")) {
-      const long v = std::strtol(qr, nullptr, 10);
-      if (v >= 1 && v <= 64) c->queue_rounds = int(v);
-    }
-    for (int i = 0; i < bug_ctx::kSlots; ++i)
-      BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
-    cudaMemPool_t pool;
-    BUG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-    uint64_t thr = UINT64_MAX;
-    BUG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    ctx_init(c.get(), device);
     *out = c.release();
   });
 }
@@ -1415,22 +1396,130 @@ int bug_ctx_create(int device, bug_ctx** out) {
 int bug_ctx_destroy(bug_ctx* c) {
   return guard([&] {
     if (!c) return;
-    cudaStreamSynchronize(c->stream);
-    for (int i = 0; i < bug_ctx::kSlots; ++i) {
-      if (c->stage_ptr[i]) cudaFreeHost(c->stage_ptr[i]);
-      cudaEventDestroy(c->stage_ev[i]);
+    if (c->child) {
+      ctx_release(c->child);
+      delete c->child;
+      c->child = nullptr;
     }
-    if (c->pinned_out) cudaFreeHost(c->pinned_out);
-    if (c->tc_err_host) cudaFreeHost(c->tc_err_host);
-    if (c->arena) cudaFreeAsync(c->arena, c->stream);
-    c->release_cached();
-    cudaStreamSynchronize(c->stream);
-    if (c->dot_counter) cudaFree(c->dot_counter);
-    if (c->sync_ev) cudaEventDestroy(c->sync_ev);
-    if (c->owns_stream) cudaStreamDestroy(c->stream);
+    ctx_release(c);
     delete c;
   });
 }
+}  // extern "C"
+
+namespace bugi {
+
+void ctx_init(bug_ctx* c, int device) {
+  c->device = device;
+  BUG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->list_cluster = bugk::stage_list_cluster();
+  // BUG_STAGE_LISTS=0 launches every stage on its own (same results; for comparisons)
+  const char* lists = std::getenv("BUG_STAGE_LISTS");
+  c->queue_enabled = !(lists && std::string(lists) == "0");
+  if (const char* qm = std::getenv("BUG_STAGE_LIST_MAX")) {
+    const long v = std::strtol(qm, nullptr, 10);
+    if (v >= 1 && v <= 4096) c->queue_max_stages = size_t(v);
+  }
+  if (const char* qr = std::getenv("BUG_STAGE_LIST_ROUNDS")) {
+    const long v = std::strtol(qr, nullptr, 10);
+    if (v >= 1 && v <= 64) c->queue_rounds = int(v);
+  }
+  for (int i = 0; i < bug_ctx::kSlots; ++i)
+    BUG_CUDA(cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
+  cudaMemPool_t pool;
+  BUG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t thr = UINT64_MAX;
+  BUG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+}
+
+// Everything a context holds, after its stream has finished (the object itself stays).
+void ctx_release(bug_ctx* c) {
+  cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < bug_ctx::kSlots; ++i) {
+    if (c->stage_ptr[i]) cudaFreeHost(c->stage_ptr[i]);
+    cudaEventDestroy(c->stage_ev[i]);
+  }
+  if (c->pinned_out) cudaFreeHost(c->pinned_out);
+  if (c->tc_err_host) cudaFreeHost(c->tc_err_host);
+  if (c->arena) cudaFreeAsync(c->arena, c->stream);
+  c->release_cached();
+  cudaStreamSynchronize(c->stream);
+  if (c->dot_counter) cudaFree(c->dot_counter);
+  if (c->sync_ev) cudaEventDestroy(c->sync_ev);
+  if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+  if (c->owns_stream) cudaStreamDestroy(c->stream);
+}
+
+// ── concurrent halves: the second stream ─────────────────────────────────────────────────────
+
+bug_ctx* fork_begin(bug_ctx* c) {
+  require(!c->alloc_owner && !c->forking, "a fork inside a fork");
+  require(!c->combiner, "parallel half-sweeps need a context with a stream of its own, not a "
+                        "combining batch");
+  if (!c->child) {
+    auto ch = std::make_unique<bug_ctx>();
+    ctx_init(ch.get(), c->device);
+    ch->alloc_owner = c;
+    c->child = ch.release();
+  }
+  bug_ctx* ch = c->child;
+  ch->queue_enabled = c->queue_enabled;
+  ch->queue_max_stages = c->queue_max_stages;
+  ch->queue_rounds = c->queue_rounds;
+  ch->mixed_min_dim = c->mixed_min_dim;
+  if (!c->fork_ev) BUG_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+  if (!ch->fork_ev) BUG_CUDA(cudaEventCreateWithFlags(&ch->fork_ev, cudaEventDisableTiming));
+  c->drain();  // every queued stage of the parent is enqueued before the fork event
+  BUG_CUDA(cudaEventRecord(c->fork_ev, c->stream));
+  BUG_CUDA(cudaStreamWaitEvent(ch->stream, c->fork_ev, 0));
+  c->forking = true;  // set before the child's thread starts
+  return ch;
+}
+
+// On the child's thread when its half is done (or failed): its queue enqueued (or dropped) and the
+// join event recorded after it.
+void fork_child_done(bug_ctx* ch, bool ok) {
+  if (ok) ch->drain();
+  else ch->discard_queue();
+  BUG_CUDA(cudaEventRecord(ch->fork_ev, ch->stream));
+}
+
+// After the child's thread has been joined: the parent stream waits for the child's work, the
+// releases parked during the fork and the child's scratch go back, and the child's accounting is
+// folded into the parent's.
+void fork_end(bug_ctx* c) {
+  bug_ctx* ch = c->child;
+  cudaError_t e = cudaStreamWaitEvent(c->stream, ch->fork_ev, 0);
+  c->forking = false;
+  std::vector<void*> parked;
+  parked.swap(c->fork_frees);
+  for (void* p : parked) c->dev_free(p);
+  for (void* p : ch->deferred) ch->dev_free(p);
+  ch->deferred.clear();
+  c->launches += ch->launches;
+  c->syncs += ch->syncs;
+  c->sync_wait_s += ch->sync_wait_s;
+  c->launch_s += ch->launch_s;
+  c->alloc_s += ch->alloc_s;
+  c->list_launches += ch->list_launches;
+  c->queued_stages += ch->queued_stages;
+  for (int f = 0; f < BUG_K_NFAMILIES; ++f) {
+    c->k_launches[f] += ch->k_launches[f];
+    c->k_flops[f] += ch->k_flops[f];
+    c->k_bytes[f] += ch->k_bytes[f];
+  }
+  ch->launches = ch->syncs = ch->list_launches = ch->queued_stages = 0;
+  ch->sync_wait_s = ch->launch_s = ch->alloc_s = 0.0;
+  for (int f = 0; f < BUG_K_NFAMILIES; ++f) {
+    ch->k_launches[f] = 0;
+    ch->k_flops[f] = ch->k_bytes[f] = 0.0;
+  }
+  BUG_CUDA(e);
+}
+
+}  // namespace bugi
+
+extern "C" {
 
 int bug_ctx_synchronize(bug_ctx* c) {
   return guard([&] {
@@ -1494,7 +1583,7 @@ int bug_ctx_host_stats(bug_ctx* c, int64_t* syncs, double* wait_s, double* launc
     *alloc_s = c->alloc_s;
   });
 }
-int64_t bug_ctx_bytes_in_use(const bug_ctx* c) { return c ? c->bytes : 0; }
+int64_t bug_ctx_bytes_in_use(const bug_ctx* c) { return c ? c->bytes.load() : 0; }
 
 int bug_tensor_create(bug_ctx* c, int rank, const int* dirs, const int* nsec, const int* charges,
                       const int* dims, int nblocks, const int* keys, bug_tensor** out) {

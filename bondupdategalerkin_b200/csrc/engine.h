@@ -210,7 +210,7 @@ struct bug_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
-  int64_t bytes = 0;
+  std::atomic<int64_t> bytes{0};  // payload bytes of the live tensors (released from either stream's thread)
   // per kernel family: launches, algorithmic flops and bytes, device time (profiling only)
   int64_t k_launches[BUG_K_NFAMILIES] = {};
   double k_flops[BUG_K_NFAMILIES] = {};
@@ -283,8 +283,31 @@ struct bug_ctx {
     const size_t step = (size_t(1) << e) / 4;
     return ((b + step - 1) / step) * step;
   }
+  //
+  // Concurrent half-sweeps (`parallel`): a second context, `child`, with its own stream, stage
+  // queue and descriptor staging, drives one half on a thread of its own and allocates from THIS
+  // context's allocator (`alloc_owner` on the child; `alloc_mu` serialises the two threads). A
+  // block handed out during the fork was released before it began, so its last use precedes the
+  // fork event both streams are ordered after; every release during the fork (`forking`) is
+  // parked in `fork_frees` until the join, where the parent stream has waited for the child's,
+  // so the blocks return to the free lists with both streams' uses behind them.
+  bug_ctx* child = nullptr;
+  bug_ctx* alloc_owner = nullptr;
+  cudaEvent_t fork_ev = nullptr;  // parent: the fork point; child: the end of its half
+  bool forking = false;
+  std::mutex alloc_mu;
+  std::vector<void*> fork_frees;
+  bug_ctx* allocator() { return alloc_owner ? alloc_owner : this; }
   void* dev_alloc(size_t bytes) {
     const auto t0 = std::chrono::steady_clock::now();
+    void* p = allocator()->alloc_on(bytes, stream);
+    alloc_s += since(t0);
+    return p;
+  }
+  // (on the allocator) a block of at least `bytes`; a new one is ordered on stream `s`
+  void* alloc_on(size_t bytes, cudaStream_t s) {
+    std::unique_lock<std::mutex> lk(alloc_mu, std::defer_lock);
+    if (child) lk.lock();
     const size_t cls = size_class(bytes);
     void* p = nullptr;
     auto it = free_.find(cls);
@@ -293,24 +316,34 @@ struct bug_ctx {
       it->second.pop_back();
       cached_bytes -= cls;
     } else {
-      cudaError_t e = cudaMallocAsync(&p, cls, stream);
+      cudaError_t e = cudaMallocAsync(&p, cls, s);
       if (e == cudaErrorMemoryAllocation) {  // give the parked blocks back and retry once
         cudaGetLastError();
-        release_cached();
-        e = cudaMallocAsync(&p, cls, stream);
+        release_cached_on(s);
+        e = cudaMallocAsync(&p, cls, s);
       }
       BUG_CUDA(e);
     }
     live_[p] = cls;
-    alloc_s += since(t0);
     return p;
   }
   void dev_free(void* p) {
+    bug_ctx* o = allocator();
+    if (o->forking) {
+      std::lock_guard<std::mutex> g(o->alloc_mu);
+      o->fork_frees.push_back(p);
+      return;
+    }
     if (!queue.empty()) {  // a queued stage may still read it: reusable once the queue is launched
       pending_free.push_back(p);
       return;
     }
     const auto t0 = std::chrono::steady_clock::now();
+    o->free_now(p);
+    alloc_s += since(t0);
+  }
+  // (on the allocator, no fork running) back to the free lists, or to the pool on this stream
+  void free_now(void* p) {
     auto it = live_.find(p);
     size_t cls = 0;
     if (it != live_.end()) {
@@ -323,11 +356,11 @@ struct bug_ctx {
     } else {
       cudaFreeAsync(p, stream);
     }
-    alloc_s += since(t0);
   }
-  void release_cached() {
+  void release_cached() { release_cached_on(stream); }
+  void release_cached_on(cudaStream_t s) {
     for (auto& kv : free_)
-      for (void* p : kv.second) cudaFreeAsync(p, stream);
+      for (void* p : kv.second) cudaFreeAsync(p, s);
     free_.clear();
     cached_bytes = 0;
   }
@@ -633,6 +666,16 @@ void dots_device(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, cons
                  double2* q);
 std::vector<double> sector_norms2(bug_ctx* c, const bug_tensor& t, int leg);
 void sector_norms2_device(bug_ctx* c, const bug_tensor& t, int leg, double2* q);
+// A context's stream, queue and staging, set up for `device` / released after its stream finished.
+void ctx_init(bug_ctx* c, int device);
+void ctx_release(bug_ctx* c);
+// Two halves on two streams: fork_begin returns the second context (made on first use), ordered
+// after everything the parent issued; the half on it ends with fork_child_done on its own thread;
+// fork_end (parent thread, after that thread joined) orders the parent after it and returns the
+// releases parked meanwhile.
+bug_ctx* fork_begin(bug_ctx* c);
+void fork_child_done(bug_ctx* ch, bool ok);
+void fork_end(bug_ctx* c);
 TensorPtr thin_qr_impl(bug_ctx* c, const bug_tensor& t, int fl, int ref_dir, double thr);
 TensorPtr scale_leg_impl(bug_ctx* c, const bug_tensor& t, int leg, const double* w);
 TensorPtr conj_impl(bug_ctx* c, const bug_tensor& t);

@@ -21,9 +21,11 @@
 #include "smallla.h"
 
 #include <complex>
+#include <exception>
 #include <limits>
 #include <numeric>
 #include <set>
+#include <thread>
 
 namespace bugs {
 
@@ -104,6 +106,23 @@ struct DrawBuf {
   void restore() {
     pos = marks.back();
     marks.pop_back();
+  }
+  // The caller's generator exactly where the values handed out so far leave it, for a draw of
+  // another kind from it (pause); resume() then saves the generator after that draw and buffers
+  // from there.
+  bool paused = false;
+  void pause() {
+    if (!open) return;
+    require(marks.empty(), "a stream fork inside a measurement of a copied stream");
+    finish();
+    x.clear();
+    base = pos = 0;
+    paused = true;
+  }
+  void resume() {
+    if (!paused) return;
+    paused = false;
+    begin();
   }
   // the caller's generator back to the step's start, then forward by the values handed out
   void finish() {
@@ -857,6 +876,9 @@ struct Params {
   int closure_checks = 0;  // the measured, multi-pass closure (_krylov_closure!, checks = true)
   int root_method = 0;     // 0 exp, 1 trapezoid, 2 radau2, 3 radau3
   bool root_shift = true;  // the implicit roots' imaginary-time spectral shift
+  bool parallel = false;   // parallel = true: halves on two streams, right halves on forked streams
+  bug_rng_fork_fn rng_fork = nullptr;
+  void* rng_fork_user = nullptr;
 };
 
 struct MPS {
@@ -1014,8 +1036,91 @@ struct Step {
   int64_t nmv = 0;
 
   Step(const Eng& eng, const MPOv& m, const Params& p, cd t, int l) : e(eng), env{e}, mpo(m), P(p), tau(t), L(l) {}
+  Step(const Step&) = delete;
+  Step& operator=(const Step&) = delete;
 
   int64_t cap_at(int bond) const { return wcap[bond - 1]; }
+
+  // ── parallel = true (bug_step.jl:222-268, frontier_closure.jl:121-145) ──
+  // this step's settings on a step bound to another engine (context and draw stream); a Step is
+  // never copied (its Env refers to its own Eng)
+  void share_settings(Step& s) const {
+    s.eshift = eshift;
+    s.root_link = root_link;
+    s.alloc = alloc;
+    s.wcap = wcap;
+  }
+  // The right half's stream: ONE 64-bit draw from the step's stream at this point seeds it (the
+  // caller makes it through rng_fork); a buffered step stream is first brought to this point.
+  std::pair<bug_normal_fn, void*> fork_stream() {
+    if (e.buf) e.buf->pause();
+    bug_normal_fn d = nullptr;
+    void* u = nullptr;
+    const int rc = P.rng_fork(P.rng_fork_user, &d, &u);
+    if (e.buf) e.buf->resume();
+    require(rc == 0 && d, "parallel: the draw-stream fork failed");
+    return {d, u};
+  }
+  // `left` on this step, `right` at the same time on a copy of it bound to the context's second
+  // stream (fork_begin) and the forked draw stream, driven by a thread of its own; both are done
+  // and the parent stream is ordered after both when this returns. The halves share no mutable
+  // state: each writes its own outputs (the one shared vector, `expanded`, at disjoint bonds).
+  // A profiled context (every launch timed on its one stream), or BUG_PARALLEL_SERIAL=1, runs the
+  // halves in turn on this context instead: the same draws and results, no second stream.
+  void run_halves(const std::function<void(Step&)>& left, const std::function<void(Step&)>& right,
+                  std::pair<bug_normal_fn, void*> stream) {
+    static const bool in_turn = [] {
+      const char* v = std::getenv("BUG_PARALLEL_SERIAL");
+      return v && std::string(v) == "1";
+    }();
+    DrawBuf rbuf;  // the forked stream is the half's alone: it is read ahead freely, never rewound
+    rbuf.draw = stream.first;
+    rbuf.user = stream.second;
+    if (in_turn || e.c->profiling) {
+      Eng er{e.c, stream.first, stream.second};
+      er.buf = &rbuf;
+      Step SR(er, mpo, P, tau, L);
+      share_settings(SR);
+      left(*this);
+      right(SR);
+      nmv += SR.nmv;
+      return;
+    }
+    bug_ctx* ch = bugi::fork_begin(e.c);
+    Eng er{ch, stream.first, stream.second};
+    er.buf = &rbuf;
+    Step SR(er, mpo, P, tau, L);
+    share_settings(SR);
+    std::exception_ptr rerr, lerr;
+    std::thread th([&] {
+      bool ok = true;
+      try {
+        right(SR);
+      } catch (...) {
+        rerr = std::current_exception();
+        ok = false;
+      }
+      try {
+        bugi::fork_child_done(ch, ok);
+      } catch (...) {
+        if (!rerr) rerr = std::current_exception();
+      }
+    });
+    try {
+      left(*this);
+    } catch (...) {
+      lerr = std::current_exception();
+    }
+    th.join();
+    try {
+      bugi::fork_end(e.c);
+    } catch (...) {
+      if (!lerr) lerr = std::current_exception();
+    }
+    nmv += SR.nmv;
+    if (lerr) std::rethrow_exception(lerr);
+    if (rerr) std::rethrow_exception(rerr);
+  }
 
   // canonical form (canonical_form.jl)
   void move_right(MPS& psi, int site) {
@@ -1747,12 +1852,12 @@ struct Step {
       T ch = env.left_boundary();
       for (int bond = 1; bond <= root_link; ++bond) {
         chain[bond] = ch;
-        if (bond < root_link) ch = env.left_step(ch, fr.lf[bond], mpo[bond]);
+        if (bond < root_link) ch = env.left_step(ch, fr.lf.at(bond), mpo[bond]);
       }
     }
     for (int bond = 1; bond <= root_link; ++bond) {
       if (!enrich) lch = chain[bond];
-      T old = Pm ? e.contract(Pm, {1}, fr.lf[bond], {0}) : fr.lf[bond];
+      T old = Pm ? e.contract(Pm, {1}, fr.lf.at(bond), {0}) : fr.lf.at(bond);
       T site_core = carry ? e.contract(carry, {1}, Fm[bond], {0}) : Fm[bond];
       BondFrame tsf = frame_onto_left(old, site_core, Fm[bond + 1]);
       const T& rch = rstack[bond + 2];
@@ -1801,12 +1906,12 @@ struct Step {
       T ch = env.right_boundary(total_charge(Fm));
       for (int bond = L - 1; bond >= root_link; --bond) {
         chain[bond] = ch;
-        if (bond > root_link) ch = env.right_step(ch, fr.rf[bond], mpo[bond + 1]);
+        if (bond > root_link) ch = env.right_step(ch, fr.rf.at(bond), mpo[bond + 1]);
       }
     }
     for (int bond = L - 1; bond >= root_link; --bond) {
       if (!enrich) rch = chain[bond];
-      T old = Pm ? e.contract(fr.rf[bond], {2}, Pm, {0}) : fr.rf[bond];
+      T old = Pm ? e.contract(fr.rf.at(bond), {2}, Pm, {0}) : fr.rf.at(bond);
       T site_core = carry ? e.contract(Fm[bond + 1], {2}, carry, {0}) : Fm[bond + 1];
       BondFrame tsf = frame_onto_right(Fm[bond], site_core, old);
       const T& lch = lstack[bond];
@@ -1851,14 +1956,23 @@ struct Step {
     std::vector<double> leaks_left, leaks_right;  // per bond: 1..root, root..L-1
   };
 
-  Sweep frontier_sweep(KL& fr, const MPS& psi, const T& core, double nrm, bool enrich = true) {
+  // `halves`: false keeps the two halves serial on the step's stream even under parallel = true
+  // (the outside-residual measurement, which the reference takes without `parallel`)
+  Sweep frontier_sweep(KL& fr, const MPS& psi, const T& core, double nrm, bool enrich = true,
+                       bool halves = true) {
     Sweep sw;
     const double nF = e.norm(core);
     if (nF <= FRONTIER_FLOOR * std::max(nrm, EPS)) return sw;
     MPS Fm = frontier_mps(psi, fr, core);
     const double amp = nF / std::max(nrm, EPS);
-    FrontierHalf rl = frontier_left(Fm, fr, amp, enrich);
-    FrontierHalf rr = frontier_right(Fm, fr, amp, enrich);
+    FrontierHalf rl, rr;
+    if (P.parallel && halves) {
+      run_halves([&](Step& s) { rl = s.frontier_left(Fm, fr, amp, enrich); },
+                 [&](Step& s) { rr = s.frontier_right(Fm, fr, amp, enrich); }, fork_stream());
+    } else {
+      rl = frontier_left(Fm, fr, amp, enrich);
+      rr = frontier_right(Fm, fr, amp, enrich);
+    }
     sw.leaks_left = rl.leak;
     sw.leaks_right = rr.leak;
     sw.ledger.merge(rl.ledger);
@@ -2596,6 +2710,10 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
             "root_method must be 0 (exp), 1 (trapezoid), 2 (radau2), 3 (radau3) or 4 (radau2_gmres)");
     P.root_method = prm->root_method;
     P.root_shift = prm->root_noshift == 0;
+    P.parallel = prm->parallel != 0;
+    P.rng_fork = prm->rng_fork;
+    P.rng_fork_user = prm->rng_fork_user;
+    require(!P.parallel || (P.rng_fork && draw), "parallel needs rng_fork and a draw stream");
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
@@ -2665,8 +2783,16 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     Ledger ledgerL, ledgerR;
     std::map<int, T> lf, rf;
     MPS psiL = psi;
-    T lenv_root = S.half_left(psiL, lf, expanded, nL, ledgerL);
-    auto rr = S.half_right(psi, rf, expanded, nR, ledgerR);
+    T lenv_root;
+    std::pair<T, T> rr;
+    if (P.parallel) {
+      S.run_halves([&](Step& s) { lenv_root = s.half_left(psiL, lf, expanded, nL, ledgerL); },
+                   [&](Step& s) { rr = s.half_right(psi, rf, expanded, nR, ledgerR); },
+                   S.fork_stream());
+    } else {
+      lenv_root = S.half_left(psiL, lf, expanded, nL, ledgerL);
+      rr = S.half_right(psi, rf, expanded, nR, ledgerR);
+    }
     T renv_root = rr.first, AR = rr.second;
     ledger.merge(ledgerL);
     ledger.merge(ledgerR);
@@ -2773,7 +2899,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
         Step::KL kf{lf, rf, lenv_root, renv_root, 0};
         if (e.buf) e.buf->save();
         else prm->rng_ctl(prm->rng_ctl_user, 0);
-        auto sw = S.frontier_sweep(kf, psi, core, std::max(e.norm(core), EPS), false);
+        auto sw = S.frontier_sweep(kf, psi, core, std::max(e.norm(core), EPS), false, false);
         if (e.buf) e.buf->restore();
         else prm->rng_ctl(prm->rng_ctl_user, 1);
         for (double x : sw.leaks_left) a.left += x * x;

@@ -22,6 +22,17 @@ UNMET_NAMES = {1: "sample", 2: "tail", 3: "krylov", 4: "trunc", 5: "projection",
 
 
 RNG_CTL_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int)
+DRAW_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double))
+RNG_FORK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(DRAW_FN),
+                               ctypes.POINTER(ctypes.c_void_p))
+
+
+def fork_rng(rng):
+    """The right half's own stream under ``parallel = true`` (``rngR = MersenneTwister(rand(rng,
+    UInt64))``, ``bug_step.jl:225``, ``frontier_closure.jl:125``): a generator seeded by ONE draw
+    of ``rng`` over the full unsigned 64-bit range."""
+    seed = int(rng.integers(0, np.iinfo(np.uint64).max, dtype=np.uint64, endpoint=True))
+    return np.random.default_rng(seed)
 
 
 class StepParams(ctypes.Structure):
@@ -38,7 +49,9 @@ class StepParams(ctypes.Structure):
                 ("eshift", ctypes.c_double), ("root_report", ctypes.c_int),
                 ("outside_residual", ctypes.c_int), ("rng_ctl", RNG_CTL_FN),
                 ("rng_ctl_user", ctypes.c_void_p), ("closure_checks", ctypes.c_int),
-                ("root_method", ctypes.c_int), ("root_noshift", ctypes.c_int)]
+                ("root_method", ctypes.c_int), ("root_noshift", ctypes.c_int),
+                ("parallel", ctypes.c_int), ("rng_fork", RNG_FORK_FN),
+                ("rng_fork_user", ctypes.c_void_p)]
 
 
 class BondLog(ctypes.Structure):
@@ -77,7 +90,6 @@ class StepInfo(ctypes.Structure):
                 ("outside_passes", ctypes.c_int), ("outside_added", ctypes.c_int)]
 
 
-DRAW_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_double))
 
 _declared = [False]
 
@@ -244,11 +256,29 @@ def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_
         raise NotImplementedError(f"root_method {root_method!r}: {tuple(methods)} are built")
     p.root_method = methods[root_method]
     p.root_noshift = 0 if root_shift else 1
+    forks = []  # the forked streams and their callbacks live until the step returns
+
+    @RNG_FORK_FN
+    def rng_fork(user, draw_out, user_out):
+        sub = fork_rng(rng)
+
+        @DRAW_FN
+        def draw_sub(u, n, out):
+            x = sub.standard_normal(int(n))
+            ctypes.memmove(out, x.ctypes.data, 8 * int(n))
+
+        forks.append((sub, draw_sub))
+        draw_out[0] = draw_sub
+        user_out[0] = None
+        return 0
+
+    p.parallel = int(parallel is True or parallel == "half_sweeps")
+    p.rng_fork = rng_fork
     p.eshift = float(eshift)
     p.root_report = int(root_report is not None)
     p.outside_residual = int(bool(outside_residual))
     p.rng_ctl = rng_ctl
-    return p, {"rng": rng, "rng_ctl": rng_ctl, "saved": saved}
+    return p, {"rng": rng, "rng_ctl": rng_ctl, "saved": saved, "rng_fork": rng_fork, "forks": forks}
 
 
 def _step_result(psi, ctx, arr, center, info, logs, nlog, order, eshift, root_report):

@@ -64,7 +64,7 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
     root_link = (L // 2) if root is None else root  # _bug_root_link: the middle bond
     if not 1 <= root_link <= L - 1:
         raise ValueError(f"root must be a bond in 1:{L - 1}, got {root_link}")
-    mode, run_parallel = _parallel_mode(parallel)
+    mode, _ = _parallel_mode(parallel)
     if mode == "full" and kls is None:
         kls = "concurrent"
     if tol_root is not None and tol_expv is not None:
@@ -106,8 +106,8 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
                              "re-enrichment")
     # valid, but not built here
     unbuilt = []
-    if run_parallel or kls is not None:
-        unbuilt.append(f"parallel = {parallel!r} / kls = {kls!r} (concurrent half-sweeps, K/L/S)")
+    if kls is not None:
+        unbuilt.append(f"parallel = {parallel!r} / kls = {kls!r} (the parallel K/L/S step)")
     if work_ceiling_rule not in BUILT_WORK_CEILING_RULES:
         unbuilt.append(f"work_ceiling_rule = :{work_ceiling_rule}")
     if frontier_tol > 0 or krylov_rank_tol > 0:

@@ -172,6 +172,20 @@ int bug_trim(bug_ctx* ctx, const bug_tensor* t, int leg, const int* counts, bug_
  * bug_step_stages.jl:309-317), so the step's own draws continue from the saved state. */
 typedef void (*bug_rng_ctl_fn)(void* user, int op);
 
+/* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
+ * sqrt(1/2), probe by probe: sectors in ascending charge, one C-ordered matrix over the fused
+ * space per sector (the caller's seeded generator stands in for the reference's `rng`,
+ * bug_step.jl:147). */
+typedef void (*bug_normal_fn)(void* user, int64_t n, double* out);
+
+/* parallel = true: the right half of a sweep draws from a stream of its own, seeded by ONE 64-bit
+ * draw from the step's stream at the point the reference calls `MersenneTwister(rand(rng,
+ * UInt64))` (bug_step.jl:225 for the half-sweeps, frontier_closure.jl:125 for each frontier
+ * sweep). The callee takes that draw from the step's stream, makes the new stream and returns its
+ * normal-draw callback in *draw / *draw_user (valid until the step returns; called from another
+ * thread than the step's). Returns 0, or non-zero to fail the step. */
+typedef int (*bug_rng_fork_fn)(void* user, bug_normal_fn* draw, void** draw_user);
+
 typedef struct {
   double tol_basis;           /* <= 0: 1e-5 */
   double tol_trunc;           /* < 0: 1e-7 */
@@ -210,13 +224,14 @@ typedef struct {
                                  4 radau2_gmres (the coupled stages by shifted GMRES) */
   int root_noshift;           /* 1: no imaginary-time spectral shift of the implicit roots
                                  (`root_shift = false`) */
+  int parallel;               /* 1: parallel = true (:half_sweeps): the two half-sweeps, and the two
+                                 halves of every frontier sweep, run at once on two streams driven
+                                 by two host threads (bug_step.jl:222-268,
+                                 frontier_closure.jl:121-145); needs rng_fork */
+  bug_rng_fork_fn rng_fork;
+  void* rng_fork_user;
 } bug_step_params;
 
-/* Fills `n` standard normal reals; the step consumes them pairwise as (re, im) scaled by
- * sqrt(1/2), probe by probe: sectors in ascending charge, one C-ordered matrix over the fused
- * space per sector (the caller's seeded generator stands in for the reference's `rng`,
- * bug_step.jl:147). */
-typedef void (*bug_normal_fn)(void* user, int64_t n, double* out);
 
 #define BUG_MAX_SITES 1024
 

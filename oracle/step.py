@@ -27,7 +27,7 @@ from __future__ import annotations
 
 import math
 import time
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -210,6 +210,16 @@ class Ctx:
     wcap: list
     rng: object
     eshift: float = 0.0  # the generators are H - eshift (shift_h, effective_operators.jl:110-129)
+    parallel: bool = False  # parallel = true: right halves draw from a stream forked off `rng`
+
+
+def fork_rng(rng):
+    """The right half-sweep's own stream under ``parallel = true``: a generator seeded by ONE 64-bit
+    draw from ``rng`` (``MersenneTwister(rand(rng, UInt64))``, ``bug_step.jl:225`` and
+    ``frontier_closure.jl:125``); here numpy's default generator seeded by ``rng.integers`` over the
+    full unsigned 64-bit range."""
+    seed = int(rng.integers(0, np.iinfo(np.uint64).max, dtype=np.uint64, endpoint=True))
+    return np.random.default_rng(seed)
 
 
 def shifted(y, x, s):
@@ -534,8 +544,11 @@ def frontier_sweep(fr: KLFrames, psi, mpo, core, degree, cx: Ctx, nrm, enrich=Tr
     FmR = Fm.copy()
     gen = fr.gen + 1
     amp = nF / max(nrm, np.finfo(float).eps)
+    # parallel: the right half draws from its own stream, forked here (frontier_closure.jl:125-145);
+    # the halves are independent, so running them one after the other gives the concurrent result
+    cxR = replace(cx, rng=fork_rng(cx.rng)) if cx.parallel else cx
     rl = frontier_left(Fm, mpo, fr, cx, amp, enrich, gen)
-    rr = frontier_right(FmR, mpo, fr, cx, amp, enrich, gen)
+    rr = frontier_right(FmR, mpo, fr, cxR, amp, enrich, gen)
     lg = Ledger()
     lg.merge(rl["ledger"])
     lg.merge(rr["ledger"])
@@ -934,8 +947,8 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
     if kls is not None and outside_residual:
         raise ValueError("the parallel K/L/S step does not combine with the outside-residual "
                          "re-enrichment")
-    if run_parallel or kls is not None:
-        raise NotImplementedError("parallel half-sweeps and the K/L/S step are not restated")
+    if kls is not None:
+        raise NotImplementedError("the parallel K/L/S step (parallel = :full, kls) is not restated")
     if work_ceiling_rule not in ("maxdim", "bond"):
         raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
     if frontier_tol > 0 or krylov_rank_tol > 0:
@@ -1009,13 +1022,17 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     nL = [0] * (L - 1)
     nR = [0] * (L - 1)
     accL, accR = HalfAcc(), HalfAcc()
-    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift)
+    run_parallel = parallel is True or parallel == "half_sweeps"
+    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel)
+    # parallel = true: the right half-sweep's stream is forked off the step's before either half
+    # runs (bug_step.jl:222-268)
+    cxR = replace(cx, rng=fork_rng(rng)) if run_parallel else cx
     ledgerL, ledgerR = Ledger(), Ledger()
     left_frames, right_frames = {}, {}
     psiL = psi.copy()
     psiR = psi
     lenv_root = half_left(psiL, left_frames, expanded, nL, accL, ledgerL, cx)
-    renv_root, AR = half_right(psiR, right_frames, expanded, nR, accR, ledgerR, cx)
+    renv_root, AR = half_right(psiR, right_frames, expanded, nR, accR, ledgerR, cxR)
     ledger.merge(ledgerL)
     ledger.merge(ledgerR)
     n_new = nL[: root_link - 1] + nR[root_link - 1:]
@@ -1076,7 +1093,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         bond_dims=psi.bond_dims(), start_ranks=bd0, workcap=wcap,
         record=dict(policy="dd_qr_streamed", qr_backend="householder",
                     closure="dd_qr_streamed" if order > 1 else "none", order=order,
-                    parallel_mode="serial", r_old=max(bd0, default=0),
+                    parallel_mode="half_sweeps" if run_parallel else "serial", r_old=max(bd0, default=0),
                     r_aug=max(max(expanded, default=0), root_frame_width),
                     r_final=max(psi.bond_dims(), default=0), maxdim=maxdim,
                     workcap=max(wcap) if isinstance(wcap, list) else wcap,

@@ -45,7 +45,6 @@ BAD = [
     (dict(kls="sequential", outside_residual=True, root_report={}), ValueError),
     (dict(kls="sequential"), NotImplementedError),
     (dict(parallel="bogus"), ValueError),
-    (dict(parallel=True), NotImplementedError),
     (dict(parallel="full"), NotImplementedError),
 ]
 
