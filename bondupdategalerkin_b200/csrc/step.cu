@@ -1174,23 +1174,23 @@ struct Step {
     return BondFrame{rl.U, core, rr.Vd, dim(rl.U, 2)};
   }
   BondFrame frame_onto_left(const T& liso, const T& carry, const T& right) {
-    SVDRes rr = svd(e, right, {0}, 0.0, -1, W_US | W_VD);
+    return frame_onto_left(liso, carry, svd(e, right, {0}, 0.0, -1, W_US | W_VD));
+  }
+  BondFrame frame_onto_left(const T& liso, const T& carry, const SVDRes& rr) {
     T ov = e.contract(liso, {0, 1}, carry, {0, 1}, true, false);
     return BondFrame{liso, e.contract(ov, {1}, US(e, rr), {0}), rr.Vd, dim(liso, 2)};
   }
   BondFrame frame_onto_right(const T& left, const T& carry, const T& riso) {
-    SVDRes rl = svd(e, left, {0, 1}, 0.0, -1, W_U | W_SVD);
+    return frame_onto_right(svd(e, left, {0, 1}, 0.0, -1, W_U | W_SVD), carry, riso);
+  }
+  BondFrame frame_onto_right(const SVDRes& rl, const T& carry, const T& riso) {
     T ov = e.contract(carry, {1, 2}, riso, {1, 2}, false, true);
     return BondFrame{rl.U, e.contract(SVd(e, rl), {1}, ov, {0}), riso, dim(riso, 0)};
   }
   T polar_frame(const T& frame, bool left) {
-    if (left) {
-      SVDRes r = svd(e, frame, {0, 1}, 0.0);
-      return e.contract(r.U, {2}, r.Vd, {0});
-    }
-    SVDRes r = svd(e, frame, {0}, 0.0);
-    return e.contract(r.U, {1}, r.Vd, {0});
+    return polar_of(left ? svd(e, frame, {0, 1}, 0.0) : svd(e, frame, {0}, 0.0), left);
   }
+  T polar_of(const SVDRes& r, bool left) { return e.contract(r.U, {left ? 2 : 1}, r.Vd, {0}); }
 
   // _record_sample! (sketch.jl:215-258): the ledger's sample maxima
   static void record_sample(Ledger* ledger, bool left, double ind) {
@@ -1859,7 +1859,17 @@ struct Step {
       if (!enrich) lch = chain[bond];
       T old = Pm ? e.contract(Pm, {1}, fr.lf.at(bond), {0}) : fr.lf.at(bond);
       T site_core = carry ? e.contract(carry, {1}, Fm[bond], {0}) : Fm[bond];
-      BondFrame tsf = frame_onto_left(old, site_core, Fm[bond + 1]);
+      // enriching: the frame's SVD and, ahead of the quiet test, the polar factor of `old` (the
+      // new frame of a quiet bond) come back together
+      SVDRes pol;
+      BondFrame tsf;
+      if (enrich) {
+        auto both = svd2(e, Fm[bond + 1], {0}, W_US | W_VD, old, {0, 1}, W_U | W_VD);
+        tsf = frame_onto_left(old, site_core, both.first);
+        pol = std::move(both.second);
+      } else {
+        tsf = frame_onto_left(old, site_core, Fm[bond + 1]);
+      }
       const T& rch = rstack[bond + 2];
       const double lk = bond_action(tsf, bond, lch, rch, true);
       out.leak.push_back(lk);
@@ -1880,7 +1890,7 @@ struct Step {
       } else {
         Wi = old;
       }
-      T Wn = enrich ? polar_frame(Wi, true) : old;
+      T Wn = !enrich ? old : (quiet ? polar_of(pol, true) : polar_frame(Wi, true));
       out.frames[bond] = Wn;
       out.added += dim(Wn, 2) - dim(old, 2);
       log_bond(out.ledger, bl, bond, 0, int(dim(Wn, 2)));
@@ -1913,7 +1923,15 @@ struct Step {
       if (!enrich) rch = chain[bond];
       T old = Pm ? e.contract(fr.rf.at(bond), {2}, Pm, {0}) : fr.rf.at(bond);
       T site_core = carry ? e.contract(Fm[bond + 1], {2}, carry, {0}) : Fm[bond + 1];
-      BondFrame tsf = frame_onto_right(Fm[bond], site_core, old);
+      SVDRes pol;
+      BondFrame tsf;
+      if (enrich) {
+        auto both = svd2(e, Fm[bond], {0, 1}, W_U | W_SVD, old, {0}, W_U | W_VD);
+        tsf = frame_onto_right(both.first, site_core, old);
+        pol = std::move(both.second);
+      } else {
+        tsf = frame_onto_right(Fm[bond], site_core, old);
+      }
       const T& lch = lstack[bond];
       const double lk = bond_action(tsf, bond, lch, rch, false);
       leak[bond] = lk;
@@ -1934,7 +1952,7 @@ struct Step {
       } else {
         Zj = old;
       }
-      T Zn = enrich ? polar_frame(Zj, false) : old;
+      T Zn = !enrich ? old : (quiet ? polar_of(pol, false) : polar_frame(Zj, false));
       out.frames[bond] = Zn;
       out.added += dim(Zn, 0) - dim(old, 0);
       log_bond(out.ledger, bl, bond, 1, int(dim(Zn, 0)));
