@@ -281,37 +281,60 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   std::vector<int> iaa(ia, ia + n), ibb(ib, ib + n);
   const std::vector<int>& fa2 = fa;
   const std::vector<int>& fb2 = fb;
-  // match blocks
-  std::map<std::vector<int>, std::vector<int>> groups;
+  // match blocks: B's blocks ordered by their contracted charges (a stable sort keeps equal ones
+  // in block order), each A block against its run; the (A block, B block) pairs of every output
+  // key then in A-block-major order, output keys ascending (a stable sort of the pair list)
+  struct BRef {
+    std::array<int, BUG_MAX_RANK> ck;
+    int bi;
+  };
+  auto ck_less = [n](const BRef& x, const BRef& y) {
+    return std::lexicographical_compare(x.ck.begin(), x.ck.begin() + n, y.ck.begin(),
+                                        y.ck.begin() + n);
+  };
+  std::vector<BRef> bref(B->blocks.size());
   for (int bi = 0; bi < int(B->blocks.size()); ++bi) {
-    std::vector<int> ck(n);
-    for (int k = 0; k < n; ++k) ck[k] = B->blocks[bi].key[ibb[k]];
-    groups[ck].push_back(bi);
+    bref[size_t(bi)].bi = bi;
+    for (int k = 0; k < n; ++k) bref[size_t(bi)].ck[size_t(k)] = B->blocks[bi].key[ibb[k]];
   }
-  std::map<Key, std::vector<std::pair<int, int>>> outmap;
+  std::stable_sort(bref.begin(), bref.end(), ck_less);
+  struct OutPair {
+    Key ok;
+    int ai, bi;
+  };
+  std::vector<OutPair> ops;
+  ops.reserve(A->blocks.size());
+  BRef probe{};
   for (int ai = 0; ai < int(A->blocks.size()); ++ai) {
-    std::vector<int> ck(n);
-    for (int k = 0; k < n; ++k) ck[k] = A->blocks[ai].key[iaa[k]];
-    auto it = groups.find(ck);
-    if (it == groups.end()) continue;
-    for (int bi : it->second) {
-      Key ok{};
+    for (int k = 0; k < n; ++k) probe.ck[size_t(k)] = A->blocks[ai].key[iaa[k]];
+    auto run = std::equal_range(bref.begin(), bref.end(), probe, ck_less);
+    for (auto it = run.first; it != run.second; ++it) {
+      OutPair e{};
       int p = 0;
-      for (int i : fa2) ok[p++] = A->blocks[ai].key[i];
-      for (int i : fb2) ok[p++] = B->blocks[bi].key[i];
-      outmap[ok].push_back({ai, bi});
+      for (int i : fa2) e.ok[p++] = A->blocks[ai].key[i];
+      for (int i : fb2) e.ok[p++] = B->blocks[it->bi].key[i];
+      e.ai = ai;
+      e.bi = it->bi;
+      ops.push_back(e);
     }
   }
+  std::stable_sort(ops.begin(), ops.end(),
+                   [](const OutPair& x, const OutPair& y) { return x.ok < y.ok; });
   std::vector<Key> keys;
-  for (auto& kv : outmap) keys.push_back(kv.first);
+  for (size_t i = 0; i < ops.size(); ++i)
+    if (i == 0 || ops[i].ok != ops[i - 1].ok) keys.push_back(ops[i].ok);
   auto out = make_tensor(c, ro, legs, keys, false);
   if (keys.empty()) return out;
   std::vector<GemmOut> outs;
   std::vector<GemmPair> pairs;
   std::vector<GemmTile> tiles;
   std::vector<int> mixed;  // outputs the tensor-core path computes
-  for (auto& kv : outmap) {
-    int oj = out->find(kv.first);
+  outs.reserve(keys.size());
+  pairs.reserve(ops.size());
+  for (size_t r0 = 0, oj = 0; r0 < ops.size(); ++oj) {
+    size_t r1 = r0 + 1;
+    while (r1 < ops.size() && ops[r1].ok == ops[r0].ok) ++r1;
+    require(out->blocks[oj].key == ops[r0].ok, "contract: output block order");
     const Block& ob = out->blocks[oj];
     GemmOut go{};
     go.C = out->mdata(oj);
@@ -321,18 +344,19 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
     go.m = int(m);
     go.n = int(nn);
     go.pair_begin = int(pairs.size());
-    for (auto& pr : kv.second) {
-      const Block& ab = A->blocks[pr.first];
-      const Block& bb = B->blocks[pr.second];
+    for (size_t r = r0; r < r1; ++r) {
+      const Block& ab = A->blocks[ops[r].ai];
+      const Block& bb = B->blocks[ops[r].bi];
       int64_t K = 1;
       for (int k = 0; k < n; ++k) K *= ab.shape[iaa[k]];
       GemmPair gp{};
       gp.k = int(K);
-      make_operand(gp.A, A->data(pr.first), ab, fa2, iaa, conja);
-      make_operand(gp.B, B->data(pr.second), bb, ibb, fb2, conjb);
+      make_operand(gp.A, A->data(ops[r].ai), ab, fa2, iaa, conja);
+      make_operand(gp.B, B->data(ops[r].bi), bb, ibb, fb2, conjb);
       pairs.push_back(gp);
     }
     go.pair_end = int(pairs.size());
+    r0 = r1;
     int o = int(outs.size());
     outs.push_back(go);
     if (c->mixed_min_dim > 0 && bugtc::mixed_block(int(m), int(nn), c->mixed_min_dim)) {
@@ -480,38 +504,48 @@ void svd_finish(bug_ctx* c, SvdJob& job, const SvdReq& q, double2* W, double* S,
   std::unique_ptr<bug_tensor>& Vd = *q.Vd;
   std::unique_ptr<bug_tensor>* USo = q.USo;
   std::unique_ptr<bug_tensor>* SVdo = q.SVdo;
-  // selection (Telum): sigma > cutoff*smax, stable descending sort, Nkeep
-  struct Entry {
-    double sv;
-    int s, j;
-  };
-  std::vector<Entry> entries;
-  double smax = 0.0;
-  for (int s = 0; s < np; ++s) {
-    int64_t r = std::min(order[s]->m, order[s]->n);
-    for (int j = 0; j < r; ++j) {
-      double v = host[soff[s] + j];
-      require(std::isfinite(v), "non-finite singular value");
-      smax = std::max(smax, v);
-      entries.push_back({v, s, j});
-    }
-  }
-  std::stable_sort(entries.begin(), entries.end(),
-                   [](const Entry& a, const Entry& b) { return a.sv > b.sv; });
-  const double thresh = cutoff * smax;
-  int nsel = 0;
-  for (auto& e : entries)
-    if (e.sv > thresh) ++nsel;
-  if (nkeep >= 0) nsel = std::min(nsel, nkeep);
   std::vector<int> kc(np, 0);
-  for (int i = 0; i < nsel; ++i) kc[entries[i].s]++;
   sv_sorted.clear();
   sv_q.clear();
-  for (auto& e : entries) {
-    sv_sorted.push_back(e.sv);
-    sv_q.push_back(order[e.s]->charge);
+  if (!host) {
+    // taken ahead (svd_ahead): every sector keeps all min(m, n) columns, which is the selection
+    // below exactly when cutoff is 0, no Nkeep applies and every singular value is positive
+    nkept = 0;
+    for (int s = 0; s < np; ++s) {
+      kc[s] = int(std::min(order[s]->m, order[s]->n));
+      nkept += kc[s];
+    }
+  } else {
+    // selection (Telum): sigma > cutoff*smax, stable descending sort, Nkeep
+    struct Entry {
+      double sv;
+      int s, j;
+    };
+    std::vector<Entry> entries;
+    double smax = 0.0;
+    for (int s = 0; s < np; ++s) {
+      int64_t r = std::min(order[s]->m, order[s]->n);
+      for (int j = 0; j < r; ++j) {
+        double v = host[soff[s] + j];
+        require(std::isfinite(v), "non-finite singular value");
+        smax = std::max(smax, v);
+        entries.push_back({v, s, j});
+      }
+    }
+    std::stable_sort(entries.begin(), entries.end(),
+                     [](const Entry& a, const Entry& b) { return a.sv > b.sv; });
+    const double thresh = cutoff * smax;
+    int nsel = 0;
+    for (auto& e : entries)
+      if (e.sv > thresh) ++nsel;
+    if (nkeep >= 0) nsel = std::min(nsel, nkeep);
+    for (int i = 0; i < nsel; ++i) kc[entries[i].s]++;
+    for (auto& e : entries) {
+      sv_sorted.push_back(e.sv);
+      sv_q.push_back(order[e.s]->charge);
+    }
+    nkept = nsel;
   }
-  nkept = nsel;
   // build U and Vd
   Leg bondU, bondV;
   bondU.dir = +1;
@@ -614,32 +648,50 @@ void svd_finish(bug_ctx* c, SvdJob& job, const SvdReq& q, double2* W, double* S,
 // The SVDs of several tensors: one Jacobi launch over all their sectors and one read-back; then
 // each tensor's Telum selection and its factors, exactly as one call per tensor would give them
 // (a sector's arithmetic does not depend on the other sectors of the launch).
-void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs) {
-  std::vector<SvdJob> jobs(reqs.size());
+// The jobs of one SVD launch: plans, workspace and where each job's parts start.
+struct SvdBatch {
+  std::vector<SvdJob> jobs;
+  std::vector<int64_t> wbase, sbase, pbase;
   int64_t wtot = 0, stot = 0, nptot = 0;
-  std::vector<int64_t> wbase(reqs.size()), sbase(reqs.size()), pbase(reqs.size());
+  double2* W0 = nullptr;
+  double* S0 = nullptr;
+};
+
+static void svd_plan_batch(bug_ctx* c, const std::vector<SvdReq>& reqs, SvdBatch& B) {
+  B.jobs.resize(reqs.size());
+  B.wbase.resize(reqs.size());
+  B.sbase.resize(reqs.size());
+  B.pbase.resize(reqs.size());
   for (size_t r = 0; r < reqs.size(); ++r) {
-    svd_plan(jobs[r], *reqs[r].t, reqs[r].nleft, reqs[r].left);
-    wbase[r] = wtot;
-    sbase[r] = stot;
-    pbase[r] = nptot;
-    wtot += jobs[r].wtot;
-    stot += jobs[r].stot;
-    nptot += jobs[r].np;
+    svd_plan(B.jobs[r], *reqs[r].t, reqs[r].nleft, reqs[r].left);
+    B.wbase[r] = B.wtot;
+    B.sbase[r] = B.stot;
+    B.pbase[r] = B.nptot;
+    B.wtot += B.jobs[r].wtot;
+    B.stot += B.jobs[r].stot;
+    B.nptot += B.jobs[r].np;
   }
-  double2* W0 = static_cast<double2*>(c->scratch(size_t(std::max<int64_t>(wtot, 1)) * sizeof(double2)));
-  double* S0 = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(stot, 1)) * sizeof(double)));
-  // singular values and sweep counts also go straight to host-mapped pinned memory
-  double* host0 = c->readback(size_t(stot) + size_t(nptot) + 1);
-  int* sweeps0 = reinterpret_cast<int*>(host0 + stot);
-  for (int64_t q = 0; q < nptot; ++q) sweeps0[q] = 0;
+  B.W0 = static_cast<double2*>(c->scratch(size_t(std::max<int64_t>(B.wtot, 1)) * sizeof(double2)));
+  B.S0 = static_cast<double*>(c->scratch(size_t(std::max<int64_t>(B.stot, 1)) * sizeof(double)));
+}
+
+// The Jacobi launch of a planned batch; singular values and sweep counts also go straight to the
+// host-mapped pinned memory at host0 (stot values) and sweeps0 (nptot counts).
+static void svd_launch_batch(bug_ctx* c, SvdBatch& B, double* host0, int* sweeps0) {
+  std::vector<SvdJob>& jobs = B.jobs;
+  double2* W0 = B.W0;
+  double* S0 = B.S0;
+  const std::vector<int64_t>& wbase = B.wbase;
+  const std::vector<int64_t>& sbase = B.sbase;
+  const std::vector<int64_t>& pbase = B.pbase;
+  for (int64_t q = 0; q < B.nptot; ++q) sweeps0[q] = 0;
   const int smem_limit = bugk::svd_smem_limit();
   std::vector<SvdDesc> sd;
   std::vector<CopyDesc> packs;
   int max_smem = 0;
   int64_t max_r = 0;
   double sbytes = 0.0, sflops = 0.0;
-  for (size_t r = 0; r < reqs.size(); ++r) {
+  for (size_t r = 0; r < jobs.size(); ++r) {
     SvdJob& j = jobs[r];
     const bug_tensor& t = *j.t;
     const std::vector<int>& L = j.L;
@@ -737,12 +789,57 @@ void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs) {
     bugk::launch_svd(blob, dsd, np, dpk, max_smem, 32 * warps, c->stream);
     c->launched(BUG_K_SVD, sflops, sbytes);
   }
+}
+
+void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs) {
+  SvdBatch B;
+  svd_plan_batch(c, reqs, B);
+  double* host0 = c->readback(size_t(B.stot) + size_t(B.nptot) + 1);
+  int* sweeps0 = reinterpret_cast<int*>(host0 + B.stot);
+  svd_launch_batch(c, B, host0, sweeps0);
   // the kernel wrote singular values and sweep counts into `host`
   c->wait();
-  for (int64_t q = 0; q < nptot; ++q)
+  for (int64_t q = 0; q < B.nptot; ++q)
     if (sweeps0[q] < 0) throw BugError(BUG_ENOTCONV, "Jacobi SVD did not converge within its sweep bound");
   for (size_t r = 0; r < reqs.size(); ++r)
-    svd_finish(c, jobs[r], reqs[r], W0 + wbase[r], S0 + sbase[r], host0 + sbase[r]);
+    svd_finish(c, B.jobs[r], reqs[r], B.W0 + B.wbase[r], B.S0 + B.sbase[r], host0 + B.sbase[r]);
+}
+
+bool svd_ahead(bug_ctx* c, const std::vector<SvdReq>& reqs) {
+  for (auto& q : reqs)
+    require(q.cutoff == 0.0 && q.nkeep < 0, "an SVD taken ahead keeps every column");
+  if (!c->ahead_host) {
+    BUG_CUDA(cudaHostAlloc((void**)&c->ahead_host, bug_ctx::kAheadCap * sizeof(double),
+                           cudaHostAllocDefault));
+  }
+  SvdBatch B;
+  svd_plan_batch(c, reqs, B);
+  const size_t need = size_t(B.stot) + size_t(B.nptot) + 1;
+  if (c->ahead_used + need > bug_ctx::kAheadCap) return false;
+  double* host0 = c->ahead_host + c->ahead_used;
+  int* sweeps0 = reinterpret_cast<int*>(host0 + B.stot);
+  c->ahead.push_back({c->ahead_used, size_t(B.stot), size_t(B.nptot)});
+  c->ahead_used += need;
+  svd_launch_batch(c, B, host0, sweeps0);
+  for (size_t r = 0; r < reqs.size(); ++r)
+    svd_finish(c, B.jobs[r], reqs[r], B.W0 + B.wbase[r], B.S0 + B.sbase[r], nullptr);
+  return true;
+}
+
+bool svd_ahead_check(bug_ctx* c) {
+  bool ok = true;
+  if (!c->ahead.empty()) {
+    c->wait();
+    for (auto& a : c->ahead) {
+      const double* sv = c->ahead_host + a.off;
+      for (size_t i = 0; i < a.nsv; ++i) ok &= std::isfinite(sv[i]) && sv[i] > 0.0;
+      const int* sw = reinterpret_cast<const int*>(sv + a.nsv);
+      for (size_t i = 0; i < a.nsweeps; ++i) ok &= sw[i] >= 0;
+    }
+  }
+  c->ahead.clear();
+  c->ahead_used = 0;
+  return ok;
 }
 
 int svd_impl(bug_ctx* c, const bug_tensor& t, int nleft, const int* left, double cutoff, int nkeep,
@@ -1126,6 +1223,8 @@ int guard(const std::function<void()>& f) {
     if (rc != BUG_OK) c->discard_queue();
     for (void* p : c->deferred) c->dev_free(p);
     c->deferred.clear();
+    c->ahead.clear();  // SVDs taken ahead and left unchecked by a failed call
+    c->ahead_used = 0;
   }
   g_active_ctx = nullptr;
   return rc;
@@ -1440,6 +1539,7 @@ void ctx_release(bug_ctx* c) {
     cudaEventDestroy(c->stage_ev[i]);
   }
   if (c->pinned_out) cudaFreeHost(c->pinned_out);
+  if (c->ahead_host) cudaFreeHost(c->ahead_host);
   if (c->tc_err_host) cudaFreeHost(c->tc_err_host);
   if (c->arena) cudaFreeAsync(c->arena, c->stream);
   c->release_cached();
@@ -1467,6 +1567,8 @@ bug_ctx* fork_begin(bug_ctx* c) {
   ch->queue_max_stages = c->queue_max_stages;
   ch->queue_rounds = c->queue_rounds;
   ch->mixed_min_dim = c->mixed_min_dim;
+  ch->ahead.clear();  // anything a failed half left unchecked
+  ch->ahead_used = 0;
   if (!c->fork_ev) BUG_CUDA(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
   if (!ch->fork_ev) BUG_CUDA(cudaEventCreateWithFlags(&ch->fork_ev, cudaEventDisableTiming));
   c->drain();  // every queued stage of the parent is enqueued before the fork event

@@ -424,6 +424,14 @@ struct bug_ctx {
   // and the host reads them after a stream synchronisation, with no copy in between.
   double* pinned_out = nullptr;
   size_t pinned_out_cap = 0;
+  // SVDs taken ahead of their check (svd_ahead): their singular values and sweep counts
+  static constexpr size_t kAheadCap = size_t(1) << 20;  // doubles
+  double* ahead_host = nullptr;
+  size_t ahead_used = 0;
+  struct Ahead {
+    size_t off, nsv, nsweeps;
+  };
+  std::vector<Ahead> ahead;
 
   void* stage(size_t bytes) {
     int s = stage_next;
@@ -655,6 +663,15 @@ struct SvdReq {
 };
 // Several tensors' SVDs (each as svd_impl) in one launch and one read-back.
 void svd_many(bug_ctx* c, const std::vector<SvdReq>& reqs);
+// SVDs with cutoff 0 and no Nkeep taken AHEAD of their read-back: every charge sector keeps all
+// min(m, n) columns, which is what svd_many returns whenever no singular value is exactly zero
+// (or non-finite) and every sector converged. Their singular values and sweep counts go to the
+// context's pinned `ahead` region; svd_ahead_check waits for the stream and says whether every
+// SVD taken ahead since the last check met that assumption, so a caller whose work is a pure
+// function of its inputs can redo it the exact way when it did not. Returns false, launching
+// nothing, when the region is full.
+bool svd_ahead(bug_ctx* c, const std::vector<SvdReq>& reqs);
+bool svd_ahead_check(bug_ctx* c);
 void dots(bug_ctx* c, const std::vector<std::pair<const bug_tensor*, const bug_tensor*>>& pairs,
           double* out_re_im);
 // sum_i coef_i t_i; with cmode[i] != 0 the coefficient of t_i is computed on the device from the

@@ -282,6 +282,25 @@ SVDRes svd(const Eng& e, const T& t, std::vector<int> left, double cutoff, int n
   return r;
 }
 
+// An SVD with cutoff 0 taken ahead of its read-back (svd_ahead: every sector keeps min(m, n)
+// columns); false when the context's region for them is full. Only the factors are returned (no
+// singular value lists): ask for U*S / S*Vd through `want`. Valid once svd_ahead_check says so.
+bool svd_ahead1(const Eng& e, const T& t, std::vector<int> left, int want, SVDRes& r) {
+  TensorPtr U, V, US_, SV_;
+  std::vector<double> sv;
+  std::vector<int> q;
+  int nk = 0;
+  if (!svd_ahead(e.c, {SvdReq{t.get(), int(left.size()), left.data(), 0.0, -1, want, &U, &V, &sv,
+                              &q, &nk, &US_, &SV_}}))
+    return false;
+  r = SVDRes{};
+  if (U) r.U = Eng::sh(std::move(U));
+  if (V) r.Vd = Eng::sh(std::move(V));
+  if (US_) r.Us = Eng::sh(std::move(US_));
+  if (SV_) r.SVd_ = Eng::sh(std::move(SV_));
+  return true;
+}
+
 // Two independent SVDs (cutoff 0, no Nkeep) in one launch and one read-back, each result as svd()
 // gives it.
 std::pair<SVDRes, SVDRes> svd2(const Eng& e, const T& t1, std::vector<int> left1, int want1,
@@ -1123,24 +1142,39 @@ struct Step {
   }
 
   // canonical form (canonical_form.jl)
-  void move_right(MPS& psi, int site) {
-    SVDRes r = svd(e, psi[site], {0, 1}, 0.0, -1, W_U | W_SVD);
+  // `ahead`: the move's SVD is taken ahead of its read-back (svd_ahead) when there is room
+  void move_right(MPS& psi, int site, bool ahead = false) {
+    SVDRes r;
+    if (!ahead || !svd_ahead1(e, psi[site], {0, 1}, W_U | W_SVD, r))
+      r = svd(e, psi[site], {0, 1}, 0.0, -1, W_U | W_SVD);
     psi[site + 1] = e.contract(SVd(e, r), {1}, psi[site + 1], {0});
     psi[site] = r.U;
   }
-  void move_left(MPS& psi, int site) {
-    SVDRes r = svd(e, psi[site], {0}, 0.0, -1, W_VD | W_US);
+  void move_left(MPS& psi, int site, bool ahead = false) {
+    SVDRes r;
+    if (!ahead || !svd_ahead1(e, psi[site], {0}, W_VD | W_US, r))
+      r = svd(e, psi[site], {0}, 0.0, -1, W_VD | W_US);
     psi[site - 1] = e.contract(psi[site - 1], {2}, US(e, r), {0});
     psi[site] = r.Vd;
   }
+  // The moves are a pure function of psi, so their SVDs are taken ahead (no read-back per move)
+  // and checked once at the end; if a move met an exactly zero or non-finite singular value (or an
+  // unconverged sector), the moves are redone from the saved state with read-backs, as the
+  // reference's svd with cutoff 0 takes them.
   void canonical(MPS& psi, int site) {
-    while (psi.center < site) {
-      move_right(psi, psi.center);
-      psi.center += 1;
-    }
-    while (psi.center > site) {
-      move_left(psi, psi.center);
-      psi.center -= 1;
+    if (psi.center == site) return;
+    MPS saved = psi;
+    for (bool ahead : {true, false}) {
+      if (!ahead) psi = saved;
+      while (psi.center < site) {
+        move_right(psi, psi.center, ahead);
+        psi.center += 1;
+      }
+      while (psi.center > site) {
+        move_left(psi, psi.center, ahead);
+        psi.center -= 1;
+      }
+      if (!ahead || svd_ahead_check(e.c)) return;
     }
   }
   int total_charge(const MPS& psi) const { return psi[psi.size()]->legs[2].q.at(0); }
@@ -1730,17 +1764,28 @@ struct Step {
     return AR;
   }
   // The outside components' squared norms go to device slots and come back in one read-back at
-  // the end, summed in the order the terms arise.
+  // the end, summed in the order the terms arise; the factors' SVDs are taken ahead (svd_ahead)
+  // and checked with that read-back, the measurement redone with read-backs if one failed.
   double projection_miss(const MPS& psi, std::map<int, T>& lf, std::map<int, T>& rf) {
+    double out = 0.0;
+    if (!projection_miss_once(psi, lf, rf, true, out)) projection_miss_once(psi, lf, rf, false, out);
+    return out;
+  }
+  bool projection_miss_once(const MPS& psi, std::map<int, T>& lf, std::map<int, T>& rf, bool ahead,
+                            double& out) {
     double2* n2 = static_cast<double2*>(e.c->scratch(size_t(L + 1) * sizeof(double2)));
     int nterm = 0;
     auto miss_term = [&](const T& x) { dots_device(e.c, {{x.get(), x.get()}}, n2 + nterm++); };
+    auto factor = [&](const T& t, std::vector<int> left, int want) {
+      SVDRes r;
+      if (!ahead || !svd_ahead1(e, t, left, want, r)) r = svd(e, t, left, 0.0, -1, want);
+      return r;
+    };
     std::vector<T> rfac(L + 2);
     for (int site = L; site >= 2; --site) {
       T carried = site == L ? psi[L] : e.contract(psi[site], {2}, rfac[site + 1], {0});
-      rfac[site] = US(e, svd(e, carried, {0}, 0.0, -1, W_US));
+      rfac[site] = US(e, factor(carried, {0}, W_US));
     }
-    double miss2 = 0.0;
     T AL;
     for (int site = 1; site <= root_link; ++site) {
       T carried = AL ? e.contract(AL, {1}, psi[site], {0}) : psi[site];
@@ -1749,9 +1794,9 @@ struct Step {
       AL = e.contract(lf[site], {0, 1}, carried, {0, 1}, true, false);
     }
     std::vector<T> lfac(L + 1);
-    lfac[root_link] = SVd(e, svd(e, AL, {0}, 0.0, -1, W_SVD));
+    lfac[root_link] = SVd(e, factor(AL, {0}, W_SVD));
     for (int bond = root_link + 1; bond <= L - 1; ++bond)
-      lfac[bond] = SVd(e, svd(e, e.contract(lfac[bond - 1], {1}, psi[bond], {0}), {0, 1}, 0.0, -1, W_SVD));
+      lfac[bond] = SVd(e, factor(e.contract(lfac[bond - 1], {1}, psi[bond], {0}), {0, 1}, W_SVD));
     T AR;
     for (int bond = L - 1; bond >= root_link; --bond) {
       T carried = AR ? e.contract(psi[bond + 1], {2}, AR, {0}) : psi[bond + 1];
@@ -1759,15 +1804,19 @@ struct Step {
       miss_term(e.contract(lfac[bond], {1}, outside, {0}));
       AR = e.contract(carried, {1, 2}, rf[bond], {1, 2}, false, true);
     }
+    double* host = e.c->readback(size_t(2 * std::max(nterm, 1)));
     if (nterm > 0) {
-      double* host = e.c->readback(size_t(2 * nterm));
       e.c->drain();  // the queued dot stages write the slots: they run before the copy
       BUG_CUDA(cudaMemcpyAsync(host, n2, size_t(nterm) * sizeof(double2), cudaMemcpyDeviceToHost,
                                e.c->stream));
-      e.c->wait();
-      for (int i = 0; i < nterm; ++i) miss2 += std::pow(std::sqrt(std::max(host[2 * i], 0.0)), 2);
     }
-    return std::sqrt(miss2);
+    const bool waited = !e.c->ahead.empty();  // the check waits, for the copy too
+    if (!svd_ahead_check(e.c)) return false;
+    if (nterm > 0 && !waited) e.c->wait();
+    double miss2 = 0.0;
+    for (int i = 0; i < nterm; ++i) miss2 += std::pow(std::sqrt(std::max(host[2 * i], 0.0)), 2);
+    out = std::sqrt(miss2);
+    return true;
   }
 
   // ── closure (single pass, folded leak) ──

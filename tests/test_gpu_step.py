@@ -313,3 +313,45 @@ def test_native_step_converges_at_order_p_plus_one(dev, order):
         errs.append(np.linalg.norm(dense - exact) / np.linalg.norm(exact))
     assert errs[0] / errs[1] > 0.85 * 2 ** (order + 1), errs
     assert errs[1] < (1e-3 if order == 1 else 1e-5), errs
+
+
+def _zero_padded_domain_wall(L):
+    """The domain-wall state with a second, all-zero charge sector on its middle bond (charge
+    h - 2 beside h = L / 2, reached from site h's left sector by a down spin and left into site
+    h + 1's right sector by an up spin): the same state, but a canonical move across that bond
+    meets singular values that are exactly zero, which the reference's cutoff-0 SVD drops."""
+    from oracle.blocks import BT, Leg
+
+    h = L // 2
+    psi = OM.domain_wall_state(L)
+    a, b = psi[h], psi[h + 1]
+    z = np.zeros((1, 1, 1), dtype=np.complex128)
+    mid = {h - 2: 1, h: 1}
+    psi.tensors[h - 1] = BT([a.legs[0], a.legs[1], Leg(+1, mid)], {**a.blocks, (h - 1, -1, h - 2): z})
+    psi.tensors[h] = BT([Leg(-1, mid), b.legs[1], b.legs[2]], {**b.blocks, (h - 2, 1, h - 1): z.copy()})
+    return psi
+
+
+@pytest.mark.parametrize("parallel", [False, True])
+def test_exact_zero_singular_values_redo_the_moves(dev, parallel):
+    """Canonical moves take their SVDs ahead of the read-back and assume no exactly zero singular
+    value; on a state padded with an all-zero sector that assumption fails, the moves are redone
+    with read-backs, and the step follows the oracle (which drops the zero sector) at the usual
+    bars."""
+    DM, _ = dev
+    from bondupdategalerkin_b200 import native as DN
+    from tests.gpu_util import to_dev
+
+    L = 12
+    ostate = _zero_padded_domain_wall(L)
+    assert ostate.bond_dims()[L // 2 - 1] == 2
+    dstate = DM.MPS([to_dev(t) for t in ostate.tensors], ostate.center)
+    ompo, dmpo = OM.xxz_mpo(L, J=1.0, delta=0.5), DM.xxz_mpo(L, J=1.0, delta=0.5)
+    orng, drng = np.random.default_rng(7), np.random.default_rng(7)
+    kw = dict(order=2, tol_basis=1e-4, maxdim=32, parallel=parallel)
+    for n in range(3):
+        oi = OS.cbe_bug_step(ostate, ompo, -0.05j, rng=orng, **kw)
+        di = DN.cbe_bug_step(dstate, dmpo, -0.05j, rng=drng, **kw)
+        assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
+        assert di["status"] == oi["status"] and di["expanded"] == oi["expanded"], n
+        assert 1.0 - fidelity(mps_to_host(dstate), ostate) <= 1e-12, n
