@@ -208,31 +208,28 @@ std::unique_ptr<bug_tensor> permute_impl(bug_ctx* c, const bug_tensor& t, const 
 // strides chain are merged, so the kernel decomposes as few indices as possible.
 void make_group(const Block& b, const std::array<int64_t, BUG_MAX_RANK>& st,
                 const std::vector<int>& legs, int& n, int* d, int64_t* s) {
-  std::vector<int> dd;
-  std::vector<int64_t> ss;
+  int dd[BUG_MAX_RANK];
+  int64_t ss[BUG_MAX_RANK];
+  int k = 0;
   for (int l : legs) {
-    if (!dd.empty() && ss.back() == int64_t(b.shape[l]) * st[l]) {
-      dd.back() *= b.shape[l];
-      ss.back() = st[l];
+    if (k > 0 && ss[k - 1] == int64_t(b.shape[l]) * st[l]) {
+      dd[k - 1] *= b.shape[l];
+      ss[k - 1] = st[l];
     } else {
-      dd.push_back(b.shape[l]);
-      ss.push_back(st[l]);
+      dd[k] = b.shape[l];
+      ss[k] = st[l];
+      ++k;
     }
   }
   // drop unit dims
-  std::vector<int> d2;
-  std::vector<int64_t> s2;
-  for (size_t i = 0; i < dd.size(); ++i)
+  n = 0;
+  for (int i = 0; i < k; ++i)
     if (dd[i] != 1) {
-      d2.push_back(dd[i]);
-      s2.push_back(ss[i]);
+      require(n < bugk::kGroup, "contract: operand index group too deep");
+      d[n] = dd[i];
+      s[n] = ss[i];
+      ++n;
     }
-  require(int(d2.size()) <= bugk::kGroup, "contract: operand index group too deep");
-  n = int(d2.size());
-  for (int i = 0; i < n; ++i) {
-    d[i] = d2[i];
-    s[i] = s2[i];
-  }
 }
 
 void make_operand(bugk::Operand& op, const double2* p, const Block& b, const std::vector<int>& rows,
@@ -245,6 +242,24 @@ void make_operand(bugk::Operand& op, const double2* p, const Block& b, const std
   make_group(b, st, cols, op.nc, op.cd, op.cs);
   op.row_fast = (op.nr > 0 && op.rs[op.nr - 1] == 1) ? 1 : 0;
 }
+
+// Per-thread planning arrays of contract_impl.
+struct BRef {
+  std::array<int, BUG_MAX_RANK> ck;  // the block's charges on the contracted legs
+  int bi;
+};
+struct OutPair {
+  Key ok;  // output block key
+  int ai, bi;
+};
+struct ContractPlan {
+  std::vector<BRef> bref;
+  std::vector<OutPair> ops;
+  std::vector<GemmOut> outs;
+  std::vector<GemmPair> pairs;
+  std::vector<GemmTile> tiles;
+  std::vector<int> mixed;
+};
 
 std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int n, const int* ia,
                                           const bug_tensor& B0, const int* ib, bool conja,
@@ -284,26 +299,21 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
   // match blocks: B's blocks ordered by their contracted charges (a stable sort keeps equal ones
   // in block order), each A block against its run; the (A block, B block) pairs of every output
   // key then in A-block-major order, output keys ascending (a stable sort of the pair list)
-  struct BRef {
-    std::array<int, BUG_MAX_RANK> ck;
-    int bi;
-  };
+  // the planning arrays live per thread across calls (their capacity is reused, no allocation)
+  thread_local ContractPlan plan;
   auto ck_less = [n](const BRef& x, const BRef& y) {
     return std::lexicographical_compare(x.ck.begin(), x.ck.begin() + n, y.ck.begin(),
                                         y.ck.begin() + n);
   };
-  std::vector<BRef> bref(B->blocks.size());
+  std::vector<BRef>& bref = plan.bref;
+  bref.resize(B->blocks.size());
   for (int bi = 0; bi < int(B->blocks.size()); ++bi) {
     bref[size_t(bi)].bi = bi;
     for (int k = 0; k < n; ++k) bref[size_t(bi)].ck[size_t(k)] = B->blocks[bi].key[ibb[k]];
   }
   std::stable_sort(bref.begin(), bref.end(), ck_less);
-  struct OutPair {
-    Key ok;
-    int ai, bi;
-  };
-  std::vector<OutPair> ops;
-  ops.reserve(A->blocks.size());
+  std::vector<OutPair>& ops = plan.ops;
+  ops.clear();
   BRef probe{};
   for (int ai = 0; ai < int(A->blocks.size()); ++ai) {
     for (int k = 0; k < n; ++k) probe.ck[size_t(k)] = A->blocks[ai].key[iaa[k]];
@@ -325,12 +335,14 @@ std::unique_ptr<bug_tensor> contract_impl(bug_ctx* c, const bug_tensor& A0, int 
     if (i == 0 || ops[i].ok != ops[i - 1].ok) keys.push_back(ops[i].ok);
   auto out = make_tensor(c, ro, legs, keys, false);
   if (keys.empty()) return out;
-  std::vector<GemmOut> outs;
-  std::vector<GemmPair> pairs;
-  std::vector<GemmTile> tiles;
-  std::vector<int> mixed;  // outputs the tensor-core path computes
-  outs.reserve(keys.size());
-  pairs.reserve(ops.size());
+  std::vector<GemmOut>& outs = plan.outs;
+  std::vector<GemmPair>& pairs = plan.pairs;
+  std::vector<GemmTile>& tiles = plan.tiles;
+  std::vector<int>& mixed = plan.mixed;  // outputs the tensor-core path computes
+  outs.clear();
+  pairs.clear();
+  tiles.clear();
+  mixed.clear();
   for (size_t r0 = 0, oj = 0; r0 < ops.size(); ++oj) {
     size_t r1 = r0 + 1;
     while (r1 < ops.size() && ops[r1].ok == ops[r0].ok) ++r1;
