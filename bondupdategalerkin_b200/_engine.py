@@ -105,7 +105,8 @@ FAMILIES = ("copy", "gemm", "svd", "dot", "lincomb", "scale", "mixed")
 # stage kind of stage_kernel, one launch per operation.
 KERNEL_NAMES = {"copy": "stage_kernel (copy stage)", "gemm": "stage_kernel (gemm stage)",
                 "svd": "jacobi_svd_kernel", "dot": "stage_kernel (dot stages)",
-                "lincomb": "stage_kernel (lincomb stage)", "scale": "stage_kernel (scale stage)"}
+                "lincomb": "stage_kernel (lincomb stage)", "scale": "stage_kernel (scale stage)",
+                "mixed": "tc_pack_kernel + tc_cgemm_kernel (3xTF32 tcgen05)"}
 
 STATUS = {0: "BUG_OK", 1: "BUG_EINVAL", 2: "BUG_ENONFINITE", 3: "BUG_ENOMEM", 4: "BUG_ETIMEOUT",
           5: "BUG_EDEVICE", 6: "BUG_ENOTCONV"}

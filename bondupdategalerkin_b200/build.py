@@ -17,7 +17,10 @@ HEADERS = ("kernels.cuh", "engine.h", "smallla.h", "tcgemm.cuh")
 OUTPUT = os.path.join(HERE, "libbug_b200.so")
 OBJDIR = os.path.join(os.path.dirname(HERE), "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC"]
+# Host code: hardware FMA for the explicit std::fma of the Krylov-weight and small dense kernels
+# (without it each is a libm call), and no contraction of other a*b+c, so every other host result
+# keeps the rounding of plain multiplies and adds.
+NVCC_FLAGS = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-mfma,-ffp-contract=off"]
 
 
 def _deps():

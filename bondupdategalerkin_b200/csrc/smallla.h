@@ -40,14 +40,27 @@ struct Mat {
 using CMat = Mat<cd>;
 using RMat = Mat<double>;
 
+// z = x y with the complex products written out on the interleaved (re, im) storage: the inner
+// loop then vectorises (std::complex's multiply carries a NaN-recovery branch per product)
 inline CMat matmul(const CMat& x, const CMat& y) {
   CMat z(x.n, y.m);
-  for (int i = 0; i < x.n; ++i)
+  const int m = y.m;
+  const double* yd = reinterpret_cast<const double*>(y.a.data());
+  double* zd = reinterpret_cast<double*>(z.a.data());
+  for (int i = 0; i < x.n; ++i) {
+    double* zr = zd + 2 * size_t(i) * m;
     for (int k = 0; k < x.m; ++k) {
       const cd v = x(i, k);
       if (v == cd(0)) continue;
-      for (int j = 0; j < y.m; ++j) z(i, j) += v * y(k, j);
+      const double vr = v.real(), vi = v.imag();
+      const double* yr = yd + 2 * size_t(k) * m;
+      for (int j = 0; j < m; ++j) {
+        const double a = yr[2 * j], b = yr[2 * j + 1];
+        zr[2 * j] += vr * a - vi * b;
+        zr[2 * j + 1] += vr * b + vi * a;
+      }
     }
+  }
   return z;
 }
 
@@ -351,7 +364,9 @@ inline std::vector<cd> eigvals_hess(const CMat& H0) {
       }
       cs[k - lo] = cc;
       sn[k - lo] = ss;
-      for (int j = k; j < n; ++j) {  // rows k, k+1: G^H
+      // only the active block's entries are updated: the eigenvalues never read the coupling to
+      // rows above `lo` or columns past `hi`, and the block's own arithmetic is unchanged
+      for (int j = k; j <= hi; ++j) {  // rows k, k+1: G^H
         const cd u = H(k, j), v = H(k + 1, j);
         H(k, j) = std::conj(cc) * u + std::conj(ss) * v;
         H(k + 1, j) = -ss * u + cc * v;
@@ -359,7 +374,7 @@ inline std::vector<cd> eigvals_hess(const CMat& H0) {
     }
     for (int k = lo; k < hi; ++k) {  // columns k, k+1: G
       const cd cc = cs[k - lo], ss = sn[k - lo];
-      for (int i = 0; i <= std::min(k + 2, hi); ++i) {
+      for (int i = lo; i <= std::min(k + 2, hi); ++i) {
         const cd u = H(i, k), v = H(i, k + 1);
         H(i, k) = u * cc + v * ss;
         H(i, k + 1) = -u * std::conj(ss) + v * std::conj(cc);

@@ -971,17 +971,25 @@ double residual_integral(int comp, const CMat& g, cd tau_eff, bool state_seed) {
   // rows e_comp^T P^r, r = 0 .. B-1
   std::vector<double> rowr(size_t(B) * n, 0.0), rowi(size_t(B) * n, 0.0);
   rowr[size_t(comp)] = 1.0;
+  // P transposed, so that (u P)_j runs along a contiguous row (same sums in the same order)
+  std::vector<double> ptr_(size_t(n) * n), pti_(size_t(n) * n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      ptr_[size_t(j) * n + i] = pr[size_t(i) * n + j];
+      pti_[size_t(j) * n + i] = pi[size_t(i) * n + j];
+    }
   for (int r = 1; r < B; ++r) {
     const double* ur = &rowr[size_t(r - 1) * n];
     const double* ui = &rowi[size_t(r - 1) * n];
     double* vr = &rowr[size_t(r) * n];
     double* vi = &rowi[size_t(r) * n];
     for (int j = 0; j < n; ++j) {
+      const double* ar = &ptr_[size_t(j) * n];
+      const double* ai = &pti_[size_t(j) * n];
       double sr = 0.0, si = 0.0;
       for (int i = 0; i < n; ++i) {  // (u P)_j = sum_i u_i P_ij
-        const double a = pr[size_t(i) * n + j], b = pi[size_t(i) * n + j];
-        sr = std::fma(ur[i], a, std::fma(-ui[i], b, sr));
-        si = std::fma(ur[i], b, std::fma(ui[i], a, si));
+        sr = std::fma(ur[i], ar[i], std::fma(-ui[i], ai[i], sr));
+        si = std::fma(ur[i], ai[i], std::fma(ui[i], ar[i], si));
       }
       vr[j] = sr;
       vi[j] = si;
