@@ -107,6 +107,7 @@ struct DrawBuf {
     pos = marks.back();
     marks.pop_back();
   }
+  void drop() { marks.pop_back(); }  // forget the last mark, keeping the position
   // The caller's generator exactly where the values handed out so far leave it, for a draw of
   // another kind from it (pause); resume() then saves the generator after that draw and buffers
   // from there.
@@ -298,6 +299,29 @@ bool svd_ahead1(const Eng& e, const T& t, std::vector<int> left, int want, SVDRe
   if (V) r.Vd = Eng::sh(std::move(V));
   if (US_) r.Us = Eng::sh(std::move(US_));
   if (SV_) r.SVd_ = Eng::sh(std::move(SV_));
+  return true;
+}
+
+// Two such SVDs taken ahead in one launch; false (nothing launched) when the region is full.
+bool svd2_ahead(const Eng& e, const T& t1, std::vector<int> left1, int want1, const T& t2,
+                std::vector<int> left2, int want2, std::pair<SVDRes, SVDRes>& out) {
+  TensorPtr U[2], V[2], US_[2], SV_[2];
+  std::vector<double> sv[2];
+  std::vector<int> q[2];
+  int nk[2] = {0, 0};
+  if (!svd_ahead(e.c, {SvdReq{t1.get(), int(left1.size()), left1.data(), 0.0, -1, want1, &U[0],
+                              &V[0], &sv[0], &q[0], &nk[0], &US_[0], &SV_[0]},
+                       SvdReq{t2.get(), int(left2.size()), left2.data(), 0.0, -1, want2, &U[1],
+                              &V[1], &sv[1], &q[1], &nk[1], &US_[1], &SV_[1]}}))
+    return false;
+  SVDRes* r[2] = {&out.first, &out.second};
+  for (int i = 0; i < 2; ++i) {
+    *r[i] = SVDRes{};
+    if (U[i]) r[i]->U = Eng::sh(std::move(U[i]));
+    if (V[i]) r[i]->Vd = Eng::sh(std::move(V[i]));
+    if (US_[i]) r[i]->Us = Eng::sh(std::move(US_[i]));
+    if (SV_[i]) r[i]->SVd_ = Eng::sh(std::move(SV_[i]));
+  }
   return true;
 }
 
@@ -1209,7 +1233,7 @@ struct Step {
   }
 
   BondFrame frame_from(const T& left, const T& right) {
-    auto both = svd2(e, left, {0, 1}, W_U | W_SVD, right, {0}, W_US | W_VD);
+    auto both = svd2x(left, {0, 1}, W_U | W_SVD, right, {0}, W_US | W_VD);
     SVDRes& rl = both.first;
     SVDRes& rr = both.second;
     T core = e.contract(SVd(e, rl), {1}, US(e, rr), {0});
@@ -1690,8 +1714,57 @@ struct Step {
   }
 
   // ── half-sweeps (half_sweeps.jl) ──
+  // A half-sweep is a function of its inputs and its draws: its frames' cutoff-0 SVDs are taken
+  // ahead (frame_from) and checked at its end; on a zero singular value the half runs again from
+  // the saved state and draw position. Only this half's outputs are restored (the other half
+  // writes its own bonds of `expanded`, possibly at the same time).
+  template <class F>
+  void half_ahead(MPS& psi, std::map<int, T>& frames, std::vector<int64_t>& expanded,
+                  int b_lo, int b_hi, std::vector<int64_t>& nn, Ledger& hl, F body) {
+    if (!e.buf) {
+      body();
+      return;
+    }
+    const MPS s_psi = psi;
+    const std::map<int, T> s_frames = frames;
+    const std::vector<int64_t> s_exp(expanded.begin() + (b_lo - 1),
+                                     expanded.begin() + std::max(b_lo - 1, b_hi));
+    const std::vector<int64_t> s_nn = nn;
+    const Ledger s_hl = hl;
+    const int64_t s_nmv = nmv;
+    e.buf->save();
+    frames_ahead = true;
+    body();
+    frames_ahead = false;
+    if (svd_ahead_check(e.c)) {
+      e.buf->drop();
+      return;
+    }
+    e.buf->restore();
+    psi = s_psi;
+    frames = s_frames;
+    std::copy(s_exp.begin(), s_exp.end(), expanded.begin() + (b_lo - 1));
+    nn = s_nn;
+    hl = s_hl;
+    nmv = s_nmv;
+    body();
+  }
   T half_left(MPS& psiL, std::map<int, T>& lf, std::vector<int64_t>& expanded,
               std::vector<int64_t>& nn, Ledger& hl) {
+    T out;
+    half_ahead(psiL, lf, expanded, 1, root_link, nn, hl,
+               [&] { out = half_left_body(psiL, lf, expanded, nn, hl); });
+    return out;
+  }
+  std::pair<T, T> half_right(MPS& psiR, std::map<int, T>& rf, std::vector<int64_t>& expanded,
+                             std::vector<int64_t>& nn, Ledger& hl) {
+    std::pair<T, T> out;
+    half_ahead(psiR, rf, expanded, root_link + 1, L - 1, nn, hl,  // bond root_link is the left's
+               [&] { out = half_right_body(psiR, rf, expanded, nn, hl); });
+    return out;
+  }
+  T half_left_body(MPS& psiL, std::map<int, T>& lf, std::vector<int64_t>& expanded,
+                   std::vector<int64_t>& nn, Ledger& hl) {
     canonical(psiL, 1);
     auto rstack = right_env_stack(psiL, 3);
     T lch = env.left_boundary();
@@ -1722,8 +1795,8 @@ struct Step {
     return lroot;
   }
 
-  std::pair<T, T> half_right(MPS& psiR, std::map<int, T>& rf, std::vector<int64_t>& expanded,
-                             std::vector<int64_t>& nn, Ledger& hl) {
+  std::pair<T, T> half_right_body(MPS& psiR, std::map<int, T>& rf, std::vector<int64_t>& expanded,
+                                  std::vector<int64_t>& nn, Ledger& hl) {
     canonical(psiR, L);
     auto lstack = left_env_stack(psiR, L - 2);
     T rch = env.right_boundary(total_charge(psiR));
@@ -1895,9 +1968,48 @@ struct Step {
     int64_t added = 0, n_h1 = 0;
   };
 
+  // A frontier half is a function of its inputs and its draws, so its cutoff-0 SVDs (the frames
+  // and polar factors) are taken ahead of their read-back (svd_ahead) and checked once at its end;
+  // if a singular value was exactly zero, the half is run again from the same draw position with
+  // read-backs. Without a buffered draw stream (nothing to rewind) it runs with read-backs.
+  bool frames_ahead = false;
+  SVDRes svdx(const T& t, std::vector<int> left, int want) {
+    SVDRes r;
+    if (!frames_ahead || !svd_ahead1(e, t, left, want, r)) r = svd(e, t, left, 0.0, -1, want);
+    return r;
+  }
+  std::pair<SVDRes, SVDRes> svd2x(const T& t1, std::vector<int> l1, int w1, const T& t2,
+                                  std::vector<int> l2, int w2) {
+    if (!frames_ahead) return svd2(e, t1, l1, w1, t2, l2, w2);
+    std::pair<SVDRes, SVDRes> r;
+    if (svd2_ahead(e, t1, l1, w1, t2, l2, w2, r)) return r;
+    return svd2(e, t1, l1, w1, t2, l2, w2);
+  }
+  template <class F> auto with_frames_ahead(F body) -> decltype(body()) {
+    if (e.buf) {
+      e.buf->save();
+      frames_ahead = true;
+      auto out = body();
+      frames_ahead = false;
+      if (svd_ahead_check(e.c)) {
+        e.buf->drop();
+        return out;
+      }
+      e.buf->restore();
+    }
+    return body();
+  }
+  FrontierHalf frontier_left(const MPS& Fm, KL& fr, double amp, bool enrich = true) {
+    return with_frames_ahead([&] { return frontier_left_body(Fm, fr, amp, enrich); });
+  }
+  FrontierHalf frontier_right(const MPS& Fm, KL& fr, double amp, bool enrich = true) {
+    return with_frames_ahead([&] { return frontier_right_body(Fm, fr, amp, enrich); });
+  }
+
   // enrich = false measures only (estimate_global_complement_action): the frames stay, the
   // environments are the frames' own
-  FrontierHalf frontier_left(MPS Fm, KL& fr, double amp, bool enrich = true) {
+  FrontierHalf frontier_left_body(const MPS& Fm0, KL& fr, double amp, bool enrich) {
+    MPS Fm = Fm0;
     FrontierHalf out;
     canonical(Fm, 1);
     auto rstack = right_env_stack(Fm, 3);
@@ -1921,11 +2033,11 @@ struct Step {
       SVDRes pol;
       BondFrame tsf;
       if (enrich) {
-        auto both = svd2(e, Fm[bond + 1], {0}, W_US | W_VD, old, {0, 1}, W_U | W_VD);
+        auto both = svd2x(Fm[bond + 1], {0}, W_US | W_VD, old, {0, 1}, W_U | W_VD);
         tsf = frame_onto_left(old, site_core, both.first);
         pol = std::move(both.second);
       } else {
-        tsf = frame_onto_left(old, site_core, Fm[bond + 1]);
+        tsf = frame_onto_left(old, site_core, svdx(Fm[bond + 1], {0}, W_US | W_VD));
       }
       const T& rch = rstack[bond + 2];
       const double lk = bond_action(tsf, bond, lch, rch, true);
@@ -1947,7 +2059,7 @@ struct Step {
       } else {
         Wi = old;
       }
-      T Wn = !enrich ? old : (quiet ? polar_of(pol, true) : polar_frame(Wi, true));
+      T Wn = !enrich ? old : (quiet ? polar_of(pol, true) : polar_of(svdx(Wi, {0, 1}, W_U | W_VD), true));
       out.frames[bond] = Wn;
       out.added += dim(Wn, 2) - dim(old, 2);
       log_bond(out.ledger, bl, bond, 0, int(dim(Wn, 2)));
@@ -1960,7 +2072,8 @@ struct Step {
     return out;
   }
 
-  FrontierHalf frontier_right(MPS Fm, KL& fr, double amp, bool enrich = true) {
+  FrontierHalf frontier_right_body(const MPS& Fm0, KL& fr, double amp, bool enrich) {
+    MPS Fm = Fm0;
     FrontierHalf out;
     canonical(Fm, L);
     auto lstack = left_env_stack(Fm, L - 2);
@@ -1983,11 +2096,11 @@ struct Step {
       SVDRes pol;
       BondFrame tsf;
       if (enrich) {
-        auto both = svd2(e, Fm[bond], {0, 1}, W_U | W_SVD, old, {0}, W_U | W_VD);
+        auto both = svd2x(Fm[bond], {0, 1}, W_U | W_SVD, old, {0}, W_U | W_VD);
         tsf = frame_onto_right(both.first, site_core, old);
         pol = std::move(both.second);
       } else {
-        tsf = frame_onto_right(Fm[bond], site_core, old);
+        tsf = frame_onto_right(svdx(Fm[bond], {0, 1}, W_U | W_SVD), site_core, old);
       }
       const T& lch = lstack[bond];
       const double lk = bond_action(tsf, bond, lch, rch, false);
@@ -2009,7 +2122,7 @@ struct Step {
       } else {
         Zj = old;
       }
-      T Zn = !enrich ? old : (quiet ? polar_of(pol, false) : polar_frame(Zj, false));
+      T Zn = !enrich ? old : (quiet ? polar_of(pol, false) : polar_of(svdx(Zj, {0}, W_U | W_VD), false));
       out.frames[bond] = Zn;
       out.added += dim(Zn, 0) - dim(old, 0);
       log_bond(out.ledger, bl, bond, 1, int(dim(Zn, 0)));

@@ -355,3 +355,46 @@ def test_exact_zero_singular_values_redo_the_moves(dev, parallel):
         assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
         assert di["status"] == oi["status"] and di["expanded"] == oi["expanded"], n
         assert 1.0 - fidelity(mps_to_host(dstate), ostate) <= 1e-12, n
+
+
+_REDO_SCRIPT = r"""
+import sys, numpy as np
+from bondupdategalerkin_b200 import models as DM, native as DN
+from tests.gpu_util import mps_to_host
+L, parallel, out = 16, sys.argv[1] == "1", sys.argv[2]
+psi, mpo = DM.domain_wall_state(L), DM.xxz_mpo(L, J=1.0, delta=0.5)
+rng = np.random.default_rng(3)
+dims = []
+for _ in range(4):
+    info = DN.cbe_bug_step(psi, mpo, -0.05j, order=2, tol_basis=1e-4, maxdim=32, rng=rng,
+                           parallel=parallel)
+    dims.append(info["bond_dims"] + list(info["expanded"]))
+h = mps_to_host(psi)
+arrs = {f"{s}:{k}": v for s in range(1, L + 1) for k, v in h[s].blocks.items()}
+np.savez(out, dims=np.array(dims), **{f"b{i}": arrs[k] for i, k in enumerate(sorted(arrs))},
+         keys=np.array(sorted(arrs)))
+"""
+
+
+@pytest.mark.parametrize("parallel", [False, True])
+def test_svd_ahead_redo_gives_the_same_steps(dev, tmp_path, parallel):
+    """With BUG_SVD_AHEAD_REDO=1 every computation that took SVDs ahead (canonical moves, the
+    projection miss, the frontier halves) is run a second time the exact way, rewinding the draws
+    of a frontier half; the steps must come out bit for bit as without it."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = []
+    for redo in ("0", "1"):
+        out = str(tmp_path / f"run{redo}.npz")
+        env = dict(os.environ, BUG_SVD_AHEAD_REDO=redo, PYTHONPATH=root)
+        subprocess.run([sys.executable, "-c", _REDO_SCRIPT, "1" if parallel else "0", out],
+                       check=True, cwd=root, env=env, timeout=600)
+        res.append(np.load(out))
+    a, b = res
+    assert np.array_equal(a["dims"], b["dims"])
+    assert list(a["keys"]) == list(b["keys"])
+    for i in range(len(a["keys"])):
+        assert np.array_equal(a[f"b{i}"], b[f"b{i}"]), a["keys"][i]
