@@ -447,10 +447,12 @@ def run_engine(args):
     assert psi_r.bond_dims() == final_dims, "profiled replay diverged from the timed steps"
 
     # ── end to end through host buffers: upload state+MPO, step, download the new state ──
-    from bondupdategalerkin_b200.api import ite_step_host, step_host, tdvp2_step_host
+    from bondupdategalerkin_b200.api import ite_step_host, step_host_flat, tdvp2_step_host
 
     host_state = [DT.to_blocks(t) for t in start_psi.tensors]
     host_mpo = [DT.to_blocks(t) for t in mpo.tensors]
+    if KIND[0] in ("xxz", "heston"):  # the flat host layout: one engine call each way
+        host_state, host_mpo = DT.host_from_blocks(host_state), DT.host_from_blocks(host_mpo)
     rng_e = np.random.default_rng()
     rng_e.bit_generator.state = start_rng
     center = start_psi.center
@@ -466,8 +468,8 @@ def run_engine(args):
             host_state, center, io = ite_step_host(host_state, center, host_mpo, ITE["dbeta"],
                                                    rng=rng_e, **ITE["kw"])
         else:
-            host_state, center, io = step_host(host_state, center, host_mpo, tau(), rng=rng_e,
-                                               **step_kwargs())
+            host_state, center, io = step_host_flat(host_state, center, host_mpo, tau(), rng=rng_e,
+                                                    **step_kwargs())
         e1.record(stream)
         ctx.synchronize()
         e2e_ms += e0.elapsed_time(e1)

@@ -45,6 +45,14 @@ SIGNATURES = {
     "bug_tensor_free": (ctypes.c_int, [_vp, _vp]),
     "bug_tensor_shape": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_int64), _c_int_p]),
     "bug_tensor_meta": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    "bug_tensors_from_host": (ctypes.c_int, [_vp, ctypes.c_int, _c_int_p, ctypes.POINTER(ctypes.c_int64),
+                                             _c_double_p, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(_vp)]),
+    "bug_tensors_layout": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_vp),
+                                          ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    "bug_tensors_to_host": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), _c_int_p,
+                                           ctypes.POINTER(ctypes.c_int64), _c_double_p,
+                                           ctypes.POINTER(ctypes.c_int64)]),
     "bug_contract": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, _vp, _c_int_p, ctypes.c_int,
                                     ctypes.c_int, ctypes.POINTER(_vp)]),
     "bug_svd": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.c_double, ctypes.c_int,

@@ -29,7 +29,7 @@ from .qtt import (HestonParams, heston_mpo, heston_op, qtt_bug_step, qtt_derivat
                   qtt_separable, qtt_shift, qtt_step_tolerance, qtt_to_mpo)
 from .tensor import from_blocks, to_blocks
 
-__all__ = ["cbe_bug_step", "Batch", "step_host", "magnetisation", "DDQRExpansion", "MPS", "MPO",
+__all__ = ["cbe_bug_step", "Batch", "step_host", "step_host_flat", "magnetisation", "DDQRExpansion", "MPS", "MPO",
            "domain_wall_state", "neel_state", "product_state", "xxz_mpo", "tdvp2_step",
            "tdvp2_step_host", "ite_step", "ite_step_host", "ite_evolve", "ite_energy", "log_panel_steps",
            "uniform_beta_steps", "beta_grid", "uniform_schedule", "geometric_schedule",
@@ -63,6 +63,22 @@ def step_host(host_state, center, host_mpo, tau, **kwargs):
     out = [to_blocks(t) for t in psi.tensors]
     d2h = sum(16 * t.nelem for t in psi.tensors)
     return out, psi.center, dict(h2d_bytes=h2d, d2h_bytes=d2h, info=info)
+
+
+def step_host_flat(state, center, mpo, tau, **kwargs):
+    """One BUG step on host-resident data in the engine's flat layout (``tensor.HostTensors``):
+    the state and the MPO go up in one engine call each, the step runs on the device, and the new
+    state comes back in one call with one synchronisation. Returns ``(new_state, new_center,
+    io)`` with ``io`` holding the bytes moved each way and the step info."""
+    from .tensor import from_host_many, to_host_many
+
+    sites = from_host_many(state)
+    ws = from_host_many(mpo)
+    psi = MPS(sites, center)
+    info = cbe_bug_step(psi, MPO(ws), tau, **kwargs)
+    out = to_host_many(psi.tensors)
+    return out, psi.center, dict(h2d_bytes=state.nbytes + mpo.nbytes, d2h_bytes=out.nbytes,
+                                 info=info)
 
 
 def tdvp2_step_host(host_state, center, host_mpo, tau, **kwargs):

@@ -1789,6 +1789,111 @@ int bug_tensor_meta(const bug_tensor* t, int* dirs, int* nsec, int* charges, int
   });
 }
 
+// The flat host layout of many tensors (include/bug_b200.h): per tensor, at meta + meta_off[i],
+// rank r, r arrows, r sector counts, the charges and the dims of all sectors leg by leg, the block
+// count nb and nb x r block keys; its payload at payload_off[i] complex values into `payload`.
+int bug_tensors_from_host(bug_ctx* c, int n, const int* meta, const int64_t* meta_off,
+                          const double* payload, const int64_t* payload_off, bug_tensor** out) {
+  return guard([&] {
+    require(c && n >= 0, "bad argument");
+    require(n == 0 || (meta && meta_off && payload && payload_off && out), "null argument");
+    std::vector<TensorPtr> made;
+    for (int i = 0; i < n; ++i) {
+      const int* m = meta + meta_off[i];
+      const int rank = m[0];
+      require(rank >= 0 && rank <= BUG_MAX_RANK, "rank out of range");
+      const int* dirs = m + 1;
+      const int* nsec = m + 1 + rank;
+      int ns = 0;
+      for (int l = 0; l < rank; ++l) {
+        require(nsec[l] >= 0, "negative sector count");
+        ns += nsec[l];
+      }
+      const int* ch = m + 1 + 2 * rank;
+      const int* dm = ch + ns;
+      std::vector<Leg> legs(rank);
+      for (int l = 0, p = 0; l < rank; ++l) {
+        require(dirs[l] == 1 || dirs[l] == -1, "leg arrow must be +1 or -1");
+        legs[l].dir = dirs[l];
+        for (int q = 0; q < nsec[l]; ++q, ++p) {
+          require(dm[p] > 0, "sector dimension must be positive");
+          require(legs[l].q.empty() || ch[p] > legs[l].q.back(), "sector charges must ascend");
+          legs[l].q.push_back(ch[p]);
+          legs[l].d.push_back(dm[p]);
+        }
+      }
+      const int nb = dm[ns];
+      require(nb >= 0, "negative block count");
+      const int* keys = dm + ns + 1;
+      std::vector<Key> ks(nb);
+      for (int b = 0; b < nb; ++b) {
+        Key k{};
+        for (int l = 0; l < rank; ++l) k[l] = keys[b * rank + l];
+        ks[b] = k;
+      }
+      made.push_back(upload_impl(c, rank, legs, ks, payload + 2 * payload_off[i]));
+    }
+    for (int i = 0; i < n; ++i) out[i] = made[size_t(i)].release();
+  });
+}
+
+int bug_tensors_layout(int n, const bug_tensor* const* t, int64_t* meta_len, int64_t* nelem) {
+  return guard([&] {
+    require(n >= 0 && (n == 0 || (t && meta_len && nelem)), "bad argument");
+    for (int i = 0; i < n; ++i) {
+      require(t[i] != nullptr, "null tensor");
+      int64_t ns = 0;
+      for (auto& l : t[i]->legs) ns += int64_t(l.q.size());
+      meta_len[i] = 2 + 2 * int64_t(t[i]->rank) + 2 * ns + int64_t(t[i]->blocks.size()) * t[i]->rank;
+      nelem[i] = t[i]->nelem;
+    }
+  });
+}
+
+int bug_tensors_to_host(bug_ctx* c, int n, const bug_tensor* const* t, int* meta,
+                        const int64_t* meta_off, double* payload, const int64_t* payload_off) {
+  return guard([&] {
+    require(c && n >= 0, "bad argument");
+    require(n == 0 || (t && meta && meta_off && payload && payload_off), "null argument");
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) {
+      require(t[i] != nullptr, "null tensor");
+      total += t[i]->nelem;
+    }
+    double* pin = c->readback(size_t(2 * std::max<int64_t>(total, 1)));
+    c->drain();
+    int64_t acc = 0;
+    for (int i = 0; i < n; ++i) {
+      if (t[i]->nelem > 0)
+        BUG_CUDA(cudaMemcpyAsync(pin + 2 * acc, t[i]->buf->ptr, size_t(t[i]->nelem) * sizeof(double2),
+                                 cudaMemcpyDeviceToHost, c->stream));
+      acc += t[i]->nelem;
+    }
+    for (int i = 0; i < n; ++i) {  // metadata from the host-side block tables meanwhile
+      const bug_tensor& x = *t[i];
+      int* m = meta + meta_off[i];
+      int p = 0;
+      m[p++] = x.rank;
+      for (int l = 0; l < x.rank; ++l) m[p++] = x.legs[l].dir;
+      for (int l = 0; l < x.rank; ++l) m[p++] = int(x.legs[l].q.size());
+      for (int l = 0; l < x.rank; ++l)
+        for (int q : x.legs[l].q) m[p++] = q;
+      for (int l = 0; l < x.rank; ++l)
+        for (int d : x.legs[l].d) m[p++] = d;
+      m[p++] = int(x.blocks.size());
+      for (auto& b : x.blocks)
+        for (int l = 0; l < x.rank; ++l) m[p++] = b.key[l];
+    }
+    c->wait();
+    acc = 0;
+    for (int i = 0; i < n; ++i) {
+      if (t[i]->nelem > 0)
+        std::memcpy(payload + 2 * payload_off[i], pin + 2 * acc, size_t(t[i]->nelem) * sizeof(double2));
+      acc += t[i]->nelem;
+    }
+  });
+}
+
 int bug_contract(bug_ctx* c, const bug_tensor* a, int n, const int* ia, const bug_tensor* b,
                  const int* ib, int conja, int conjb, bug_tensor** out) {
   return guard([&] {

@@ -145,23 +145,34 @@ def from_blocks(legs, blocks: dict, ctx: E.Context | None = None) -> DT:
     """Create an engine tensor from host blocks (``key -> ndarray``) and upload the payload."""
     ctx = ctx or E.context()
     rank = len(legs)
-    dirs = [l.dir for l in legs]
-    nsec = [len(l.sectors) for l in legs]
-    charges = [q for l in legs for q in l.sectors]
-    dims = [d for l in legs for d in l.sectors.values()]
     keys = sorted(blocks)
-    flat = [q for k in keys for q in k]
-    a_d, p_d = _ints(dirs or [0])
-    a_n, p_n = _ints(nsec or [0])
-    a_c, p_c = _ints(charges or [0])
-    a_m, p_m = _ints(dims or [0])
-    a_k, p_k = _ints(flat or [0])
+    # one int32 array carries the arrows, sector counts, charges, dims and keys (views into it)
+    nsec = [len(l.sectors) for l in legs]
+    ns = sum(nsec)
+    meta = np.empty(2 * rank + 2 * ns + rank * len(keys) + 1, dtype=np.int32)
+    meta[:rank] = [l.dir for l in legs]
+    meta[rank:2 * rank] = nsec
+    p = 2 * rank
+    for l in legs:
+        k = len(l.sectors)
+        meta[p:p + k] = list(l.sectors)
+        meta[p + ns:p + ns + k] = list(l.sectors.values())
+        p += k
+    p = 2 * rank + 2 * ns
+    if keys:
+        meta[p:p + rank * len(keys)] = np.array(keys, dtype=np.int32).reshape(-1)
+    base = meta.ctypes.data
+    i4 = 4
+
+    def at(off):
+        return ctypes.cast(base + i4 * off, _ip)
+
     h = _vp()
-    E.check(ctx.lib.bug_tensor_create(ctx.h, rank, p_d, p_n, p_c, p_m, len(keys), p_k, ctypes.byref(h)))
+    E.check(ctx.lib.bug_tensor_create(ctx.h, rank, at(0), at(rank), at(2 * rank), at(2 * rank + ns),
+                                      len(keys), at(p), ctypes.byref(h)))
     t = DT(ctx, h)
     if keys:
-        data = np.concatenate([np.ascontiguousarray(blocks[k], dtype=np.complex128).reshape(-1) for k in keys])
-        data = np.ascontiguousarray(data)
+        data = np.concatenate([blocks[k].reshape(-1) for k in keys]).astype(np.complex128, copy=False)
         E.check(ctx.lib.bug_tensor_upload(ctx.h, h, data.ctypes.data_as(_dp), data.size))
     return t
 
@@ -415,3 +426,108 @@ def gaussian_fused(rng, la: Leg, lb: Leg, cols: dict, new_first: bool, ctx=None)
             else:
                 blocks[(qa, qb, c)] = np.ascontiguousarray(blk)
     return from_blocks(legs, blocks, ctx)
+
+
+# ── many tensors through one flat host layout (bug_tensors_from_host / bug_tensors_to_host) ──
+
+
+@dataclass
+class HostTensors:
+    """Tensors in host memory in the engine's flat layout: ``meta`` (int32) holds, per tensor at
+    ``meta_off[i]``, its rank, arrows, sector counts, sector charges and dims, block count and
+    block keys; ``payload`` (complex128) holds its blocks in key order from ``payload_off[i]``."""
+
+    meta: np.ndarray
+    meta_off: np.ndarray
+    payload: np.ndarray
+    payload_off: np.ndarray
+
+    def __len__(self):
+        return len(self.meta_off)
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.payload.nbytes)
+
+
+def _i64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+
+
+def to_host_many(ts, ctx: E.Context | None = None) -> HostTensors:
+    """Download tensors into the flat host layout: two engine calls, one synchronisation."""
+    ctx = ctx or ts[0].ctx
+    n = len(ts)
+    arr = (_vp * max(n, 1))(*[t.h.value for t in ts])
+    mlen = np.zeros(max(n, 1), np.int64)
+    nel = np.zeros(max(n, 1), np.int64)
+    E.check(ctx.lib.bug_tensors_layout(n, arr, _i64p(mlen), _i64p(nel)))
+    moff = np.zeros(max(n, 1), np.int64)
+    poff = np.zeros(max(n, 1), np.int64)
+    if n > 1:
+        moff[1:n] = np.cumsum(mlen[:n - 1])
+        poff[1:n] = np.cumsum(nel[:n - 1])
+    meta = np.zeros(max(int(mlen[:n].sum()), 1), np.int32)
+    payload = np.zeros(max(int(nel[:n].sum()), 1), np.complex128)
+    E.check(ctx.lib.bug_tensors_to_host(ctx.h, n, arr, meta.ctypes.data_as(_ip), _i64p(moff),
+                                        payload.ctypes.data_as(_dp), _i64p(poff)))
+    return HostTensors(meta, moff[:n], payload, poff[:n])
+
+
+def from_host_many(ht: HostTensors, ctx: E.Context | None = None) -> list:
+    """Create and upload tensors from the flat host layout: one engine call, no wait."""
+    ctx = ctx or E.context()
+    n = len(ht)
+    out = (_vp * max(n, 1))()
+    moff = np.ascontiguousarray(ht.meta_off, dtype=np.int64)
+    poff = np.ascontiguousarray(ht.payload_off, dtype=np.int64)
+    E.check(ctx.lib.bug_tensors_from_host(ctx.h, n, ht.meta.ctypes.data_as(_ip), _i64p(moff),
+                                          ht.payload.ctypes.data_as(_dp), _i64p(poff), out))
+    return [DT(ctx, _vp(out[i])) for i in range(n)]
+
+
+def host_from_blocks(tensors) -> HostTensors:
+    """The flat host layout of ``(legs, {key: ndarray})`` tensors (as ``to_blocks`` returns)."""
+    metas, pays = [], []
+    for legs, blocks in tensors:
+        keys = sorted(blocks)
+        m = [len(legs)] + [l.dir for l in legs] + [len(l.sectors) for l in legs]
+        m += [q for l in legs for q in l.sectors] + [d for l in legs for d in l.sectors.values()]
+        m += [len(keys)] + [q for k in keys for q in k]
+        metas.append(np.array(m, np.int32))
+        pays.append(np.concatenate([np.asarray(blocks[k], np.complex128).reshape(-1) for k in keys])
+                    if keys else np.zeros(0, np.complex128))
+    moff = np.concatenate([[0], np.cumsum([len(m) for m in metas])[:-1]]).astype(np.int64)
+    poff = np.concatenate([[0], np.cumsum([len(p) for p in pays])[:-1]]).astype(np.int64)
+    meta = np.concatenate(metas) if metas else np.zeros(1, np.int32)
+    payload = np.concatenate(pays) if pays else np.zeros(1, np.complex128)
+    if payload.size == 0:
+        payload = np.zeros(1, np.complex128)
+    return HostTensors(meta, moff, payload, poff)
+
+
+def host_to_blocks(ht: HostTensors) -> list:
+    """``(legs, {key: ndarray})`` per tensor of a flat host layout."""
+    out = []
+    for i in range(len(ht)):
+        m = ht.meta[int(ht.meta_off[i]):]
+        r = int(m[0])
+        dirs, nsec = m[1:1 + r], m[1 + r:1 + 2 * r]
+        ns = int(nsec.sum())
+        ch, dm = m[1 + 2 * r:1 + 2 * r + ns], m[1 + 2 * r + ns:1 + 2 * r + 2 * ns]
+        nb = int(m[1 + 2 * r + 2 * ns])
+        keys = m[2 + 2 * r + 2 * ns:2 + 2 * r + 2 * ns + nb * r].reshape(nb, r) if r else []
+        legs, p = [], 0
+        for l in range(r):
+            k = int(nsec[l])
+            legs.append(Leg(int(dirs[l]), {int(ch[p + j]): int(dm[p + j]) for j in range(k)}))
+            p += k
+        blocks, off = {}, int(ht.payload_off[i])
+        for row in keys:
+            key = tuple(int(x) for x in row)
+            shape = tuple(legs[j].sectors[q] for j, q in enumerate(key))
+            size = int(np.prod(shape))
+            blocks[key] = ht.payload[off:off + size].reshape(shape).copy()
+            off += size
+        out.append((legs, blocks))
+    return out

@@ -110,6 +110,20 @@ int bug_tensor_free(bug_ctx* ctx, bug_tensor* t);
 int bug_tensor_shape(const bug_tensor* t, int* rank, int* nblocks, int64_t* nelem, int* total_sectors);
 /* dirs[rank], nsec[rank], charges[total_sectors], dims[total_sectors], keys[nblocks*rank]. */
 int bug_tensor_meta(const bug_tensor* t, int* dirs, int* nsec, int* charges, int* dims, int* keys);
+/* Many tensors through one flat host layout (no reference counterpart: the reference's tensors
+ * live in host memory; a host that keeps an MPS and MPO there moves them with one call each way).
+ * Tensor i's metadata sits at meta + meta_off[i]: rank r, r arrows, r sector counts, every
+ * sector's charge (leg by leg, ascending within a leg), every sector's dimension (same order),
+ * the block count nb and nb x r block keys (ascending); its payload, complex interleaved, blocks in
+ * key order and each C-ordered, at payload_off[i] complex values into `payload`.
+ * bug_tensors_from_host creates and uploads n tensors (through pinned staging, no wait);
+ * bug_tensors_layout gives each tensor's metadata length (ints) and payload size (complex values);
+ * bug_tensors_to_host writes n tensors' metadata and payloads with ONE synchronisation. */
+int bug_tensors_from_host(bug_ctx* ctx, int n, const int* meta, const int64_t* meta_off,
+                          const double* payload, const int64_t* payload_off, bug_tensor** out);
+int bug_tensors_layout(int n, const bug_tensor* const* t, int64_t* meta_len, int64_t* nelem);
+int bug_tensors_to_host(bug_ctx* ctx, int n, const bug_tensor* const* t, int* meta,
+                        const int64_t* meta_off, double* payload, const int64_t* payload_off);
 
 /* ── algebra ──────────────────────────────────────────────────────────────────────────────── */
 /* Telum `contract(A, ia, B, ib)` (deps/Telum/src/contract.jl:2686-2691): paired legs must have
