@@ -249,15 +249,26 @@ inline CMat solve(CMat P, CMat Q) {
     for (int i = k + 1; i < n; ++i) {
       const cd f = P(i, k) / P(k, k);
       if (f == cd(0)) continue;
-      for (int j = k; j < n; ++j) P(i, j) -= f * P(k, j);
-      for (int j = 0; j < Q.m; ++j) Q(i, j) -= f * Q(k, j);
+      // x -= f y with the product written out as std::complex forms it for finite values
+      const double fr = f.real(), fi = f.imag();
+      auto axpy = [fr, fi](cd& x, const cd& y) {
+        const double yr = y.real(), yi = y.imag();
+        x = cd(x.real() - (fr * yr - fi * yi), x.imag() - (fr * yi + fi * yr));
+      };
+      for (int j = k; j < n; ++j) axpy(P(i, j), P(k, j));
+      for (int j = 0; j < Q.m; ++j) axpy(Q(i, j), Q(k, j));
     }
   }
   for (int k = n - 1; k >= 0; --k) {
     for (int j = 0; j < Q.m; ++j) {
-      cd s = Q(k, j);
-      for (int i = k + 1; i < n; ++i) s -= P(k, i) * Q(i, j);
-      Q(k, j) = s / P(k, k);
+      double sr = Q(k, j).real(), si = Q(k, j).imag();
+      for (int i = k + 1; i < n; ++i) {
+        const double ar = P(k, i).real(), ai = P(k, i).imag();
+        const double br = Q(i, j).real(), bi = Q(i, j).imag();
+        sr = sr - (ar * br - ai * bi);
+        si = si - (ar * bi + ai * br);
+      }
+      Q(k, j) = cd(sr, si) / P(k, k);
     }
   }
   return Q;
@@ -366,18 +377,32 @@ inline std::vector<cd> eigvals_hess(const CMat& H0) {
       sn[k - lo] = ss;
       // only the active block's entries are updated: the eigenvalues never read the coupling to
       // rows above `lo` or columns past `hi`, and the block's own arithmetic is unchanged
+      // the complex products written out as (ac - bd, ad + bc), the operations and order of
+      // std::complex's multiply for finite values, without its per-product NaN branch
+      const double cr = cc.real(), ci = cc.imag(), sr = ss.real(), si = ss.imag();
+      const double nci = -ci, nsi = -si, nsr = -sr;
       for (int j = k; j <= hi; ++j) {  // rows k, k+1: G^H
-        const cd u = H(k, j), v = H(k + 1, j);
-        H(k, j) = std::conj(cc) * u + std::conj(ss) * v;
-        H(k + 1, j) = -ss * u + cc * v;
+        const double ur = H(k, j).real(), ui = H(k, j).imag();
+        const double vr = H(k + 1, j).real(), vi = H(k + 1, j).imag();
+        // conj(cc) u + conj(ss) v ; -ss u + cc v
+        H(k, j) = cd((cr * ur - nci * ui) + (sr * vr - nsi * vi),
+                     (cr * ui + nci * ur) + (sr * vi + nsi * vr));
+        H(k + 1, j) = cd((nsr * ur - nsi * ui) + (cr * vr - ci * vi),
+                         (nsr * ui + nsi * ur) + (cr * vi + ci * vr));
       }
     }
     for (int k = lo; k < hi; ++k) {  // columns k, k+1: G
-      const cd cc = cs[k - lo], ss = sn[k - lo];
+      const double cr = cs[k - lo].real(), ci = cs[k - lo].imag();
+      const double sr = sn[k - lo].real(), si = sn[k - lo].imag();
+      const double nci = -ci, nsi = -si;
       for (int i = lo; i <= std::min(k + 2, hi); ++i) {
-        const cd u = H(i, k), v = H(i, k + 1);
-        H(i, k) = u * cc + v * ss;
-        H(i, k + 1) = -u * std::conj(ss) + v * std::conj(cc);
+        const double ur = H(i, k).real(), ui = H(i, k).imag();
+        const double vr = H(i, k + 1).real(), vi = H(i, k + 1).imag();
+        const double nur = -ur, nui = -ui;
+        // u cc + v ss ; (-u) conj(ss) + v conj(cc)
+        H(i, k) = cd((ur * cr - ui * ci) + (vr * sr - vi * si), (ur * ci + ui * cr) + (vr * si + vi * sr));
+        H(i, k + 1) = cd((nur * sr - nui * nsi) + (vr * cr - vi * nci),
+                         (nur * nsi + nui * sr) + (vr * nci + vi * cr));
       }
     }
     for (int k = lo; k <= hi; ++k) H(k, k) += mu;
