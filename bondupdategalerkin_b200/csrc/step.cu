@@ -719,6 +719,59 @@ T gaussian_fused(const Eng& e, const Leg& la, const Leg& lb, const std::map<int,
   return e.upload(3, legs, blocks);
 }
 
+// the complete fused basis of la (x) lb (fusion_basis, dd_cbe.jl:140-148): the n_c x n_c identity
+// in every fused sector, rows and columns in gaussian_fused's (qa, qb)-pair order and layouts
+T identity_fused(const Eng& e, const Leg& la, const Leg& lb, bool new_first) {
+  const int gdir = new_first ? -1 : +1;
+  Fused f = fused_of(la, lb, gdir);
+  Leg g;
+  g.dir = gdir;
+  for (auto& kv : f.pairs) {
+    int64_t n = 0;
+    for (auto& pr : kv.second) n += int64_t(la.dim_of(pr.first)) * lb.dim_of(pr.second);
+    if (n > 0) {
+      g.q.push_back(kv.first);
+      g.d.push_back(int(n));
+    }
+  }
+  if (g.q.empty()) return nullptr;
+  std::vector<Leg> legs = new_first ? std::vector<Leg>{g, la, lb} : std::vector<Leg>{la, lb, g};
+  std::map<Key, std::vector<cd>> blocks;
+  for (auto& kv : f.pairs) {
+    const int c = kv.first;
+    const int64_t n = g.dim_of(c);
+    if (n == 0) continue;
+    int64_t off = 0;
+    for (auto& pr : kv.second) {
+      const int da = la.dim_of(pr.first), db = lb.dim_of(pr.second);
+      const int64_t r = int64_t(da) * db;
+      if (r == 0) continue;
+      std::vector<cd> blk(size_t(r * n), cd(0));
+      // row off + i of the identity has its one in column off + i
+      for (int64_t i = 0; i < r; ++i)
+        blk[size_t(new_first ? (off + i) * r + i : i * n + off + i)] = cd(1);
+      blocks[new_first ? Key{c, pr.first, pr.second, 0, 0, 0} : Key{pr.first, pr.second, c, 0, 0, 0}] =
+          std::move(blk);
+      off += r;
+    }
+  }
+  return e.upload(3, legs, blocks);
+}
+
+// _dd_probe(...; exact = true) (dd_cbe.jl:140-161): the complete fused basis with the opposite
+// frame projected out, or null when there is no discarded space or nothing survives. No draws.
+T dd_probe_exact(const Eng& e, const T& opp, bool oleft) {
+  Fused f = fused_dims(opp, oleft);
+  int64_t tot = 0;
+  for (auto& kv : f.dfull) tot += std::max<int64_t>(kv.second - f.dT[kv.first], 0);
+  if (tot == 0) return nullptr;
+  T om = oleft ? identity_fused(e, opp->legs[0], opp->legs[1], false)
+               : identity_fused(e, opp->legs[1], opp->legs[2], true);
+  if (!om) return nullptr;
+  T pr = oleft ? perp_left(e, opp, om) : perp_right(e, opp, om);
+  return e.norm(pr) > 0 ? pr : nullptr;
+}
+
 // _boost! (cbe.jl:206-216): raise the targeted sectors' columns, capped by the room `cap`
 void boost_columns(std::map<int, int>& cols, const std::map<int, int64_t>& boost,
                    const std::map<int, int64_t>& cap) {
@@ -922,6 +975,8 @@ struct Params {
   bool parallel = false;   // parallel = true: halves on two streams, right halves on forked streams
   bug_rng_fork_fn rng_fork = nullptr;
   void* rng_fork_user = nullptr;
+  bool exact = false;  // exact = true: DD expansions sketch the complete fused basis (no draws)
+  bool fold = true;    // fold_omega: frontier leaks from folded closures (sampled), else exact
 };
 
 struct MPS {
@@ -1436,7 +1491,16 @@ struct Step {
     T Om, directions, Y;
     double nY = 0.0;
     int64_t direction_count = 0;
-    if (P.dd_mode == 1) {
+    if (P.exact) {
+      // exact = true: the complete DD-projected fused basis sketched once and _dd_select's QR; the
+      // certified range without an allocation stops after this pass, its width cap being its start
+      // width (dd_cbe_expand.jl:91,346-360; sketch.jl:119-132). The mode is not consulted.
+      T probe = dd_probe_exact(e, opp, !left);
+      if (probe) {
+        directions = dd_select(e, frame, sketch(probe), left);
+        direction_count = directions ? dim(directions, fl) : 0;
+      }
+    } else if (P.dd_mode == 1) {
       const int64_t dmax = std::max({dim(U0, 0), old_rank, dim(V0, 2)});
       const int64_t grow = int64_t(std::ceil(ADAPTIVE_GROWTH * double(dmax))) - old_rank;
       const int64_t initial_width = int64_t(std::ceil(1.2 * double(std::max<int64_t>(grow, 1))));
@@ -1927,11 +1991,20 @@ struct Step {
     return m;
   }
 
-  // folded sketch closures + sampled leak (cbe.jl:62-144, 355-391; krylov_frontier_bonds.jl:80-100)
+  // _bond_action (krylov_frontier_bonds.jl:80-100). Folded: the sketch closures with the probe
+  // folded into the environment contractions and the sampled leak (cbe.jl:62-144, 355-391).
+  // Unfolded (fold_omega = false): the two-site action X = H Theta_F formed once and the exact
+  // leak |(I - U0 U0^dag) X| or |X (I - V0^dag V0)| (_left_leak/_right_leak, :37-66), no draws.
   double bond_action(const BondFrame& fr, int bond, const T& lenv, const T& renv, bool left) {
     const T& Wl = mpo[bond];
     const T& Wr = mpo[bond + 1];
     T theta = frame_theta(e, fr);
+    if (!P.fold) {
+      T X = env.two_site(lenv, Wl, Wr, renv, theta);  // (l, s1, s2, r)
+      if (left) return e.norm(perp_left(e, fr.U0, X));
+      T ov = e.contract(X, {2, 3}, fr.V0, {1, 2}, false, true);  // (l, s1, bond)
+      return e.norm(e.lin({{1.0, X}, {-1.0, e.contract(ov, {2}, fr.V0, {0})}}));
+    }
     const int64_t grown = left ? dim(fr.U0, 2) : dim(fr.V0, 0);
     const int count = int(std::max<int64_t>(8, (grown + 3) / 4));
     if (left) {
@@ -1965,7 +2038,7 @@ struct Step {
     T env;
     Ledger ledger;
     std::vector<double> leak;
-    int64_t added = 0, n_h1 = 0;
+    int64_t added = 0, n_h1 = 0, n_h2 = 0;
   };
 
   // A frontier half is a function of its inputs and its draws, so its cutoff-0 SVDs (the frames
@@ -2041,6 +2114,7 @@ struct Step {
       }
       const T& rch = rstack[bond + 2];
       const double lk = bond_action(tsf, bond, lch, rch, true);
+      if (!P.fold) out.n_h2 += 1;
       out.leak.push_back(lk);
       Ledger bl;
       const bool quiet = indicator(alloc, lk) <= alloc.per_bond;
@@ -2104,6 +2178,7 @@ struct Step {
       }
       const T& lch = lstack[bond];
       const double lk = bond_action(tsf, bond, lch, rch, false);
+      if (!P.fold) out.n_h2 += 1;
       leak[bond] = lk;
       Ledger bl;
       const bool quiet = indicator(alloc, lk) <= alloc.per_bond;
@@ -2186,6 +2261,7 @@ struct Step {
     }
     sw.ledger.n_closure_sweeps = 1;
     sw.ledger.n_h1_closure = rl.n_h1 + rr.n_h1;
+    sw.ledger.n_h2_leak = rl.n_h2 + rr.n_h2;
     sw.capped = sw.ledger.workcap_reached;
     return sw;
   }
@@ -2902,6 +2978,10 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     P.rng_fork = prm->rng_fork;
     P.rng_fork_user = prm->rng_fork_user;
     require(!P.parallel || (P.rng_fork && draw), "parallel needs rng_fork and a draw stream");
+    P.exact = prm->exact != 0;
+    require(prm->fold_omega >= 0 && prm->fold_omega <= 2, "fold_omega must be 0 (default), 1 or 2");
+    // bug_step_stages.jl:67: the folded closures are the default above order 1 unless exact
+    P.fold = prm->fold_omega == 0 ? (P.order > 1 && !P.exact) : prm->fold_omega == 1;
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
@@ -2934,7 +3014,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     S.eshift = prm->eshift;
     require(!prm->outside_residual || prm->root_report, "outside_residual needs root_report");
     require(!prm->outside_residual || prm->rng_ctl, "outside_residual needs rng_ctl (a copy of the draw stream)");
-    require(!prm->outside_residual || P.order > 1, "the outside residual with the exact (unfolded) leak is not built");
+    require(!prm->outside_residual || P.fold, "the outside residual with the exact (unfolded) leak is not built");
     S.root_link = P.root > 0 ? P.root : std::max(1, std::min(L - 1, L / 2));
     require(S.root_link >= 1 && S.root_link <= L - 1, "root must be a bond in 1:L-1");
 
@@ -3227,6 +3307,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     o.defect = ledger.defect;
     o.n_root_frontier = ledger.n_root_frontier;
     o.n_h1_closure = ledger.n_h1_closure;
+    o.n_h2_leak = ledger.n_h2_leak;
     o.n_compress = ledger.n_compress;
     o.leak1 = ledger.leak.size() > 1 ? ledger.leak[1] : 0.0;
     for (int b = 0; b < L - 1 && b < BUG_MAX_SITES; ++b) {

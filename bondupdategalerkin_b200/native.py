@@ -51,7 +51,8 @@ class StepParams(ctypes.Structure):
                 ("rng_ctl_user", ctypes.c_void_p), ("closure_checks", ctypes.c_int),
                 ("root_method", ctypes.c_int), ("root_noshift", ctypes.c_int),
                 ("parallel", ctypes.c_int), ("rng_fork", RNG_FORK_FN),
-                ("rng_fork_user", ctypes.c_void_p)]
+                ("rng_fork_user", ctypes.c_void_p), ("exact", ctypes.c_int),
+                ("fold_omega", ctypes.c_int)]
 
 
 class BondLog(ctypes.Structure):
@@ -87,7 +88,8 @@ class StepInfo(ctypes.Structure):
                 ("e_pre", ctypes.c_double), ("e_root", ctypes.c_double), ("resid", ctypes.c_double),
                 ("resid_initial", ctypes.c_double), ("outside", ctypes.c_double),
                 ("outside_left", ctypes.c_double), ("outside_right", ctypes.c_double),
-                ("outside_passes", ctypes.c_int), ("outside_added", ctypes.c_int)]
+                ("outside_passes", ctypes.c_int), ("outside_added", ctypes.c_int),
+                ("n_h2_leak", ctypes.c_int64)]
 
 
 
@@ -116,7 +118,8 @@ def _lib():
 def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None, order=1,
                 maxdim=None, hermitian=True, expansion=None, root=None, reorth=True, truncate=True,
                 work_ceiling_rule="bond", bond_ceiling_factor=None, root_maxiter=30,
-                krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None, closure_checks=False):
+                krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None, closure_checks=False,
+                exact=False):
     """The keyword arguments of ``cbe_bug_step!`` as the C-ABI's ``bug_step_params`` (checked the
     way the reference checks them, ``bug_step_stages.jl:15-142``)."""
     if L < 2:
@@ -127,8 +130,6 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r}")
     if frontier_tol or krylov_rank_tol:
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0")
-    if fold_omega is False and order > 1:
-        raise NotImplementedError("the exact (unfolded) closure leak")
     mode, width, tail_factor, kmode, fixed_depth = "rank_tail", 8, 0.10, "auto", 0
     holdout, batch, capsel, accept = 4, 1, "storage", 1.0
     if expansion is not None:
@@ -148,7 +149,7 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
     if holdout < 1:
         raise ValueError("holdout_width must be positive")
     resolve_krylov_recurrence(kmode, hermitian)  # refuses an unknown recurrence by name
-    if mode not in ("rank_tail", "adaptive"):
+    if mode not in ("rank_tail", "adaptive") and not exact:
         raise NotImplementedError(f"DD mode {mode!r}: :rank_tail and :adaptive are built")
     return StepParams(
         tol_basis=tol_basis or 0.0, tol_trunc=-1.0 if tol_trunc is None else tol_trunc,
@@ -161,7 +162,8 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         krylov_mode={"auto": 0, "lanczos": 1, "arnoldi": 2}[kmode], krylov_fixed_depth=fixed_depth,
         dd_mode=1 if mode == "adaptive" else 0, holdout_width=holdout, batch_blocks=batch,
         cap_selection=1 if capsel == "svd" else 0, acceptance_factor=accept,
-        closure_checks=int(bool(closure_checks)))
+        closure_checks=int(bool(closure_checks)), exact=int(bool(exact)),
+        fold_omega=0 if fold_omega is None else (1 if fold_omega else 2))
 
 
 def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_root=None,
@@ -234,12 +236,16 @@ def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_
         root_report=root_report, truncate=truncate, outside_residual=outside_residual)
     if outside_residual and root_report is None:
         raise ValueError("outside_residual needs root_report")
+    fold = (order > 1 and not exact) if fold_omega is None else bool(fold_omega)
+    if outside_residual and not fold:
+        raise NotImplementedError("the outside residual with the exact (unfolded) leak")
     p = step_params(L, tol_basis=tol_basis, tol_trunc=tol_trunc, tol_expv=tol_expv,
                     tol_krylov=tol_krylov, order=order, maxdim=maxdim, hermitian=hermitian,
                     expansion=expansion, root=root, reorth=reorth, truncate=truncate,
                     work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
                     root_maxiter=root_maxiter, krylov_rank_tol=krylov_rank_tol,
-                    frontier_tol=frontier_tol, fold_omega=fold_omega, closure_checks=closure_checks)
+                    frontier_tol=frontier_tol, fold_omega=fold_omega, closure_checks=closure_checks,
+                    exact=exact)
     if rng is None:
         rng = np.random.default_rng(0x5EED)
     saved = []
@@ -300,7 +306,7 @@ def _step_result(psi, ctx, arr, center, info, logs, nlog, order, eshift, root_re
         proj_err=info.proj_err, r_old=info.r_old, r_aug=info.r_aug, r_final=info.r_final,
         order=order, n_passes=info.n_passes, n_closure_sweeps=info.n_closure_sweeps,
         defect=info.defect, n_root_frontier=info.n_root_frontier, n_h1_closure=info.n_h1_closure,
-        n_compress=info.n_compress,
+        n_h2_leak=info.n_h2_leak, n_compress=info.n_compress,
         bond_log=[{f: getattr(logs[i], f) for f, _ in BondLog._fields_} for i in range(nlog)]
         if logs is not None else [],
     )

@@ -118,8 +118,6 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
         unbuilt.append("keep_states")
     if frames_only or frames_report is not None:
         unbuilt.append("frames_only / frames_report")
-    if exact:
-        unbuilt.append("exact = true (the complete DD-projected probe)")
     if unbuilt:
         raise NotImplementedError("not built: " + "; ".join(unbuilt))
     return tol_expv

@@ -244,6 +244,14 @@ typedef struct {
                                  frontier_closure.jl:121-145); needs rng_fork */
   bug_rng_fork_fn rng_fork;
   void* rng_fork_user;
+  int exact;                  /* 1: exact = true, the deterministic reference: every DD expansion
+                                 sketches the complete fused basis with the opposite frame projected
+                                 out (_dd_probe(...; exact = true), dd_cbe.jl:140-161) and keeps what
+                                 _dd_select's QR admits in one pass (dd_cbe_expand.jl:91,346-360) */
+  int fold_omega;             /* 0: the reference's default, folded above order 1 unless exact
+                                 (bug_step_stages.jl:67); 1: folded closures, sampled frontier leaks;
+                                 2: the exact leak of the formed two-site action
+                                 (krylov_frontier_bonds.jl:80-100) */
 } bug_step_params;
 
 
@@ -285,11 +293,13 @@ typedef struct {
    * and bound relative to ||psi_1||, the re-enrichment passes and directions added */
   double e_pre, e_root, resid, resid_initial, outside, outside_left, outside_right;
   int outside_passes, outside_added;
+  int64_t n_h2_leak; /* two-site applications that measured a frontier leak (fold_omega = false) */
 } bug_step_info;
 
 /* One rank-adaptive BUG step in place: `cbe_bug_step!(psi, mpo, tau; ...)`
- * (src/BUG/TimeEvolution/bug_step.jl:17-513), DD-QR :rank_tail or :adaptive expansion, Lanczos/Arnoldi local
- * Krylov, order-p single-pass closure with folded leak estimates, :exp root. `psi_io[L]` holds the
+ * (src/BUG/TimeEvolution/bug_step.jl:17-513), DD-QR :rank_tail, :adaptive or exact expansion,
+ * Lanczos/Arnoldi local Krylov, order-p single-pass or checked closure with folded (sampled) or
+ * exact frontier leaks, :exp or implicit root. `psi_io[L]` holds the
  * state's site handles on entry; on return each slot holds a new handle owned by the caller, or
  * NULL where the caller's handle is unchanged. The MPO handles are only read. */
 int bug_mps_step(bug_ctx* ctx, int L, bug_tensor** psi_io, int* center_io,

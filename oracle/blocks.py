@@ -454,6 +454,19 @@ def gaussian_fused(rng, la: Leg, lb: Leg, cols: dict, new_first: bool) -> BT | N
     C-ordered ``(n_c, cols[c])`` matrix, its rows the ``(qa, qb)`` pairs ascending, each pair
     ``dim(qa)*dim(qb)`` rows in C order. ``new_first=False`` gives legs ``(la, lb, g:+1)``
     (a left frame's layout), ``True`` gives ``(g:-1, la, lb)`` (a right frame's)."""
+    return _fused(la, lb, cols, new_first, lambda n, k: complex_normals(rng, n * k).reshape(n, k))
+
+
+def identity_fused(la: Leg, lb: Leg, new_first: bool) -> BT | None:
+    """The complete fused basis of ``la (x) lb`` (``fusion_basis``, used by ``_dd_probe(...;
+    exact = true)``, ``dd_cbe.jl:140-148``): in every fused sector ``c`` the ``n_c x n_c`` identity,
+    rows and columns both in the ``(qa, qb)``-pair order of :func:`gaussian_fused`, same layouts."""
+    fs = fused_sectors(la, lb, -1 if new_first else +1)
+    cols = {c: sum(la.sectors[qa] * lb.sectors[qb] for qa, qb in pairs) for c, pairs in fs.items()}
+    return _fused(la, lb, cols, new_first, lambda n, k: np.eye(n, k, dtype=np.complex128))
+
+
+def _fused(la: Leg, lb: Leg, cols: dict, new_first: bool, matrix) -> BT | None:
     gdir = -1 if new_first else +1
     fs = fused_sectors(la, lb, gdir)
     gsec = {c: cols.get(c, 0) for c in fs if cols.get(c, 0) > 0}
@@ -469,7 +482,7 @@ def gaussian_fused(rng, la: Leg, lb: Leg, cols: dict, new_first: bool) -> BT | N
         pairs = fs[c]
         rd = [la.sectors[qa] * lb.sectors[qb] for qa, qb in pairs]
         n = sum(rd)
-        M = complex_normals(rng, n * k).reshape(n, k)
+        M = matrix(n, k)
         off = 0
         for (qa, qb), r in zip(pairs, rd):
             blk = M[off:off + r].reshape(la.sectors[qa], lb.sectors[qb], k)

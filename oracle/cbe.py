@@ -9,7 +9,10 @@ TEST INFRASTRUCTURE (see ``oracle/blocks.py``). Restates:
   ``sector_graded_sketch(...; comp_ratio = nothing)`` (``sketch.jl:14-54``), ``_sample_residual``
   (``sketch.jl:141-180``), ``sampled_leak`` (``cbe.jl:355-391``), ``_fold_sketch_closures``
   (``cbe.jl:62-144``);
-* ``dd_cbe_expand`` with its default ``tail_dd`` branch (``dd_cbe_expand.jl:19-301,383-419``).
+* ``dd_cbe_expand`` with its default ``tail_dd`` branch (``dd_cbe_expand.jl:19-301,383-419``),
+  the incremental controller and the deterministic ``exact = true`` branch (the complete fused
+  basis, ``_dd_probe(...; exact = true)``, and the one-pass certified range, ``:346-360``);
+* ``_bond_action`` with ``fold = false``: the exact two-site leak (``krylov_frontier_bonds.jl:37-100``).
 
 A right frame's bond leg is incoming; an SVD over ``(site, link_r)`` returns that leg outgoing, so
 the orthonormal rows are re-expressed on an incoming leg (:func:`rows_from_u`) before they join a
@@ -151,6 +154,23 @@ def dd_probe(opp, oside, width, rng, boost=None):
         om = B.gaussian_fused(rng, opp.legs[0], opp.legs[1], cols, new_first=False)
     else:
         om = B.gaussian_fused(rng, opp.legs[1], opp.legs[2], cols, new_first=True)
+    if om is None:
+        return None
+    projected = (perp_left if oside == "left" else perp_right)(opp, om)
+    return projected if B.norm(projected) > 0 else None
+
+
+def dd_probe_exact(opp, oside):
+    """``_dd_probe(...; exact = true)`` (``dd_cbe.jl:140-161``): the complete fused basis of
+    ``opp``'s two local legs with ``opp`` projected out; ``None`` when there is no discarded space
+    or nothing survives the projection. Draws nothing."""
+    dfull, dT = fused_dims(opp, oside)
+    if sum(max(dfull[c] - dT[c], 0) for c in dfull) == 0:
+        return None
+    if oside == "left":
+        om = B.identity_fused(opp.legs[0], opp.legs[1], new_first=False)
+    else:
+        om = B.identity_fused(opp.legs[1], opp.legs[2], new_first=True)
     if om is None:
         return None
     projected = (perp_left if oside == "left" else perp_right)(opp, om)
@@ -527,6 +547,20 @@ def folded_closures(fr: BondFrame, mpo, bond, lenv, renv):
     return skl, skr
 
 
+def exact_leak(fr: BondFrame, mpo, bond, lenv, renv, side) -> float:
+    """``_bond_action`` with ``fold = false`` (``krylov_frontier_bonds.jl:94-99``): the two-site
+    action ``X = H Theta_F`` formed once and the exact leak ``||(I - U0 U0^dag) X||``
+    (``_left_leak``) or ``||X (I - V0^dag V0)||`` (``_right_leak``) of the frame's prescribed
+    isometry. Draws nothing."""
+    from .tdvp import apply_two_site
+
+    X = apply_two_site(lenv, mpo[bond], mpo[bond + 1], renv, frame_theta(fr))  # (l, s1, s2, r)
+    if side == "left":
+        return B.norm(perp_left(fr.U0, X))
+    ov = B.contract(X, (2, 3), fr.V0, (1, 2), conjb=True)  # (l, s1, bond)
+    return B.norm(B.sub(X, B.contract(ov, (2,), fr.V0, (0,))))
+
+
 def sampled_leak(fr: BondFrame, skl, skr, side, column_count, rng) -> float:
     """``sampled_leak`` (``cbe.jl:355-391``)."""
     if side == "left":
@@ -548,13 +582,18 @@ class Expansion:
 
 def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, workcap, rng,
                   fixed_width=8, tail_factor=0.10, mode="rank_tail", holdout_width=DD_HOLDOUT,
-                  batch_blocks=1, cap_selection="storage", acceptance_factor=1.0) -> Expansion:
+                  batch_blocks=1, cap_selection="storage", acceptance_factor=1.0,
+                  exact=False) -> Expansion:
     """Grow one frame of the bond by the DD-projected sketch (``dd_cbe_expand.jl:19-419``): rank
     by tail bisection (``:rank_tail``, ``tail_dd``) or by the incremental controller
-    (``:adaptive``, ``_dd_controller``)."""
-    if mode not in ("rank_tail", "adaptive"):
+    (``:adaptive``, ``_dd_controller``). ``exact = true`` (the deterministic reference) sketches
+    the complete DD-projected fused basis once and keeps what ``_dd_select``'s QR admits: the
+    ``_certified_range`` call with no allocation (``dd_cbe_expand.jl:346-360``), whose
+    ``_range_find`` stops after one pass because its width cap is its start width
+    (``dd_cbe_expand.jl:91``, ``sketch.jl:119-132``); the mode is then not consulted."""
+    if mode not in ("rank_tail", "adaptive") and not exact:
         raise NotImplementedError(f"DD mode {mode!r}: only :rank_tail and :adaptive are restated")
-    if fixed_width < 1:
+    if mode == "rank_tail" and fixed_width < 1:
         raise ValueError("rank_tail requires positive fixed_width")
     if not 0 < tail_factor <= 1:
         raise ValueError("tail_factor must lie in (0,1]")
@@ -593,7 +632,13 @@ def dd_cbe_expand(fr: BondFrame, mpo, bond, lenv, renv, side, alloc, ledger, wor
             return perp_right(V0, b)
 
     directions, direction_count = None, 0
-    if mode == "adaptive":
+    if exact:
+        Om = dd_probe_exact(opp, oside)
+        if Om is not None:
+            directions = dd_select(frame, sketch(Om), side)
+            direction_count = 0 if directions is None else directions.dim(fl)
+        Om = None
+    elif mode == "adaptive":
         dmax = max(U0.dim(0), old_rank, V0.dim(2))
         initial_width = math.ceil(1.2 * max(math.ceil(ADAPTIVE_GROWTH * dmax) - old_rank, 1))
         wcap = full_opp

@@ -19,8 +19,9 @@ TEST INFRASTRUCTURE (see ``oracle/blocks.py``). Restates, in the reference's ord
   ``_assemble_and_compress!`` (``diagnostics.jl:269-337``).
 
 Scope: ``mode = :rank_tail`` DD-QR expansion, Lanczos/Arnoldi local Krylov with the sequential
-rule, ``order >= 1`` with the single-pass closure (``closure_checks = false``) and folded leak
-estimates, root ``:exp`` only, no ``keep_states``/K-L-S/root report. Those keywords raise.
+rule, ``order >= 1`` with the single-pass or checked closure and the folded (sampled) or, with
+``fold_omega = false``, exact frontier leaks; ``exact = true`` expands by the complete DD-projected
+fused basis. ``keep_states``, ``frames_only`` and the K/L/S schedules raise.
 """
 
 from __future__ import annotations
@@ -36,8 +37,8 @@ from . import krylov as K
 from .budget import (DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
                      basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
                      work_ceiling)
-from .cbe import (BondFrame, cap_to_local_room, dd_cbe_expand, folded_closures, perp_left,
-                  perp_right, rank_cut, reortho, rows_from_u, sampled_leak)
+from .cbe import (BondFrame, cap_to_local_room, dd_cbe_expand, exact_leak, folded_closures,
+                  perp_left, perp_right, rank_cut, reortho, rows_from_u, sampled_leak)
 from .env import (ZeroSiteH, apply_one_site, left_boundary, left_env_stack, left_step,
                   right_boundary, right_env_stack, right_step, total_charge)
 
@@ -211,6 +212,8 @@ class Ctx:
     rng: object
     eshift: float = 0.0  # the generators are H - eshift (shift_h, effective_operators.jl:110-129)
     parallel: bool = False  # parallel = true: right halves draw from a stream forked off `rng`
+    exact: bool = False  # exact = true: DD expansions sketch the complete fused basis, no draws
+    fold: bool = True  # fold_omega: frontier leaks sampled from folded closures, else exact
 
 
 def fork_rng(rng):
@@ -244,7 +247,7 @@ def expand(cx: Ctx, fr, bond, lch, rch, side, ledger):
                          holdout_width=cx.expansion.holdout_width,
                          batch_blocks=cx.expansion.batch_blocks,
                          cap_selection=cx.expansion.cap_selection,
-                         acceptance_factor=cx.expansion.acceptance_factor)
+                         acceptance_factor=cx.expansion.acceptance_factor, exact=cx.exact)
 
 
 def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
@@ -406,8 +409,12 @@ def frontier_mps(psi, fr: KLFrames, core):
     return MPS(ts, root)
 
 
-def bond_action(fr2: BondFrame, mpo, bond, lch, rch, side, rng):
-    """``_bond_action`` with ``fold = true`` (``krylov_frontier_bonds.jl:80-100``)."""
+def bond_action(fr2: BondFrame, mpo, bond, lch, rch, side, rng, fold=True):
+    """``_bond_action`` (``krylov_frontier_bonds.jl:80-100``): with ``fold = true`` the sampled
+    leak of the folded closures, with ``fold = false`` the exact leak of the formed two-site
+    action (one two-site application, no draws)."""
+    if not fold:
+        return exact_leak(fr2, mpo, bond, lch, rch, side)
     skl, skr = folded_closures(fr2, mpo, bond, lch, rch)
     grown = fr2.U0.dim(2) if side == "left" else fr2.V0.dim(0)
     count = max(8, -(-grown // 4))
@@ -424,7 +431,7 @@ def frontier_left(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
     Wn = {}
     lg = Ledger()
     leak = [0.0] * (root + 1)
-    out = dict(added=0, nskip=0, n_h1=0)
+    out = dict(added=0, nskip=0, n_h1=0, n_h2=0)
     if not enrich:
         chain = {}
         ch = left_boundary()
@@ -439,7 +446,8 @@ def frontier_left(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
         site_core = Fm[bond] if carry is None else B.contract(carry, (1,), Fm[bond], (0,))
         tsf = frame_onto_left(old, site_core, Fm[bond + 1])
         rch = rstack[bond + 2]
-        leak[bond] = bond_action(tsf, mpo, bond, lch, rch, "left", cx.rng)
+        leak[bond] = bond_action(tsf, mpo, bond, lch, rch, "left", cx.rng, cx.fold)
+        out["n_h2"] += 0 if cx.fold else 1
         bl = Ledger()
         quiet = indicator(cx.alloc, leak[bond]) <= cx.alloc.per_bond
         if enrich and not quiet:
@@ -472,7 +480,7 @@ def frontier_left(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
         if enrich and bond < root:
             lch = left_step(lch, Wn[bond], mpo[bond])
     return dict(frames=Wn, env=lenv, ledger=lg, leak=leak[1:], added=out["added"],
-                n_h1=out["n_h1"])
+                n_h1=out["n_h1"], n_h2=out["n_h2"])
 
 
 def frontier_right(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
@@ -485,7 +493,7 @@ def frontier_right(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
     Zn = {}
     lg = Ledger()
     leak = [0.0] * L
-    out = dict(added=0, nskip=0, n_h1=0)
+    out = dict(added=0, nskip=0, n_h1=0, n_h2=0)
     if not enrich:
         chain = {}
         ch = right_boundary(total_charge(Fm))
@@ -500,7 +508,8 @@ def frontier_right(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
         site_core = Fm[bond + 1] if carry is None else B.contract(Fm[bond + 1], (2,), carry, (0,))
         tsf = frame_onto_right(Fm[bond], site_core, old)
         lch = lstack[bond]
-        leak[bond] = bond_action(tsf, mpo, bond, lch, rch, "right", cx.rng)
+        leak[bond] = bond_action(tsf, mpo, bond, lch, rch, "right", cx.rng, cx.fold)
+        out["n_h2"] += 0 if cx.fold else 1
         bl = Ledger()
         quiet = indicator(cx.alloc, leak[bond]) <= cx.alloc.per_bond
         if enrich and not quiet:
@@ -533,7 +542,7 @@ def frontier_right(Fm, mpo, fr: KLFrames, cx: Ctx, amp, enrich, gen):
         if enrich and bond > root:
             rch = right_step(rch, Zn[bond], mpo[bond + 1])
     return dict(frames=Zn, env=renv, ledger=lg, leak=[leak[b] for b in range(root, L)],
-                added=out["added"], n_h1=out["n_h1"])
+                added=out["added"], n_h1=out["n_h1"], n_h2=out["n_h2"])
 
 
 def frontier_sweep(fr: KLFrames, psi, mpo, core, degree, cx: Ctx, nrm, enrich=True):
@@ -568,6 +577,7 @@ def frontier_sweep(fr: KLFrames, psi, mpo, core, degree, cx: Ctx, nrm, enrich=Tr
         fr.lenv, fr.renv, fr.gen = rl["env"], rr["env"], gen
     lg.n_closure_sweeps = 1
     lg.n_h1_closure = rl["n_h1"] + rr["n_h1"]
+    lg.n_h2_leak = rl["n_h2"] + rr["n_h2"]
     return dict(added=added, leak=leak, met=met, capped=enrich and lg.workcap_reached, ledger=lg,
                 leaks_left=rl["leak"], leaks_right=rr["leak"])
 
@@ -955,8 +965,8 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
-    if len(keep_states) or frames_only or frames_report is not None or exact:
-        raise NotImplementedError("keep_states, frames_only, frames_report and exact are not restated")
+    if len(keep_states) or frames_only or frames_report is not None:
+        raise NotImplementedError("keep_states, frames_only and frames_report are not restated")
     return root_link, tol_expv
 
 
@@ -987,9 +997,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         raise ValueError(f"order must be >= 1, got {order}")
     if bond_ceiling_factor is None:
         bond_ceiling_factor = DEFAULT_BOND_CEILING_FACTOR if work_ceiling_rule == "bond" else 0.0
-    fold = (order > 1) if fold_omega is None else fold_omega
-    if order > 1 and not fold:
-        raise NotImplementedError("the exact (unfolded) closure leak is not restated")
+    # bug_step_stages.jl:67: the folded closures are the default above order 1 unless exact
+    fold = (order > 1 and not exact) if fold_omega is None else bool(fold_omega)
     if outside_residual and root_report is None:
         raise ValueError("outside_residual needs root_report")
     if outside_residual and not fold:
@@ -1023,7 +1032,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     nR = [0] * (L - 1)
     accL, accR = HalfAcc(), HalfAcc()
     run_parallel = parallel is True or parallel == "half_sweeps"
-    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel)
+    cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel,
+             bool(exact), fold)
     # parallel = true: the right half-sweep's stream is forked off the step's before either half
     # runs (bug_step.jl:222-268)
     cxR = replace(cx, rng=fork_rng(rng)) if run_parallel else cx

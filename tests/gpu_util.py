@@ -80,3 +80,13 @@ def overlap(a, b):
 def fidelity(a, b):
     ab = overlap(a, b)
     return abs(ab) ** 2 / (overlap(a, a).real * overlap(b, b).real)
+
+
+def perturbed_mpo(mpo, seed, eps=1e-14):
+    """The oracle MPO with every core perturbed by eps (relative): another valid compression of
+    the same operator, whose runs show which of the oracle's decisions hang on round-off."""
+    from oracle.models import MPO
+
+    r = np.random.default_rng(seed)
+    return MPO([OB.BT(t.legs, {k: v * (1 + eps * r.standard_normal(v.shape))
+                               for k, v in t.blocks.items()}) for t in mpo.tensors])

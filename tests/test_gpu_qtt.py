@@ -25,7 +25,7 @@ import pytest
 
 from oracle import qtt as Q
 from oracle import step as OS
-from tests.gpu_util import mps_to_host, overlap
+from tests.gpu_util import mps_to_host, overlap, perturbed_mpo
 
 pytestmark = pytest.mark.gpu
 
@@ -49,13 +49,7 @@ def _perturbed(psi, seed, eps=1e-15):
 
 
 def _perturbed_mpo(mpo, seed, eps=1e-14):
-    """The oracle MPO with every core perturbed by eps (relative): another valid compression."""
-    from oracle.blocks import BT
-    from oracle.models import MPO
-
-    r = np.random.default_rng(seed)
-    return MPO([BT(t.legs, {k: v * (1 + eps * r.standard_normal(v.shape))
-                           for k, v in t.blocks.items()}) for t in mpo.tensors])
+    return perturbed_mpo(mpo, seed, eps)
 
 
 def run_heston(nbits, steps, maxdim, native, mpo_from="product", norm_tol=1e-10, spread=None,

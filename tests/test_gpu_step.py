@@ -13,7 +13,7 @@ import pytest
 
 from oracle import models as OM
 from oracle import step as OS
-from tests.gpu_util import fidelity, mps_to_host
+from tests.gpu_util import fidelity, mps_to_host, perturbed_mpo
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +30,13 @@ def dev():
 
 
 def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_every=1,
-             native=False, widths=True, **kw):
+             native=False, widths=True, selected_ties=0, sz_tol=1e-10, **kw):
+    """The device step against the oracle's on the same seeded chain, step by step. With
+    ``selected_ties = n`` the oracle also runs n copies whose MPO cores are perturbed at 1e-14, and
+    the device's ``n_selected`` may equal any of theirs: under ``exact = true`` the first QR pass
+    admits directions whose pivots sit at round-off level beside its floor, so that count is not a
+    function of the exact inputs (everything else is still held to the unperturbed oracle).
+    ``sz_tol`` is the bar on the relative S^z difference (default 1e-10)."""
     DM, DS = dev
     from bondupdategalerkin_b200 import native as DN
 
@@ -46,9 +52,14 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
         e = kw["expansion"]
         okw["expansion"] = OS.DDQRExpansion(**e)
         dkw["expansion"] = DS.DDQRExpansion(**e)
+    copies = [(getattr(OM, start)(L, symmetry=sym), perturbed_mpo(ompo, s), np.random.default_rng(1234))
+              for s in range(1, selected_ties + 1)]
     worst = (0.0, 0.0)
     for n in range(1, steps + 1):
         oi = OS.cbe_bug_step(ostate, ompo, tau, order=order, rng=orng, **okw)
+        ties = {oi["ledger"].n_selected} | {
+            OS.cbe_bug_step(p, m, tau, order=order, rng=r, **okw)["ledger"].n_selected
+            for p, m, r in copies}
         di = dstep(dstate, dmpo, tau, order=order, rng=drng, **dkw)
         assert di["bond_dims"] == oi["bond_dims"], (n, di["bond_dims"], oi["bond_dims"])
         assert di["status"] == oi["status"], n
@@ -56,8 +67,9 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
         assert di["ledger"].expv_iters == oi["ledger"].expv_iters, n
         if widths:
             assert di["expanded"] == oi["expanded"], n
-            for f in ("n_probes", "n_holdout", "n_targeted", "n_selected"):
+            for f in ("n_probes", "n_holdout", "n_targeted"):
                 assert getattr(di["ledger"], f) == getattr(oi["ledger"], f), (n, f)
+            assert di["ledger"].n_selected in ties, (n, di["ledger"].n_selected, ties)
         if n % check_every == 0 or n == steps:
             h = mps_to_host(dstate)
             inf = 1.0 - fidelity(h, ostate)
@@ -66,7 +78,7 @@ def run_pair(dev, L, steps, start, delta, order, sym="U1", tau=-0.05j, check_eve
             rel = np.max(np.abs(sz_d - sz_o)) / max(np.max(np.abs(sz_o)), 1e-300)
             worst = (max(worst[0], inf), max(worst[1], rel))
             assert inf <= 1e-12, (n, inf)
-            assert rel <= 1e-10, (n, rel)
+            assert rel <= sz_tol, (n, rel)
     return ostate, dstate, worst
 
 

@@ -7,7 +7,7 @@ the other. ``test/BUG/TimeEvolution/test_parallel_half_sweeps.jl:15-55`` runs th
 (XXZ, delta = 1, tau = -0.05i, tol_basis 1e-7, tol_trunc 1e-9, tol_expv 1e-10, maxdim 64) for two
 steps at order 1 and 2: with randomised selection the parallel state matches the serial one to
 1 - fidelity < 1e-8 (the sketches differ) and two parallel runs agree to < 1e-13 (here: exactly);
-its exact-selection half (no draws, agreement to round-off) needs ``exact = true``, not built.
+its exact-selection half (no draws, agreement to round-off) is in ``test_exact_oracle.py``.
 """
 
 import numpy as np

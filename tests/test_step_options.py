@@ -40,7 +40,8 @@ BAD = [
     (dict(frames_only=True), ValueError),
     (dict(frames_only=True, truncate=False), NotImplementedError),
     (dict(frames_report={}), NotImplementedError),
-    (dict(exact=True), NotImplementedError),
+    (dict(order=2, fold_omega=False, outside_residual=True, root_report={}), NotImplementedError),
+    (dict(exact=True, order=2, outside_residual=True, root_report={}), NotImplementedError),
     (dict(kls="foo"), ValueError),
     (dict(kls="sequential", outside_residual=True, root_report={}), ValueError),
     (dict(kls="sequential"), NotImplementedError),
