@@ -29,7 +29,7 @@ def test_exact_xxz_quench_vs_oracle(dev, order):  # noqa: F811
 
 def test_exact_order3_neel_vs_oracle(dev):  # noqa: F811
     run_pair(dev, 8, 3, "neel_state", 1.0, 3, tau=-0.2j, tol_basis=1e-8, tol_root=1e-12,
-             tol_trunc=1e-12, maxdim=64, exact=True, selected_ties=2)
+             tol_trunc=1e-12, maxdim=64, exact=True)
 
 
 def test_exact_wide_bonds_vs_oracle(dev):  # noqa: F811
@@ -64,7 +64,7 @@ def test_exact_serial_equals_parallel_reference_setting(dev, order):  # noqa: F8
     DM, _ = dev
     from bondupdategalerkin_b200 import native as DN
 
-    kw = dict(tol_basis=1e-7, tol_trunc=1e-9, tol_expv=1e-10, maxdim=64, exact=True, selected_ties=2)
+    kw = dict(tol_basis=1e-7, tol_trunc=1e-9, tol_expv=1e-10, maxdim=64, exact=True)
     mpo = DM.xxz_mpo(6, J=1.0, delta=1.0)
     serial, par = DM.neel_state(6), DM.neel_state(6)
     rs = np.random.default_rng(9)
