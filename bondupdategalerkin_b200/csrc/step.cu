@@ -60,6 +60,7 @@ constexpr double EXPV_SHIFT_TRIGGER = 30.0;
 constexpr double EXPV_MAX_NORM = 1e150;
 constexpr double FRONTIER_FLOOR = 1e-14;
 constexpr double REORTH_KEEP = 0.70710678118654752440;  // _REORTH_KEEP, dd_cbe.jl:273
+constexpr double UNION_KEEP = 0.5;                        // _UNION_KEEP, half_sweeps.jl:127
 constexpr int DD_HOLDOUT = 4;                             // _DD_HOLDOUT, dd_cbe_controller.jl:12
 constexpr double ADAPTIVE_GROWTH = 1.2;                   // basis_budget.jl:565
 
@@ -977,6 +978,9 @@ struct Params {
   void* rng_fork_user = nullptr;
   bool exact = false;  // exact = true: DD expansions sketch the complete fused basis (no draws)
   bool fold = true;    // fold_omega: frontier leaks from folded closures (sampled), else exact
+  std::vector<std::vector<T>> keep;  // keep_states: each kept state's L sites (borrowed)
+  std::vector<double> keep_tols;     // per kept state: 0 contained exactly, > 0 admitted at it
+  bool cap_keep = false;             // :bond ceiling: admitted states fill frames to the ceiling
 };
 
 struct MPS {
@@ -1827,6 +1831,43 @@ struct Step {
                [&] { out = half_right_body(psiR, rf, expanded, nn, hl); });
     return out;
   }
+  // ── kept states (keep_states / keep_tols, half_sweeps.jl:127-204) ──
+  // _union_fresh: orthonormal directions of `cand` outside `frame` that survive a second
+  // projection, at most `room` of them (the strongest), or null. tol = 0 admits every direction
+  // above the numerical floor (`cand` is contained exactly); tol > 0 only those carrying more
+  // than about tol |cand|.
+  T union_fresh(const T& frame, const T& cand, bool left, double tol, int64_t room) {
+    if (room <= 0) return nullptr;
+    const std::vector<int> legs = left ? std::vector<int>{0, 1} : std::vector<int>{1, 2};
+    auto perp = [&](const T& x) { return left ? perp_left(e, frame, x) : perp_right(e, frame, x); };
+    auto orient = [&](const T& U) { return left ? U : rows_from_u(e, U); };
+    T res = perp(cand);
+    const auto nn = e.norms(cand, res);
+    const double ncand = nn.first, nres = nn.second;
+    if (nres <= CBE_EPS * std::max(ncand, 1.0) || nres <= tol * ncand) return nullptr;
+    const double first_cut = std::max(rank_cut(0.0, ncand, nres), tol * ncand / nres);
+    T basis = orient(svd(e, e.scale(res, cd(1.0 / nres)), legs, first_cut, -1, W_U).U);
+    res = perp(basis);
+    double smax = 0.0;
+    for (auto& k : svd(e, res, legs, 1e-13, -1, W_U).kept) smax = std::max(smax, k.first);
+    if (smax < UNION_KEEP) return nullptr;
+    const int nkeep = room >= int64_t(INT32_MAX) ? -1 : int(room);
+    return orient(svd(e, res, legs, UNION_KEEP / smax, nkeep, W_U).U);
+  }
+  // every kept state's carried site tensor unioned into `frame` in turn (_union_left/_right and
+  // the loops at half_sweeps.jl:281-297, 385-398); under the :bond ceiling a tolerance-admitted
+  // state fills the frame only up to the bond's work ceiling (_keep_room, :179-181)
+  T union_kept(T frame, const std::vector<T>& cands, bool left, int bond) {
+    const int fl = left ? 2 : 0;
+    for (size_t i = 0; i < cands.size(); ++i) {
+      const double tol = P.keep_tols[i];
+      const int64_t room = P.cap_keep && tol > 0 ? cap_at(bond) - dim(frame, fl) : INT64_MAX;
+      T fresh = union_fresh(frame, cands[i], left, tol, room);
+      if (fresh) frame = e.oplus({frame, fresh}, fl);
+    }
+    return frame;
+  }
+
   T half_left_body(MPS& psiL, std::map<int, T>& lf, std::vector<int64_t>& expanded,
                    std::vector<int64_t>& nn, Ledger& hl) {
     canonical(psiL, 1);
@@ -1834,6 +1875,7 @@ struct Step {
     T lch = env.left_boundary();
     T lroot = lch;
     T carry;
+    std::vector<T> kcar(P.keep.size());  // each kept state's carry (b_i, link)
     for (int bond = 1; bond <= root_link; ++bond) {
       T carried = carry ? e.contract(carry, {1}, psiL[bond], {0}) : psiL[bond];
       BondFrame fr = frame_from(carried, psiL[bond + 1]);
@@ -1849,6 +1891,15 @@ struct Step {
       nmv += kr.second.n_h1;
       record_krylov(bl, kr.second);
       T Wk = kr.first;
+      if (!P.keep.empty()) {
+        std::vector<T> kx;
+        for (size_t i = 0; i < P.keep.size(); ++i) {
+          const T& site = P.keep[i][size_t(bond - 1)];
+          kx.push_back(kcar[i] ? e.contract(kcar[i], {1}, site, {0}) : site);
+        }
+        Wk = union_kept(Wk, kx, true, bond);  // every union before any carry
+        for (size_t i = 0; i < kx.size(); ++i) kcar[i] = e.contract(Wk, {0, 1}, kx[i], {0, 1}, true, false);
+      }
       lf[bond] = Wk;
       expanded[bond - 1] = dim(Wk, 2);
       log_bond(hl, bl, bond, 0, int(expanded[bond - 1]));
@@ -1866,6 +1917,7 @@ struct Step {
     T rch = env.right_boundary(total_charge(psiR));
     T rroot = rch;
     T carry;
+    std::vector<T> kcar(P.keep.size());  // each kept state's carry (link, b_j)
     for (int bond = L - 1; bond >= root_link; --bond) {
       T carried = carry ? e.contract(psiR[bond + 1], {2}, carry, {0}) : psiR[bond + 1];
       BondFrame fr = frame_from(psiR[bond], carried);
@@ -1881,6 +1933,15 @@ struct Step {
       nmv += kr.second.n_h1;
       record_krylov(bl, kr.second);
       T Zk = kr.first;
+      if (!P.keep.empty()) {
+        std::vector<T> kx;
+        for (size_t i = 0; i < P.keep.size(); ++i) {
+          const T& site = P.keep[i][size_t(bond)];
+          kx.push_back(kcar[i] ? e.contract(site, {2}, kcar[i], {0}) : site);
+        }
+        Zk = union_kept(Zk, kx, false, bond);
+        for (size_t i = 0; i < kx.size(); ++i) kcar[i] = e.contract(kx[i], {1, 2}, Zk, {1, 2}, false, true);
+      }
       rf[bond] = Zk;
       if (bond != root_link) expanded[bond - 1] = dim(Zk, 0);
       log_bond(hl, bl, bond, 1, int(dim(Zk, 0)));
@@ -2982,6 +3043,20 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     require(prm->fold_omega >= 0 && prm->fold_omega <= 2, "fold_omega must be 0 (default), 1 or 2");
     // bug_step_stages.jl:67: the folded closures are the default above order 1 unless exact
     P.fold = prm->fold_omega == 0 ? (P.order > 1 && !P.exact) : prm->fold_omega == 1;
+    require(prm->n_keep >= 0 && (prm->n_keep == 0 || prm->keep_sites), "keep_states: no site handles");
+    for (int k = 0; k < prm->n_keep; ++k) {
+      std::vector<T> sites;
+      for (int i = 0; i < L; ++i) {
+        const bug_tensor* t = prm->keep_sites[size_t(k) * size_t(L) + size_t(i)];
+        require(t != nullptr && t->rank == 3, "keep_states: a site is not a rank-3 tensor");
+        sites.push_back(T(const_cast<bug_tensor*>(t), [](bug_tensor*) {}));
+      }
+      P.keep.push_back(std::move(sites));
+      const double tol = prm->keep_tols ? prm->keep_tols[k] : 0.0;
+      require(tol >= 0, "keep_tols must be >= 0");
+      P.keep_tols.push_back(tol);
+    }
+    P.cap_keep = prm->work_ceiling_rule == 0;
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");

@@ -52,7 +52,9 @@ class StepParams(ctypes.Structure):
                 ("root_method", ctypes.c_int), ("root_noshift", ctypes.c_int),
                 ("parallel", ctypes.c_int), ("rng_fork", RNG_FORK_FN),
                 ("rng_fork_user", ctypes.c_void_p), ("exact", ctypes.c_int),
-                ("fold_omega", ctypes.c_int)]
+                ("fold_omega", ctypes.c_int), ("n_keep", ctypes.c_int),
+                ("keep_sites", ctypes.POINTER(ctypes.c_void_p)),
+                ("keep_tols", ctypes.POINTER(ctypes.c_double))]
 
 
 class BondLog(ctypes.Structure):
@@ -284,7 +286,21 @@ def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_
     p.root_report = int(root_report is not None)
     p.outside_residual = int(bool(outside_residual))
     p.rng_ctl = rng_ctl
-    return p, {"rng": rng, "rng_ctl": rng_ctl, "saved": saved, "rng_fork": rng_fork, "forks": forks}
+    held = {"rng": rng, "rng_ctl": rng_ctl, "saved": saved, "rng_fork": rng_fork, "forks": forks}
+    if len(keep_states):
+        # the kept states' site handles, state-major, and their tolerances (0: contained exactly)
+        for k in keep_states:
+            if len(k) != L:
+                raise ValueError(f"a kept state has {len(k)} sites, the state has {L}")
+        sites = (ctypes.c_void_p * (len(keep_states) * L))(
+            *[t.h.value for k in keep_states for t in k.tensors])
+        tols = [float(t) for t in keep_tols] if len(keep_tols) else [0.0] * len(keep_states)
+        ctols = (ctypes.c_double * len(tols))(*tols)
+        p.n_keep = len(keep_states)
+        p.keep_sites = ctypes.cast(sites, ctypes.POINTER(ctypes.c_void_p))
+        p.keep_tols = ctypes.cast(ctols, ctypes.POINTER(ctypes.c_double))
+        held["keep"] = (sites, ctols, list(keep_states))
+    return p, held
 
 
 def _step_result(psi, ctx, arr, center, info, logs, nlog, order, eshift, root_report):

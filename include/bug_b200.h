@@ -252,6 +252,15 @@ typedef struct {
                                  (bug_step_stages.jl:67); 1: folded closures, sampled frontier leaks;
                                  2: the exact leak of the formed two-site action
                                  (krylov_frontier_bonds.jl:80-100) */
+  int n_keep;                 /* keep_states: how many MPS the trial space must contain; each
+                                 half-sweep unions their carried sites into its frames
+                                 (_union_fresh, half_sweeps.jl:143-204) */
+  const bug_tensor* const* keep_sites; /* n_keep x L borrowed site handles, state-major (state k's
+                                 site i at [k L + i]), legs as psi's; read during the call only */
+  const double* keep_tols;    /* n_keep entries or NULL (all 0): 0 contains the state exactly,
+                                 > 0 admits only its directions carrying more than ~tol of it; under
+                                 work_ceiling_rule :bond an admitted state fills a frame only up to
+                                 its bond's ceiling */
 } bug_step_params;
 
 

@@ -37,8 +37,9 @@ from . import krylov as K
 from .budget import (DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
                      basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
                      work_ceiling)
-from .cbe import (BondFrame, cap_to_local_room, dd_cbe_expand, exact_leak, folded_closures,
-                  perp_left, perp_right, rank_cut, reortho, rows_from_u, sampled_leak)
+from .cbe import (CBE_EPS, BondFrame, cap_to_local_room, dd_cbe_expand, exact_leak,
+                  folded_closures, perp_left, perp_right, rank_cut, reortho, rows_from_u,
+                  sampled_leak)
 from .env import (ZeroSiteH, apply_one_site, left_boundary, left_env_stack, left_step,
                   right_boundary, right_env_stack, right_step, total_charge)
 
@@ -214,6 +215,9 @@ class Ctx:
     parallel: bool = False  # parallel = true: right halves draw from a stream forked off `rng`
     exact: bool = False  # exact = true: DD expansions sketch the complete fused basis, no draws
     fold: bool = True  # fold_omega: frontier leaks sampled from folded closures, else exact
+    keep_states: tuple = ()  # MPS the frames must contain (keep_states)
+    keep_tols: tuple = ()  # per kept state: 0 contained exactly, > 0 admitted at that tolerance
+    cap_keep: bool = False  # work_ceiling_rule = :bond: admitted states fill frames to the ceiling
 
 
 def fork_rng(rng):
@@ -250,6 +254,51 @@ def expand(cx: Ctx, fr, bond, lch, rch, side, ledger):
                          acceptance_factor=cx.expansion.acceptance_factor, exact=cx.exact)
 
 
+UNION_KEEP = 0.5  # ``_UNION_KEEP`` (half_sweeps.jl:127)
+
+
+def union_fresh(frame, cand, side, tol=0.0, room=None):
+    """``_union_fresh`` (``half_sweeps.jl:143-176``): orthonormal directions of ``cand`` outside
+    ``frame`` that survive a second projection, at most ``room`` of them (the strongest), or
+    ``None``. ``tol = 0`` admits every direction above the numerical floor (``cand`` is contained
+    exactly); ``tol > 0`` only those carrying more than about ``tol |cand|``."""
+    if room is not None and room <= 0:
+        return None
+    left = side == "left"
+    perp = perp_left if left else perp_right
+    legs = (0, 1) if left else (1, 2)
+
+    def orient(U):
+        return U if left else rows_from_u(U)
+
+    res = perp(frame, cand)
+    nres, ncand = B.norm(res), B.norm(cand)
+    if nres <= CBE_EPS * max(ncand, 1.0) or nres <= tol * ncand:
+        return None
+    first_cut = max(rank_cut(0.0, ncand, nres), tol * ncand / nres)
+    basis = orient(B.svd(B.scale(res, 1.0 / nres), legs, cutoff=first_cut).U)
+    res = perp(frame, basis)
+    fac = B.svd(res, legs, cutoff=1e-13)
+    smax = max((sv for sv, *_ in fac.kept), default=0.0)
+    if smax < UNION_KEEP:
+        return None
+    return orient(B.svd(res, legs, cutoff=UNION_KEEP / smax, nkeep=room).U)
+
+
+def union_kept(frame, cands, side, cx: Ctx, bond):
+    """Every kept state's carried site tensor unioned into ``frame`` in turn (``_union_left`` /
+    ``_union_right``, ``half_sweeps.jl:184-204``, the loops at ``:281-297`` and ``:385-398``);
+    under the per-bond ceiling a tolerance-admitted state fills the frame only up to the bond's
+    work ceiling (``_keep_room``, ``:179-181``)."""
+    fl = 2 if side == "left" else 0
+    for cand, tol in zip(cands, cx.keep_tols):
+        room = cap_at(cx.wcap, bond) - frame.dim(fl) if cx.cap_keep and tol > 0 else None
+        fresh = union_fresh(frame, cand, side, tol, room)
+        if fresh is not None:
+            frame = B.oplus([frame, fresh], fl)
+    return frame
+
+
 def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
     mpo, root = cx.mpo, cx.root_link
     canonical(psiL, 1)
@@ -257,6 +306,7 @@ def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
     lch = left_boundary()
     lroot = lch
     carry = None
+    kcar = [None] * len(cx.keep_states)  # each kept state's carry (b_i, link)
     for bond in range(1, root + 1):
         carried = psiL[bond] if carry is None else B.contract(carry, (1,), psiL[bond], (0,))
         fr = frame_from(carried, psiL[bond + 1])
@@ -276,6 +326,11 @@ def half_left(psiL, left_frames, expanded, nn, acc, hledger, cx: Ctx):
                                workcap=cap_at(cx.wcap, bond), recurrence=cx.recurrence,
                                fixed_depth=cx.expansion.krylov_fixed_depth)
         record_krylov(bl, st, cx.alloc)
+        if cx.keep_states:
+            kx = [k[bond] if c is None else B.contract(c, (1,), k[bond], (0,))
+                  for k, c in zip(cx.keep_states, kcar)]
+            Wk = union_kept(Wk, kx, "left", cx, bond)
+            kcar = [B.contract(Wk, (0, 1), x, (0, 1), conja=True) for x in kx]
         left_frames[bond] = Wk
         expanded[bond - 1] = Wk.dim(2)
         log_bond(hledger, bl, bond, "left", expanded[bond - 1])
@@ -295,6 +350,7 @@ def half_right(psiR, right_frames, expanded, nn, acc, hledger, cx: Ctx):
     rch = right_boundary(total_charge(psiR))
     rroot = rch
     carry = None
+    kcar = [None] * len(cx.keep_states)  # each kept state's carry (link, b_j)
     for bond in range(L - 1, root - 1, -1):
         carried = psiR[bond + 1] if carry is None else B.contract(psiR[bond + 1], (2,), carry, (0,))
         fr = frame_from(psiR[bond], carried)
@@ -314,6 +370,11 @@ def half_right(psiR, right_frames, expanded, nn, acc, hledger, cx: Ctx):
                                workcap=cap_at(cx.wcap, bond), recurrence=cx.recurrence,
                                fixed_depth=cx.expansion.krylov_fixed_depth)
         record_krylov(bl, st, cx.alloc)
+        if cx.keep_states:
+            kx = [k[bond + 1] if c is None else B.contract(k[bond + 1], (2,), c, (0,))
+                  for k, c in zip(cx.keep_states, kcar)]
+            Zk = union_kept(Zk, kx, "right", cx, bond)
+            kcar = [B.contract(x, (1, 2), Zk, (1, 2), conjb=True) for x in kx]
         right_frames[bond] = Zk
         if bond != root:
             expanded[bond - 1] = Zk.dim(0)
@@ -965,8 +1026,8 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
-    if len(keep_states) or frames_only or frames_report is not None:
-        raise NotImplementedError("keep_states, frames_only and frames_report are not restated")
+    if frames_only or frames_report is not None:
+        raise NotImplementedError("frames_only and frames_report are not restated")
     return root_link, tol_expv
 
 
@@ -1032,8 +1093,9 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     nR = [0] * (L - 1)
     accL, accR = HalfAcc(), HalfAcc()
     run_parallel = parallel is True or parallel == "half_sweeps"
+    ktols = tuple(float(t) for t in keep_tols) if len(keep_tols) else (0.0,) * len(keep_states)
     cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel,
-             bool(exact), fold)
+             bool(exact), fold, tuple(keep_states), ktols, work_ceiling_rule == "bond")
     # parallel = true: the right half-sweep's stream is forked off the step's before either half
     # runs (bug_step.jl:222-268)
     cxR = replace(cx, rng=fork_rng(rng)) if run_parallel else cx

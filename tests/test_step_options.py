@@ -36,7 +36,6 @@ BAD = [
     (dict(closure_probe=2), NotImplementedError),
     (dict(keep_tols=[0.1]), ValueError),
     (dict(keep_states="psi", keep_tols=[-1.0]), ValueError),
-    (dict(keep_states="psi"), NotImplementedError),
     (dict(frames_only=True), ValueError),
     (dict(frames_only=True, truncate=False), NotImplementedError),
     (dict(frames_report={}), NotImplementedError),
