@@ -3057,6 +3057,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
       P.keep_tols.push_back(tol);
     }
     P.cap_keep = prm->work_ceiling_rule == 0;
+    require(!prm->frames_only || (!prm->root_report && !prm->truncate),
+            "frames_only needs root_report = nothing, kls = nothing and truncate = false");
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
     P.batch_blocks = prm->batch_blocks > 0 ? prm->batch_blocks : 1;
     require(P.batch_blocks <= 8, "batch_blocks must lie in 1:8");
@@ -3219,7 +3221,19 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
                                           P.root_method, P.root_shift);
     };
     Step::ExpvRep rep;
-    T root_result = solve_root(root_start, rep);
+    // frames_only: the caller solves its own root on these frames, so the start is carried and no
+    // expv report is read (bug_step.jl:381-382)
+    T root_result = prm->frames_only ? root_start : solve_root(root_start, rep);
+    if (prm->frames_out) {
+      // frames_report (bug_step.jl:455-467): new handles owned by the caller, payloads shared
+      auto out = [](const T& t) { return t ? std::make_unique<bug_tensor>(*t).release() : nullptr; };
+      for (int b = 1; b < L; ++b) {
+        prm->frames_out[b - 1] = b <= S.root_link ? out(lf[b]) : nullptr;
+        prm->frames_out[L - 1 + b - 1] = b >= S.root_link ? out(rf[b]) : nullptr;
+      }
+      prm->frames_out[2 * L - 2] = out(lenv_root);
+      prm->frames_out[2 * L - 1] = out(renv_root);
+    }
     // the root report (_report_root!, bug_step_stages.jl:243-390)
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     double r_e_pre = NaN, r_e_root = NaN, r_resid = NaN, r_init = NaN, r_out = NaN, r_outl = NaN,

@@ -54,7 +54,8 @@ class StepParams(ctypes.Structure):
                 ("rng_fork_user", ctypes.c_void_p), ("exact", ctypes.c_int),
                 ("fold_omega", ctypes.c_int), ("n_keep", ctypes.c_int),
                 ("keep_sites", ctypes.POINTER(ctypes.c_void_p)),
-                ("keep_tols", ctypes.POINTER(ctypes.c_double))]
+                ("keep_tols", ctypes.POINTER(ctypes.c_double)), ("frames_only", ctypes.c_int),
+                ("frames_out", ctypes.POINTER(ctypes.c_void_p))]
 
 
 class BondLog(ctypes.Structure):
@@ -216,6 +217,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     E.check(_lib().bug_mps_step(ctx.h, L, arr, ctypes.byref(center), warr, tau.real, tau.imag,
                                 ctypes.byref(p), draw, None, ctypes.byref(info), logs, cap,
                                 ctypes.byref(nlog)))
+    _frames_report(ctx, keep, L)
     return _step_result(psi, ctx, arr, center, info, logs, min(nlog.value, cap), order, eshift,
                         root_report)
 
@@ -300,7 +302,26 @@ def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_
         p.keep_sites = ctypes.cast(sites, ctypes.POINTER(ctypes.c_void_p))
         p.keep_tols = ctypes.cast(ctols, ctypes.POINTER(ctypes.c_double))
         held["keep"] = (sites, ctols, list(keep_states))
+    p.frames_only = int(bool(frames_only))
+    if frames_report is not None:
+        slots = (ctypes.c_void_p * (2 * L))()
+        p.frames_out = ctypes.cast(slots, ctypes.POINTER(ctypes.c_void_p))
+        held["frames"] = (slots, frames_report, float(eshift))
     return p, held
+
+
+def _frames_report(ctx, held, L):
+    """Fills the caller's ``frames_report`` dict from the step's frame handles (the reference's
+    ``KLFrames``, ``bug_step.jl:455-467``): left frames of bonds 1..root, right frames of bonds
+    root..L-1, the root's environments."""
+    if "frames" not in held:
+        return
+    slots, report, eshift = held["frames"]
+    own = [None if not slots[i] else DT(ctx, ctypes.c_void_p(slots[i])) for i in range(2 * L)]
+    left = {b: own[b - 1] for b in range(1, L) if own[b - 1] is not None}
+    right = {b: own[L - 2 + b] for b in range(1, L) if own[L - 2 + b] is not None}
+    report.update(left_frames=left, right_frames=right, root_link=max(left), lenv=own[2 * L - 2],
+                  renv=own[2 * L - 1], eshift=eshift)
 
 
 def _step_result(psi, ctx, arr, center, info, logs, nlog, order, eshift, root_report):

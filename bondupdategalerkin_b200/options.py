@@ -114,8 +114,6 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
         unbuilt.append("frontier_tol / krylov_rank_tol > 0")
     if closure_probe > 0:
         unbuilt.append("closure_probe > 0 (the frontier measurement of order-1 steps)")
-    if frames_only or frames_report is not None:
-        unbuilt.append("frames_only / frames_report")
     if unbuilt:
         raise NotImplementedError("not built: " + "; ".join(unbuilt))
     return tol_expv

@@ -261,6 +261,13 @@ typedef struct {
                                  > 0 admits only its directions carrying more than ~tol of it; under
                                  work_ceiling_rule :bond an admitted state fills a frame only up to
                                  its bond's ceiling */
+  int frames_only;            /* 1: skip the root solve; the state comes back as psi in the frames
+                                 (bug_step.jl:381-382); needs truncate = 0 and no root report */
+  bug_tensor** frames_out;    /* frames_report: NULL, or 2L slots the step fills with new handles
+                                 owned by the caller (bug_step.jl:455-467): [b-1] the left frame of
+                                 bond b for b <= root, [L-2+b] the right frame of bond b for
+                                 b >= root (NULL elsewhere), [2L-2] and [2L-1] the root's left and
+                                 right environments */
 } bug_step_params;
 
 

@@ -21,7 +21,8 @@ TEST INFRASTRUCTURE (see ``oracle/blocks.py``). Restates, in the reference's ord
 Scope: ``mode = :rank_tail`` DD-QR expansion, Lanczos/Arnoldi local Krylov with the sequential
 rule, ``order >= 1`` with the single-pass or checked closure and the folded (sampled) or, with
 ``fold_omega = false``, exact frontier leaks; ``exact = true`` expands by the complete DD-projected
-fused basis. ``keep_states``, ``frames_only`` and the K/L/S schedules raise.
+fused basis, ``keep_states`` are unioned into the frames, ``frames_only`` skips the root solve and
+``frames_report`` (a dict) receives the frames. The K/L/S schedules raise.
 """
 
 from __future__ import annotations
@@ -1026,8 +1027,6 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
-    if frames_only or frames_report is not None:
-        raise NotImplementedError("frames_only and frames_report are not restated")
     return root_link, tol_expv
 
 
@@ -1139,7 +1138,9 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
                       tol=1e-15, reorth=reorth, conv_tol=budget.expv, substeps=0,
                       root_method=root_method, rational_shift=root_shift)
 
-    root_result, rep = solve_with(gen, root_start)
+    # frames_only: the caller solves its own root on these frames, so the start is carried
+    # (bug_step.jl:381-382) and no expv report is read
+    root_result, rep = (root_start, None) if frames_only else solve_with(gen, root_start)
     if root_report is not None:
         rr = report_root(root_report, psi, mpo, left_frames, right_frames, root_link, lenv_root,
                          renv_root, gen, root_start, root_result, solve_with, cx=cx, nrm=nrm,
@@ -1148,10 +1149,15 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
         root_start, root_result = rr["root_start"], rr["root_result"]
         if rr["rep"] is not None:
             rep = rr["rep"]
-    ledger.expv_err = rep[2]
-    ledger.expv_iters = rep[0]
-    if rep[2] > budget.expv * (1 + 1e-8):
-        ledger.unmet_("expv")
+    if rep is not None:
+        ledger.expv_err = rep[2]
+        ledger.expv_iters = rep[0]
+        if rep[2] > budget.expv * (1 + 1e-8):
+            ledger.unmet_("expv")
+    if frames_report is not None:  # the KLFrames the step integrated in (bug_step.jl:455-467)
+        frames_report.update(left_frames=dict(left_frames), right_frames=dict(right_frames),
+                             root_link=root_link, lenv=lenv_root, renv=renv_root,
+                             eshift=float(eshift))
     res = B.svd(root_result, (0,), cutoff=0.0)
     expanded[root_link - 1] = left_frames[root_link].dim(2)
     root_frame_width = right_frames[root_link].dim(0)

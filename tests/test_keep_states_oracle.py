@@ -6,7 +6,8 @@ Each half-sweep unions every kept state's carried site tensor into the new frame
 tolerance it widens the frames no more than that; under ``work_ceiling_rule = :bond`` an admitted
 state fills a frame only up to its bond's work ceiling (``_keep_room``). The cases are those of
 ``test/BUG/TimeEvolution/test_step_keep_states.jl:12-60`` (Heisenberg L = 8, U(1), exact
-selection, order 2).
+selection, order 2), with its ``frames_only`` / ``frames_report`` half: a frames-only step returns
+the state in the frames of the full step.
 """
 
 import numpy as np
@@ -14,6 +15,7 @@ import pytest
 
 from oracle import models as M
 from oracle import step as S
+from tests.gpu_util import fidelity
 
 L = 8
 SETTINGS = dict(order=2, tol_basis=1e-8, tol_trunc=1e-12, maxdim=64, exact=True)
@@ -30,7 +32,7 @@ def chain():
     return mpo, start, kept
 
 
-def _step(chain, capture=None, **kw):
+def _step(chain, **kw):
     mpo, start, _ = chain
     psi = start.copy()
     k = dict(SETTINGS)
@@ -58,32 +60,42 @@ def test_admitted_state_stays_within_the_bond_ceilings(chain):
     assert all(c <= x for c, x in zip(capped, ceilings))
 
 
-def test_exactly_kept_state_lies_in_the_frames(chain, monkeypatch):
-    """The frames the step ends with (after the frontier sweep) contain the kept state: its
-    projection miss on them is round-off."""
+def test_exactly_kept_state_lies_in_the_frames(chain):
+    """The frames the step ends with (``frames_report``, after the frontier sweep) contain the
+    kept state: its projection miss on them is round-off; without the keep they miss it."""
     kept = chain[2]
-    seen = {}
-    half_left, half_right = S.half_left, S.half_right
-
-    def spy_left(psiL, left_frames, *a):
-        seen["left"] = left_frames
-        return half_left(psiL, left_frames, *a)
-
-    def spy_right(psiR, right_frames, *a):
-        seen["right"] = right_frames
-        return half_right(psiR, right_frames, *a)
-
-    monkeypatch.setattr(S, "half_left", spy_left)
-    monkeypatch.setattr(S, "half_right", spy_right)
-    _, psi = _step(chain, keep_states=[kept])
     root = S.bug_root_link(L)
     k = kept.copy()
     S.canonical(k, root)
-    miss = S.projection_miss(k, seen["left"], seen["right"], root)
-    assert miss <= 1e-12 * np.sqrt(S.B.norm(k[k.center]) ** 2)
-    # without the kept state the frames miss it
-    _step(chain)
-    assert S.projection_miss(k, seen["left"], seen["right"], root) > 1e-6
+    nk = S.B.norm(k[k.center])
+    with_keep, without = {}, {}
+    _step(chain, keep_states=[kept], frames_report=with_keep)
+    _step(chain, frames_report=without)
+    assert with_keep["root_link"] == root
+    miss = S.projection_miss(k, with_keep["left_frames"], with_keep["right_frames"], root)
+    assert miss <= 1e-12 * nk
+    assert S.projection_miss(k, without["left_frames"], without["right_frames"], root) > 1e-6 * nk
+
+
+def test_frames_only_returns_the_state_in_the_full_steps_frames(chain):
+    """``frames_only`` skips the root solve: the state comes back as itself in the frames, and the
+    frames are those of the full step (``test_step_keep_states.jl:62-80``)."""
+    mpo, start, _ = chain
+    full, only = {}, {}
+    _step(chain, frames_report=full)
+    psi = start.copy()
+    info = S.cbe_bug_step(psi, mpo, -0.2j, truncate=False, frames_only=True, frames_report=only,
+                          **SETTINGS)
+    assert 1.0 - fidelity(psi, start) < 1e-12
+    assert info["ledger"].expv_iters == 0
+    widths = {b: f.dim(2) for b, f in only["left_frames"].items()}
+    assert widths == {b: f.dim(2) for b, f in full["left_frames"].items()}
+
+
+def test_frames_only_with_a_truncation_is_refused(chain):
+    mpo, start, _ = chain
+    with pytest.raises(ValueError, match="frames_only"):
+        S.cbe_bug_step(start.copy(), mpo, -0.2j, frames_only=True, **SETTINGS)
 
 
 def test_two_kept_states_and_their_tolerances(chain):

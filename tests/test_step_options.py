@@ -37,8 +37,6 @@ BAD = [
     (dict(keep_tols=[0.1]), ValueError),
     (dict(keep_states="psi", keep_tols=[-1.0]), ValueError),
     (dict(frames_only=True), ValueError),
-    (dict(frames_only=True, truncate=False), NotImplementedError),
-    (dict(frames_report={}), NotImplementedError),
     (dict(order=2, fold_omega=False, outside_residual=True, root_report={}), NotImplementedError),
     (dict(exact=True, order=2, outside_residual=True, root_report={}), NotImplementedError),
     (dict(kls="foo"), ValueError),
