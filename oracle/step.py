@@ -148,12 +148,31 @@ def extend_frame(frame, residual, direction, side, weight, allowance, room):
     return B.oplus([frame, nb], fl), nb.dim(fl), fits
 
 
+def append_ranked(frame, cands, side, allowance, workcap):
+    """``_append_ranked`` (``krylov_enrichment.jl:186-195``): one SVD of the collected weighted
+    residuals' direct sum ranks their local directions, and the fewest top ones whose discarded
+    tail fits ``allowance`` join the frame; ``fits = False`` when the work ceiling cut more."""
+    if not cands:
+        return frame, 0, True
+    fl = 2 if side == "left" else 0
+    room = workcap - frame.dim(fl) if workcap > 0 else 1 << 62
+    block = cands[0] if len(cands) == 1 else B.oplus(cands, fl)
+    if room <= 0:
+        return frame, 0, B.norm(block) <= allowance
+    return extend_frame(frame, block, block, side, 1.0, allowance, room)
+
+
 def krylov_enrich(seed, applyH, start_frame, side, tau, alloc, workcap=0, amp=1.0,
                   state_seed=True, recurrence="arnoldi", fixed_depth=0):
+    """``_krylov_enrich`` (``krylov_enrichment.jl:213-292``): Tests C/D on each Krylov direction,
+    appending in chain order, or with ``alloc.krylov_rank > 0`` collecting every direction above
+    the allowance against the start frame and ranking them at the end (:func:`append_ranked`)."""
     perp = perp_left if side == "left" else perp_right
     fl = 2 if side == "left" else 0
     allow = alloc.krylov
-    st = dict(frame=start_frame, eta_c=0.0, eta_d=0.0, added=0, added_d=0)
+    ranked = alloc.krylov_rank > 0
+    cands = []
+    st = dict(frame=start_frame, eta_c=0.0, eta_d=0.0, added=0, added_d=0, nd=0)
 
     def score(direction, weight, first):
         residual = perp(st["frame"], direction)
@@ -163,6 +182,11 @@ def krylov_enrich(seed, applyH, start_frame, side, tau, alloc, workcap=0, amp=1.
         else:
             st["eta_d"] = max(st["eta_d"], eta)
         if not eta > allow:
+            return True
+        if ranked:  # the frame stays the start frame: every candidate against the same frame
+            cands.append(B.scale(residual, weight))
+            if not first:
+                st["nd"] += 1
             return True
         room = workcap - st["frame"].dim(fl) if workcap > 0 else 1 << 62
         if room <= 0:
@@ -177,6 +201,11 @@ def krylov_enrich(seed, applyH, start_frame, side, tau, alloc, workcap=0, amp=1.
     kb = K.krylov_basis(VOPS, seed, applyH, tau, alloc.krylov, score, amp=amp,
                         state_seed=state_seed, recurrence=recurrence, fixed_depth=fixed_depth)
     capped = kb["capped"]
+    if ranked:
+        st["frame"], st["added"], fits = append_ranked(start_frame, cands, side,
+                                                       alloc.krylov_rank, workcap)
+        st["added_d"] = st["added"] if st["nd"] > 0 else 0
+        capped = capped or not fits
     stats = dict(eta_c=st["eta_c"], eta_d=st["eta_d"], added=st["added"], n_h1=kb["n_h1"],
                  d_after_c=st["eta_c"] <= alloc.krylov and st["added_d"] > 0, capped=capped,
                  met=kb["closed"] and not capped)
@@ -1023,8 +1052,8 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("the parallel K/L/S step (parallel = :full, kls) is not restated")
     if work_ceiling_rule not in ("maxdim", "bond"):
         raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
-    if frontier_tol > 0 or krylov_rank_tol > 0:
-        raise NotImplementedError("frontier_tol / krylov_rank_tol > 0 are not restated")
+    if frontier_tol > 0:
+        raise NotImplementedError("frontier_tol > 0 is not restated")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
     return root_link, tol_expv
