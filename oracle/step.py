@@ -22,7 +22,9 @@ Scope: ``mode = :rank_tail`` DD-QR expansion, Lanczos/Arnoldi local Krylov with 
 rule, ``order >= 1`` with the single-pass or checked closure and the folded (sampled) or, with
 ``fold_omega = false``, exact frontier leaks; ``exact = true`` expands by the complete DD-projected
 fused basis, ``keep_states`` are unioned into the frames, ``frames_only`` skips the root solve and
-``frames_report`` (a dict) receives the frames. The K/L/S schedules raise.
+``frames_report`` (a dict) receives the frames, ``krylov_rank_tol`` ranks the local Krylov
+directions and ``frontier_tol`` compresses each frontier before its sweep. The K/L/S schedules
+raise.
 """
 
 from __future__ import annotations
@@ -248,6 +250,7 @@ class Ctx:
     keep_states: tuple = ()  # MPS the frames must contain (keep_states)
     keep_tols: tuple = ()  # per kept state: 0 contained exactly, > 0 admitted at that tolerance
     cap_keep: bool = False  # work_ceiling_rule = :bond: admitted states fill frames to the ceiling
+    frontier_tol: float = 0.0  # > 0: each frontier compressed to its own rank before its sweep
 
 
 def fork_rng(rng):
@@ -641,6 +644,14 @@ def frontier_sweep(fr: KLFrames, psi, mpo, core, degree, cx: Ctx, nrm, enrich=Tr
     if nF <= FRONTIER_FLOOR * max(nrm, K.np.finfo(float).eps):
         return dict(added=0, leak=0.0, met=True, capped=False, ledger=Ledger())
     Fm = frontier_mps(psi, fr, core)
+    if cx.frontier_tol > 0:
+        # frontier_tol > 0 (frontier_closure.jl:102-120): the frontier, written in the frames with
+        # frame-wide bonds, is compressed to its own rank at that weight tolerance (no rank cap:
+        # the widest frame); its Schmidt vectors stay in the frames' span
+        L = len(Fm)
+        width = max(max(fr.left_frames[b].dim(2) for b in range(1, fr.root_link + 1)),
+                    max(fr.right_frames[b].dim(0) for b in range(fr.root_link, L)))
+        truncate_recursive(Fm, fr.root_link, width, cx.frontier_tol, [0.0] * (L - 1))
     FmR = Fm.copy()
     gen = fr.gen + 1
     amp = nF / max(nrm, np.finfo(float).eps)
@@ -1052,8 +1063,6 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("the parallel K/L/S step (parallel = :full, kls) is not restated")
     if work_ceiling_rule not in ("maxdim", "bond"):
         raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
-    if frontier_tol > 0:
-        raise NotImplementedError("frontier_tol > 0 is not restated")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
     return root_link, tol_expv
@@ -1123,7 +1132,8 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     run_parallel = parallel is True or parallel == "half_sweeps"
     ktols = tuple(float(t) for t in keep_tols) if len(keep_tols) else (0.0,) * len(keep_states)
     cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel,
-             bool(exact), fold, tuple(keep_states), ktols, work_ceiling_rule == "bond")
+             bool(exact), fold, tuple(keep_states), ktols, work_ceiling_rule == "bond",
+             float(frontier_tol))
     # parallel = true: the right half-sweep's stream is forked off the step's before either half
     # runs (bug_step.jl:222-268)
     cxR = replace(cx, rng=fork_rng(rng)) if run_parallel else cx

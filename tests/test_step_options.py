@@ -23,7 +23,6 @@ BAD = [
     (dict(tol_root=1e-6, tol_expv=1e-6), ValueError),
     (dict(order=0), ValueError),
     (dict(frontier_tol=-1.0), ValueError),
-    (dict(frontier_tol=1e-3), NotImplementedError),
     (dict(work_ceiling_rule="foo"), ValueError),
     (dict(work_ceiling_rule="bond_strict"), NotImplementedError),
     (dict(work_ceiling_rule="frame_root"), NotImplementedError),
@@ -71,7 +70,7 @@ def test_hosts_refuse_as_the_reference_does(kw, exc):
 
 
 # restated in the oracle ahead of the device step: the product names them as not built
-ORACLE_AHEAD = [dict(krylov_rank_tol=0.1)]
+ORACLE_AHEAD = [dict(krylov_rank_tol=0.1), dict(frontier_tol=1e-3)]
 
 
 @pytest.mark.parametrize("kw", ORACLE_AHEAD, ids=[repr(k) for k in ORACLE_AHEAD])
