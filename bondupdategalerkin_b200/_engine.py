@@ -87,6 +87,10 @@ SIGNATURES = {
     "bug_oplus": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
     "bug_trim": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _c_int_p, ctypes.POINTER(_vp)]),
     "bug_la_expm": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p]),
+    "bug_work_ceilings": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.c_int64, ctypes.c_int64, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_double,
+                                         ctypes.POINTER(ctypes.c_int64)]),
     "bug_la_eigh": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p]),
     "bug_la_eigh_tridiag": (ctypes.c_int, [ctypes.c_int, _c_double_p, _c_double_p, _c_double_p,
                                            _c_double_p]),

@@ -962,6 +962,44 @@ struct MPOv {
 
 // ── the step ────────────────────────────────────────────────────────────────────────────────
 
+// Per-bond work ceilings from the bonds before the step (basis_budget.jl:454-555): rule 0 :bond
+// (ceil(f d D_b), 2 d D_b at f = 0), 1 :maxdim (one ceiling d max(maxdim, max D_b)),
+// 2 :bond_strict (ceil(f D_b), f > 1), 3 :frame_root (ceil(f D_b), f = 2 at 0, and
+// ceil(root_factor D_root) at the root bond); each within [1, maxdim] except :maxdim's. `factor`
+// < 0 is the keyword's default (1.2 under :bond, 0 otherwise), `root_factor` <= 0 is 1.2. Products
+// are rounded to nine decimals before the ceiling, as the reference rounds them.
+std::vector<int64_t> work_ceilings(int rule, const std::vector<int64_t>& bonds, int64_t dloc,
+                                   int64_t maxdim, double factor, int root_link, double root_factor) {
+  require(rule >= 0 && rule <= 3, "work_ceiling_rule must be 0 (:bond), 1 (:maxdim), 2 (:bond_strict) or 3 (:frame_root)");
+  if (factor < 0) factor = rule == 0 ? 1.2 : 0.0;
+  require(factor == 0 || (factor > 1 && rule != 1),
+          "bond_ceiling_factor must be 0, or > 1 with work_ceiling_rule = bond");
+  auto ceil9 = [](double x) { return int64_t(std::ceil(std::round(x * 1e9) / 1e9)); };
+  std::vector<int64_t> w;
+  if (rule == 1) {
+    const int64_t mx = bonds.empty() ? 0 : *std::max_element(bonds.begin(), bonds.end());
+    w.assign(bonds.size(), std::max<int64_t>({dloc * maxdim, dloc * mx, 1}));
+    return w;
+  }
+  if (rule == 2) require(factor > 1, "strict bond factor must exceed 1");
+  if (rule == 3) {
+    if (factor == 0) factor = 2.0;
+    if (root_factor <= 0) root_factor = 1.2;
+    require(root_factor > 1, "root_ceiling_factor must exceed one");
+    require(root_factor <= factor, "root_ceiling_factor must not exceed the frame factor");
+    require(root_link >= 1 && root_link <= int(bonds.size()), "root bond outside the chain");
+  }
+  for (size_t b = 0; b < bonds.size(); ++b) {
+    const int64_t r = bonds[b];
+    int64_t c;
+    if (rule == 0) c = factor > 0 ? ceil9(factor * double(dloc) * double(r)) : 2 * dloc * r;
+    else if (rule == 2) c = ceil9(factor * double(r));
+    else c = ceil9((int(b) + 1 == root_link ? root_factor : factor) * double(r));
+    w.push_back(std::max<int64_t>(std::min<int64_t>(c, maxdim), 1));
+  }
+  return w;
+}
+
 struct Params {
   double tol_basis, tol_trunc, tol_expv, tol_krylov;
   int order, maxdim, hermitian, rule_maxdim, root, reorth, truncate, root_maxiter, fixed_width;
@@ -3056,7 +3094,7 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
       require(tol >= 0, "keep_tols must be >= 0");
       P.keep_tols.push_back(tol);
     }
-    P.cap_keep = prm->work_ceiling_rule == 0;
+    P.cap_keep = prm->work_ceiling_rule != 1;  // :bond, :bond_strict and :frame_root
     require(!prm->frames_only || (!prm->root_report && !prm->truncate),
             "frames_only needs root_report = nothing, kls = nothing and truncate = false");
     P.holdout_width = prm->holdout_width > 0 ? prm->holdout_width : DD_HOLDOUT;
@@ -3099,25 +3137,8 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     std::vector<int64_t> bd0 = psi.bond_dims();
     int64_t dloc = 1;
     for (int s = 1; s <= L; ++s) dloc = std::max<int64_t>(dloc, dim(psi[s], 1));
-    double factor = P.bond_ceiling_factor;
-    if (factor < 0) factor = P.rule_maxdim ? 0.0 : 1.2;
-    require(factor == 0 || (factor > 1 && !P.rule_maxdim),
-            "bond_ceiling_factor must be 0, or > 1 with work_ceiling_rule = bond");
-    if (P.rule_maxdim) {
-      const int64_t mx = bd0.empty() ? 0 : *std::max_element(bd0.begin(), bd0.end());
-      S.wcap.assign(L - 1, std::max<int64_t>({dloc * P.maxdim, dloc * mx, 1}));
-    } else {
-      for (int64_t r : bd0) {
-        int64_t ceil_r;
-        if (factor > 0) {
-          const double x = factor * double(dloc) * double(r);
-          ceil_r = int64_t(std::ceil(std::round(x * 1e9) / 1e9));
-        } else {
-          ceil_r = 2 * dloc * r;
-        }
-        S.wcap.push_back(std::max<int64_t>(std::min<int64_t>(ceil_r, P.maxdim), 1));
-      }
-    }
+    S.wcap = work_ceilings(prm->work_ceiling_rule, bd0, dloc, P.maxdim, P.bond_ceiling_factor,
+                           S.root_link, prm->root_ceiling_factor);
     const double nrm = (psi.center >= 1 && psi.center <= L) ? e.norm(psi[psi.center]) : 1.0;
     S.alloc = basis_allocation(P.tol_basis, L - 1, tau, nrm, P.order, P.tol_krylov, 0.0);
     Ledger ledger;
@@ -3730,6 +3751,17 @@ extern "C" int bug_apply_two_site(bug_ctx* c, const bug_tensor* lenv, const bug_
     Eng e{c, nullptr, nullptr};
     Env env{e};
     *out = hand_out(env.two_site(borrow(lenv), borrow(Wl), borrow(Wr), borrow(renv), borrow(theta)));
+  });
+}
+
+extern "C" int bug_work_ceilings(int rule, int nbonds, const int64_t* bonds, int64_t site_dim,
+                                 int64_t maxdim, double factor, int root_link, double root_factor,
+                                 int64_t* out) {
+  return guard([&] {
+    require(nbonds >= 0 && (nbonds == 0 || (bonds && out)), "bad arguments");
+    std::vector<int64_t> b(bonds, bonds + nbonds);
+    const std::vector<int64_t> w = work_ceilings(rule, b, site_dim, maxdim, factor, root_link, root_factor);
+    std::copy(w.begin(), w.end(), out);
   });
 }
 

@@ -55,6 +55,7 @@ class StepParams(ctypes.Structure):
                 ("fold_omega", ctypes.c_int), ("n_keep", ctypes.c_int),
                 ("keep_sites", ctypes.POINTER(ctypes.c_void_p)),
                 ("keep_tols", ctypes.POINTER(ctypes.c_double)), ("frames_only", ctypes.c_int),
+                ("root_ceiling_factor", ctypes.c_double),
                 ("frames_out", ctypes.POINTER(ctypes.c_void_p))]
 
 
@@ -120,17 +121,18 @@ def _lib():
 
 def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=None, order=1,
                 maxdim=None, hermitian=True, expansion=None, root=None, reorth=True, truncate=True,
-                work_ceiling_rule="bond", bond_ceiling_factor=None, root_maxiter=30,
-                krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None, closure_checks=False,
-                exact=False):
+                work_ceiling_rule="bond", bond_ceiling_factor=None, root_ceiling_factor=1.2,
+                root_maxiter=30, krylov_rank_tol=0.0, frontier_tol=0.0, fold_omega=None,
+                closure_checks=False, exact=False):
     """The keyword arguments of ``cbe_bug_step!`` as the C-ABI's ``bug_step_params`` (checked the
     way the reference checks them, ``bug_step_stages.jl:15-142``)."""
     if L < 2:
         raise ValueError("cbe_bug_step needs at least two sites")
     if L - 1 > MAX_SITES:
         raise ValueError(f"at most {MAX_SITES + 1} sites")
-    if work_ceiling_rule not in ("bond", "maxdim"):
-        raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r}")
+    rules = {"bond": 0, "maxdim": 1, "bond_strict": 2, "frame_root": 3}
+    if work_ceiling_rule not in rules:
+        raise ValueError(f"work_ceiling_rule {work_ceiling_rule!r}")
     if frontier_tol or krylov_rank_tol:
         raise NotImplementedError("frontier_tol / krylov_rank_tol > 0")
     mode, width, tail_factor, kmode, fixed_depth = "rank_tail", 8, 0.10, "auto", 0
@@ -158,7 +160,7 @@ def step_params(L, *, tol_basis=None, tol_trunc=None, tol_expv=None, tol_krylov=
         tol_basis=tol_basis or 0.0, tol_trunc=-1.0 if tol_trunc is None else tol_trunc,
         tol_expv=tol_expv or 0.0, tol_krylov=tol_krylov or 0.0, order=order,
         maxdim=maxdim or 0, hermitian=int(hermitian),
-        work_ceiling_rule=1 if work_ceiling_rule == "maxdim" else 0,
+        work_ceiling_rule=rules[work_ceiling_rule], root_ceiling_factor=float(root_ceiling_factor),
         bond_ceiling_factor=-1.0 if bond_ceiling_factor is None else float(bond_ceiling_factor),
         root=root or 0, reorth=int(reorth), truncate=int(truncate), root_maxiter=root_maxiter,
         fixed_width=width, tail_factor=tail_factor,
@@ -247,6 +249,7 @@ def _step_setup(psi, mpo, rng, *, tol_basis, tol_trunc, tol_expv, tol_root, tol_
                     tol_krylov=tol_krylov, order=order, maxdim=maxdim, hermitian=hermitian,
                     expansion=expansion, root=root, reorth=reorth, truncate=truncate,
                     work_ceiling_rule=work_ceiling_rule, bond_ceiling_factor=bond_ceiling_factor,
+                    root_ceiling_factor=root_ceiling_factor,
                     root_maxiter=root_maxiter, krylov_rank_tol=krylov_rank_tol,
                     frontier_tol=frontier_tol, fold_omega=fold_omega, closure_checks=closure_checks,
                     exact=exact)

@@ -35,7 +35,7 @@ class DDQRExpansion:
 
 KLS_SCHEDULES = ("sequential", "kl_then_s", "concurrent")  # parallel_kls.jl:7
 WORK_CEILING_RULES = ("maxdim", "bond", "bond_strict", "frame_root")
-BUILT_WORK_CEILING_RULES = ("maxdim", "bond")
+BUILT_WORK_CEILING_RULES = ("maxdim", "bond", "bond_strict", "frame_root")
 
 
 def _parallel_mode(parallel):
@@ -104,6 +104,10 @@ def check_step_options(L, mpo_len, *, root=None, parallel=False, kls=None, tol_e
         if outside_residual:
             raise ValueError("the parallel K/L/S step does not combine with the outside-residual "
                              "re-enrichment")
+    # bond_work_ceilings_strict refuses a factor of at most one (basis_budget.jl:506), which the
+    # step's default factor 0 under :bond_strict is
+    if work_ceiling_rule == "bond_strict" and not bond_ceiling_factor > 1:
+        raise ValueError("strict bond factor must exceed 1")
     # valid, but not built here
     unbuilt = []
     if kls is not None:

@@ -208,7 +208,7 @@ typedef struct {
   int order;                  /* temporal order p >= 1 */
   int maxdim;                 /* <= 0: 128 */
   int hermitian;              /* 1: Lanczos root solve, 0: Arnoldi */
-  int work_ceiling_rule;      /* 0: :bond, 1: :maxdim */
+  int work_ceiling_rule;      /* 0: :bond, 1: :maxdim, 2: :bond_strict, 3: :frame_root */
   double bond_ceiling_factor; /* < 0: 1.2 under :bond, 0 under :maxdim */
   int root;                   /* root link; <= 0: L/2 */
   int reorth;                 /* re-orthogonalise the root Lanczos basis */
@@ -263,6 +263,7 @@ typedef struct {
                                  its bond's ceiling */
   int frames_only;            /* 1: skip the root solve; the state comes back as psi in the frames
                                  (bug_step.jl:381-382); needs truncate = 0 and no root report */
+  double root_ceiling_factor; /* :frame_root's root-bond factor, in (1, frame factor]; <= 0: 1.2 */
   bug_tensor** frames_out;    /* frames_report: NULL, or 2L slots the step fills with new handles
                                  owned by the caller (bug_step.jl:455-467): [b-1] the left frame of
                                  bond b for b <= root, [L-2+b] the right frame of bond b for
@@ -502,6 +503,13 @@ int bug_batch_destroy(bug_batch* b);
 /* exp(A) for a complex n x n row-major matrix (Pade-13 scaling and squaring); replaces Julia's
  * matrix `exp` in _kry_weight/_hess_coeffs (krylov_enrichment.jl:89-120, root_methods.jl:136-141). */
 int bug_la_expm(int n, const double* a, double* out);
+/* The step's per-bond work ceilings from the bond dimensions before it (bond_work_ceilings,
+ * bond_work_ceilings_strict, bond_frame_root_ceilings, work_ceiling; basis_budget.jl:454-555):
+ * rule 0 :bond, 1 :maxdim, 2 :bond_strict, 3 :frame_root; factor < 0 is bond_ceiling_factor's
+ * default, root_factor <= 0 is root_ceiling_factor's (1.2); root_link is the root bond (1-based).
+ * Writes nbonds ceilings to out; BUG_EINVAL with the reference's reason for a refused factor. */
+int bug_work_ceilings(int rule, int nbonds, const int64_t* bonds, int64_t site_dim, int64_t maxdim,
+                      double factor, int root_link, double root_factor, int64_t* out);
 /* Eigen-decomposition of a real symmetric n x n matrix (cyclic Jacobi): ascending eigenvalues and
  * eigenvectors as columns (row-major n x n). */
 int bug_la_eigh(int n, const double* a, double* vals, double* vecs);

@@ -196,6 +196,32 @@ def bond_work_ceilings(bond_ranks, site_dim: int, maxdim: int, factor: float = 0
     return [max(min(ceiling_of(r), maxdim), 1) for r in bond_ranks]
 
 
+def bond_work_ceilings_strict(bond_ranks, maxdim: int, factor: float = 1.2):
+    """``bond_work_ceilings_strict`` (``basis_budget.jl:497-508``): ``ceil(f D_b)`` per bond,
+    without the local dimension."""
+    if not factor > 1:
+        raise ValueError("strict bond factor must exceed 1")
+    return [max(1, min(maxdim, _ceil9(factor * r))) for r in bond_ranks]
+
+
+def bond_frame_root_ceilings(old_bonds, maxdim: int, root_bond: int, frame_factor: float = 2.0,
+                             root_factor: float = 1.2):
+    """``bond_frame_root_ceilings`` (``basis_budget.jl:511-545``): ``ceil(frame_factor D_b)``
+    away from the root bond, ``ceil(root_factor D_root)`` at it."""
+    if not 1 <= root_bond <= len(old_bonds):
+        raise ValueError(f"root bond {root_bond} outside 1:{len(old_bonds)}")
+    if not frame_factor > 1:
+        raise ValueError("frame_factor must exceed 1")
+    if not root_factor > 1:
+        raise ValueError("root_factor must exceed 1")
+    if root_factor > frame_factor:
+        raise ValueError("root_factor cannot exceed frame_factor")
+    if maxdim < 1:
+        raise ValueError("maxdim must be positive")
+    return [max(1, min(maxdim, _ceil9((root_factor if b + 1 == root_bond else frame_factor) * r)))
+            for b, r in enumerate(old_bonds)]
+
+
 def tail_rank(lst, scale: float, allowance: float, kmax: int, base: float = 0.0):
     """Test A: the smallest ``keep <= kmax`` whose scaled tail fits ``allowance``
     (``truncation.jl:262-278``)."""

@@ -38,8 +38,8 @@ import numpy as np
 from . import blocks as B
 from . import krylov as K
 from .budget import (DEFAULT_BOND_CEILING_FACTOR, TOL_DEFAULTS, Budget, Ledger,
-                     basis_allocation, bond_work_ceilings, indicator, log_bond, tail_rank,
-                     work_ceiling)
+                     basis_allocation, bond_frame_root_ceilings, bond_work_ceilings,
+                     bond_work_ceilings_strict, indicator, log_bond, tail_rank, work_ceiling)
 from .cbe import (CBE_EPS, BondFrame, cap_to_local_room, dd_cbe_expand, exact_leak,
                   folded_closures, perp_left, perp_right, rank_cut, reortho, rows_from_u,
                   sampled_leak)
@@ -1061,8 +1061,8 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
                          "re-enrichment")
     if kls is not None:
         raise NotImplementedError("the parallel K/L/S step (parallel = :full, kls) is not restated")
-    if work_ceiling_rule not in ("maxdim", "bond"):
-        raise NotImplementedError(f"work_ceiling_rule {work_ceiling_rule!r} is not restated")
+    if work_ceiling_rule == "bond_strict" and not bond_ceiling_factor > 1:
+        raise ValueError("strict bond factor must exceed 1")
     if closure_probe > 0:
         raise NotImplementedError("closure_probe > 0 is not restated")
     return root_link, tol_expv
@@ -1104,8 +1104,15 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     eshift = float(eshift)
     maxdim = 128 if maxdim is None else maxdim
     bond_ranks = psi.bond_dims()
+    # the work ceilings from the bonds before the step (bug_step_stages.jl:114-129)
     if work_ceiling_rule == "bond":
         wcap = bond_work_ceilings(bond_ranks, local_dim(psi), maxdim, factor=bond_ceiling_factor)
+    elif work_ceiling_rule == "bond_strict":
+        wcap = bond_work_ceilings_strict(bond_ranks, maxdim, factor=bond_ceiling_factor)
+    elif work_ceiling_rule == "frame_root":
+        wcap = bond_frame_root_ceilings(
+            bond_ranks, maxdim, root_link, root_factor=root_ceiling_factor,
+            frame_factor=2.0 if bond_ceiling_factor == 0 else bond_ceiling_factor)
     else:
         wcap = work_ceiling(maxdim, max(bond_ranks, default=0), local_dim(psi))
     expansion = DDQRExpansion() if expansion is None else expansion
@@ -1132,7 +1139,7 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
     run_parallel = parallel is True or parallel == "half_sweeps"
     ktols = tuple(float(t) for t in keep_tols) if len(keep_tols) else (0.0,) * len(keep_states)
     cx = Ctx(mpo, tau, root_link, alloc, expansion, recurrence, wcap, rng, eshift, run_parallel,
-             bool(exact), fold, tuple(keep_states), ktols, work_ceiling_rule == "bond",
+             bool(exact), fold, tuple(keep_states), ktols, work_ceiling_rule != "maxdim",
              float(frontier_tol))
     # parallel = true: the right half-sweep's stream is forked off the step's before either half
     # runs (bug_step.jl:222-268)

@@ -24,8 +24,8 @@ BAD = [
     (dict(order=0), ValueError),
     (dict(frontier_tol=-1.0), ValueError),
     (dict(work_ceiling_rule="foo"), ValueError),
-    (dict(work_ceiling_rule="bond_strict"), NotImplementedError),
-    (dict(work_ceiling_rule="frame_root"), NotImplementedError),
+    (dict(work_ceiling_rule="bond_strict"), ValueError),  # its default factor 0 is no strict factor
+    (dict(work_ceiling_rule="bond_strict", bond_ceiling_factor=1.0), ValueError),
     (dict(bond_ceiling_factor=0.5), ValueError),
     (dict(bond_ceiling_factor=1.5, work_ceiling_rule="maxdim"), ValueError),
     (dict(root_ceiling_factor=1.0), ValueError),
