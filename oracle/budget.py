@@ -107,6 +107,10 @@ class Ledger:
     leak: list = field(default_factory=list)
     defect: float = 0.0
     n_root_frontier: int = 0
+    # the frontiers measured on the half-sweeps' frames before any closure enrichment
+    # (basis_budget.jl:219-225): time-weighted leaks and scale-free ||(I - P) A F_j|| / ||F_j||
+    leak_initial: list = field(default_factory=list)
+    rho_initial: list = field(default_factory=list)
     n_h2_leak: int = 0
     n_h1_closure: int = 0
     closure_log: list = field(default_factory=list)
@@ -158,6 +162,8 @@ class Ledger:
         self.leak += o.leak
         self.defect = max(self.defect, o.defect)
         self.n_root_frontier += o.n_root_frontier
+        self.leak_initial += o.leak_initial
+        self.rho_initial += o.rho_initial
         self.n_h2_leak += o.n_h2_leak
         self.n_h1_closure += o.n_h1_closure
         self.closure_log += o.closure_log

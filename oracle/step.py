@@ -29,6 +29,7 @@ raise.
 
 from __future__ import annotations
 
+import copy
 import math
 import time
 from dataclasses import dataclass, replace
@@ -749,6 +750,40 @@ def closure_loop(frontier, sweep, order, maxpass, include_zero=False):
     return dict(passes=maxpass, converged=False, exhausted=True, capped=False)
 
 
+def measure_frontiers(fr: KLFrames, psi, mpo, root_start, cx: Ctx, count, nrm):
+    """``_measure_frontiers`` (``frontier_closure.jl:289-359``, serial): frontiers 0..count-1 of
+    the root generator, each swept without enrichment on the frames as they stand; their leaks
+    and scale-free ``||(I - P) A F_j|| / ||F_j||`` go to the ledger's ``leak_initial`` /
+    ``rho_initial``. The frames are not touched."""
+    state = dict(nroot=0)
+    op = root_generator(mpo, fr)
+
+    def applyB(v):
+        state["nroot"] += 1
+        return op.apply(v)
+
+    cores = [root_start]
+    if count > 1:
+        cores += projected_frontiers(applyB, root_start, cx.tau, count - 1)
+    lg = Ledger()
+    leak, rho, met, met0 = [0.0] * count, [0.0] * count, True, True
+    for d, core in enumerate(cores):
+        sw = frontier_sweep(fr, psi, mpo, core, d, cx, nrm, enrich=False)
+        lg.merge(sw["ledger"])
+        nF = B.norm(core)
+        raw = math.sqrt(sum(x * x for x in sw.get("leaks_left", ())) +
+                        sum(x * x for x in sw.get("leaks_right", ())))
+        leak[d] = sw["leak"]
+        rho[d] = raw / nF if nF > 0 else 0.0
+        if d >= 1:
+            met &= sw["met"]
+        else:
+            met0 = sw["met"]
+    lg.leak_initial, lg.rho_initial = leak, rho
+    lg.n_root_frontier = state["nroot"]
+    return dict(leak=leak, rho=rho, met=met, met0=met0, ledger=lg, n_root=state["nroot"])
+
+
 def checked_closure(fr: KLFrames, psi, mpo, root_start, cx: Ctx, order, nrm, ledger):
     """``_krylov_closure!`` with ``checks = true`` (``krylov_closure_loop.jl:18-194``, serial,
     ``include_zero = false``): measure every frontier on the incoming frames first
@@ -1063,8 +1098,6 @@ def step_options(L, mpo_len, root, parallel, kls, tol_expv, tol_root, order, wor
         raise NotImplementedError("the parallel K/L/S step (parallel = :full, kls) is not restated")
     if work_ceiling_rule == "bond_strict" and not bond_ceiling_factor > 1:
         raise ValueError("strict bond factor must exceed 1")
-    if closure_probe > 0:
-        raise NotImplementedError("closure_probe > 0 is not restated")
     return root_link, tol_expv
 
 
@@ -1166,6 +1199,12 @@ def cbe_bug_step(psi, mpo, tau, *, tol_basis=None, tol_trunc=None, tol_expv=None
             expanded[b - 1] = right_frames[b].dim(0)
         lenv_root, renv_root, root_start = fr.lenv, fr.renv, cl["root_start"]
         nclose = cl["n_h1"] + cl["n_root"]
+    elif closure_probe > 0:
+        # a measurement only (bug_step_stages.jl:221-236): a copied generator and untouched
+        # frames, so the step itself stays bit-identical
+        probe = measure_frontiers(fr, psi, mpo, root_start, replace(cx, rng=copy.deepcopy(rng)),
+                                  closure_probe, nrm)
+        ledger.merge(probe["ledger"])
     npsi = B.norm(psi[psi.center])
     ledger.r_aug = max(max(expanded, default=0), right_frames[root_link].dim(0))
     ledger.proj_err = projection_miss(psi, left_frames, right_frames, root_link) / npsi if npsi > 0 else 0.0

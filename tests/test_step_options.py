@@ -32,7 +32,6 @@ BAD = [
     (dict(work_ceiling_rule="frame_root", bond_ceiling_factor=1.5, root_ceiling_factor=1.8),
      ValueError),
     (dict(closure_probe=-1), ValueError),
-    (dict(closure_probe=2), NotImplementedError),
     (dict(keep_tols=[0.1]), ValueError),
     (dict(keep_states="psi", keep_tols=[-1.0]), ValueError),
     (dict(frames_only=True), ValueError),
@@ -70,7 +69,7 @@ def test_hosts_refuse_as_the_reference_does(kw, exc):
 
 
 # restated in the oracle ahead of the device step: the product names them as not built
-ORACLE_AHEAD = [dict(krylov_rank_tol=0.1), dict(frontier_tol=1e-3)]
+ORACLE_AHEAD = [dict(krylov_rank_tol=0.1), dict(frontier_tol=1e-3), dict(closure_probe=2)]
 
 
 @pytest.mark.parametrize("kw", ORACLE_AHEAD, ids=[repr(k) for k in ORACLE_AHEAD])
