@@ -10,7 +10,6 @@ selection, order 2), with its ``frames_only`` / ``frames_report`` half: a frames
 the state in the frames of the full step.
 """
 
-import numpy as np
 import pytest
 
 from oracle import models as M
