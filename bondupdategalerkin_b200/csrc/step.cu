@@ -1002,7 +1002,7 @@ std::vector<int64_t> work_ceilings(int rule, const std::vector<int64_t>& bonds, 
 
 struct Params {
   double tol_basis, tol_trunc, tol_expv, tol_krylov;
-  int order, maxdim, hermitian, rule_maxdim, root, reorth, truncate, root_maxiter, fixed_width;
+  int order, maxdim, hermitian, root, reorth, truncate, root_maxiter, fixed_width;
   double tail_factor, bond_ceiling_factor;
   int lanczos, fixed_depth;
   int dd_mode;  // 0 :rank_tail, 1 :adaptive
@@ -3056,7 +3056,6 @@ extern "C" int bug_mps_step(bug_ctx* c, int L, bug_tensor** psi_io, int* center_
     require(P.order >= 1, "order must be >= 1");
     P.maxdim = prm->maxdim > 0 ? prm->maxdim : 128;
     P.hermitian = prm->hermitian;
-    P.rule_maxdim = prm->work_ceiling_rule == 1;
     P.root = prm->root;
     P.reorth = prm->reorth;
     P.truncate = prm->truncate;
