@@ -796,17 +796,13 @@ def checked_closure(fr: KLFrames, psi, mpo, root_start, cx: Ctx, order, nrm, led
         state["nroot"] += 1
         return state["op"].apply(v)
 
-    cores = [root_start] + projected_frontiers(applyB, root_start, cx.tau, order - 1)
-    final_leak = {}
-    met, met0 = True, True
-    for d, core in enumerate(cores):
-        sw = frontier_sweep(fr, psi, mpo, core, d, cx, nrm, enrich=False)
-        lg.merge(sw["ledger"])
-        final_leak[d] = sw["leak"]
-        if d >= 1:
-            met &= sw["met"]
-        else:
-            met0 = sw["met"]
+    # the frontiers measured on the incoming frames (leak_initial / rho_initial)
+    probe = measure_frontiers(fr, psi, mpo, root_start, cx, order, nrm)
+    state["nroot"] += probe["n_root"]
+    probe["ledger"].n_root_frontier = 0  # counted once, with the closure's, below
+    lg.merge(probe["ledger"])
+    final_leak = dict(enumerate(probe["leak"]))
+    met, met0 = probe["met"], probe["met0"]
     gen0 = fr.gen
     if met:
         res = dict(passes=0, converged=True)
